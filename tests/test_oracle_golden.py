@@ -1,0 +1,72 @@
+"""Pins the CPU oracle (oracle/nsf_oracle.hpp) to the reference solver itself.
+
+The fixtures in tests/golden/*.npz were produced by the unmodified reference (tests/golden/make_golden.py,
+through oracle/ref_harness.cpp). The restatement must reproduce them bit for bit: node classification,
+ghost lists with body-intercept and image points, filter-node lists, the dt and change-norm histories and
+all twelve flow fields.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+CASES = {
+    "sphere_small": "tests/golden/cases/sphere_small.cfg",
+    "tgv_small": "tests/golden/cases/tgv_small.cfg",
+    "two_spheres": "tests/golden/cases/two_spheres.cfg",
+    "cylinder_sym": "tests/golden/cases/cylinder_sym.cfg",
+    "shipped_small": "tests/golden/cases/shipped_small.cfg",
+    "sphere48": "3d-ns-fsi_b200/cases/sphere48.cfg",
+}
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name + ".npz"))
+
+
+@pytest.mark.parametrize("name", [n for n in CASES if n != "sphere48"])
+def test_oracle_matches_reference_bitwise(name):
+    g = load(name)
+    o = po.Oracle(open(os.path.join(ROOT, CASES[name])).read())
+    assert np.array_equal(o.geometry(), g["geometry"])
+    assert np.array_equal(o.node_types(), g["types"])
+    assert o.dt == float(g["dt0"])
+    bodies = o.bodies()
+    assert len(bodies) == int(g["nbodies"])
+    for b, (gh, fl, closure) in enumerate(bodies):
+        assert np.array_equal(gh, g["ghosts_%d" % b])
+        assert np.array_equal(fl, g["filter_%d" % b])
+    done = 0
+    for d in g["dumps"]:
+        o.march(int(d) - done)
+        done = int(d)
+        assert o.t == float(g["t_%d" % d])
+        f = o.fields()
+        ref = g["fields_%d" % d]
+        assert np.array_equal(f, ref), [float(np.abs(a - b).max()) for a, b in zip(f, ref)]
+    h = o.history()
+    gh = g["history"][: len(h)]
+    assert np.array_equal(h[:, 0], gh[:, 0]) and np.array_equal(h[:, 1], gh[:, 1])
+    assert np.array_equal(h[:, 2:], gh[:, 3:])
+
+
+@pytest.mark.slow
+def test_oracle_matches_reference_sphere48_100_steps():
+    """The 48^3 single-sphere workload (inflow/outflow in x, periodic y/z, 100 RK4 steps)."""
+    g = load("sphere48")
+    o = po.Oracle(open(os.path.join(ROOT, CASES["sphere48"])).read())
+    assert np.array_equal(o.node_types(), g["types"])
+    for b, (gh, fl, closure) in enumerate(o.bodies()):
+        assert closure == 0
+        assert np.array_equal(gh, g["ghosts_%d" % b])
+        assert np.array_equal(fl, g["filter_%d" % b])
+    o.march(100)
+    f = o.fields()[:, g["sample_idx"]]
+    assert np.array_equal(f, g["fields_100"])
+    h = o.history()
+    assert np.array_equal(h[:, 1], g["history"][:, 1])
+    assert np.array_equal(h[:, 2:], g["history"][:, 3:])

@@ -1,0 +1,693 @@
+// C ABI implementation (include/nsfsi.h): the solver handle, device residency of all fields, the
+// device-side lists built from the host setup, and one captured CUDA graph per RK4 step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "nsf_device.cuh"
+#include "nsf_internal.h"
+
+using namespace nsf;
+
+struct nsf_solver {
+  nsf_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  HostSetup setup;
+  bool initialized = false;
+  bool hostOnly = false;  // device < 0: host setup only (classification queries), no GPU work
+  std::vector<void*> allocs;
+  Grid hGrid{};
+  Grid* dGrid = nullptr;
+  StepCtl* dCtl = nullptr;
+  LaunchPlan plan{};
+  cudaGraphExec_t graphExec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int launchesPerStep = 0;
+  int nSM = 0;
+  // solid inactive nodes with stored primitive values (downloads)
+  long long* dDlNode = nullptr;
+  double* dDlPrim = nullptr;    // values after the first step (periodic copies applied)
+  double* dDlPrimIc = nullptr;  // values before any step (each node's own initial values)
+  long long* dDlNodeIc = nullptr;
+  int nDl = 0, nDlIc = 0;
+  std::string err;
+};
+
+namespace {
+
+nsf_status cuda_fail(nsf_solver* s, cudaError_t e, const char* what) {
+  s->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return NSF_ERR_CUDA;
+}
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(s, e_, #call);    \
+  } while (0)
+
+template <class T>
+nsf_status dalloc(nsf_solver* s, T** p, size_t count) {
+  void* q = nullptr;
+  CK(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)));
+  s->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return NSF_OK;
+}
+template <class T>
+nsf_status upload(nsf_solver* s, T** p, const std::vector<T>& v) {
+  nsf_status st = dalloc(s, p, v.size());
+  if (st != NSF_OK) return st;
+  if (!v.empty()) CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return NSF_OK;
+}
+
+// Physical and stencil constants, each evaluated as the reference writes it (Solver.cpp:202-360).
+Consts make_consts(const nsf_config& c, const HostSetup& s) {
+  Consts K{};
+  const double dx = s.d[0], dy = s.d[1], dz = s.d[2];
+  K.gamma = c.gamma;
+  K.gm1 = c.gamma - 1;
+  K.pr = c.pr;
+  K.re = c.re;
+  K.sc1 = 1 + c.sutherlands_c2 / c.t0;
+  K.pf = 1 / (K.gm1 * c.pr);
+  K.h0 = 1. / (c.gamma - 1);
+  K.vmod = std::max(4. / 3, c.gamma / c.pr);
+  K.convLim = std::fabs(c.conv_stability_limit);
+  K.viscLim = std::fabs(c.visc_stability_limit);
+  K.m0 = c.m0;
+  K.tEnd = c.t_end;
+  K.dx = dx;
+  K.dy = dy;
+  K.dz = dz;
+  K.dxdydz = dx * dy * dz;
+  K.ax = -1. / (2 * dx);
+  K.ay = -1. / (2 * dy);
+  K.az = -1. / (2 * dz);
+  K.xm_xx = 2. / (3 * dx * dx);
+  K.xm_yy = 1. / (2 * dy * dy);
+  K.xm_zz = 1. / (2 * dz * dz);
+  K.xm_yx = -1. / (6 * dy * dx);
+  K.xm_xy = 1. / (4 * dx * dy);
+  K.xm_zx = -1. / (6 * dz * dx);
+  K.xm_xz = 1. / (4 * dx * dz);
+  K.ym_xx = 1. / (2 * dx * dx);
+  K.ym_yy = 2. / (3 * dy * dy);
+  K.ym_zz = 1. / (2 * dz * dz);
+  K.ym_xy = -1. / (6 * dx * dy);
+  K.ym_yx = 1. / (4 * dy * dx);
+  K.ym_zy = -1. / (6 * dz * dy);
+  K.ym_yz = 1. / (4 * dy * dz);
+  K.zm_xx = 1. / (2 * dx * dx);
+  K.zm_yy = 1. / (2 * dy * dy);
+  K.zm_zz = 2. / (3 * dz * dz);
+  K.zm_zx = 1. / (4 * dz * dx);
+  K.zm_xz = -1. / (6 * dx * dz);
+  K.zm_zy = 1. / (4 * dz * dy);
+  K.zm_yz = -1. / (6 * dy * dz);
+  K.e_xx23 = 2. / (3 * dx * dx);
+  K.e_xx12 = 1. / (2 * dx * dx);
+  K.e_yx6 = -1. / (6 * dy * dx);
+  K.e_zx6 = -1. / (6 * dz * dx);
+  K.e_yx4 = 1. / (4 * dy * dx);
+  K.e_zx4 = 1. / (4 * dz * dx);
+  K.e_yy12 = 1. / (2 * dy * dy);
+  K.e_yy23 = 2. / (3 * dy * dy);
+  K.e_zy6 = -1. / (6 * dz * dy);
+  K.e_zy4 = 1. / (4 * dz * dy);
+  K.e_zz12 = 1. / (2 * dz * dz);
+  K.e_zz23 = 2. / (3 * dz * dz);
+  K.endTime = c.stop_criterion == 1;
+  K.convHistory = c.conv_history;
+  K.nFilterIv = c.n_filter_intervals;
+  for (int q = 0; q < c.n_filter_intervals; ++q) K.filterIv[q] = c.filter_intervals[q];
+  K.nChange = c.n_filter_change_times;
+  for (int q = 0; q < c.n_filter_change_times; ++q) K.changeT[q] = c.filter_change_times[q];
+  return K;
+}
+
+// Solver::updateTimeStepSize at t = 0 (Solver.cpp:80-126), on the host from the initial fields.
+double initial_dt(const nsf_config& c, const HostSetup& s, const std::vector<double>& cons,
+                  const std::vector<double>& prim) {
+  const size_t N = s.N;
+  double mX = 0, mY = 0, mZ = 0, mNu = 0;
+  const double mod = std::max(4. / 3, c.gamma / c.pr);
+  for (size_t i = 0; i < N; ++i) {
+    double ci = std::sqrt((1 + c.gamma * prim[3 * N + i]) / (1 + cons[i]));
+    mX = std::max(mX, ci + std::fabs(prim[i]));
+    mY = std::max(mY, ci + std::fabs(prim[N + i]));
+    mZ = std::max(mZ, ci + std::fabs(prim[2 * N + i]));
+    mNu = std::max(mNu, prim[5 * N + i] / (cons[i] + 1) * mod);
+  }
+  double conv = std::fabs(c.conv_stability_limit) / (mX / s.d[0] + mY / s.d[1] + mZ / s.d[2]);
+  double dx2 = s.d[0] * s.d[0], dy2 = s.d[1] * s.d[1], dz2 = s.d[2] * s.d[2];
+  double visc = std::fabs(c.visc_stability_limit) / (mNu * (1 / dx2 + 1 / dy2 + 1 / dz2));
+  double dt = std::min(conv, visc);
+  if (c.stop_criterion == 1 && 0 + dt > c.t_end) dt = c.t_end - 0;
+  return dt;
+}
+
+nsf_status build_device(nsf_solver* s) {
+  const HostSetup& S = s->setup;
+  const nsf_config& cfg = s->cfg;
+  const size_t N = S.N;
+  Grid& G = s->hGrid;
+  G = Grid{};
+  G.NI = int(S.NI);
+  G.NJ = int(S.NJ);
+  G.NK = int(S.NK);
+  G.sI = (long long)(S.NJ * S.NK);
+  G.sJ = (long long)S.NK;
+  G.N = (long long)N;
+  G.C = make_consts(cfg, S);
+
+  // initial condition
+  std::vector<double> cons, prim;
+  initial_condition(cfg, S, cons, prim);
+  double* fields = nullptr;
+  nsf_status st = dalloc(s, &fields, 20 * N);
+  if (st != NSF_OK) return st;
+  CK(cudaMemset(fields, 0, 20 * N * sizeof(double)));
+  for (int b = 0; b < 3; ++b)
+    for (int f = 0; f < 5; ++f) G.bufs[b][f] = fields + (size_t(b) * 5 + f) * N;
+  for (int f = 0; f < 5; ++f) G.acc[f] = fields + (15 + size_t(f)) * N;
+  for (int f = 0; f < 5; ++f) CK(cudaMemcpy(G.bufs[0][f], cons.data() + f * N, N * sizeof(double), cudaMemcpyHostToDevice));
+
+  // node types with the filter bit, filter slots
+  std::vector<uint8_t> type = S.type;
+  for (auto& e : S.edges)
+    for (size_t i = e.owned.i0; i <= e.owned.i1; ++i)
+      for (size_t j = e.owned.j0; j <= e.owned.j1; ++j)
+        for (size_t k = e.owned.k0; k <= e.owned.k1; ++k) type[i * S.NJ * S.NK + j * S.NK + k] |= EDGE_PLANE_BIT;
+  std::vector<long long> fnode;
+  for (auto& b : S.bodies)
+    for (size_t f : b.filter) fnode.push_back((long long)f);
+  std::vector<double> fpre(2 * fnode.size());
+  for (size_t q = 0; q < fnode.size(); ++q) {
+    type[fnode[q]] |= FILTER_BIT;
+    fpre[2 * q] = cons[fnode[q]];
+    fpre[2 * q + 1] = cons[4 * N + fnode[q]];
+  }
+  uint8_t* dType;
+  if ((st = upload(s, &dType, type)) != NSF_OK) return st;
+  G.type = dType;
+  G.nFilter = int(fnode.size());
+  if (!fnode.empty()) {
+    std::vector<int> fidx(N, -1);
+    for (size_t q = 0; q < fnode.size(); ++q) fidx[fnode[q]] = int(q);
+    int* dF;
+    if ((st = upload(s, &dF, fidx)) != NSF_OK) return st;
+    G.fidx = dF;
+  }
+  long long* dFnode;
+  double *dFpre, *dFnew;
+  if ((st = upload(s, &dFnode, fnode)) != NSF_OK) return st;
+  if ((st = upload(s, &dFpre, fpre)) != NSF_OK) return st;
+  if ((st = upload(s, &dFnew, fpre)) != NSF_OK) return st;
+  G.fnode = dFnode;
+  G.fpre = dFpre;
+  G.fnew = dFnew;
+
+  // ghost nodes: cells and the points / normals the weight solve needs
+  std::vector<long long> gnode, gcell;
+  std::vector<double> pts, nrm, ipl;
+  std::vector<uint8_t> gfl;
+  for (auto& b : S.bodies)
+    for (auto& g : b.ghosts) {
+      gnode.push_back((long long)(g.i * S.NJ * S.NK + g.j * S.NK + g.k));
+      Box box;
+      surrounding_box(S, g.ip, box);
+      int64_t cs[8];
+      box_corners(S, box, cs);
+      double lo[3];
+      node_position(S, box.i0, box.j0, box.k0, lo);
+      for (int q = 0; q < 3; ++q) ipl.push_back(g.ip[q]);
+      for (int q = 0; q < 3; ++q) ipl.push_back(lo[q]);
+      for (int m = 0; m < 8; ++m) {
+        gcell.push_back(cs[m]);
+        const size_t cn = size_t(cs[m]);
+        if (S.type[cn] == SOLID_GHOST) {
+          const GhostRec& og = b.ghosts[b.ghostIndex.at(cn)];
+          double d[3] = {og.ip[0] - og.bi[0], og.ip[1] - og.bi[1], og.ip[2] - og.bi[2]};
+          double len = std::sqrt(std::pow(d[0], 2) + std::pow(d[1], 2) + std::pow(d[2], 2));
+          for (int q = 0; q < 3; ++q) pts.push_back(og.bi[q]);
+          for (int q = 0; q < 3; ++q) nrm.push_back(d[q] / len);
+          gfl.push_back(1);
+        } else {
+          double p[3];
+          size_t ci = cn / (S.NJ * S.NK), cj = cn % (S.NJ * S.NK) / S.NK, ck = cn % S.NK;
+          node_position(S, ci, cj, ck, p);
+          for (int q = 0; q < 3; ++q) pts.push_back(p[q]);
+          for (int q = 0; q < 3; ++q) nrm.push_back(0);
+          gfl.push_back(0);
+        }
+      }
+    }
+  G.nGhost = int(gnode.size());
+  long long *dGnode, *dGcell;
+  double *dPts, *dNrm, *dIpl, *dW;
+  uint8_t* dFl;
+  if ((st = upload(s, &dGnode, gnode)) != NSF_OK) return st;
+  if ((st = upload(s, &dGcell, gcell)) != NSF_OK) return st;
+  if ((st = upload(s, &dPts, pts)) != NSF_OK) return st;
+  if ((st = upload(s, &dNrm, nrm)) != NSF_OK) return st;
+  if ((st = upload(s, &dIpl, ipl)) != NSF_OK) return st;
+  if ((st = upload(s, &dFl, gfl)) != NSF_OK) return st;
+  if ((st = dalloc(s, &dW, 16 * gnode.size())) != NSF_OK) return st;
+  launch_ghost_weights(G.nGhost, dPts, dNrm, dFl, dIpl, S.d[0], S.d[1], S.d[2], dW, s->stream);
+  CK(cudaGetLastError());
+  G.gnode = dGnode;
+  G.gcell = dGcell;
+  G.gw = dW;
+
+  // solid nodes: copy list (ghost + inactive); inactive primitive values as the reference holds them
+  std::vector<long long> snode, inode, dlNode, dlNodeIc;
+  std::vector<double> iprim, dlPrim, dlPrimIc;
+  // owner edge of every boundary-plane node, to follow periodic copies of solid nodes
+  std::vector<int> edgeOf(N, -1);
+  for (size_t e = 0; e < S.edges.size(); ++e) {
+    const Box& b = S.edges[e].owned;
+    for (size_t i = b.i0; i <= b.i1; ++i)
+      for (size_t j = b.j0; j <= b.j1; ++j)
+        for (size_t k = b.k0; k <= b.k1; ++k) edgeOf[i * S.NJ * S.NK + j * S.NK + k] = int(e);
+  }
+  for (size_t n = 0; n < N; ++n) {
+    uint8_t t = S.type[n];
+    if (t != SOLID_GHOST && t != SOLID_INACTIVE) continue;
+    snode.push_back((long long)n);
+    if (t != SOLID_INACTIVE) continue;
+    // Follow periodic copies to the node whose primitive values land here (Boundary.cpp:344-367).
+    size_t src = n;
+    bool dynamic = false;
+    for (int hop = 0; hop < 4 && edgeOf[src] >= 0; ++hop) {
+      const EdgeBC& e = S.edges[edgeOf[src]];
+      if (e.bc != NSF_BC_PERIODIC) {
+        dynamic = true;
+        break;
+      }
+      size_t ijk[3] = {src / (S.NJ * S.NK), src % (S.NJ * S.NK) / S.NK, src % S.NK};
+      size_t nAx[3] = {S.NI, S.NJ, S.NK};
+      ijk[e.axis] = e.side == 0 ? nAx[e.axis] - 2 : 1;
+      src = ijk[0] * S.NJ * S.NK + ijk[1] * S.NK + ijk[2];
+    }
+    if (S.type[src] != SOLID_INACTIVE) dynamic = true;
+    inode.push_back((long long)n);
+    dlNodeIc.push_back((long long)n);
+    for (int q = 0; q < 7; ++q) dlPrimIc.push_back(prim[q * N + n]);
+    if (dynamic) {
+      // values copied with the conserved ones from a node whose primitives follow its conserved values
+      for (int q = 0; q < 5; ++q) iprim.push_back(std::nan(""));
+    } else {
+      iprim.push_back(prim[src]);
+      iprim.push_back(prim[N + src]);
+      iprim.push_back(prim[2 * N + src]);
+      iprim.push_back(prim[3 * N + src]);
+      iprim.push_back(prim[5 * N + src]);
+      dlNode.push_back((long long)n);
+      for (int q = 0; q < 7; ++q) dlPrim.push_back(prim[q * N + src]);
+    }
+  }
+  G.nSolid = int(snode.size());
+  G.nInactive = int(inode.size());
+  long long *dS, *dI;
+  double* dIp;
+  if ((st = upload(s, &dS, snode)) != NSF_OK) return st;
+  if ((st = upload(s, &dI, inode)) != NSF_OK) return st;
+  if ((st = upload(s, &dIp, iprim)) != NSF_OK) return st;
+  G.snode = dS;
+  G.inode = dI;
+  G.iprim = dIp;
+  s->nDl = int(dlNode.size());
+  if ((st = upload(s, &s->dDlNode, dlNode)) != NSF_OK) return st;
+  if ((st = upload(s, &s->dDlPrim, dlPrim)) != NSF_OK) return st;
+  s->nDlIc = int(dlNodeIc.size());
+  if ((st = upload(s, &s->dDlNodeIc, dlNodeIc)) != NSF_OK) return st;
+  if ((st = upload(s, &s->dDlPrimIc, dlPrimIc)) != NSF_OK) return st;
+
+  // boundary conditions in application order
+  G.nEdge = int(S.edges.size());
+  for (size_t e = 0; e < S.edges.size(); ++e) {
+    G.eAxis[e] = S.edges[e].axis;
+    G.eSide[e] = S.edges[e].side;
+    G.eBc[e] = S.edges[e].bc;
+    const Box& b = S.edges[e].owned;
+    int bx[6] = {int(b.i0), int(b.i1), int(b.j0), int(b.j1), int(b.k0), int(b.k1)};
+    std::memcpy(G.eBox[e], bx, sizeof bx);
+  }
+
+  // launch plan: stage work items (tile x i-chunk), grids of the small kernels
+  LaunchPlan& L = s->plan;
+  L = LaunchPlan{};
+  L.nSM = s->nSM;
+  CK(cudaError_t(stage_configure()));
+  const int occ = std::max(1, stage_occupancy());
+  const int TJ = stage_tile_j(), TK = stage_tile_k();
+  const int nj = int((S.NJ - 2 + TJ - 1) / TJ), nk = int((S.NK - 2 + TK - 1) / TK);
+  const int tiles = nj * nk, planes = int(S.NI - 2);
+  const int slots = s->nSM * occ;
+  const int chunks = std::max(1, std::min(planes, (8 * slots + tiles - 1) / tiles));
+  const int clen = (planes + chunks - 1) / chunks;
+  std::vector<StageItem> items;
+  for (int c0 = 1; c0 <= planes; c0 += clen)
+    for (int tj = 0; tj < nj; ++tj)
+      for (int tk = 0; tk < nk; ++tk)
+        items.push_back(StageItem{1 + tj * TJ, 1 + tk * TK, c0, std::min(planes, c0 + clen - 1)});
+  L.nItems = int(items.size());
+  L.stageBlocks = std::min(L.nItems, slots);
+  if ((st = upload(s, &L.items, items)) != NSF_OK) return st;
+  for (int a = 0; a < 3; ++a) {
+    int n1 = 1, n2 = 1;
+    for (auto& e : S.edges)
+      if (e.axis == a) {
+        const Box& b = e.owned;
+        size_t lo[3] = {b.i0, b.j0, b.k0}, hi[3] = {b.i1, b.j1, b.k1};
+        int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
+        n1 = std::max(n1, int(hi[ax1] - lo[ax1] + 1));
+        n2 = std::max(n2, int(hi[ax2] - lo[ax2] + 1));
+      }
+    L.edgeGrid[a][0] = (n2 + 31) / 32;
+    L.edgeGrid[a][1] = (n1 + 7) / 8;
+    L.edgeGrid[a][2] = 2;
+  }
+  L.hasFilter = G.nFilter > 0;
+  L.filterBlocks = std::max(1, std::min(s->nSM, (G.nFilter + 255) / 256));
+  L.hasSolid = G.nSolid > 0;
+  L.solidBlocks = std::max(1, std::min(4 * s->nSM, (G.nSolid + 255) / 256));
+  const int ghostWork = G.nGhost + G.nFilter + G.nInactive;
+  L.hasGhostWork = ghostWork > 0;
+  L.ghostBlocks = std::max(1, std::min(4 * s->nSM, (ghostWork + 255) / 256));
+  L.gfBlocks = 4 * s->nSM;
+  L.nSlots = L.stageBlocks + (L.hasFilter ? L.filterBlocks : 0);
+  double* dNorm;
+  if ((st = dalloc(s, &dNorm, 5 * size_t(L.nSlots))) != NSF_OK) return st;
+  CK(cudaMemset(dNorm, 0, 5 * size_t(L.nSlots) * sizeof(double)));
+  G.normPart = dNorm;
+  G.nNormSlots = L.nSlots;
+  double* dHist;
+  if ((st = dalloc(s, &dHist, 7 * size_t(MAX_HIST))) != NSF_OK) return st;
+  G.hist = dHist;
+
+  // control block
+  StepCtl ctl{};
+  ctl.t = 0;
+  ctl.dt = initial_dt(cfg, S, cons, prim);
+  ctl.level = 0;
+  for (int f = 0; f < 5; ++f) {
+    ctl.perm[f][0] = 0;
+    ctl.perm[f][1] = 1;
+    ctl.perm[f][2] = 2;
+  }
+  if ((st = dalloc(s, &s->dCtl, 1)) != NSF_OK) return st;
+  CK(cudaMemcpy(s->dCtl, &ctl, sizeof ctl, cudaMemcpyHostToDevice));
+  G.ctl = s->dCtl;
+  if ((st = dalloc(s, &s->dGrid, 1)) != NSF_OK) return st;
+  CK(cudaMemcpy(s->dGrid, &G, sizeof G, cudaMemcpyHostToDevice));
+  CK(cudaStreamSynchronize(s->stream));
+
+  // one step as a CUDA graph
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  s->launchesPerStep = enqueue_step(s->dGrid, L, s->stream);
+  CK(cudaStreamEndCapture(s->stream, &s->graph));
+  CK(cudaGraphInstantiate(&s->graphExec, s->graph, 0));
+  return NSF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nsf_status nsf_create(const nsf_config* cfg, int32_t device, nsf_solver** out) {
+  if (!cfg || !out) return NSF_ERR_ARG;
+  *out = nullptr;
+  auto* s = new nsf_solver;
+  s->cfg = *cfg;
+  s->device = device;
+  if (device < 0) {
+    s->hostOnly = true;
+    *out = s;
+    return NSF_OK;
+  }
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count <= device || device < 0) {
+    s->err = "no CUDA device available for the B200 time-marching path";
+    *out = s;
+    return NSF_ERR_CUDA;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+    s->err = "device is not an sm_100 (Blackwell B200) GPU; this library is built for sm_100a only";
+    *out = s;
+    return NSF_ERR_CUDA;
+  }
+  s->nSM = prop.multiProcessorCount;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    s->err = "could not create a CUDA stream";
+    *out = s;
+    return NSF_ERR_CUDA;
+  }
+  *out = s;
+  return NSF_OK;
+}
+
+nsf_status nsf_initialize(nsf_solver* s) {
+  if (!s) return NSF_ERR_ARG;
+  if (s->initialized) {
+    s->err = "nsf_initialize called twice";
+    return NSF_ERR_STATE;
+  }
+  std::string err;
+  nsf_status st = build_setup(s->cfg, s->setup, err);
+  if (st != NSF_OK) {
+    s->err = err;
+    return st;
+  }
+  if (s->hostOnly) {
+    s->initialized = true;
+    return NSF_OK;
+  }
+  if (!s->stream) return NSF_ERR_CUDA;
+  CK(cudaSetDevice(s->device));
+  st = build_device(s);
+  if (st != NSF_OK) return st;
+  s->initialized = true;
+  return NSF_OK;
+}
+
+nsf_status nsf_march(nsf_solver* s, uint64_t nsteps) {
+  if (!s) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) {
+    s->err = s->hostOnly ? "host-only handle (device -1) cannot march" : "nsf_march before nsf_initialize";
+    return NSF_ERR_STATE;
+  }
+  CK(cudaSetDevice(s->device));
+  for (uint64_t q = 0; q < nsteps; ++q) CK(cudaGraphLaunch(s->graphExec, s->stream));
+  return NSF_OK;
+}
+
+nsf_status nsf_sync(nsf_solver* s) {
+  if (!s || !s->initialized || s->hostOnly) return s ? NSF_ERR_STATE : NSF_ERR_ARG;
+  CK(cudaStreamSynchronize(s->stream));
+  StepCtl ctl;
+  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  if (ctl.nonFinite) {
+    s->err = "Non-finite value found in the conserved variables";
+    return NSF_ERR_NONFINITE;
+  }
+  return NSF_OK;
+}
+
+nsf_status nsf_get_time(nsf_solver* s, double* t, uint64_t* level, double* dt) {
+  if (!s || !s->initialized || s->hostOnly) return s ? NSF_ERR_STATE : NSF_ERR_ARG;
+  CK(cudaStreamSynchronize(s->stream));
+  StepCtl ctl;
+  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  if (t) *t = ctl.t;
+  if (level) *level = ctl.level;
+  if (dt) *dt = ctl.dt;
+  return NSF_OK;
+}
+
+nsf_status nsf_download(nsf_solver* s, uint32_t mask, double* host) {
+  if (!s || !host) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  CK(cudaStreamSynchronize(s->stream));
+  StepCtl ctl;
+  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  const size_t N = s->setup.N;
+  size_t outF = 0;
+  for (int f = 0; f < 5; ++f)
+    if (mask & (1u << f)) CK(cudaMemcpy(host + (outF++) * N, s->hGrid.bufs[ctl.perm[f][0]][f], N * sizeof(double),
+                                        cudaMemcpyDeviceToHost));
+  if (mask & 0xFE0u) {
+    double* tmp = nullptr;
+    CK(cudaMalloc(&tmp, 7 * N * sizeof(double)));
+    if (ctl.level == 0)
+      launch_download_prims(s->dGrid, (long long)N, tmp, s->dDlNodeIc, s->dDlPrimIc, s->nDlIc, s->nSM, s->stream);
+    else
+      launch_download_prims(s->dGrid, (long long)N, tmp, s->dDlNode, s->dDlPrim, s->nDl, s->nSM, s->stream);
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    for (int f = 5; f < 12 && e == cudaSuccess; ++f)
+      if (mask & (1u << f)) e = cudaMemcpy(host + (outF++) * N, tmp + (f - 5) * N, N * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(s, e, "download primitive fields");
+  }
+  return NSF_OK;
+}
+
+nsf_status nsf_upload_conserved(nsf_solver* s, const double* host) {
+  if (!s || !host) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  CK(cudaStreamSynchronize(s->stream));
+  StepCtl ctl;
+  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  const size_t N = s->setup.N;
+  for (int f = 0; f < 5; ++f)
+    CK(cudaMemcpyAsync(s->hGrid.bufs[ctl.perm[f][0]][f], host + f * N, N * sizeof(double), cudaMemcpyHostToDevice,
+                       s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return NSF_OK;
+}
+
+nsf_status nsf_get_node_types(nsf_solver* s, uint8_t* out) {
+  if (!s || !out) return NSF_ERR_ARG;
+  if (!s->initialized) return NSF_ERR_STATE;
+  std::memcpy(out, s->setup.type.data(), s->setup.N);
+  return NSF_OK;
+}
+
+nsf_status nsf_get_num_bodies(nsf_solver* s, uint32_t* nb) {
+  if (!s || !nb) return NSF_ERR_ARG;
+  if (!s->initialized) return NSF_ERR_STATE;
+  *nb = uint32_t(s->setup.bodies.size());
+  return NSF_OK;
+}
+
+nsf_status nsf_get_body_counts(nsf_solver* s, uint32_t body, uint64_t* ng, uint64_t* nf, uint64_t* cl) {
+  if (!s) return NSF_ERR_ARG;
+  if (!s->initialized) return NSF_ERR_STATE;
+  if (body >= s->setup.bodies.size()) return NSF_ERR_ARG;
+  const BodyRec& b = s->setup.bodies[body];
+  if (ng) *ng = b.ghosts.size();
+  if (nf) *nf = b.filter.size();
+  if (cl) *cl = b.closureAdded;
+  return NSF_OK;
+}
+
+nsf_status nsf_get_ghosts(nsf_solver* s, uint32_t body, double* out) {
+  if (!s || !out) return NSF_ERR_ARG;
+  if (!s->initialized) return NSF_ERR_STATE;
+  if (body >= s->setup.bodies.size()) return NSF_ERR_ARG;
+  const BodyRec& b = s->setup.bodies[body];
+  for (size_t q = 0; q < b.ghosts.size(); ++q) {
+    const GhostRec& g = b.ghosts[q];
+    double row[9] = {double(g.i), double(g.j), double(g.k), g.bi[0], g.bi[1], g.bi[2], g.ip[0], g.ip[1], g.ip[2]};
+    std::memcpy(out + 9 * q, row, sizeof row);
+  }
+  return NSF_OK;
+}
+
+nsf_status nsf_get_filter_nodes(nsf_solver* s, uint32_t body, uint64_t* out) {
+  if (!s || !out) return NSF_ERR_ARG;
+  if (!s->initialized) return NSF_ERR_STATE;
+  if (body >= s->setup.bodies.size()) return NSF_ERR_ARG;
+  const BodyRec& b = s->setup.bodies[body];
+  for (size_t q = 0; q < b.filter.size(); ++q) out[q] = b.filter[q];
+  return NSF_OK;
+}
+
+nsf_status nsf_get_history(nsf_solver* s, uint64_t first, uint64_t count, double* out, uint64_t* available) {
+  if (!s) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  CK(cudaStreamSynchronize(s->stream));
+  StepCtl ctl;
+  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  if (available) *available = ctl.level;
+  if (!out || !count) return NSF_OK;
+  if (first + count > ctl.level || ctl.level - first > (uint64_t)MAX_HIST) {
+    s->err = "history rows out of range (only the last 2^20 steps are kept on the device)";
+    return NSF_ERR_ARG;
+  }
+  for (uint64_t q = 0; q < count; ++q)
+    CK(cudaMemcpy(out + 7 * q, s->hGrid.hist + 7 * ((first + q) % MAX_HIST), 7 * sizeof(double), cudaMemcpyDeviceToHost));
+  return NSF_OK;
+}
+
+nsf_status nsf_march_timed(nsf_solver* s, uint64_t nsteps, double* elapsed_ms) {
+  if (!s || !elapsed_ms) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  CK(cudaSetDevice(s->device));
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, s->stream));
+  for (uint64_t q = 0; q < nsteps; ++q) CK(cudaGraphLaunch(s->graphExec, s->stream));
+  CK(cudaEventRecord(b, s->stream));
+  CK(cudaEventSynchronize(b));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *elapsed_ms = ms;
+  return NSF_OK;
+}
+
+nsf_status nsf_profile_steps(nsf_solver* s, uint64_t nsteps, double* stage_ms, double* step_ms) {
+  if (!s || !stage_ms || !step_ms) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  CK(cudaSetDevice(s->device));
+  std::vector<cudaEvent_t> ev(2 * 4 * nsteps + 2);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(ev[0], s->stream));
+  for (uint64_t q = 0; q < nsteps; ++q) {
+    cudaEvent_t* se = ev.data() + 2 + 8 * q;
+    enqueue_step_profiled(s->dGrid, s->plan, s->stream, se);
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ev[1], s->stream));
+  CK(cudaEventSynchronize(ev[1]));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+  *step_ms = ms / double(nsteps ? nsteps : 1);
+  for (int st = 0; st < 4; ++st) {
+    double tot = 0;
+    for (uint64_t q = 0; q < nsteps; ++q) {
+      float m = 0;
+      CK(cudaEventElapsedTime(&m, ev[2 + 8 * q + 2 * st], ev[2 + 8 * q + 2 * st + 1]));
+      tot += m;
+    }
+    stage_ms[st] = tot / double(nsteps ? nsteps : 1);
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return NSF_OK;
+}
+
+nsf_status nsf_launches_per_step(nsf_solver* s, uint64_t* n) {
+  if (!s || !n) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  *n = uint64_t(s->launchesPerStep);
+  return NSF_OK;
+}
+
+const char* nsf_last_error(nsf_solver* s) { return s ? s->err.c_str() : "null solver handle"; }
+
+void nsf_destroy(nsf_solver* s) {
+  if (!s) return;
+  if (s->stream) {
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+  }
+  if (s->graphExec) cudaGraphExecDestroy(s->graphExec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+}  // extern "C"

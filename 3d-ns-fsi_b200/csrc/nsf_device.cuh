@@ -1,0 +1,138 @@
+// Device-side data structures shared by the kernels in nsf_kernels.cu and the host driver.
+//
+// Buffer model. The reference keeps two conserved-variable buffers, `conservedVariables` (the stage
+// target, written in place by every stage) and `conservedVariablesOld` (U0, read only), and swaps them
+// at the start of each step (Mesh::swapConservedVariables, Mesh.cpp:144-151). Values at non-interior
+// nodes therefore persist across steps and are read stale by the near-body filter and the periodic
+// copies. A fused stencil kernel cannot write its input in place, so here each field has THREE
+// physical buffers whose roles (cons / old / scratch) rotate: stage s reads I_s and writes O_s, with
+// O_1 = O_3 = the reference's `conservedVariables` and O_2 = O_4 = scratch; before the boundary
+// conditions of stages 2-4 the solid-node values of I_s are copied into O_s, so every buffer holds,
+// node for node, what the reference's buffer holds at that point. Roles are kept in device memory
+// (StepCtl) so that one captured CUDA graph serves every step, including the ones where the global
+// density filter swaps the density buffers (Mesh::applyFilter_ifAppropriate, Mesh.cpp:108-140).
+#ifndef NSF_DEVICE_CUH
+#define NSF_DEVICE_CUH
+
+#include <cstdint>
+
+namespace nsf {
+
+constexpr int MAX_HIST = 1 << 20;  // per-step history rows kept on the device (ring)
+
+// Physical constants and the reference's precomputed stencil coefficients (Solver.cpp:202-360),
+// evaluated on the host exactly as the reference writes them.
+struct Consts {
+  double gamma, gm1, pr, re, sc1, pf, h0, vmod, convLim, viscLim, m0, tEnd;
+  double dx, dy, dz, dxdydz;
+  // continuity / inviscid: -1/(2d)
+  double ax, ay, az;
+  // x-momentum: 2/(3dx^2), 1/(2dy^2), 1/(2dz^2), -1/(6dydx), 1/(4dxdy), -1/(6dzdx), 1/(4dxdz)
+  double xm_xx, xm_yy, xm_zz, xm_yx, xm_xy, xm_zx, xm_xz;
+  // y-momentum: 1/(2dx^2), 2/(3dy^2), 1/(2dz^2), -1/(6dxdy), 1/(4dydx), -1/(6dzdy), 1/(4dydz)
+  double ym_xx, ym_yy, ym_zz, ym_xy, ym_yx, ym_zy, ym_yz;
+  // z-momentum: 1/(2dx^2), 1/(2dy^2), 2/(3dz^2), 1/(4dzdx), -1/(6dxdz), 1/(4dzdy), -1/(6dydz)
+  double zm_xx, zm_yy, zm_zz, zm_zx, zm_xz, zm_zy, zm_yz;
+  // energy: 2/(3dx^2), 1/(2dx^2), -1/(6dydx), -1/(6dzdx), 1/(4dydx), 1/(4dzdx), 1/(2dy^2), 2/(3dy^2),
+  //         -1/(6dzdy), 1/(4dzdy), 1/(2dz^2), 2/(3dz^2)
+  double e_xx23, e_xx12, e_yx6, e_zx6, e_yx4, e_zx4, e_yy12, e_yy23, e_zy6, e_zy4, e_zz12, e_zz23;
+  int endTime, convHistory;
+  int nFilterIv, nChange;
+  unsigned filterIv[16];
+  double changeT[16];
+};
+
+// Per-step control block in device memory, updated by the prologue / finalize kernels.
+struct StepCtl {
+  // persistent state
+  double t;               // simulated time (Simulation::t)
+  double dt;              // dt of the coming step (Solver::dt)
+  unsigned long long level;  // timeLevel
+  int perm[5][3];         // per field: physical buffer of [cons, old, scratch]
+  int nonFinite;          // sticky NaN/Inf flag (Mesh::checkFinity)
+  int rhoIcBuffer;        // unused placeholder for layout stability
+  // per-step decisions (prologue)
+  int active;             // 0: step is a no-op (end_time reached)
+  int filterNow;          // global density filter on this step
+  double* gfSrc;          // filter input (the reference's conservedVariables.rho before the swaps)
+  double* gfDst;          // filter output (conservedVariablesOld.rho before the swaps)
+  double* U0[5];
+  double* I[4][5];
+  double* O[4][5];
+  double* R[4];           // density used for the primitive variables of the stage input
+  int copyMask[4];        // fields whose solid-node values are copied I -> O before the stage's BCs
+  double stageT[4];       // boundary-condition time of each stage
+  double dtUsed;
+  // stage-4 reductions
+  unsigned long long mx[4];  // bit patterns of non-negative maxima: c+|u|, c+|v|, c+|w|, mu/(1+rho)*mod
+};
+
+// Everything a kernel needs to know about one grid (one ensemble member).
+struct Grid {
+  int NI, NJ, NK;
+  long long sI, sJ, N;
+  Consts C;
+  StepCtl* ctl;
+  double* bufs[3][5];
+  double* acc[5];
+  const uint8_t* type;    // NodeTypeEnum | FILTER_BIT
+  const int* fidx;        // node -> filter slot (only read where FILTER_BIT is set)
+  double* fpre;           // [F][2] pre-filter rho, rho_E of the last near-body filter
+  double* fnew;           // [F][2] filtered values (written back after the ghost update)
+  const long long* fnode; // [F] node of each filter slot
+  int nFilter;
+  // ghost nodes
+  int nGhost;
+  const long long* gnode;   // [G]
+  const long long* gcell;   // [G][8]
+  const double* gw;         // [G][16]: Neumann weights (rho, rho_E) then Dirichlet weights (momenta)
+  // solid-node copy list (ghost + inactive) and the inactive nodes' stored primitive values
+  int nSolid;
+  const long long* snode;   // [S]
+  int nInactive;
+  const long long* inode;   // [Q] inactive nodes (not on a boundary plane)
+  const double* iprim;      // [Q][5] u, v, w, p, mu as the reference holds them
+  // boundary conditions in application order
+  int nEdge;
+  int eAxis[6], eSide[6], eBc[6];
+  int eBox[6][6];           // owned box i0,i1,j0,j1,k0,k1
+  // reductions
+  double* normPart;         // [nNormSlots][5]
+  int nNormSlots;
+  double* hist;             // [MAX_HIST][7]
+};
+
+struct StageItem {
+  int j0, k0, i0, i1;  // tile origin (first computed j, k) and inclusive i range
+};
+
+// Launch geometry of one step, fixed at initialisation.
+struct LaunchPlan {
+  int nSM;
+  int stageBlocks;
+  int nItems;
+  StageItem* items;  // device
+  int edgeGrid[3][3];  // per axis: grid x, y, z
+  int filterBlocks, ghostBlocks, solidBlocks, gfBlocks;
+  int nSlots;
+  bool hasBodies;
+  bool hasFilter, hasGhostWork, hasSolid;
+};
+
+// Host entry points of nsf_kernels.cu.
+size_t stage_smem_bytes();
+int stage_configure();
+int stage_tile_j();
+int stage_tile_k();
+int stage_occupancy();
+int enqueue_step(Grid* dg, const LaunchPlan& L, void* stream);
+// Same sequence, launched eagerly, with events recorded around each of the four stage kernels
+// (events[2*s], events[2*s+1]); used for per-kernel timing.
+int enqueue_step_profiled(Grid* dg, const LaunchPlan& L, void* stream, void* events);
+void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,
+                          double dx, double dy, double dz, double* w, void* stream);
+void launch_download_prims(const Grid* dg, long long N, double* out, const long long* inodes, const double* ip7,
+                           int nInactive, int nSM, void* stream);
+
+}  // namespace nsf
+#endif

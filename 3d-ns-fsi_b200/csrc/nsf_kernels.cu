@@ -1,0 +1,998 @@
+// CUDA kernels (sm_100a, FP64) of the RK4 time-marching path. One RK4 step (Solver::marchTimeStep,
+// Solver.cpp:130-167) is the launch sequence enqueue_step() builds:
+//
+//   k_prologue            stop criterion, filter decision, buffer roles        (Solver.cpp:133-135)
+//   k_density_filter      global 2nd-order density filter, rare              (Mesh.cpp:108-140)
+//   4 x { k_stage         fused RHS + primitive recompute + RK4 combine      (Solver.cpp:141-159, 170-507)
+//         k_solid_copy    stale solid-node values, I -> O                    (buffer semantics, see nsf_device.cuh)
+//         k_edge_bc x3    outlet/inlet, then y faces, then z faces           (Boundary.cpp:250-417)
+//         k_body_filter   near-body filter of rho, rho_E                     (Boundary.cpp:618-652)
+//         k_ghost         image-point interpolation with cached weights      (Boundary.cpp:427-457, 655-883) }
+//   k_finalize            change norms, next dt, time, history              (Solver.cpp:80-126, 510-530)
+//
+// Stage 4 also carries the dt maxima, the change norms and the NaN check as block reductions, so no
+// kernel re-reads the fields for them.
+#include <cfloat>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "nsf_device.cuh"
+#include "nsf_internal.h"
+
+namespace nsf {
+
+// ----------------------------------------------------------------------------------------------
+// Thermodynamics (updatePrimitiveVariables, Solver.cpp:446-479; derive*, FlowVariableGroupStructs.h).
+// pow(1+T, 1.5) is evaluated as x*sqrt(x); the three divisions by (1+rho) share one reciprocal.
+// Both differ from the reference by rounding only.
+struct Prim {
+  double u, v, w, p, T, mu, ka;
+};
+
+__device__ __forceinline__ Prim prims_of(const Consts& C, double rho, double ru, double rv, double rw, double rE) {
+  Prim q;
+  const double r1 = 1.0 / (rho + 1.0);
+  q.u = ru * r1;
+  q.v = rv * r1;
+  q.w = rw * r1;
+  q.p = C.gm1 * (rE - (rho + 1.0) * 0.5 * (q.u * q.u + q.v * q.v + q.w * q.w));
+  q.T = (C.gamma * q.p - rho) * r1;
+  const double x = 1.0 + q.T;
+  q.mu = x * sqrt(x) * C.sc1 / (C.re * (q.T + C.sc1));
+  q.ka = q.mu * C.pf;
+  return q;
+}
+
+__device__ __forceinline__ double mu_of_T(const Consts& C, double T) {
+  const double x = 1.0 + T;
+  return x * sqrt(x) * C.sc1 / (C.re * (T + C.sc1));
+}
+
+// Conserved values from primitive values (deriveConservedVariables, FlowVariableGroupStructs.h:152-161).
+__device__ __forceinline__ void cons_of(const Consts& C, double u, double v, double w, double p, double T,
+                                        double out[5]) {
+  const double rho = (C.gamma * p - T) / (1.0 + T);
+  out[0] = rho;
+  out[1] = (1.0 + rho) * u;
+  out[2] = (1.0 + rho) * v;
+  out[3] = (1.0 + rho) * w;
+  out[4] = p / C.gm1 + (1.0 + rho) * 0.5 * (u * u + v * v + w * w);
+}
+
+// Non-negative doubles compare like their bit patterns, so maxima reduce with integer atomicMax.
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
+  if (v > 0) atomicMax(a, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+struct DtAcc {
+  double sx = 0, sy = 0, sz = 0, nu = 0;
+  __device__ __forceinline__ void add(const Consts& C, double rho, double u, double v, double w, double p, double mu) {
+    // getInviscidTimeStepLimit / getViscousTimeStepLimit terms, Solver.cpp:100-122
+    const double c = sqrt((1.0 + C.gamma * p) / (1.0 + rho));
+    sx = fmax(sx, c + fabs(u));
+    sy = fmax(sy, c + fabs(v));
+    sz = fmax(sz, c + fabs(w));
+    nu = fmax(nu, mu / (rho + 1.0) * C.vmod);
+  }
+};
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Linear thread index and thread count of the block (1-D or 2-D blocks).
+__device__ __forceinline__ int block_tid() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+__device__ __forceinline__ int block_threads() { return blockDim.x * blockDim.y * blockDim.z; }
+
+// Block-wide reduction of the four dt maxima into ctl->mx (order independent). Thread count % 32 == 0.
+__device__ void flush_dt(StepCtl* ctl, DtAcc a, double* scratch /*[4*32]*/) {
+  const int tid = block_tid(), lane = tid & 31, wid = tid >> 5, nw = block_threads() >> 5;
+  double v[4] = {warp_max(a.sx), warp_max(a.sy), warp_max(a.sz), warp_max(a.nu)};
+  __syncthreads();
+  if (lane == 0)
+    for (int q = 0; q < 4; ++q) scratch[q * 32 + wid] = v[q];
+  __syncthreads();
+  if (wid == 0) {
+    for (int q = 0; q < 4; ++q) {
+      double m = lane < nw ? scratch[q * 32 + lane] : 0.0;
+      m = warp_max(m);
+      if (lane == 0) atomic_max_pos(&ctl->mx[q], m);
+    }
+  }
+  __syncthreads();
+}
+
+// Block-wide sums of the five change-norm partials into a per-block slot (fixed order: deterministic).
+__device__ void flush_norms(double* slot, const double s[5], double* scratch /*[5*32]*/) {
+  const int tid = block_tid(), lane = tid & 31, wid = tid >> 5, nw = block_threads() >> 5;
+  double v[5];
+  for (int q = 0; q < 5; ++q) v[q] = warp_sum(s[q]);
+  __syncthreads();
+  if (lane == 0)
+    for (int q = 0; q < 5; ++q) scratch[q * 32 + wid] = v[q];
+  __syncthreads();
+  if (wid == 0)
+    for (int q = 0; q < 5; ++q) {
+      double m = lane < nw ? scratch[q * 32 + lane] : 0.0;
+      m = warp_sum(m);
+      if (lane == 0) slot[q] = m;
+    }
+  __syncthreads();
+}
+
+// ----------------------------------------------------------------------------------------------
+// Prologue: Simulation::checkStoppingCriterion (end_time), Mesh::checkFilterCondition (Mesh.cpp:85-103),
+// the buffer swaps of Mesh.cpp:133-151 expressed as role changes, and per-stage buffer roles.
+__global__ void k_prologue(Grid* g) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  StepCtl* c = g->ctl;
+  const Consts& C = g->C;
+  c->active = C.endTime ? (c->t < C.tEnd) : 1;
+  if (!c->active) return;
+  int counter = 0;
+  for (int q = 0; q < C.nChange; ++q)
+    if (c->t > C.changeT[q]) ++counter;
+  int filt = 0;
+  if (counter < C.nFilterIv) {
+    unsigned iv = C.filterIv[counter];
+    if (iv > 0 && (c->level + 1) % iv == 0) filt = 1;
+  }
+  c->filterNow = filt;
+  int cons[5], old[5], scr[5];
+  for (int f = 0; f < 5; ++f) {
+    cons[f] = c->perm[f][0];
+    old[f] = c->perm[f][1];
+    scr[f] = c->perm[f][2];
+  }
+  if (filt) {  // the filter writes rho into the old buffer, then the two rho buffers trade places
+    c->gfSrc = g->bufs[cons[0]][0];
+    c->gfDst = g->bufs[old[0]][0];
+    int t = cons[0];
+    cons[0] = old[0];
+    old[0] = t;
+  }
+  for (int f = 0; f < 5; ++f) {  // swapConservedVariables
+    int t = cons[f];
+    cons[f] = old[f];
+    old[f] = t;
+  }
+  int A[5], B[5];
+  for (int f = 0; f < 5; ++f) {
+    A[f] = cons[f];
+    B[f] = scr[f];
+  }
+  if (filt) {  // stage 1 cannot write the unfiltered density it reads: it writes the scratch buffer
+    A[0] = scr[0];
+    B[0] = cons[0];
+  }
+  for (int f = 0; f < 5; ++f) {
+    c->U0[f] = g->bufs[old[f]][f];
+    c->I[0][f] = g->bufs[old[f]][f];
+    c->O[0][f] = g->bufs[A[f]][f];
+    c->I[1][f] = g->bufs[A[f]][f];
+    c->O[1][f] = g->bufs[B[f]][f];
+    c->I[2][f] = g->bufs[B[f]][f];
+    c->O[2][f] = g->bufs[A[f]][f];
+    c->I[3][f] = g->bufs[A[f]][f];
+    c->O[3][f] = g->bufs[B[f]][f];
+  }
+  c->R[0] = filt ? g->bufs[cons[0]][0] : g->bufs[old[0]][0];
+  c->R[1] = g->bufs[A[0]][0];
+  c->R[2] = g->bufs[B[0]][0];
+  c->R[3] = g->bufs[A[0]][0];
+  c->copyMask[0] = filt ? 1 : 0;
+  c->copyMask[1] = c->copyMask[2] = c->copyMask[3] = 31;
+  const double dt = c->dt;
+  c->dtUsed = dt;
+  c->stageT[0] = c->t + dt / 2;
+  c->stageT[1] = c->t + dt / 2;
+  c->stageT[2] = c->t + dt;
+  c->stageT[3] = c->t + dt;
+  for (int f = 0; f < 5; ++f) {  // roles after the step: final state = B, scratch = A
+    c->perm[f][0] = B[f];
+    c->perm[f][1] = old[f];
+    c->perm[f][2] = A[f];
+  }
+  for (int q = 0; q < 4; ++q) c->mx[q] = 0ull;
+}
+
+// Mesh::applyFilter_ifAppropriate body (Mesh.cpp:110-134): interior nodes get the 7-point filter,
+// every node of an edge boundary's owned box (whatever its type) and every solid-ghost node is copied,
+// the remaining solid inactive nodes are left as they are.
+__global__ void k_density_filter(const Grid* __restrict__ g) {
+  const StepCtl* c = g->ctl;
+  if (!c->active || !c->filterNow) return;
+  const double* __restrict__ src = c->gfSrc;
+  double* __restrict__ dst = c->gfDst;
+  const long long sI = g->sI, sJ = g->sJ;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g->N; n += (long long)gridDim.x * blockDim.x) {
+    const uint8_t raw = g->type[n], t = raw & TYPE_MASK;
+    if (t == FLUID_INTERIOR)
+      dst[n] = (6 * src[n] + src[n + sI] + src[n - sI] + src[n + sJ] + src[n - sJ] + src[n + 1] + src[n - 1]) / 12;
+    else if (t != SOLID_INACTIVE || (raw & EDGE_PLANE_BIT))
+      dst[n] = src[n];
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Fused stage kernel. 2.5-D: a block owns a TJ x TK column tile (k fastest, one thread per column) and
+// marches a chunk of i-planes. Each plane of the tile plus a one-node halo is staged once: the five
+// conserved values are loaded (prefetched one plane ahead into registers), the seven primitive /
+// transport values are computed once per staged node, and eleven values per node go to shared memory
+// in a three-plane ring. The RHS of the reference's five flux loops (Solver.cpp:181-418) is then
+// evaluated from shared memory in the reference's term order, and the RK4 combine
+// (Solver.cpp:435-442, 494-507) is applied in the epilogue with an accumulator acc = k1 + 2k2 + 2k3.
+namespace stage {
+constexpr int TK = 32, TJ = 8, NT = TK * TJ;
+constexpr int HK = TK + 2, HJ = TJ + 2, HP = HK * HJ;  // staged plane: tile + halo (with corners)
+constexpr int NV = 11;                                  // ru rv rw rE u v w p T mu ka
+constexpr int PER_THREAD = (HP + NT - 1) / NT;          // staged nodes per thread (2)
+enum { RU, RV, RW, RE, U, V, W, P, TT, MU, KA };
+constexpr size_t SMEM = size_t(3) * NV * HP * sizeof(double) + 3 * HP + 16 * 32 * sizeof(double);
+}  // namespace stage
+
+struct Staged {  // one staged node held in registers between its load and its shared-memory store
+  double rho, ru, rv, rw, rE, rhoP, rEP;
+  uint8_t type;
+  bool valid;
+};
+
+__device__ __forceinline__ void stage_load(const Grid& G, const StepCtl& c, int s, int i, int j0, int k0, int q,
+                                           Staged& st) {
+  using namespace stage;
+  const int hj = q / HK, hk = q - hj * HK;
+  const int j = j0 - 1 + hj, k = k0 - 1 + hk;
+  st.valid = (q < HP) && (j < G.NJ) && (k < G.NK) && (i < G.NI);
+  if (!st.valid) return;
+  const long long n = i * G.sI + j * G.sJ + k;
+  st.type = G.type[n];
+  st.rho = c.R[s][n];
+  st.ru = c.I[s][1][n];
+  st.rv = c.I[s][2][n];
+  st.rw = c.I[s][3][n];
+  st.rE = c.I[s][4][n];
+  st.rhoP = st.rho;
+  st.rEP = st.rE;
+  if (st.type & FILTER_BIT) {  // primitives of a filtered node are those before the filter
+    const int f = G.fidx[n];
+    st.rhoP = G.fpre[2 * f];
+    st.rEP = G.fpre[2 * f + 1];
+  }
+}
+
+__device__ __forceinline__ void stage_store(const Consts& C, double* __restrict__ sm, uint8_t* __restrict__ st8,
+                                            int slot, int q, const Staged& st) {
+  using namespace stage;
+  if (!st.valid) return;
+  double* b = sm + size_t(slot) * NV * HP;
+  const Prim p = prims_of(C, st.rhoP, st.ru, st.rv, st.rw, st.rEP);
+  b[RU * HP + q] = st.ru;
+  b[RV * HP + q] = st.rv;
+  b[RW * HP + q] = st.rw;
+  b[RE * HP + q] = st.rE;
+  b[U * HP + q] = p.u;
+  b[V * HP + q] = p.v;
+  b[W * HP + q] = p.w;
+  b[P * HP + q] = p.p;
+  b[TT * HP + q] = p.T;
+  b[MU * HP + q] = p.mu;
+  b[KA * HP + q] = p.ka;
+  st8[slot * HP + q] = st.type;
+}
+
+// Right-hand side at one node from the three staged planes (W = i-1, P = i, E = i+1).
+__device__ __forceinline__ void rhs_node(const Consts& C, const double* __restrict__ sW, const double* __restrict__ sP,
+                                         const double* __restrict__ sE, int c, double out[5]) {
+  using namespace stage;
+  constexpr int jn = HK, jk = 1;
+#define F_(b, v, o) (b)[(v)*HP + c + (o)]
+  // neighbours in the centre plane: N/S = j+-1, U/D = k+-1
+  const int oN = jn, oS = -jn, oU = jk, oD = -jk;
+  // ---- continuity, Solver.cpp:181-196
+  {
+    const double fx = C.ax * (F_(sE, RU, 0) - F_(sW, RU, 0));
+    const double fy = C.ay * (F_(sP, RV, oN) - F_(sP, RV, oS));
+    const double fz = C.az * (F_(sP, RW, oU) - F_(sP, RW, oD));
+    out[0] = fx + fy + fz;
+  }
+  const double muP = F_(sP, MU, 0), muE = F_(sE, MU, 0), muW = F_(sW, MU, 0), muN = F_(sP, MU, oN),
+               muS = F_(sP, MU, oS), muU = F_(sP, MU, oU), muD = F_(sP, MU, oD);
+  const double uP = F_(sP, U, 0), uE = F_(sE, U, 0), uW = F_(sW, U, 0), uN = F_(sP, U, oN), uS = F_(sP, U, oS),
+               uU = F_(sP, U, oU), uD = F_(sP, U, oD);
+  const double vP = F_(sP, V, 0), vE = F_(sE, V, 0), vW = F_(sW, V, 0), vN = F_(sP, V, oN), vS = F_(sP, V, oS),
+               vU = F_(sP, V, oU), vD = F_(sP, V, oD);
+  const double wP = F_(sP, W, 0), wE = F_(sE, W, 0), wW = F_(sW, W, 0), wN = F_(sP, W, oN), wS = F_(sP, W, oS),
+               wU = F_(sP, W, oU), wD = F_(sP, W, oD);
+  const double pE = F_(sE, P, 0), pW = F_(sW, P, 0), pN = F_(sP, P, oN), pS = F_(sP, P, oS), pU = F_(sP, P, oU),
+               pD = F_(sP, P, oD);
+  // edge neighbours: velocity values only
+  const double vEN = F_(sE, V, oN), vES = F_(sE, V, oS), vWN = F_(sW, V, oN), vWS = F_(sW, V, oS);
+  const double uEN = F_(sE, U, oN), uES = F_(sE, U, oS), uWN = F_(sW, U, oN), uWS = F_(sW, U, oS);
+  const double wEU = F_(sE, W, oU), wED = F_(sE, W, oD), wWU = F_(sW, W, oU), wWD = F_(sW, W, oD);
+  const double uEU = F_(sE, U, oU), uED = F_(sE, U, oD), uWU = F_(sW, U, oU), uWD = F_(sW, U, oD);
+  const double wNU = F_(sP, W, oN + oU), wND = F_(sP, W, oN + oD), wSU = F_(sP, W, oS + oU), wSD = F_(sP, W, oS + oD);
+  const double vNU = F_(sP, V, oN + oU), vND = F_(sP, V, oN + oD), vSU = F_(sP, V, oS + oU), vSD = F_(sP, V, oS + oD);
+  // ---- x-momentum, Solver.cpp:199-243
+  {
+    const double ruE = F_(sE, RU, 0), ruW = F_(sW, RU, 0), ruN = F_(sP, RU, oN), ruS = F_(sP, RU, oS),
+                 ruU = F_(sP, RU, oU), ruD = F_(sP, RU, oD);
+    const double cX = C.ax * (ruE * uE + pE - ruW * uW - pW);
+    const double cY = C.ay * (ruN * vN - ruS * vS);
+    const double cZ = C.az * (ruU * wU - ruD * wD);
+    const double vXX = C.xm_xx * ((muE + muP) * (uE - uP) - (muW + muP) * (uP - uW));
+    const double vYY = C.xm_yy * ((muN + muP) * (uN - uP) - (muS + muP) * (uP - uS));
+    const double vZZ = C.xm_zz * ((muU + muP) * (uU - uP) - (muD + muP) * (uP - uD));
+    const double vXY = C.xm_xy * (muN * (vEN - vWN) - muS * (vES - vWS));
+    const double vYX = C.xm_yx * (muE * (vEN - vES) - muW * (vWN - vWS));
+    const double vXZ = C.xm_xz * (muU * (wEU - wWU) - muD * (wED - wWD));
+    const double vZX = C.xm_zx * (muE * (wEU - wED) - muW * (wWU - wWD));
+    out[1] = cX + cY + cZ + vXX + vYY + vZZ + vXY + vYX + vXZ + vZX;
+  }
+  // ---- y-momentum, Solver.cpp:246-290
+  {
+    const double rvE = F_(sE, RV, 0), rvW = F_(sW, RV, 0), rvN = F_(sP, RV, oN), rvS = F_(sP, RV, oS),
+                 rvU = F_(sP, RV, oU), rvD = F_(sP, RV, oD);
+    const double cX = C.ax * (rvE * uE - rvW * uW);
+    const double cY = C.ay * (rvN * vN + pN - rvS * vS - pS);
+    const double cZ = C.az * (rvU * wU - rvD * wD);
+    const double vXX = C.ym_xx * ((muE + muP) * (vE - vP) - (muW + muP) * (vP - vW));
+    const double vYY = C.ym_yy * ((muN + muP) * (vN - vP) - (muS + muP) * (vP - vS));
+    const double vZZ = C.ym_zz * ((muU + muP) * (vU - vP) - (muD + muP) * (vP - vD));
+    const double vYX = C.ym_yx * (muE * (uEN - uES) - muW * (uWN - uWS));
+    const double vXY = C.ym_xy * (muN * (uEN - uWN) - muS * (uES - uWS));
+    const double vYZ = C.ym_yz * (muU * (wNU - wSU) - muD * (wND - wSD));
+    const double vZY = C.ym_zy * (muN * (wNU - wND) - muS * (wSU - wSD));
+    out[2] = cX + cY + cZ + vXX + vYY + vZZ + vYX + vXY + vYZ + vZY;
+  }
+  // ---- z-momentum, Solver.cpp:293-339
+  {
+    const double rwE = F_(sE, RW, 0), rwW = F_(sW, RW, 0), rwN = F_(sP, RW, oN), rwS = F_(sP, RW, oS),
+                 rwU = F_(sP, RW, oU), rwD = F_(sP, RW, oD);
+    const double cX = C.ax * (rwE * uE - rwW * uW);
+    const double cY = C.ay * (rwN * vN - rwS * vS);
+    const double cZ = C.az * (rwU * wU + pU - rwD * wD - pD);
+    const double vXX = C.zm_xx * ((muE + muP) * (wE - wP) - (muW + muP) * (wP - wW));
+    const double vYY = C.zm_yy * ((muN + muP) * (wN - wP) - (muS + muP) * (wP - wS));
+    const double vZZ = C.zm_zz * ((muU + muP) * (wU - wP) - (muD + muP) * (wP - wD));
+    const double vZX = C.zm_zx * (muE * (uEU - uED) - muW * (uWU - uWD));
+    const double vXZ = C.zm_xz * (muU * (uEU - uWU) - muD * (uED - uWD));
+    const double vZY = C.zm_zy * (muN * (vNU - vND) - muS * (vSU - vSD));
+    const double vYZ = C.zm_yz * (muU * (vNU - vSU) - muD * (vND - vSD));
+    out[3] = cX + cY + cZ + vXX + vYY + vZZ + vZX + vXZ + vZY + vYZ;
+  }
+  // ---- energy, Solver.cpp:342-418
+  {
+    const double H0 = C.h0;
+    const double EE = F_(sE, RE, 0), EW = F_(sW, RE, 0), EN = F_(sP, RE, oN), ES = F_(sP, RE, oS),
+                 EU = F_(sP, RE, oU), ED = F_(sP, RE, oD);
+    const double inv = C.ax * ((H0 + EE + pE) * uE - (H0 + EW + pW) * uW) +
+                       C.ay * ((H0 + EN + pN) * vN - (H0 + ES + pS) * vS) +
+                       C.az * ((H0 + EU + pU) * wU - (H0 + ED + pD) * wD);
+    const double vfX = C.e_xx23 * ((muE * uE + muP * uP) * (uE - uP) - (muW * uW + muP * uP) * (uP - uW)) +
+                       C.e_xx12 * ((muE * vE + muP * vP) * (vE - vP) - (muW * vW + muP * vP) * (vP - vW)) +
+                       C.e_xx12 * ((muE * wE + muP * wP) * (wE - wP) - (muW * wW + muP * wP) * (wP - wW)) +
+                       C.e_yx6 * (muE * uE * (vEN - vES) - muW * uW * (vWN - vWS)) +
+                       C.e_zx6 * (muE * uE * (wEU - wED) - muW * uW * (wWU - wWD)) +
+                       C.e_yx4 * (muE * vE * (uEN - uES) - muW * vW * (uWN - uWS)) +
+                       C.e_zx4 * (muE * wE * (uEU - uED) - muW * wW * (uWU - uWD));
+    const double vfY = C.e_yy12 * ((muN * uN + muP * uP) * (uN - uP) - (muS * uS + muP * uP) * (uP - uS)) +
+                       C.e_yy23 * ((muN * vN + muP * vP) * (vN - vP) - (muS * vS + muP * vP) * (vP - vS)) +
+                       C.e_yy12 * ((muN * wN + muP * wP) * (wN - wP) - (muS * wS + muP * wP) * (wP - wS)) +
+                       C.e_yx6 * (muN * vN * (uEN - uWN) - muS * vS * (uES - uWS)) +
+                       C.e_zy6 * (muN * vN * (wNU - wND) - muS * vS * (wSU - wSD)) +
+                       C.e_yx4 * (muN * uN * (vEN - vWN) - muS * uS * (vES - vWS)) +
+                       C.e_zy4 * (muN * wN * (vNU - vND) - muS * wS * (vSU - vSD));
+    const double vfZ = C.e_zz12 * ((muU * uU + muP * uP) * (uU - uP) - (muD * uD + muP * uP) * (uP - uD)) +
+                       C.e_zz12 * ((muU * vU + muP * vP) * (vU - vP) - (muD * vD + muP * vP) * (vP - vD)) +
+                       C.e_zz23 * ((muU * wU + muP * wP) * (wU - wP) - (muD * wD + muP * wP) * (wP - wD)) +
+                       C.e_zx6 * (muU * wU * (uEU - uWU) - muD * wD * (uED - uWD)) +
+                       C.e_zy6 * (muU * wU * (vNU - vSU) - muD * wD * (vND - vSD)) +
+                       C.e_zx4 * (muU * uU * (wEU - wWU) - muD * uD * (wED - wWD)) +
+                       C.e_zy4 * (muU * vU * (wNU - wSU) - muD * vD * (wND - wSD));
+    const double kP = F_(sP, KA, 0), TP = F_(sP, TT, 0);
+    const double hf = C.e_xx12 * ((F_(sE, KA, 0) + kP) * (F_(sE, TT, 0) - TP) - (F_(sW, KA, 0) + kP) * (TP - F_(sW, TT, 0))) +
+                      C.e_yy12 * ((F_(sP, KA, oN) + kP) * (F_(sP, TT, oN) - TP) - (F_(sP, KA, oS) + kP) * (TP - F_(sP, TT, oS))) +
+                      C.e_zz12 * ((F_(sP, KA, oU) + kP) * (F_(sP, TT, oU) - TP) - (F_(sP, KA, oD) + kP) * (TP - F_(sP, TT, oD)));
+    out[4] = inv + vfX + vfY + vfZ + hf;
+  }
+#undef F_
+}
+
+__global__ void __launch_bounds__(stage::NT, 2)
+    k_stage(const Grid* __restrict__ gp, const StageItem* __restrict__ items, int nItems, int s) {
+  using namespace stage;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* sm = reinterpret_cast<double*>(smraw);
+  uint8_t* st8 = smraw + size_t(3) * NV * HP * sizeof(double);
+  double* red = reinterpret_cast<double*>(st8 + 3 * HP + (8 - (3 * HP) % 8) % 8);
+  __shared__ Grid G;
+  __shared__ StepCtl ctl;
+  if (threadIdx.x == 0) {
+    G = *gp;
+    ctl = *gp->ctl;
+  }
+  __syncthreads();
+  if (!ctl.active) return;
+  const Consts& C = G.C;
+  const int tid = threadIdx.x, tx = tid % TK, ty = tid / TK;
+  const int cidx = (ty + 1) * HK + (tx + 1);
+  const double dtUsed = ctl.dtUsed;
+  const double inc = (s == 2) ? dtUsed : dtUsed / 2;  // dt/2, dt/2, dt (Solver.cpp:142-152)
+  const double dtFactor = dtUsed / 6;                 // Solver.cpp:501
+  double nsum[5] = {0, 0, 0, 0, 0};
+  DtAcc dta;
+  int bad = 0;
+
+  for (int it = blockIdx.x; it < nItems; it += gridDim.x) {
+    const StageItem w = items[it];
+    const int j = w.j0 + ty, k = w.k0 + tx;
+    Staged pre[PER_THREAD];
+    // prime the ring with planes i0-1 and i0, prefetch i0+1
+    for (int pl = 0; pl < 2; ++pl) {
+      const int i = w.i0 - 1 + pl;
+      for (int r = 0; r < PER_THREAD; ++r) {
+        Staged st;
+        stage_load(G, ctl, s, i, w.j0, w.k0, tid + r * NT, st);
+        stage_store(C, sm, st8, (i + 3) % 3, tid + r * NT, st);
+      }
+    }
+    for (int r = 0; r < PER_THREAD; ++r) stage_load(G, ctl, s, w.i0 + 1, w.j0, w.k0, tid + r * NT, pre[r]);
+    for (int i = w.i0; i <= w.i1; ++i) {
+      for (int r = 0; r < PER_THREAD; ++r) stage_store(C, sm, st8, (i + 1) % 3, tid + r * NT, pre[r]);
+      __syncthreads();
+      if (i + 2 <= w.i1 + 1)
+        for (int r = 0; r < PER_THREAD; ++r) stage_load(G, ctl, s, i + 2, w.j0, w.k0, tid + r * NT, pre[r]);
+      const uint8_t t = st8[(i % 3) * HP + cidx];
+      if (j <= G.NJ - 2 && k <= G.NK - 2 && (t & TYPE_MASK) == FLUID_INTERIOR) {
+        double kk[5];
+        rhs_node(C, sm + size_t((i + 2) % 3) * NV * HP, sm + size_t(i % 3) * NV * HP, sm + size_t((i + 1) % 3) * NV * HP,
+                 cidx, kk);
+        const long long n = i * G.sI + j * G.sJ + k;
+        if (s == 0) {
+          for (int f = 0; f < 5; ++f) {
+            G.acc[f][n] = kk[f];
+            ctl.O[0][f][n] = ctl.U0[f][n] + inc * kk[f];
+          }
+        } else if (s < 3) {
+          for (int f = 0; f < 5; ++f) {
+            G.acc[f][n] = G.acc[f][n] + 2 * kk[f];
+            ctl.O[s][f][n] = ctl.U0[f][n] + inc * kk[f];
+          }
+        } else {
+          double un[5], u0[5];
+          for (int f = 0; f < 5; ++f) {
+            u0[f] = ctl.U0[f][n];
+            un[f] = u0[f] + dtFactor * (G.acc[f][n] + kk[f]);
+            ctl.O[3][f][n] = un[f];
+            bad |= !isfinite(un[f]);
+          }
+          const bool filtered = (t & FILTER_BIT) != 0;  // rho, rho_E change again in the near-body filter
+          for (int f = 0; f < 5; ++f) {
+            if (filtered && (f == 0 || f == 4)) continue;
+            const double d = u0[f] - un[f];
+            nsum[f] += d * d;
+          }
+          if (!filtered) {
+            const Prim q = prims_of(C, un[0], un[1], un[2], un[3], un[4]);
+            dta.add(C, un[0], q.u, q.v, q.w, q.p, q.mu);
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (s == 3) {
+    flush_dt(gp->ctl, dta, red);
+    flush_norms(G.normPart + 5 * blockIdx.x, nsum, red);
+    if (bad) atomicOr(&gp->ctl->nonFinite, 1);
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Solid-node values the reference's stage buffer still holds from earlier writes (see nsf_device.cuh).
+__global__ void k_solid_copy(const Grid* __restrict__ g, int s) {
+  const StepCtl* c = g->ctl;
+  if (!c->active) return;
+  const int mask = c->copyMask[s];
+  if (!mask) return;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < g->nSolid; q += gridDim.x * blockDim.x) {
+    const long long n = g->snode[q];
+    if (mask & 1) c->O[s][0][n] = c->R[s][n];
+    for (int f = 1; f < 5; ++f)
+      if (mask & (1 << f)) c->O[s][f][n] = c->I[s][f][n];
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Mesh-edge boundary conditions of one axis (both faces; the faces of one axis never read each other's
+// nodes). Launched for x, then y, then z: the reference's application order outlet/inlet (x), y-max,
+// y-min, z-max, z-min (Mesh.cpp:155-167 after the reversal at Mesh.cpp:70). Threads cover the owned box.
+__global__ void k_edge_bc(const Grid* __restrict__ gp, int s, int axis) {
+  __shared__ double red[4 * 32];
+  const Grid& G = *gp;
+  StepCtl* c = G.ctl;
+  if (!c->active) return;
+  const Consts& C = G.C;
+  int e = -1, seen = 0;
+  for (int q = 0; q < G.nEdge; ++q)
+    if (G.eAxis[q] == axis) {
+      if (seen == (int)blockIdx.z) e = q;
+      ++seen;
+    }
+  DtAcc dta;
+  int bad = 0;
+  if (e >= 0) {
+    const int* b = G.eBox[e];
+    // in-plane coordinates: (a, bb) = the two axes other than `axis`, in (i, j, k) order
+    const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
+    const int a = b[2 * ax1] + blockIdx.y * blockDim.y + threadIdx.y;
+    const int bb = b[2 * ax2] + blockIdx.x * blockDim.x + threadIdx.x;
+    if (a <= b[2 * ax1 + 1] && bb <= b[2 * ax2 + 1]) {
+      int ijk[3];
+      ijk[axis] = b[2 * axis];
+      ijk[ax1] = a;
+      ijk[ax2] = bb;
+      const long long st = axis == 0 ? G.sI : axis == 1 ? G.sJ : 1;
+      const long long n = ijk[0] * G.sI + ijk[1] * G.sJ + ijk[2];
+      const int side = G.eSide[e], bc = G.eBc[e];
+      double** O = c->O[s];
+      const long long a1 = side == 0 ? n + st : n - st, a2 = side == 0 ? n + 2 * st : n - 2 * st;  // Boundary.cpp:74-108
+      double cv[5];
+      double u = 0, v = 0, w = 0, p = 0, T = 0;
+      bool primKnown = false;
+      if (bc == NSF_BC_INLET) {  // Boundary.cpp:250-296 with filterInletDensity :142-245
+        // extrapolated density of this node and of its in-plane neighbours inside the owned box
+        const long long s1 = ax1 == 0 ? G.sI : G.sJ, s2 = ax2 == 1 ? G.sJ : 1;
+        auto ext = [&](long long m) { return 2 * O[0][side == 0 ? m + st : m - st] - O[0][side == 0 ? m + 2 * st : m - 2 * st]; };
+        double f = 0;
+        unsigned nn = 0;
+        if (a < b[2 * ax1 + 1]) { f += ext(n + s1); ++nn; }
+        if (a > b[2 * ax1]) { f += ext(n - s1); ++nn; }
+        if (bb < b[2 * ax2 + 1]) { f += ext(n + s2); ++nn; }
+        if (bb > b[2 * ax2]) { f += ext(n - s2); ++nn; }
+        f += nn * ext(n);
+        f /= 2 * nn;
+        const double rho = f;
+        double vel = fmin(1., c->stageT[s] / 10.) * C.m0;
+        if (side == 1) vel *= -1;
+        u = axis == 0 ? vel : 0;
+        v = axis == 1 ? vel : 0;
+        w = axis == 2 ? vel : 0;
+        T = 0;
+        p = (T * (1 + rho) + rho) / C.gamma;
+        cons_of(C, u, v, w, p, T, cv);
+        primKnown = true;
+      } else if (bc == NSF_BC_OUTLET) {  // Boundary.cpp:304-336
+        const double rho = 2 * O[0][a1] - O[0][a2];
+        const double ru = 2 * O[1][a1] - O[1][a2];
+        const double rv = 2 * O[2][a1] - O[2][a2];
+        const double rw = 2 * O[3][a1] - O[3][a2];
+        p = 0;
+        u = ru / (1 + rho);
+        v = rv / (1 + rho);
+        w = rw / (1 + rho);
+        T = (C.gamma * p - rho) / (1 + rho);
+        cv[0] = rho;
+        cv[1] = ru;
+        cv[2] = rv;
+        cv[3] = rw;
+        cv[4] = p / C.gm1 + (1 + rho) / 2 * (u * u + v * v + w * w);
+        primKnown = true;
+      } else if (bc == NSF_BC_PERIODIC) {  // Boundary.cpp:344-367, opposite index :111-133
+        int src[3] = {ijk[0], ijk[1], ijk[2]};
+        const int nAx = axis == 0 ? G.NI : axis == 1 ? G.NJ : G.NK;
+        src[axis] = side == 0 ? nAx - 2 : 1;
+        const long long m = src[0] * G.sI + src[1] * G.sJ + src[2];
+        for (int f = 0; f < 5; ++f) cv[f] = O[f][m];
+      } else {  // symmetry, Boundary.cpp:377-417: mirror the primitives of the second interior node
+        const Prim q = prims_of(C, O[0][a2], O[1][a2], O[2][a2], O[3][a2], O[4][a2]);
+        u = q.u;
+        v = q.v;
+        w = q.w;
+        if (axis == 0) u = -q.u;
+        if (axis == 1) v = -q.v;
+        if (axis == 2) w = -q.w;
+        p = q.p;
+        T = q.T;
+        cons_of(C, u, v, w, p, T, cv);
+        primKnown = true;
+      }
+      for (int f = 0; f < 5; ++f) O[f][n] = cv[f];
+      if (s == 3) {
+        const uint8_t t = G.type[n] & TYPE_MASK;
+        if (t == FLUID_EDGE || t == FLUID_GHOST) {
+          double mu;
+          if (primKnown) {
+            mu = mu_of_T(C, T);
+          } else {
+            const Prim q = prims_of(C, cv[0], cv[1], cv[2], cv[3], cv[4]);
+            u = q.u;
+            v = q.v;
+            w = q.w;
+            p = q.p;
+            mu = q.mu;
+          }
+          dta.add(C, cv[0], u, v, w, p, mu);
+          for (int f = 0; f < 5; ++f) bad |= !isfinite(cv[f]);
+        }
+      }
+    }
+  }
+  if (s == 3) {
+    flush_dt(c, dta, red);
+    if (bad) atomicOr(&c->nonFinite, 1);
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Near-body filter (ImmersedBoundary::filterClosestFluidNodes, Boundary.cpp:618-652). Jacobi: every
+// filtered value is computed from unfiltered neighbours; results go to fnew and are written back by
+// k_ghost. The values before the filter go to fpre: the reference does not recompute the primitive
+// variables of these nodes after filtering, so the next stage builds their primitives from fpre.
+__global__ void k_body_filter(const Grid* __restrict__ gp, int s, int slotBase) {
+  __shared__ double red[5 * 32];
+  const Grid& G = *gp;
+  StepCtl* c = G.ctl;
+  if (!c->active) return;
+  const Consts& C = G.C;
+  double* const* O = c->O[s];
+  DtAcc dta;
+  double nsum[5] = {0, 0, 0, 0, 0};
+  int bad = 0;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < G.nFilter; f += gridDim.x * blockDim.x) {
+    const long long n = G.fnode[f];
+    const double* r = O[0];
+    const double* e = O[4];
+    const double rf = (6 * r[n] + r[n + G.sI] + r[n - G.sI] + r[n + G.sJ] + r[n - G.sJ] + r[n + 1] + r[n - 1]) / 12;
+    const double ef = (6 * e[n] + e[n + G.sI] + e[n - G.sI] + e[n + G.sJ] + e[n - G.sJ] + e[n + 1] + e[n - 1]) / 12;
+    const double r0 = r[n], e0 = e[n];
+    G.fpre[2 * f] = r0;
+    G.fpre[2 * f + 1] = e0;
+    G.fnew[2 * f] = rf;
+    G.fnew[2 * f + 1] = ef;
+    if (s == 3) {
+      const Prim q = prims_of(C, r0, O[1][n], O[2][n], O[3][n], e0);
+      dta.add(C, rf, q.u, q.v, q.w, q.p, q.mu);
+      const double d0 = c->U0[0][n] - rf, d4 = c->U0[4][n] - ef;
+      nsum[0] += d0 * d0;
+      nsum[4] += d4 * d4;
+      bad |= !isfinite(rf) || !isfinite(ef);
+    }
+  }
+  if (s == 3) {
+    flush_dt(c, dta, red);
+    flush_norms(G.normPart + 5 * (slotBase + blockIdx.x), nsum, red);
+    if (bad) atomicOr(&c->nonFinite, 1);
+  }
+}
+
+// Ghost nodes (Boundary.cpp:432-456): image-point value = cached weights x the 8 surrounding values
+// (Neumann weights for rho and rho_E, Dirichlet weights for the momenta, zero weight on ghost corners);
+// ghost value = image value with momentum negated (getGhostNodeBCVariables, :777-785). The same
+// launch writes the filtered values back (ghosts read them through fnew) and, on stage 4, adds the dt
+// terms of the solid inactive nodes, whose primitive values the reference never updates.
+__global__ void k_ghost(const Grid* __restrict__ gp, int s) {
+  __shared__ double red[4 * 32];
+  const Grid& G = *gp;
+  StepCtl* c = G.ctl;
+  if (!c->active) return;
+  const Consts& C = G.C;
+  double* const* O = c->O[s];
+  DtAcc dta;
+  int bad = 0;
+  const int total = G.nGhost + G.nFilter + (s == 3 ? G.nInactive : 0);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+    if (q < G.nGhost) {
+      const long long* cell = G.gcell + 8 * (long long)q;
+      const double* w = G.gw + 16 * (long long)q;
+      double ip[5] = {0, 0, 0, 0, 0};
+      for (int m = 0; m < 8; ++m) {
+        const double wn = w[m], wd = w[8 + m];
+        if (wn == 0.0 && wd == 0.0) continue;
+        const long long cn = cell[m];
+        double rho = O[0][cn], rE = O[4][cn];
+        if (G.type[cn] & FILTER_BIT) {
+          const int f = G.fidx[cn];
+          rho = G.fnew[2 * f];
+          rE = G.fnew[2 * f + 1];
+        }
+        ip[0] += wn * rho;
+        ip[4] += wn * rE;
+        ip[1] += wd * O[1][cn];
+        ip[2] += wd * O[2][cn];
+        ip[3] += wd * O[3][cn];
+      }
+      const double gc[5] = {ip[0], -ip[1], -ip[2], -ip[3], ip[4]};
+      const long long n = G.gnode[q];
+      for (int f = 0; f < 5; ++f) O[f][n] = gc[f];
+      if (s == 3) {
+        const Prim p = prims_of(C, gc[0], gc[1], gc[2], gc[3], gc[4]);
+        dta.add(C, gc[0], p.u, p.v, p.w, p.p, p.mu);
+        for (int f = 0; f < 5; ++f) bad |= !isfinite(gc[f]);
+      }
+    } else if (q < G.nGhost + G.nFilter) {
+      const int f = q - G.nGhost;
+      const long long n = G.fnode[f];
+      O[0][n] = G.fnew[2 * f];
+      O[4][n] = G.fnew[2 * f + 1];
+    } else {
+      const int z = q - G.nGhost - G.nFilter;
+      const long long n = G.inode[z];
+      const double* pr = G.iprim + 5 * (long long)z;
+      if (isnan(pr[0])) {  // periodic copy of a node whose primitives follow its conserved values
+        const Prim p = prims_of(C, O[0][n], O[1][n], O[2][n], O[3][n], O[4][n]);
+        dta.add(C, O[0][n], p.u, p.v, p.w, p.p, p.mu);
+      } else {
+        dta.add(C, O[0][n], pr[0], pr[1], pr[2], pr[3], pr[4]);
+      }
+    }
+  }
+  if (s == 3) {
+    flush_dt(c, dta, red);
+    if (bad) atomicOr(&c->nonFinite, 1);
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// End of step: change norms (Mesh::getNormOfChange, Mesh.cpp:171-178), next dt
+// (Solver::updateTimeStepSize, Solver.cpp:80-126), t += dt, ++timeLevel, history row.
+__global__ void k_finalize(Grid* g, int nSlots) {
+  __shared__ double red[5 * 32];
+  StepCtl* c = g->ctl;
+  if (!c->active) return;
+  const Consts& C = g->C;
+  double s[5] = {0, 0, 0, 0, 0};
+  for (int q = threadIdx.x; q < nSlots; q += blockDim.x)
+    for (int f = 0; f < 5; ++f) s[f] += g->normPart[5 * q + f];
+  __shared__ double tot[5];
+  flush_norms(tot, s, red);
+  if (threadIdx.x != 0) return;
+  double mx[4];
+  for (int q = 0; q < 4; ++q) mx[q] = __longlong_as_double(static_cast<long long>(c->mx[q]));
+  const double conv = C.convLim / (mx[0] / C.dx + mx[1] / C.dy + mx[2] / C.dz);
+  const double dx2 = C.dx * C.dx, dy2 = C.dy * C.dy, dz2 = C.dz * C.dz;
+  const double visc = C.viscLim / (mx[3] * (1 / dx2 + 1 / dy2 + 1 / dz2));
+  const double tNew = c->t + c->dtUsed;
+  double dt = (visc < conv) ? visc : conv;
+  if (C.endTime && tNew + dt > C.tEnd) dt = C.tEnd - tNew;
+  double* h = g->hist + 7 * (c->level % MAX_HIST);
+  h[0] = tNew;
+  h[1] = c->dtUsed;
+  for (int f = 0; f < 5; ++f) {
+    const bool kept = (f == 0 && C.convHistory != 0) || C.convHistory == 2;
+    h[2 + f] = kept ? sqrt(C.dxdydz * tot[f]) : -1.0;
+  }
+  c->t = tNew;
+  c->dt = dt;
+  c->level += 1;
+}
+
+// ----------------------------------------------------------------------------------------------
+// Setup: interpolation weights of every ghost node, solved once. For image-point cells whose eight
+// nodes are all fluid the weights are those of the reference's nested linear interpolation
+// (Boundary.cpp:732-757). Otherwise the reference solves V c = phi with the Vandermonde rows
+// [1, x, y, z, xy, xz, yz, xyz] (Neumann rows [0, n, ...] at ghost corners, Boundary.cpp:788-817) and
+// evaluates b^T c at the image point; the value is w^T phi with V^T w = b. The system is solved here in
+// cell-local scaled coordinates x' = (x - x0)/dx (the bilinear basis is invariant under per-axis affine
+// maps; a Neumann row transforms with n'_a = n_a/d_a), which keeps its condition number near 10 instead
+// of ~1e6 for the raw coordinates. Gaussian elimination with partial pivoting, in registers, one thread
+// per ghost.
+__device__ void solve8T(double A[8][8], double b[8]) {
+  // solve A^T x = b in place (x returned in b)
+  double M[8][8];
+  for (int r = 0; r < 8; ++r)
+    for (int q = 0; q < 8; ++q) M[r][q] = A[q][r];
+  for (int k = 0; k < 8; ++k) {
+    int piv = k;
+    double best = fabs(M[k][k]);
+    for (int r = k + 1; r < 8; ++r)
+      if (fabs(M[r][k]) > best) {
+        best = fabs(M[r][k]);
+        piv = r;
+      }
+    if (piv != k) {
+      for (int q = 0; q < 8; ++q) {
+        double t = M[k][q];
+        M[k][q] = M[piv][q];
+        M[piv][q] = t;
+      }
+      double t = b[k];
+      b[k] = b[piv];
+      b[piv] = t;
+    }
+    for (int r = k + 1; r < 8; ++r) {
+      const double l = M[r][k] / M[k][k];
+      for (int q = k; q < 8; ++q) M[r][q] -= l * M[k][q];
+      b[r] -= l * b[k];
+    }
+  }
+  for (int k = 7; k >= 0; --k) {
+    double acc = b[k];
+    for (int q = k + 1; q < 8; ++q) acc -= M[k][q] * b[q];
+    b[k] = acc / M[k][k];
+  }
+}
+
+// in: per ghost 8 x (x, y, z) corner points (node position, or body-intercept point for a ghost corner),
+// 8 x (nx, ny, nz) unit normals (ghost corners only), 8 flags, image point, lower cell node position.
+__global__ void k_ghost_weights(int nGhost, const double* __restrict__ pts, const double* __restrict__ nrm,
+                                const uint8_t* __restrict__ flags, const double* __restrict__ ipl,
+                                double dx, double dy, double dz, double* __restrict__ wout) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nGhost) return;
+  const double* P = pts + 24 * (long long)q;
+  const double* Nn = nrm + 24 * (long long)q;
+  const uint8_t* fl = flags + 8 * (long long)q;
+  const double* L = ipl + 6 * (long long)q;  // image point, lower node position
+  const double X = (L[0] - L[3]) / dx, Y = (L[1] - L[4]) / dy, Z = (L[2] - L[5]) / dz;
+  double* w = wout + 16 * (long long)q;
+  bool anyGhost = false;
+  for (int m = 0; m < 8; ++m) anyGhost |= fl[m] != 0;
+  if (!anyGhost) {
+    // corner m = (di, dj, dk) in asIndexList order: m = 4*di + 2*dj + dk
+    for (int m = 0; m < 8; ++m) {
+      const int di = m >> 2, dj = (m >> 1) & 1, dk = m & 1;
+      const double wv = (di ? X : 1 - X) * (dj ? Y : 1 - Y) * (dk ? Z : 1 - Z);
+      w[m] = wv;
+      w[8 + m] = wv;
+    }
+    return;
+  }
+  for (int set = 0; set < 2; ++set) {  // 0: Neumann rows at ghost corners, 1: Dirichlet everywhere
+    double V[8][8], b[8];
+    for (int m = 0; m < 8; ++m) {
+      const double x = (P[3 * m] - L[3]) / dx, y = (P[3 * m + 1] - L[4]) / dy, z = (P[3 * m + 2] - L[5]) / dz;
+      if (set == 0 && fl[m]) {
+        const double nx = Nn[3 * m] / (1.0 / dx), ny = Nn[3 * m + 1] / (1.0 / dy), nz = Nn[3 * m + 2] / (1.0 / dz);
+        // gradient of the basis in scaled coordinates: d/dx = (1/dx) d/dx'; the row is n . grad
+        const double ax = nx / (dx * dx), ay = ny / (dy * dy), az = nz / (dz * dz);
+        V[m][0] = 0;
+        V[m][1] = ax;
+        V[m][2] = ay;
+        V[m][3] = az;
+        V[m][4] = x * ay + y * ax;
+        V[m][5] = x * az + z * ax;
+        V[m][6] = y * az + z * ay;
+        V[m][7] = x * y * az + x * z * ay + y * z * ax;
+      } else {
+        V[m][0] = 1;
+        V[m][1] = x;
+        V[m][2] = y;
+        V[m][3] = z;
+        V[m][4] = x * y;
+        V[m][5] = x * z;
+        V[m][6] = y * z;
+        V[m][7] = x * y * z;
+      }
+    }
+    b[0] = 1;
+    b[1] = X;
+    b[2] = Y;
+    b[3] = Z;
+    b[4] = X * Y;
+    b[5] = X * Z;
+    b[6] = Y * Z;
+    b[7] = X * Y * Z;
+    solve8T(V, b);
+    for (int m = 0; m < 8; ++m) w[8 * set + m] = fl[m] ? 0.0 : b[m];
+  }
+}
+
+// Primitive / transport fields as the reference holds them, for downloads: recomputed from the
+// conserved values, except filtered nodes (values before the last near-body filter) and solid inactive
+// nodes (never updated by the reference; stored).
+__global__ void k_download_prims(const Grid* __restrict__ gp, double* __restrict__ out) {
+  const Grid& G = *gp;
+  const StepCtl* c = G.ctl;
+  const Consts& C = G.C;
+  const double* U[5];
+  for (int f = 0; f < 5; ++f) U[f] = G.bufs[c->perm[f][0]][f];
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x) {
+    double rho = U[0][n], rE = U[4][n];
+    const uint8_t t = G.type[n];
+    if (t & FILTER_BIT) {
+      const int f = G.fidx[n];
+      rho = G.fpre[2 * f];
+      rE = G.fpre[2 * f + 1];
+    }
+    const Prim q = prims_of(C, rho, U[1][n], U[2][n], U[3][n], rE);
+    out[0 * G.N + n] = q.u;
+    out[1 * G.N + n] = q.v;
+    out[2 * G.N + n] = q.w;
+    out[3 * G.N + n] = q.p;
+    out[4 * G.N + n] = q.T;
+    out[5 * G.N + n] = q.mu;
+    out[6 * G.N + n] = q.ka;
+  }
+}
+
+// Solid inactive nodes: overwrite the recomputed download values with the stored ones.
+__global__ void k_download_inactive(const Grid* __restrict__ gp, const long long* __restrict__ nodes,
+                                    const double* __restrict__ p7, int count, double* __restrict__ out) {
+  const Grid& G = *gp;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    const long long n = nodes[q];
+    for (int f = 0; f < 7; ++f) out[f * G.N + n] = p7[7 * (long long)q + f];
+  }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Host-side launch helpers (called from nsf_capi.cpp).
+size_t stage_smem_bytes() { return stage::SMEM + 64; }
+
+int stage_configure() {
+  return int(cudaFuncSetAttribute(k_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stage_smem_bytes())));
+}
+
+int stage_tile_j() { return stage::TJ; }
+int stage_tile_k() { return stage::TK; }
+int stage_threads() { return stage::NT; }
+
+int stage_occupancy() {
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stage, stage::NT, stage_smem_bytes());
+  return nb;
+}
+
+// Enqueue one RK4 step. Returns the number of kernel launches.
+static int enqueue_impl(Grid* dg, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev) {
+  int launches = 0;
+  k_prologue<<<1, 32, 0, st>>>(dg);
+  ++launches;
+  k_density_filter<<<L.gfBlocks, 256, 0, st>>>(dg);
+  ++launches;
+  for (int s = 0; s < 4; ++s) {
+    if (ev) cudaEventRecord(ev[2 * s], st);
+    k_stage<<<L.stageBlocks, stage::NT, stage_smem_bytes(), st>>>(dg, L.items, L.nItems, s);
+    if (ev) cudaEventRecord(ev[2 * s + 1], st);
+    ++launches;
+    if (L.hasSolid) {
+      k_solid_copy<<<L.solidBlocks, 256, 0, st>>>(dg, s);
+      ++launches;
+    }
+    for (int a = 0; a < 3; ++a) {
+      dim3 grid(L.edgeGrid[a][0], L.edgeGrid[a][1], L.edgeGrid[a][2]);
+      k_edge_bc<<<grid, dim3(32, 8), 0, st>>>(dg, s, a);
+      ++launches;
+    }
+    if (L.hasFilter) {
+      k_body_filter<<<L.filterBlocks, 256, 0, st>>>(dg, s, L.stageBlocks);
+      ++launches;
+    }
+    if (L.hasGhostWork) {
+      k_ghost<<<L.ghostBlocks, 256, 0, st>>>(dg, s);
+      ++launches;
+    }
+  }
+  k_finalize<<<1, 256, 0, st>>>(dg, L.nSlots);
+  ++launches;
+  return launches;
+}
+
+int enqueue_step(Grid* dg, const LaunchPlan& L, void* stream) {
+  return enqueue_impl(dg, L, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int enqueue_step_profiled(Grid* dg, const LaunchPlan& L, void* stream, void* events) {
+  return enqueue_impl(dg, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events));
+}
+
+void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,
+                          double dx, double dy, double dz, double* w, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (nGhost > 0) k_ghost_weights<<<(nGhost + 127) / 128, 128, 0, st>>>(nGhost, pts, nrm, flags, ipl, dx, dy, dz, w);
+}
+
+void launch_download_prims(const Grid* dg, long long N, double* out, const long long* inodes, const double* ip7,
+                           int nInactive, int nSM, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_download_prims<<<nSM * 8, 256, 0, st>>>(dg, out);
+  if (nInactive > 0) k_download_inactive<<<(nInactive + 255) / 256, 256, 0, st>>>(dg, inodes, ip7, nInactive, out);
+}
+
+}  // namespace nsf

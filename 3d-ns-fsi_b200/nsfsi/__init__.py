@@ -1,0 +1,245 @@
+"""ctypes binding of the C ABI in include/nsfsi.h (the B200 time-marching path).
+
+The library is 3d-ns-fsi_b200/lib/libnsfsi.so, built in-tree by ``__graft_entry__.build()``. There is no
+CPU fallback: if the library is missing or no sm_100 device is present, the calls fail loudly.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "lib", "libnsfsi.so")
+HEADER = os.path.join(ROOT, "include", "nsfsi.h")
+CASES = os.path.join(PKG, "cases")
+
+FIELDS = ["rho", "rho_u", "rho_v", "rho_w", "rho_E", "u", "v", "w", "p", "T", "mu", "kappa"]
+STATUS = {0: "NSF_OK", 1: "NSF_ERR_CONFIG", 2: "NSF_ERR_CUDA", 3: "NSF_ERR_NONFINITE", 4: "NSF_ERR_GEOMETRY",
+          5: "NSF_ERR_TIMEOUT", 6: "NSF_ERR_ARG", 7: "NSF_ERR_STATE"}
+BC = {"periodic": 0, "symmetry": 1, "inlet": 2, "outlet": 3}
+IC = {"stagnation": 0, "freestream_noise": 1, "tgv": 2}
+MAXF, MAXS, MAXC = 16, 64, 16
+
+
+class Sphere(ctypes.Structure):
+    _fields_ = [("cx", ctypes.c_double), ("cy", ctypes.c_double), ("cz", ctypes.c_double), ("r", ctypes.c_double)]
+
+
+class Cylinder(ctypes.Structure):
+    _fields_ = [("axis", ctypes.c_int32), ("cx", ctypes.c_double), ("cy", ctypes.c_double), ("cz", ctypes.c_double),
+                ("r", ctypes.c_double)]
+
+
+class Config(ctypes.Structure):
+    """nsf_config: every ConfigSettings member plus the case description."""
+    _i32, _u64, _d = ctypes.c_int32, ctypes.c_uint64, ctypes.c_double
+    _fields_ = [("NI", _u64), ("NJ", _u64), ("NK", _u64), ("stop_criterion", _i32), ("stop_time_level", _u64),
+                ("t_end", _d), ("conv_stability_limit", _d), ("visc_stability_limit", _d),
+                ("n_filter_intervals", _i32), ("filter_intervals", ctypes.c_uint32 * MAXF),
+                ("n_filter_change_times", _i32), ("filter_change_times", _d * MAXF), ("status_report_interval", _d),
+                ("save_density", _i32), ("save_momentum", _i32), ("save_energy", _i32), ("save_velocity", _i32),
+                ("save_pressure", _i32), ("save_temperature", _i32), ("save_viscosity", _i32),
+                ("save_thermal_cond", _i32), ("save_ic", _i32), ("save_final", _i32), ("save_intervals", _i32),
+                ("save_period", _d), ("save_intervals_start_time", _d), ("save_intervals_end_time", _d),
+                ("conv_history", _i32), ("gamma", _d), ("pr", _d), ("r_gas", _d), ("re", _d), ("sutherlands_c1", _d),
+                ("sutherlands_c2", _d), ("m0", _d), ("t0", _d), ("lx", _d), ("ly", _d), ("lz", _d),
+                ("machine_precision_buffer", _d), ("shipped_case", _i32), ("bc", (_i32 * 2) * 3),
+                ("n_spheres", _i32), ("spheres", Sphere * MAXS), ("n_cylinders", _i32),
+                ("cylinders", Cylinder * MAXC), ("ic", _i32), ("noise_amp", _d), ("seed", _u64)]
+
+
+class NsfError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s: %s" % (STATUS.get(code, code), msg))
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libnsfsi.so and declare its signatures (raises if the native library is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("native library %s is missing: run __graft_entry__.build()" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, u32, u64, dp = ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)
+    cp = ctypes.POINTER(Config)
+    sig = {
+        "nsf_abi_version": (i32, []),
+        "nsf_config_defaults": (i32, [cp]),
+        "nsf_config_load": (i32, [ctypes.c_char_p, cp, ctypes.c_char_p, ctypes.c_size_t]),
+        "nsf_config_parse": (i32, [ctypes.c_char_p, cp, ctypes.c_char_p, ctypes.c_size_t]),
+        "nsf_create": (i32, [cp, i32, ctypes.POINTER(vp)]),
+        "nsf_initialize": (i32, [vp]),
+        "nsf_march": (i32, [vp, u64]),
+        "nsf_sync": (i32, [vp]),
+        "nsf_get_time": (i32, [vp, dp, ctypes.POINTER(u64), dp]),
+        "nsf_download": (i32, [vp, u32, dp]),
+        "nsf_upload_conserved": (i32, [vp, dp]),
+        "nsf_get_node_types": (i32, [vp, ctypes.POINTER(ctypes.c_uint8)]),
+        "nsf_get_num_bodies": (i32, [vp, ctypes.POINTER(u32)]),
+        "nsf_get_body_counts": (i32, [vp, u32, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]),
+        "nsf_get_ghosts": (i32, [vp, u32, dp]),
+        "nsf_get_filter_nodes": (i32, [vp, u32, ctypes.POINTER(u64)]),
+        "nsf_get_history": (i32, [vp, u64, u64, dp, ctypes.POINTER(u64)]),
+        "nsf_launches_per_step": (i32, [vp, ctypes.POINTER(u64)]),
+        "nsf_march_timed": (i32, [vp, u64, dp]),
+        "nsf_profile_steps": (i32, [vp, u64, dp, dp]),
+        "nsf_last_error": (ctypes.c_char_p, [vp]),
+        "nsf_destroy": (None, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def config_defaults():
+    c = Config()
+    lib().nsf_config_defaults(ctypes.byref(c))
+    return c
+
+
+def config_parse(text):
+    c = Config()
+    err = ctypes.create_string_buffer(1024)
+    st = lib().nsf_config_parse(text.encode(), ctypes.byref(c), err, 1024)
+    if st:
+        raise NsfError(st, err.value.decode())
+    return c
+
+
+def config_load(path):
+    c = Config()
+    err = ctypes.create_string_buffer(1024)
+    st = lib().nsf_config_load(path.encode(), ctypes.byref(c), err, 1024)
+    if st:
+        raise NsfError(st, err.value.decode())
+    return c
+
+
+def case_path(name):
+    return os.path.join(CASES, name + ".cfg")
+
+
+class Solver:
+    """One solver handle: Solver / Mesh / Simulation state resident on one GPU."""
+
+    def __init__(self, cfg, device=0, initialize=True):
+        if isinstance(cfg, str):
+            cfg = config_load(cfg) if os.path.exists(cfg) else config_parse(cfg)
+        self.cfg = cfg
+        self.h = ctypes.c_void_p()
+        L = lib()
+        st = L.nsf_create(ctypes.byref(cfg), device, ctypes.byref(self.h))
+        if st:
+            msg = L.nsf_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise NsfError(st, msg)
+        self.N = int(cfg.NI * cfg.NJ * cfg.NK)
+        if initialize:
+            self._check(L.nsf_initialize(self.h))
+
+    def _check(self, st):
+        if st:
+            raise NsfError(st, lib().nsf_last_error(self.h).decode())
+
+    def close(self):
+        if self.h:
+            lib().nsf_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def march(self, nsteps):
+        self._check(lib().nsf_march(self.h, nsteps))
+
+    def sync(self):
+        self._check(lib().nsf_sync(self.h))
+
+    def time(self):
+        t, lv, dt = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_double()
+        self._check(lib().nsf_get_time(self.h, ctypes.byref(t), ctypes.byref(lv), ctypes.byref(dt)))
+        return t.value, lv.value, dt.value
+
+    def download(self, fields=range(12)):
+        fields = sorted(fields)
+        mask = 0
+        for f in fields:
+            mask |= 1 << f
+        out = np.empty((len(fields), self.N))
+        self._check(lib().nsf_download(self.h, mask, _dp(out)))
+        return out
+
+    def upload_conserved(self, u5):
+        a = np.ascontiguousarray(u5, dtype=np.float64)
+        self._check(lib().nsf_upload_conserved(self.h, _dp(a)))
+
+    def node_types(self):
+        out = np.empty(self.N, np.uint8)
+        self._check(lib().nsf_get_node_types(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        return out
+
+    def bodies(self):
+        L = lib()
+        nb = ctypes.c_uint32()
+        self._check(L.nsf_get_num_bodies(self.h, ctypes.byref(nb)))
+        res = []
+        for b in range(nb.value):
+            ng, nf, cl = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+            self._check(L.nsf_get_body_counts(self.h, b, ctypes.byref(ng), ctypes.byref(nf), ctypes.byref(cl)))
+            g = np.zeros((ng.value, 9))
+            f = np.zeros(nf.value, np.uint64)
+            if ng.value:
+                self._check(L.nsf_get_ghosts(self.h, b, _dp(g)))
+            if nf.value:
+                self._check(L.nsf_get_filter_nodes(self.h, b, f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+            res.append((g, f, cl.value))
+        return res
+
+    def history(self, first=0, count=None):
+        avail = ctypes.c_uint64()
+        self._check(lib().nsf_get_history(self.h, 0, 0, None, ctypes.byref(avail)))
+        count = avail.value - first if count is None else count
+        out = np.zeros((count, 7))
+        if count:
+            self._check(lib().nsf_get_history(self.h, first, count, _dp(out), ctypes.byref(avail)))
+        return out
+
+    def march_timed(self, nsteps):
+        """March nsteps; device time (ms) from CUDA events on the solver's own stream."""
+        ms = ctypes.c_double()
+        self._check(lib().nsf_march_timed(self.h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def profile_steps(self, nsteps):
+        """March nsteps launched eagerly; returns (mean ms of each stage kernel [4], mean ms per step)."""
+        st = np.zeros(4)
+        step = ctypes.c_double()
+        self._check(lib().nsf_profile_steps(self.h, nsteps, _dp(st), ctypes.byref(step)))
+        return st, step.value
+
+    def launches_per_step(self):
+        n = ctypes.c_uint64()
+        self._check(lib().nsf_launches_per_step(self.h, ctypes.byref(n)))
+        return n.value

@@ -1,0 +1,260 @@
+"""Benchmark of the B200 time-marching path: FP64 node-RK4-steps/s on the 256^3 Taylor-Green workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload tgv256|sphere48]
+
+A step is one RK4 step (Solver::marchTimeStep) over the whole grid. Each rank runs an independent replica
+(the single-grid path does not shard), so value = ranks x nodes x K / max-over-ranks device time.
+Timing: CUDA events on the solver's own stream around K graph-launched steps after W warm-up steps; the
+resident fields (2.7 GB) are far larger than L2, so no flush is needed between steps.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "3d-ns-fsi_b200"))
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    "tgv256": dict(case="tgv256", desc="Taylor-Green vortex, periodic 256^3, M0=0.1, Re=1600, CFL 0.5, FP64"),
+    "sphere48": dict(case="sphere48", desc="single sphere 48^3, inflow/outflow x, periodic y/z, M0=0.3, Re_D=100"),
+}
+BYTES_PER_NODE_STEP = 680  # algorithmic HBM bytes per node per RK4 step (stage-fused scheme)
+STAGE_BYTES = [120, 200, 200, 160]
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Stage-kernel DRAM bytes per node-step from the committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", "k_stage_tgv256.md")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_node_step:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(case_path, nodes):
+    """Serial CPU reference timed on this host: the reference build (oracle/_ref) if present, else the
+    oracle port. Sample: one RK4 step of the same workload at full size."""
+    from oracle import pyoracle as po
+    if po.ref_available():
+        r = po.time_reference(case_path, 0, 1)
+        return {"value": r["node_steps_per_s"], "unit": "node-RK4-steps/s", "cores": 1, "kind": "reference",
+                "sample": "1 RK4 step of the full workload grid (%d nodes), serial reference build, %.1f s" %
+                          (nodes, r["seconds"]),
+                "host_cores_present": os.cpu_count()}
+    o = po.Oracle(open(case_path).read())
+    sec = o.march(1)
+    o.close()
+    return {"value": nodes / sec, "unit": "node-RK4-steps/s", "cores": 1, "kind": "port",
+            "sample": "1 RK4 step of the full workload grid (%d nodes), serial oracle port, %.1f s" % (nodes, sec),
+            "host_cores_present": os.cpu_count()}
+
+
+def run_reference_arm(args, rank, world):
+    wl = WORKLOADS[args.workload]
+    import nsfsi  # only for the case-file path
+    case = nsfsi.case_path(wl["case"])
+    if rank != 0:
+        return
+    from oracle import pyoracle as po
+    c = nsfsi.config_load(case)
+    nodes = int(c.NI * c.NJ * c.NK)
+    k = max(1, min(args.steps, 3))
+    if po.ref_available():
+        r = po.time_reference(case, 0, k)
+        value, sec, kind = r["node_steps_per_s"], r["seconds"], "reference"
+    else:
+        o = po.Oracle(open(case).read())
+        sec = o.march(k)
+        value, kind = nodes * k / sec, "port"
+    line = {"impl": "reference", "metric": "node-RK4-steps/s (FP64)", "value": value, "unit": "node-RK4-steps/s",
+            "n_gpus": 0, "steps": k, "warmup": 0, "ms_per_step": 1e3 * sec / k, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": wl["desc"], "grid": [int(c.NI), int(c.NJ), int(c.NK)]},
+            "cpu_baseline": {"value": value, "unit": "node-RK4-steps/s", "cores": 1, "kind": kind,
+                             "sample": "%d of the requested %d RK4 steps of the full %s grid, serial, 1 core of %d" %
+                                       (k, args.steps, args.workload, os.cpu_count())},
+            "e2e": {"value": value, "unit": "node-RK4-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tgv256", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import nsfsi
+    wl = WORKLOADS[args.workload]
+    case = nsfsi.case_path(wl["case"])
+    cfg = nsfsi.config_load(case)
+    nodes = int(cfg.NI * cfg.NJ * cfg.NK)
+
+    s = nsfsi.Solver(cfg, device=local)
+    s.march(args.warmup)
+    s.sync()
+    import torch
+    if dist:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        ms = s.march_timed(args.steps)
+        s.sync()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nodes * args.steps / (ms / 1e3)
+    launches = s.launches_per_step()
+
+    # dominant kernel: live CUDA-event timing of the four stage kernels inside eagerly launched steps
+    stage_ms, step_ms = s.profile_steps(5)
+    achieved = BYTES_PER_NODE_STEP * nodes / (stage_ms.sum() / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profile_traffic()
+    s.close()
+
+    # end to end through the C ABI with host buffers: pinned upload of the initial state, K steps with
+    # the per-step t/dt/timeLevel read-back Simulation::run needs, pinned download of the final state
+    e2e = None
+    if rank == 0 or True:
+        s2 = nsfsi.Solver(cfg, device=local)
+        u0 = s2.download(range(5))
+        pin_in = torch.empty((5, nodes), dtype=torch.float64, pin_memory=True)
+        pin_in.numpy()[:] = u0
+        pin_out = torch.empty((5, nodes), dtype=torch.float64, pin_memory=True)
+        import ctypes
+        dp = ctypes.POINTER(ctypes.c_double)
+        L = nsfsi.lib()
+        s2.march(args.warmup)
+        s2.sync()
+        t0 = time.perf_counter()
+        s2._check(L.nsf_upload_conserved(s2.h, ctypes.cast(pin_in.data_ptr(), dp)))
+        for _ in range(args.steps):
+            s2.march(1)
+            s2.time()
+        s2._check(L.nsf_download(s2.h, 31, ctypes.cast(pin_out.data_ptr(), dp)))
+        wall = time.perf_counter() - t0
+        s2.close()
+        e2e = {"value": world * nodes * args.steps / wall, "unit": "node-RK4-steps/s",
+               "h2d_bytes_per_step": 5 * 8 * nodes / args.steps,
+               "d2h_bytes_per_step": (5 * 8 * nodes + 24 * args.steps) / args.steps,
+               "timing": "host wall clock around upload + K x (march 1, read t/dt/timeLevel) + download"}
+
+    if rank == 0:
+        line = {
+            "metric": "node-RK4-steps/s (FP64)", "value": value, "unit": "node-RK4-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": wl["desc"], "grid": [int(cfg.NI), int(cfg.NJ), int(cfg.NK)],
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "resident fields 2.7 GB >> 126 MB L2; no flush"},
+            "e2e": e2e,
+            "gpu_launches": launches * args.steps,
+            "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": (traffic * nodes / 4) if traffic else None,
+                         "kernel": "k_stage", "stage_ms": [round(x, 4) for x in stage_ms],
+                         "algorithmic_bytes_per_node_step": BYTES_PER_NODE_STEP, "peak_kind": peak_kind,
+                         "frac_of_8000": achieved / 8000.0},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline(case, nodes)
+            except Exception as e:  # noqa: BLE001
+                line["cpu_baseline"] = {"value": None, "error": str(e)}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

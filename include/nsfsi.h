@@ -1,0 +1,168 @@
+/*
+ * nsfsi.h -- C ABI of the B200 (sm_100a) time-marching path for the 3D-NS-FSI compressible
+ * Navier-Stokes solver. Plain C types only; every call returns an nsf_status (0 = success).
+ *
+ * The reference (Frederik-Kris/3D-NS-FSI) is a pure C++ program with no foreign-function interface.
+ * Each entry point below replaces one piece of its C++ call surface, cited as path:line in the
+ * reference project; the C++ host classes in 3d-ns-fsi_b200/host/ (ConfigSettings, Solver, Mesh,
+ * Simulation) are re-expressed on top of these calls.
+ *
+ * Memory model: the solver handle owns all device memory (allocated in nsf_create / nsf_initialize,
+ * freed in nsf_destroy) and one CUDA stream. Fields stay resident in HBM in the reference's SoA layout
+ * (one array per variable, index i*NJ*NK + j*NK + k, k fastest). Host buffers passed to the download /
+ * upload calls belong to the caller. No device pointer escapes through this interface.
+ * Threading: calls on one handle must be serialised by the caller; different handles are independent.
+ */
+#ifndef NSFSI_H
+#define NSFSI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NSF_ABI_VERSION 1
+
+typedef enum nsf_status {
+  NSF_OK = 0,
+  NSF_ERR_CONFIG = 1,    /* ConfigFile / nsf_config problem (ConfigSettings::errorOccurred) */
+  NSF_ERR_CUDA = 2,      /* a CUDA runtime call failed, or no usable sm_100 device */
+  NSF_ERR_NONFINITE = 3, /* a conserved variable became NaN/Inf (Mesh::checkFinity) */
+  NSF_ERR_GEOMETRY = 4,  /* a body leaves the mesh or bodies interact (cases the reference mishandles) */
+  NSF_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
+  NSF_ERR_ARG = 6,       /* bad argument (null pointer, wrong state, index out of range) */
+  NSF_ERR_STATE = 7      /* call out of order (e.g. nsf_march before nsf_initialize) */
+} nsf_status;
+
+/* Boundary type per mesh face (the MeshEdgeBoundary subclasses, Boundary.h:80-181). */
+typedef enum nsf_bc { NSF_BC_PERIODIC = 0, NSF_BC_SYMMETRY = 1, NSF_BC_INLET = 2, NSF_BC_OUTLET = 3 } nsf_bc;
+/* Initial condition (Solver::applyStagnation_IC, Solver.cpp:31-51, and the seeded/analytic extensions). */
+typedef enum nsf_ic { NSF_IC_STAGNATION = 0, NSF_IC_FREESTREAM_NOISE = 1, NSF_IC_TGV = 2 } nsf_ic;
+/* Field indices for downloads: conserved (Solver.cpp:446-479 names), primitive, transport. */
+enum {
+  NSF_RHO = 0, NSF_RHO_U, NSF_RHO_V, NSF_RHO_W, NSF_RHO_E,
+  NSF_U, NSF_V, NSF_W, NSF_P, NSF_T, NSF_MU, NSF_KAPPA, NSF_NUM_FIELDS
+};
+
+#define NSF_MAX_FILTER_INTERVALS 16
+#define NSF_MAX_SPHERES 64
+#define NSF_MAX_CYLINDERS 16
+
+typedef struct nsf_sphere { double cx, cy, cz, r; } nsf_sphere;          /* SphereBody, Boundary.h:318-345 */
+typedef struct nsf_cylinder { int32_t axis; double cx, cy, cz, r; } nsf_cylinder; /* CylinderBody, :287-316 */
+
+/* Every ConfigSettings member (ConfigSettings.h:33-80) plus the case description that the reference
+ * hard-codes in Mesh::setupBoundaries (Mesh.cpp:25-58) and Solver::initialize (Solver.cpp:22-28). */
+typedef struct nsf_config {
+  uint64_t NI, NJ, NK;
+  int32_t stop_criterion; /* 0 = "timesteps", 1 = "end_time" */
+  uint64_t stop_time_level;
+  double t_end;
+  double conv_stability_limit, visc_stability_limit;
+  int32_t n_filter_intervals;
+  uint32_t filter_intervals[NSF_MAX_FILTER_INTERVALS];
+  int32_t n_filter_change_times;
+  double filter_change_times[NSF_MAX_FILTER_INTERVALS];
+  double status_report_interval;
+  int32_t save_density, save_momentum, save_energy, save_velocity, save_pressure, save_temperature,
+      save_viscosity, save_thermal_cond, save_ic, save_final, save_intervals;
+  double save_period, save_intervals_start_time, save_intervals_end_time;
+  int32_t conv_history; /* 0 "none", 1 "density", 2 "all" */
+  double gamma, pr, r_gas, re, sutherlands_c1, sutherlands_c2, m0, t0, lx, ly, lz;
+  double machine_precision_buffer; /* derived: DBL_EPSILON*(lx+ly+lz), ConfigSettings.cpp:160-163 */
+  /* case description */
+  int32_t shipped_case; /* 1: the reference's own hard-coded case (z-cylinder, symmetry y, in/out x) */
+  int32_t bc[3][2];     /* [axis x,y,z][min,max] -> nsf_bc */
+  int32_t n_spheres;
+  nsf_sphere spheres[NSF_MAX_SPHERES];
+  int32_t n_cylinders;
+  nsf_cylinder cylinders[NSF_MAX_CYLINDERS];
+  int32_t ic; /* nsf_ic */
+  double noise_amp;
+  uint64_t seed;
+} nsf_config;
+
+typedef struct nsf_solver nsf_solver;
+
+/* ABI version of the loaded library. */
+int32_t nsf_abi_version(void);
+
+/* Fill *cfg with the values of the reference's shipped ConfigFile and its hard-coded case. */
+nsf_status nsf_config_defaults(nsf_config* cfg);
+
+/* Parse a ConfigFile (libconfig syntax) into *cfg.
+ * Replaces ConfigSettings::ConfigSettings / loadSettings (ConfigSettings.cpp:11-33, :77-163):
+ * same setting names, same strict int/float typing, same consistency check on the filter lists.
+ * An optional `case = { ... }` group describes boundaries, bodies and the initial condition.
+ * On failure returns NSF_ERR_CONFIG and writes a message into err (if err != NULL). */
+nsf_status nsf_config_load(const char* path, nsf_config* cfg, char* err, size_t errlen);
+nsf_status nsf_config_parse(const char* text, nsf_config* cfg, char* err, size_t errlen);
+
+/* Allocate a solver on CUDA device `device`. Replaces Solver::Solver / Mesh::Mesh
+ * (Solver.cpp:13-18, Mesh.cpp:10-21). device = -1 makes a host-only handle: nsf_initialize then runs
+ * the host setup (classification, ghost and filter lists) and no GPU work; marching is refused. */
+nsf_status nsf_create(const nsf_config* cfg, int32_t device, nsf_solver** out);
+
+/* Replaces Solver::initialize (Solver.cpp:22-28): boundary setup and node classification on the host
+ * (bit-exact with Mesh::categorizeNodes, Mesh.cpp:61-82), ghost-node interpolation weights solved on
+ * the device, initial condition, initial dt. */
+nsf_status nsf_initialize(nsf_solver* s);
+
+/* Replaces `nsteps` calls of Solver::marchTimeStep(t, timeLevel) (Solver.cpp:130-167). Asynchronous:
+ * the steps are queued on the handle's stream (one CUDA graph per step). In end_time mode, steps after
+ * t reaches t_end are no-ops, as Simulation::run (Simulation.cpp:19-30) would not call them. */
+nsf_status nsf_march(nsf_solver* s, uint64_t nsteps);
+
+/* Wait for queued work; returns NSF_ERR_NONFINITE if a non-finite conserved value was seen. */
+nsf_status nsf_sync(nsf_solver* s);
+
+/* t, timeLevel and the dt of the next step (Simulation::t, ::timeLevel, Solver::dt). Synchronises. */
+nsf_status nsf_get_time(nsf_solver* s, double* t, uint64_t* time_level, double* dt);
+
+/* Copy selected fields (bit i of field_mask = field i, see NSF_RHO..NSF_KAPPA) to host memory, packed
+ * in increasing field order, N doubles each, reference layout. Replaces reading Mesh's public arrays
+ * (Mesh.h:82-86), as OutputManager does (OutputManager.cpp:152-258). Synchronises. */
+nsf_status nsf_download(nsf_solver* s, uint32_t field_mask, double* host);
+
+/* Overwrite the current conserved fields (5 x N doubles: rho, rho_u, rho_v, rho_w, rho_E) from host
+ * memory at every node. The stored primitive state is not recomputed, exactly as writing
+ * Mesh::conservedVariables directly would leave it. */
+nsf_status nsf_upload_conserved(nsf_solver* s, const double* host);
+
+/* Node classification (NodeTypeEnum values, Node.h:27-34), N bytes. */
+nsf_status nsf_get_node_types(nsf_solver* s, uint8_t* out);
+/* Number of immersed bodies and, per body, ghost / filter counts and how many ghosts the image-point
+ * closure loop added (Boundary.cpp:910-916). */
+nsf_status nsf_get_num_bodies(nsf_solver* s, uint32_t* nbodies);
+nsf_status nsf_get_body_counts(nsf_solver* s, uint32_t body, uint64_t* nghost, uint64_t* nfilter,
+                               uint64_t* closure_added);
+/* Per ghost, 9 doubles: i, j, k, body-intercept x,y,z, image point x,y,z (GhostNode, Node.h:15-22). */
+nsf_status nsf_get_ghosts(nsf_solver* s, uint32_t body, double* out);
+/* Filter-node indices of a body (ImmersedBoundary::filterNodes, Boundary.h:208). */
+nsf_status nsf_get_filter_nodes(nsf_solver* s, uint32_t body, uint64_t* out);
+
+/* Per-step history rows [first, first+count): t after the step, dt used, and the five change norms
+ * (Solver::storeNormsOfChange, Solver.cpp:510-530; -1 where the norm is not recorded). 7 doubles per row.
+ * *available receives the number of recorded steps. Synchronises. */
+nsf_status nsf_get_history(nsf_solver* s, uint64_t first, uint64_t count, double* out, uint64_t* available);
+
+/* Instrumentation. nsf_march_timed: nsf_march with CUDA events recorded on the handle's stream around
+ * the queued steps; waits and returns the elapsed device time. nsf_profile_steps: runs nsteps steps
+ * launched one kernel at a time (not as a graph) with events around each of the four stage kernels;
+ * returns their mean durations (stage_ms[4]) and the mean step time. Both advance the solution. */
+nsf_status nsf_march_timed(nsf_solver* s, uint64_t nsteps, double* elapsed_ms);
+nsf_status nsf_profile_steps(nsf_solver* s, uint64_t nsteps, double* stage_ms, double* step_ms);
+/* Kernel launches issued per RK4 step (for instrumentation). */
+nsf_status nsf_launches_per_step(nsf_solver* s, uint64_t* launches);
+
+/* Text of the last error on this handle (static storage owned by the handle). */
+const char* nsf_last_error(nsf_solver* s);
+
+void nsf_destroy(nsf_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NSFSI_H */

@@ -160,10 +160,12 @@ def ref_available():
     return os.path.exists(REF_RUNNER)
 
 
-def run_reference(cfg_path, dumps, outdir=None):
+def run_reference(cfg_path, dumps, outdir=None, final=False):
     outdir = outdir or tempfile.mkdtemp(prefix="nsf_ref_")
-    subprocess.run([REF_RUNNER, cfg_path, outdir, "--dump", ",".join(str(d) for d in dumps)], check=True,
-                   stdout=subprocess.DEVNULL)
+    cmd = [REF_RUNNER, cfg_path, outdir, "--dump", ",".join(str(d) for d in dumps)]
+    if final:
+        cmd.append("--final")
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
     return outdir
 
 
@@ -204,7 +206,7 @@ def read_ref_setup(outdir):
 
 
 def read_ref_fields(outdir, level):
-    path = os.path.join(outdir, "fields_%06d.bin" % level)
+    path = os.path.join(outdir, "fields_final.bin" if level == "final" else "fields_%06d.bin" % level)
     raw = np.fromfile(path, dtype=np.float64)
     t, lvl, dt = raw[0], raw[1:2].view(np.uint64)[0], raw[2]
     return dict(t=t, level=int(lvl), dt=dt, fields=raw[3:].reshape(12, -1))

@@ -13,7 +13,9 @@
 // explicit-instantiation access idiom (C++17 [temp.spec]/6), so no reference source is modified.
 // case.kind = "shipped" instead calls Solver::initialize() unchanged (the reference's default case).
 //
-// Usage: ref_runner <case.cfg> <outdir> [--dump s1,s2,...] [--time W K]
+// Usage: ref_runner <case.cfg> <outdir> [--dump s1,s2,...] [--final] [--time W K]
+// The dump loop stops where Simulation::checkStoppingCriterion (Simulation.cpp:34-52) would stop an
+// end_time run; --final then also writes that last state as fields_final.bin.
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -91,6 +93,7 @@ int main(int argc, char** argv) {
   std::string cfgPath = argv[1], outDir = argv[2];
   std::set<unsigned long> dumps;
   long timeWarm = -1, timeSteps = -1;
+  bool dumpFinal = false;
   for (int a = 3; a < argc; ++a) {
     if (!std::strcmp(argv[a], "--dump") && a + 1 < argc) {
       std::string s = argv[++a];
@@ -101,6 +104,8 @@ int main(int argc, char** argv) {
         if (e == std::string::npos) break;
         b = e + 1;
       }
+    } else if (!std::strcmp(argv[a], "--final")) {
+      dumpFinal = true;
     } else if (!std::strcmp(argv[a], "--time") && a + 2 < argc) {
       timeWarm = std::stol(argv[++a]);
       timeSteps = std::stol(argv[++a]);
@@ -254,9 +259,12 @@ int main(int argc, char** argv) {
     o.f64(solver.dt);
   }
 
-  auto dumpFields = [&](double t, unsigned long level) {
+  auto dumpFields = [&](double t, unsigned long level, bool final_ = false) {
     char name[64];
-    std::snprintf(name, sizeof name, "/fields_%06lu.bin", level);
+    if (final_)
+      std::snprintf(name, sizeof name, "/fields_final.bin");
+    else
+      std::snprintf(name, sizeof name, "/fields_%06lu.bin", level);
     FileOut o(outDir + name);
     o.f64(t);
     o.u64(level);
@@ -288,6 +296,7 @@ int main(int argc, char** argv) {
   FileOut hist(outDir + "/history.bin");
   if (dumps.count(0)) dumpFields(t, 0);
   while (timeLevel < lastDump) {
+    if (params.stopCriterion == StopCriterionEnum::end_time && !(t < params.t_end)) break;
     double dtUsed = solver.dt;
     solver.marchTimeStep(t, timeLevel);
     hist.f64(t);
@@ -298,5 +307,6 @@ int main(int argc, char** argv) {
     for (auto* v : hv) hist.f64(v->empty() ? -1.0 : v->back());
     if (dumps.count(timeLevel)) dumpFields(t, timeLevel);
   }
+  if (dumpFinal) dumpFields(t, timeLevel, true);
   return 0;
 }

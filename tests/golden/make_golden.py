@@ -8,7 +8,9 @@ into oracle/_ref/ref_runner):
 For every case file in tests/golden/cases/ it runs the unmodified reference (through oracle/ref_harness.cpp)
 and stores, in <case>.npz: node types, per-body ghost lists (i, j, k, body-intercept point, image point)
 and filter-node lists, the initial dt, the per-step history (t, dt used, dt next, five change norms) and
-all twelve fields (rho, rho_u, rho_v, rho_w, rho_E, u, v, w, p, T, mu, kappa) at the listed steps.
+all twelve fields (rho, rho_u, rho_v, rho_w, rho_E, u, v, w, p, T, mu, kappa) at the listed steps and
+at the last step run (an end_time case stops where Simulation::run stops, so later listed steps are
+replaced by that final step).
 For the 48^3 sphere workload it stores a fixed node subsample of the fields instead of whole arrays.
 """
 import os
@@ -26,7 +28,7 @@ CASES = {
     "sphere_small": ("tests/golden/cases/sphere_small.cfg", [7, 30], None),
     "tgv_small": ("tests/golden/cases/tgv_small.cfg", [25], None),
     "two_spheres": ("tests/golden/cases/two_spheres.cfg", [20], None),
-    "cylinder_sym": ("tests/golden/cases/cylinder_sym.cfg", [24], None),
+    "cylinder_sym": ("tests/golden/cases/cylinder_sym.cfg", [4, 60], None),
     "shipped_small": ("tests/golden/cases/shipped_small.cfg", [40], None),
     "sphere48": ("3d-ns-fsi_b200/cases/sphere48.cfg", [100], 13),
 }
@@ -34,15 +36,19 @@ CASES = {
 
 def make(name):
     cfg, dumps, stride = CASES[name]
-    out = po.run_reference(os.path.join(ROOT, cfg), [0] + dumps)
+    out = po.run_reference(os.path.join(ROOT, cfg), [0] + dumps, final=True)
     s = po.read_ref_setup(out)
     rec = dict(shape=np.array(s["shape"]), geometry=s["geometry"], types=s["types"], dt0=np.array(s["dt0"]),
                history=po.read_ref_history(out), dumps=np.array(dumps), nbodies=np.array(len(s["bodies"])))
     for b, (g, f) in enumerate(s["bodies"]):
         rec["ghosts_%d" % b] = g
         rec["filter_%d" % b] = f
+    fin = po.read_ref_fields(out, "final")
+    rec["final_level"] = np.array(fin["level"])
+    dumps = [d for d in dumps if d < fin["level"]] + [fin["level"]]
+    rec["dumps"] = np.array(dumps)
     for d in dumps:
-        fl = po.read_ref_fields(out, d)
+        fl = fin if d == fin["level"] else po.read_ref_fields(out, d)
         f = fl["fields"]
         if stride:
             idx = np.arange(0, f.shape[1], stride)

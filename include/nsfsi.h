@@ -157,6 +157,21 @@ nsf_status nsf_profile_steps(nsf_solver* s, uint64_t nsteps, double* stage_ms, d
 /* Kernel launches issued per RK4 step (for instrumentation). */
 nsf_status nsf_launches_per_step(nsf_solver* s, uint64_t* launches);
 
+/* End-of-step metrics for conserved fields the caller keeps in device memory, allocating nothing.
+ * No counterpart in the reference: it exists for callers that cannot let a library allocate device
+ * memory -- host frameworks that own all device memory, code running while a stream is captured into a
+ * CUDA graph, real-time loops that must not allocate after start-up. d_old / d_new: 5 x N doubles
+ * (rho, rho_u, rho_v, rho_w, rho_E, reference layout, N = NI*NJ*NK); d_types: N node-type bytes or NULL
+ * (then every node off the mesh faces is interior); d_out: 6 doubles written on `stream` (a
+ * cudaStream_t, NULL = default stream): the five change norms sqrt(dx*dy*dz*sum (old-new)^2) over
+ * interior nodes, then the next dt from the primitive values of d_new at every node (what nsf_march
+ * records when the case has no immersed body). Scratch is a fixed 8 MiB device array inside the library,
+ * so at most 29,826,048 nodes (larger grids: NSF_ERR_ARG). The first call on a device resolves that
+ * array's device address (cudaGetSymbolAddress); make it before any stream capture. Calls that overlap
+ * on the GPU share the array and race: serialise them. */
+nsf_status nsf_step_metrics_noalloc(const nsf_config* cfg, const double* d_old, const double* d_new,
+                                    const uint8_t* d_types, double* d_out, void* stream);
+
 /* Text of the last error on this handle (static storage owned by the handle). */
 const char* nsf_last_error(nsf_solver* s);
 

@@ -1,5 +1,7 @@
 // C ABI implementation (include/nsfsi.h): the solver handle, device residency of all fields, the
 // device-side lists built from the host setup, and one captured CUDA graph per RK4 step.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +39,8 @@ struct nsf_solver {
   long long* dDlNodeIc = nullptr;
   int nDl = 0, nDlIc = 0;
   std::string err;
+  std::vector<CUtensorMap> hostMaps;
+  void* encodeFn = nullptr;
 };
 
 namespace {
@@ -153,31 +157,81 @@ double initial_dt(const nsf_config& c, const HostSetup& s, const std::vector<dou
   return dt;
 }
 
+// Device layout: the reference's i/j/k order with the k rows padded to a pitch NKp (a multiple of 16),
+// so every row of doubles starts on a 128-byte boundary, every row of node-type bytes on a 16-byte
+// boundary, and TMA boxes can start at any tile origin.
+long long dev_index(const HostSetup& S, size_t NKp, size_t n) {
+  const size_t i = n / (S.NJ * S.NK), j = n % (S.NJ * S.NK) / S.NK, k = n % S.NK;
+  return (long long)(i * S.NJ * NKp + j * NKp + k);
+}
+
 nsf_status build_device(nsf_solver* s) {
   const HostSetup& S = s->setup;
   const nsf_config& cfg = s->cfg;
   const size_t N = S.N;
+  const size_t NKp = (S.NK + 15) / 16 * 16;
+  const size_t Nd = S.NI * S.NJ * NKp;
+  auto dev = [&](size_t n) { return dev_index(S, NKp, n); };
   Grid& G = s->hGrid;
   G = Grid{};
   G.NI = int(S.NI);
   G.NJ = int(S.NJ);
   G.NK = int(S.NK);
-  G.sI = (long long)(S.NJ * S.NK);
-  G.sJ = (long long)S.NK;
-  G.N = (long long)N;
+  G.NKp = int(NKp);
+  G.sI = (long long)(S.NJ * NKp);
+  G.sJ = (long long)NKp;
+  G.N = (long long)Nd;
   G.C = make_consts(cfg, S);
 
   // initial condition
   std::vector<double> cons, prim;
   initial_condition(cfg, S, cons, prim);
   double* fields = nullptr;
-  nsf_status st = dalloc(s, &fields, 20 * N);
+  nsf_status st = dalloc(s, &fields, 20 * Nd);
   if (st != NSF_OK) return st;
-  CK(cudaMemset(fields, 0, 20 * N * sizeof(double)));
+  CK(cudaMemset(fields, 0, 20 * Nd * sizeof(double)));
   for (int b = 0; b < 3; ++b)
-    for (int f = 0; f < 5; ++f) G.bufs[b][f] = fields + (size_t(b) * 5 + f) * N;
-  for (int f = 0; f < 5; ++f) G.acc[f] = fields + (15 + size_t(f)) * N;
-  for (int f = 0; f < 5; ++f) CK(cudaMemcpy(G.bufs[0][f], cons.data() + f * N, N * sizeof(double), cudaMemcpyHostToDevice));
+    for (int f = 0; f < 5; ++f) G.bufs[b][f] = fields + (size_t(b) * 5 + f) * Nd;
+  for (int f = 0; f < 5; ++f) G.acc[f] = fields + (15 + size_t(f)) * Nd;
+  for (int f = 0; f < 5; ++f)
+    CK(cudaMemcpy2D(G.bufs[0][f], NKp * sizeof(double), cons.data() + f * N, S.NK * sizeof(double),
+                    S.NK * sizeof(double), S.NI * S.NJ, cudaMemcpyHostToDevice));
+
+  // TMA descriptors: staged planes (box 34 x 10 x 1) and epilogue tiles (34 x 8 x 1) of every physical
+  // buffer field, and epilogue tiles of the accumulator.
+  {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    CK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &qr));
+    if (!fn || qr != cudaDriverEntryPointSuccess) {
+      s->err = "cuTensorMapEncodeTiled is not available from the driver";
+      return NSF_ERR_CUDA;
+    }
+    auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    std::vector<CUtensorMap> maps(stage_num_maps());
+    auto mk = [&](CUtensorMap* m, double* base, cuuint32_t rows) {
+      cuuint64_t gdim[3] = {S.NK, S.NJ, S.NI};
+      cuuint64_t gstr[2] = {NKp * sizeof(double), S.NJ * NKp * sizeof(double)};
+      cuuint32_t box[3] = {cuuint32_t(stage_tile_k() + 2), rows, 1};
+      cuuint32_t es[3] = {1, 1, 1};
+      return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    };
+    const cuuint32_t haloRows = cuuint32_t(stage_tile_j() + 2), tileRows = cuuint32_t(stage_tile_j());
+    bool okMaps = true;
+    for (int b = 0; b < 3; ++b)
+      for (int f = 0; f < 5; ++f) {
+        okMaps &= mk(&maps[b * 5 + f], G.bufs[b][f], haloRows) == CUDA_SUCCESS;
+        okMaps &= mk(&maps[15 + b * 5 + f], G.bufs[b][f], tileRows) == CUDA_SUCCESS;
+      }
+    for (int f = 0; f < 5; ++f) okMaps &= mk(&maps[30 + f], G.acc[f], tileRows) == CUDA_SUCCESS;
+    if (!okMaps) {
+      s->err = "cuTensorMapEncodeTiled rejected a field descriptor";
+      return NSF_ERR_CUDA;
+    }
+    s->hostMaps = maps;
+    s->encodeFn = fn;
+  }
 
   // node types with the filter bit, filter slots
   std::vector<uint8_t> type = S.type;
@@ -194,12 +248,31 @@ nsf_status build_device(nsf_solver* s) {
     fpre[2 * q] = cons[fnode[q]];
     fpre[2 * q + 1] = cons[4 * N + fnode[q]];
   }
+  std::vector<uint8_t> typeDev(Nd, SOLID_INACTIVE);  // pitch padding never takes part
+  for (size_t n = 0; n < N; ++n) typeDev[dev(n)] = type[n];
+  for (auto& f : fnode) f = dev(size_t(f));
   uint8_t* dType;
-  if ((st = upload(s, &dType, type)) != NSF_OK) return st;
+  if ((st = upload(s, &dType, typeDev)) != NSF_OK) return st;
   G.type = dType;
+  {  // node-type boxes (48 x 10 x 1 bytes) for the stage kernel, then all descriptors to the device
+    auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(s->encodeFn);
+    cuuint64_t gdim[3] = {S.NK, S.NJ, S.NI};
+    cuuint64_t gstr[2] = {NKp, S.NJ * NKp};
+    cuuint32_t box[3] = {48, cuuint32_t(stage_tile_j() + 2), 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    if (encode(&s->hostMaps[stage_num_maps() - 1], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dType, gdim, gstr, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+      s->err = "cuTensorMapEncodeTiled rejected the node-type descriptor";
+      return NSF_ERR_CUDA;
+    }
+    CUtensorMap* dMaps = nullptr;
+    if ((st = upload(s, &dMaps, s->hostMaps)) != NSF_OK) return st;
+    G.tmaps = dMaps;
+  }
   G.nFilter = int(fnode.size());
   if (!fnode.empty()) {
-    std::vector<int> fidx(N, -1);
+    std::vector<int> fidx(Nd, -1);
     for (size_t q = 0; q < fnode.size(); ++q) fidx[fnode[q]] = int(q);
     int* dF;
     if ((st = upload(s, &dF, fidx)) != NSF_OK) return st;
@@ -220,7 +293,7 @@ nsf_status build_device(nsf_solver* s) {
   std::vector<uint8_t> gfl;
   for (auto& b : S.bodies)
     for (auto& g : b.ghosts) {
-      gnode.push_back((long long)(g.i * S.NJ * S.NK + g.j * S.NK + g.k));
+      gnode.push_back(dev(g.i * S.NJ * S.NK + g.j * S.NK + g.k));
       Box box;
       surrounding_box(S, g.ip, box);
       int64_t cs[8];
@@ -230,7 +303,7 @@ nsf_status build_device(nsf_solver* s) {
       for (int q = 0; q < 3; ++q) ipl.push_back(g.ip[q]);
       for (int q = 0; q < 3; ++q) ipl.push_back(lo[q]);
       for (int m = 0; m < 8; ++m) {
-        gcell.push_back(cs[m]);
+        gcell.push_back(dev(size_t(cs[m])));
         const size_t cn = size_t(cs[m]);
         if (S.type[cn] == SOLID_GHOST) {
           const GhostRec& og = b.ghosts[b.ghostIndex.at(cn)];
@@ -280,7 +353,7 @@ nsf_status build_device(nsf_solver* s) {
   for (size_t n = 0; n < N; ++n) {
     uint8_t t = S.type[n];
     if (t != SOLID_GHOST && t != SOLID_INACTIVE) continue;
-    snode.push_back((long long)n);
+    snode.push_back(dev(n));
     if (t != SOLID_INACTIVE) continue;
     // Follow periodic copies to the node whose primitive values land here (Boundary.cpp:344-367).
     size_t src = n;
@@ -297,8 +370,8 @@ nsf_status build_device(nsf_solver* s) {
       src = ijk[0] * S.NJ * S.NK + ijk[1] * S.NK + ijk[2];
     }
     if (S.type[src] != SOLID_INACTIVE) dynamic = true;
-    inode.push_back((long long)n);
-    dlNodeIc.push_back((long long)n);
+    inode.push_back(dev(n));
+    dlNodeIc.push_back(dev(n));
     for (int q = 0; q < 7; ++q) dlPrimIc.push_back(prim[q * N + n]);
     if (dynamic) {
       // values copied with the conserved ones from a node whose primitives follow its conserved values
@@ -309,7 +382,7 @@ nsf_status build_device(nsf_solver* s) {
       iprim.push_back(prim[2 * N + src]);
       iprim.push_back(prim[3 * N + src]);
       iprim.push_back(prim[5 * N + src]);
-      dlNode.push_back((long long)n);
+      dlNode.push_back(dev(n));
       for (int q = 0; q < 7; ++q) dlPrim.push_back(prim[q * N + src]);
     }
   }
@@ -351,7 +424,19 @@ nsf_status build_device(nsf_solver* s) {
   const int nj = int((S.NJ - 2 + TJ - 1) / TJ), nk = int((S.NK - 2 + TK - 1) / TK);
   const int tiles = nj * nk, planes = int(S.NI - 2);
   const int slots = s->nSM * occ;
-  const int chunks = std::max(1, std::min(planes, (8 * slots + tiles - 1) / tiles));
+  // i-chunk count: minimise the planes the busiest CTA streams (whole waves of items, each item
+  // streaming its chunk plus two halo planes).
+  int chunks = 1;
+  double best = 1e300;
+  for (int c = 1; c <= planes; ++c) {
+    const int len = (planes + c - 1) / c;
+    const double waves = std::ceil(double(tiles) * c / slots);
+    const double cost = waves * (len + 2);
+    if (cost < best - 1e-9) {
+      best = cost;
+      chunks = c;
+    }
+  }
   const int clen = (planes + chunks - 1) / chunks;
   std::vector<StageItem> items;
   for (int c0 = 1; c0 <= planes; c0 += clen)
@@ -496,6 +581,10 @@ nsf_status nsf_sync(nsf_solver* s) {
   CK(cudaStreamSynchronize(s->stream));
   StepCtl ctl;
   CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  if (ctl.timeout) {
+    s->err = "a bounded wait in the stage kernel gave up; results of the affected steps are invalid";
+    return NSF_ERR_TIMEOUT;
+  }
   if (ctl.nonFinite) {
     s->err = "Non-finite value found in the conserved variables";
     return NSF_ERR_NONFINITE;
@@ -520,21 +609,24 @@ nsf_status nsf_download(nsf_solver* s, uint32_t mask, double* host) {
   CK(cudaStreamSynchronize(s->stream));
   StepCtl ctl;
   CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
-  const size_t N = s->setup.N;
+  const HostSetup& S = s->setup;
+  const size_t N = S.N, NKp = size_t(s->hGrid.NKp), Nd = size_t(s->hGrid.N);
+  const size_t hp = S.NK * sizeof(double), dp = NKp * sizeof(double), rows = S.NI * S.NJ;
   size_t outF = 0;
   for (int f = 0; f < 5; ++f)
-    if (mask & (1u << f)) CK(cudaMemcpy(host + (outF++) * N, s->hGrid.bufs[ctl.perm[f][0]][f], N * sizeof(double),
-                                        cudaMemcpyDeviceToHost));
+    if (mask & (1u << f))
+      CK(cudaMemcpy2D(host + (outF++) * N, hp, s->hGrid.bufs[ctl.perm[f][0]][f], dp, hp, rows, cudaMemcpyDeviceToHost));
   if (mask & 0xFE0u) {
     double* tmp = nullptr;
-    CK(cudaMalloc(&tmp, 7 * N * sizeof(double)));
+    CK(cudaMalloc(&tmp, 7 * Nd * sizeof(double)));
     if (ctl.level == 0)
-      launch_download_prims(s->dGrid, (long long)N, tmp, s->dDlNodeIc, s->dDlPrimIc, s->nDlIc, s->nSM, s->stream);
+      launch_download_prims(s->dGrid, (long long)Nd, tmp, s->dDlNodeIc, s->dDlPrimIc, s->nDlIc, s->nSM, s->stream);
     else
-      launch_download_prims(s->dGrid, (long long)N, tmp, s->dDlNode, s->dDlPrim, s->nDl, s->nSM, s->stream);
+      launch_download_prims(s->dGrid, (long long)Nd, tmp, s->dDlNode, s->dDlPrim, s->nDl, s->nSM, s->stream);
     cudaError_t e = cudaStreamSynchronize(s->stream);
     for (int f = 5; f < 12 && e == cudaSuccess; ++f)
-      if (mask & (1u << f)) e = cudaMemcpy(host + (outF++) * N, tmp + (f - 5) * N, N * sizeof(double), cudaMemcpyDeviceToHost);
+      if (mask & (1u << f))
+        e = cudaMemcpy2D(host + (outF++) * N, hp, tmp + (f - 5) * Nd, dp, hp, rows, cudaMemcpyDeviceToHost);
     cudaFree(tmp);
     if (e != cudaSuccess) return cuda_fail(s, e, "download primitive fields");
   }
@@ -547,10 +639,11 @@ nsf_status nsf_upload_conserved(nsf_solver* s, const double* host) {
   CK(cudaStreamSynchronize(s->stream));
   StepCtl ctl;
   CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
-  const size_t N = s->setup.N;
+  const HostSetup& S = s->setup;
+  const size_t N = S.N, NKp = size_t(s->hGrid.NKp);
   for (int f = 0; f < 5; ++f)
-    CK(cudaMemcpyAsync(s->hGrid.bufs[ctl.perm[f][0]][f], host + f * N, N * sizeof(double), cudaMemcpyHostToDevice,
-                       s->stream));
+    CK(cudaMemcpy2DAsync(s->hGrid.bufs[ctl.perm[f][0]][f], NKp * sizeof(double), host + f * N, S.NK * sizeof(double),
+                         S.NK * sizeof(double), S.NI * S.NJ, cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return NSF_OK;
 }

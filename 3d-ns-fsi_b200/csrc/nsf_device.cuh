@@ -61,6 +61,10 @@ struct StepCtl {
   double* O[4][5];
   double* R[4];           // density used for the primitive variables of the stage input
   int copyMask[4];        // fields whose solid-node values are copied I -> O before the stage's BCs
+  int iPhys[4][5];        // physical buffer of each stage input field (selects its TMA descriptor)
+  int rPhys[4];           // physical buffer of the density used for primitives
+  int u0Phys[5];          // physical buffer of each U0 field
+  int timeout;            // sticky: a bounded device wait gave up (the step's results are invalid)
   double stageT[4];       // boundary-condition time of each stage
   double dtUsed;
   // stage-4 reductions
@@ -75,7 +79,9 @@ struct Grid {
   StepCtl* ctl;
   double* bufs[3][5];
   double* acc[5];
-  const uint8_t* type;    // NodeTypeEnum | FILTER_BIT
+  int NKp;                // k pitch of the device layout (multiple of 4: rows start on 32-byte boundaries)
+  const void* tmaps;      // device array of TMA descriptors (see nsf_stage_tma.cu)
+  const uint8_t* type;    // NodeTypeEnum | FILTER_BIT | EDGE_PLANE_BIT
   const int* fidx;        // node -> filter slot (only read where FILTER_BIT is set)
   double* fpre;           // [F][2] pre-filter rho, rho_E of the last near-body filter
   double* fnew;           // [F][2] filtered values (written back after the ghost update)
@@ -124,7 +130,10 @@ size_t stage_smem_bytes();
 int stage_configure();
 int stage_tile_j();
 int stage_tile_k();
+int stage_threads();
 int stage_occupancy();
+int stage_num_maps();
+void launch_stage(const Grid* dg, const LaunchPlan& L, int s, void* stream);
 int enqueue_step(Grid* dg, const LaunchPlan& L, void* stream);
 // Same sequence, launched eagerly, with events recorded around each of the four stage kernels
 // (events[2*s], events[2*s+1]); used for per-kernel timing.

@@ -3,7 +3,8 @@
 //
 //   k_prologue            stop criterion, filter decision, buffer roles        (Solver.cpp:133-135)
 //   k_density_filter      global 2nd-order density filter, rare              (Mesh.cpp:108-140)
-//   4 x { k_stage         fused RHS + primitive recompute + RK4 combine      (Solver.cpp:141-159, 170-507)
+//   4 x { k_stage_tma     fused RHS + primitive recompute + RK4 combine      (Solver.cpp:141-159, 170-507;
+//                         TMA-fed, warp-specialised: nsf_stage_tma.cu)
 //         k_solid_copy    stale solid-node values, I -> O                    (buffer semantics, see nsf_device.cuh)
 //         k_edge_bc x3    outlet/inlet, then y faces, then z faces           (Boundary.cpp:250-417)
 //         k_body_filter   near-body filter of rho, rho_E                     (Boundary.cpp:618-652)
@@ -18,112 +19,9 @@
 
 #include "nsf_device.cuh"
 #include "nsf_internal.h"
+#include "nsf_physics.cuh"
 
 namespace nsf {
-
-// ----------------------------------------------------------------------------------------------
-// Thermodynamics (updatePrimitiveVariables, Solver.cpp:446-479; derive*, FlowVariableGroupStructs.h).
-// pow(1+T, 1.5) is evaluated as x*sqrt(x); the three divisions by (1+rho) share one reciprocal.
-// Both differ from the reference by rounding only.
-struct Prim {
-  double u, v, w, p, T, mu, ka;
-};
-
-__device__ __forceinline__ Prim prims_of(const Consts& C, double rho, double ru, double rv, double rw, double rE) {
-  Prim q;
-  const double r1 = 1.0 / (rho + 1.0);
-  q.u = ru * r1;
-  q.v = rv * r1;
-  q.w = rw * r1;
-  q.p = C.gm1 * (rE - (rho + 1.0) * 0.5 * (q.u * q.u + q.v * q.v + q.w * q.w));
-  q.T = (C.gamma * q.p - rho) * r1;
-  const double x = 1.0 + q.T;
-  q.mu = x * sqrt(x) * C.sc1 / (C.re * (q.T + C.sc1));
-  q.ka = q.mu * C.pf;
-  return q;
-}
-
-__device__ __forceinline__ double mu_of_T(const Consts& C, double T) {
-  const double x = 1.0 + T;
-  return x * sqrt(x) * C.sc1 / (C.re * (T + C.sc1));
-}
-
-// Conserved values from primitive values (deriveConservedVariables, FlowVariableGroupStructs.h:152-161).
-__device__ __forceinline__ void cons_of(const Consts& C, double u, double v, double w, double p, double T,
-                                        double out[5]) {
-  const double rho = (C.gamma * p - T) / (1.0 + T);
-  out[0] = rho;
-  out[1] = (1.0 + rho) * u;
-  out[2] = (1.0 + rho) * v;
-  out[3] = (1.0 + rho) * w;
-  out[4] = p / C.gm1 + (1.0 + rho) * 0.5 * (u * u + v * v + w * w);
-}
-
-// Non-negative doubles compare like their bit patterns, so maxima reduce with integer atomicMax.
-__device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
-  if (v > 0) atomicMax(a, static_cast<unsigned long long>(__double_as_longlong(v)));
-}
-
-struct DtAcc {
-  double sx = 0, sy = 0, sz = 0, nu = 0;
-  __device__ __forceinline__ void add(const Consts& C, double rho, double u, double v, double w, double p, double mu) {
-    // getInviscidTimeStepLimit / getViscousTimeStepLimit terms, Solver.cpp:100-122
-    const double c = sqrt((1.0 + C.gamma * p) / (1.0 + rho));
-    sx = fmax(sx, c + fabs(u));
-    sy = fmax(sy, c + fabs(v));
-    sz = fmax(sz, c + fabs(w));
-    nu = fmax(nu, mu / (rho + 1.0) * C.vmod);
-  }
-};
-
-__device__ __forceinline__ double warp_max(double v) {
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Linear thread index and thread count of the block (1-D or 2-D blocks).
-__device__ __forceinline__ int block_tid() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
-__device__ __forceinline__ int block_threads() { return blockDim.x * blockDim.y * blockDim.z; }
-
-// Block-wide reduction of the four dt maxima into ctl->mx (order independent). Thread count % 32 == 0.
-__device__ void flush_dt(StepCtl* ctl, DtAcc a, double* scratch /*[4*32]*/) {
-  const int tid = block_tid(), lane = tid & 31, wid = tid >> 5, nw = block_threads() >> 5;
-  double v[4] = {warp_max(a.sx), warp_max(a.sy), warp_max(a.sz), warp_max(a.nu)};
-  __syncthreads();
-  if (lane == 0)
-    for (int q = 0; q < 4; ++q) scratch[q * 32 + wid] = v[q];
-  __syncthreads();
-  if (wid == 0) {
-    for (int q = 0; q < 4; ++q) {
-      double m = lane < nw ? scratch[q * 32 + lane] : 0.0;
-      m = warp_max(m);
-      if (lane == 0) atomic_max_pos(&ctl->mx[q], m);
-    }
-  }
-  __syncthreads();
-}
-
-// Block-wide sums of the five change-norm partials into a per-block slot (fixed order: deterministic).
-__device__ void flush_norms(double* slot, const double s[5], double* scratch /*[5*32]*/) {
-  const int tid = block_tid(), lane = tid & 31, wid = tid >> 5, nw = block_threads() >> 5;
-  double v[5];
-  for (int q = 0; q < 5; ++q) v[q] = warp_sum(s[q]);
-  __syncthreads();
-  if (lane == 0)
-    for (int q = 0; q < 5; ++q) scratch[q * 32 + wid] = v[q];
-  __syncthreads();
-  if (wid == 0)
-    for (int q = 0; q < 5; ++q) {
-      double m = lane < nw ? scratch[q * 32 + lane] : 0.0;
-      m = warp_sum(m);
-      if (lane == 0) slot[q] = m;
-    }
-  __syncthreads();
-}
 
 // ----------------------------------------------------------------------------------------------
 // Prologue: Simulation::checkStoppingCriterion (end_time), Mesh::checkFilterCondition (Mesh.cpp:85-103),
@@ -171,6 +69,17 @@ __global__ void k_prologue(Grid* g) {
     B[0] = cons[0];
   }
   for (int f = 0; f < 5; ++f) {
+    c->u0Phys[f] = old[f];
+    c->iPhys[0][f] = old[f];
+    c->iPhys[1][f] = A[f];
+    c->iPhys[2][f] = B[f];
+    c->iPhys[3][f] = A[f];
+  }
+  c->rPhys[0] = filt ? cons[0] : old[0];
+  c->rPhys[1] = A[0];
+  c->rPhys[2] = B[0];
+  c->rPhys[3] = A[0];
+  for (int f = 0; f < 5; ++f) {
     c->U0[f] = g->bufs[old[f]][f];
     c->I[0][f] = g->bufs[old[f]][f];
     c->O[0][f] = g->bufs[A[f]][f];
@@ -216,280 +125,6 @@ __global__ void k_density_filter(const Grid* __restrict__ g) {
       dst[n] = (6 * src[n] + src[n + sI] + src[n - sI] + src[n + sJ] + src[n - sJ] + src[n + 1] + src[n - 1]) / 12;
     else if (t != SOLID_INACTIVE || (raw & EDGE_PLANE_BIT))
       dst[n] = src[n];
-  }
-}
-
-// ----------------------------------------------------------------------------------------------
-// Fused stage kernel. 2.5-D: a block owns a TJ x TK column tile (k fastest, one thread per column) and
-// marches a chunk of i-planes. Each plane of the tile plus a one-node halo is staged once: the five
-// conserved values are loaded (prefetched one plane ahead into registers), the seven primitive /
-// transport values are computed once per staged node, and eleven values per node go to shared memory
-// in a three-plane ring. The RHS of the reference's five flux loops (Solver.cpp:181-418) is then
-// evaluated from shared memory in the reference's term order, and the RK4 combine
-// (Solver.cpp:435-442, 494-507) is applied in the epilogue with an accumulator acc = k1 + 2k2 + 2k3.
-namespace stage {
-constexpr int TK = 32, TJ = 8, NT = TK * TJ;
-constexpr int HK = TK + 2, HJ = TJ + 2, HP = HK * HJ;  // staged plane: tile + halo (with corners)
-constexpr int NV = 11;                                  // ru rv rw rE u v w p T mu ka
-constexpr int PER_THREAD = (HP + NT - 1) / NT;          // staged nodes per thread (2)
-enum { RU, RV, RW, RE, U, V, W, P, TT, MU, KA };
-constexpr size_t SMEM = size_t(3) * NV * HP * sizeof(double) + 3 * HP + 16 * 32 * sizeof(double);
-}  // namespace stage
-
-struct Staged {  // one staged node held in registers between its load and its shared-memory store
-  double rho, ru, rv, rw, rE, rhoP, rEP;
-  uint8_t type;
-  bool valid;
-};
-
-__device__ __forceinline__ void stage_load(const Grid& G, const StepCtl& c, int s, int i, int j0, int k0, int q,
-                                           Staged& st) {
-  using namespace stage;
-  const int hj = q / HK, hk = q - hj * HK;
-  const int j = j0 - 1 + hj, k = k0 - 1 + hk;
-  st.valid = (q < HP) && (j < G.NJ) && (k < G.NK) && (i < G.NI);
-  if (!st.valid) return;
-  const long long n = i * G.sI + j * G.sJ + k;
-  st.type = G.type[n];
-  st.rho = c.R[s][n];
-  st.ru = c.I[s][1][n];
-  st.rv = c.I[s][2][n];
-  st.rw = c.I[s][3][n];
-  st.rE = c.I[s][4][n];
-  st.rhoP = st.rho;
-  st.rEP = st.rE;
-  if (st.type & FILTER_BIT) {  // primitives of a filtered node are those before the filter
-    const int f = G.fidx[n];
-    st.rhoP = G.fpre[2 * f];
-    st.rEP = G.fpre[2 * f + 1];
-  }
-}
-
-__device__ __forceinline__ void stage_store(const Consts& C, double* __restrict__ sm, uint8_t* __restrict__ st8,
-                                            int slot, int q, const Staged& st) {
-  using namespace stage;
-  if (!st.valid) return;
-  double* b = sm + size_t(slot) * NV * HP;
-  const Prim p = prims_of(C, st.rhoP, st.ru, st.rv, st.rw, st.rEP);
-  b[RU * HP + q] = st.ru;
-  b[RV * HP + q] = st.rv;
-  b[RW * HP + q] = st.rw;
-  b[RE * HP + q] = st.rE;
-  b[U * HP + q] = p.u;
-  b[V * HP + q] = p.v;
-  b[W * HP + q] = p.w;
-  b[P * HP + q] = p.p;
-  b[TT * HP + q] = p.T;
-  b[MU * HP + q] = p.mu;
-  b[KA * HP + q] = p.ka;
-  st8[slot * HP + q] = st.type;
-}
-
-// Right-hand side at one node from the three staged planes (W = i-1, P = i, E = i+1).
-__device__ __forceinline__ void rhs_node(const Consts& C, const double* __restrict__ sW, const double* __restrict__ sP,
-                                         const double* __restrict__ sE, int c, double out[5]) {
-  using namespace stage;
-  constexpr int jn = HK, jk = 1;
-#define F_(b, v, o) (b)[(v)*HP + c + (o)]
-  // neighbours in the centre plane: N/S = j+-1, U/D = k+-1
-  const int oN = jn, oS = -jn, oU = jk, oD = -jk;
-  // ---- continuity, Solver.cpp:181-196
-  {
-    const double fx = C.ax * (F_(sE, RU, 0) - F_(sW, RU, 0));
-    const double fy = C.ay * (F_(sP, RV, oN) - F_(sP, RV, oS));
-    const double fz = C.az * (F_(sP, RW, oU) - F_(sP, RW, oD));
-    out[0] = fx + fy + fz;
-  }
-  const double muP = F_(sP, MU, 0), muE = F_(sE, MU, 0), muW = F_(sW, MU, 0), muN = F_(sP, MU, oN),
-               muS = F_(sP, MU, oS), muU = F_(sP, MU, oU), muD = F_(sP, MU, oD);
-  const double uP = F_(sP, U, 0), uE = F_(sE, U, 0), uW = F_(sW, U, 0), uN = F_(sP, U, oN), uS = F_(sP, U, oS),
-               uU = F_(sP, U, oU), uD = F_(sP, U, oD);
-  const double vP = F_(sP, V, 0), vE = F_(sE, V, 0), vW = F_(sW, V, 0), vN = F_(sP, V, oN), vS = F_(sP, V, oS),
-               vU = F_(sP, V, oU), vD = F_(sP, V, oD);
-  const double wP = F_(sP, W, 0), wE = F_(sE, W, 0), wW = F_(sW, W, 0), wN = F_(sP, W, oN), wS = F_(sP, W, oS),
-               wU = F_(sP, W, oU), wD = F_(sP, W, oD);
-  const double pE = F_(sE, P, 0), pW = F_(sW, P, 0), pN = F_(sP, P, oN), pS = F_(sP, P, oS), pU = F_(sP, P, oU),
-               pD = F_(sP, P, oD);
-  // edge neighbours: velocity values only
-  const double vEN = F_(sE, V, oN), vES = F_(sE, V, oS), vWN = F_(sW, V, oN), vWS = F_(sW, V, oS);
-  const double uEN = F_(sE, U, oN), uES = F_(sE, U, oS), uWN = F_(sW, U, oN), uWS = F_(sW, U, oS);
-  const double wEU = F_(sE, W, oU), wED = F_(sE, W, oD), wWU = F_(sW, W, oU), wWD = F_(sW, W, oD);
-  const double uEU = F_(sE, U, oU), uED = F_(sE, U, oD), uWU = F_(sW, U, oU), uWD = F_(sW, U, oD);
-  const double wNU = F_(sP, W, oN + oU), wND = F_(sP, W, oN + oD), wSU = F_(sP, W, oS + oU), wSD = F_(sP, W, oS + oD);
-  const double vNU = F_(sP, V, oN + oU), vND = F_(sP, V, oN + oD), vSU = F_(sP, V, oS + oU), vSD = F_(sP, V, oS + oD);
-  // ---- x-momentum, Solver.cpp:199-243
-  {
-    const double ruE = F_(sE, RU, 0), ruW = F_(sW, RU, 0), ruN = F_(sP, RU, oN), ruS = F_(sP, RU, oS),
-                 ruU = F_(sP, RU, oU), ruD = F_(sP, RU, oD);
-    const double cX = C.ax * (ruE * uE + pE - ruW * uW - pW);
-    const double cY = C.ay * (ruN * vN - ruS * vS);
-    const double cZ = C.az * (ruU * wU - ruD * wD);
-    const double vXX = C.xm_xx * ((muE + muP) * (uE - uP) - (muW + muP) * (uP - uW));
-    const double vYY = C.xm_yy * ((muN + muP) * (uN - uP) - (muS + muP) * (uP - uS));
-    const double vZZ = C.xm_zz * ((muU + muP) * (uU - uP) - (muD + muP) * (uP - uD));
-    const double vXY = C.xm_xy * (muN * (vEN - vWN) - muS * (vES - vWS));
-    const double vYX = C.xm_yx * (muE * (vEN - vES) - muW * (vWN - vWS));
-    const double vXZ = C.xm_xz * (muU * (wEU - wWU) - muD * (wED - wWD));
-    const double vZX = C.xm_zx * (muE * (wEU - wED) - muW * (wWU - wWD));
-    out[1] = cX + cY + cZ + vXX + vYY + vZZ + vXY + vYX + vXZ + vZX;
-  }
-  // ---- y-momentum, Solver.cpp:246-290
-  {
-    const double rvE = F_(sE, RV, 0), rvW = F_(sW, RV, 0), rvN = F_(sP, RV, oN), rvS = F_(sP, RV, oS),
-                 rvU = F_(sP, RV, oU), rvD = F_(sP, RV, oD);
-    const double cX = C.ax * (rvE * uE - rvW * uW);
-    const double cY = C.ay * (rvN * vN + pN - rvS * vS - pS);
-    const double cZ = C.az * (rvU * wU - rvD * wD);
-    const double vXX = C.ym_xx * ((muE + muP) * (vE - vP) - (muW + muP) * (vP - vW));
-    const double vYY = C.ym_yy * ((muN + muP) * (vN - vP) - (muS + muP) * (vP - vS));
-    const double vZZ = C.ym_zz * ((muU + muP) * (vU - vP) - (muD + muP) * (vP - vD));
-    const double vYX = C.ym_yx * (muE * (uEN - uES) - muW * (uWN - uWS));
-    const double vXY = C.ym_xy * (muN * (uEN - uWN) - muS * (uES - uWS));
-    const double vYZ = C.ym_yz * (muU * (wNU - wSU) - muD * (wND - wSD));
-    const double vZY = C.ym_zy * (muN * (wNU - wND) - muS * (wSU - wSD));
-    out[2] = cX + cY + cZ + vXX + vYY + vZZ + vYX + vXY + vYZ + vZY;
-  }
-  // ---- z-momentum, Solver.cpp:293-339
-  {
-    const double rwE = F_(sE, RW, 0), rwW = F_(sW, RW, 0), rwN = F_(sP, RW, oN), rwS = F_(sP, RW, oS),
-                 rwU = F_(sP, RW, oU), rwD = F_(sP, RW, oD);
-    const double cX = C.ax * (rwE * uE - rwW * uW);
-    const double cY = C.ay * (rwN * vN - rwS * vS);
-    const double cZ = C.az * (rwU * wU + pU - rwD * wD - pD);
-    const double vXX = C.zm_xx * ((muE + muP) * (wE - wP) - (muW + muP) * (wP - wW));
-    const double vYY = C.zm_yy * ((muN + muP) * (wN - wP) - (muS + muP) * (wP - wS));
-    const double vZZ = C.zm_zz * ((muU + muP) * (wU - wP) - (muD + muP) * (wP - wD));
-    const double vZX = C.zm_zx * (muE * (uEU - uED) - muW * (uWU - uWD));
-    const double vXZ = C.zm_xz * (muU * (uEU - uWU) - muD * (uED - uWD));
-    const double vZY = C.zm_zy * (muN * (vNU - vND) - muS * (vSU - vSD));
-    const double vYZ = C.zm_yz * (muU * (vNU - vSU) - muD * (vND - vSD));
-    out[3] = cX + cY + cZ + vXX + vYY + vZZ + vZX + vXZ + vZY + vYZ;
-  }
-  // ---- energy, Solver.cpp:342-418
-  {
-    const double H0 = C.h0;
-    const double EE = F_(sE, RE, 0), EW = F_(sW, RE, 0), EN = F_(sP, RE, oN), ES = F_(sP, RE, oS),
-                 EU = F_(sP, RE, oU), ED = F_(sP, RE, oD);
-    const double inv = C.ax * ((H0 + EE + pE) * uE - (H0 + EW + pW) * uW) +
-                       C.ay * ((H0 + EN + pN) * vN - (H0 + ES + pS) * vS) +
-                       C.az * ((H0 + EU + pU) * wU - (H0 + ED + pD) * wD);
-    const double vfX = C.e_xx23 * ((muE * uE + muP * uP) * (uE - uP) - (muW * uW + muP * uP) * (uP - uW)) +
-                       C.e_xx12 * ((muE * vE + muP * vP) * (vE - vP) - (muW * vW + muP * vP) * (vP - vW)) +
-                       C.e_xx12 * ((muE * wE + muP * wP) * (wE - wP) - (muW * wW + muP * wP) * (wP - wW)) +
-                       C.e_yx6 * (muE * uE * (vEN - vES) - muW * uW * (vWN - vWS)) +
-                       C.e_zx6 * (muE * uE * (wEU - wED) - muW * uW * (wWU - wWD)) +
-                       C.e_yx4 * (muE * vE * (uEN - uES) - muW * vW * (uWN - uWS)) +
-                       C.e_zx4 * (muE * wE * (uEU - uED) - muW * wW * (uWU - uWD));
-    const double vfY = C.e_yy12 * ((muN * uN + muP * uP) * (uN - uP) - (muS * uS + muP * uP) * (uP - uS)) +
-                       C.e_yy23 * ((muN * vN + muP * vP) * (vN - vP) - (muS * vS + muP * vP) * (vP - vS)) +
-                       C.e_yy12 * ((muN * wN + muP * wP) * (wN - wP) - (muS * wS + muP * wP) * (wP - wS)) +
-                       C.e_yx6 * (muN * vN * (uEN - uWN) - muS * vS * (uES - uWS)) +
-                       C.e_zy6 * (muN * vN * (wNU - wND) - muS * vS * (wSU - wSD)) +
-                       C.e_yx4 * (muN * uN * (vEN - vWN) - muS * uS * (vES - vWS)) +
-                       C.e_zy4 * (muN * wN * (vNU - vND) - muS * wS * (vSU - vSD));
-    const double vfZ = C.e_zz12 * ((muU * uU + muP * uP) * (uU - uP) - (muD * uD + muP * uP) * (uP - uD)) +
-                       C.e_zz12 * ((muU * vU + muP * vP) * (vU - vP) - (muD * vD + muP * vP) * (vP - vD)) +
-                       C.e_zz23 * ((muU * wU + muP * wP) * (wU - wP) - (muD * wD + muP * wP) * (wP - wD)) +
-                       C.e_zx6 * (muU * wU * (uEU - uWU) - muD * wD * (uED - uWD)) +
-                       C.e_zy6 * (muU * wU * (vNU - vSU) - muD * wD * (vND - vSD)) +
-                       C.e_zx4 * (muU * uU * (wEU - wWU) - muD * uD * (wED - wWD)) +
-                       C.e_zy4 * (muU * vU * (wNU - wSU) - muD * vD * (wND - wSD));
-    const double kP = F_(sP, KA, 0), TP = F_(sP, TT, 0);
-    const double hf = C.e_xx12 * ((F_(sE, KA, 0) + kP) * (F_(sE, TT, 0) - TP) - (F_(sW, KA, 0) + kP) * (TP - F_(sW, TT, 0))) +
-                      C.e_yy12 * ((F_(sP, KA, oN) + kP) * (F_(sP, TT, oN) - TP) - (F_(sP, KA, oS) + kP) * (TP - F_(sP, TT, oS))) +
-                      C.e_zz12 * ((F_(sP, KA, oU) + kP) * (F_(sP, TT, oU) - TP) - (F_(sP, KA, oD) + kP) * (TP - F_(sP, TT, oD)));
-    out[4] = inv + vfX + vfY + vfZ + hf;
-  }
-#undef F_
-}
-
-__global__ void __launch_bounds__(stage::NT, 2)
-    k_stage(const Grid* __restrict__ gp, const StageItem* __restrict__ items, int nItems, int s) {
-  using namespace stage;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  double* sm = reinterpret_cast<double*>(smraw);
-  uint8_t* st8 = smraw + size_t(3) * NV * HP * sizeof(double);
-  double* red = reinterpret_cast<double*>(st8 + 3 * HP + (8 - (3 * HP) % 8) % 8);
-  __shared__ Grid G;
-  __shared__ StepCtl ctl;
-  if (threadIdx.x == 0) {
-    G = *gp;
-    ctl = *gp->ctl;
-  }
-  __syncthreads();
-  if (!ctl.active) return;
-  const Consts& C = G.C;
-  const int tid = threadIdx.x, tx = tid % TK, ty = tid / TK;
-  const int cidx = (ty + 1) * HK + (tx + 1);
-  const double dtUsed = ctl.dtUsed;
-  const double inc = (s == 2) ? dtUsed : dtUsed / 2;  // dt/2, dt/2, dt (Solver.cpp:142-152)
-  const double dtFactor = dtUsed / 6;                 // Solver.cpp:501
-  double nsum[5] = {0, 0, 0, 0, 0};
-  DtAcc dta;
-  int bad = 0;
-
-  for (int it = blockIdx.x; it < nItems; it += gridDim.x) {
-    const StageItem w = items[it];
-    const int j = w.j0 + ty, k = w.k0 + tx;
-    Staged pre[PER_THREAD];
-    // prime the ring with planes i0-1 and i0, prefetch i0+1
-    for (int pl = 0; pl < 2; ++pl) {
-      const int i = w.i0 - 1 + pl;
-      for (int r = 0; r < PER_THREAD; ++r) {
-        Staged st;
-        stage_load(G, ctl, s, i, w.j0, w.k0, tid + r * NT, st);
-        stage_store(C, sm, st8, (i + 3) % 3, tid + r * NT, st);
-      }
-    }
-    for (int r = 0; r < PER_THREAD; ++r) stage_load(G, ctl, s, w.i0 + 1, w.j0, w.k0, tid + r * NT, pre[r]);
-    for (int i = w.i0; i <= w.i1; ++i) {
-      for (int r = 0; r < PER_THREAD; ++r) stage_store(C, sm, st8, (i + 1) % 3, tid + r * NT, pre[r]);
-      __syncthreads();
-      if (i + 2 <= w.i1 + 1)
-        for (int r = 0; r < PER_THREAD; ++r) stage_load(G, ctl, s, i + 2, w.j0, w.k0, tid + r * NT, pre[r]);
-      const uint8_t t = st8[(i % 3) * HP + cidx];
-      if (j <= G.NJ - 2 && k <= G.NK - 2 && (t & TYPE_MASK) == FLUID_INTERIOR) {
-        double kk[5];
-        rhs_node(C, sm + size_t((i + 2) % 3) * NV * HP, sm + size_t(i % 3) * NV * HP, sm + size_t((i + 1) % 3) * NV * HP,
-                 cidx, kk);
-        const long long n = i * G.sI + j * G.sJ + k;
-        if (s == 0) {
-          for (int f = 0; f < 5; ++f) {
-            G.acc[f][n] = kk[f];
-            ctl.O[0][f][n] = ctl.U0[f][n] + inc * kk[f];
-          }
-        } else if (s < 3) {
-          for (int f = 0; f < 5; ++f) {
-            G.acc[f][n] = G.acc[f][n] + 2 * kk[f];
-            ctl.O[s][f][n] = ctl.U0[f][n] + inc * kk[f];
-          }
-        } else {
-          double un[5], u0[5];
-          for (int f = 0; f < 5; ++f) {
-            u0[f] = ctl.U0[f][n];
-            un[f] = u0[f] + dtFactor * (G.acc[f][n] + kk[f]);
-            ctl.O[3][f][n] = un[f];
-            bad |= !isfinite(un[f]);
-          }
-          const bool filtered = (t & FILTER_BIT) != 0;  // rho, rho_E change again in the near-body filter
-          for (int f = 0; f < 5; ++f) {
-            if (filtered && (f == 0 || f == 4)) continue;
-            const double d = u0[f] - un[f];
-            nsum[f] += d * d;
-          }
-          if (!filtered) {
-            const Prim q = prims_of(C, un[0], un[1], un[2], un[3], un[4]);
-            dta.add(C, un[0], q.u, q.v, q.w, q.p, q.mu);
-          }
-        }
-      }
-      __syncthreads();
-    }
-  }
-  if (s == 3) {
-    flush_dt(gp->ctl, dta, red);
-    flush_norms(G.normPart + 5 * blockIdx.x, nsum, red);
-    if (bad) atomicOr(&gp->ctl->nonFinite, 1);
   }
 }
 
@@ -923,23 +558,6 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 
 // ----------------------------------------------------------------------------------------------
 // Host-side launch helpers (called from nsf_capi.cpp).
-size_t stage_smem_bytes() { return stage::SMEM + 64; }
-
-int stage_configure() {
-  return int(cudaFuncSetAttribute(k_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stage_smem_bytes())));
-}
-
-int stage_tile_j() { return stage::TJ; }
-int stage_tile_k() { return stage::TK; }
-int stage_threads() { return stage::NT; }
-
-int stage_occupancy() {
-  int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stage, stage::NT, stage_smem_bytes());
-  return nb;
-}
-
-// Enqueue one RK4 step. Returns the number of kernel launches.
 static int enqueue_impl(Grid* dg, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev) {
   int launches = 0;
   k_prologue<<<1, 32, 0, st>>>(dg);
@@ -948,7 +566,7 @@ static int enqueue_impl(Grid* dg, const LaunchPlan& L, cudaStream_t st, cudaEven
   ++launches;
   for (int s = 0; s < 4; ++s) {
     if (ev) cudaEventRecord(ev[2 * s], st);
-    k_stage<<<L.stageBlocks, stage::NT, stage_smem_bytes(), st>>>(dg, L.items, L.nItems, s);
+    launch_stage(dg, L, s, st);
     if (ev) cudaEventRecord(ev[2 * s + 1], st);
     ++launches;
     if (L.hasSolid) {

@@ -1,0 +1,358 @@
+// Device helpers shared by the kernels: thermodynamics (primitive values from conserved values and
+// back), dt-limit terms, block reductions, and the right-hand side of the reference's five flux loops.
+#ifndef NSF_PHYSICS_CUH
+#define NSF_PHYSICS_CUH
+
+#include "nsf_device.cuh"
+
+namespace nsf {
+
+// ----------------------------------------------------------------------------------------------
+// Thermodynamics (updatePrimitiveVariables, Solver.cpp:446-479; derive*, FlowVariableGroupStructs.h).
+// pow(1+T, 1.5) is evaluated as x*sqrt(x); the three divisions by (1+rho) share one reciprocal.
+// Both differ from the reference by rounding only.
+struct Prim {
+  double u, v, w, p, T, mu, ka;
+};
+
+__device__ __forceinline__ Prim prims_of(const Consts& C, double rho, double ru, double rv, double rw, double rE) {
+  Prim q;
+  const double r1 = 1.0 / (rho + 1.0);
+  q.u = ru * r1;
+  q.v = rv * r1;
+  q.w = rw * r1;
+  q.p = C.gm1 * (rE - (rho + 1.0) * 0.5 * (q.u * q.u + q.v * q.v + q.w * q.w));
+  q.T = (C.gamma * q.p - rho) * r1;
+  const double x = 1.0 + q.T;
+  q.mu = x * sqrt(x) * C.sc1 / (C.re * (q.T + C.sc1));
+  q.ka = q.mu * C.pf;
+  return q;
+}
+
+__device__ __forceinline__ double mu_of_T(const Consts& C, double T) {
+  const double x = 1.0 + T;
+  return x * sqrt(x) * C.sc1 / (C.re * (T + C.sc1));
+}
+
+// Conserved values from primitive values (deriveConservedVariables, FlowVariableGroupStructs.h:152-161).
+__device__ __forceinline__ void cons_of(const Consts& C, double u, double v, double w, double p, double T,
+                                        double out[5]) {
+  const double rho = (C.gamma * p - T) / (1.0 + T);
+  out[0] = rho;
+  out[1] = (1.0 + rho) * u;
+  out[2] = (1.0 + rho) * v;
+  out[3] = (1.0 + rho) * w;
+  out[4] = p / C.gm1 + (1.0 + rho) * 0.5 * (u * u + v * v + w * w);
+}
+
+// Non-negative doubles compare like their bit patterns, so maxima reduce with integer atomicMax.
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
+  if (v > 0) atomicMax(a, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+struct DtAcc {
+  double sx = 0, sy = 0, sz = 0, nu = 0;
+  __device__ __forceinline__ void add(const Consts& C, double rho, double u, double v, double w, double p, double mu) {
+    // getInviscidTimeStepLimit / getViscousTimeStepLimit terms, Solver.cpp:100-122
+    const double c = sqrt((1.0 + C.gamma * p) / (1.0 + rho));
+    sx = fmax(sx, c + fabs(u));
+    sy = fmax(sy, c + fabs(v));
+    sz = fmax(sz, c + fabs(w));
+    nu = fmax(nu, mu / (rho + 1.0) * C.vmod);
+  }
+};
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Linear thread index and thread count of the block (1-D or 2-D blocks).
+__device__ __forceinline__ int block_tid() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+__device__ __forceinline__ int block_threads() { return blockDim.x * blockDim.y * blockDim.z; }
+
+// Block-wide reduction of the four dt maxima into ctl->mx (order independent). Thread count % 32 == 0.
+__device__ inline void flush_dt(StepCtl* ctl, DtAcc a, double* scratch /*[4*32]*/) {
+  const int tid = block_tid(), lane = tid & 31, wid = tid >> 5, nw = block_threads() >> 5;
+  double v[4] = {warp_max(a.sx), warp_max(a.sy), warp_max(a.sz), warp_max(a.nu)};
+  __syncthreads();
+  if (lane == 0)
+    for (int q = 0; q < 4; ++q) scratch[q * 32 + wid] = v[q];
+  __syncthreads();
+  if (wid == 0) {
+    for (int q = 0; q < 4; ++q) {
+      double m = lane < nw ? scratch[q * 32 + lane] : 0.0;
+      m = warp_max(m);
+      if (lane == 0) atomic_max_pos(&ctl->mx[q], m);
+    }
+  }
+  __syncthreads();
+}
+
+// Block-wide sums of the five change-norm partials into a per-block slot (fixed order: deterministic).
+__device__ inline void flush_norms(double* slot, const double s[5], double* scratch /*[5*32]*/) {
+  const int tid = block_tid(), lane = tid & 31, wid = tid >> 5, nw = block_threads() >> 5;
+  double v[5];
+  for (int q = 0; q < 5; ++q) v[q] = warp_sum(s[q]);
+  __syncthreads();
+  if (lane == 0)
+    for (int q = 0; q < 5; ++q) scratch[q * 32 + wid] = v[q];
+  __syncthreads();
+  if (wid == 0)
+    for (int q = 0; q < 5; ++q) {
+      double m = lane < nw ? scratch[q * 32 + lane] : 0.0;
+      m = warp_sum(m);
+      if (lane == 0) slot[q] = m;
+    }
+  __syncthreads();
+}
+
+
+// Right-hand side of the five flux loops at one node (continuity Solver.cpp:181-196, x/y/z momentum
+// :199-339, energy :342-418), terms evaluated in the reference's order. Inputs are three staged planes
+// (W = i-1, P = i, E = i+1), each holding the conserved values (fields 0..4: rho, rho_u, rho_v, rho_w,
+// rho_E) and the primitive / transport values (fields 0..6: u, v, w, p, T, mu, kappa) of a (j, k) tile
+// with a one-node halo, rows of HK values, field stride FS. c = index of the node in its plane.
+template <int HK, int FS>
+__device__ __forceinline__ void rhs_eval(const Consts& C, const double* __restrict__ cW, const double* __restrict__ cP,
+                                         const double* __restrict__ cE, const double* __restrict__ pW,
+                                         const double* __restrict__ pP, const double* __restrict__ pE, int c,
+                                         double out[5]) {
+  enum { RU = 1, RV = 2, RW = 3, RE = 4 };
+  enum { U = 0, V = 1, W = 2, P = 3, TT = 4, MU = 5, KA = 6 };
+#define F_(b, v, o) (b)[(v)*FS + c + (o)]
+  constexpr int oN = HK, oS = -HK, oU = 1, oD = -1;
+  {
+    const double fx = C.ax * (F_(cE, RU, 0) - F_(cW, RU, 0));
+    const double fy = C.ay * (F_(cP, RV, oN) - F_(cP, RV, oS));
+    const double fz = C.az * (F_(cP, RW, oU) - F_(cP, RW, oD));
+    out[0] = fx + fy + fz;
+  }
+  const double muP = F_(pP, MU, 0), muE = F_(pE, MU, 0), muW = F_(pW, MU, 0), muN = F_(pP, MU, oN),
+               muS = F_(pP, MU, oS), muU = F_(pP, MU, oU), muD = F_(pP, MU, oD);
+  const double uP = F_(pP, U, 0), uE = F_(pE, U, 0), uW = F_(pW, U, 0), uN = F_(pP, U, oN), uS = F_(pP, U, oS),
+               uU = F_(pP, U, oU), uD = F_(pP, U, oD);
+  const double vP = F_(pP, V, 0), vE = F_(pE, V, 0), vW = F_(pW, V, 0), vN = F_(pP, V, oN), vS = F_(pP, V, oS),
+               vU = F_(pP, V, oU), vD = F_(pP, V, oD);
+  const double wP = F_(pP, W, 0), wE = F_(pE, W, 0), wW = F_(pW, W, 0), wN = F_(pP, W, oN), wS = F_(pP, W, oS),
+               wU = F_(pP, W, oU), wD = F_(pP, W, oD);
+  const double pE_ = F_(pE, P, 0), pW_ = F_(pW, P, 0), pN = F_(pP, P, oN), pS = F_(pP, P, oS), pU = F_(pP, P, oU),
+               pD = F_(pP, P, oD);
+  const double vEN = F_(pE, V, oN), vES = F_(pE, V, oS), vWN = F_(pW, V, oN), vWS = F_(pW, V, oS);
+  const double uEN = F_(pE, U, oN), uES = F_(pE, U, oS), uWN = F_(pW, U, oN), uWS = F_(pW, U, oS);
+  const double wEU = F_(pE, W, oU), wED = F_(pE, W, oD), wWU = F_(pW, W, oU), wWD = F_(pW, W, oD);
+  const double uEU = F_(pE, U, oU), uED = F_(pE, U, oD), uWU = F_(pW, U, oU), uWD = F_(pW, U, oD);
+  const double wNU = F_(pP, W, oN + oU), wND = F_(pP, W, oN + oD), wSU = F_(pP, W, oS + oU), wSD = F_(pP, W, oS + oD);
+  const double vNU = F_(pP, V, oN + oU), vND = F_(pP, V, oN + oD), vSU = F_(pP, V, oS + oU), vSD = F_(pP, V, oS + oD);
+  {
+    const double ruE = F_(cE, RU, 0), ruW = F_(cW, RU, 0), ruN = F_(cP, RU, oN), ruS = F_(cP, RU, oS),
+                 ruU = F_(cP, RU, oU), ruD = F_(cP, RU, oD);
+    const double cX = C.ax * (ruE * uE + pE_ - ruW * uW - pW_);
+    const double cY = C.ay * (ruN * vN - ruS * vS);
+    const double cZ = C.az * (ruU * wU - ruD * wD);
+    const double vXX = C.xm_xx * ((muE + muP) * (uE - uP) - (muW + muP) * (uP - uW));
+    const double vYY = C.xm_yy * ((muN + muP) * (uN - uP) - (muS + muP) * (uP - uS));
+    const double vZZ = C.xm_zz * ((muU + muP) * (uU - uP) - (muD + muP) * (uP - uD));
+    const double vXY = C.xm_xy * (muN * (vEN - vWN) - muS * (vES - vWS));
+    const double vYX = C.xm_yx * (muE * (vEN - vES) - muW * (vWN - vWS));
+    const double vXZ = C.xm_xz * (muU * (wEU - wWU) - muD * (wED - wWD));
+    const double vZX = C.xm_zx * (muE * (wEU - wED) - muW * (wWU - wWD));
+    out[1] = cX + cY + cZ + vXX + vYY + vZZ + vXY + vYX + vXZ + vZX;
+  }
+  {
+    const double rvE = F_(cE, RV, 0), rvW = F_(cW, RV, 0), rvN = F_(cP, RV, oN), rvS = F_(cP, RV, oS),
+                 rvU = F_(cP, RV, oU), rvD = F_(cP, RV, oD);
+    const double cX = C.ax * (rvE * uE - rvW * uW);
+    const double cY = C.ay * (rvN * vN + pN - rvS * vS - pS);
+    const double cZ = C.az * (rvU * wU - rvD * wD);
+    const double vXX = C.ym_xx * ((muE + muP) * (vE - vP) - (muW + muP) * (vP - vW));
+    const double vYY = C.ym_yy * ((muN + muP) * (vN - vP) - (muS + muP) * (vP - vS));
+    const double vZZ = C.ym_zz * ((muU + muP) * (vU - vP) - (muD + muP) * (vP - vD));
+    const double vYX = C.ym_yx * (muE * (uEN - uES) - muW * (uWN - uWS));
+    const double vXY = C.ym_xy * (muN * (uEN - uWN) - muS * (uES - uWS));
+    const double vYZ = C.ym_yz * (muU * (wNU - wSU) - muD * (wND - wSD));
+    const double vZY = C.ym_zy * (muN * (wNU - wND) - muS * (wSU - wSD));
+    out[2] = cX + cY + cZ + vXX + vYY + vZZ + vYX + vXY + vYZ + vZY;
+  }
+  {
+    const double rwE = F_(cE, RW, 0), rwW = F_(cW, RW, 0), rwN = F_(cP, RW, oN), rwS = F_(cP, RW, oS),
+                 rwU = F_(cP, RW, oU), rwD = F_(cP, RW, oD);
+    const double cX = C.ax * (rwE * uE - rwW * uW);
+    const double cY = C.ay * (rwN * vN - rwS * vS);
+    const double cZ = C.az * (rwU * wU + pU - rwD * wD - pD);
+    const double vXX = C.zm_xx * ((muE + muP) * (wE - wP) - (muW + muP) * (wP - wW));
+    const double vYY = C.zm_yy * ((muN + muP) * (wN - wP) - (muS + muP) * (wP - wS));
+    const double vZZ = C.zm_zz * ((muU + muP) * (wU - wP) - (muD + muP) * (wP - wD));
+    const double vZX = C.zm_zx * (muE * (uEU - uED) - muW * (uWU - uWD));
+    const double vXZ = C.zm_xz * (muU * (uEU - uWU) - muD * (uED - uWD));
+    const double vZY = C.zm_zy * (muN * (vNU - vND) - muS * (vSU - vSD));
+    const double vYZ = C.zm_yz * (muU * (vNU - vSU) - muD * (vND - vSD));
+    out[3] = cX + cY + cZ + vXX + vYY + vZZ + vZX + vXZ + vZY + vYZ;
+  }
+  {
+    const double H0 = C.h0;
+    const double EE = F_(cE, RE, 0), EW = F_(cW, RE, 0), EN = F_(cP, RE, oN), ES = F_(cP, RE, oS),
+                 EU = F_(cP, RE, oU), ED = F_(cP, RE, oD);
+    const double inv = C.ax * ((H0 + EE + pE_) * uE - (H0 + EW + pW_) * uW) +
+                       C.ay * ((H0 + EN + pN) * vN - (H0 + ES + pS) * vS) +
+                       C.az * ((H0 + EU + pU) * wU - (H0 + ED + pD) * wD);
+    const double vfX = C.e_xx23 * ((muE * uE + muP * uP) * (uE - uP) - (muW * uW + muP * uP) * (uP - uW)) +
+                       C.e_xx12 * ((muE * vE + muP * vP) * (vE - vP) - (muW * vW + muP * vP) * (vP - vW)) +
+                       C.e_xx12 * ((muE * wE + muP * wP) * (wE - wP) - (muW * wW + muP * wP) * (wP - wW)) +
+                       C.e_yx6 * (muE * uE * (vEN - vES) - muW * uW * (vWN - vWS)) +
+                       C.e_zx6 * (muE * uE * (wEU - wED) - muW * uW * (wWU - wWD)) +
+                       C.e_yx4 * (muE * vE * (uEN - uES) - muW * vW * (uWN - uWS)) +
+                       C.e_zx4 * (muE * wE * (uEU - uED) - muW * wW * (uWU - uWD));
+    const double vfY = C.e_yy12 * ((muN * uN + muP * uP) * (uN - uP) - (muS * uS + muP * uP) * (uP - uS)) +
+                       C.e_yy23 * ((muN * vN + muP * vP) * (vN - vP) - (muS * vS + muP * vP) * (vP - vS)) +
+                       C.e_yy12 * ((muN * wN + muP * wP) * (wN - wP) - (muS * wS + muP * wP) * (wP - wS)) +
+                       C.e_yx6 * (muN * vN * (uEN - uWN) - muS * vS * (uES - uWS)) +
+                       C.e_zy6 * (muN * vN * (wNU - wND) - muS * vS * (wSU - wSD)) +
+                       C.e_yx4 * (muN * uN * (vEN - vWN) - muS * uS * (vES - vWS)) +
+                       C.e_zy4 * (muN * wN * (vNU - vND) - muS * wS * (vSU - vSD));
+    const double vfZ = C.e_zz12 * ((muU * uU + muP * uP) * (uU - uP) - (muD * uD + muP * uP) * (uP - uD)) +
+                       C.e_zz12 * ((muU * vU + muP * vP) * (vU - vP) - (muD * vD + muP * vP) * (vP - vD)) +
+                       C.e_zz23 * ((muU * wU + muP * wP) * (wU - wP) - (muD * wD + muP * wP) * (wP - wD)) +
+                       C.e_zx6 * (muU * wU * (uEU - uWU) - muD * wD * (uED - uWD)) +
+                       C.e_zy6 * (muU * wU * (vNU - vSU) - muD * wD * (vND - vSD)) +
+                       C.e_zx4 * (muU * uU * (wEU - wWU) - muD * uD * (wED - wWD)) +
+                       C.e_zy4 * (muU * vU * (wNU - wSU) - muD * vD * (wND - wSD));
+    const double kP = F_(pP, KA, 0), TP = F_(pP, TT, 0);
+    const double hf = C.e_xx12 * ((F_(pE, KA, 0) + kP) * (F_(pE, TT, 0) - TP) - (F_(pW, KA, 0) + kP) * (TP - F_(pW, TT, 0))) +
+                      C.e_yy12 * ((F_(pP, KA, oN) + kP) * (F_(pP, TT, oN) - TP) - (F_(pP, KA, oS) + kP) * (TP - F_(pP, TT, oS))) +
+                      C.e_zz12 * ((F_(pP, KA, oU) + kP) * (F_(pP, TT, oU) - TP) - (F_(pP, KA, oD) + kP) * (TP - F_(pP, TT, oD)));
+    out[4] = inv + vfX + vfY + vfZ + hf;
+  }
+#undef F_
+}
+
+// ---------------------------------------------------------------------------------------------------
+// The same right-hand side split by direction, for kernels that stream along i and keep the thread's
+// own (j, k) column in registers. For the x direction the reference's terms are differences of
+// per-node quantities and of per-face quantities along the column:
+//   x-part(P) = [G(E) - G(W)] + [F(P,E) - F(W,P)]
+// with G the convective/inviscid flux and the mixed-derivative products of a node, and F the normal
+// viscous and heat-flux products of an x-face, e.g. for x-momentum
+//   G = ax (rho_u u + p) + xm_yx mu (v_N - v_S) + xm_zx mu (w_U - w_D),   F = xm_xx (mu_a + mu_b)(u_b - u_a).
+// F(W,P) is bit-for-bit the reference's (mu_W + mu_P)(u_P - u_W) (addition commutes); G differences
+// regroup the reference's sums and differ from it by rounding only.
+struct XNode {  // G of one node for the five equations
+  double g[5];
+};
+struct XOwn {  // a node's values that the next x-face needs
+  double mu, u, v, w, T, ka;
+};
+
+// G at one node. own: rho_u, rho_v, rho_w, rho_E, u, v, w, p, mu; d*: in-plane differences at the node
+// (v_N - v_S, u_N - u_S, w_U - w_D, u_U - u_D).
+__device__ __forceinline__ XNode x_node(const Consts& C, double ru, double rv, double rw, double rE, double u,
+                                        double v, double w, double p, double mu, double dyv, double dyu, double dzw,
+                                        double dzu) {
+  XNode n;
+  n.g[0] = C.ax * ru;
+  n.g[1] = C.ax * (ru * u + p) + C.xm_yx * (mu * dyv) + C.xm_zx * (mu * dzw);
+  n.g[2] = C.ax * (rv * u) + C.ym_yx * (mu * dyu);
+  n.g[3] = C.ax * (rw * u) + C.zm_zx * (mu * dzu);
+  n.g[4] = C.ax * ((C.h0 + rE + p) * u) + C.e_yx6 * (mu * u * dyv) + C.e_zx6 * (mu * u * dzw) +
+           C.e_yx4 * (mu * v * dyu) + C.e_zx4 * (mu * w * dzu);
+  return n;
+}
+
+// F of the x-face between a (lower i) and b.
+__device__ __forceinline__ void x_face(const Consts& C, const XOwn& a, const XOwn& b, double f[5]) {
+  const double ms = a.mu + b.mu;
+  f[0] = 0.0;
+  f[1] = C.xm_xx * (ms * (b.u - a.u));
+  f[2] = C.ym_xx * (ms * (b.v - a.v));
+  f[3] = C.zm_xx * (ms * (b.w - a.w));
+  f[4] = C.e_xx23 * ((a.mu * a.u + b.mu * b.u) * (b.u - a.u)) + C.e_xx12 * ((a.mu * a.v + b.mu * b.v) * (b.v - a.v)) +
+         C.e_xx12 * ((a.mu * a.w + b.mu * b.w) * (b.w - a.w)) + C.e_xx12 * ((a.ka + b.ka) * (b.T - a.T));
+}
+
+// y- and z-direction part of the right-hand side at P (the reference's terms not covered by G and F).
+// cP/pP: staged centre plane; pE/pW: staged neighbour planes (only their N/S/U/D velocity values are
+// read, for the mixed x-derivatives at the in-plane neighbours); own: P's own values.
+template <int HK, int FS>
+__device__ __forceinline__ void yz_part(const Consts& C, const double* __restrict__ cP, const double* __restrict__ pW,
+                                        const double* __restrict__ pP, const double* __restrict__ pE, int c,
+                                        const XOwn& own, double out[5]) {
+  enum { RU = 1, RV = 2, RW = 3, RE = 4 };
+  enum { U = 0, V = 1, W = 2, P = 3, TT = 4, MU = 5, KA = 6 };
+#define F_(b, v, o) (b)[(v)*FS + c + (o)]
+  constexpr int oN = HK, oS = -HK, oU = 1, oD = -1;
+  const double muP = own.mu, uP = own.u, vP = own.v, wP = own.w, TP = own.T, kP = own.ka;
+  const double muN = F_(pP, MU, oN), muS = F_(pP, MU, oS), muU = F_(pP, MU, oU), muD = F_(pP, MU, oD);
+  const double uN = F_(pP, U, oN), uS = F_(pP, U, oS), uU = F_(pP, U, oU), uD = F_(pP, U, oD);
+  const double vN = F_(pP, V, oN), vS = F_(pP, V, oS), vU = F_(pP, V, oU), vD = F_(pP, V, oD);
+  const double wN = F_(pP, W, oN), wS = F_(pP, W, oS), wU = F_(pP, W, oU), wD = F_(pP, W, oD);
+  const double pN = F_(pP, P, oN), pS = F_(pP, P, oS), pU = F_(pP, P, oU), pD = F_(pP, P, oD);
+  const double vEN = F_(pE, V, oN), vES = F_(pE, V, oS), vWN = F_(pW, V, oN), vWS = F_(pW, V, oS);
+  const double uEN = F_(pE, U, oN), uES = F_(pE, U, oS), uWN = F_(pW, U, oN), uWS = F_(pW, U, oS);
+  const double wEU = F_(pE, W, oU), wED = F_(pE, W, oD), wWU = F_(pW, W, oU), wWD = F_(pW, W, oD);
+  const double uEU = F_(pE, U, oU), uED = F_(pE, U, oD), uWU = F_(pW, U, oU), uWD = F_(pW, U, oD);
+  const double wNU = F_(pP, W, oN + oU), wND = F_(pP, W, oN + oD), wSU = F_(pP, W, oS + oU), wSD = F_(pP, W, oS + oD);
+  const double vNU = F_(pP, V, oN + oU), vND = F_(pP, V, oN + oD), vSU = F_(pP, V, oS + oU), vSD = F_(pP, V, oS + oD);
+  out[0] = C.ay * (F_(cP, RV, oN) - F_(cP, RV, oS)) + C.az * (F_(cP, RW, oU) - F_(cP, RW, oD));
+  {
+    const double ruN = F_(cP, RU, oN), ruS = F_(cP, RU, oS), ruU = F_(cP, RU, oU), ruD = F_(cP, RU, oD);
+    const double cY = C.ay * (ruN * vN - ruS * vS);
+    const double cZ = C.az * (ruU * wU - ruD * wD);
+    const double vYY = C.xm_yy * ((muN + muP) * (uN - uP) - (muS + muP) * (uP - uS));
+    const double vZZ = C.xm_zz * ((muU + muP) * (uU - uP) - (muD + muP) * (uP - uD));
+    const double vXY = C.xm_xy * (muN * (vEN - vWN) - muS * (vES - vWS));
+    const double vXZ = C.xm_xz * (muU * (wEU - wWU) - muD * (wED - wWD));
+    out[1] = cY + cZ + vYY + vZZ + vXY + vXZ;
+  }
+  {
+    const double rvN = F_(cP, RV, oN), rvS = F_(cP, RV, oS), rvU = F_(cP, RV, oU), rvD = F_(cP, RV, oD);
+    const double cY = C.ay * (rvN * vN + pN - rvS * vS - pS);
+    const double cZ = C.az * (rvU * wU - rvD * wD);
+    const double vYY = C.ym_yy * ((muN + muP) * (vN - vP) - (muS + muP) * (vP - vS));
+    const double vZZ = C.ym_zz * ((muU + muP) * (vU - vP) - (muD + muP) * (vP - vD));
+    const double vXY = C.ym_xy * (muN * (uEN - uWN) - muS * (uES - uWS));
+    const double vYZ = C.ym_yz * (muU * (wNU - wSU) - muD * (wND - wSD));
+    const double vZY = C.ym_zy * (muN * (wNU - wND) - muS * (wSU - wSD));
+    out[2] = cY + cZ + vYY + vZZ + vXY + vYZ + vZY;
+  }
+  {
+    const double rwN = F_(cP, RW, oN), rwS = F_(cP, RW, oS), rwU = F_(cP, RW, oU), rwD = F_(cP, RW, oD);
+    const double cY = C.ay * (rwN * vN - rwS * vS);
+    const double cZ = C.az * (rwU * wU + pU - rwD * wD - pD);
+    const double vYY = C.zm_yy * ((muN + muP) * (wN - wP) - (muS + muP) * (wP - wS));
+    const double vZZ = C.zm_zz * ((muU + muP) * (wU - wP) - (muD + muP) * (wP - wD));
+    const double vXZ = C.zm_xz * (muU * (uEU - uWU) - muD * (uED - uWD));
+    const double vZY = C.zm_zy * (muN * (vNU - vND) - muS * (vSU - vSD));
+    const double vYZ = C.zm_yz * (muU * (vNU - vSU) - muD * (vND - vSD));
+    out[3] = cY + cZ + vYY + vZZ + vXZ + vZY + vYZ;
+  }
+  {
+    const double H0 = C.h0;
+    const double EN = F_(cP, RE, oN), ES = F_(cP, RE, oS), EU = F_(cP, RE, oU), ED = F_(cP, RE, oD);
+    const double inv = C.ay * ((H0 + EN + pN) * vN - (H0 + ES + pS) * vS) + C.az * ((H0 + EU + pU) * wU - (H0 + ED + pD) * wD);
+    const double vfY = C.e_yy12 * ((muN * uN + muP * uP) * (uN - uP) - (muS * uS + muP * uP) * (uP - uS)) +
+                       C.e_yy23 * ((muN * vN + muP * vP) * (vN - vP) - (muS * vS + muP * vP) * (vP - vS)) +
+                       C.e_yy12 * ((muN * wN + muP * wP) * (wN - wP) - (muS * wS + muP * wP) * (wP - wS)) +
+                       C.e_yx6 * (muN * vN * (uEN - uWN) - muS * vS * (uES - uWS)) +
+                       C.e_zy6 * (muN * vN * (wNU - wND) - muS * vS * (wSU - wSD)) +
+                       C.e_yx4 * (muN * uN * (vEN - vWN) - muS * uS * (vES - vWS)) +
+                       C.e_zy4 * (muN * wN * (vNU - vND) - muS * wS * (vSU - vSD));
+    const double vfZ = C.e_zz12 * ((muU * uU + muP * uP) * (uU - uP) - (muD * uD + muP * uP) * (uP - uD)) +
+                       C.e_zz12 * ((muU * vU + muP * vP) * (vU - vP) - (muD * vD + muP * vP) * (vP - vD)) +
+                       C.e_zz23 * ((muU * wU + muP * wP) * (wU - wP) - (muD * wD + muP * wP) * (wP - wD)) +
+                       C.e_zx6 * (muU * wU * (uEU - uWU) - muD * wD * (uED - uWD)) +
+                       C.e_zy6 * (muU * wU * (vNU - vSU) - muD * wD * (vND - vSD)) +
+                       C.e_zx4 * (muU * uU * (wEU - wWU) - muD * uD * (wED - wWD)) +
+                       C.e_zy4 * (muU * vU * (wNU - wSU) - muD * vD * (wND - wSD));
+    const double hf = C.e_yy12 * ((F_(pP, KA, oN) + kP) * (F_(pP, TT, oN) - TP) - (F_(pP, KA, oS) + kP) * (TP - F_(pP, TT, oS))) +
+                      C.e_zz12 * ((F_(pP, KA, oU) + kP) * (F_(pP, TT, oU) - TP) - (F_(pP, KA, oD) + kP) * (TP - F_(pP, TT, oD)));
+    out[4] = inv + vfY + vfZ + hf;
+  }
+#undef F_
+}
+
+}  // namespace nsf
+#endif

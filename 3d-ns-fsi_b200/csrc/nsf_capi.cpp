@@ -419,6 +419,10 @@ nsf_status build_device(nsf_solver* s) {
   L = LaunchPlan{};
   L.nSM = s->nSM;
   CK(cudaError_t(stage_configure()));
+  if (!stage_register_split_ok()) {
+    s->err = "stage kernel: its launch registers do not cover its setmaxnreg split";
+    return NSF_ERR_CUDA;
+  }
   const int occ = std::max(1, stage_occupancy());
   const int TJ = stage_tile_j(), TK = stage_tile_k();
   const int nj = int((S.NJ - 2 + TJ - 1) / TJ), nk = int((S.NK - 2 + TK - 1) / TK);
@@ -497,7 +501,7 @@ nsf_status build_device(nsf_solver* s) {
 
   // one step as a CUDA graph
   CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-  s->launchesPerStep = enqueue_step(s->dGrid, L, s->stream);
+  s->launchesPerStep = enqueue_step(s->dGrid, G, L, s->stream);
   CK(cudaStreamEndCapture(s->stream, &s->graph));
   CK(cudaGraphInstantiate(&s->graphExec, s->graph, 0));
   return NSF_OK;
@@ -740,7 +744,7 @@ nsf_status nsf_profile_steps(nsf_solver* s, uint64_t nsteps, double* stage_ms, d
   CK(cudaEventRecord(ev[0], s->stream));
   for (uint64_t q = 0; q < nsteps; ++q) {
     cudaEvent_t* se = ev.data() + 2 + 8 * q;
-    enqueue_step_profiled(s->dGrid, s->plan, s->stream, se);
+    enqueue_step_profiled(s->dGrid, s->hGrid, s->plan, s->stream, se);
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(ev[1], s->stream));

@@ -133,11 +133,17 @@ int stage_tile_k();
 int stage_threads();
 int stage_occupancy();
 int stage_num_maps();
-void launch_stage(const Grid* dg, const LaunchPlan& L, int s, void* stream);
-int enqueue_step(Grid* dg, const LaunchPlan& L, void* stream);
+// Registers per thread the stage kernel is launched with; stage_register_split_ok() checks that the
+// kernel's setmaxnreg split fits in them (a split above the launch total would never be granted).
+int stage_launch_registers();
+bool stage_register_split_ok();
+void launch_stage(const Grid& hg, const LaunchPlan& L, int s, void* stream);
+// dg: the grid in device memory (read by the small kernels); hg: the same grid on the host (passed by
+// value to the stage kernel, whose coefficients then come from the constant bank).
+int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream);
 // Same sequence, launched eagerly, with events recorded around each of the four stage kernels
 // (events[2*s], events[2*s+1]); used for per-kernel timing.
-int enqueue_step_profiled(Grid* dg, const LaunchPlan& L, void* stream, void* events);
+int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events);
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,
                           double dx, double dy, double dz, double* w, void* stream);
 void launch_download_prims(const Grid* dg, long long N, double* out, const long long* inodes, const double* ip7,

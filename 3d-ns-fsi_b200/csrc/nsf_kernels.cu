@@ -3,8 +3,8 @@
 //
 //   k_prologue            stop criterion, filter decision, buffer roles        (Solver.cpp:133-135)
 //   k_density_filter      global 2nd-order density filter, rare              (Mesh.cpp:108-140)
-//   4 x { k_stage_tma     fused RHS + primitive recompute + RK4 combine      (Solver.cpp:141-159, 170-507;
-//                         TMA-fed, warp-specialised: nsf_stage_tma.cu)
+//   4 x { k_stage_ws      fused RHS + primitive recompute + RK4 combine      (Solver.cpp:141-159, 170-507;
+//                         TMA-fed, warp-specialised: nsf_stage_ws.cu)
 //         k_solid_copy    stale solid-node values, I -> O                    (buffer semantics, see nsf_device.cuh)
 //         k_edge_bc x3    outlet/inlet, then y faces, then z faces           (Boundary.cpp:250-417)
 //         k_body_filter   near-body filter of rho, rho_E                     (Boundary.cpp:618-652)
@@ -558,7 +558,7 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 
 // ----------------------------------------------------------------------------------------------
 // Host-side launch helpers (called from nsf_capi.cpp).
-static int enqueue_impl(Grid* dg, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev) {
+static int enqueue_impl(Grid* dg, const Grid& hg, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev) {
   int launches = 0;
   k_prologue<<<1, 32, 0, st>>>(dg);
   ++launches;
@@ -566,7 +566,7 @@ static int enqueue_impl(Grid* dg, const LaunchPlan& L, cudaStream_t st, cudaEven
   ++launches;
   for (int s = 0; s < 4; ++s) {
     if (ev) cudaEventRecord(ev[2 * s], st);
-    launch_stage(dg, L, s, st);
+    launch_stage(hg, L, s, st);
     if (ev) cudaEventRecord(ev[2 * s + 1], st);
     ++launches;
     if (L.hasSolid) {
@@ -592,12 +592,12 @@ static int enqueue_impl(Grid* dg, const LaunchPlan& L, cudaStream_t st, cudaEven
   return launches;
 }
 
-int enqueue_step(Grid* dg, const LaunchPlan& L, void* stream) {
-  return enqueue_impl(dg, L, static_cast<cudaStream_t>(stream), nullptr);
+int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream) {
+  return enqueue_impl(dg, hg, L, static_cast<cudaStream_t>(stream), nullptr);
 }
 
-int enqueue_step_profiled(Grid* dg, const LaunchPlan& L, void* stream, void* events) {
-  return enqueue_impl(dg, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events));
+int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events) {
+  return enqueue_impl(dg, hg, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events));
 }
 
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,

@@ -1,0 +1,464 @@
+// Fused RK4 stage kernel for sm_100a: TMA-fed, warp-specialised, 2.5-D plane streaming along i.
+//
+// One CTA of 384 threads per SM, persistent over a static list of work items (a TJ x TK tile of (j, k)
+// columns and a chunk of i-planes). Three warpgroups with separate jobs, decoupled by mbarrier rings:
+//
+//   warpgroup 0, warp 0, lane 0 -- producer: issues cp.async.bulk.tensor (TMA) loads as soon as a ring
+//     slot is free: for every staged i-plane the five conserved fields and the node types of the tile
+//     plus a one-node halo (box 34 x 10) into the conserved ring, and for every computed plane the U0
+//     and RK4-accumulator tile (box 34 x 8) into the epilogue ring. It never blocks on one slot, so no
+//     ordering between the rings can deadlock.
+//   warpgroup 0, warps 1-3 -- staging: the primitive and transport values (u, v, w, p, T, mu, kappa) of
+//     the 340 staged nodes of each plane, once per plane, into the primitive ring. Filtered nodes take
+//     their values from before the near-body filter, as the reference does (its primitives are not
+//     recomputed after the filter).
+//   warpgroups 1-2 -- columns: one thread per (j, k) column of the tile. For each plane the thread forms
+//     its node's x-direction quantities (G of the node, F of the face towards the previous plane,
+//     see x_node / x_face in nsf_physics.cuh) and carries them in registers along the column; the
+//     RHS of the previous plane is then G/F differences plus the y/z terms read from the staged planes,
+//     and the RK4 combine is written with coalesced 256-byte row stores.
+// Warpgroup 0 runs with 72 registers per thread and the column warpgroups with 216 (setmaxnreg), so
+// the register-hungry RHS does not spill while the CTA still has twelve warps.
+//
+// Ring slots have a "full" and an "empty" mbarrier. Every wait is bounded: a wait that gives up sets
+// StepCtl::timeout and a CTA-wide abort flag that ends every other wait at once; the producer then
+// waits (bounded) for every copy it issued before the CTA exits.
+//
+// Algorithmic HBM bytes per node: stage 1 reads U0 (40) and writes U1 and acc (80); stages 2-3 read
+// U_s, U0, acc (120) and write U_{s+1}, acc (80); stage 4 reads U3, U0, acc (120) and writes U_new (40).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "nsf_device.cuh"
+#include "nsf_internal.h"
+#include "nsf_physics.cuh"
+
+namespace nsf {
+namespace ws {
+constexpr int TK = 32, TJ = 8, NCOL = TK * TJ;   // column threads (warpgroups 1-2)
+constexpr int NTHREADS = 128 + NCOL;
+constexpr int NSTAGE = 96;                        // staging threads (warps 1-3)
+constexpr int HK = TK + 2, HJ = TJ + 2, HP = HK * HJ;
+constexpr int FS = 352;                           // doubles per staged field (2816 B, a multiple of 128 B)
+constexpr int EFS = HK * TJ;                      // doubles per epilogue field (2176 B = 17 x 128 B)
+constexpr int NC = 5, NP = 4, NE = 3;             // conserved / primitive / epilogue ring depths
+constexpr int TYW = 48;                           // row width of the staged node-type box (bytes, >= HK)
+constexpr uint32_t CONS_BOX_BYTES = HK * HJ * 8;
+constexpr uint32_t TYPE_BOX_BYTES = TYW * HJ;
+constexpr uint32_t EPI_BOX_BYTES = HK * TJ * 8;
+constexpr size_t TYPE_OFF = size_t(5) * FS * 8;  // node types follow the five fields in a staged slot
+constexpr size_t CONS_SLOT = TYPE_OFF + 512;
+constexpr size_t PRIM_SLOT = size_t(7) * FS * 8;
+constexpr size_t EPI_SLOT = size_t(10) * EFS * 8;
+constexpr size_t OFF_CONS = 0;
+constexpr size_t OFF_PRIM = OFF_CONS + NC * CONS_SLOT;
+constexpr size_t OFF_EPI = OFF_PRIM + NP * PRIM_SLOT;
+constexpr size_t OFF_BAR = OFF_EPI + NE * EPI_SLOT;
+constexpr size_t OFF_FLAG = OFF_BAR + 2 * (NC + NP + NE) * 8;
+constexpr size_t OFF_RED = (OFF_FLAG + 16 + 127) / 128 * 128;
+constexpr size_t OFF_CTL = OFF_RED + 5 * 32 * 8;
+constexpr size_t SMEM = OFF_CTL + ((sizeof(StepCtl) + 127) / 128) * 128;
+static_assert(OFF_PRIM % 128 == 0 && OFF_EPI % 128 == 0 && CONS_SLOT % 128 == 0 && TYPE_OFF % 128 == 0,
+              "TMA destinations need 128 B alignment");
+static_assert(TYPE_BOX_BYTES <= 512, "type box fits its slot region");
+static_assert(SMEM <= 227 * 1024, "shared memory budget");
+static_assert(NSTAGE * 4 >= HP, "four staging passes cover a plane");
+constexpr int MAP_CONS = 0, MAP_EPI = 15, MAP_ACC = 30, MAP_TYPE = 35, NMAPS = 36;
+constexpr long long WAIT_LIMIT = 1ll << 22;  // polls before a wait is declared failed
+// Register split (setmaxnreg): the launch gives every thread 168 registers (384 x 168 = 64,512); the
+// split must not exceed that total: 128 x 72 + 256 x 216 = 64,512.
+constexpr int REG_LAUNCH = 168, REG_LOW = 72, REG_HIGH = 216;
+static_assert(128 * REG_LOW + NCOL * REG_HIGH <= NTHREADS * REG_LAUNCH, "register split exceeds the launch total");
+}  // namespace ws
+
+namespace {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the completion of the phase with the given parity; gives up early when another
+// thread has raised the CTA's abort flag.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, const volatile int* abortFlag) {
+  for (long long it = 0; it < ws::WAIT_LIMIT; ++it) {
+    if (mbar_try(b, parity)) return true;
+    if (*abortFlag) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load3(void* dst, const void* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+template <int N>
+__device__ __forceinline__ void reg_dealloc() {
+  asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(N));
+}
+template <int N>
+__device__ __forceinline__ void reg_alloc() {
+  asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(N));
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(ws::NTHREADS, 1)
+    k_stage_ws(const __grid_constant__ Grid G, const StageItem* __restrict__ items, int nItems, int s) {
+  using namespace ws;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  uint64_t* consFull = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
+  uint64_t* consEmpty = consFull + NC;
+  uint64_t* primFull = consEmpty + NC;
+  uint64_t* primEmpty = primFull + NP;
+  uint64_t* epiFull = primEmpty + NP;
+  uint64_t* epiEmpty = epiFull + NE;
+  volatile int* abortFlag = reinterpret_cast<volatile int*>(sm + OFF_FLAG);
+  double* red = reinterpret_cast<double*>(sm + OFF_RED);
+  StepCtl& ctl = *reinterpret_cast<StepCtl*>(sm + OFF_CTL);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    ctl = *G.ctl;
+    *abortFlag = 0;
+    for (int q = 0; q < NC; ++q) {
+      mbar_init(&consFull[q], 1);
+      mbar_init(&consEmpty[q], NCOL / 32);
+    }
+    for (int q = 0; q < NP; ++q) {
+      mbar_init(&primFull[q], NSTAGE / 32);
+      mbar_init(&primEmpty[q], NCOL / 32);
+    }
+    for (int q = 0; q < NE; ++q) {
+      mbar_init(&epiFull[q], 1);
+      mbar_init(&epiEmpty[q], NCOL / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (!ctl.active) return;
+  const Consts& C = G.C;
+  DtAcc dta;
+  double nsum[5] = {0, 0, 0, 0, 0};
+  int bad = 0;
+  auto fail = [&]() {
+    *abortFlag = 1;
+    atomicExch(&G.ctl->timeout, 1);
+  };
+
+  if (warp < 4) {
+    reg_dealloc<REG_LOW>();
+    if (warp == 0) {
+      // ------------------------------------------------------------------ producer (one thread)
+      if (lane == 0) {
+        const CUtensorMap* maps = static_cast<const CUtensorMap*>(G.tmaps);
+        const int epiFields = s == 0 ? 5 : 10;
+        int cIt = blockIdx.x, cP = cIt < nItems ? items[cIt].i0 - 1 : 0;  // next staged plane
+        int eIt = blockIdx.x, eP = eIt < nItems ? items[eIt].i0 : 0;      // next computed plane
+        uint32_t cq = 0, eq = 0;
+        long long idle = 0;
+        while ((cIt < nItems || eIt < nItems) && !*abortFlag) {
+          bool progressed = false;
+          if (cIt < nItems) {
+            const uint32_t sl = cq % NC;
+            if (cq < NC || mbar_try(&consEmpty[sl], ((cq / NC) - 1) & 1)) {
+              const StageItem w = items[cIt];
+              unsigned char* dst = sm + OFF_CONS + sl * CONS_SLOT;
+              mbar_expect_tx(&consFull[sl], 5 * CONS_BOX_BYTES + TYPE_BOX_BYTES);
+              tma_load3(dst, &maps[MAP_CONS + ctl.rPhys[s] * 5 + 0], w.k0 - 1, w.j0 - 1, cP, &consFull[sl]);
+              for (int f = 1; f < 5; ++f)
+                tma_load3(dst + size_t(f) * FS * 8, &maps[MAP_CONS + ctl.iPhys[s][f] * 5 + f], w.k0 - 1, w.j0 - 1, cP,
+                          &consFull[sl]);
+              tma_load3(dst + TYPE_OFF, &maps[MAP_TYPE], w.k0 - 1, w.j0 - 1, cP, &consFull[sl]);
+              ++cq;
+              if (++cP > w.i1 + 1) {
+                cIt += gridDim.x;
+                if (cIt < nItems) cP = items[cIt].i0 - 1;
+              }
+              progressed = true;
+            }
+          }
+          if (eIt < nItems) {
+            const uint32_t se = eq % NE;
+            if (eq < NE || mbar_try(&epiEmpty[se], ((eq / NE) - 1) & 1)) {
+              const StageItem w = items[eIt];
+              unsigned char* dst = sm + OFF_EPI + se * EPI_SLOT;
+              mbar_expect_tx(&epiFull[se], epiFields * EPI_BOX_BYTES);
+              for (int f = 0; f < 5; ++f)
+                tma_load3(dst + size_t(f) * EFS * 8, &maps[MAP_EPI + ctl.u0Phys[f] * 5 + f], w.k0 - 1, w.j0, eP,
+                          &epiFull[se]);
+              if (s > 0)
+                for (int f = 0; f < 5; ++f)
+                  tma_load3(dst + size_t(5 + f) * EFS * 8, &maps[MAP_ACC + f], w.k0 - 1, w.j0, eP, &epiFull[se]);
+              ++eq;
+              if (++eP > w.i1) {
+                eIt += gridDim.x;
+                if (eIt < nItems) eP = items[eIt].i0;
+              }
+              progressed = true;
+            }
+          }
+          if (progressed) {
+            idle = 0;
+          } else if (++idle > WAIT_LIMIT) {
+            fail();
+            break;
+          }
+        }
+        // Every copy issued must have landed before the CTA exits: wait for the last phase of each slot.
+        const volatile int never = 0;
+        for (uint32_t sl = 0; sl < NC; ++sl)
+          if (cq > sl) {
+            const uint32_t last = cq - 1 - ((cq - 1 - sl) % NC);
+            if (!mbar_wait(&consFull[sl], (last / NC) & 1, &never)) atomicExch(&G.ctl->timeout, 1);
+          }
+        for (uint32_t se = 0; se < NE; ++se)
+          if (eq > se) {
+            const uint32_t last = eq - 1 - ((eq - 1 - se) % NE);
+            if (!mbar_wait(&epiFull[se], (last / NE) & 1, &never)) atomicExch(&G.ctl->timeout, 1);
+          }
+      }
+    } else {
+      // ------------------------------------------------------------------ staging (warps 1-3)
+      const int st = tid - 32;
+      const double* __restrict__ fpre = G.fpre;
+      uint32_t q = 0;  // staged-plane sequence number, continues across items
+      bool ok = true;
+      for (int it = blockIdx.x; it < nItems && ok; it += gridDim.x) {
+        const StageItem w = items[it];
+        for (int p = w.i0 - 1; p <= w.i1 + 1; ++p, ++q) {
+          const uint32_t sl = q % NC, ps = q % NP;
+          if (q >= NP) ok = mbar_wait(&primEmpty[ps], ((q / NP) - 1) & 1, abortFlag);
+          ok = ok && mbar_wait(&consFull[sl], (q / NC) & 1, abortFlag);
+          if (!ok) {
+            fail();
+            break;
+          }
+          const double* cs = reinterpret_cast<const double*>(sm + OFF_CONS + sl * CONS_SLOT);
+          const uint8_t* ts = reinterpret_cast<const uint8_t*>(cs) + TYPE_OFF;
+          double* pv = reinterpret_cast<double*>(sm + OFF_PRIM + ps * PRIM_SLOT);
+#pragma unroll 1
+          for (int idx = st; idx < HP; idx += NSTAGE) {
+            const int hj = idx / HK, hk = idx - hj * HK;
+            double rho = cs[0 * FS + idx], rE = cs[4 * FS + idx];
+            if (ts[hj * TYW + hk] & FILTER_BIT) {
+              const long long n = (long long)p * G.sI + (long long)(w.j0 - 1 + hj) * G.sJ + (w.k0 - 1 + hk);
+              const int f = __ldg(G.fidx + n);
+              rho = fpre[2 * f];
+              rE = fpre[2 * f + 1];
+            }
+            // Nodes past the mesh read TMA zero fill: finite values that are never used.
+            const Prim pr = prims_of(C, rho, cs[1 * FS + idx], cs[2 * FS + idx], cs[3 * FS + idx], rE);
+            pv[0 * FS + idx] = pr.u;
+            pv[1 * FS + idx] = pr.v;
+            pv[2 * FS + idx] = pr.w;
+            pv[3 * FS + idx] = pr.p;
+            pv[4 * FS + idx] = pr.T;
+            pv[5 * FS + idx] = pr.mu;
+            pv[6 * FS + idx] = pr.ka;
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&primFull[ps]);
+        }
+      }
+    }
+  } else {
+    reg_alloc<REG_HIGH>();
+    // -------------------------------------------------------------------- columns (warpgroups 1-2)
+    const int ct = tid - 128, tx = ct % TK, ty = ct / TK;
+    const int cidx = (ty + 1) * HK + (tx + 1);   // this column's node in a staged plane
+    const int eidx = ty * HK + tx + 1;           // ... in an epilogue tile
+    const int tcix = (ty + 1) * TYW + (tx + 1);  // ... in a staged type box
+    const double dtUsed = ctl.dtUsed;
+    const double inc = (s == 2) ? dtUsed : dtUsed / 2;
+    const double dtFactor = dtUsed / 6;
+    double* const out0 = ctl.O[s][0];
+    double* const out1 = ctl.O[s][1];
+    double* const out2 = ctl.O[s][2];
+    double* const out3 = ctl.O[s][3];
+    double* const out4 = ctl.O[s][4];
+    double* const accb = G.acc[0];  // accumulator fields are contiguous, G.N doubles apart
+    const long long NdF = G.N;
+    const unsigned char* const consBase = sm + OFF_CONS;
+    const unsigned char* const primBase = sm + OFF_PRIM;
+    uint32_t q = 0, e = 0;  // staged-plane and computed-plane sequence numbers
+    bool ok = true;
+    for (int it = blockIdx.x; it < nItems && ok; it += gridDim.x) {
+      const StageItem w = items[it];
+      const int j = w.j0 + ty, k = w.k0 + tx;
+      const bool inTile = (j <= G.NJ - 2) && (k <= G.NK - 2);
+      const int L = w.i1 - w.i0 + 1;
+      long long nR = (long long)w.i0 * G.sI + (long long)j * G.sJ + k;  // node of the next computed plane
+      XNode gm1{}, gm2{};
+      double fprev[5] = {0, 0, 0, 0, 0};
+      XOwn ownPrev{};
+      // Iteration a forms the x quantities of plane i0-1+a and, from a = 2 on, computes the RHS of
+      // plane i0-2+a.
+      for (int a = 0; a <= L + 1; ++a) {
+        const uint32_t qx = q + a;
+        const int pX = qx % NP, cX = qx % NC;
+        ok = mbar_wait(&primFull[pX], (qx / NP) & 1, abortFlag) && mbar_wait(&consFull[cX], (qx / NC) & 1, abortFlag);
+        if (!ok) {
+          fail();
+          break;
+        }
+        constexpr int oN = HK, oU = 1;
+        XNode gcur;
+        XOwn ownCur;
+        double fcur[5] = {0, 0, 0, 0, 0};
+        {
+          const double* cs = reinterpret_cast<const double*>(consBase + cX * CONS_SLOT);
+          const double* ps = reinterpret_cast<const double*>(primBase + pX * PRIM_SLOT);
+          ownCur = XOwn{ps[5 * FS + cidx], ps[0 * FS + cidx], ps[1 * FS + cidx],
+                        ps[2 * FS + cidx], ps[4 * FS + cidx], ps[6 * FS + cidx]};
+          gcur = x_node(C, cs[1 * FS + cidx], cs[2 * FS + cidx], cs[3 * FS + cidx], cs[4 * FS + cidx], ownCur.u,
+                        ownCur.v, ownCur.w, ps[3 * FS + cidx], ownCur.mu,
+                        ps[1 * FS + cidx + oN] - ps[1 * FS + cidx - oN], ps[0 * FS + cidx + oN] - ps[0 * FS + cidx - oN],
+                        ps[2 * FS + cidx + oU] - ps[2 * FS + cidx - oU], ps[0 * FS + cidx + oU] - ps[0 * FS + cidx - oU]);
+          if (a >= 1) x_face(C, ownPrev, ownCur, fcur);
+        }
+        if (a == 0) {  // plane i0-1: its conserved values have no other reader
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&consEmpty[cX]);
+        }
+        if (a >= 2) {
+          const int pR = (qx - 1) % NP, pW = (qx - 2) % NP, cR = (qx - 1) % NC;
+          const uint32_t se = e % NE;
+          ok = mbar_wait(&epiFull[se], (e / NE) & 1, abortFlag);
+          if (!ok) {
+            fail();
+            break;
+          }
+          const double* cP = reinterpret_cast<const double*>(consBase + cR * CONS_SLOT);
+          const uint8_t tc = (reinterpret_cast<const uint8_t*>(cP) + TYPE_OFF)[tcix];
+          const bool valid = inTile && (tc & TYPE_MASK) == FLUID_INTERIOR;
+          double kk5[5];
+          yz_part<HK, FS>(C, cP, reinterpret_cast<const double*>(primBase + pW * PRIM_SLOT),
+                          reinterpret_cast<const double*>(primBase + pR * PRIM_SLOT),
+                          reinterpret_cast<const double*>(primBase + pX * PRIM_SLOT), cidx, ownPrev, kk5);
+#pragma unroll
+          for (int f = 0; f < 5; ++f) kk5[f] += (gcur.g[f] - gm2.g[f]) + (fcur[f] - fprev[f]);
+          const double* ep = reinterpret_cast<const double*>(sm + OFF_EPI + se * EPI_SLOT);
+          double u0[5], res[5];
+#pragma unroll
+          for (int f = 0; f < 5; ++f) u0[f] = ep[f * EFS + eidx];
+          if (s == 0) {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) res[f] = u0[f] + inc * kk5[f];
+            if (valid) {
+#pragma unroll
+              for (int f = 0; f < 5; ++f) accb[f * NdF + nR] = kk5[f];
+            }
+          } else if (s < 3) {
+            double an[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+              an[f] = ep[(5 + f) * EFS + eidx] + 2 * kk5[f];
+              res[f] = u0[f] + inc * kk5[f];
+            }
+            if (valid) {
+#pragma unroll
+              for (int f = 0; f < 5; ++f) accb[f * NdF + nR] = an[f];
+            }
+          } else {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) res[f] = u0[f] + dtFactor * (ep[(5 + f) * EFS + eidx] + kk5[f]);
+            const bool filtered = (tc & FILTER_BIT) != 0;  // rho, rho_E change again in the near-body filter
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+              const double d = u0[f] - res[f];
+              nsum[f] += (valid && !(filtered && (f == 0 || f == 4))) ? d * d : 0.0;
+            }
+            bad |= valid && !(isfinite(res[0]) && isfinite(res[1]) && isfinite(res[2]) && isfinite(res[3]) &&
+                              isfinite(res[4]));
+            if (valid && !filtered) {
+              const Prim pr = prims_of(C, res[0], res[1], res[2], res[3], res[4]);
+              dta.add(C, res[0], pr.u, pr.v, pr.w, pr.p, pr.mu);
+            }
+          }
+          if (valid) {
+            out0[nR] = res[0];
+            out1[nR] = res[1];
+            out2[nR] = res[2];
+            out3[nR] = res[3];
+            out4[nR] = res[4];
+          }
+          __syncwarp();
+          if (lane == 0) {
+            mbar_arrive(&epiEmpty[se]);
+            mbar_arrive(&consEmpty[cR]);   // plane i0-3+a: its last reader was this RHS
+            mbar_arrive(&primEmpty[pW]);   // plane i0-4+a: read for the last time as the west plane
+          }
+          ++e;
+          nR += G.sI;
+          if (a == L + 1) {  // the item's last two planes' primitives, its last plane's conserved values
+            if (lane == 0) {
+              mbar_arrive(&consEmpty[cX]);
+              mbar_arrive(&primEmpty[pR]);
+              mbar_arrive(&primEmpty[pX]);
+            }
+          }
+        }
+        gm2 = gm1;
+        gm1 = gcur;
+#pragma unroll
+        for (int f = 0; f < 5; ++f) fprev[f] = fcur[f];
+        ownPrev = ownCur;
+      }
+      q += L + 2;
+    }
+  }
+  __syncwarp();
+  if (s == 3) {
+    flush_dt(G.ctl, dta, red);
+    flush_norms(G.normPart + 5 * blockIdx.x, nsum, red);
+    if (bad) atomicOr(&G.ctl->nonFinite, 1);
+  }
+}
+
+size_t stage_smem_bytes() { return ws::SMEM; }
+int stage_configure() {
+  return int(cudaFuncSetAttribute(k_stage_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ws::SMEM)));
+}
+int stage_tile_j() { return ws::TJ; }
+int stage_tile_k() { return ws::TK; }
+int stage_threads() { return ws::NTHREADS; }
+int stage_occupancy() {
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stage_ws, ws::NTHREADS, ws::SMEM);
+  return nb;
+}
+int stage_num_maps() { return ws::NMAPS; }
+// Registers per thread the kernel is launched with (the setmaxnreg split above assumes ws::REG_LAUNCH).
+int stage_launch_registers() {
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, k_stage_ws) != cudaSuccess) return -1;
+  return fa.numRegs;
+}
+bool stage_register_split_ok() {
+  const int r = stage_launch_registers();
+  return r > 0 && 128 * ws::REG_LOW + ws::NCOL * ws::REG_HIGH <= ws::NTHREADS * r;
+}
+void launch_stage(const Grid& hg, const LaunchPlan& L, int s, void* stream) {
+  k_stage_ws<<<L.stageBlocks, ws::NTHREADS, ws::SMEM, static_cast<cudaStream_t>(stream)>>>(hg, L.items, L.nItems, s);
+}
+
+}  // namespace nsf

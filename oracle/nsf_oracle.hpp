@@ -17,6 +17,7 @@
 #include <map>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "fullpiv_lu.h"
@@ -124,6 +125,12 @@ class Solver {
   bool nonFinite = false;
   // Optional frozen dt sequence (used by gradient checks, where dt must not depend on the state).
   std::vector<double> frozenDt;
+  // Optional: solve the image-point Vandermonde systems in extended precision (long double) instead of the
+  // reference's double-precision complete-pivoting LU. The raw-coordinate matrices are ill-conditioned on
+  // fine grids, so the reference's double solve amplifies last-bit differences of its inputs (up to ~1e-9
+  // relative after two steps on a 1/126 grid); this mode gives the reference's algorithm with that rounding
+  // amplification removed, as the comparison point for implementations that round differently.
+  bool exactImageSolve = false;
   size_t stepCounter = 0;
 
   explicit Solver(const Params& p, const Case& c)
@@ -886,10 +893,17 @@ class Solver {
             VN[r][7] = px[r] * py[r] * nv.z + px[r] * pz[r] * nv.y + py[r] * pz[r] * nv.x;
             ++cnt;
           }
+        const double X = g.ip.x, Y = g.ip.y, Z = g.ip.z;
+        if constexpr (std::is_same<T, double>::value) {
+          if (exactImageSolve) {
+            for (int f = 0; f < 5; ++f) ipv[f] = solveExtended(f == 0 || f == 4, px, py, pz, gf, normals, val[f], X, Y, Z);
+            goto ghost_value;
+          }
+        }
+        {
         oracle_lu::FullPivLU<8> luD, luN;
         luD.compute(VD);
         luN.compute(VN);
-        const double X = g.ip.x, Y = g.ip.y, Z = g.ip.z;
         for (int f = 0; f < 5; ++f) {
           T rhs[8], co[8];
           for (int c = 0; c < 8; ++c) rhs[c] = val[f][c];
@@ -900,13 +914,60 @@ class Solver {
           ipv[f] = co[0] + co[1] * X + co[2] * Y + co[3] * Z + co[4] * X * Y + co[5] * X * Z + co[6] * Y * Z +
                    co[7] * X * Y * Z;
         }
+        }
       }
+    ghost_value:
       // getGhostNodeBCVariables, Boundary.cpp:777-785
       T gc[5] = {ipv[0], -ipv[1], -ipv[2], -ipv[3], ipv[4]}, gp[5], m, kap;
       derivePrimitive(gc, gp);
       deriveTransport(gp, m, kap);
       setAll(id(g.i, g.j, g.k), gc, gp, m, kap);
     }
+  }
+
+  // Extended-precision counterpart of populateVandermonde* + trilinearInterpolation (Boundary.cpp:788-834):
+  // the matrix entries (products of the reference's double positions and normals), the solve (Gaussian
+  // elimination with partial pivoting) and the polynomial are all evaluated in long double and rounded
+  // once to double. Rounding the raw-coordinate entries to double already perturbs the interpolant by
+  // about cond(V) * 1e-16, so the entries must be formed in extended precision as well.
+  static double solveExtended(bool neumann, const double (&px)[8], const double (&py)[8], const double (&pz)[8],
+                              const bool (&gf)[8], const std::vector<V3>& normals, const double (&v)[8], double X,
+                              double Y, double Z) {
+    long double A[8][9];
+    size_t cnt = 0;
+    for (int r = 0; r < 8; ++r) {
+      const long double x = px[r], y = py[r], z = pz[r];
+      if (neumann && gf[r]) {
+        const long double nx = normals[cnt].x, ny = normals[cnt].y, nz = normals[cnt].z;
+        ++cnt;
+        const long double row[8] = {0, nx, ny, nz, x * ny + y * nx, x * nz + z * nx, y * nz + z * ny,
+                                    x * y * nz + x * z * ny + y * z * nx};
+        for (int c = 0; c < 8; ++c) A[r][c] = row[c];
+      } else {
+        const long double row[8] = {1, x, y, z, x * y, x * z, y * z, x * y * z};
+        for (int c = 0; c < 8; ++c) A[r][c] = row[c];
+      }
+      A[r][8] = v[r];
+    }
+    for (int c = 0; c < 8; ++c) {
+      int p = c;
+      for (int r = c + 1; r < 8; ++r)
+        if (std::fabs(A[r][c]) > std::fabs(A[p][c])) p = r;
+      for (int q = 0; q < 9; ++q) std::swap(A[c][q], A[p][q]);
+      for (int r = c + 1; r < 8; ++r) {
+        const long double m = A[r][c] / A[c][c];
+        for (int q = c; q < 9; ++q) A[r][q] -= m * A[c][q];
+      }
+    }
+    long double co[8];
+    for (int r = 7; r >= 0; --r) {
+      long double s = A[r][8];
+      for (int q = r + 1; q < 8; ++q) s -= A[r][q] * co[q];
+      co[r] = s / A[r][r];
+    }
+    const long double x = X, y = Y, z = Z;
+    return double(co[0] + co[1] * x + co[2] * y + co[3] * z + co[4] * x * y + co[5] * x * z + co[6] * y * z +
+                  co[7] * x * y * z);
   }
 
   // Mesh::applyAllBoundaryConditions, Mesh.cpp:155-167.

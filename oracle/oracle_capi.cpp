@@ -132,6 +132,8 @@ int nsfo_initialize(void* hp, char* err, int errlen) {
   }
 }
 
+void nsfo_set_exact_image_solve(void* hp, int on) { static_cast<Handle*>(hp)->s->exactImageSolve = on != 0; }
+
 void nsfo_set_frozen_dt(void* hp, const double* dts, uint64_t n) {
   auto* h = static_cast<Handle*>(hp);
   h->s->frozenDt.assign(dts, dts + n);

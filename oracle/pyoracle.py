@@ -33,6 +33,7 @@ def lib():
         L.nsfo_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
         L.nsfo_initialize.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         L.nsfo_set_frozen_dt.argtypes = [vp, ctypes.POINTER(dbl), u64]
+        L.nsfo_set_exact_image_solve.argtypes = [vp, ctypes.c_int]
         L.nsfo_march.restype = dbl
         L.nsfo_march.argtypes = [vp, u64]
         for name, rt in [("nsfo_num_nodes", u64), ("nsfo_time", dbl), ("nsfo_time_level", u64), ("nsfo_dt", dbl),
@@ -63,12 +64,15 @@ def _dp(a):
 class Oracle:
     """The CPU restatement of the reference solver, driven like Solver/Simulation."""
 
-    def __init__(self, cfg_text):
+    def __init__(self, cfg_text, exact_image_solve=False):
+        """exact_image_solve: solve the image-point systems in extended precision (see nsf_oracle.hpp)."""
         L = lib()
         err = ctypes.create_string_buffer(512)
         self.h = L.nsfo_create(cfg_text.encode(), 1, err, 512)
         if not self.h:
             raise RuntimeError("oracle config error: " + err.value.decode())
+        if exact_image_solve:
+            L.nsfo_set_exact_image_solve(self.h, 1)
         if L.nsfo_initialize(self.h, err, 512) != 0:
             raise RuntimeError("oracle initialize error: " + err.value.decode())
         self.N = int(L.nsfo_num_nodes(self.h))

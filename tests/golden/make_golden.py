@@ -11,7 +11,8 @@ and filter-node lists, the initial dt, the per-step history (t, dt used, dt next
 all twelve fields (rho, rho_u, rho_v, rho_w, rho_E, u, v, w, p, T, mu, kappa) at the listed steps and
 at the last step run (an end_time case stops where Simulation::run stops, so later listed steps are
 replaced by that final step).
-For the 48^3 sphere workload it stores a fixed node subsample of the fields instead of whole arrays.
+For the 48^3 sphere workload and the 16-sphere 256x128x128 workload it stores a fixed node subsample of the
+fields instead of whole arrays (the 16-sphere run stops after its last listed step).
 """
 import os
 import sys
@@ -31,6 +32,7 @@ CASES = {
     "cylinder_sym": ("tests/golden/cases/cylinder_sym.cfg", [4, 60], None),
     "shipped_small": ("tests/golden/cases/shipped_small.cfg", [40], None),
     "sphere48": ("3d-ns-fsi_b200/cases/sphere48.cfg", [100], 13),
+    "spheres16": ("3d-ns-fsi_b200/cases/spheres16.cfg", [2], 509),
 }
 
 

@@ -21,6 +21,7 @@ CASES = {
     "cylinder_sym": "tests/golden/cases/cylinder_sym.cfg",
     "shipped_small": "tests/golden/cases/shipped_small.cfg",
     "sphere48": "3d-ns-fsi_b200/cases/sphere48.cfg",
+    "spheres16": "3d-ns-fsi_b200/cases/spheres16.cfg",
 }
 
 
@@ -28,7 +29,7 @@ def load(name):
     return np.load(os.path.join(GOLD, name + ".npz"))
 
 
-@pytest.mark.parametrize("name", [n for n in CASES if n != "sphere48"])
+@pytest.mark.parametrize("name", [n for n in CASES if n not in ("sphere48", "spheres16")])
 def test_oracle_matches_reference_bitwise(name):
     g = load(name)
     o = po.Oracle(open(os.path.join(ROOT, CASES[name])).read())
@@ -70,3 +71,36 @@ def test_oracle_matches_reference_sphere48_100_steps():
     h = o.history()
     assert np.array_equal(h[:, 1], g["history"][:, 1])
     assert np.array_equal(h[:, 2:], g["history"][:, 3:])
+
+
+@pytest.mark.slow
+def test_oracle_matches_reference_spheres16_two_steps():
+    """The 16-sphere 256x128x128 workload (8139 ghost nodes): setup and two RK4 steps."""
+    g = load("spheres16")
+    o = po.Oracle(open(os.path.join(ROOT, CASES["spheres16"])).read())
+    assert np.array_equal(o.node_types(), g["types"])
+    bodies = o.bodies()
+    assert len(bodies) == 16
+    for b, (gh, fl, closure) in enumerate(bodies):
+        assert np.array_equal(gh, g["ghosts_%d" % b])
+        assert np.array_equal(fl, g["filter_%d" % b])
+    o.march(2)
+    assert o.t == float(g["t_2"])
+    assert np.array_equal(o.fields()[:, g["sample_idx"]], g["fields_2"])
+
+
+@pytest.mark.slow
+def test_reference_image_point_solve_conditioning_spheres16():
+    """Why the 16-sphere case is compared with an extended-precision oracle: the reference's double LU on
+    the raw-coordinate Vandermonde systems (spacing 1/126) carries rounding errors far above 1e-10, while on
+    the coarse sphere grid it stays below 1e-11. Both statements are measured here on the oracle, which
+    reproduces the reference bit for bit."""
+    from test_parity_gpu import field_errors
+    for name, steps, lo, hi in [("spheres16", 2, 1e-10, 1e-8), ("sphere48", 100, 0.0, 1e-10)]:
+        text = open(os.path.join(ROOT, CASES[name])).read()
+        a = po.Oracle(text)
+        b = po.Oracle(text, exact_image_solve=True)
+        a.march(steps)
+        b.march(steps)
+        d = field_errors(b.fields(), a.fields()).max()
+        assert lo < d < hi, (name, d)

@@ -18,6 +18,7 @@ CASES = {
     "cylinder_sym": "tests/golden/cases/cylinder_sym.cfg",
     "shipped_small": "tests/golden/cases/shipped_small.cfg",
     "sphere48": "3d-ns-fsi_b200/cases/sphere48.cfg",
+    "spheres16": "3d-ns-fsi_b200/cases/spheres16.cfg",
 }
 
 

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -174,6 +175,11 @@ nsf_status build_device(nsf_solver* s) {
   auto dev = [&](size_t n) { return dev_index(S, NKp, n); };
   Grid& G = s->hGrid;
   G = Grid{};
+  // stage-kernel tile shape: NSF_STAGE_TILE=16x16 or 32x8 (default)
+  const int tile = [] {
+    const char* e = std::getenv("NSF_STAGE_TILE");
+    return e && std::string(e) == "16x16" ? int(STAGE_TILE_16x16) : int(STAGE_TILE_32x8);
+  }();
   G.NI = int(S.NI);
   G.NJ = int(S.NJ);
   G.NK = int(S.NK);
@@ -197,8 +203,8 @@ nsf_status build_device(nsf_solver* s) {
     CK(cudaMemcpy2D(G.bufs[0][f], NKp * sizeof(double), cons.data() + f * N, S.NK * sizeof(double),
                     S.NK * sizeof(double), S.NI * S.NJ, cudaMemcpyHostToDevice));
 
-  // TMA descriptors: staged planes (box 34 x 10 x 1) and epilogue tiles (34 x 8 x 1) of every physical
-  // buffer field, and epilogue tiles of the accumulator.
+  // TMA descriptors: staged planes (box (TK + 2) x (TJ + 2) x 1) and epilogue tiles ((TK + 2) x TJ x 1) of every
+  // physical buffer field, and epilogue tiles of the accumulator.
   {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult qr;
@@ -212,12 +218,12 @@ nsf_status build_device(nsf_solver* s) {
     auto mk = [&](CUtensorMap* m, double* base, cuuint32_t rows) {
       cuuint64_t gdim[3] = {S.NK, S.NJ, S.NI};
       cuuint64_t gstr[2] = {NKp * sizeof(double), S.NJ * NKp * sizeof(double)};
-      cuuint32_t box[3] = {cuuint32_t(stage_tile_k() + 2), rows, 1};
+      cuuint32_t box[3] = {cuuint32_t(stage_tile_k(tile) + 2), rows, 1};
       cuuint32_t es[3] = {1, 1, 1};
       return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     };
-    const cuuint32_t haloRows = cuuint32_t(stage_tile_j() + 2), tileRows = cuuint32_t(stage_tile_j());
+    const cuuint32_t haloRows = cuuint32_t(stage_tile_j(tile) + 2), tileRows = cuuint32_t(stage_tile_j(tile));
     bool okMaps = true;
     for (int b = 0; b < 3; ++b)
       for (int f = 0; f < 5; ++f) {
@@ -254,11 +260,11 @@ nsf_status build_device(nsf_solver* s) {
   uint8_t* dType;
   if ((st = upload(s, &dType, typeDev)) != NSF_OK) return st;
   G.type = dType;
-  {  // node-type boxes (48 x 10 x 1 bytes) for the stage kernel, then all descriptors to the device
+  {  // node-type boxes (row width x (TJ + 2) x 1 bytes) for the stage kernel, then all descriptors to the device
     auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(s->encodeFn);
     cuuint64_t gdim[3] = {S.NK, S.NJ, S.NI};
     cuuint64_t gstr[2] = {NKp, S.NJ * NKp};
-    cuuint32_t box[3] = {48, cuuint32_t(stage_tile_j() + 2), 1};
+    cuuint32_t box[3] = {cuuint32_t(stage_type_box_width(tile)), cuuint32_t(stage_tile_j(tile) + 2), 1};
     cuuint32_t es[3] = {1, 1, 1};
     if (encode(&s->hostMaps[stage_num_maps() - 1], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dType, gdim, gstr, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -418,13 +424,14 @@ nsf_status build_device(nsf_solver* s) {
   LaunchPlan& L = s->plan;
   L = LaunchPlan{};
   L.nSM = s->nSM;
-  CK(cudaError_t(stage_configure()));
-  if (!stage_register_split_ok()) {
+  L.tile = tile;
+  CK(cudaError_t(stage_configure(tile)));
+  if (!stage_register_split_ok(tile)) {
     s->err = "stage kernel: its launch registers do not cover its setmaxnreg split";
     return NSF_ERR_CUDA;
   }
-  const int occ = std::max(1, stage_occupancy());
-  const int TJ = stage_tile_j(), TK = stage_tile_k();
+  const int occ = std::max(1, stage_occupancy(tile));
+  const int TJ = stage_tile_j(tile), TK = stage_tile_k(tile);
   const int nj = int((S.NJ - 2 + TJ - 1) / TJ), nk = int((S.NK - 2 + TK - 1) / TK);
   const int tiles = nj * nk, planes = int(S.NI - 2);
   const int slots = s->nSM * occ;

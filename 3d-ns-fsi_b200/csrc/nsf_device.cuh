@@ -108,6 +108,9 @@ struct Grid {
   double* hist;             // [MAX_HIST][7]
 };
 
+// Stage-kernel tile shapes (one column thread per (j, k) column, 256 columns per CTA).
+enum StageTile { STAGE_TILE_32x8 = 0, STAGE_TILE_16x16 = 1 };
+
 struct StageItem {
   int j0, k0, i0, i1;  // tile origin (first computed j, k) and inclusive i range
 };
@@ -115,6 +118,7 @@ struct StageItem {
 // Launch geometry of one step, fixed at initialisation.
 struct LaunchPlan {
   int nSM;
+  int tile;  // StageTile
   int stageBlocks;
   int nItems;
   StageItem* items;  // device
@@ -126,17 +130,19 @@ struct LaunchPlan {
 };
 
 // Host entry points of nsf_kernels.cu.
-size_t stage_smem_bytes();
-int stage_configure();
-int stage_tile_j();
-int stage_tile_k();
-int stage_threads();
-int stage_occupancy();
+// Stage-kernel variant queries (v: StageTile).
+size_t stage_smem_bytes(int v);
+int stage_configure(int v);
+int stage_tile_j(int v);
+int stage_tile_k(int v);
+int stage_type_box_width(int v);
+int stage_threads(int v);
+int stage_occupancy(int v);
 int stage_num_maps();
 // Registers per thread the stage kernel is launched with; stage_register_split_ok() checks that the
 // kernel's setmaxnreg split fits in them (a split above the launch total would never be granted).
-int stage_launch_registers();
-bool stage_register_split_ok();
+int stage_launch_registers(int v);
+bool stage_register_split_ok(int v);
 void launch_stage(const Grid& hg, const LaunchPlan& L, int s, void* stream);
 // dg: the grid in device memory (read by the small kernels); hg: the same grid on the host (passed by
 // value to the stage kernel, whose coefficients then come from the constant bank).

@@ -17,7 +17,7 @@
 //     see x_node / x_face in nsf_physics.cuh) and carries them in registers along the column; the
 //     RHS of the previous plane is then G/F differences plus the y/z terms read from the staged planes,
 //     and the RK4 combine is written with coalesced 256-byte row stores.
-// Warpgroup 0 runs with 72 registers per thread and the column warpgroups with 216 (setmaxnreg), so
+// Warpgroup 0 runs with 88 registers per thread and the column warpgroups with 208 (setmaxnreg), so
 // the register-hungry RHS does not spill while the CTA still has twelve warps.
 //
 // Ring slots have a "full" and an "empty" mbarrier. Every wait is bounded: a wait that gives up sets
@@ -37,40 +37,49 @@
 
 namespace nsf {
 namespace ws {
-constexpr int TK = 32, TJ = 8, NCOL = TK * TJ;   // column threads (warpgroups 1-2)
-constexpr int NTHREADS = 128 + NCOL;
 constexpr int NSTAGE = 96;                        // staging threads (warps 1-3)
-constexpr int HK = TK + 2, HJ = TJ + 2, HP = HK * HJ;
-constexpr int FS = 352;                           // doubles per staged field (2816 B, a multiple of 128 B)
-constexpr int EFS = HK * TJ;                      // doubles per epilogue field (2176 B = 17 x 128 B)
 constexpr int NC = 5, NP = 4, NE = 3;             // conserved / primitive / epilogue ring depths
-constexpr int TYW = 48;                           // row width of the staged node-type box (bytes, >= HK)
-constexpr uint32_t CONS_BOX_BYTES = HK * HJ * 8;
-constexpr uint32_t TYPE_BOX_BYTES = TYW * HJ;
-constexpr uint32_t EPI_BOX_BYTES = HK * TJ * 8;
-constexpr size_t TYPE_OFF = size_t(5) * FS * 8;  // node types follow the five fields in a staged slot
-constexpr size_t CONS_SLOT = TYPE_OFF + 512;
-constexpr size_t PRIM_SLOT = size_t(7) * FS * 8;
-constexpr size_t EPI_SLOT = size_t(10) * EFS * 8;
-constexpr size_t OFF_CONS = 0;
-constexpr size_t OFF_PRIM = OFF_CONS + NC * CONS_SLOT;
-constexpr size_t OFF_EPI = OFF_PRIM + NP * PRIM_SLOT;
-constexpr size_t OFF_BAR = OFF_EPI + NE * EPI_SLOT;
-constexpr size_t OFF_FLAG = OFF_BAR + 2 * (NC + NP + NE) * 8;
-constexpr size_t OFF_RED = (OFF_FLAG + 16 + 127) / 128 * 128;
-constexpr size_t OFF_CTL = OFF_RED + 5 * 32 * 8;
-constexpr size_t SMEM = OFF_CTL + ((sizeof(StepCtl) + 127) / 128) * 128;
-static_assert(OFF_PRIM % 128 == 0 && OFF_EPI % 128 == 0 && CONS_SLOT % 128 == 0 && TYPE_OFF % 128 == 0,
-              "TMA destinations need 128 B alignment");
-static_assert(TYPE_BOX_BYTES <= 512, "type box fits its slot region");
-static_assert(SMEM <= 227 * 1024, "shared memory budget");
-static_assert(NSTAGE * 4 >= HP, "four staging passes cover a plane");
 constexpr int MAP_CONS = 0, MAP_EPI = 15, MAP_ACC = 30, MAP_TYPE = 35, NMAPS = 36;
 constexpr long long WAIT_LIMIT = 1ll << 22;  // polls before a wait is declared failed
 // Register split (setmaxnreg): the launch gives every thread 168 registers (384 x 168 = 64,512); the
-// split must not exceed that total: 128 x 72 + 256 x 216 = 64,512.
-constexpr int REG_LAUNCH = 168, REG_LOW = 72, REG_HIGH = 216;
-static_assert(128 * REG_LOW + NCOL * REG_HIGH <= NTHREADS * REG_LAUNCH, "register split exceeds the launch total");
+// split must not exceed that total: 128 x 88 + 256 x 208 = 64,512.
+constexpr int REG_LAUNCH = 168, REG_LOW = 88, REG_HIGH = 208;
+
+constexpr int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// Tile geometry of one kernel variant: TK x TJ columns (one column thread each, 256 in total).
+template <int TK_, int TJ_>
+struct Tile {
+  static constexpr int TK = TK_, TJ = TJ_, NCOL = TK * TJ;
+  static constexpr int NTHREADS = 128 + NCOL;
+  static constexpr int HK = TK + 2, HJ = TJ + 2, HP = HK * HJ;
+  static constexpr int FS = round_up(HP, 16);     // doubles per staged field (a multiple of 128 B)
+  static constexpr int EFS = HK * TJ;             // doubles per epilogue field
+  static constexpr int TYW = round_up(HK, 16);    // row width of the staged node-type box (bytes)
+  static constexpr uint32_t CONS_BOX_BYTES = HK * HJ * 8;
+  static constexpr uint32_t TYPE_BOX_BYTES = TYW * HJ;
+  static constexpr uint32_t EPI_BOX_BYTES = HK * TJ * 8;
+  static constexpr size_t TYPE_OFF = size_t(5) * FS * 8;  // node types follow the five fields in a slot
+  static constexpr size_t CONS_SLOT = TYPE_OFF + size_t(round_up(TYW * HJ, 128));
+  static constexpr size_t PRIM_SLOT = size_t(7) * FS * 8;
+  static constexpr size_t EPI_SLOT = size_t(10) * EFS * 8;
+  static constexpr size_t OFF_CONS = 0;
+  static constexpr size_t OFF_PRIM = OFF_CONS + NC * CONS_SLOT;
+  static constexpr size_t OFF_EPI = OFF_PRIM + NP * PRIM_SLOT;
+  static constexpr size_t OFF_BAR = OFF_EPI + NE * EPI_SLOT;
+  static constexpr size_t OFF_FLAG = OFF_BAR + 2 * (NC + NP + NE) * 8;
+  static constexpr size_t OFF_RED = (OFF_FLAG + 16 + 127) / 128 * 128;
+  static constexpr size_t OFF_CTL = OFF_RED + 5 * 32 * 8;
+  static constexpr size_t SMEM = OFF_CTL + ((sizeof(StepCtl) + 127) / 128) * 128;
+  static_assert(NCOL == 256, "two column warpgroups");
+  static_assert(TK % 16 == 0, "box x coordinate k0 - 1 = TK * t must be 16-byte aligned for TMA");
+  static_assert((EFS * 8) % 128 == 0 && (FS * 8) % 128 == 0, "TMA destinations need 128 B alignment");
+  static_assert(OFF_PRIM % 128 == 0 && OFF_EPI % 128 == 0 && CONS_SLOT % 128 == 0 && TYPE_OFF % 128 == 0,
+                "TMA destinations need 128 B alignment");
+  static_assert(SMEM <= 227 * 1024, "shared memory budget");
+  static_assert(NSTAGE * 4 >= HP, "four staging passes cover a plane");
+  static_assert(128 * REG_LOW + NCOL * REG_HIGH <= NTHREADS * REG_LAUNCH, "register split exceeds the launch total");
+};
 }  // namespace ws
 
 namespace {
@@ -120,11 +129,36 @@ __device__ __forceinline__ void reg_alloc() {
   asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(N));
 }
 
+// dt-limit terms of a node of the new state (getInviscidTimeStepLimit / getViscousTimeStepLimit,
+// Solver.cpp:91-126) with one reciprocal of 1 + rho for all the divisions by it. The terms only enter
+// maxima, so their last-bit rounding moves dt by at most an ulp or two.
+__device__ __forceinline__ void dt_terms(const Consts& C, const double (&u)[5], DtAcc& a) {
+  const double r1 = 1.0 / (u[0] + 1.0);
+  const double vx = u[1] * r1, vy = u[2] * r1, vz = u[3] * r1;
+  const double p = C.gm1 * (u[4] - (u[0] + 1.0) * 0.5 * (vx * vx + vy * vy + vz * vz));
+  const double T = (C.gamma * p - u[0]) * r1;
+  const double x = 1.0 + T;
+  const double c = sqrt((1.0 + C.gamma * p) * r1);
+  a.sx = fmax(a.sx, c + fabs(vx));
+  a.sy = fmax(a.sy, c + fabs(vy));
+  a.sz = fmax(a.sz, c + fabs(vz));
+  a.nu = fmax(a.nu, x * sqrt(x) * C.sc1 * r1 / (C.re * (T + C.sc1)) * C.vmod);
+}
+
 }  // namespace
 
-__global__ void __launch_bounds__(ws::NTHREADS, 1)
+template <int TK_, int TJ_>
+__global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
     k_stage_ws(const __grid_constant__ Grid G, const StageItem* __restrict__ items, int nItems, int s) {
   using namespace ws;
+  using TL = Tile<TK_, TJ_>;
+  constexpr int TK = TL::TK, NCOL = TL::NCOL, HK = TL::HK, HP = TL::HP, FS = TL::FS, EFS = TL::EFS,
+                TYW = TL::TYW;
+  constexpr uint32_t CONS_BOX_BYTES = TL::CONS_BOX_BYTES, TYPE_BOX_BYTES = TL::TYPE_BOX_BYTES,
+                     EPI_BOX_BYTES = TL::EPI_BOX_BYTES;
+  constexpr size_t TYPE_OFF = TL::TYPE_OFF, CONS_SLOT = TL::CONS_SLOT, PRIM_SLOT = TL::PRIM_SLOT,
+                   EPI_SLOT = TL::EPI_SLOT, OFF_CONS = TL::OFF_CONS, OFF_PRIM = TL::OFF_PRIM, OFF_EPI = TL::OFF_EPI,
+                   OFF_BAR = TL::OFF_BAR, OFF_FLAG = TL::OFF_FLAG, OFF_RED = TL::OFF_RED, OFF_CTL = TL::OFF_CTL;
   extern __shared__ __align__(1024) unsigned char sm[];
   uint64_t* consFull = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
   uint64_t* consEmpty = consFull + NC;
@@ -255,25 +289,42 @@ __global__ void __launch_bounds__(ws::NTHREADS, 1)
           const double* cs = reinterpret_cast<const double*>(sm + OFF_CONS + sl * CONS_SLOT);
           const uint8_t* ts = reinterpret_cast<const uint8_t*>(cs) + TYPE_OFF;
           double* pv = reinterpret_cast<double*>(sm + OFF_PRIM + ps * PRIM_SLOT);
+          // Two nodes per pass (idx and idx + NSTAGE) so that their long dependency chains (reciprocal,
+          // square root, division) overlap. Nodes past the mesh read TMA zero fill: finite values that
+          // are never used. Slots past the plane (idx >= HP) compute a dummy node and store nothing.
 #pragma unroll 1
-          for (int idx = st; idx < HP; idx += NSTAGE) {
-            const int hj = idx / HK, hk = idx - hj * HK;
-            double rho = cs[0 * FS + idx], rE = cs[4 * FS + idx];
-            if (ts[hj * TYW + hk] & FILTER_BIT) {
-              const long long n = (long long)p * G.sI + (long long)(w.j0 - 1 + hj) * G.sJ + (w.k0 - 1 + hk);
-              const int f = __ldg(G.fidx + n);
-              rho = fpre[2 * f];
-              rE = fpre[2 * f + 1];
+          for (int idx = st; idx < HP; idx += 2 * NSTAGE) {
+            const int idy = idx + NSTAGE, idyc = idy < HP ? idy : idx;
+            double rho[2] = {cs[0 * FS + idx], cs[0 * FS + idyc]}, rE[2] = {cs[4 * FS + idx], cs[4 * FS + idyc]};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int id = h ? idyc : idx;
+              const int hj = id / HK, hk = id - hj * HK;
+              if (ts[hj * TYW + hk] & FILTER_BIT) {
+                const long long n = (long long)p * G.sI + (long long)(w.j0 - 1 + hj) * G.sJ + (w.k0 - 1 + hk);
+                const int f = __ldg(G.fidx + n);
+                rho[h] = fpre[2 * f];
+                rE[h] = fpre[2 * f + 1];
+              }
             }
-            // Nodes past the mesh read TMA zero fill: finite values that are never used.
-            const Prim pr = prims_of(C, rho, cs[1 * FS + idx], cs[2 * FS + idx], cs[3 * FS + idx], rE);
-            pv[0 * FS + idx] = pr.u;
-            pv[1 * FS + idx] = pr.v;
-            pv[2 * FS + idx] = pr.w;
-            pv[3 * FS + idx] = pr.p;
-            pv[4 * FS + idx] = pr.T;
-            pv[5 * FS + idx] = pr.mu;
-            pv[6 * FS + idx] = pr.ka;
+            const Prim a0 = prims_of(C, rho[0], cs[1 * FS + idx], cs[2 * FS + idx], cs[3 * FS + idx], rE[0]);
+            const Prim a1 = prims_of(C, rho[1], cs[1 * FS + idyc], cs[2 * FS + idyc], cs[3 * FS + idyc], rE[1]);
+            pv[0 * FS + idx] = a0.u;
+            pv[1 * FS + idx] = a0.v;
+            pv[2 * FS + idx] = a0.w;
+            pv[3 * FS + idx] = a0.p;
+            pv[4 * FS + idx] = a0.T;
+            pv[5 * FS + idx] = a0.mu;
+            pv[6 * FS + idx] = a0.ka;
+            if (idy < HP) {
+              pv[0 * FS + idy] = a1.u;
+              pv[1 * FS + idy] = a1.v;
+              pv[2 * FS + idy] = a1.w;
+              pv[3 * FS + idy] = a1.p;
+              pv[4 * FS + idy] = a1.T;
+              pv[5 * FS + idy] = a1.mu;
+              pv[6 * FS + idy] = a1.ka;
+            }
           }
           __syncwarp();
           if (lane == 0) mbar_arrive(&primFull[ps]);
@@ -389,10 +440,7 @@ __global__ void __launch_bounds__(ws::NTHREADS, 1)
             }
             bad |= valid && !(isfinite(res[0]) && isfinite(res[1]) && isfinite(res[2]) && isfinite(res[3]) &&
                               isfinite(res[4]));
-            if (valid && !filtered) {
-              const Prim pr = prims_of(C, res[0], res[1], res[2], res[3], res[4]);
-              dta.add(C, res[0], pr.u, pr.v, pr.w, pr.p, pr.mu);
-            }
+            if (valid && !filtered) dt_terms(C, res, dta);
           }
           if (valid) {
             out0[nR] = res[0];
@@ -434,31 +482,56 @@ __global__ void __launch_bounds__(ws::NTHREADS, 1)
   }
 }
 
-size_t stage_smem_bytes() { return ws::SMEM; }
-int stage_configure() {
-  return int(cudaFuncSetAttribute(k_stage_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ws::SMEM)));
+// Kernel variants (tile shapes), selected per solver (see StageTile in nsf_device.cuh).
+namespace {
+struct VariantInfo {
+  int tk, tj, threads, typeBoxW;
+  size_t smem;
+  const void* fn;
+};
+template <int TK, int TJ>
+VariantInfo variant_info() {
+  using TL = ws::Tile<TK, TJ>;
+  return VariantInfo{TK, TJ, TL::NTHREADS, TL::TYW, TL::SMEM, reinterpret_cast<const void*>(&k_stage_ws<TK, TJ>)};
 }
-int stage_tile_j() { return ws::TJ; }
-int stage_tile_k() { return ws::TK; }
-int stage_threads() { return ws::NTHREADS; }
-int stage_occupancy() {
+VariantInfo info(int v) { return v == STAGE_TILE_16x16 ? variant_info<16, 16>() : variant_info<32, 8>(); }
+}  // namespace
+
+size_t stage_smem_bytes(int v) { return info(v).smem; }
+int stage_configure(int v) {
+  const VariantInfo vi = info(v);
+  return int(cudaFuncSetAttribute(vi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vi.smem)));
+}
+int stage_tile_j(int v) { return info(v).tj; }
+int stage_tile_k(int v) { return info(v).tk; }
+int stage_type_box_width(int v) { return info(v).typeBoxW; }
+int stage_threads(int v) { return info(v).threads; }
+int stage_occupancy(int v) {
+  const VariantInfo vi = info(v);
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stage_ws, ws::NTHREADS, ws::SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, vi.fn, vi.threads, vi.smem);
   return nb;
 }
 int stage_num_maps() { return ws::NMAPS; }
-// Registers per thread the kernel is launched with (the setmaxnreg split above assumes ws::REG_LAUNCH).
-int stage_launch_registers() {
+// Registers per thread the kernel is launched with (the setmaxnreg split assumes ws::REG_LAUNCH).
+int stage_launch_registers(int v) {
   cudaFuncAttributes fa{};
-  if (cudaFuncGetAttributes(&fa, k_stage_ws) != cudaSuccess) return -1;
+  if (cudaFuncGetAttributes(&fa, info(v).fn) != cudaSuccess) return -1;
   return fa.numRegs;
 }
-bool stage_register_split_ok() {
-  const int r = stage_launch_registers();
-  return r > 0 && 128 * ws::REG_LOW + ws::NCOL * ws::REG_HIGH <= ws::NTHREADS * r;
+bool stage_register_split_ok(int v) {
+  const int r = stage_launch_registers(v);
+  return r > 0 && 128 * ws::REG_LOW + 256 * ws::REG_HIGH <= info(v).threads * r;
 }
 void launch_stage(const Grid& hg, const LaunchPlan& L, int s, void* stream) {
-  k_stage_ws<<<L.stageBlocks, ws::NTHREADS, ws::SMEM, static_cast<cudaStream_t>(stream)>>>(hg, L.items, L.nItems, s);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (L.tile == STAGE_TILE_16x16) {
+    using TL = ws::Tile<16, 16>;
+    k_stage_ws<16, 16><<<L.stageBlocks, TL::NTHREADS, TL::SMEM, st>>>(hg, L.items, L.nItems, s);
+  } else {
+    using TL = ws::Tile<32, 8>;
+    k_stage_ws<32, 8><<<L.stageBlocks, TL::NTHREADS, TL::SMEM, st>>>(hg, L.items, L.nItems, s);
+  }
 }
 
 }  // namespace nsf

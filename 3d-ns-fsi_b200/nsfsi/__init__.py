@@ -10,7 +10,8 @@ import numpy as np
 
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ROOT = os.path.dirname(PKG)
-LIB_PATH = os.path.join(PKG, "lib", "libnsfsi.so")
+# NSFSI_LIB overrides the library path (e.g. to compare two builds of the native library).
+LIB_PATH = os.environ.get("NSFSI_LIB") or os.path.join(PKG, "lib", "libnsfsi.so")
 HEADER = os.path.join(ROOT, "include", "nsfsi.h")
 CASES = os.path.join(PKG, "cases")
 

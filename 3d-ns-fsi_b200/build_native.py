@@ -1,4 +1,5 @@
-"""Builds the native library of the package in-tree: 3d-ns-fsi_b200/lib/libnsfsi.so.
+"""Builds the native library of the package in-tree: 3d-ns-fsi_b200/lib/libnsfsi.so, and the reference-style
+driver program 3d-ns-fsi_b200/bin/nsfsi_main (host/main.cpp).
 
 CUDA sources are compiled by nvcc for sm_100a only; the host setup, config reader and C ABI are C++
 compiled with -ffp-contract=off (the setup must reproduce the reference's floating-point expressions
@@ -13,6 +14,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIB_DIR, "libnsfsi.so")
+MAIN = os.path.join(PKG, "bin", "nsfsi_main")
 BUILD = os.path.join(PKG, "_build")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
@@ -66,6 +68,13 @@ def build(verbose=False, ptxas_info=False):
     if _stale(LIB, objs):
         _run(["g++", "-shared", "-o", LIB, *objs, "-L" + os.path.join(CUDA, "lib64"), "-lcudart_static", "-ldl", "-lrt",
               "-lpthread", "-Wl,--no-undefined"])
+    # the reference-style driver program (host/main.cpp over host/nsfsi_host.hpp)
+    main_src = os.path.join(PKG, "host", "main.cpp")
+    deps = [main_src, os.path.join(PKG, "host", "nsfsi_host.hpp"), os.path.join(ROOT, "include", "nsfsi.h"), LIB]
+    if _stale(MAIN, deps):
+        os.makedirs(os.path.dirname(MAIN), exist_ok=True)
+        _run(["g++", "-std=c++17", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(PKG, "host"),
+              main_src, "-o", MAIN, "-L" + LIB_DIR, "-lnsfsi", "-Wl,-rpath,$ORIGIN/../lib"])
     return LIB
 
 

@@ -666,6 +666,16 @@ nsf_status nsf_get_node_types(nsf_solver* s, uint8_t* out) {
   return NSF_OK;
 }
 
+nsf_status nsf_get_geometry(nsf_solver* s, double* out) {
+  if (!s || !out) return NSF_ERR_ARG;
+  if (!s->initialized) return NSF_ERR_STATE;
+  for (int a = 0; a < 3; ++a) {
+    out[a] = s->setup.d[a];
+    out[3 + a] = s->setup.off[a];
+  }
+  return NSF_OK;
+}
+
 nsf_status nsf_get_num_bodies(nsf_solver* s, uint32_t* nb) {
   if (!s || !nb) return NSF_ERR_ARG;
   if (!s->initialized) return NSF_ERR_STATE;

@@ -82,6 +82,7 @@ def lib():
         "nsf_download": (i32, [vp, u32, dp]),
         "nsf_upload_conserved": (i32, [vp, dp]),
         "nsf_get_node_types": (i32, [vp, ctypes.POINTER(ctypes.c_uint8)]),
+        "nsf_get_geometry": (i32, [vp, dp]),
         "nsf_get_num_bodies": (i32, [vp, ctypes.POINTER(u32)]),
         "nsf_get_body_counts": (i32, [vp, u32, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]),
         "nsf_get_ghosts": (i32, [vp, u32, dp]),

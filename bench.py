@@ -26,6 +26,9 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     "tgv256": dict(case="tgv256", desc="Taylor-Green vortex, periodic 256^3, M0=0.1, Re=1600, CFL 0.5, FP64"),
     "sphere48": dict(case="sphere48", desc="single sphere 48^3, inflow/outflow x, periodic y/z, M0=0.3, Re_D=100"),
+    "spheres16": dict(case="spheres16", desc="16 spheres, 256x128x128, inflow/outflow x, periodic y/z, M0=0.3, "
+                                             "Re_D=200 on the mean diameter"),
+    "tgv128": dict(case="tgv128", desc="Taylor-Green vortex, periodic 128^3 (profiling size), FP64"),
 }
 BYTES_PER_NODE_STEP = 680  # algorithmic HBM bytes per node per RK4 step (stage-fused scheme)
 STAGE_BYTES = [120, 200, 200, 160]
@@ -40,8 +43,9 @@ def measured_peak():
 
 
 def profile_traffic():
-    """Stage-kernel DRAM bytes per node-step from the committed ncu summary, if one exists."""
-    p = os.path.join(ROOT, "profiles", "k_stage_tgv256.md")
+    """Stage-kernel DRAM bytes per node-step from the committed ncu summary (captured on the 128^3
+    Taylor-Green case; DRAM traffic of the streaming kernel grows in proportion to the nodes), if present."""
+    p = os.path.join(ROOT, "profiles", "k_stage_ws_tgv128.md")
     try:
         for line in open(p):
             if line.startswith("dram_bytes_per_node_step:"):
@@ -150,6 +154,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tgv256", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -204,7 +209,8 @@ def main():
     # end to end through the C ABI with host buffers: pinned upload of the initial state, K steps with
     # the per-step t/dt/timeLevel read-back Simulation::run needs, pinned download of the final state
     # (every rank runs its replica; the slowest rank's wall time counts)
-    if True:
+    e2e = None
+    if not args.no_e2e:
         s2 = nsfsi.Solver(cfg, device=local)
         u0 = s2.download(range(5))
         pin_in = torch.empty((5, nodes), dtype=torch.float64, pin_memory=True)

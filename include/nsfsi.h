@@ -4,8 +4,8 @@
  *
  * The reference (Frederik-Kris/3D-NS-FSI) is a pure C++ program with no foreign-function interface.
  * Each entry point below replaces one piece of its C++ call surface, cited as path:line in the
- * reference project; the C++ host classes in 3d-ns-fsi_b200/host/ (ConfigSettings, Solver, Mesh,
- * Simulation) are re-expressed on top of these calls.
+ * reference project; the C++ host classes in 3d-ns-fsi_b200/host/nsfsi_host.hpp (ConfigSettings, Solver,
+ * Mesh, OutputManager, Simulation) are re-expressed on top of these calls.
  *
  * Memory model: the solver handle owns all device memory (allocated in nsf_create / nsf_initialize,
  * freed in nsf_destroy) and one CUDA stream. Fields stay resident in HBM in the reference's SoA layout
@@ -133,6 +133,9 @@ nsf_status nsf_upload_conserved(nsf_solver* s, const double* host);
 
 /* Node classification (NodeTypeEnum values, Node.h:27-34), N bytes. */
 nsf_status nsf_get_node_types(nsf_solver* s, uint8_t* out);
+/* Grid spacing and origin offset, 6 doubles: dx, dy, dz, positionOffset x, y, z (Mesh::dx/dy/dz and
+ * Mesh::positionOffset, set by boundary type in Mesh::setupBoundaries, Mesh.cpp:40-49). */
+nsf_status nsf_get_geometry(nsf_solver* s, double* out);
 /* Number of immersed bodies and, per body, ghost / filter counts and how many ghosts the image-point
  * closure loop added (Boundary.cpp:910-916). */
 nsf_status nsf_get_num_bodies(nsf_solver* s, uint32_t* nbodies);

@@ -13,17 +13,21 @@
 // explicit-instantiation access idiom (C++17 [temp.spec]/6), so no reference source is modified.
 // case.kind = "shipped" instead calls Solver::initialize() unchanged (the reference's default case).
 //
-// Usage: ref_runner <case.cfg> <outdir> [--dump s1,s2,...] [--final] [--time W K]
+// Usage: ref_runner <case.cfg> <outdir> [--dump s1,s2,...] [--final] [--vtk] [--time W K]
+// --vtk: after the run, the reference's OutputManager writes the VTK snapshot, times.dat and the norm
+// files of the final state into <outdir>/output.
 // The dump loop stops where Simulation::checkStoppingCriterion (Simulation.cpp:34-52) would stop an
 // end_time run; --final then also writes that last state as fields_final.bin.
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <chrono>
+#include <filesystem>
 #include <string>
 #include <vector>
 #include <set>
 
+#include "OutputManager.h"
 #include "Solver.h"
 
 // ---- access to private members (explicit-instantiation idiom) -------------------------------------
@@ -56,6 +60,21 @@ struct BodyFilter {
   friend type get(BodyFilter);
 };
 template struct Grab<BodyFilter, &ImmersedBoundary::filterNodes>;
+struct OutStore {
+  typedef void (OutputManager::*type)(const Mesh&, double);
+  friend type get(OutStore);
+};
+template struct Grab<OutStore, &OutputManager::storeCurrentSolution>;
+struct OutTimes {
+  typedef void (OutputManager::*type)();
+  friend type get(OutTimes);
+};
+template struct Grab<OutTimes, &OutputManager::writeOutputTimes>;
+struct OutNorms {
+  typedef void (OutputManager::*type)(const ConservedVariablesVectorGroup&);
+  friend type get(OutNorms);
+};
+template struct Grab<OutNorms, &OutputManager::writeConvergenceHistoryFiles>;
 
 // ---- seeded noise shared with the product (splitmix64, Steele/Lea/Flood 2014) ----------------------
 static uint64_t splitmix64(uint64_t& s) {
@@ -93,7 +112,7 @@ int main(int argc, char** argv) {
   std::string cfgPath = argv[1], outDir = argv[2];
   std::set<unsigned long> dumps;
   long timeWarm = -1, timeSteps = -1;
-  bool dumpFinal = false;
+  bool dumpFinal = false, writeVtk = false;
   for (int a = 3; a < argc; ++a) {
     if (!std::strcmp(argv[a], "--dump") && a + 1 < argc) {
       std::string s = argv[++a];
@@ -106,6 +125,8 @@ int main(int argc, char** argv) {
       }
     } else if (!std::strcmp(argv[a], "--final")) {
       dumpFinal = true;
+    } else if (!std::strcmp(argv[a], "--vtk")) {
+      writeVtk = true;
     } else if (!std::strcmp(argv[a], "--time") && a + 2 < argc) {
       timeWarm = std::stol(argv[++a]);
       timeSteps = std::stol(argv[++a]);
@@ -308,5 +329,15 @@ int main(int argc, char** argv) {
     if (dumps.count(timeLevel)) dumpFields(t, timeLevel);
   }
   if (dumpFinal) dumpFields(t, timeLevel, true);
+  if (writeVtk) {
+    // The reference's own output writer on the final state: out.vtk.0, times.dat and norm_*.dat in
+    // <outdir>/output (OutputManager writes to ./output).
+    std::filesystem::create_directories(outDir + "/output");
+    std::filesystem::current_path(outDir);
+    OutputManager out(params);
+    (out.*get(OutStore()))(mesh, t);
+    (out.*get(OutTimes()))();
+    (out.*get(OutNorms()))(solver.getConvergenceHistory());
+  }
   return 0;
 }

@@ -62,8 +62,30 @@ def make(name):
     print(name, "ok", os.path.getsize(os.path.join(HERE, name + ".npz")))
 
 
+# VTK / times.dat / norm files written by the reference's own OutputManager at the end of a run
+# (ref_runner --vtk), gzipped into tests/golden/vtk_<case>/.
+VTK_CASES = {"sphere_small": ("tests/golden/cases/sphere_small.cfg", 30)}
+
+
+def make_vtk(name):
+    import gzip
+    import shutil
+    import subprocess
+    import tempfile
+    cfg, steps = VTK_CASES[name]
+    out = tempfile.mkdtemp(prefix="nsf_vtk_")
+    subprocess.run([po.REF_RUNNER, os.path.join(ROOT, cfg), out, "--dump", str(steps), "--vtk"], check=True,
+                   stdout=subprocess.DEVNULL)
+    dst = os.path.join(HERE, "vtk_" + name)
+    os.makedirs(dst, exist_ok=True)
+    for f in sorted(os.listdir(os.path.join(out, "output"))):
+        with open(os.path.join(out, "output", f), "rb") as src, gzip.open(os.path.join(dst, f + ".gz"), "wb") as g:
+            shutil.copyfileobj(src, g)
+    print("vtk_" + name, "ok", sorted(os.listdir(dst)))
+
+
 if __name__ == "__main__":
     if not po.ref_available():
         sys.exit("oracle/_ref/ref_runner is not built; run make -f oracle/Makefile.ref first")
-    for n in (sys.argv[1:] or CASES):
-        make(n)
+    for n in (sys.argv[1:] or list(CASES) + ["vtk_" + v for v in VTK_CASES]):
+        make_vtk(n[4:]) if n.startswith("vtk_") else make(n)

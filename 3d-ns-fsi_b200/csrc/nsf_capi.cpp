@@ -17,32 +17,7 @@
 
 using namespace nsf;
 
-struct nsf_solver {
-  nsf_config cfg{};
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  HostSetup setup;
-  bool initialized = false;
-  bool hostOnly = false;  // device < 0: host setup only (classification queries), no GPU work
-  std::vector<void*> allocs;
-  Grid hGrid{};
-  Grid* dGrid = nullptr;
-  StepCtl* dCtl = nullptr;
-  LaunchPlan plan{};
-  cudaGraphExec_t graphExec = nullptr;
-  cudaGraph_t graph = nullptr;
-  int launchesPerStep = 0;
-  int nSM = 0;
-  // solid inactive nodes with stored primitive values (downloads)
-  long long* dDlNode = nullptr;
-  double* dDlPrim = nullptr;    // values after the first step (periodic copies applied)
-  double* dDlPrimIc = nullptr;  // values before any step (each node's own initial values)
-  long long* dDlNodeIc = nullptr;
-  int nDl = 0, nDlIc = 0;
-  std::string err;
-  std::vector<CUtensorMap> hostMaps;
-  void* encodeFn = nullptr;
-};
+#include "nsf_solver_impl.h"
 
 namespace {
 
@@ -175,8 +150,9 @@ nsf_status build_device(nsf_solver* s) {
   auto dev = [&](size_t n) { return dev_index(S, NKp, n); };
   Grid& G = s->hGrid;
   G = Grid{};
-  // stage-kernel tile shape: NSF_STAGE_TILE=16x16 or 32x8 (default)
-  const int tile = [] {
+  // stage-kernel tile shape: the handle's request (ensembles, tuned plans), else NSF_STAGE_TILE=16x16 or
+  // 32x8 (default)
+  const int tile = s->tileRequest >= 0 ? s->tileRequest : [] {
     const char* e = std::getenv("NSF_STAGE_TILE");
     return e && std::string(e) == "16x16" ? int(STAGE_TILE_16x16) : int(STAGE_TILE_32x8);
   }();
@@ -453,9 +429,19 @@ nsf_status build_device(nsf_solver* s) {
   for (int c0 = 1; c0 <= planes; c0 += clen)
     for (int tj = 0; tj < nj; ++tj)
       for (int tk = 0; tk < nk; ++tk)
-        items.push_back(StageItem{1 + tj * TJ, 1 + tk * TK, c0, std::min(planes, c0 + clen - 1)});
+        items.push_back(StageItem{1 + tj * TJ, 1 + tk * TK, c0, std::min(planes, c0 + clen - 1), 0});
   L.nItems = int(items.size());
   L.stageBlocks = std::min(L.nItems, slots);
+  {  // CTA b takes items b, b + stageBlocks, ... (whole waves of equal items), stored contiguously
+    std::vector<StageItem> ordered;
+    std::vector<int> start(1, 0);
+    for (int b = 0; b < L.stageBlocks; ++b) {
+      for (int q = b; q < L.nItems; q += L.stageBlocks) ordered.push_back(items[q]);
+      start.push_back(int(ordered.size()));
+    }
+    items.swap(ordered);
+    if ((st = upload(s, &L.ctaStart, start)) != NSF_OK) return st;
+  }
   if ((st = upload(s, &L.items, items)) != NSF_OK) return st;
   for (int a = 0; a < 3; ++a) {
     int n1 = 1, n2 = 1;
@@ -485,6 +471,7 @@ nsf_status build_device(nsf_solver* s) {
   CK(cudaMemset(dNorm, 0, 5 * size_t(L.nSlots) * sizeof(double)));
   G.normPart = dNorm;
   G.nNormSlots = L.nSlots;
+  G.normSlotFilter = L.stageBlocks;
   double* dHist;
   if ((st = dalloc(s, &dHist, 7 * size_t(MAX_HIST))) != NSF_OK) return st;
   G.hist = dHist;

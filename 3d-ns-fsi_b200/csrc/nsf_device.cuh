@@ -103,8 +103,9 @@ struct Grid {
   int eAxis[6], eSide[6], eBc[6];
   int eBox[6][6];           // owned box i0,i1,j0,j1,k0,k1
   // reductions
-  double* normPart;         // [nNormSlots][5]
+  double* normPart;         // [nNormSlots][5]: stage-kernel CTAs first, then the near-body filter's blocks
   int nNormSlots;
+  int normSlotFilter;       // first slot of the near-body filter's partial sums
   double* hist;             // [MAX_HIST][7]
 };
 
@@ -113,6 +114,7 @@ enum StageTile { STAGE_TILE_32x8 = 0, STAGE_TILE_16x16 = 1 };
 
 struct StageItem {
   int j0, k0, i0, i1;  // tile origin (first computed j, k) and inclusive i range
+  int g;               // ensemble member (0 for a single grid)
 };
 
 // Launch geometry of one step, fixed at initialisation.
@@ -121,7 +123,8 @@ struct LaunchPlan {
   int tile;  // StageTile
   int stageBlocks;
   int nItems;
-  StageItem* items;  // device
+  StageItem* items;  // device; the items of CTA b are items[ctaStart[b] .. ctaStart[b + 1])
+  int* ctaStart;     // device, stageBlocks + 1 entries
   int edgeGrid[3][3];  // per axis: grid x, y, z
   int filterBlocks, ghostBlocks, solidBlocks, gfBlocks;
   int nSlots;
@@ -144,12 +147,16 @@ int stage_num_maps();
 int stage_launch_registers(int v);
 bool stage_register_split_ok(int v);
 void launch_stage(const Grid& hg, const LaunchPlan& L, int s, void* stream);
+void launch_stage_ensemble(const Grid* dGrids, const LaunchPlan& L, int s, void* stream);
 // dg: the grid in device memory (read by the small kernels); hg: the same grid on the host (passed by
 // value to the stage kernel, whose coefficients then come from the constant bank).
 int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream);
 // Same sequence, launched eagerly, with events recorded around each of the four stage kernels
 // (events[2*s], events[2*s+1]); used for per-kernel timing.
 int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events);
+// One RK4 step of every member of an ensemble (dGrids: device array of `members` grids; L: the ensemble's
+// combined plan). events: NULL, or 8 events recorded around the four stage kernels.
+int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* stream, void* events);
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,
                           double dx, double dy, double dz, double* w, void* stream);
 void launch_download_prims(const Grid* dg, long long N, double* out, const long long* inodes, const double* ip7,

@@ -26,9 +26,12 @@ namespace nsf {
 // ----------------------------------------------------------------------------------------------
 // Prologue: Simulation::checkStoppingCriterion (end_time), Mesh::checkFilterCondition (Mesh.cpp:85-103),
 // the buffer swaps of Mesh.cpp:133-151 expressed as role changes, and per-stage buffer roles.
-__global__ void k_prologue(Grid* g) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Member m = blockIdx.x of the grid array (a single grid: one block).
+__global__ void k_prologue(Grid* grids) {
+  if (threadIdx.x != 0) return;
+  Grid* g = grids + blockIdx.x;
   StepCtl* c = g->ctl;
+  for (int f = 0; f < 5; ++f) g->normPart[f] = 0.0;  // slot 0: the ensemble stage kernel adds into it
   const Consts& C = g->C;
   c->active = C.endTime ? (c->t < C.tEnd) : 1;
   if (!c->active) return;
@@ -113,7 +116,8 @@ __global__ void k_prologue(Grid* g) {
 // Mesh::applyFilter_ifAppropriate body (Mesh.cpp:110-134): interior nodes get the 7-point filter,
 // every node of an edge boundary's owned box (whatever its type) and every solid-ghost node is copied,
 // the remaining solid inactive nodes are left as they are.
-__global__ void k_density_filter(const Grid* __restrict__ g) {
+__global__ void k_density_filter(const Grid* __restrict__ grids) {
+  const Grid* g = grids + blockIdx.y;
   const StepCtl* c = g->ctl;
   if (!c->active || !c->filterNow) return;
   const double* __restrict__ src = c->gfSrc;
@@ -130,7 +134,8 @@ __global__ void k_density_filter(const Grid* __restrict__ g) {
 
 // ----------------------------------------------------------------------------------------------
 // Solid-node values the reference's stage buffer still holds from earlier writes (see nsf_device.cuh).
-__global__ void k_solid_copy(const Grid* __restrict__ g, int s) {
+__global__ void k_solid_copy(const Grid* __restrict__ grids, int s) {
+  const Grid* g = grids + blockIdx.y;
   const StepCtl* c = g->ctl;
   if (!c->active) return;
   const int mask = c->copyMask[s];
@@ -147,16 +152,18 @@ __global__ void k_solid_copy(const Grid* __restrict__ g, int s) {
 // Mesh-edge boundary conditions of one axis (both faces; the faces of one axis never read each other's
 // nodes). Launched for x, then y, then z: the reference's application order outlet/inlet (x), y-max,
 // y-min, z-max, z-min (Mesh.cpp:155-167 after the reversal at Mesh.cpp:70). Threads cover the owned box.
-__global__ void k_edge_bc(const Grid* __restrict__ gp, int s, int axis) {
+// blockIdx.z = 2 * member + (which of the axis's edges).
+__global__ void k_edge_bc(const Grid* __restrict__ grids, int s, int axis) {
   __shared__ double red[4 * 32];
-  const Grid& G = *gp;
+  const Grid& G = grids[blockIdx.z >> 1];
+  const int edgeSlot = blockIdx.z & 1;
   StepCtl* c = G.ctl;
   if (!c->active) return;
   const Consts& C = G.C;
   int e = -1, seen = 0;
   for (int q = 0; q < G.nEdge; ++q)
     if (G.eAxis[q] == axis) {
-      if (seen == (int)blockIdx.z) e = q;
+      if (seen == edgeSlot) e = q;
       ++seen;
     }
   DtAcc dta;
@@ -269,9 +276,9 @@ __global__ void k_edge_bc(const Grid* __restrict__ gp, int s, int axis) {
 // filtered value is computed from unfiltered neighbours; results go to fnew and are written back by
 // k_ghost. The values before the filter go to fpre: the reference does not recompute the primitive
 // variables of these nodes after filtering, so the next stage builds their primitives from fpre.
-__global__ void k_body_filter(const Grid* __restrict__ gp, int s, int slotBase) {
+__global__ void k_body_filter(const Grid* __restrict__ grids, int s) {
   __shared__ double red[5 * 32];
-  const Grid& G = *gp;
+  const Grid& G = grids[blockIdx.y];
   StepCtl* c = G.ctl;
   if (!c->active) return;
   const Consts& C = G.C;
@@ -301,7 +308,7 @@ __global__ void k_body_filter(const Grid* __restrict__ gp, int s, int slotBase) 
   }
   if (s == 3) {
     flush_dt(c, dta, red);
-    flush_norms(G.normPart + 5 * (slotBase + blockIdx.x), nsum, red);
+    flush_norms(G.normPart + 5 * (G.normSlotFilter + blockIdx.x), nsum, red);
     if (bad) atomicOr(&c->nonFinite, 1);
   }
 }
@@ -311,9 +318,9 @@ __global__ void k_body_filter(const Grid* __restrict__ gp, int s, int slotBase) 
 // ghost value = image value with momentum negated (getGhostNodeBCVariables, :777-785). The same
 // launch writes the filtered values back (ghosts read them through fnew) and, on stage 4, adds the dt
 // terms of the solid inactive nodes, whose primitive values the reference never updates.
-__global__ void k_ghost(const Grid* __restrict__ gp, int s) {
+__global__ void k_ghost(const Grid* __restrict__ grids, int s) {
   __shared__ double red[4 * 32];
-  const Grid& G = *gp;
+  const Grid& G = grids[blockIdx.y];
   StepCtl* c = G.ctl;
   if (!c->active) return;
   const Consts& C = G.C;
@@ -376,8 +383,10 @@ __global__ void k_ghost(const Grid* __restrict__ gp, int s) {
 // ----------------------------------------------------------------------------------------------
 // End of step: change norms (Mesh::getNormOfChange, Mesh.cpp:171-178), next dt
 // (Solver::updateTimeStepSize, Solver.cpp:80-126), t += dt, ++timeLevel, history row.
-__global__ void k_finalize(Grid* g, int nSlots) {
+__global__ void k_finalize(Grid* grids) {
   __shared__ double red[5 * 32];
+  Grid* g = grids + blockIdx.x;
+  const int nSlots = g->nNormSlots;
   StepCtl* c = g->ctl;
   if (!c->active) return;
   const Consts& C = g->C;
@@ -558,46 +567,58 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 
 // ----------------------------------------------------------------------------------------------
 // Host-side launch helpers (called from nsf_capi.cpp).
-static int enqueue_impl(Grid* dg, const Grid& hg, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev) {
+// One RK4 step for `members` grids (dg: device array of them). hg: the grid on the host for a single-grid
+// solver (its stage kernel takes the grid by value), or NULL for an ensemble (the ensemble stage kernel
+// reads every member from dg). The small kernels carry the member in a grid dimension; their block
+// counts in L are the maxima over the members.
+static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev) {
   int launches = 0;
-  k_prologue<<<1, 32, 0, st>>>(dg);
+  const unsigned M = unsigned(members);
+  k_prologue<<<M, 32, 0, st>>>(dg);
   ++launches;
-  k_density_filter<<<L.gfBlocks, 256, 0, st>>>(dg);
+  k_density_filter<<<dim3(L.gfBlocks, M), 256, 0, st>>>(dg);
   ++launches;
   for (int s = 0; s < 4; ++s) {
     if (ev) cudaEventRecord(ev[2 * s], st);
-    launch_stage(hg, L, s, st);
+    if (hg)
+      launch_stage(*hg, L, s, st);
+    else
+      launch_stage_ensemble(dg, L, s, st);
     if (ev) cudaEventRecord(ev[2 * s + 1], st);
     ++launches;
     if (L.hasSolid) {
-      k_solid_copy<<<L.solidBlocks, 256, 0, st>>>(dg, s);
+      k_solid_copy<<<dim3(L.solidBlocks, M), 256, 0, st>>>(dg, s);
       ++launches;
     }
     for (int a = 0; a < 3; ++a) {
-      dim3 grid(L.edgeGrid[a][0], L.edgeGrid[a][1], L.edgeGrid[a][2]);
+      dim3 grid(L.edgeGrid[a][0], L.edgeGrid[a][1], 2 * M);
       k_edge_bc<<<grid, dim3(32, 8), 0, st>>>(dg, s, a);
       ++launches;
     }
     if (L.hasFilter) {
-      k_body_filter<<<L.filterBlocks, 256, 0, st>>>(dg, s, L.stageBlocks);
+      k_body_filter<<<dim3(L.filterBlocks, M), 256, 0, st>>>(dg, s);
       ++launches;
     }
     if (L.hasGhostWork) {
-      k_ghost<<<L.ghostBlocks, 256, 0, st>>>(dg, s);
+      k_ghost<<<dim3(L.ghostBlocks, M), 256, 0, st>>>(dg, s);
       ++launches;
     }
   }
-  k_finalize<<<1, 256, 0, st>>>(dg, L.nSlots);
+  k_finalize<<<M, 256, 0, st>>>(dg);
   ++launches;
   return launches;
 }
 
 int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream) {
-  return enqueue_impl(dg, hg, L, static_cast<cudaStream_t>(stream), nullptr);
+  return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* stream, void* events) {
+  return enqueue_impl(dGrids, nullptr, members, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events));
 }
 
 int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events) {
-  return enqueue_impl(dg, hg, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events));
+  return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events));
 }
 
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,

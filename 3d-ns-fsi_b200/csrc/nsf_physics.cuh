@@ -15,7 +15,14 @@ struct Prim {
   double u, v, w, p, T, mu, ka;
 };
 
-__device__ __forceinline__ Prim prims_of(const Consts& C, double rho, double ru, double rv, double rw, double rE) {
+// The constants prims_of reads, small enough to keep in registers.
+struct ThermoConsts {
+  double gamma, gm1, sc1, re, pf;
+};
+
+// CT: Consts, or any struct with the members gamma, gm1, sc1, re and pf (ThermoConsts).
+template <class CT>
+__device__ __forceinline__ Prim prims_of(const CT& C, double rho, double ru, double rv, double rw, double rE) {
   Prim q;
   const double r1 = 1.0 / (rho + 1.0);
   q.u = ru * r1;

@@ -1,0 +1,42 @@
+// The solver handle behind the C ABI (include/nsfsi.h), shared by nsf_capi.cpp and nsf_ensemble.cpp.
+#ifndef NSF_SOLVER_IMPL_H
+#define NSF_SOLVER_IMPL_H
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "nsf_device.cuh"
+#include "nsf_internal.h"
+
+struct nsf_solver {
+  nsf_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  nsf::HostSetup setup;
+  bool initialized = false;
+  bool hostOnly = false;  // device < 0: host setup only (classification queries), no GPU work
+  std::vector<void*> allocs;
+  nsf::Grid hGrid{};
+  nsf::Grid* dGrid = nullptr;
+  nsf::StepCtl* dCtl = nullptr;
+  nsf::LaunchPlan plan{};
+  cudaGraphExec_t graphExec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int launchesPerStep = 0;
+  int nSM = 0;
+  // solid inactive nodes with stored primitive values (downloads)
+  long long* dDlNode = nullptr;
+  double* dDlPrim = nullptr;    // values after the first step (periodic copies applied)
+  double* dDlPrimIc = nullptr;  // values before any step (each node's own initial values)
+  long long* dDlNodeIc = nullptr;
+  int nDl = 0, nDlIc = 0;
+  std::string err;
+  std::vector<CUtensorMap> hostMaps;
+  void* encodeFn = nullptr;
+  int tileRequest = -1;  // StageTile to use, or -1 for the default
+};
+
+#endif

@@ -70,7 +70,10 @@ struct Tile {
   static constexpr size_t OFF_FLAG = OFF_BAR + 2 * (NC + NP + NE) * 8;
   static constexpr size_t OFF_RED = (OFF_FLAG + 16 + 127) / 128 * 128;
   static constexpr size_t OFF_CTL = OFF_RED + 5 * 32 * 8;
-  static constexpr size_t SMEM = OFF_CTL + ((sizeof(StepCtl) + 127) / 128) * 128;
+  // ensemble kernels: one copy of the current member's Consts per column warp
+  static constexpr size_t CSM_BYTES = (sizeof(Consts) + 15) / 16 * 16;
+  static constexpr size_t OFF_CSM = OFF_CTL + ((sizeof(StepCtl) + 127) / 128) * 128;
+  static constexpr size_t SMEM = OFF_CSM + 8 * CSM_BYTES;
   static_assert(NCOL == 256, "two column warpgroups");
   static_assert(TK % 16 == 0, "box x coordinate k0 - 1 = TK * t must be 16-byte aligned for TMA");
   static_assert((EFS * 8) % 128 == 0 && (FS * 8) % 128 == 0, "TMA destinations need 128 B alignment");
@@ -147,9 +150,14 @@ __device__ __forceinline__ void dt_terms(const Consts& C, const double (&u)[5], 
 
 }  // namespace
 
-template <int TK_, int TJ_>
+// ENS = false: one grid, passed by value (its stencil coefficients are then constant-bank operands).
+// ENS = true: an ensemble; every work item names its member (StageItem::g) in the device array `grids`,
+// and each member's StepCtl is read from device memory.
+// Work items of CTA b: items[ctaStart[b] .. ctaStart[b + 1]).
+template <int TK_, int TJ_, bool ENS>
 __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
-    k_stage_ws(const __grid_constant__ Grid G, const StageItem* __restrict__ items, int nItems, int s) {
+    k_stage_ws(const __grid_constant__ Grid G0, const Grid* __restrict__ grids, const StageItem* __restrict__ items,
+               const int* __restrict__ ctaStart, int s) {
   using namespace ws;
   using TL = Tile<TK_, TJ_>;
   constexpr int TK = TL::TK, NCOL = TL::NCOL, HK = TL::HK, HP = TL::HP, FS = TL::FS, EFS = TL::EFS,
@@ -158,7 +166,8 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
                      EPI_BOX_BYTES = TL::EPI_BOX_BYTES;
   constexpr size_t TYPE_OFF = TL::TYPE_OFF, CONS_SLOT = TL::CONS_SLOT, PRIM_SLOT = TL::PRIM_SLOT,
                    EPI_SLOT = TL::EPI_SLOT, OFF_CONS = TL::OFF_CONS, OFF_PRIM = TL::OFF_PRIM, OFF_EPI = TL::OFF_EPI,
-                   OFF_BAR = TL::OFF_BAR, OFF_FLAG = TL::OFF_FLAG, OFF_RED = TL::OFF_RED, OFF_CTL = TL::OFF_CTL;
+                   OFF_BAR = TL::OFF_BAR, OFF_FLAG = TL::OFF_FLAG, OFF_RED = TL::OFF_RED, OFF_CTL = TL::OFF_CTL,
+                   OFF_CSM = TL::OFF_CSM, CSM_BYTES = TL::CSM_BYTES;
   extern __shared__ __align__(1024) unsigned char sm[];
   uint64_t* consFull = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
   uint64_t* consEmpty = consFull + NC;
@@ -168,10 +177,19 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
   uint64_t* epiEmpty = epiFull + NE;
   volatile int* abortFlag = reinterpret_cast<volatile int*>(sm + OFF_FLAG);
   double* red = reinterpret_cast<double*>(sm + OFF_RED);
-  StepCtl& ctl = *reinterpret_cast<StepCtl*>(sm + OFF_CTL);
+  StepCtl& ctl0 = *reinterpret_cast<StepCtl*>(sm + OFF_CTL);  // single grid: a copy of its StepCtl
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int itBegin = ctaStart[blockIdx.x], itEnd = ctaStart[blockIdx.x + 1];
+  auto grid_of = [&](const StageItem& w) -> const Grid& {
+    if constexpr (ENS) return grids[w.g];
+    else return G0;
+  };
+  auto ctl_of = [&](const Grid& g) -> const StepCtl& {
+    if constexpr (ENS) return *g.ctl;
+    else return ctl0;
+  };
   if (tid == 0) {
-    ctl = *G.ctl;
+    if (!ENS) ctl0 = *G0.ctl;
     *abortFlag = 0;
     for (int q = 0; q < NC; ++q) {
       mbar_init(&consFull[q], 1);
@@ -188,64 +206,87 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  if (!ctl.active) return;
-  const Consts& C = G.C;
+  if (!ENS && !ctl0.active) return;
   DtAcc dta;
   double nsum[5] = {0, 0, 0, 0, 0};
   int bad = 0;
-  auto fail = [&]() {
+  auto fail = [&](const Grid& g) {
     *abortFlag = 1;
-    atomicExch(&G.ctl->timeout, 1);
+    atomicExch(&g.ctl->timeout, 1);
   };
+  // an ensemble member whose run has ended (end_time reached) is skipped by every role
+  auto skip = [&](const StageItem& w) { return ENS && !ctl_of(grid_of(w)).active; };
 
   if (warp < 4) {
     reg_dealloc<REG_LOW>();
     if (warp == 0) {
       // ------------------------------------------------------------------ producer (one thread)
       if (lane == 0) {
-        const CUtensorMap* maps = static_cast<const CUtensorMap*>(G.tmaps);
         const int epiFields = s == 0 ? 5 : 10;
-        int cIt = blockIdx.x, cP = cIt < nItems ? items[cIt].i0 - 1 : 0;  // next staged plane
-        int eIt = blockIdx.x, eP = eIt < nItems ? items[eIt].i0 : 0;      // next computed plane
+        auto next_item = [&](int it) {
+          while (it < itEnd && skip(items[it])) ++it;
+          return it;
+        };
+        int cIt = next_item(itBegin), cP = cIt < itEnd ? items[cIt].i0 - 1 : 0;  // next staged plane
+        int eIt = cIt, eP = eIt < itEnd ? items[eIt].i0 : 0;                     // next computed plane
         uint32_t cq = 0, eq = 0;
         long long idle = 0;
-        while ((cIt < nItems || eIt < nItems) && !*abortFlag) {
+        // descriptors of the item each cursor is in (reloaded only when the cursor moves to a new item)
+        const CUtensorMap* cMaps = nullptr;
+        const CUtensorMap* eMaps = nullptr;
+        int cPhys[5] = {0, 0, 0, 0, 0}, ePhys[5] = {0, 0, 0, 0, 0};
+        int cLoaded = -1, eLoaded = -1;
+        while ((cIt < itEnd || eIt < itEnd) && !*abortFlag) {
           bool progressed = false;
-          if (cIt < nItems) {
+          if (cIt < itEnd) {
             const uint32_t sl = cq % NC;
             if (cq < NC || mbar_try(&consEmpty[sl], ((cq / NC) - 1) & 1)) {
               const StageItem w = items[cIt];
+              if (cLoaded != cIt) {
+                const Grid& G = grid_of(w);
+                const StepCtl& ctl = ctl_of(G);
+                cMaps = static_cast<const CUtensorMap*>(G.tmaps);
+                cPhys[0] = ctl.rPhys[s];
+                for (int f = 1; f < 5; ++f) cPhys[f] = ctl.iPhys[s][f];
+                cLoaded = cIt;
+              }
               unsigned char* dst = sm + OFF_CONS + sl * CONS_SLOT;
               mbar_expect_tx(&consFull[sl], 5 * CONS_BOX_BYTES + TYPE_BOX_BYTES);
-              tma_load3(dst, &maps[MAP_CONS + ctl.rPhys[s] * 5 + 0], w.k0 - 1, w.j0 - 1, cP, &consFull[sl]);
-              for (int f = 1; f < 5; ++f)
-                tma_load3(dst + size_t(f) * FS * 8, &maps[MAP_CONS + ctl.iPhys[s][f] * 5 + f], w.k0 - 1, w.j0 - 1, cP,
+              for (int f = 0; f < 5; ++f)
+                tma_load3(dst + size_t(f) * FS * 8, &cMaps[MAP_CONS + cPhys[f] * 5 + f], w.k0 - 1, w.j0 - 1, cP,
                           &consFull[sl]);
-              tma_load3(dst + TYPE_OFF, &maps[MAP_TYPE], w.k0 - 1, w.j0 - 1, cP, &consFull[sl]);
+              tma_load3(dst + TYPE_OFF, &cMaps[MAP_TYPE], w.k0 - 1, w.j0 - 1, cP, &consFull[sl]);
               ++cq;
               if (++cP > w.i1 + 1) {
-                cIt += gridDim.x;
-                if (cIt < nItems) cP = items[cIt].i0 - 1;
+                cIt = next_item(cIt + 1);
+                if (cIt < itEnd) cP = items[cIt].i0 - 1;
               }
               progressed = true;
             }
           }
-          if (eIt < nItems) {
+          if (eIt < itEnd) {
             const uint32_t se = eq % NE;
             if (eq < NE || mbar_try(&epiEmpty[se], ((eq / NE) - 1) & 1)) {
               const StageItem w = items[eIt];
+              if (eLoaded != eIt) {
+                const Grid& G = grid_of(w);
+                const StepCtl& ctl = ctl_of(G);
+                eMaps = static_cast<const CUtensorMap*>(G.tmaps);
+                for (int f = 0; f < 5; ++f) ePhys[f] = ctl.u0Phys[f];
+                eLoaded = eIt;
+              }
               unsigned char* dst = sm + OFF_EPI + se * EPI_SLOT;
               mbar_expect_tx(&epiFull[se], epiFields * EPI_BOX_BYTES);
               for (int f = 0; f < 5; ++f)
-                tma_load3(dst + size_t(f) * EFS * 8, &maps[MAP_EPI + ctl.u0Phys[f] * 5 + f], w.k0 - 1, w.j0, eP,
+                tma_load3(dst + size_t(f) * EFS * 8, &eMaps[MAP_EPI + ePhys[f] * 5 + f], w.k0 - 1, w.j0, eP,
                           &epiFull[se]);
               if (s > 0)
                 for (int f = 0; f < 5; ++f)
-                  tma_load3(dst + size_t(5 + f) * EFS * 8, &maps[MAP_ACC + f], w.k0 - 1, w.j0, eP, &epiFull[se]);
+                  tma_load3(dst + size_t(5 + f) * EFS * 8, &eMaps[MAP_ACC + f], w.k0 - 1, w.j0, eP, &epiFull[se]);
               ++eq;
               if (++eP > w.i1) {
-                eIt += gridDim.x;
-                if (eIt < nItems) eP = items[eIt].i0;
+                eIt = next_item(eIt + 1);
+                if (eIt < itEnd) eP = items[eIt].i0;
               }
               progressed = true;
             }
@@ -253,37 +294,42 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           if (progressed) {
             idle = 0;
           } else if (++idle > WAIT_LIMIT) {
-            fail();
+            fail(grid_of(items[cIt < itEnd ? cIt : eIt]));
             break;
           }
         }
         // Every copy issued must have landed before the CTA exits: wait for the last phase of each slot.
         const volatile int never = 0;
+        const Grid& Gf = ENS ? grids[0] : G0;  // where a failed drain is reported
         for (uint32_t sl = 0; sl < NC; ++sl)
           if (cq > sl) {
             const uint32_t last = cq - 1 - ((cq - 1 - sl) % NC);
-            if (!mbar_wait(&consFull[sl], (last / NC) & 1, &never)) atomicExch(&G.ctl->timeout, 1);
+            if (!mbar_wait(&consFull[sl], (last / NC) & 1, &never)) atomicExch(&Gf.ctl->timeout, 1);
           }
         for (uint32_t se = 0; se < NE; ++se)
           if (eq > se) {
             const uint32_t last = eq - 1 - ((eq - 1 - se) % NE);
-            if (!mbar_wait(&epiFull[se], (last / NE) & 1, &never)) atomicExch(&G.ctl->timeout, 1);
+            if (!mbar_wait(&epiFull[se], (last / NE) & 1, &never)) atomicExch(&Gf.ctl->timeout, 1);
           }
       }
     } else {
       // ------------------------------------------------------------------ staging (warps 1-3)
       const int st = tid - 32;
-      const double* __restrict__ fpre = G.fpre;
       uint32_t q = 0;  // staged-plane sequence number, continues across items
       bool ok = true;
-      for (int it = blockIdx.x; it < nItems && ok; it += gridDim.x) {
+      for (int it = itBegin; it < itEnd && ok; ++it) {
         const StageItem w = items[it];
+        if (skip(w)) continue;
+        const Grid& G = grid_of(w);
+        const ThermoConsts C{G.C.gamma, G.C.gm1, G.C.sc1, G.C.re, G.C.pf};
+        const double* __restrict__ fpre = G.fpre;
+        const long long sIs = G.sI, sJs = G.sJ;
         for (int p = w.i0 - 1; p <= w.i1 + 1; ++p, ++q) {
           const uint32_t sl = q % NC, ps = q % NP;
           if (q >= NP) ok = mbar_wait(&primEmpty[ps], ((q / NP) - 1) & 1, abortFlag);
           ok = ok && mbar_wait(&consFull[sl], (q / NC) & 1, abortFlag);
           if (!ok) {
-            fail();
+            fail(G);
             break;
           }
           const double* cs = reinterpret_cast<const double*>(sm + OFF_CONS + sl * CONS_SLOT);
@@ -301,7 +347,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
               const int id = h ? idyc : idx;
               const int hj = id / HK, hk = id - hj * HK;
               if (ts[hj * TYW + hk] & FILTER_BIT) {
-                const long long n = (long long)p * G.sI + (long long)(w.j0 - 1 + hj) * G.sJ + (w.k0 - 1 + hk);
+                const long long n = (long long)p * sIs + (long long)(w.j0 - 1 + hj) * sJs + (w.k0 - 1 + hk);
                 const int f = __ldg(G.fidx + n);
                 rho[h] = fpre[2 * f];
                 rE[h] = fpre[2 * f + 1];
@@ -338,26 +384,39 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
     const int cidx = (ty + 1) * HK + (tx + 1);   // this column's node in a staged plane
     const int eidx = ty * HK + tx + 1;           // ... in an epilogue tile
     const int tcix = (ty + 1) * TYW + (tx + 1);  // ... in a staged type box
-    const double dtUsed = ctl.dtUsed;
-    const double inc = (s == 2) ? dtUsed : dtUsed / 2;
-    const double dtFactor = dtUsed / 6;
-    double* const out0 = ctl.O[s][0];
-    double* const out1 = ctl.O[s][1];
-    double* const out2 = ctl.O[s][2];
-    double* const out3 = ctl.O[s][3];
-    double* const out4 = ctl.O[s][4];
-    double* const accb = G.acc[0];  // accumulator fields are contiguous, G.N doubles apart
-    const long long NdF = G.N;
     const unsigned char* const consBase = sm + OFF_CONS;
     const unsigned char* const primBase = sm + OFF_PRIM;
     uint32_t q = 0, e = 0;  // staged-plane and computed-plane sequence numbers
     bool ok = true;
-    for (int it = blockIdx.x; it < nItems && ok; it += gridDim.x) {
+    for (int it = itBegin; it < itEnd && ok; ++it) {
       const StageItem w = items[it];
+      if (skip(w)) continue;
+      const Grid& G = grid_of(w);
+      const StepCtl& ctl = ctl_of(G);
+      Consts* const myC = reinterpret_cast<Consts*>(sm + OFF_CSM + (warp - 4) * CSM_BYTES);
+      if constexpr (ENS) {  // this warp's copy of the member's coefficients (shared-memory operands)
+        __syncwarp();
+        const double* src = reinterpret_cast<const double*>(&G.C);
+        double* dst = reinterpret_cast<double*>(myC);
+        for (int q = lane; q < int(sizeof(Consts) / 8); q += 32) dst[q] = src[q];
+        __syncwarp();
+      }
+      const Consts& C = ENS ? *myC : G.C;
+      const long long sI = G.sI;
+      const double dtUsed = ctl.dtUsed;
+      const double inc = (s == 2) ? dtUsed : dtUsed / 2;
+      const double dtFactor = dtUsed / 6;
+      double* const out0 = ctl.O[s][0];
+      double* const out1 = ctl.O[s][1];
+      double* const out2 = ctl.O[s][2];
+      double* const out3 = ctl.O[s][3];
+      double* const out4 = ctl.O[s][4];
+      double* const accb = G.acc[0];  // accumulator fields are contiguous, G.N doubles apart
+      const long long NdF = G.N;
       const int j = w.j0 + ty, k = w.k0 + tx;
       const bool inTile = (j <= G.NJ - 2) && (k <= G.NK - 2);
       const int L = w.i1 - w.i0 + 1;
-      long long nR = (long long)w.i0 * G.sI + (long long)j * G.sJ + k;  // node of the next computed plane
+      long long nR = (long long)w.i0 * sI + (long long)j * G.sJ + k;  // node of the next computed plane
       XNode gm1{}, gm2{};
       double fprev[5] = {0, 0, 0, 0, 0};
       XOwn ownPrev{};
@@ -368,7 +427,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
         const int pX = qx % NP, cX = qx % NC;
         ok = mbar_wait(&primFull[pX], (qx / NP) & 1, abortFlag) && mbar_wait(&consFull[cX], (qx / NC) & 1, abortFlag);
         if (!ok) {
-          fail();
+          fail(G);
           break;
         }
         constexpr int oN = HK, oU = 1;
@@ -395,7 +454,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           const uint32_t se = e % NE;
           ok = mbar_wait(&epiFull[se], (e / NE) & 1, abortFlag);
           if (!ok) {
-            fail();
+            fail(G);
             break;
           }
           const double* cP = reinterpret_cast<const double*>(consBase + cR * CONS_SLOT);
@@ -456,7 +515,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
             mbar_arrive(&primEmpty[pW]);   // plane i0-4+a: read for the last time as the west plane
           }
           ++e;
-          nR += G.sI;
+          nR += sI;
           if (a == L + 1) {  // the item's last two planes' primitives, its last plane's conserved values
             if (lane == 0) {
               mbar_arrive(&consEmpty[cX]);
@@ -472,13 +531,31 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
         ownPrev = ownCur;
       }
       q += L + 2;
+      if (ENS && s == 3) {
+        // an ensemble CTA moves between members: hand this item's dt maxima, change norms and NaN flag
+        // to its member now (warp reductions, then one atomic per warp and quantity)
+        const double mx[4] = {warp_max(dta.sx), warp_max(dta.sy), warp_max(dta.sz), warp_max(dta.nu)};
+        double sm5[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) sm5[f] = warp_sum(nsum[f]);
+        const bool anyBad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) {
+          for (int qm = 0; qm < 4; ++qm) atomic_max_pos(&G.ctl->mx[qm], mx[qm]);
+          for (int f = 0; f < 5; ++f) atomicAdd(&G.normPart[f], sm5[f]);
+          if (anyBad) atomicOr(&G.ctl->nonFinite, 1);
+        }
+        dta = DtAcc{};
+#pragma unroll
+        for (int f = 0; f < 5; ++f) nsum[f] = 0;
+        bad = 0;
+      }
     }
   }
   __syncwarp();
-  if (s == 3) {
-    flush_dt(G.ctl, dta, red);
-    flush_norms(G.normPart + 5 * blockIdx.x, nsum, red);
-    if (bad) atomicOr(&G.ctl->nonFinite, 1);
+  if (!ENS && s == 3) {
+    flush_dt(G0.ctl, dta, red);
+    flush_norms(G0.normPart + 5 * blockIdx.x, nsum, red);
+    if (bad) atomicOr(&G0.ctl->nonFinite, 1);
   }
 }
 
@@ -487,20 +564,30 @@ namespace {
 struct VariantInfo {
   int tk, tj, threads, typeBoxW;
   size_t smem;
-  const void* fn;
+  const void* fn;     // single grid
+  const void* fnEns;  // ensemble
 };
 template <int TK, int TJ>
 VariantInfo variant_info() {
   using TL = ws::Tile<TK, TJ>;
-  return VariantInfo{TK, TJ, TL::NTHREADS, TL::TYW, TL::SMEM, reinterpret_cast<const void*>(&k_stage_ws<TK, TJ>)};
+  return VariantInfo{TK, TJ, TL::NTHREADS, TL::TYW, TL::SMEM, reinterpret_cast<const void*>(&k_stage_ws<TK, TJ, false>),
+                     reinterpret_cast<const void*>(&k_stage_ws<TK, TJ, true>)};
 }
 VariantInfo info(int v) { return v == STAGE_TILE_16x16 ? variant_info<16, 16>() : variant_info<32, 8>(); }
+
+template <int TK, int TJ, bool ENS>
+void launch_variant(const Grid& hg, const Grid* dGrids, const LaunchPlan& L, int s, cudaStream_t st) {
+  using TL = ws::Tile<TK, TJ>;
+  k_stage_ws<TK, TJ, ENS><<<L.stageBlocks, TL::NTHREADS, TL::SMEM, st>>>(hg, dGrids, L.items, L.ctaStart, s);
+}
 }  // namespace
 
 size_t stage_smem_bytes(int v) { return info(v).smem; }
 int stage_configure(int v) {
   const VariantInfo vi = info(v);
-  return int(cudaFuncSetAttribute(vi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vi.smem)));
+  cudaError_t e = cudaFuncSetAttribute(vi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vi.smem));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(vi.fnEns, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vi.smem));
+  return int(e);
 }
 int stage_tile_j(int v) { return info(v).tj; }
 int stage_tile_k(int v) { return info(v).tk; }
@@ -513,11 +600,13 @@ int stage_occupancy(int v) {
   return nb;
 }
 int stage_num_maps() { return ws::NMAPS; }
-// Registers per thread the kernel is launched with (the setmaxnreg split assumes ws::REG_LAUNCH).
+// Registers per thread the kernels are launched with (the setmaxnreg split assumes ws::REG_LAUNCH); the
+// smaller of the single-grid and ensemble instantiations.
 int stage_launch_registers(int v) {
-  cudaFuncAttributes fa{};
-  if (cudaFuncGetAttributes(&fa, info(v).fn) != cudaSuccess) return -1;
-  return fa.numRegs;
+  cudaFuncAttributes a{}, b{};
+  if (cudaFuncGetAttributes(&a, info(v).fn) != cudaSuccess) return -1;
+  if (cudaFuncGetAttributes(&b, info(v).fnEns) != cudaSuccess) return -1;
+  return a.numRegs < b.numRegs ? a.numRegs : b.numRegs;
 }
 bool stage_register_split_ok(int v) {
   const int r = stage_launch_registers(v);
@@ -525,13 +614,20 @@ bool stage_register_split_ok(int v) {
 }
 void launch_stage(const Grid& hg, const LaunchPlan& L, int s, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (L.tile == STAGE_TILE_16x16) {
-    using TL = ws::Tile<16, 16>;
-    k_stage_ws<16, 16><<<L.stageBlocks, TL::NTHREADS, TL::SMEM, st>>>(hg, L.items, L.nItems, s);
-  } else {
-    using TL = ws::Tile<32, 8>;
-    k_stage_ws<32, 8><<<L.stageBlocks, TL::NTHREADS, TL::SMEM, st>>>(hg, L.items, L.nItems, s);
-  }
+  if (!hg.tmaps || !hg.ctl || !L.items || !L.ctaStart) return;  // never launch on an unbuilt grid
+  if (L.tile == STAGE_TILE_16x16)
+    launch_variant<16, 16, false>(hg, nullptr, L, s, st);
+  else
+    launch_variant<32, 8, false>(hg, nullptr, L, s, st);
+}
+void launch_stage_ensemble(const Grid* dGrids, const LaunchPlan& L, int s, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!dGrids || !L.items || !L.ctaStart) return;
+  const Grid none{};
+  if (L.tile == STAGE_TILE_16x16)
+    launch_variant<16, 16, true>(none, dGrids, L, s, st);
+  else
+    launch_variant<32, 8, true>(none, dGrids, L, s, st);
 }
 
 }  // namespace nsf

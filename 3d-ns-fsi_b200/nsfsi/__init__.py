@@ -92,6 +92,16 @@ def lib():
         "nsf_march_timed": (i32, [vp, u64, dp]),
         "nsf_profile_steps": (i32, [vp, u64, dp, dp]),
         "nsf_step_metrics_noalloc": (i32, [cp, vp, vp, vp, vp, vp]),
+        "nsf_ensemble_create": (i32, [cp, u32, i32, ctypes.c_char_p, ctypes.POINTER(vp)]),
+        "nsf_ensemble_march": (i32, [vp, u64]),
+        "nsf_ensemble_march_timed": (i32, [vp, u64, dp]),
+        "nsf_ensemble_sync": (i32, [vp]),
+        "nsf_ensemble_profile_steps": (i32, [vp, u64, dp, dp]),
+        "nsf_ensemble_member": (i32, [vp, u32, ctypes.POINTER(vp)]),
+        "nsf_ensemble_info": (i32, [vp, ctypes.POINTER(i32), ctypes.POINTER(u64), ctypes.POINTER(u32)]),
+        "nsf_ensemble_last_error": (ctypes.c_char_p, [vp]),
+        "nsf_ensemble_destroy": (None, [vp]),
+        "nsf_autotune": (i32, [cp, i32, ctypes.c_char_p, ctypes.POINTER(i32), dp]),
         "nsf_last_error": (ctypes.c_char_p, [vp]),
         "nsf_destroy": (None, [vp]),
     }
@@ -246,3 +256,129 @@ class Solver:
         n = ctypes.c_uint64()
         self._check(lib().nsf_launches_per_step(self.h, ctypes.byref(n)))
         return n.value
+
+    def geometry(self):
+        """dx, dy, dz and Mesh::positionOffset x, y, z."""
+        g = np.zeros(6)
+        self._check(lib().nsf_get_geometry(self.h, _dp(g)))
+        return g
+
+
+class Member(Solver):
+    """Read-only view of one ensemble member (owned by its Ensemble: never destroyed or marched here)."""
+
+    def __init__(self, handle, cfg):
+        self.cfg = cfg
+        self.h = handle
+        self.N = int(cfg.NI * cfg.NJ * cfg.NK)
+
+    def close(self):
+        self.h = ctypes.c_void_p()
+
+
+class Ensemble:
+    """Independent grids advanced together: one CUDA graph per RK4 step for all members."""
+
+    def __init__(self, cfgs, device=0, tune_cache=None):
+        self.cfgs = [config_load(c) if isinstance(c, str) and os.path.exists(c) else
+                     (config_parse(c) if isinstance(c, str) else c) for c in cfgs]
+        arr = (Config * len(self.cfgs))(*self.cfgs)
+        self.h = ctypes.c_void_p()
+        st = lib().nsf_ensemble_create(arr, len(self.cfgs), device, tune_cache.encode() if tune_cache else None,
+                                       ctypes.byref(self.h))
+        if st:
+            msg = lib().nsf_ensemble_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise NsfError(st, msg)
+
+    def _check(self, st):
+        if st:
+            raise NsfError(st, lib().nsf_ensemble_last_error(self.h).decode())
+
+    def close(self):
+        if self.h:
+            lib().nsf_ensemble_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def march(self, nsteps):
+        self._check(lib().nsf_ensemble_march(self.h, nsteps))
+
+    def march_timed(self, nsteps):
+        ms = ctypes.c_double()
+        self._check(lib().nsf_ensemble_march_timed(self.h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        self._check(lib().nsf_ensemble_sync(self.h))
+
+    def profile_steps(self, nsteps):
+        """(mean ms of each stage launch [4], mean ms per step), kernels launched one by one."""
+        st = np.zeros(4)
+        step = ctypes.c_double()
+        self._check(lib().nsf_ensemble_profile_steps(self.h, nsteps, _dp(st), ctypes.byref(step)))
+        return st, step.value
+
+    def member(self, m):
+        h = ctypes.c_void_p()
+        self._check(lib().nsf_ensemble_member(self.h, m, ctypes.byref(h)))
+        return Member(h, self.cfgs[m])
+
+    def info(self):
+        """(tile shape, launches per step, stage work items)."""
+        tile, lps, items = ctypes.c_int32(), ctypes.c_uint64(), ctypes.c_uint32()
+        self._check(lib().nsf_ensemble_info(self.h, ctypes.byref(tile), ctypes.byref(lps), ctypes.byref(items)))
+        return tile.value, lps.value, items.value
+
+
+def autotune(cfg, device=0, cache=None):
+    """(faster tile shape: 0 = 32x8, 1 = 16x16; ns per node and stage for both)."""
+    tile = ctypes.c_int32()
+    ns = np.zeros(2)
+    st = lib().nsf_autotune(ctypes.byref(cfg), device, cache.encode() if cache else None, ctypes.byref(tile), _dp(ns))
+    if st:
+        raise NsfError(st, "autotune failed")
+    return tile.value, ns
+
+
+ENSEMBLE_SHAPES = [(32, 32, 32), (48, 48, 48), (64, 64, 64), (96, 64, 64), (128, 64, 64)]
+
+
+def ensemble_configs(n=64, seed=20240301, steps=200):
+    """The batched-ensemble workload: n single-sphere flows (inflow/outflow in x, periodic y and z) with
+    grid shapes drawn from ENSEMBLE_SHAPES, Mach from U[0.2, 0.4], Re from U[50, 300] on the diameter,
+    sphere diameter from U[0.15, 0.25] of the domain width (L_y = L_z = 1), centre at 40 % of the domain
+    length; L_x makes dx equal to dy. Freestream + seeded 1e-4 noise, `steps` RK4 steps each."""
+    rng = np.random.default_rng(seed)
+    base = config_load(case_path("sphere48"))
+    out = []
+    for m in range(n):
+        NI, NJ, NK = ENSEMBLE_SHAPES[int(rng.integers(len(ENSEMBLE_SHAPES)))]
+        mach = float(rng.uniform(0.2, 0.4))
+        re_d = float(rng.uniform(50.0, 300.0))
+        d = float(rng.uniform(0.15, 0.25))
+        c = Config()
+        ctypes.memmove(ctypes.byref(c), ctypes.byref(base), ctypes.sizeof(Config))
+        c.NI, c.NJ, c.NK = NI, NJ, NK
+        c.stop_time_level = steps
+        c.lx = float(NI - 1) / float(NJ - 2)
+        c.ly = c.lz = 1.0
+        c.m0 = mach
+        c.re = re_d / (mach * d)
+        c.machine_precision_buffer = np.finfo(np.float64).eps * (c.lx + c.ly + c.lz)
+        c.n_spheres = 1
+        c.spheres[0] = Sphere(0.4 * c.lx, 0.5, 0.5, d / 2)
+        c.seed = seed + m
+        out.append(c)
+    return out

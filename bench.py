@@ -118,6 +118,51 @@ def cpu_baseline(case_path, nodes):
             "host_cores_present": os.cpu_count()}
 
 
+TUNE_CACHE = os.path.join(ROOT, "3d-ns-fsi_b200", "tuning", "stage_tiles.jsonl")
+
+
+def ensemble_leg(steps, device, nsfsi, sequential=True):
+    """Batched ensemble (64 seeded single-sphere flows on 5 grid shapes) against the same 64 runs made one
+    after another on the plain path. Both timed on the device (CUDA events), setup excluded."""
+    cfgs = nsfsi.ensemble_configs(n=64, steps=steps)
+    nodes = [int(c.NI * c.NJ * c.NK) for c in cfgs]
+    os.makedirs(os.path.dirname(TUNE_CACHE), exist_ok=True)
+
+    def sync(x):
+        # Members whose flow becomes non-finite keep marching, as the reference does (Mesh::checkFinity
+        # prints and continues); the reference's own algorithm diverges on the same members.
+        try:
+            x.sync()
+            return 0
+        except nsfsi.NsfError as e:
+            if e.code != 3:
+                raise
+            return 1
+
+    with nsfsi.Ensemble(cfgs, device=device, tune_cache=TUNE_CACHE) as ens:
+        tile, lps, items = ens.info()
+        ens.march(3)
+        sync(ens)
+        ens_ms = ens.march_timed(steps)
+        sync(ens)
+    seq_ms = 0.0
+    nonfinite = 0
+    for c in (cfgs if sequential else []):
+        with nsfsi.Solver(c, device=device) as s:
+            s.march(3)
+            sync(s)
+            seq_ms += s.march_timed(steps)
+            nonfinite += sync(s)
+    work = sum(nodes) * steps
+    return {"workload": "64 single-sphere flows, shapes 32^3/48^3/64^3/96x64x64/128x64x64, M U[0.2,0.4], "
+                        "Re_D U[50,300], D U[0.15,0.25]", "members": len(cfgs), "nodes": sum(nodes),
+            "steps": steps, "value": work / (ens_ms / 1e3), "unit": "node-RK4-steps/s",
+            "sequential_value": work / (seq_ms / 1e3) if sequential else None,
+            "speedup_vs_sequential": seq_ms / ens_ms if sequential else None,
+            "ms": ens_ms, "sequential_ms": seq_ms if sequential else None, "tile": ["32x8", "16x16"][tile], "launches_per_step": lps,
+            "stage_work_items": items, "nonfinite_members": nonfinite}
+
+
 def run_reference_arm(args, rank, world):
     wl = WORKLOADS[args.workload]
     import nsfsi  # only for the case-file path
@@ -155,6 +200,9 @@ def main():
     ap.add_argument("--workload", default="tgv256", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--ensemble-steps", type=int, default=200, help="RK4 steps of the ensemble leg (0: skip)")
+    ap.add_argument("--ensemble-only", action="store_true", help="run only the ensemble leg (profiling)")
+    ap.add_argument("--no-seq", action="store_true", help="ensemble leg without the sequential comparison")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -178,6 +226,9 @@ def main():
         return
 
     import nsfsi
+    if args.ensemble_only:
+        print(json.dumps(ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq)), flush=True)
+        return
     wl = WORKLOADS[args.workload]
     case = nsfsi.case_path(wl["case"])
     cfg = nsfsi.config_load(case)
@@ -255,6 +306,8 @@ def main():
                          "algorithmic_bytes_per_node_step": BYTES_PER_NODE_STEP, "peak_kind": peak_kind,
                          "frac_of_8000": achieved / 8000.0},
         }
+        if args.ensemble_steps > 0 and args.workload == "tgv256":
+            line["ensemble"] = ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq)
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(case, nodes)

@@ -175,6 +175,38 @@ nsf_status nsf_launches_per_step(nsf_solver* s, uint64_t* launches);
 nsf_status nsf_step_metrics_noalloc(const nsf_config* cfg, const double* d_old, const double* d_new,
                                     const uint8_t* d_types, double* d_out, void* stream);
 
+/* ---------------------------------------------------------------------------------------------------
+ * Ensembles: n independent grids (each member its own case: grid shape, Mach, Re, bodies) advanced
+ * together -- ONE CUDA graph per RK4 step for all members, each of the four stage launches a single
+ * persistent kernel over the union of the members' work items. No counterpart in the reference; every
+ * member advances exactly as Solver::marchTimeStep (Solver.cpp:130-167) advances its own grid.
+ * tune_cache: NULL (default 32 x 8 tiles), or a file of autotuner results (created/extended as needed)
+ * from which the stage-kernel tile shape is chosen; shapes not yet in it are timed on the device first.
+ * Results: nsf_ensemble_member returns member m's handle (valid until nsf_ensemble_destroy; do not
+ * destroy or march it) after waiting for the queued ensemble steps, for nsf_get_time / nsf_download / ... */
+typedef struct nsf_ensemble nsf_ensemble;
+nsf_status nsf_ensemble_create(const nsf_config* cfgs, uint32_t n, int32_t device, const char* tune_cache,
+                               nsf_ensemble** out);
+nsf_status nsf_ensemble_march(nsf_ensemble* e, uint64_t nsteps);
+nsf_status nsf_ensemble_march_timed(nsf_ensemble* e, uint64_t nsteps, double* elapsed_ms);
+/* nsteps steps launched one kernel at a time with events around the four stage launches: mean stage-kernel
+ * times (stage_ms[4]) and mean step time. Advances every member. */
+nsf_status nsf_ensemble_profile_steps(nsf_ensemble* e, uint64_t nsteps, double* stage_ms, double* step_ms);
+/* Wait; NSF_ERR_NONFINITE / NSF_ERR_TIMEOUT if any member saw one. */
+nsf_status nsf_ensemble_sync(nsf_ensemble* e);
+nsf_status nsf_ensemble_member(nsf_ensemble* e, uint32_t m, nsf_solver** member);
+/* Chosen tile shape (0: 32 x 8, 1: 16 x 16), kernel launches per step, stage work items. */
+nsf_status nsf_ensemble_info(nsf_ensemble* e, int32_t* tile, uint64_t* launches_per_step, uint32_t* work_items);
+const char* nsf_ensemble_last_error(nsf_ensemble* e);
+void nsf_ensemble_destroy(nsf_ensemble* e);
+
+/* Stage-kernel autotuner: times the stage kernels of this configuration's grid for each tile shape
+ * (32 x 8 and 16 x 16 columns) on `device`, caches the result per device and grid shape in cache_path
+ * (JSON lines; NULL: no cache) and returns the faster shape and the mean time per node and stage in
+ * nanoseconds for both (ns_per_node[2]). A cached shape is not timed again. */
+nsf_status nsf_autotune(const nsf_config* cfg, int32_t device, const char* cache_path, int32_t* tile,
+                        double* ns_per_node);
+
 /* Text of the last error on this handle (static storage owned by the handle). */
 const char* nsf_last_error(nsf_solver* s);
 

@@ -60,3 +60,20 @@ def test_body_too_close_to_face_is_rejected():
     with pytest.raises(nsfsi.NsfError) as e:
         Solver(txt, device=-1)
     assert e.value.code == 4
+
+
+def test_ensemble_workload_members_are_valid_cases():
+    """The 64 seeded ensemble members (5 grid shapes, Mach, Re, sphere size) all pass the host setup."""
+    cfgs = nsfsi.ensemble_configs()
+    shapes = set()
+    for c in cfgs:
+        s = Solver(c, device=-1)
+        assert len(s.bodies()) == 1 and len(s.bodies()[0][0]) > 0
+        shapes.add((c.NI, c.NJ, c.NK))
+        s.close()
+    assert len(cfgs) == 64 and shapes == set(nsfsi.ENSEMBLE_SHAPES)
+
+
+def test_ensemble_needs_a_device():
+    with pytest.raises(nsfsi.NsfError):
+        nsfsi.Ensemble(nsfsi.ensemble_configs(n=2))

@@ -231,7 +231,7 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
   if ((st = ens_alloc(e, &L.ctaStart, start.size())) != NSF_OK) return st;
   CKE(cudaMemcpy(L.ctaStart, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
   // small kernels: block counts = maxima over the members
-  L.gfBlocks = 4 * e->nSM;
+  L.gfBlocks = std::max(8, 4 * e->nSM / M);  // grid-stride over each member's nodes
   for (nsf_solver* s : e->members) {
     const LaunchPlan& P = s->plan;
     for (int a = 0; a < 3; ++a)

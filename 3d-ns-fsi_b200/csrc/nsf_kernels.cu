@@ -168,7 +168,17 @@ __global__ void k_edge_bc(const Grid* __restrict__ grids, int s, int axis) {
     }
   DtAcc dta;
   int bad = 0;
-  if (e >= 0) {
+  // blocks outside this member's edge box (ensembles launch the largest member's grid) leave at once;
+  // the test is uniform over the block, so no thread of it reaches the block reductions below
+  if (e < 0) return;
+  {
+    const int* b = G.eBox[e];
+    const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
+    if (b[2 * ax1] + int(blockIdx.y * blockDim.y) > b[2 * ax1 + 1] ||
+        b[2 * ax2] + int(blockIdx.x * blockDim.x) > b[2 * ax2 + 1])
+      return;
+  }
+  {
     const int* b = G.eBox[e];
     // in-plane coordinates: (a, bb) = the two axes other than `axis`, in (i, j, k) order
     const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
@@ -286,6 +296,8 @@ __global__ void k_body_filter(const Grid* __restrict__ grids, int s) {
   DtAcc dta;
   double nsum[5] = {0, 0, 0, 0, 0};
   int bad = 0;
+  // a block past this member's filter nodes never writes its norm slot, which stays zero
+  if (int(blockIdx.x * blockDim.x) >= G.nFilter) return;
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < G.nFilter; f += gridDim.x * blockDim.x) {
     const long long n = G.fnode[f];
     const double* r = O[0];
@@ -328,6 +340,7 @@ __global__ void k_ghost(const Grid* __restrict__ grids, int s) {
   DtAcc dta;
   int bad = 0;
   const int total = G.nGhost + G.nFilter + (s == 3 ? G.nInactive : 0);
+  if (int(blockIdx.x * blockDim.x) >= total) return;  // the whole block is past this member's work
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
     if (q < G.nGhost) {
       const long long* cell = G.gcell + 8 * (long long)q;

@@ -1,0 +1,487 @@
+// Discrete adjoint driver (C ABI: nsf_adj_configure / nsf_adj_forward / nsf_adj_backward / nsf_adj_get_dt).
+//
+// Objective: J = (1/n_avg) sum over the last n_avg steps of F_x(U_n), the x-force of the pressure on the
+// immersed bodies, F_x = -dA sum_g p(U_g) n_x(g) over the ghost nodes g (p from the ghost's conserved
+// values, which equal the image point's pressure; n = unit normal of the body at the ghost's body-intercept
+// point; dA = (dx dy dz)^(2/3)). Parameters: the conserved field at level 0 (every node) and a factor per
+// (j, k) node of the x-inlet's velocity profile (the inlet velocity is min(1, t/10) M0 times the factor;
+// 1 everywhere is the reference's uniform inflow). The dt sequence of the first forward run is frozen
+// and used by every later run (forward, recomputation and finite-difference checks alike).
+//
+// Backward: binomial checkpointing over the steps (Griewank's schedule: with c free snapshots the longest
+// reversible run in t sweeps is C(c+t, t)); a step whose adjoint is due is recomputed kernel by kernel
+// from its snapshot, keeping each stage's inputs, and the adjoint kernels (nsf_adjoint.cu) then run in
+// reverse kernel order on adjoint arrays that mirror the physical field buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "nsf_adjoint.h"
+#include "nsf_device.cuh"
+#include "nsf_internal.h"
+#include "nsf_solver_impl.h"
+
+using namespace nsf;
+
+struct AdjCtx {
+  int nsteps = 0, navg = 50, nsnap = 20;
+  bool haveDt = false, haveForward = false;
+  std::vector<double> dts;
+  double* dDt = nullptr;
+  double* dInflow = nullptr;
+  double* dU0 = nullptr;  // 5 x Nd: the forward run's level-0 state
+  double* dNx = nullptr;
+  double dA = 0;
+  double* dAcc = nullptr;
+  long long* cnode = nullptr;
+  int* coff = nullptr;
+  int* cent = nullptr;
+  int ncell = 0;
+  long long* fsNodes = nullptr;
+  int nfs = 0;
+  bool inletX = false;
+  double* lam = nullptr;  // 20 x Nd: adjoint of bufs[b][f] at (5 b + f) Nd, accumulator at (15 + f) Nd
+  double* lamFpre = nullptr;
+  double* lamFnew = nullptr;
+  double* lamInflow = nullptr;
+  double* tmpLam = nullptr;
+  double* tmpV = nullptr;
+  double* ipbar = nullptr;
+  double* fbar = nullptr;
+  std::vector<double*> slot;
+  std::vector<StepCtl*> slotCtl;
+  double* stageSnap = nullptr;  // 4 x (11 Nd + 2F): I (5), R (1), O before the edge conditions (5), fpre
+  StepCtl roles{};
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+nsf_status fail(nsf_solver* s, nsf_status st, const std::string& msg) {
+  s->err = msg;
+  return st;
+}
+
+#define CKA(call)                                                                  \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+nsf_status aalloc(nsf_solver* s, AdjCtx* a, T** p, size_t count) {
+  void* q = nullptr;
+  CKA(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)));
+  a->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return NSF_OK;
+}
+
+size_t nd(const nsf_solver* s) { return size_t(s->hGrid.N); }
+size_t nf(const nsf_solver* s) { return size_t(s->hGrid.nFilter); }
+size_t per_stage(const nsf_solver* s) { return 11 * nd(s) + 2 * nf(s); }
+
+int phys(const nsf_solver* s, const double* p, int f) {
+  for (int b = 0; b < 3; ++b)
+    if (s->hGrid.bufs[b][f] == p) return b;
+  return 0;
+}
+
+double* lamOf(const nsf_solver* s, const AdjCtx* a, int b, int f) { return a->lam + (size_t(b) * 5 + f) * nd(s); }
+
+nsf_status push_grid(nsf_solver* s) {
+  CKA(cudaMemcpy(s->dGrid, &s->hGrid, sizeof(Grid), cudaMemcpyHostToDevice));
+  return NSF_OK;
+}
+
+nsf_status setup(nsf_solver* s) {
+  if (s->adj) return NSF_OK;
+  if (!s->initialized || s->hostOnly) return fail(s, NSF_ERR_STATE, "the adjoint needs an initialized device solver");
+  const nsf_config& c = s->cfg;
+  if (c.stop_criterion != 0) return fail(s, NSF_ERR_ARG, "the adjoint needs stopCriterion = \"timesteps\"");
+  const HostSetup& S = s->setup;
+  for (const auto& e : S.edges) {
+    const bool ok = e.bc == NSF_BC_PERIODIC || (e.axis == 0 && (e.bc == NSF_BC_INLET || e.bc == NSF_BC_OUTLET));
+    if (!ok) return fail(s, NSF_ERR_ARG, "the adjoint supports periodic faces and x-inlet/x-outlet faces only");
+  }
+  if (S.NI < 6 || S.NJ < 4 || S.NK < 4) return fail(s, NSF_ERR_ARG, "grid too small for the adjoint");
+  auto* a = new AdjCtx;
+  s->adj = a;
+  a->nsteps = int(c.stop_time_level);
+  const Grid& G = s->hGrid;
+  const size_t N = nd(s), F = nf(s), NG = size_t(G.nGhost), plane = size_t(G.NJ) * G.NKp;
+  nsf_status st;
+  for (const auto& e : S.edges) a->inletX |= e.axis == 0 && e.bc == NSF_BC_INLET;
+  if ((st = aalloc(s, a, &a->dDt, size_t(a->nsteps) + 1)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->dInflow, plane)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->dU0, 5 * N)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->dAcc, 1)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->lam, 20 * N)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->lamFpre, 2 * F)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->lamFnew, 2 * F)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->lamInflow, plane)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->tmpLam, 5 * N)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->tmpV, 11 * N)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->ipbar, 5 * NG)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->fbar, 2 * plane)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->stageSnap, 4 * per_stage(s))) != NSF_OK) return st;
+  // objective: body normals at the ghosts' body-intercept points (gnode order), area weight
+  std::vector<double> nx;
+  for (const auto& b : S.bodies)
+    for (const auto& g : b.ghosts) {
+      double d[3] = {g.bi[0] - b.c[0], g.bi[1] - b.c[1], g.bi[2] - b.c[2]};
+      if (!b.sphere) d[b.axis] = 0;
+      const double len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      nx.push_back(len > 0 ? d[0] / len : 0.0);
+    }
+  a->dA = std::pow(S.d[0] * S.d[1] * S.d[2], 2.0 / 3.0);
+  if ((st = aalloc(s, a, &a->dNx, nx.size())) != NSF_OK) return st;
+  if (!nx.empty()) CKA(cudaMemcpy(a->dNx, nx.data(), nx.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // reverse map of the image-point cells: node -> (ghost, corner) entries with non-zero weights
+  std::vector<long long> gcell(8 * NG);
+  std::vector<uint8_t> type(N);
+  if (NG) CKA(cudaMemcpy(gcell.data(), G.gcell, gcell.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+  CKA(cudaMemcpy(type.data(), G.type, N, cudaMemcpyDeviceToHost));
+  std::map<long long, std::vector<int>> byNode;
+  for (size_t q = 0; q < NG; ++q)
+    for (int m = 0; m < 8; ++m) {
+      const long long n = gcell[8 * q + m];
+      if ((type[n] & TYPE_MASK) == SOLID_GHOST) continue;  // a body-intercept row: zero weight
+      byNode[n].push_back(int(8 * q + m));
+    }
+  std::vector<long long> cn;
+  std::vector<int> co(1, 0), ce;
+  for (auto& kv : byNode) {
+    cn.push_back(kv.first);
+    ce.insert(ce.end(), kv.second.begin(), kv.second.end());
+    co.push_back(int(ce.size()));
+  }
+  a->ncell = int(cn.size());
+  if ((st = aalloc(s, a, &a->cnode, cn.size())) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->coff, co.size())) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->cent, ce.size())) != NSF_OK) return st;
+  if (!cn.empty()) {
+    CKA(cudaMemcpy(a->cnode, cn.data(), cn.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    CKA(cudaMemcpy(a->cent, ce.data(), ce.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  CKA(cudaMemcpy(a->coff, co.data(), co.size() * sizeof(int), cudaMemcpyHostToDevice));
+  // nodes of the near-body filter stencils
+  std::vector<long long> fnode(F);
+  if (F) CKA(cudaMemcpy(fnode.data(), G.fnode, F * sizeof(long long), cudaMemcpyDeviceToHost));
+  std::set<long long> fs;
+  for (long long n : fnode)
+    for (long long o : {0LL, G.sI, -G.sI, G.sJ, -G.sJ, 1LL, -1LL}) fs.insert(n + o);
+  std::vector<long long> fsv(fs.begin(), fs.end());
+  a->nfs = int(fsv.size());
+  if ((st = aalloc(s, a, &a->fsNodes, fsv.size())) != NSF_OK) return st;
+  if (!fsv.empty()) CKA(cudaMemcpy(a->fsNodes, fsv.data(), fsv.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  // inflow profile factor 1; the initial condition of the case as the default level-0 state
+  std::vector<double> ones(plane, 1.0);
+  CKA(cudaMemcpy(a->dInflow, ones.data(), plane * sizeof(double), cudaMemcpyHostToDevice));
+  std::vector<double> cons, prim;
+  initial_condition(c, S, cons, prim);
+  const size_t hp = S.NK * sizeof(double), dp = size_t(G.NKp) * sizeof(double);
+  CKA(cudaMemset(a->dU0, 0, 5 * N * sizeof(double)));
+  for (int f = 0; f < 5; ++f)
+    CKA(cudaMemcpy2D(a->dU0 + f * N, dp, cons.data() + f * S.N, hp, hp, S.NI * S.NJ, cudaMemcpyHostToDevice));
+  s->hGrid.inflow = a->dInflow;
+  return push_grid(s);
+}
+
+nsf_status alloc_slots(nsf_solver* s, AdjCtx* a) {
+  const size_t words = 15 * nd(s) + 2 * nf(s);
+  while (int(a->slot.size()) < a->nsnap + 1) {
+    double* p;
+    StepCtl* c;
+    nsf_status st;
+    if ((st = aalloc(s, a, &p, words)) != NSF_OK) return st;
+    if ((st = aalloc(s, a, &c, 1)) != NSF_OK) return st;
+    a->slot.push_back(p);
+    a->slotCtl.push_back(c);
+  }
+  return NSF_OK;
+}
+
+// Level-0 state: bufs[0] = U0, the other buffers zero (the reference's zero-initialised second buffer),
+// fpre from U0, the control block of initialisation (dt of step 0 from the frozen sequence, if any).
+nsf_status reset(nsf_solver* s, AdjCtx* a) {
+  const size_t N = nd(s);
+  Grid& G = s->hGrid;
+  CKA(cudaMemcpyAsync(G.bufs[0][0], a->dU0, 5 * N * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  CKA(cudaMemsetAsync(G.bufs[1][0], 0, 15 * N * sizeof(double), s->stream));  // buffers 1, 2 and the accumulator
+  launch_fpre_init(s->dGrid, G.nFilter, G.bufs[0][0], G.bufs[0][4], s->nSM, s->stream);
+  StepCtl c = s->ctlInit;
+  if (a->haveDt) c.dt = a->dts[0];
+  CKA(cudaMemcpyAsync(s->dCtl, &c, sizeof c, cudaMemcpyHostToDevice, s->stream));
+  CKA(cudaStreamSynchronize(s->stream));
+  return NSF_OK;
+}
+
+nsf_status save(nsf_solver* s, AdjCtx* a, int k) {
+  const size_t N = nd(s), F = nf(s);
+  CKA(cudaMemcpyAsync(a->slot[k], s->hGrid.bufs[0][0], 15 * N * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  if (F)
+    CKA(cudaMemcpyAsync(a->slot[k] + 15 * N, s->hGrid.fpre, 2 * F * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  CKA(cudaMemcpyAsync(a->slotCtl[k], s->dCtl, sizeof(StepCtl), cudaMemcpyDeviceToDevice, s->stream));
+  return NSF_OK;
+}
+
+nsf_status restore(nsf_solver* s, AdjCtx* a, int k) {
+  const size_t N = nd(s), F = nf(s);
+  CKA(cudaMemcpyAsync(s->hGrid.bufs[0][0], a->slot[k], 15 * N * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  if (F)
+    CKA(cudaMemcpyAsync(s->hGrid.fpre, a->slot[k] + 15 * N, 2 * F * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  CKA(cudaMemcpyAsync(s->dCtl, a->slotCtl[k], sizeof(StepCtl), cudaMemcpyDeviceToDevice, s->stream));
+  return NSF_OK;
+}
+
+nsf_status advance(nsf_solver* s, int n) {
+  for (int q = 0; q < n; ++q) CKA(cudaGraphLaunch(s->graphExec, s->stream));
+  return NSF_OK;
+}
+
+// Keeps the roles of the step and, per stage, the values its nonlinear adjoints need.
+struct SnapHook : StepHook {
+  nsf_solver* s;
+  AdjCtx* a;
+  cudaError_t err = cudaSuccess;
+  SnapHook(nsf_solver* s_, AdjCtx* a_) : s(s_), a(a_) {}
+  void copy(double* dst, const double* src, size_t words) {
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(dst, src, words * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
+  }
+  void after_prologue() override {
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s->stream);
+    if (err == cudaSuccess) err = cudaMemcpy(&a->roles, s->dCtl, sizeof(StepCtl), cudaMemcpyDeviceToHost);
+  }
+  void before_stage(int q) override {
+    const size_t N = nd(s);
+    double* base = a->stageSnap + q * per_stage(s);
+    for (int f = 0; f < 5; ++f) copy(base + f * N, a->roles.I[q][f], N);
+    copy(base + 5 * N, a->roles.R[q], N);
+    if (nf(s)) copy(base + 11 * N, s->hGrid.fpre, 2 * nf(s));
+  }
+  void before_edges(int q) override {
+    const size_t N = nd(s);
+    double* base = a->stageSnap + q * per_stage(s);
+    for (int f = 0; f < 5; ++f) copy(base + (6 + f) * N, a->roles.O[q][f], N);
+  }
+};
+
+// The adjoint of step k: the working state holds U_k on entry (U_{k+1} on exit); the adjoint arrays hold
+// the adjoint of U_{k+1} on entry and of U_k on exit.
+nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
+  SnapHook hook(s, a);
+  enqueue_step_hooked(s->dGrid, s->hGrid, s->plan, s->stream, &hook);
+  if (hook.err != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint recomputation: ") + cudaGetErrorString(hook.err));
+  CKA(cudaGetLastError());
+  const StepCtl& R = a->roles;
+  const Grid& G = s->hGrid;
+  const size_t N = nd(s);
+  const int nSM = s->nSM;
+  cudaStream_t st = s->stream;
+  if (k + 1 > a->nsteps - a->navg) {  // F_x of U_{k+1} enters J
+    AdjPtrs A{};
+    for (int f = 0; f < 5; ++f) {
+      A.val[f] = R.O[3][f];
+      A.lamO[f] = lamOf(s, a, phys(s, R.O[3][f], f), f);
+    }
+    launch_adj_objective(s->dGrid, A, G.nGhost, a->dNx, a->dA, 1.0 / a->navg, nSM, st);
+  }
+  for (int q = 3; q >= 0; --q) {
+    const double* snap = a->stageSnap + q * per_stage(s);
+    AdjPtrs A{};
+    for (int f = 0; f < 5; ++f) {
+      A.lamO[f] = lamOf(s, a, phys(s, R.O[q][f], f), f);
+      A.lamI[f] = lamOf(s, a, phys(s, R.I[q][f], f), f);
+      A.lamU0[f] = lamOf(s, a, phys(s, R.U0[f], f), f);
+      A.lamAcc[f] = a->lam + (15 + size_t(f)) * N;
+    }
+    A.lamR = lamOf(s, a, phys(s, R.R[q], 0), 0);
+    A.lamFpre = a->lamFpre;
+    A.lamFnew = a->lamFnew;
+    // near-body filter and ghosts
+    launch_adj_ghost(s->dGrid, A, G.nGhost, G.nFilter, a->ipbar, a->cnode, a->coff, a->cent, a->ncell, nSM, st);
+    launch_adj_filter(s->dGrid, A, a->fsNodes, a->nfs, G.nFilter, nSM, st);
+    // edge conditions: z, y, then x (reads the stage output before the edge conditions)
+    for (int f = 0; f < 5; ++f) A.val[f] = snap + (6 + f) * N;
+    for (int axis = 2; axis >= 0; --axis)
+      launch_adj_edge(s->dGrid, A, s->plan, axis, R.stageT[q], a->fbar, a->lamInflow, a->inletX, st);
+    launch_adj_solid(s->dGrid, A, G.nSolid, R.copyMask[q], nSM, st);
+    // stage kernel: RK4 combine, transposed RHS, primitives of the stage input
+    for (int f = 0; f < 5; ++f) A.val[f] = snap + f * N;
+    A.valR = snap + 5 * N;
+    A.valFpre = snap + 11 * N;
+    const double inc = q == 2 ? R.dtUsed : R.dtUsed / 2;
+    launch_adj_stage(s->dGrid, A, (long long)N, q, inc, R.dtUsed / 6, a->tmpLam, a->tmpV, nSM, st);
+  }
+  if (R.filterNow) {
+    double* dst = lamOf(s, a, phys(s, R.gfDst, 0), 0);
+    double* src = lamOf(s, a, phys(s, R.gfSrc, 0), 0);
+    launch_adj_density_filter(s->dGrid, (long long)N, dst, dst, src, nSM, st);
+  }
+  CKA(cudaGetLastError());
+  return NSF_OK;
+}
+
+double binom(int n, int k) {
+  double r = 1;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+
+// Reverse steps [a0, b) with c free snapshot slots above `depth`; slot `depth` holds the state at a0.
+nsf_status reverse(nsf_solver* s, AdjCtx* a, int a0, int b, int c, int depth) {
+  nsf_status st;
+  if (b - a0 == 1) {
+    if ((st = restore(s, a, depth)) != NSF_OK) return st;
+    return adjoint_step(s, a, a0);
+  }
+  if (c == 0) {
+    for (int k = b - 1; k >= a0; --k) {
+      if ((st = restore(s, a, depth)) != NSF_OK) return st;
+      if ((st = advance(s, k - a0)) != NSF_OK) return st;
+      if ((st = adjoint_step(s, a, k)) != NSF_OK) return st;
+    }
+    return NSF_OK;
+  }
+  const int n = b - a0;
+  int t = 0;
+  while (binom(c + t, t) < n) ++t;
+  const int right = int(std::min<double>(binom(c - 1 + t, t), n - 1));
+  const int m = a0 + std::max(1, n - right);
+  if ((st = restore(s, a, depth)) != NSF_OK) return st;
+  if ((st = advance(s, m - a0)) != NSF_OK) return st;
+  if ((st = save(s, a, depth + 1)) != NSF_OK) return st;
+  if ((st = reverse(s, a, m, b, c - 1, depth + 1)) != NSF_OK) return st;
+  return reverse(s, a, a0, m, c, depth);
+}
+
+}  // namespace
+
+void nsf_adjoint_free(nsf_solver* s) {
+  if (!s || !s->adj) return;
+  for (void* p : s->adj->allocs) cudaFree(p);
+  delete s->adj;
+  s->adj = nullptr;
+}
+
+extern "C" {
+
+nsf_status nsf_adj_configure(nsf_solver* s, uint32_t avg_last_steps, uint32_t snapshots) {
+  if (!s) return NSF_ERR_ARG;
+  nsf_status st = setup(s);
+  if (st != NSF_OK) return st;
+  AdjCtx* a = s->adj;
+  if (avg_last_steps == 0 || int(avg_last_steps) > a->nsteps || snapshots == 0 || snapshots > 4096)
+    return fail(s, NSF_ERR_ARG, "nsf_adj_configure: 1 <= avg_last_steps <= steps and 1 <= snapshots <= 4096");
+  a->navg = int(avg_last_steps);
+  a->nsnap = int(snapshots);
+  return NSF_OK;
+}
+
+nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow, double* J) {
+  if (!s || !J) return NSF_ERR_ARG;
+  nsf_status st = setup(s);
+  if (st != NSF_OK) return st;
+  AdjCtx* a = s->adj;
+  a->navg = std::min(a->navg, a->nsteps);
+  if ((st = alloc_slots(s, a)) != NSF_OK) return st;
+  const HostSetup& S = s->setup;
+  Grid& G = s->hGrid;
+  const size_t N = nd(s), hp = S.NK * sizeof(double), dp = size_t(G.NKp) * sizeof(double);
+  CKA(cudaSetDevice(s->device));
+  CKA(cudaStreamSynchronize(s->stream));
+  if (u0) {
+    CKA(cudaMemset(a->dU0, 0, 5 * N * sizeof(double)));
+    for (int f = 0; f < 5; ++f)
+      CKA(cudaMemcpy2D(a->dU0 + f * N, dp, u0 + f * S.N, hp, hp, S.NI * S.NJ, cudaMemcpyHostToDevice));
+  }
+  if (inflow) {
+    CKA(cudaMemcpy2D(a->dInflow, dp, inflow, hp, hp, S.NJ, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<double> ones(size_t(G.NJ) * G.NKp, 1.0);
+    CKA(cudaMemcpy(a->dInflow, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  G.inflow = a->dInflow;
+  G.dtFrozen = a->haveDt ? a->dDt : nullptr;
+  G.nDtFrozen = a->haveDt ? a->nsteps : 0;
+  if ((st = push_grid(s)) != NSF_OK) return st;
+  if ((st = reset(s, a)) != NSF_OK) return st;
+  if ((st = save(s, a, 0)) != NSF_OK) return st;
+  CKA(cudaMemsetAsync(a->dAcc, 0, sizeof(double), s->stream));
+  for (int n = 0; n < a->nsteps; ++n) {
+    CKA(cudaGraphLaunch(s->graphExec, s->stream));
+    if (n + 1 > a->nsteps - a->navg) launch_objective(s->dGrid, a->dNx, a->dA, 1.0 / a->navg, a->dAcc, s->stream);
+  }
+  CKA(cudaGetLastError());
+  if ((st = nsf_sync(s)) != NSF_OK) return st;
+  CKA(cudaMemcpy(J, a->dAcc, sizeof(double), cudaMemcpyDeviceToHost));
+  if (!a->haveDt) {  // freeze the dt sequence of this run
+    std::vector<double> rows(7 * size_t(a->nsteps));
+    uint64_t avail = 0;
+    if ((st = nsf_get_history(s, 0, uint64_t(a->nsteps), rows.data(), &avail)) != NSF_OK) return st;
+    a->dts.resize(a->nsteps);
+    for (int n = 0; n < a->nsteps; ++n) a->dts[n] = rows[7 * size_t(n) + 1];
+    CKA(cudaMemcpy(a->dDt, a->dts.data(), a->nsteps * sizeof(double), cudaMemcpyHostToDevice));
+    a->haveDt = true;
+    G.dtFrozen = a->dDt;
+    G.nDtFrozen = a->nsteps;
+    if ((st = push_grid(s)) != NSF_OK) return st;
+  }
+  a->haveForward = true;
+  return NSF_OK;
+}
+
+nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* g_u0) {
+  if (!s) return NSF_ERR_ARG;
+  AdjCtx* a = s->adj;
+  if (!a || !a->haveForward) return fail(s, NSF_ERR_STATE, "nsf_adj_backward needs a preceding nsf_adj_forward");
+  const HostSetup& S = s->setup;
+  const Grid& G = s->hGrid;
+  const size_t N = nd(s), F = nf(s), plane = size_t(G.NJ) * G.NKp;
+  CKA(cudaSetDevice(s->device));
+  CKA(cudaMemsetAsync(a->lam, 0, 20 * N * sizeof(double), s->stream));
+  if (F) {
+    CKA(cudaMemsetAsync(a->lamFpre, 0, 2 * F * sizeof(double), s->stream));
+    CKA(cudaMemsetAsync(a->lamFnew, 0, 2 * F * sizeof(double), s->stream));
+  }
+  CKA(cudaMemsetAsync(a->lamInflow, 0, plane * sizeof(double), s->stream));
+  CKA(cudaMemsetAsync(a->fbar, 0, 2 * plane * sizeof(double), s->stream));
+  nsf_status st = reverse(s, a, 0, a->nsteps, a->nsnap, 0);
+  if (st != NSF_OK) return st;
+  // level-0 fpre was copied from U0
+  launch_fpre_init_adj(s->dGrid, G.nFilter, a->lamFpre, lamOf(s, a, 0, 0), lamOf(s, a, 0, 4), s->nSM, s->stream);
+  CKA(cudaStreamSynchronize(s->stream));
+  StepCtl ctl;
+  CKA(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  if (ctl.timeout) return fail(s, NSF_ERR_TIMEOUT, "a bounded wait in the stage kernel gave up during the adjoint");
+  const size_t hp = S.NK * sizeof(double), dp = size_t(G.NKp) * sizeof(double);
+  if (g_u0) {
+    for (int f = 0; f < 5; ++f)
+      CKA(cudaMemcpy2D(g_u0 + f * S.N, hp, lamOf(s, a, 0, f), dp, hp, S.NI * S.NJ, cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < 5 * S.N; ++q) g_u0[q] *= dJ;
+  }
+  if (g_inflow) {
+    CKA(cudaMemcpy2D(g_inflow, hp, a->lamInflow, dp, hp, S.NJ, cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < S.NJ * S.NK; ++q) g_inflow[q] *= dJ;
+  }
+  return NSF_OK;
+}
+
+nsf_status nsf_adj_get_dt(nsf_solver* s, double* dts, uint64_t* count) {
+  if (!s || !count) return NSF_ERR_ARG;
+  AdjCtx* a = s->adj;
+  if (!a || !a->haveDt) return fail(s, NSF_ERR_STATE, "no frozen dt sequence yet (run nsf_adj_forward first)");
+  *count = uint64_t(a->nsteps);
+  if (dts) std::memcpy(dts, a->dts.data(), a->nsteps * sizeof(double));
+  return NSF_OK;
+}
+
+}  // extern "C"

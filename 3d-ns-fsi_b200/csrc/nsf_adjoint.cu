@@ -1,0 +1,519 @@
+// Discrete adjoint of the RK4 time step: one kernel per forward kernel, in gather form.
+//
+// The forward step (nsf_kernels.cu, nsf_stage_ws.cu) is a sequence of kernels that read and write the
+// physical field buffers (three per conserved field, the RK4 accumulator, the near-body filter's pre- and
+// post-filter values). The adjoint keeps one adjoint array per physical buffer and runs the transpose of
+// every kernel in reverse order: a kernel that overwrites values consumes (zeroes) their adjoints and adds
+// its Jacobian-transposed contributions to the adjoints of the values it read. Because the adjoint state
+// mirrors the physical buffers, the reference's stale-buffer semantics (values that persist across the
+// buffer swaps, primitives of filter nodes taken before the near-body filter) are differentiated exactly
+// as the forward path reproduces them. Every kernel writes only adjoints of its own nodes (gathers over
+// precomputed reverse maps where the forward kernel scatters): no atomics, deterministic results.
+//
+// The dt sequence is frozen (the gradient does not differentiate the CFL limit), as the gradient checks
+// against finite differences and the dual-number oracle do.
+#include <cuda_runtime.h>
+
+#include "nsf_adjoint.h"
+#include "nsf_device.cuh"
+#include "nsf_internal.h"
+#include "nsf_physics.cuh"
+#include "nsf_rhs_adjoint.cuh"
+
+namespace nsf {
+namespace {
+
+__device__ __forceinline__ void ijk_of(const Grid& G, long long n, int& i, int& j, int& k) {
+  i = int(n / G.sI);
+  const long long r = n - (long long)i * G.sI;
+  j = int(r / G.sJ);
+  k = int(r - (long long)j * G.sJ);
+}
+
+// Pressure of conserved values (prims_of's p).
+__device__ __forceinline__ double pressure(const Consts& C, const double u[5], double g[5]) {
+  const double r1 = 1.0 / (u[0] + 1.0);
+  const double vx = u[1] * r1, vy = u[2] * r1, vz = u[3] * r1;
+  const double K = 0.5 * (vx * vx + vy * vy + vz * vz);
+  if (g) {  // gradient of p with respect to the five conserved values
+    g[0] = C.gm1 * K;
+    g[1] = -C.gm1 * vx;
+    g[2] = -C.gm1 * vy;
+    g[3] = -C.gm1 * vz;
+    g[4] = C.gm1;
+  }
+  return C.gm1 * (u[4] - (u[0] + 1.0) * K);
+}
+
+// --------------------------------------------------------------------------------------- objective
+// F_x = -dA * sum_g p(U_g) n_x(g) over the ghost nodes of the current state (the buffers the step just
+// finished in, StepCtl::perm[f][0]); one block, fixed summation order.
+__global__ void k_objective(const Grid* __restrict__ gp, const double* __restrict__ nx, double dA, double weight,
+                            double* acc) {
+  __shared__ double red[32];
+  const Grid& G = *gp;
+  const StepCtl* c = G.ctl;
+  double s = 0;
+  for (int q = threadIdx.x; q < G.nGhost; q += blockDim.x) {
+    const long long n = G.gnode[q];
+    double u[5];
+    for (int f = 0; f < 5; ++f) u[f] = G.bufs[c->perm[f][0]][f][n];
+    s += -dA * nx[q] * pressure(G.C, u, nullptr);
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[w];
+    *acc += weight * t;
+  }
+}
+
+__global__ void k_adj_objective(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ nx, double dA,
+                                double weight) {
+  const Grid& G = *gp;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < G.nGhost; q += gridDim.x * blockDim.x) {
+    const long long n = G.gnode[q];
+    double u[5], g[5];
+    for (int f = 0; f < 5; ++f) u[f] = A.val[f][n];
+    pressure(G.C, u, g);
+    for (int f = 0; f < 5; ++f) A.lamO[f][n] += weight * (-dA * nx[q]) * g[f];
+  }
+}
+
+// ------------------------------------------------------------------------------------------- ghosts
+// k_ghost writes the ghost values (weights x cell values, momenta negated) and writes the filtered
+// values back to the filter nodes. Phase 1: consume the adjoints of everything k_ghost wrote.
+__global__ void k_adj_ghost_consume(const Grid* __restrict__ gp, AdjPtrs A, double* __restrict__ ipbar) {
+  const Grid& G = *gp;
+  const int total = G.nGhost + G.nFilter;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+    if (q < G.nGhost) {
+      const long long n = G.gnode[q];
+      const double sgn[5] = {1, -1, -1, -1, 1};
+      for (int f = 0; f < 5; ++f) {
+        ipbar[f * (long long)G.nGhost + q] = sgn[f] * A.lamO[f][n];
+        A.lamO[f][n] = 0.0;
+      }
+    } else {
+      const int f = q - G.nGhost;
+      const long long n = G.fnode[f];
+      A.lamFnew[2 * f] += A.lamO[0][n];
+      A.lamFnew[2 * f + 1] += A.lamO[4][n];
+      A.lamO[0][n] = 0.0;
+      A.lamO[4][n] = 0.0;
+    }
+  }
+}
+
+// Phase 2: every image-point cell node gathers weight x image-point adjoint from the ghosts that read it
+// (reverse map in CSR form: entries 8 * ghost + corner).
+__global__ void k_adj_ghost_gather(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ ipbar,
+                                   const long long* __restrict__ cnode, const int* __restrict__ coff,
+                                   const int* __restrict__ cent, int ncell) {
+  const Grid& G = *gp;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+    const long long m = cnode[c];
+    double a[5] = {0, 0, 0, 0, 0};
+    for (int e = coff[c]; e < coff[c + 1]; ++e) {
+      const int q = cent[e] >> 3, slot = cent[e] & 7;
+      const double wn = G.gw[16 * (long long)q + slot], wd = G.gw[16 * (long long)q + 8 + slot];
+      a[0] += wn * ipbar[q];
+      a[4] += wn * ipbar[4 * (long long)G.nGhost + q];
+      for (int f = 1; f < 4; ++f) a[f] += wd * ipbar[f * (long long)G.nGhost + q];
+    }
+    if (G.type[m] & FILTER_BIT) {  // k_ghost read the filtered values of this node
+      const int f = G.fidx[m];
+      A.lamFnew[2 * f] += a[0];
+      A.lamFnew[2 * f + 1] += a[4];
+    } else {
+      A.lamO[0][m] += a[0];
+      A.lamO[4][m] += a[4];
+    }
+    for (int f = 1; f < 4; ++f) A.lamO[f][m] += a[f];
+  }
+}
+
+// ------------------------------------------------------------------------------- near-body filter
+// k_body_filter: fpre = O at the filter node, fnew = (6 O[n] + sum of the 6 neighbours)/12 (rho, rho_E).
+// Every node of the filter stencils gathers from the filter nodes whose stencil holds it.
+__global__ void k_adj_filter(const Grid* __restrict__ gp, AdjPtrs A, const long long* __restrict__ nodes, int count) {
+  const Grid& G = *gp;
+  const long long off[6] = {G.sI, -G.sI, G.sJ, -G.sJ, 1, -1};
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    const long long m = nodes[q];
+    double ar = 0, ae = 0;
+    if (G.type[m] & FILTER_BIT) {
+      const int f = G.fidx[m];
+      ar += 0.5 * A.lamFnew[2 * f] + A.lamFpre[2 * f];
+      ae += 0.5 * A.lamFnew[2 * f + 1] + A.lamFpre[2 * f + 1];
+    }
+    for (int d = 0; d < 6; ++d) {
+      const long long n = m + off[d];
+      if (n < 0 || n >= G.N || !(G.type[n] & FILTER_BIT)) continue;
+      const int f = G.fidx[n];
+      ar += A.lamFnew[2 * f] / 12;
+      ae += A.lamFnew[2 * f + 1] / 12;
+    }
+    A.lamO[0][m] += ar;
+    A.lamO[4][m] += ae;
+  }
+}
+
+__global__ void k_adj_filter_clear(AdjPtrs A, int nFilter) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * nFilter; q += gridDim.x * blockDim.x) {
+    A.lamFnew[q] = 0.0;
+    A.lamFpre[q] = 0.0;
+  }
+}
+
+// -------------------------------------------------------------------------------- edge boundaries
+// One axis, both faces, same launch geometry as k_edge_bc. Phase 1 (periodic, outlet, inlet part 1):
+// consume the adjoint of every edge node; periodic and outlet add to their (one-to-one) source nodes,
+// the inlet keeps the adjoint of its filtered extrapolated density per node for phase 2.
+__global__ void k_adj_edge(const Grid* __restrict__ gp, AdjPtrs A, int axis, double stageT,
+                           double* __restrict__ fbar, double* __restrict__ lamInflow) {
+  const Grid& G = *gp;
+  const Consts& C = G.C;
+  int e = -1, seen = 0;
+  for (int q = 0; q < G.nEdge; ++q)
+    if (G.eAxis[q] == axis) {
+      if (seen == (int)blockIdx.z) e = q;
+      ++seen;
+    }
+  if (e < 0) return;
+  const int* b = G.eBox[e];
+  const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
+  const int a = b[2 * ax1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int bb = b[2 * ax2] + blockIdx.x * blockDim.x + threadIdx.x;
+  if (a > b[2 * ax1 + 1] || bb > b[2 * ax2 + 1]) return;
+  int ijk[3];
+  ijk[axis] = b[2 * axis];
+  ijk[ax1] = a;
+  ijk[ax2] = bb;
+  const long long st = axis == 0 ? G.sI : axis == 1 ? G.sJ : 1;
+  const long long n = ijk[0] * G.sI + ijk[1] * G.sJ + ijk[2];
+  const int side = G.eSide[e], bc = G.eBc[e];
+  double lam[5];
+  for (int f = 0; f < 5; ++f) {
+    lam[f] = A.lamO[f][n];
+    A.lamO[f][n] = 0.0;
+  }
+  if (bc == NSF_BC_PERIODIC) {
+    int src[3] = {ijk[0], ijk[1], ijk[2]};
+    const int nAx = axis == 0 ? G.NI : axis == 1 ? G.NJ : G.NK;
+    src[axis] = side == 0 ? nAx - 2 : 1;
+    const long long m = src[0] * G.sI + src[1] * G.sJ + src[2];
+    for (int f = 0; f < 5; ++f) A.lamO[f][m] += lam[f];
+  } else if (bc == NSF_BC_OUTLET) {
+    const long long a1 = side == 0 ? n + st : n - st, a2 = side == 0 ? n + 2 * st : n - 2 * st;
+    const double rho = 2 * A.val[0][a1] - A.val[0][a2];
+    double u[3];
+    for (int f = 1; f < 4; ++f) u[f - 1] = (2 * A.val[f][a1] - A.val[f][a2]) / (1 + rho);
+    // rho_E = (1 + rho)/2 |u|^2 with u = m/(1 + rho): d/drho = -|u|^2/2, d/dm = u
+    const double rbar = lam[0] - 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) * lam[4];
+    A.lamO[0][a1] += 2 * rbar;
+    A.lamO[0][a2] -= rbar;
+    for (int f = 1; f < 4; ++f) {
+      const double mbar = lam[f] + u[f - 1] * lam[4];
+      A.lamO[f][a1] += 2 * mbar;
+      A.lamO[f][a2] -= mbar;
+    }
+  } else if (bc == NSF_BC_INLET) {
+    // rho = f (filtered extrapolation); u_axis = ramp * M0 * profile; T = 0; p = rho / gamma
+    const long long s1 = ax1 == 0 ? G.sI : G.sJ, s2 = ax2 == 1 ? G.sJ : 1;
+    auto ext = [&](long long m) {
+      return 2 * A.val[0][side == 0 ? m + st : m - st] - A.val[0][side == 0 ? m + 2 * st : m - 2 * st];
+    };
+    double f = 0;
+    unsigned nn = 0;
+    if (a < b[2 * ax1 + 1]) { f += ext(n + s1); ++nn; }
+    if (a > b[2 * ax1]) { f += ext(n - s1); ++nn; }
+    if (bb < b[2 * ax2 + 1]) { f += ext(n + s2); ++nn; }
+    if (bb > b[2 * ax2]) { f += ext(n - s2); ++nn; }
+    f += nn * ext(n);
+    f /= 2 * nn;
+    const double ramp = fmin(1., stageT / 10.) * C.m0 * (side == 1 ? -1.0 : 1.0);
+    const double prof = (G.inflow && axis == 0) ? G.inflow[a * G.NKp + bb] : 1.0;
+    const double vel = ramp * prof;
+    const double fb = lam[0] + vel * lam[axis + 1] + (1 / (C.gamma * C.gm1) + 0.5 * vel * vel) * lam[4];
+    const double velbar = (1 + f) * (lam[axis + 1] + vel * lam[4]);
+    if (axis == 0) lamInflow[a * G.NKp + bb] += velbar * ramp;
+    fbar[(long long)a * G.NKp + bb + (side ? (long long)G.NJ * G.NKp : 0)] = fb;
+  }
+}
+
+// Inlet phase 2 (x faces only): every node of the two planes behind the inlet gathers from the inlet
+// nodes whose filtered extrapolation used it.
+__global__ void k_adj_inlet_gather(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ fbar) {
+  const Grid& G = *gp;
+  const int e = blockIdx.z;
+  if (e >= G.nEdge || G.eAxis[e] != 0 || G.eBc[e] != NSF_BC_INLET) return;
+  const int* b = G.eBox[e];
+  const int a = b[2] + blockIdx.y * blockDim.y + threadIdx.y;   // j
+  const int bb = b[4] + blockIdx.x * blockDim.x + threadIdx.x;  // k
+  if (a > b[3] || bb > b[5]) return;
+  const int side = G.eSide[e];
+  const long long base = side ? (long long)G.NJ * G.NKp : 0;
+  auto nnOf = [&](int ca, int cb) {
+    return unsigned(ca < b[3]) + unsigned(ca > b[2]) + unsigned(cb < b[5]) + unsigned(cb > b[4]);
+  };
+  double g = 0;
+  const int da[5] = {0, 1, -1, 0, 0}, db[5] = {0, 0, 0, 1, -1};
+  for (int c = 0; c < 5; ++c) {
+    const int ca = a + da[c], cb = bb + db[c];
+    if (ca < b[2] || ca > b[3] || cb < b[4] || cb > b[5]) continue;
+    const unsigned nn = nnOf(ca, cb);
+    const double w = c == 0 ? double(nn) / (2 * nn) : 1.0 / (2 * nn);
+    g += w * fbar[base + (long long)ca * G.NKp + cb];
+  }
+  const long long n = (long long)b[0] * G.sI + (long long)a * G.sJ + bb;
+  const long long st = G.sI;
+  A.lamO[0][side == 0 ? n + st : n - st] += 2 * g;
+  A.lamO[0][side == 0 ? n + 2 * st : n - 2 * st] -= g;
+}
+
+// ------------------------------------------------------------------------------------ solid copy
+__global__ void k_adj_solid(const Grid* __restrict__ gp, AdjPtrs A, int mask) {
+  const Grid& G = *gp;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < G.nSolid; q += gridDim.x * blockDim.x) {
+    const long long n = G.snode[q];
+    if (mask & 1) {
+      A.lamR[n] += A.lamO[0][n];
+      A.lamO[0][n] = 0.0;
+    }
+    for (int f = 1; f < 5; ++f)
+      if (mask & (1 << f)) {
+        A.lamI[f][n] += A.lamO[f][n];
+        A.lamO[f][n] = 0.0;
+      }
+  }
+}
+
+// ------------------------------------------------------------------------------------------ stage
+// RK4 combine at the interior nodes: s = 0: O = U0 + inc k, acc = k; s = 1, 2: O = U0 + inc k,
+// acc += 2 k; s = 3: O = U0 + dt/6 (acc + k). Writes the RHS adjoint lam (zero elsewhere beforehand).
+__global__ void k_adj_combine(const Grid* __restrict__ gp, AdjPtrs A, int s, double inc, double dtF,
+                              double* __restrict__ lam) {
+  const Grid& G = *gp;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x) {
+    if ((G.type[n] & TYPE_MASK) != FLUID_INTERIOR) continue;
+    for (int f = 0; f < 5; ++f) {
+      const double o = A.lamO[f][n];
+      double k;
+      if (s == 0) {
+        k = inc * o + A.lamAcc[f][n];
+        A.lamAcc[f][n] = 0.0;
+      } else if (s < 3) {
+        k = inc * o + 2 * A.lamAcc[f][n];
+      } else {
+        k = dtF * o;
+        A.lamAcc[f][n] += dtF * o;
+      }
+      lam[f * G.N + n] = k;
+      A.lamU0[f][n] += o;
+      A.lamO[f][n] = 0.0;
+    }
+  }
+}
+
+// Input quantities of the stage's RHS at every node, as the stage kernel stages them: momenta and
+// rho_E from I, density from R, filter nodes' density and rho_E from fpre (for the primitives).
+__global__ void k_adj_values(const Grid* __restrict__ gp, AdjPtrs A, double* __restrict__ V) {
+  const Grid& G = *gp;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x) {
+    double rho = A.valR[n], rE = A.val[4][n];
+    if (G.type[n] & FILTER_BIT) {
+      const int f = G.fidx[n];
+      rho = A.valFpre[2 * f];
+      rE = A.valFpre[2 * f + 1];
+    }
+    const Prim pr = prims_of(G.C, rho, A.val[1][n], A.val[2][n], A.val[3][n], rE);
+    const double q[11] = {A.val[1][n], A.val[2][n], A.val[3][n], A.val[4][n], pr.u, pr.v, pr.w, pr.p, pr.T, pr.mu, pr.ka};
+    for (int v = 0; v < 11; ++v) V[v * G.N + n] = q[v];
+  }
+}
+
+// Transposed RHS (generated gather) and the chain rule through the primitive / transport values.
+__global__ void k_adj_rhs(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ lam,
+                          const double* __restrict__ V) {
+  const Grid& G = *gp;
+  const Consts& C = G.C;
+  const long long N = G.N, sI = G.sI, sJ = G.sJ;
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < N; m += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    ijk_of(G, m, i, j, k);
+    if (k >= G.NK) continue;
+    auto lamAt = [&](int e, long long b) { return lam[e * N + b]; };
+    auto valAt = [&](int q, long long b) { return V[q * N + b]; };
+    auto inner = [&](int di, int dj, int dk) {
+      const int a = i - di, b = j - dj, c = k - dk;
+      return a >= 1 && a <= G.NI - 2 && b >= 1 && b <= G.NJ - 2 && c >= 1 && c <= G.NK - 2;
+    };
+    double bar[11];
+    rhs_adjoint_gather(C, m, sI, sJ, lamAt, valAt, inner, bar);
+    // chain rule: u = m r1, p = gm1 (rE - (rho+1) K), T = (gamma p - rho) r1, mu = x sqrt(x) sc1/(re (T+sc1)),
+    // kappa = mu pf, with r1 = 1/(rho+1), K = |u|^2/2, x = 1 + T
+    double rho = A.valR[m], rE = A.val[4][m];
+    const bool filt = (G.type[m] & FILTER_BIT) != 0;
+    const int fi = filt ? G.fidx[m] : 0;
+    if (filt) {
+      rho = A.valFpre[2 * fi];
+      rE = A.valFpre[2 * fi + 1];
+    }
+    (void)rE;
+    const double r1 = 1.0 / (rho + 1.0);
+    const double u = V[4 * N + m], v = V[5 * N + m], w = V[6 * N + m], p = V[7 * N + m], T = V[8 * N + m];
+    const double K = 0.5 * (u * u + v * v + w * w);
+    double ub = bar[4], vb = bar[5], wb = bar[6], pb = bar[7], Tb = bar[8], mub = bar[9];
+    mub += C.pf * bar[10];
+    const double x = 1.0 + T, sx = sqrt(x), den = T + C.sc1;
+    Tb += mub * C.sc1 / C.re * (1.5 * sx * den - x * sx) / (den * den);
+    pb += C.gamma * r1 * Tb;
+    double rhob = -r1 * Tb - T * r1 * Tb;
+    double rEb = C.gm1 * pb;
+    rhob += -C.gm1 * K * pb;
+    const double Kb = -C.gm1 * (rho + 1.0) * pb;
+    ub += Kb * u;
+    vb += Kb * v;
+    wb += Kb * w;
+    rhob += -(u * ub + v * vb + w * wb) * r1;
+    A.lamI[1][m] += bar[0] + r1 * ub;
+    A.lamI[2][m] += bar[1] + r1 * vb;
+    A.lamI[3][m] += bar[2] + r1 * wb;
+    A.lamI[4][m] += bar[3];
+    if (filt) {
+      A.lamFpre[2 * fi] += rhob;
+      A.lamFpre[2 * fi + 1] += rEb;
+    } else {
+      A.lamR[m] += rhob;
+      A.lamI[4][m] += rEb;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------- density filter
+// k_density_filter: dst = (6 src + 6 neighbours)/12 at interior nodes, dst = src at edge-plane and ghost
+// nodes; solid inactive nodes off the edge planes keep their value.
+__device__ __forceinline__ int df_kind(uint8_t raw) {  // 2: filtered, 1: copied, 0: untouched
+  const uint8_t t = raw & TYPE_MASK;
+  return t == FLUID_INTERIOR ? 2 : (t != SOLID_INACTIVE || (raw & EDGE_PLANE_BIT)) ? 1 : 0;
+}
+
+__global__ void k_adj_density_filter(const Grid* __restrict__ gp, const double* __restrict__ lamDst,
+                                     double* __restrict__ lamSrc) {
+  const Grid& G = *gp;
+  const long long off[6] = {G.sI, -G.sI, G.sJ, -G.sJ, 1, -1};
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < G.N; m += (long long)gridDim.x * blockDim.x) {
+    const int kind = df_kind(G.type[m]);
+    double a = kind == 2 ? 0.5 * lamDst[m] : kind == 1 ? lamDst[m] : 0.0;
+    for (int d = 0; d < 6; ++d) {
+      const long long n = m + off[d];
+      if (n < 0 || n >= G.N) continue;
+      if (df_kind(G.type[n]) == 2) a += lamDst[n] / 12;
+    }
+    lamSrc[m] += a;
+  }
+}
+
+__global__ void k_adj_density_filter_clear(const Grid* __restrict__ gp, double* __restrict__ lamDst) {
+  const Grid& G = *gp;
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < G.N; m += (long long)gridDim.x * blockDim.x)
+    if (df_kind(G.type[m])) lamDst[m] = 0.0;
+}
+
+int blocks_for(long long n, int nSM) {
+  const long long b = (n + 255) / 256;
+  return int(b < 8 * nSM ? (b > 0 ? b : 1) : 8 * nSM);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------ launchers
+void launch_objective(const Grid* dg, const double* nx, double dA, double weight, double* acc, void* stream) {
+  k_objective<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, nx, dA, weight, acc);
+}
+
+// fpre = the density and rho_E of the filter nodes in buffer `U` (the state at level 0).
+__global__ void k_fpre_init(const Grid* __restrict__ gp, const double* __restrict__ rho, const double* __restrict__ rE) {
+  const Grid& G = *gp;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < G.nFilter; q += gridDim.x * blockDim.x) {
+    G.fpre[2 * q] = rho[G.fnode[q]];
+    G.fpre[2 * q + 1] = rE[G.fnode[q]];
+  }
+}
+
+// The adjoint of that copy: the filter nodes' density / rho_E adjoints gather the fpre adjoints.
+__global__ void k_fpre_init_adj(const Grid* __restrict__ gp, const double* __restrict__ lamFpre, double* lamRho,
+                                double* lamRE) {
+  const Grid& G = *gp;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < G.nFilter; q += gridDim.x * blockDim.x) {
+    lamRho[G.fnode[q]] += lamFpre[2 * q];
+    lamRE[G.fnode[q]] += lamFpre[2 * q + 1];
+  }
+}
+
+void launch_fpre_init(const Grid* dg, int nFilter, const double* rho, const double* rE, int nSM, void* stream) {
+  if (nFilter > 0) k_fpre_init<<<blocks_for(nFilter, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, rho, rE);
+}
+
+void launch_fpre_init_adj(const Grid* dg, int nFilter, const double* lamFpre, double* lamRho, double* lamRE, int nSM,
+                          void* stream) {
+  if (nFilter > 0)
+    k_fpre_init_adj<<<blocks_for(nFilter, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, lamFpre, lamRho, lamRE);
+}
+
+void launch_adj_objective(const Grid* dg, const AdjPtrs& A, int nGhost, const double* nx, double dA, double weight,
+                          int nSM, void* stream) {
+  if (nGhost > 0)
+    k_adj_objective<<<blocks_for(nGhost, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, nx, dA, weight);
+}
+
+void launch_adj_ghost(const Grid* dg, const AdjPtrs& A, int nGhost, int nFilter, double* ipbar, const long long* cnode,
+                      const int* coff, const int* cent, int ncell, int nSM, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (nGhost + nFilter > 0) k_adj_ghost_consume<<<blocks_for(nGhost + nFilter, nSM), 256, 0, st>>>(dg, A, ipbar);
+  if (ncell > 0) k_adj_ghost_gather<<<blocks_for(ncell, nSM), 256, 0, st>>>(dg, A, ipbar, cnode, coff, cent, ncell);
+}
+
+void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes, int count, int nFilter, int nSM,
+                       void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (count > 0) k_adj_filter<<<blocks_for(count, nSM), 256, 0, st>>>(dg, A, nodes, count);
+  if (nFilter > 0) k_adj_filter_clear<<<blocks_for(2 * nFilter, nSM), 256, 0, st>>>(A, nFilter);
+}
+
+void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int axis, double stageT, double* fbar,
+                     double* lamInflow, bool inletGather, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  dim3 grid(L.edgeGrid[axis][0], L.edgeGrid[axis][1], 2);
+  k_adj_edge<<<grid, dim3(32, 8), 0, st>>>(dg, A, axis, stageT, fbar, lamInflow);
+  if (axis == 0 && inletGather) {
+    dim3 g2(L.edgeGrid[0][0], L.edgeGrid[0][1], 6);
+    k_adj_inlet_gather<<<g2, dim3(32, 8), 0, st>>>(dg, A, fbar);
+  }
+}
+
+void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, int nSM, void* stream) {
+  if (nSolid > 0 && mask)
+    k_adj_solid<<<blocks_for(nSolid, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, mask);
+}
+
+void launch_adj_stage(const Grid* dg, const AdjPtrs& A, long long N, int s, double inc, double dtF, double* lam,
+                      double* V, int nSM, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(lam, 0, 5 * N * sizeof(double), st);
+  k_adj_combine<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, s, inc, dtF, lam);
+  k_adj_values<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, V);
+  k_adj_rhs<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, lam, V);
+}
+
+void launch_adj_density_filter(const Grid* dg, long long N, const double* lamDstConst, double* lamDst, double* lamSrc,
+                               int nSM, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_adj_density_filter<<<blocks_for(N, nSM), 256, 0, st>>>(dg, lamDstConst, lamSrc);
+  k_adj_density_filter_clear<<<blocks_for(N, nSM), 256, 0, st>>>(dg, lamDst);
+}
+
+}  // namespace nsf

@@ -486,6 +486,7 @@ nsf_status build_device(nsf_solver* s) {
     ctl.perm[f][1] = 1;
     ctl.perm[f][2] = 2;
   }
+  s->ctlInit = ctl;
   if ((st = dalloc(s, &s->dCtl, 1)) != NSF_OK) return st;
   CK(cudaMemcpy(s->dCtl, &ctl, sizeof ctl, cudaMemcpyHostToDevice));
   G.ctl = s->dCtl;
@@ -786,6 +787,7 @@ void nsf_destroy(nsf_solver* s) {
   }
   if (s->graphExec) cudaGraphExecDestroy(s->graphExec);
   if (s->graph) cudaGraphDestroy(s->graph);
+  nsf_adjoint_free(s);
   for (void* p : s->allocs) cudaFree(p);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;

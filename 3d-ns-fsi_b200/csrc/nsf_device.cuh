@@ -102,6 +102,11 @@ struct Grid {
   int nEdge;
   int eAxis[6], eSide[6], eBc[6];
   int eBox[6][6];           // owned box i0,i1,j0,j1,k0,k1
+  // gradient support (NULL / 0 for a plain run): an x-inlet velocity profile factor per (j, k) node of the
+  // inlet plane, and a prescribed dt per step (the adjoint differentiates with the dt sequence frozen)
+  const double* inflow;     // [NJ * NKp], index j * NKp + k
+  const double* dtFrozen;   // [nDtFrozen]: dt of step n
+  int nDtFrozen;
   // reductions
   double* normPart;         // [nNormSlots][5]: stage-kernel CTAs first, then the near-body filter's blocks
   int nNormSlots;
@@ -154,6 +159,15 @@ int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream);
 // Same sequence, launched eagerly, with events recorded around each of the four stage kernels
 // (events[2*s], events[2*s+1]); used for per-kernel timing.
 int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events);
+// Callbacks of a step launched kernel by kernel (enqueue_step_hooked): after the prologue, before each
+// stage kernel, and before each stage's edge boundary conditions (after the solid-node copy).
+struct StepHook {
+  virtual ~StepHook() = default;
+  virtual void after_prologue() {}
+  virtual void before_stage(int) {}
+  virtual void before_edges(int) {}
+};
+int enqueue_step_hooked(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, StepHook* hook);
 // One RK4 step of every member of an ensemble (dGrids: device array of `members` grids; L: the ensemble's
 // combined plan). events: NULL, or 8 events recorded around the four stage kernels.
 int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* stream, void* events);

@@ -211,6 +211,7 @@ __global__ void k_edge_bc(const Grid* __restrict__ grids, int s, int axis) {
         f /= 2 * nn;
         const double rho = f;
         double vel = fmin(1., c->stageT[s] / 10.) * C.m0;
+        if (G.inflow && axis == 0) vel *= G.inflow[a * G.NKp + bb];  // profile factor (1 in a plain run)
         if (side == 1) vel *= -1;
         u = axis == 0 ? vel : 0;
         v = axis == 1 ? vel : 0;
@@ -417,6 +418,7 @@ __global__ void k_finalize(Grid* grids) {
   const double tNew = c->t + c->dtUsed;
   double dt = (visc < conv) ? visc : conv;
   if (C.endTime && tNew + dt > C.tEnd) dt = C.tEnd - tNew;
+  if (g->dtFrozen && c->level + 1 < (unsigned long long)g->nDtFrozen) dt = g->dtFrozen[c->level + 1];
   double* h = g->hist + 7 * (c->level % MAX_HIST);
   h[0] = tNew;
   h[1] = c->dtUsed;
@@ -584,15 +586,18 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 // solver (its stage kernel takes the grid by value), or NULL for an ensemble (the ensemble stage kernel
 // reads every member from dg). The small kernels carry the member in a grid dimension; their block
 // counts in L are the maxima over the members.
-static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev) {
+static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev,
+                        StepHook* hook = nullptr) {
   int launches = 0;
   const unsigned M = unsigned(members);
   k_prologue<<<M, 32, 0, st>>>(dg);
   ++launches;
+  if (hook) hook->after_prologue();
   k_density_filter<<<dim3(L.gfBlocks, M), 256, 0, st>>>(dg);
   ++launches;
   for (int s = 0; s < 4; ++s) {
     if (ev) cudaEventRecord(ev[2 * s], st);
+    if (hook) hook->before_stage(s);
     if (hg)
       launch_stage(*hg, L, s, st);
     else
@@ -603,6 +608,7 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
       k_solid_copy<<<dim3(L.solidBlocks, M), 256, 0, st>>>(dg, s);
       ++launches;
     }
+    if (hook) hook->before_edges(s);
     for (int a = 0; a < 3; ++a) {
       dim3 grid(L.edgeGrid[a][0], L.edgeGrid[a][1], 2 * M);
       k_edge_bc<<<grid, dim3(32, 8), 0, st>>>(dg, s, a);
@@ -624,6 +630,10 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
 
 int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream) {
   return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int enqueue_step_hooked(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, StepHook* hook) {
+  return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), nullptr, hook);
 }
 
 int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* stream, void* events) {

@@ -37,6 +37,11 @@ struct nsf_solver {
   std::vector<CUtensorMap> hostMaps;
   void* encodeFn = nullptr;
   int tileRequest = -1;  // StageTile to use, or -1 for the default
+  nsf::StepCtl ctlInit{};  // the control block at level 0 (the discrete adjoint restarts from it)
+  struct AdjCtx* adj = nullptr;  // discrete-adjoint state (nsf_adjoint.cpp), created on first use
 };
+
+// Frees the adjoint state of a handle (nsf_adjoint.cpp).
+void nsf_adjoint_free(nsf_solver* s);
 
 #endif

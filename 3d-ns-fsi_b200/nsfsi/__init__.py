@@ -102,6 +102,10 @@ def lib():
         "nsf_ensemble_last_error": (ctypes.c_char_p, [vp]),
         "nsf_ensemble_destroy": (None, [vp]),
         "nsf_autotune": (i32, [cp, i32, ctypes.c_char_p, ctypes.POINTER(i32), dp]),
+        "nsf_adj_configure": (i32, [vp, u32, u32]),
+        "nsf_adj_forward": (i32, [vp, dp, dp, dp]),
+        "nsf_adj_backward": (i32, [vp, ctypes.c_double, dp, dp]),
+        "nsf_adj_get_dt": (i32, [vp, dp, ctypes.POINTER(u64)]),
         "nsf_last_error": (ctypes.c_char_p, [vp]),
         "nsf_destroy": (None, [vp]),
     }
@@ -256,6 +260,35 @@ class Solver:
         n = ctypes.c_uint64()
         self._check(lib().nsf_launches_per_step(self.h, ctypes.byref(n)))
         return n.value
+
+    # ---------------------------------------------------------------- discrete adjoint
+    def adj_configure(self, avg_last_steps=50, snapshots=20):
+        self._check(lib().nsf_adj_configure(self.h, avg_last_steps, snapshots))
+
+    def adj_forward(self, u0=None, inflow=None):
+        """J of a run from level 0 (u0: (5, N) conserved field or None for the case's IC; inflow: (NJ, NK)
+        inlet profile factor or None for 1)."""
+        J = ctypes.c_double()
+        a = None if u0 is None else np.ascontiguousarray(u0, dtype=np.float64)
+        b = None if inflow is None else np.ascontiguousarray(inflow, dtype=np.float64)
+        self._check(lib().nsf_adj_forward(self.h, None if a is None else _dp(a), None if b is None else _dp(b),
+                                          ctypes.byref(J)))
+        return J.value
+
+    def adj_backward(self, dJ=1.0):
+        """(gradient w.r.t. the inflow profile factor (NJ, NK), gradient w.r.t. the level-0 field (5, N))."""
+        c = self.cfg
+        gi = np.zeros((int(c.NJ), int(c.NK)))
+        gu = np.zeros((5, self.N))
+        self._check(lib().nsf_adj_backward(self.h, dJ, _dp(gi), _dp(gu)))
+        return gi, gu
+
+    def adj_dt(self):
+        n = ctypes.c_uint64()
+        self._check(lib().nsf_adj_get_dt(self.h, None, ctypes.byref(n)))
+        out = np.zeros(n.value)
+        self._check(lib().nsf_adj_get_dt(self.h, _dp(out), ctypes.byref(n)))
+        return out
 
     def geometry(self):
         """dx, dy, dz and Mesh::positionOffset x, y, z."""

@@ -207,6 +207,25 @@ void nsf_ensemble_destroy(nsf_ensemble* e);
 nsf_status nsf_autotune(const nsf_config* cfg, int32_t device, const char* cache_path, int32_t* tile,
                         double* ns_per_node);
 
+/* ---------------------------------------------------------------------------------------------------
+ * Discrete adjoint (a forward / backward pair; no counterpart in the reference, whose marchTimeStep,
+ * Solver.cpp:130-167, it differentiates). Objective of a run of stop_time_level steps from level 0:
+ *   J = (1/n_avg) sum over the last n_avg steps of F_x(U_n),  F_x = -(dx dy dz)^(2/3) sum_g p(U_g) n_x(g)
+ * over the ghost nodes g of the immersed bodies (p: the ghost's pressure, equal to its image point's;
+ * n: the body's outward unit normal at the ghost's body-intercept point). Parameters: the conserved field
+ * at level 0 (5 x N doubles, every node, reference layout) and the x-inlet velocity profile factor
+ * (NJ x NK doubles, index j*NK + k; the inlet velocity is min(1, t/10) M0 times the factor; only the
+ * inlet's own nodes j, k in [1, N-2] matter). Cases: periodic faces and x inlet / outlet faces, spheres
+ * and cylinders; stopCriterion "timesteps".
+ * The first nsf_adj_forward freezes its dt sequence; later runs (and the backward pass) use it.
+ * nsf_adj_backward: gradients of dJ * J; binomial checkpointing with `snapshots` stored states
+ * (default 20) and recomputation. Both leave the handle's state at some level of the run. */
+nsf_status nsf_adj_configure(nsf_solver* s, uint32_t avg_last_steps, uint32_t snapshots);
+nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow, double* J);
+nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* g_u0);
+/* The frozen dt sequence (count values: dt of step n). */
+nsf_status nsf_adj_get_dt(nsf_solver* s, double* dts, uint64_t* count);
+
 /* Text of the last error on this handle (static storage owned by the handle). */
 const char* nsf_last_error(nsf_solver* s);
 

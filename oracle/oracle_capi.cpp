@@ -175,6 +175,16 @@ void nsfo_get_fields(void* hp, double* out) {
                                       &s->prim[1], &s->prim[2], &s->prim[3], &s->prim[4], &s->mu, &s->kappa};
   for (int f = 0; f < 12; ++f) std::memcpy(out + f * s->N, a[f]->data(), s->N * sizeof(double));
 }
+// The right-hand side (Solver.cpp:181-418) of the current conserved and stored primitive fields at the
+// interior nodes (5 x N, zero elsewhere): a check of the RHS term table of the adjoint generator.
+void nsfo_rhs(void* hp, double* out) {
+  auto* s = static_cast<Handle*>(hp)->s;
+  std::vector<double> k[5];
+  for (auto& v : k) v.assign(s->N, 0.0);
+  s->rhs(s->cons, k);
+  for (int f = 0; f < 5; ++f) std::memcpy(out + f * s->N, k[f].data(), s->N * sizeof(double));
+}
+
 // The "old" conserved buffers (5 x N), which hold state the reference carries across steps.
 void nsfo_get_old(void* hp, double* out) {
   auto* s = static_cast<Handle*>(hp)->s;

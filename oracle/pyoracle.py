@@ -43,6 +43,7 @@ def lib():
         L.nsfo_geometry.argtypes = [vp, ctypes.POINTER(dbl)]
         L.nsfo_get_fields.argtypes = [vp, ctypes.POINTER(dbl)]
         L.nsfo_get_old.argtypes = [vp, ctypes.POINTER(dbl)]
+        L.nsfo_rhs.argtypes = [vp, ctypes.POINTER(dbl)]
         L.nsfo_set_conserved.argtypes = [vp, ctypes.POINTER(dbl)]
         L.nsfo_get_types.argtypes = [vp, ctypes.POINTER(ctypes.c_uint8)]
         for name in ("nsfo_num_ghosts", "nsfo_num_filter", "nsfo_closure_added"):
@@ -119,6 +120,12 @@ class Oracle:
     def fields(self):
         out = np.empty((12, self.N))
         lib().nsfo_get_fields(self.h, _dp(out))
+        return out
+
+    def rhs(self):
+        """RHS (5, N) of the current state at the interior nodes (zero elsewhere)."""
+        out = np.zeros((5, self.N))
+        lib().nsfo_rhs(self.h, _dp(out))
         return out
 
     def old_conserved(self):

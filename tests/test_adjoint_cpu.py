@@ -1,0 +1,78 @@
+"""The term table of the discrete adjoint (3d-ns-fsi_b200/csrc/gen_rhs_adjoint.py) on the CPU:
+
+* its forward polynomial reproduces the reference's right-hand side (the oracle's, Solver.cpp:181-418)
+  on a flow state, and
+* its gather-form adjoint is the transpose of that polynomial's Jacobian (dot-product test against
+  central finite differences of the forward polynomial).
+"""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+spec = importlib.util.spec_from_file_location("gen", os.path.join(ROOT, "3d-ns-fsi_b200", "csrc", "gen_rhs_adjoint.py"))
+gen = importlib.util.module_from_spec(spec)
+spec.loader.exec_module(gen)
+
+CNAMES = ["ax", "ay", "az", "h0", "xm_xx", "xm_yy", "xm_zz", "xm_yx", "xm_xy", "xm_zx", "xm_xz", "ym_xx", "ym_yy",
+          "ym_zz", "ym_xy", "ym_yx", "ym_zy", "ym_yz", "zm_xx", "zm_yy", "zm_zz", "zm_zx", "zm_xz", "zm_zy", "zm_yz",
+          "e_xx23", "e_xx12", "e_yx6", "e_zx6", "e_yx4", "e_zx4", "e_yy12", "e_yy23", "e_zy6", "e_zy4", "e_zz12",
+          "e_zz23"]
+
+
+def consts(dx, dy, dz, gamma):
+    C = dict(ax=-1 / (2 * dx), ay=-1 / (2 * dy), az=-1 / (2 * dz), h0=1 / (gamma - 1),
+             xm_xx=2 / (3 * dx * dx), xm_yy=1 / (2 * dy * dy), xm_zz=1 / (2 * dz * dz), xm_yx=-1 / (6 * dy * dx),
+             xm_xy=1 / (4 * dx * dy), xm_zx=-1 / (6 * dz * dx), xm_xz=1 / (4 * dx * dz),
+             ym_xx=1 / (2 * dx * dx), ym_yy=2 / (3 * dy * dy), ym_zz=1 / (2 * dz * dz), ym_xy=-1 / (6 * dx * dy),
+             ym_yx=1 / (4 * dy * dx), ym_zy=-1 / (6 * dz * dy), ym_yz=1 / (4 * dy * dz),
+             zm_xx=1 / (2 * dx * dx), zm_yy=1 / (2 * dy * dy), zm_zz=2 / (3 * dz * dz), zm_zx=1 / (4 * dz * dx),
+             zm_xz=-1 / (6 * dx * dz), zm_zy=1 / (4 * dz * dy), zm_yz=-1 / (6 * dy * dz),
+             e_xx23=2 / (3 * dx * dx), e_xx12=1 / (2 * dx * dx), e_yx6=-1 / (6 * dy * dx), e_zx6=-1 / (6 * dz * dx),
+             e_yx4=1 / (4 * dy * dx), e_zx4=1 / (4 * dz * dx), e_yy12=1 / (2 * dy * dy), e_yy23=2 / (3 * dy * dy),
+             e_zy6=-1 / (6 * dz * dy), e_zy4=1 / (4 * dz * dy), e_zz12=1 / (2 * dz * dz), e_zz23=2 / (3 * dz * dz))
+    assert set(C) == set(CNAMES)
+    return C
+
+
+def test_term_table_reproduces_the_reference_rhs():
+    o = po.Oracle(open(os.path.join(ROOT, "tests/golden/cases/sphere_small.cfg")).read())
+    o.march(5)
+    f = o.fields()
+    shape = tuple(int(x) for x in np.load(os.path.join(ROOT, "tests/golden/sphere_small.npz"))["shape"])
+    g = o.geometry()
+    C = consts(g[0], g[1], g[2], 1.4)
+    fields = {q: f[i].reshape(shape) for q, i in zip(gen.VARS, [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11])}
+    mine = gen.forward(gen.rhs_polys(), fields, C)
+    ref = o.rhs()
+    interior = o.node_types() == 0
+    for e in range(5):
+        a, b = mine[e].reshape(-1)[interior], ref[e][interior]
+        assert np.abs(a - b).max() <= 1e-12 * max(np.abs(b).max(), 1e-12), e
+
+
+def test_adjoint_gather_is_the_transpose():
+    rng = np.random.default_rng(7)
+    shape = (9, 8, 7)
+    fields = {q: rng.uniform(0.5, 1.5, shape) for q in gen.VARS}
+    C = consts(0.11, 0.13, 0.17, 1.4)
+    eqs = gen.rhs_polys()
+    inner = np.zeros(shape, bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    lam = [rng.standard_normal(shape) * inner for _ in range(5)]
+    bar = gen.adjoint(gen.adjoint_terms(eqs), fields, lam, C)
+    for q in gen.VARS:
+        d = rng.standard_normal(shape)
+        h = 1e-6
+        fp = dict(fields)
+        fm = dict(fields)
+        fp[q] = fields[q] + h * d
+        fm[q] = fields[q] - h * d
+        rp, rm = gen.forward(eqs, fp, C), gen.forward(eqs, fm, C)
+        jvp = sum(((rp[e] - rm[e]) / (2 * h) * lam[e]).sum() for e in range(5))
+        vjp = (bar[q] * d).sum()
+        assert abs(jvp - vjp) <= 1e-7 * max(abs(vjp), 1.0), (q, jvp, vjp)

@@ -57,7 +57,13 @@ struct AdjCtx {
   std::vector<double*> slot;
   std::vector<StepCtl*> slotCtl;
   double* stageSnap = nullptr;  // 4 x (11 Nd + 2F): I (5), R (1), O before the edge conditions (5), fpre
-  StepCtl roles{};
+  StepCtl* dHist = nullptr;      // [nsteps]: each step's control block after its prologue (written on the device)
+  std::vector<StepCtl> hist;     // host copy of dHist from the last forward run
+  std::vector<std::pair<int, int>> chain;  // (level, slot) checkpoints the forward run stores
+  bool chainStored = false;                // the slots still hold the last forward run's checkpoints
+  StepCtl* dCur = nullptr;                 // the control block of the step being reversed (after its prologue)
+  // one CUDA graph per distinct pattern of buffer roles (the roles rotate with a short period)
+  std::map<std::vector<uintptr_t>, cudaGraphExec_t> graphs;
   std::vector<void*> allocs;
 };
 
@@ -131,6 +137,10 @@ nsf_status setup(nsf_solver* s) {
   if ((st = aalloc(s, a, &a->ipbar, 5 * NG)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->fbar, 2 * plane)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->stageSnap, 4 * per_stage(s))) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->dHist, size_t(a->nsteps))) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->dCur, 1)) != NSF_OK) return st;
+  s->hGrid.ctlHist = a->dHist;
+  s->hGrid.nCtlHist = a->nsteps;
   // objective: body normals at the ghosts' body-intercept points (gnode order), area weight
   std::vector<double> nx;
   for (const auto& b : S.bodies)
@@ -246,47 +256,50 @@ nsf_status advance(nsf_solver* s, int n) {
   return NSF_OK;
 }
 
-// Keeps the roles of the step and, per stage, the values its nonlinear adjoints need.
+// Keeps the step's control block and, per stage, the values the nonlinear adjoints need. The step's roles
+// (which physical buffer plays which part) are known on the host from the forward run's record, so nothing
+// waits here and the whole adjoint step can be captured as a graph.
 struct SnapHook : StepHook {
   nsf_solver* s;
   AdjCtx* a;
+  const StepCtl& R;
   cudaError_t err = cudaSuccess;
-  SnapHook(nsf_solver* s_, AdjCtx* a_) : s(s_), a(a_) {}
+  SnapHook(nsf_solver* s_, AdjCtx* a_, const StepCtl& r) : s(s_), a(a_), R(r) {}
   void copy(double* dst, const double* src, size_t words) {
     if (err == cudaSuccess)
       err = cudaMemcpyAsync(dst, src, words * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
   }
   void after_prologue() override {
-    if (err == cudaSuccess) err = cudaStreamSynchronize(s->stream);
-    if (err == cudaSuccess) err = cudaMemcpy(&a->roles, s->dCtl, sizeof(StepCtl), cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(a->dCur, s->dCtl, sizeof(StepCtl), cudaMemcpyDeviceToDevice, s->stream);
   }
   void before_stage(int q) override {
     const size_t N = nd(s);
     double* base = a->stageSnap + q * per_stage(s);
-    for (int f = 0; f < 5; ++f) copy(base + f * N, a->roles.I[q][f], N);
-    copy(base + 5 * N, a->roles.R[q], N);
+    for (int f = 0; f < 5; ++f) copy(base + f * N, R.I[q][f], N);
+    copy(base + 5 * N, R.R[q], N);
     if (nf(s)) copy(base + 11 * N, s->hGrid.fpre, 2 * nf(s));
   }
   void before_edges(int q) override {
     const size_t N = nd(s);
     double* base = a->stageSnap + q * per_stage(s);
-    for (int f = 0; f < 5; ++f) copy(base + (6 + f) * N, a->roles.O[q][f], N);
+    for (int f = 0; f < 5; ++f) copy(base + (6 + f) * N, R.O[q][f], N);
   }
 };
 
-// The adjoint of step k: the working state holds U_k on entry (U_{k+1} on exit); the adjoint arrays hold
-// the adjoint of U_{k+1} on entry and of U_k on exit.
-nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
-  SnapHook hook(s, a);
+// Enqueues the adjoint of a step with roles R: the working state holds U_k on entry (U_{k+1} on exit);
+// the adjoint arrays hold the adjoint of U_{k+1} on entry and of U_k on exit. objective: F_x(U_{k+1})
+// enters J.
+nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool objective) {
+  const StepCtl* dR = a->dCur;
+  SnapHook hook(s, a, R);
   enqueue_step_hooked(s->dGrid, s->hGrid, s->plan, s->stream, &hook);
   if (hook.err != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint recomputation: ") + cudaGetErrorString(hook.err));
   CKA(cudaGetLastError());
-  const StepCtl& R = a->roles;
   const Grid& G = s->hGrid;
   const size_t N = nd(s);
   const int nSM = s->nSM;
   cudaStream_t st = s->stream;
-  if (k + 1 > a->nsteps - a->navg) {  // F_x of U_{k+1} enters J
+  if (objective) {
     AdjPtrs A{};
     for (int f = 0; f < 5; ++f) {
       A.val[f] = R.O[3][f];
@@ -312,14 +325,13 @@ nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
     // edge conditions: z, y, then x (reads the stage output before the edge conditions)
     for (int f = 0; f < 5; ++f) A.val[f] = snap + (6 + f) * N;
     for (int axis = 2; axis >= 0; --axis)
-      launch_adj_edge(s->dGrid, A, s->plan, axis, R.stageT[q], a->fbar, a->lamInflow, a->inletX, st);
+      launch_adj_edge(s->dGrid, A, s->plan, axis, dR, q, a->fbar, a->lamInflow, a->inletX, st);
     launch_adj_solid(s->dGrid, A, G.nSolid, R.copyMask[q], nSM, st);
     // stage kernel: RK4 combine, transposed RHS, primitives of the stage input
     for (int f = 0; f < 5; ++f) A.val[f] = snap + f * N;
     A.valR = snap + 5 * N;
     A.valFpre = snap + 11 * N;
-    const double inc = q == 2 ? R.dtUsed : R.dtUsed / 2;
-    launch_adj_stage(s->dGrid, A, (long long)N, q, inc, R.dtUsed / 6, a->tmpLam, a->tmpV, nSM, st);
+    launch_adj_stage(s->dGrid, A, (long long)N, q, dR, a->tmpLam, a->tmpV, nSM, st);
   }
   if (R.filterNow) {
     double* dst = lamOf(s, a, phys(s, R.gfDst, 0), 0);
@@ -330,14 +342,82 @@ nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
   return NSF_OK;
 }
 
+// Everything the enqueued work of an adjoint step depends on besides fixed buffers.
+std::vector<uintptr_t> role_key(const StepCtl& R, bool objective) {
+  std::vector<uintptr_t> key;
+  auto put = [&](const void* p) { key.push_back(reinterpret_cast<uintptr_t>(p)); };
+  for (int q = 0; q < 4; ++q) {
+    for (int f = 0; f < 5; ++f) {
+      put(R.I[q][f]);
+      put(R.O[q][f]);
+    }
+    put(R.R[q]);
+    key.push_back(uintptr_t(R.copyMask[q]));
+  }
+  for (int f = 0; f < 5; ++f) put(R.U0[f]);
+  key.push_back(uintptr_t(R.filterNow));
+  put(R.filterNow ? R.gfSrc : nullptr);
+  put(R.filterNow ? R.gfDst : nullptr);
+  key.push_back(uintptr_t(objective));
+  return key;
+}
+
+// The adjoint of step k, launched as the cached graph of its role pattern.
+nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
+  const StepCtl& R = a->hist[k];
+  const bool objective = k + 1 > a->nsteps - a->navg;
+  const auto key = role_key(R, objective);
+  auto it = a->graphs.find(key);
+  if (it == a->graphs.end()) {
+    CKA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const nsf_status st = enqueue_adjoint_step(s, a, R, objective);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (st != NSF_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint step capture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t x = nullptr;
+    const cudaError_t e2 = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint step graph: ") + cudaGetErrorString(e2));
+    it = a->graphs.emplace(key, x).first;
+  }
+  CKA(cudaGraphLaunch(it->second, s->stream));
+  return NSF_OK;
+}
+
 double binom(int n, int k) {
   double r = 1;
   for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
   return r;
 }
 
+int split(int a0, int b, int c) {
+  const int n = b - a0;
+  int t = 0;
+  while (binom(c + t, t) < n) ++t;
+  const int right = int(std::min<double>(binom(c - 1 + t, t), n - 1));
+  return a0 + std::max(1, n - right);
+}
+
+// The checkpoints of the schedule's first descent (state at `level` into `slot`): the forward run stores
+// them as it passes, so the backward run starts at the last step without recomputing.
+std::vector<std::pair<int, int>> first_descent(int n, int c) {
+  std::vector<std::pair<int, int>> out;
+  int a0 = 0, depth = 0;
+  while (n - a0 > 1 && c > 0) {
+    a0 = split(a0, n, c);
+    out.push_back({a0, ++depth});
+    --c;
+  }
+  return out;
+}
+
 // Reverse steps [a0, b) with c free snapshot slots above `depth`; slot `depth` holds the state at a0.
-nsf_status reverse(nsf_solver* s, AdjCtx* a, int a0, int b, int c, int depth) {
+// stored: the checkpoints of this call's first descent are already in their slots.
+nsf_status reverse(nsf_solver* s, AdjCtx* a, int a0, int b, int c, int depth, bool stored = false) {
   nsf_status st;
   if (b - a0 == 1) {
     if ((st = restore(s, a, depth)) != NSF_OK) return st;
@@ -351,15 +431,13 @@ nsf_status reverse(nsf_solver* s, AdjCtx* a, int a0, int b, int c, int depth) {
     }
     return NSF_OK;
   }
-  const int n = b - a0;
-  int t = 0;
-  while (binom(c + t, t) < n) ++t;
-  const int right = int(std::min<double>(binom(c - 1 + t, t), n - 1));
-  const int m = a0 + std::max(1, n - right);
-  if ((st = restore(s, a, depth)) != NSF_OK) return st;
-  if ((st = advance(s, m - a0)) != NSF_OK) return st;
-  if ((st = save(s, a, depth + 1)) != NSF_OK) return st;
-  if ((st = reverse(s, a, m, b, c - 1, depth + 1)) != NSF_OK) return st;
+  const int m = split(a0, b, c);
+  if (!stored) {
+    if ((st = restore(s, a, depth)) != NSF_OK) return st;
+    if ((st = advance(s, m - a0)) != NSF_OK) return st;
+    if ((st = save(s, a, depth + 1)) != NSF_OK) return st;
+  }
+  if ((st = reverse(s, a, m, b, c - 1, depth + 1, stored)) != NSF_OK) return st;
   return reverse(s, a, a0, m, c, depth);
 }
 
@@ -367,6 +445,7 @@ nsf_status reverse(nsf_solver* s, AdjCtx* a, int a0, int b, int c, int depth) {
 
 void nsf_adjoint_free(nsf_solver* s) {
   if (!s || !s->adj) return;
+  for (auto& kv : s->adj->graphs) cudaGraphExecDestroy(kv.second);
   for (void* p : s->adj->allocs) cudaFree(p);
   delete s->adj;
   s->adj = nullptr;
@@ -381,7 +460,12 @@ nsf_status nsf_adj_configure(nsf_solver* s, uint32_t avg_last_steps, uint32_t sn
   AdjCtx* a = s->adj;
   if (avg_last_steps == 0 || int(avg_last_steps) > a->nsteps || snapshots == 0 || snapshots > 4096)
     return fail(s, NSF_ERR_ARG, "nsf_adj_configure: 1 <= avg_last_steps <= steps and 1 <= snapshots <= 4096");
+  if (int(avg_last_steps) != a->navg) {  // the graphs hold the objective's weight
+    for (auto& kv : a->graphs) cudaGraphExecDestroy(kv.second);
+    a->graphs.clear();
+  }
   a->navg = int(avg_last_steps);
+  if (int(snapshots) != a->nsnap) a->chainStored = false;
   a->nsnap = int(snapshots);
   return NSF_OK;
 }
@@ -416,13 +500,19 @@ nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow
   if ((st = reset(s, a)) != NSF_OK) return st;
   if ((st = save(s, a, 0)) != NSF_OK) return st;
   CKA(cudaMemsetAsync(a->dAcc, 0, sizeof(double), s->stream));
+  a->chain = first_descent(a->nsteps, a->nsnap);
+  size_t next = 0;
   for (int n = 0; n < a->nsteps; ++n) {
     CKA(cudaGraphLaunch(s->graphExec, s->stream));
     if (n + 1 > a->nsteps - a->navg) launch_objective(s->dGrid, a->dNx, a->dA, 1.0 / a->navg, a->dAcc, s->stream);
+    if (next < a->chain.size() && a->chain[next].first == n + 1)
+      if ((st = save(s, a, a->chain[next++].second)) != NSF_OK) return st;
   }
   CKA(cudaGetLastError());
   if ((st = nsf_sync(s)) != NSF_OK) return st;
   CKA(cudaMemcpy(J, a->dAcc, sizeof(double), cudaMemcpyDeviceToHost));
+  a->hist.resize(a->nsteps);
+  CKA(cudaMemcpy(a->hist.data(), a->dHist, a->nsteps * sizeof(StepCtl), cudaMemcpyDeviceToHost));
   if (!a->haveDt) {  // freeze the dt sequence of this run
     std::vector<double> rows(7 * size_t(a->nsteps));
     uint64_t avail = 0;
@@ -436,6 +526,7 @@ nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow
     if ((st = push_grid(s)) != NSF_OK) return st;
   }
   a->haveForward = true;
+  a->chainStored = true;
   return NSF_OK;
 }
 
@@ -447,6 +538,8 @@ nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* 
   const Grid& G = s->hGrid;
   const size_t N = nd(s), F = nf(s), plane = size_t(G.NJ) * G.NKp;
   CKA(cudaSetDevice(s->device));
+  nsf_status st = alloc_slots(s, a);
+  if (st != NSF_OK) return st;
   CKA(cudaMemsetAsync(a->lam, 0, 20 * N * sizeof(double), s->stream));
   if (F) {
     CKA(cudaMemsetAsync(a->lamFpre, 0, 2 * F * sizeof(double), s->stream));
@@ -454,7 +547,8 @@ nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* 
   }
   CKA(cudaMemsetAsync(a->lamInflow, 0, plane * sizeof(double), s->stream));
   CKA(cudaMemsetAsync(a->fbar, 0, 2 * plane * sizeof(double), s->stream));
-  nsf_status st = reverse(s, a, 0, a->nsteps, a->nsnap, 0);
+  st = reverse(s, a, 0, a->nsteps, a->nsnap, 0, a->chainStored);
+  a->chainStored = false;  // the schedule has reused the slots
   if (st != NSF_OK) return st;
   // level-0 fpre was copied from U0
   launch_fpre_init_adj(s->dGrid, G.nFilter, a->lamFpre, lamOf(s, a, 0, 0), lamOf(s, a, 0, 4), s->nSM, s->stream);

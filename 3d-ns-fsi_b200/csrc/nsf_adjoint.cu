@@ -172,9 +172,10 @@ __global__ void k_adj_filter_clear(AdjPtrs A, int nFilter) {
 // One axis, both faces, same launch geometry as k_edge_bc. Phase 1 (periodic, outlet, inlet part 1):
 // consume the adjoint of every edge node; periodic and outlet add to their (one-to-one) source nodes,
 // the inlet keeps the adjoint of its filtered extrapolated density per node for phase 2.
-__global__ void k_adj_edge(const Grid* __restrict__ gp, AdjPtrs A, int axis, double stageT,
+__global__ void k_adj_edge(const Grid* __restrict__ gp, AdjPtrs A, int axis, const StepCtl* __restrict__ roles, int s,
                            double* __restrict__ fbar, double* __restrict__ lamInflow) {
   const Grid& G = *gp;
+  const double stageT = roles->stageT[s];
   const Consts& C = G.C;
   int e = -1, seen = 0;
   for (int q = 0; q < G.nEdge; ++q)
@@ -294,9 +295,11 @@ __global__ void k_adj_solid(const Grid* __restrict__ gp, AdjPtrs A, int mask) {
 // ------------------------------------------------------------------------------------------ stage
 // RK4 combine at the interior nodes: s = 0: O = U0 + inc k, acc = k; s = 1, 2: O = U0 + inc k,
 // acc += 2 k; s = 3: O = U0 + dt/6 (acc + k). Writes the RHS adjoint lam (zero elsewhere beforehand).
-__global__ void k_adj_combine(const Grid* __restrict__ gp, AdjPtrs A, int s, double inc, double dtF,
+__global__ void k_adj_combine(const Grid* __restrict__ gp, AdjPtrs A, int s, const StepCtl* __restrict__ roles,
                               double* __restrict__ lam) {
   const Grid& G = *gp;
+  const double dtUsed = roles->dtUsed;
+  const double inc = s == 2 ? dtUsed : dtUsed / 2, dtF = dtUsed / 6;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x) {
     if ((G.type[n] & TYPE_MASK) != FLUID_INTERIOR) continue;
     for (int f = 0; f < 5; ++f) {
@@ -336,7 +339,7 @@ __global__ void k_adj_values(const Grid* __restrict__ gp, AdjPtrs A, double* __r
 }
 
 // Transposed RHS (generated gather) and the chain rule through the primitive / transport values.
-__global__ void k_adj_rhs(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ lam,
+__global__ void __launch_bounds__(256, 2) k_adj_rhs(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ lam,
                           const double* __restrict__ V) {
   const Grid& G = *gp;
   const Consts& C = G.C;
@@ -355,16 +358,12 @@ __global__ void k_adj_rhs(const Grid* __restrict__ gp, AdjPtrs A, const double* 
     rhs_adjoint_gather(C, m, sI, sJ, lamAt, valAt, inner, bar);
     // chain rule: u = m r1, p = gm1 (rE - (rho+1) K), T = (gamma p - rho) r1, mu = x sqrt(x) sc1/(re (T+sc1)),
     // kappa = mu pf, with r1 = 1/(rho+1), K = |u|^2/2, x = 1 + T
-    double rho = A.valR[m], rE = A.val[4][m];
+    // the density of the primitives: the stage's density input, or the pre-filter copy at filter nodes
     const bool filt = (G.type[m] & FILTER_BIT) != 0;
     const int fi = filt ? G.fidx[m] : 0;
-    if (filt) {
-      rho = A.valFpre[2 * fi];
-      rE = A.valFpre[2 * fi + 1];
-    }
-    (void)rE;
+    const double rho = filt ? A.valFpre[2 * fi] : A.valR[m];
     const double r1 = 1.0 / (rho + 1.0);
-    const double u = V[4 * N + m], v = V[5 * N + m], w = V[6 * N + m], p = V[7 * N + m], T = V[8 * N + m];
+    const double u = V[4 * N + m], v = V[5 * N + m], w = V[6 * N + m], T = V[8 * N + m];
     const double K = 0.5 * (u * u + v * v + w * w);
     double ub = bar[4], vb = bar[5], wb = bar[6], pb = bar[7], Tb = bar[8], mub = bar[9];
     mub += C.pf * bar[10];
@@ -484,11 +483,11 @@ void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes,
   if (nFilter > 0) k_adj_filter_clear<<<blocks_for(2 * nFilter, nSM), 256, 0, st>>>(A, nFilter);
 }
 
-void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int axis, double stageT, double* fbar,
-                     double* lamInflow, bool inletGather, void* stream) {
+void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
+                     double* fbar, double* lamInflow, bool inletGather, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   dim3 grid(L.edgeGrid[axis][0], L.edgeGrid[axis][1], 2);
-  k_adj_edge<<<grid, dim3(32, 8), 0, st>>>(dg, A, axis, stageT, fbar, lamInflow);
+  k_adj_edge<<<grid, dim3(32, 8), 0, st>>>(dg, A, axis, roles, s, fbar, lamInflow);
   if (axis == 0 && inletGather) {
     dim3 g2(L.edgeGrid[0][0], L.edgeGrid[0][1], 6);
     k_adj_inlet_gather<<<g2, dim3(32, 8), 0, st>>>(dg, A, fbar);
@@ -500,11 +499,11 @@ void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, in
     k_adj_solid<<<blocks_for(nSolid, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, mask);
 }
 
-void launch_adj_stage(const Grid* dg, const AdjPtrs& A, long long N, int s, double inc, double dtF, double* lam,
+void launch_adj_stage(const Grid* dg, const AdjPtrs& A, long long N, int s, const StepCtl* roles, double* lam,
                       double* V, int nSM, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaMemsetAsync(lam, 0, 5 * N * sizeof(double), st);
-  k_adj_combine<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, s, inc, dtF, lam);
+  k_adj_combine<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, s, roles, lam);
   k_adj_values<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, V);
   k_adj_rhs<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, lam, V);
 }

@@ -30,10 +30,11 @@ void launch_adj_ghost(const Grid* dg, const AdjPtrs& A, int nGhost, int nFilter,
                       const int* coff, const int* cent, int ncell, int nSM, void* stream);
 void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes, int count, int nFilter, int nSM,
                        void* stream);
-void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int axis, double stageT, double* fbar,
-                     double* lamInflow, bool inletGather, void* stream);
+// roles: device copy of the step's control block (stage times, dt).
+void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
+                     double* fbar, double* lamInflow, bool inletGather, void* stream);
 void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, int nSM, void* stream);
-void launch_adj_stage(const Grid* dg, const AdjPtrs& A, long long N, int s, double inc, double dtF, double* lam,
+void launch_adj_stage(const Grid* dg, const AdjPtrs& A, long long N, int s, const StepCtl* roles, double* lam,
                       double* V, int nSM, void* stream);
 void launch_adj_density_filter(const Grid* dg, long long N, const double* lamDstConst, double* lamDst, double* lamSrc,
                                int nSM, void* stream);

@@ -107,6 +107,8 @@ struct Grid {
   const double* inflow;     // [NJ * NKp], index j * NKp + k
   const double* dtFrozen;   // [nDtFrozen]: dt of step n
   int nDtFrozen;
+  StepCtl* ctlHist;         // [nCtlHist]: the control block of step n right after its prologue (roles)
+  int nCtlHist;
   // reductions
   double* normPart;         // [nNormSlots][5]: stage-kernel CTAs first, then the near-body filter's blocks
   int nNormSlots;

@@ -111,6 +111,7 @@ __global__ void k_prologue(Grid* grids) {
     c->perm[f][2] = A[f];
   }
   for (int q = 0; q < 4; ++q) c->mx[q] = 0ull;
+  if (g->ctlHist && c->level < (unsigned long long)g->nCtlHist) g->ctlHist[c->level] = *c;
 }
 
 // Mesh::applyFilter_ifAppropriate body (Mesh.cpp:110-134): interior nodes get the 7-point filter,

@@ -1,0 +1,150 @@
+"""Discrete adjoint (nsf_adj_configure / nsf_adj_forward / nsf_adj_backward): the gradient of the
+time-averaged x-force on the immersed sphere with respect to the level-0 conserved field and the x-inlet's
+velocity-profile factor, checked against central finite differences of the forward run along seeded random
+directions, plus the properties of the checkpointing schedule (the result does not depend on the number of
+snapshots; a second backward run after one forward run gives the same gradient)."""
+import numpy as np
+import pytest
+
+import nsfsi
+
+FD_STEP = 1e-6   # finite-difference step along each direction
+FD_TOL = 1e-6    # |adjoint - central difference| relative to the derivative (see fd_error)
+
+
+def solver(case, steps=None):
+    c = nsfsi.config_load(nsfsi.case_path(case))
+    if steps is not None:
+        c.stop_time_level = steps
+    return nsfsi.Solver(c)
+
+
+def fd_check(s, u0, gi, gu, du, di, h):
+    """(adjoint directional derivative, central difference, size of the derivative's terms) along (du, di).
+
+    The directional derivative of a random direction is a sum of about a million terms of random sign; the
+    last value, the 2-norm of those terms, is the derivative's expected size, which the sum itself can fall
+    far below when the terms happen to cancel (a seeded direction is not chosen to avoid that)."""
+    ad = (0.0 if du is None else float((gu * du).sum())) + (0.0 if di is None else float((gi * di).sum()))
+    terms = np.sqrt((0.0 if du is None else float(((gu * du) ** 2).sum()))
+                    + (0.0 if di is None else float(((gi * di) ** 2).sum())))
+    up = None if du is None else u0 + h * du
+    um = None if du is None else u0 - h * du
+    ip = None if di is None else 1 + h * di
+    im = None if di is None else 1 - h * di
+    fd = (s.adj_forward(up, ip) - s.adj_forward(um, im)) / (2 * h)
+    return ad, fd, terms
+
+
+def fd_error(ad, fd, terms):
+    """|adjoint - central difference| relative to the larger of |derivative| and its terms' 2-norm."""
+    return abs(fd - ad) / max(abs(ad), terms)
+
+
+def seeded_directions(s, u0, count, seed):
+    """count directions: the first three quarters perturb the level-0 field (each variable scaled by its
+    largest magnitude) together with the inflow profile, the rest the inflow profile alone (amplitude 10)."""
+    rng = np.random.default_rng(seed)
+    c = s.cfg
+    scale = np.maximum(np.abs(u0).max(axis=1), 1e-3)[:, None]
+    out = []
+    for d in range(count):
+        di = rng.standard_normal((int(c.NJ), int(c.NK)))
+        if d < 3 * count // 4:
+            out.append((rng.standard_normal(u0.shape) * scale, di))
+        else:
+            out.append((None, 10 * di))
+    return out
+
+
+@pytest.mark.gpu
+def test_adjoint_matches_finite_differences_64():
+    """64^3 channel with a sphere, 200 RK4 steps, J averaged over the last 50, 20 snapshots."""
+    with solver("adj64") as s:
+        u0 = s.download(range(5))
+        s.adj_configure(50, 20)
+        s.adj_forward()
+        gi, gu = s.adj_backward()
+        assert np.isfinite(gu).all() and np.isfinite(gi).all()
+        assert np.abs(gi).max() > 0 and np.abs(gu).max() > 0
+        worst = 0.0
+        for du, di in seeded_directions(s, u0, 16, seed=2024):
+            ad, fd, terms = fd_check(s, u0, gi, gu, du, di, FD_STEP)
+            rel = fd_error(ad, fd, terms)
+            worst = max(worst, rel)
+            assert rel <= FD_TOL, (ad, fd, terms, rel)
+        print("worst relative error over 16 directions: %.2e" % worst)
+
+
+@pytest.mark.gpu
+def test_adjoint_short_run_tight():
+    """32^3, 12 steps (no density-filter step is reached; the near-body filter runs every step), J over
+    the last 4 steps, 3 snapshots so that the schedule recurses: the gradient matches the central
+    difference at h = 1e-5 to 1e-8 in every direction, including single-node perturbations at the nodes of
+    largest sensitivity, up to the central difference's own rounding floor (16 eps |J| / h: a single node
+    moves J by little more than its last bits)."""
+    h = 1e-5
+    with solver("adj32", steps=12) as s:
+        u0 = s.download(range(5))
+        s.adj_configure(4, 3)
+        J = s.adj_forward()
+        gi, gu = s.adj_backward()
+        floor = 16 * np.finfo(float).eps * abs(J) / h
+        dirs = seeded_directions(s, u0, 4, seed=7)
+        # single nodes: the largest-gradient node of each variable
+        for f in range(5):
+            du = np.zeros_like(u0)
+            n = int(np.abs(gu[f]).argmax())
+            du[f, n] = max(abs(u0[f, n]), 1e-2)
+            dirs.append((du, None))
+        for du, di in dirs:
+            ad, fd, terms = fd_check(s, u0, gi, gu, du, di, h)
+            assert abs(fd - ad) <= 1e-8 * max(abs(ad), terms) + floor, (ad, fd, terms, floor)
+
+
+@pytest.mark.gpu
+def test_adjoint_schedule_does_not_change_the_gradient():
+    """The recomputation is deterministic and the adjoint kernels run in the same order whatever the
+    checkpointing schedule, so the gradient is bit-identical for 1, 4 and 40 snapshots (40 > steps: no
+    recomputation), and a second backward run after one forward run repeats it."""
+    ref = None
+    for snaps in (40, 4, 1):
+        with solver("adj32", steps=30) as s:
+            s.adj_configure(10, snaps)
+            s.adj_forward()
+            gi, gu = s.adj_backward()
+            gi2, gu2 = s.adj_backward()
+            assert np.array_equal(gi, gi2) and np.array_equal(gu, gu2)
+            if ref is None:
+                ref = (gi, gu)
+            else:
+                assert np.array_equal(gi, ref[0]) and np.array_equal(gu, ref[1]), snaps
+
+
+@pytest.mark.gpu
+def test_adjoint_dt_is_frozen_from_the_plain_run():
+    """The frozen dt sequence is the plain solver's dt history for the same run."""
+    with solver("adj32", steps=30) as s:
+        s.adj_configure(10, 4)
+        s.adj_forward()
+        dts = s.adj_dt()
+    with solver("adj32", steps=30) as p:
+        p.march(30)
+        p.sync()
+        hist = p.history()
+    assert np.array_equal(dts, hist[:, 1])
+
+
+@pytest.mark.gpu
+def test_adjoint_rejects_unsupported_cases():
+    """An end-time stop criterion (no fixed step count) and symmetry y faces are refused."""
+    c = nsfsi.config_load(nsfsi.case_path("adj32"))
+    c.stop_criterion = 1
+    with nsfsi.Solver(c) as s:
+        with pytest.raises(nsfsi.NsfError):
+            s.adj_configure(10, 4)
+    c = nsfsi.config_load(nsfsi.case_path("adj32"))
+    c.bc[1][0] = c.bc[1][1] = nsfsi.BC["symmetry"]
+    with nsfsi.Solver(c) as s:
+        with pytest.raises(nsfsi.NsfError):
+            s.adj_configure(10, 4)

@@ -208,15 +208,32 @@ def adjoint(terms, fields, lam, C):
 
 
 # ------------------------------------------------------------------------------------------- CUDA
+def _coef_expr(coef):
+    cs = []
+    for k, x in sorted(coef.items()):
+        c = " * ".join(["C.%s" % n for n in k]) if k else ""
+        if x == 1.0:
+            cs.append(c or "1.0")
+        elif x == -1.0:
+            cs.append("-" + (c or "1.0"))
+        else:
+            cs.append(("%r * " % x) + c if c else "%r" % x)
+    return "(" + " + ".join(cs) + ")" if len(cs) > 1 else cs[0]
+
+
+SUB_VALUES = 64  # most input values one block reads (64: one block per RHS node, which measured fastest)
+
+
 def emit_cuda(terms):
     lines = []
     w = lines.append
     w("// Generated by gen_rhs_adjoint.py from the RHS term table: do not edit. The transposed stencil of the")
     w("// right-hand side (rhs_eval, nsf_physics.cuh) in gather form: rhs_adjoint_gather(...) returns, for node")
-    w("// (i, j, k), the adjoint of each input quantity (RU, RV, RW, RE, u, v, w, p, T, mu, ka) summed over every")
-    w("// interior node whose RHS reads it. lam(e, b): RHS adjoint of equation e at linear node b (zero where no")
-    w("// RHS is taken); val(q, b): input quantity q at node b; inner(di, dj, dk): the node (i-di, j-dj, k-dk)")
-    w("// is one whose RHS was taken (its whole stencil then lies inside the grid).")
+    w("// X = (i, j, k), the adjoint of each input quantity (RU, RV, RW, RE, u, v, w, p, T, mu, ka) summed over")
+    w("// every interior node whose RHS reads it. lam(e, b): RHS adjoint of equation e at linear node b (zero where")
+    w("// no RHS is taken); val(q, b): input quantity q at node b; inner(di, dj, dk): the node (i-di, j-dj, k-dk)")
+    w("// is one whose RHS was taken (its whole stencil then lies inside the grid). The terms of one RHS node")
+    w("// are grouped by equation.")
     w("#ifndef NSF_RHS_ADJOINT_CUH")
     w("#define NSF_RHS_ADJOINT_CUH")
     w("")
@@ -227,40 +244,55 @@ def emit_cuda(terms):
     w("                                                   const Lam& lam, const Val& val, const Inner& inner,")
     w("                                                   double bar[%d]) {" % len(VARS))
     w("  for (int q = 0; q < %d; ++q) bar[q] = 0.0;" % len(VARS))
+    rel = sorted({(q, tuple(o2[a] - t[1][a] for a in range(3))) for t in terms for (q, o2) in t[4]},
+                 key=lambda x: (x[1], VIDX[x[0]]))
+    names = {x: "w%d" % n for n, x in enumerate(rel)}
     by_o = {}
     for t in terms:
         by_o.setdefault(t[1], []).append(t)
-    for o in sorted(by_o):
-        w("  if (inner(%d, %d, %d)) {" % o)
-        w("    const long long b = X - (%d * sI + %d * sJ + %d);" % o)
-        eqs_used = sorted({t[0] for t in by_o[o]})
-        for e in eqs_used:
-            w("    const double l%d = lam(%d, b);" % (e, e))
-        vals = sorted({f for t in by_o[o] for f in t[4]})
-        names = {}
-        for n, (q, o2) in enumerate(vals):
-            names[(q, o2)] = "v%d" % n
-            w("    const double v%d = val(%d, b + (%d * sI + %d * sJ + %d));  // %s %s" % (n, VIDX[q], *o2, q, o2))
-        for q in VARS:
-            parts = []
-            for e, _, qq, coef, others in by_o[o]:
-                if qq != q:
+    for o in sorted(by_o, key=lambda o: (sum(map(abs, o)), o)):
+        def rel_of(others):
+            return {(q2, tuple(o2[a] - o[a] for a in range(3))) for q2, o2 in others}
+
+        # outputs grouped so that no group reads more than SUB_VALUES input values: each group is a block
+        # of its own (the RHS node's values are then never all live at once)
+        used = {}
+        for _, _, q, _, others in by_o[o]:
+            used.setdefault(q, set()).update(rel_of(others))
+        groups = []
+        for q in sorted(used, key=lambda q: -len(used[q])):
+            for g in groups:
+                if len(g[1] | used[q]) <= SUB_VALUES:
+                    g[0].append(q)
+                    g[1] |= used[q]
+                    break
+            else:
+                groups.append([[q], set(used[q])])
+        for outs, vals in groups:
+            # a compiler fence per block: each block loads its own values (a value shared by several blocks
+            # would otherwise stay in a register from its first to its last use, and with all of them live
+            # the kernel runs out of registers)
+            w("  asm volatile(\"\" ::: \"memory\");")
+            w("  if (inner(%d, %d, %d)) {" % o)
+            w("    const long long b = X - (%d * sI + %d * sJ + %d);" % o)
+            for e in sorted({t[0] for t in by_o[o] if t[2] in outs}):
+                w("    const double l%d = lam(%d, b);" % (e, e))
+            for q, a in sorted(vals, key=lambda x: (x[1], VIDX[x[0]])):
+                w("    const double %s = val(%d, X + (%d * sI + %d * sJ + %d));  // %s %s"
+                  % (names[(q, a)], VIDX[q], *a, q, a))
+            for q in VARS:
+                if q not in outs:
                     continue
-                cs = []
-                for k, x in sorted(coef.items()):
-                    c = " * ".join(["C.%s" % n for n in k]) if k else ""
-                    if x == 1.0:
-                        cs.append(c or "1.0")
-                    elif x == -1.0:
-                        cs.append("-" + (c or "1.0"))
-                    else:
-                        cs.append(("%r * " % x) + c if c else "%r" % x)
-                cexpr = "(" + " + ".join(cs) + ")" if len(cs) > 1 else cs[0]
-                prod = " * ".join([names[f] for f in others])
-                parts.append("l%d * %s%s" % (e, cexpr, (" * " + prod) if prod else ""))
-            if parts:
+                parts_by_e = {}
+                for e, _, qq, coef, others in by_o[o]:
+                    if qq != q:
+                        continue
+                    prod = " * ".join(names[(q2, tuple(o2[a] - o[a] for a in range(3)))] for q2, o2 in others)
+                    parts_by_e.setdefault(e, []).append(_coef_expr(coef) + ((" * " + prod) if prod else ""))
+                parts = ["l%d * (%s)" % (e, " + ".join(g)) if len(g) > 1 else "l%d * %s" % (e, g[0])
+                         for e, g in sorted(parts_by_e.items())]
                 w("    bar[%d] += %s;  // %s" % (VIDX[q], " + ".join(parts), q))
-        w("  }")
+            w("  }")
     w("}")
     w("")
     w("}  // namespace nsf")

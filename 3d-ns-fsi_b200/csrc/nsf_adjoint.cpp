@@ -264,10 +264,19 @@ struct SnapHook : StepHook {
   AdjCtx* a;
   const StepCtl& R;
   cudaError_t err = cudaSuccess;
+  const double* src[kMaxCopies];
+  double* dst[kMaxCopies];
+  long long words[kMaxCopies];
+  int n = 0;
   SnapHook(nsf_solver* s_, AdjCtx* a_, const StepCtl& r) : s(s_), a(a_), R(r) {}
-  void copy(double* dst, const double* src, size_t words) {
-    if (err == cudaSuccess)
-      err = cudaMemcpyAsync(dst, src, words * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
+  void add(double* d, const double* sr, size_t w) {
+    src[n] = sr;
+    dst[n] = d;
+    words[n++] = (long long)w;
+  }
+  void flush() {
+    launch_copies(src, dst, words, n, s->nSM, s->stream);
+    n = 0;
   }
   void after_prologue() override {
     if (err == cudaSuccess) err = cudaMemcpyAsync(a->dCur, s->dCtl, sizeof(StepCtl), cudaMemcpyDeviceToDevice, s->stream);
@@ -275,24 +284,56 @@ struct SnapHook : StepHook {
   void before_stage(int q) override {
     const size_t N = nd(s);
     double* base = a->stageSnap + q * per_stage(s);
-    for (int f = 0; f < 5; ++f) copy(base + f * N, R.I[q][f], N);
-    copy(base + 5 * N, R.R[q], N);
-    if (nf(s)) copy(base + 11 * N, s->hGrid.fpre, 2 * nf(s));
+    for (int f = 0; f < 5; ++f) add(base + f * N, R.I[q][f], N);
+    add(base + 5 * N, R.R[q], N);
+    if (nf(s)) add(base + 11 * N, s->hGrid.fpre, 2 * nf(s));
+    flush();
   }
   void before_edges(int q) override {
     const size_t N = nd(s);
     double* base = a->stageSnap + q * per_stage(s);
-    for (int f = 0; f < 5; ++f) copy(base + (6 + f) * N, R.O[q][f], N);
+    for (int f = 0; f < 5; ++f) add(base + (6 + f) * N, R.O[q][f], N);
+    flush();
+  }
+};
+
+// Phases of an adjoint step, for nsf_adj_profile_step.
+enum AdjPhase { PH_RECOMPUTE, PH_OBJECTIVE, PH_GHOST, PH_FILTER, PH_EDGE, PH_SOLID, PH_PREPARE, PH_RHS, PH_DFILTER,
+                PH_COUNT };
+
+// Events recorded between the phases of an eagerly launched adjoint step.
+struct PhaseTimer {
+  cudaStream_t st;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> phase;
+  void mark(int ph) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, st);
+    ev.push_back(e);
+    phase.push_back(ph);
+  }
+  void collect(double* ms) {
+    for (size_t q = 1; q < ev.size(); ++q) {
+      float t = 0;
+      if (cudaEventElapsedTime(&t, ev[q - 1], ev[q]) == cudaSuccess) ms[phase[q]] += t;
+    }
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
   }
 };
 
 // Enqueues the adjoint of a step with roles R: the working state holds U_k on entry (U_{k+1} on exit);
 // the adjoint arrays hold the adjoint of U_{k+1} on entry and of U_k on exit. objective: F_x(U_{k+1})
-// enters J.
-nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool objective) {
+// enters J. pt: NULL, or events between the phases (eager launches only).
+nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool objective, PhaseTimer* pt = nullptr) {
+  auto mark = [&](int ph) {
+    if (pt) pt->mark(ph);
+  };
   const StepCtl* dR = a->dCur;
   SnapHook hook(s, a, R);
+  mark(-1);
   enqueue_step_hooked(s->dGrid, s->hGrid, s->plan, s->stream, &hook);
+  mark(PH_RECOMPUTE);
   if (hook.err != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint recomputation: ") + cudaGetErrorString(hook.err));
   CKA(cudaGetLastError());
   const Grid& G = s->hGrid;
@@ -306,6 +347,7 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
       A.lamO[f] = lamOf(s, a, phys(s, R.O[3][f], f), f);
     }
     launch_adj_objective(s->dGrid, A, G.nGhost, a->dNx, a->dA, 1.0 / a->navg, nSM, st);
+    mark(PH_OBJECTIVE);
   }
   for (int q = 3; q >= 0; --q) {
     const double* snap = a->stageSnap + q * per_stage(s);
@@ -321,22 +363,30 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     A.lamFnew = a->lamFnew;
     // near-body filter and ghosts
     launch_adj_ghost(s->dGrid, A, G.nGhost, G.nFilter, a->ipbar, a->cnode, a->coff, a->cent, a->ncell, nSM, st);
+    mark(PH_GHOST);
     launch_adj_filter(s->dGrid, A, a->fsNodes, a->nfs, G.nFilter, nSM, st);
+    mark(PH_FILTER);
     // edge conditions: z, y, then x (reads the stage output before the edge conditions)
     for (int f = 0; f < 5; ++f) A.val[f] = snap + (6 + f) * N;
     for (int axis = 2; axis >= 0; --axis)
       launch_adj_edge(s->dGrid, A, s->plan, axis, dR, q, a->fbar, a->lamInflow, a->inletX, st);
+    mark(PH_EDGE);
     launch_adj_solid(s->dGrid, A, G.nSolid, R.copyMask[q], nSM, st);
+    mark(PH_SOLID);
     // stage kernel: RK4 combine, transposed RHS, primitives of the stage input
     for (int f = 0; f < 5; ++f) A.val[f] = snap + f * N;
     A.valR = snap + 5 * N;
     A.valFpre = snap + 11 * N;
-    launch_adj_stage(s->dGrid, A, (long long)N, q, dR, a->tmpLam, a->tmpV, nSM, st);
+    launch_adj_prepare(s->dGrid, G, A, q, dR, a->tmpLam, a->tmpV, nSM, st);
+    mark(PH_PREPARE);
+    launch_adj_rhs(s->dGrid, G, A, a->tmpLam, a->tmpV, st);
+    mark(PH_RHS);
   }
   if (R.filterNow) {
     double* dst = lamOf(s, a, phys(s, R.gfDst, 0), 0);
     double* src = lamOf(s, a, phys(s, R.gfSrc, 0), 0);
     launch_adj_density_filter(s->dGrid, (long long)N, dst, dst, src, nSM, st);
+    mark(PH_DFILTER);
   }
   CKA(cudaGetLastError());
   return NSF_OK;
@@ -567,6 +617,24 @@ nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* 
     for (size_t q = 0; q < S.NJ * S.NK; ++q) g_inflow[q] *= dJ;
   }
   return NSF_OK;
+}
+
+nsf_status nsf_adj_profile_step(nsf_solver* s, uint64_t step, double* ms) {
+  if (!s || !ms) return NSF_ERR_ARG;
+  AdjCtx* a = s->adj;
+  if (!a || !a->haveForward) return fail(s, NSF_ERR_STATE, "nsf_adj_profile_step needs a preceding nsf_adj_forward");
+  if (step >= uint64_t(a->nsteps)) return fail(s, NSF_ERR_ARG, "nsf_adj_profile_step: step out of range");
+  CKA(cudaSetDevice(s->device));
+  // the state at `step`: from level 0 (slot 0 keeps it for the whole forward/backward cycle)
+  nsf_status st = restore(s, a, 0);
+  if (st == NSF_OK) st = advance(s, int(step));
+  if (st != NSF_OK) return st;
+  PhaseTimer pt{s->stream, {}, {}};
+  st = enqueue_adjoint_step(s, a, a->hist[step], int(step) + 1 > a->nsteps - a->navg, &pt);
+  CKA(cudaStreamSynchronize(s->stream));
+  for (int q = 0; q < PH_COUNT; ++q) ms[q] = 0;
+  pt.collect(ms);
+  return st;
 }
 
 nsf_status nsf_adj_get_dt(nsf_solver* s, double* dts, uint64_t* count) {

@@ -23,13 +23,6 @@
 namespace nsf {
 namespace {
 
-__device__ __forceinline__ void ijk_of(const Grid& G, long long n, int& i, int& j, int& k) {
-  i = int(n / G.sI);
-  const long long r = n - (long long)i * G.sI;
-  j = int(r / G.sJ);
-  k = int(r - (long long)j * G.sJ);
-}
-
 // Pressure of conserved values (prims_of's p).
 __device__ __forceinline__ double pressure(const Consts& C, const double u[5], double g[5]) {
   const double r1 = 1.0 / (u[0] + 1.0);
@@ -295,64 +288,98 @@ __global__ void k_adj_solid(const Grid* __restrict__ gp, AdjPtrs A, int mask) {
 // ------------------------------------------------------------------------------------------ stage
 // RK4 combine at the interior nodes: s = 0: O = U0 + inc k, acc = k; s = 1, 2: O = U0 + inc k,
 // acc += 2 k; s = 3: O = U0 + dt/6 (acc + k). Writes the RHS adjoint lam (zero elsewhere beforehand).
-__global__ void k_adj_combine(const Grid* __restrict__ gp, AdjPtrs A, int s, const StepCtl* __restrict__ roles,
-                              double* __restrict__ lam) {
+// Before the stage kernel's adjoint: the RK4 combine's adjoint and the stage's RHS input quantities.
+// Combine (interior fluid nodes; lam is zero elsewhere): with o = the adjoint of the stage output,
+//   stage 1:    k = dt/2 o + acc, acc = 0      stages 2, 3: k = inc o + 2 acc      stage 4: k = dt/6 o, acc += k
+// (inc = dt/2, dt), lam = k is the adjoint of the stage's RHS; U0 receives o, o is consumed.
+// Values: momenta and rho_E from I, density from R, filter nodes' density and rho_E from fpre (for the
+// primitives), then the primitives and transport properties, as the stage kernel stages them.
+__global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, const StepCtl* __restrict__ roles,
+                              double* __restrict__ lam, double* __restrict__ V) {
   const Grid& G = *gp;
   const double dtUsed = roles->dtUsed;
   const double inc = s == 2 ? dtUsed : dtUsed / 2, dtF = dtUsed / 6;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x) {
-    if ((G.type[n] & TYPE_MASK) != FLUID_INTERIOR) continue;
+    // every load first (about twenty independent loads in flight per thread), then the arithmetic
+    const uint8_t ty = G.type[n];
+    const bool interior = (ty & TYPE_MASK) == FLUID_INTERIOR;
+    const double m1 = A.val[1][n], m2 = A.val[2][n], m3 = A.val[3][n], e4 = A.val[4][n];
+    double rho = A.valR[n], rE = e4;
+    double o[5], acc[5], u0[5];
+    if (interior)
+      for (int f = 0; f < 5; ++f) {
+        o[f] = A.lamO[f][n];
+        acc[f] = A.lamAcc[f][n];
+        u0[f] = A.lamU0[f][n];
+      }
+    if (ty & FILTER_BIT) {
+      const int f = G.fidx[n];
+      rho = A.valFpre[2 * f];
+      rE = A.valFpre[2 * f + 1];
+    }
+    const Prim pr = prims_of(G.C, rho, m1, m2, m3, rE);
+    const double q[11] = {m1, m2, m3, e4, pr.u, pr.v, pr.w, pr.p, pr.T, pr.mu, pr.ka};
+    for (int v = 0; v < 11; ++v) V[v * G.N + n] = q[v];
+    if (!interior) {
+      for (int f = 0; f < 5; ++f) lam[f * G.N + n] = 0.0;
+      continue;
+    }
     for (int f = 0; f < 5; ++f) {
-      const double o = A.lamO[f][n];
       double k;
       if (s == 0) {
-        k = inc * o + A.lamAcc[f][n];
+        k = inc * o[f] + acc[f];
         A.lamAcc[f][n] = 0.0;
       } else if (s < 3) {
-        k = inc * o + 2 * A.lamAcc[f][n];
+        k = inc * o[f] + 2 * acc[f];
       } else {
-        k = dtF * o;
-        A.lamAcc[f][n] += dtF * o;
+        k = dtF * o[f];
+        A.lamAcc[f][n] = acc[f] + dtF * o[f];
       }
       lam[f * G.N + n] = k;
-      A.lamU0[f][n] += o;
+      A.lamU0[f][n] = u0[f] + o[f];
       A.lamO[f][n] = 0.0;
     }
   }
 }
 
-// Input quantities of the stage's RHS at every node, as the stage kernel stages them: momenta and
-// rho_E from I, density from R, filter nodes' density and rho_E from fpre (for the primitives).
-__global__ void k_adj_values(const Grid* __restrict__ gp, AdjPtrs A, double* __restrict__ V) {
-  const Grid& G = *gp;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x) {
-    double rho = A.valR[n], rE = A.val[4][n];
-    if (G.type[n] & FILTER_BIT) {
-      const int f = G.fidx[n];
-      rho = A.valFpre[2 * f];
-      rE = A.valFpre[2 * f + 1];
-    }
-    const Prim pr = prims_of(G.C, rho, A.val[1][n], A.val[2][n], A.val[3][n], rE);
-    const double q[11] = {A.val[1][n], A.val[2][n], A.val[3][n], A.val[4][n], pr.u, pr.v, pr.w, pr.p, pr.T, pr.mu, pr.ka};
-    for (int v = 0; v < 11; ++v) V[v * G.N + n] = q[v];
-  }
+// Several device-to-device copies in one launch (blockIdx.y: the copy).
+struct CopySet {
+  const double* src[kMaxCopies];
+  double* dst[kMaxCopies];
+  long long words[kMaxCopies];
+};
+
+__global__ void k_copy_set(CopySet S) {
+  const int c = blockIdx.y;
+  const double* __restrict__ src = S.src[c];
+  double* __restrict__ dst = S.dst[c];
+  const long long n = S.words[c];
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x)
+    dst[m] = src[m];
 }
 
 // Transposed RHS (generated gather) and the chain rule through the primitive / transport values.
-__global__ void __launch_bounds__(256, 2) k_adj_rhs(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ lam,
-                          const double* __restrict__ V) {
+// One node per thread: threads run along k (32 per row), 8 rows of (i, j) per block (no loop, so nothing is
+// kept in registers across nodes).
+constexpr int kAdjRhsRows = 8;    // rows of 32 nodes per block
+constexpr int kAdjRhsBlocks = 2;  // resident blocks per SM the register budget is set for
+__global__ void __launch_bounds__(32 * kAdjRhsRows, kAdjRhsBlocks) k_adj_rhs(const Grid* __restrict__ gp, const __grid_constant__ Consts C,
+                                                    AdjPtrs A, const double* __restrict__ lam,
+                                                    const double* __restrict__ V) {
   const Grid& G = *gp;
-  const Consts& C = G.C;
   const long long N = G.N, sI = G.sI, sJ = G.sJ;
-  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < N; m += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    ijk_of(G, m, i, j, k);
-    if (k >= G.NK) continue;
+  const int NI = G.NI, NJ = G.NJ, NK = G.NK;
+  const int r = blockIdx.x * blockDim.y + threadIdx.y, k = blockIdx.y * 32 + threadIdx.x;
+  if (r < NI * NJ && k < NK) {
+    const int i = r / NJ, j = r - i * NJ;
+    const long long m = i * sI + j * sJ + k;
     auto lamAt = [&](int e, long long b) { return lam[e * N + b]; };
     auto valAt = [&](int q, long long b) { return V[q * N + b]; };
+    // the per-RHS-node conditions also bound the compiler's scheduling regions (without them it
+    // interleaves all 19 blocks and runs out of registers)
     auto inner = [&](int di, int dj, int dk) {
       const int a = i - di, b = j - dj, c = k - dk;
-      return a >= 1 && a <= G.NI - 2 && b >= 1 && b <= G.NJ - 2 && c >= 1 && c <= G.NK - 2;
+      return a >= 1 && a <= NI - 2 && b >= 1 && b <= NJ - 2 && c >= 1 && c <= NK - 2;
     };
     double bar[11];
     rhs_adjoint_gather(C, m, sI, sJ, lamAt, valAt, inner, bar);
@@ -487,10 +514,10 @@ void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int 
                      double* fbar, double* lamInflow, bool inletGather, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   dim3 grid(L.edgeGrid[axis][0], L.edgeGrid[axis][1], 2);
-  k_adj_edge<<<grid, dim3(32, 8), 0, st>>>(dg, A, axis, roles, s, fbar, lamInflow);
+  k_adj_edge<<<grid, dim3(32, kEdgeRows), 0, st>>>(dg, A, axis, roles, s, fbar, lamInflow);
   if (axis == 0 && inletGather) {
     dim3 g2(L.edgeGrid[0][0], L.edgeGrid[0][1], 6);
-    k_adj_inlet_gather<<<g2, dim3(32, 8), 0, st>>>(dg, A, fbar);
+    k_adj_inlet_gather<<<g2, dim3(32, kEdgeRows), 0, st>>>(dg, A, fbar);
   }
 }
 
@@ -499,13 +526,30 @@ void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, in
     k_adj_solid<<<blocks_for(nSolid, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, mask);
 }
 
-void launch_adj_stage(const Grid* dg, const AdjPtrs& A, long long N, int s, const StepCtl* roles, double* lam,
-                      double* V, int nSM, void* stream) {
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  cudaMemsetAsync(lam, 0, 5 * N * sizeof(double), st);
-  k_adj_combine<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, s, roles, lam);
-  k_adj_values<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, V);
-  k_adj_rhs<<<blocks_for(N, nSM), 256, 0, st>>>(dg, A, lam, V);
+void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, double* lam,
+                        double* V, int nSM, void* stream) {
+  k_adj_prepare<<<blocks_for(hg.N, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, s, roles, lam, V);
+}
+
+void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V,
+                    void* stream) {
+  const dim3 grid((hg.NI * hg.NJ + kAdjRhsRows - 1) / kAdjRhsRows, (hg.NK + 31) / 32);
+  k_adj_rhs<<<grid, dim3(32, kAdjRhsRows), 0, static_cast<cudaStream_t>(stream)>>>(dg, hg.C, A, lam, V);
+}
+
+void launch_copies(const double* const* src, double* const* dst, const long long* words, int count, int nSM,
+                   void* stream) {
+  if (count <= 0) return;
+  CopySet S{};
+  long long most = 1;
+  for (int c = 0; c < count; ++c) {
+    S.src[c] = src[c];
+    S.dst[c] = dst[c];
+    S.words[c] = words[c];
+    most = words[c] > most ? words[c] : most;
+  }
+  const long long b = (most + 255) / 256, cap = 2LL * nSM;
+  k_copy_set<<<dim3(unsigned(b < cap ? b : cap), count), 256, 0, static_cast<cudaStream_t>(stream)>>>(S);
 }
 
 void launch_adj_density_filter(const Grid* dg, long long N, const double* lamDstConst, double* lamDst, double* lamSrc,

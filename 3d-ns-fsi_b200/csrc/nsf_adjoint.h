@@ -34,10 +34,18 @@ void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes,
 void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
                      double* fbar, double* lamInflow, bool inletGather, void* stream);
 void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, int nSM, void* stream);
-void launch_adj_stage(const Grid* dg, const AdjPtrs& A, long long N, int s, const StepCtl* roles, double* lam,
-                      double* V, int nSM, void* stream);
+// The stage kernel's adjoint: prepare = RK4 combine adjoint into lam and the RHS input quantities into V
+// (11 x N); rhs = transposed RHS gather and the chain rule into the stage input's adjoints.
+void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, double* lam,
+                        double* V, int nSM, void* stream);
+void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V,
+                    void* stream);
 void launch_adj_density_filter(const Grid* dg, long long N, const double* lamDstConst, double* lamDst, double* lamSrc,
                                int nSM, void* stream);
+// count (<= kMaxCopies) device-to-device copies of words[c] doubles in one launch.
+constexpr int kMaxCopies = 8;
+void launch_copies(const double* const* src, double* const* dst, const long long* words, int count, int nSM,
+                   void* stream);
 
 }  // namespace nsf
 #endif

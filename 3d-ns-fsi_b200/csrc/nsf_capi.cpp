@@ -454,7 +454,7 @@ nsf_status build_device(nsf_solver* s) {
         n2 = std::max(n2, int(hi[ax2] - lo[ax2] + 1));
       }
     L.edgeGrid[a][0] = (n2 + 31) / 32;
-    L.edgeGrid[a][1] = (n1 + 7) / 8;
+    L.edgeGrid[a][1] = (n1 + kEdgeRows - 1) / kEdgeRows;
     L.edgeGrid[a][2] = 2;
   }
   L.hasFilter = G.nFilter > 0;

@@ -125,6 +125,10 @@ struct StageItem {
 };
 
 // Launch geometry of one step, fixed at initialisation.
+// Edge-condition kernels: blocks of 32 x kEdgeRows threads over a face (small blocks spread a face's
+// few thousand nodes over many SMs).
+constexpr int kEdgeRows = 2;
+
 struct LaunchPlan {
   int nSM;
   int tile;  // StageTile
@@ -132,7 +136,7 @@ struct LaunchPlan {
   int nItems;
   StageItem* items;  // device; the items of CTA b are items[ctaStart[b] .. ctaStart[b + 1])
   int* ctaStart;     // device, stageBlocks + 1 entries
-  int edgeGrid[3][3];  // per axis: grid x, y, z
+  int edgeGrid[3][3];  // per axis: grid x, y, z of blocks of 32 x kEdgeRows threads
   int filterBlocks, ghostBlocks, solidBlocks, gfBlocks;
   int nSlots;
   bool hasBodies;

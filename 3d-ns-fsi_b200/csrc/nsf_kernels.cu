@@ -612,7 +612,7 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
     if (hook) hook->before_edges(s);
     for (int a = 0; a < 3; ++a) {
       dim3 grid(L.edgeGrid[a][0], L.edgeGrid[a][1], 2 * M);
-      k_edge_bc<<<grid, dim3(32, 8), 0, st>>>(dg, s, a);
+      k_edge_bc<<<grid, dim3(32, kEdgeRows), 0, st>>>(dg, s, a);
       ++launches;
     }
     if (L.hasFilter) {

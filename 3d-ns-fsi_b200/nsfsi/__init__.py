@@ -106,6 +106,7 @@ def lib():
         "nsf_adj_forward": (i32, [vp, dp, dp, dp]),
         "nsf_adj_backward": (i32, [vp, ctypes.c_double, dp, dp]),
         "nsf_adj_get_dt": (i32, [vp, dp, ctypes.POINTER(u64)]),
+        "nsf_adj_profile_step": (i32, [vp, u64, dp]),
         "nsf_last_error": (ctypes.c_char_p, [vp]),
         "nsf_destroy": (None, [vp]),
     }
@@ -282,6 +283,14 @@ class Solver:
         gu = np.zeros((5, self.N))
         self._check(lib().nsf_adj_backward(self.h, dJ, _dp(gi), _dp(gu)))
         return gi, gu
+
+    ADJ_PHASES = ("recompute", "objective", "ghost", "filter", "edge", "solid", "prepare", "rhs", "density_filter")
+
+    def adj_profile_step(self, step=0):
+        """{phase: device ms} of one eagerly launched adjoint step (after adj_forward)."""
+        ms = np.zeros(len(self.ADJ_PHASES))
+        self._check(lib().nsf_adj_profile_step(self.h, step, _dp(ms)))
+        return dict(zip(self.ADJ_PHASES, ms.tolist()))
 
     def adj_dt(self):
         n = ctypes.c_uint64()

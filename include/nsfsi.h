@@ -225,6 +225,11 @@ nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow
 nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* g_u0);
 /* The frozen dt sequence (count values: dt of step n). */
 nsf_status nsf_adj_get_dt(nsf_solver* s, double* dts, uint64_t* count);
+/* Device time (ms, CUDA events) of the phases of one adjoint step, launched eagerly after a forward run:
+ * ms[0] recomputation of the step with its stage snapshots, [1] objective, [2] ghost nodes, [3] near-body
+ * filter, [4] edge conditions, [5] solid-node copies, [6] RK4 combine and RHS input quantities,
+ * [7] transposed RHS, [8] density filter (summed over the four stages). Gradients are unaffected. */
+nsf_status nsf_adj_profile_step(nsf_solver* s, uint64_t step, double* ms);
 
 /* Text of the last error on this handle (static storage owned by the handle). */
 const char* nsf_last_error(nsf_solver* s);

@@ -76,3 +76,10 @@ def test_adjoint_gather_is_the_transpose():
         jvp = sum(((rp[e] - rm[e]) / (2 * h) * lam[e]).sum() for e in range(5))
         vjp = (bar[q] * d).sum()
         assert abs(jvp - vjp) <= 1e-7 * max(abs(vjp), 1.0), (q, jvp, vjp)
+
+
+def test_generated_gather_is_up_to_date():
+    """The committed CUDA gather (nsf_rhs_adjoint.cuh) is what the generator emits from the term table."""
+    text = gen.emit_cuda(gen.adjoint_terms(gen.rhs_polys()))
+    with open(os.path.join(ROOT, "3d-ns-fsi_b200", "csrc", "nsf_rhs_adjoint.cuh")) as f:
+        assert f.read() == text

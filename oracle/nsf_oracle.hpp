@@ -132,6 +132,9 @@ class Solver {
   // amplification removed, as the comparison point for implementations that round differently.
   bool exactImageSolve = false;
   size_t stepCounter = 0;
+  // Optional x-inlet velocity profile factor, index j * NK + k (the inlet velocity is min(1, t/10) M_0 times
+  // the factor; empty: 1, the reference's uniform inflow). A parameter of the adjoint's gradient checks.
+  std::vector<T> inflowProfile;
 
   explicit Solver(const Params& p, const Case& c)
       : P(p), C(c), NI(p.NI), NJ(p.NJ), NK(p.NK), N(p.NI * p.NJ * p.NK) {
@@ -700,17 +703,20 @@ class Solver {
         rho[idx] = 2 * rho[a1] - rho[a2];
       });
       inletFilter(e);
-      double vel = std::min(1., t / 10.) * P.M_0;
-      if (e.side == 1) vel *= -1;
-      double uu = 0, vv = 0, ww = 0;
-      if (e.axis == 0) uu = vel;
-      if (e.axis == 1) vv = vel;
-      if (e.axis == 2) ww = vel;
-      forOwned(e, [&](size_t, size_t, size_t, size_t idx) {
+      const double ramp = std::min(1., t / 10.) * P.M_0;
+      const bool profiled = e.axis == 0 && !inflowProfile.empty();
+      forOwned(e, [&](size_t, size_t j, size_t kk, size_t idx) {
+        T vel = T(ramp);
+        if (profiled) vel = vel * inflowProfile[j * NK + kk];
+        if (e.side == 1) vel = vel * -1.0;
+        T uu = T(0.0), vv = T(0.0), ww = T(0.0);
+        if (e.axis == 0) uu = vel;
+        if (e.axis == 1) vv = vel;
+        if (e.axis == 2) ww = vel;
         T r = rho[idx];
         T Tt = T(0.0);
         T p = (Tt * (1 + r) + r) / P.Gamma;
-        T pr[5] = {T(uu), T(vv), T(ww), p, Tt}, cv[5], m, kap;
+        T pr[5] = {uu, vv, ww, p, Tt}, cv[5], m, kap;
         deriveConserved(pr, cv);
         deriveTransport(pr, m, kap);
         setAll(idx, cv, pr, m, kap);
@@ -1056,6 +1062,41 @@ class Solver {
       for (int f = 1; f < 5; ++f) normHistory(f);
   }
   void normHistory(int f) { normHist[f].push_back(val(normOfChange(old[f], cons[f]))); }
+
+  // The adjoint's objective term: the x-force of the pressure on the bodies, -dA sum_g p(U_g) n_x(g) over
+  // the ghost nodes (p from the ghost's conserved values, as the primitive variables are derived; n: the
+  // body's unit normal at the ghost's body-intercept point, in the body's cross-section for cylinders;
+  // dA = (dx dy dz)^(2/3)).
+  T forceX() const {
+    const double dA = std::pow(dx * dy * dz, 2.0 / 3.0);
+    T s = T(0.0);
+    for (const Body& b : bodies)
+      for (const Ghost& g : b.ghosts) {
+        double d[3] = {g.bi.x - (b.sphere ? b.s.cx : b.c.cx), g.bi.y - (b.sphere ? b.s.cy : b.c.cy),
+                       g.bi.z - (b.sphere ? b.s.cz : b.c.cz)};
+        if (!b.sphere) d[b.c.axis] = 0;
+        const double len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        const double nx = len > 0 ? d[0] / len : 0.0;
+        const size_t n = id(g.i, g.j, g.k);
+        const T rho = cons[0][n], r1 = 1.0 / (rho + 1.0);
+        const T u = cons[1][n] * r1, v = cons[2][n] * r1, w = cons[3][n] * r1;
+        const T p = (P.Gamma - 1) * (cons[4][n] - (rho + 1.0) * 0.5 * (u * u + v * v + w * w));
+        s += -dA * nx * p;
+      }
+    return s;
+  }
+
+  // Level-0 state of a run from a given conserved field (every node): the primitive and transport values
+  // are derived from it at every node; the other buffers stay zero.
+  void setInitialConserved(const std::vector<T> u0[5]) {
+    for (size_t idx = 0; idx < N; ++idx) {
+      T cv[5], pr[5], m, kap;
+      for (int f = 0; f < 5; ++f) cv[f] = u0[f][idx];
+      derivePrimitive(cv, pr);
+      deriveTransport(pr, m, kap);
+      setAll(idx, cv, pr, m, kap);
+    }
+  }
 
   static double val(double x) { return x; }
   template <class U>

@@ -11,6 +11,7 @@
 #include <string>
 
 #include "libconfig.h++"
+#include "nsf_dual.hpp"
 #include "nsf_oracle.hpp"
 
 using nsfo::Solver;
@@ -241,5 +242,54 @@ void nsfo_destroy(void* hp) {
   auto* h = static_cast<Handle*>(hp);
   delete h->s;
   delete h;
+}
+
+// The adjoint's objective and its directional derivative by forward-mode (dual-number) differentiation of
+// a whole run: J = (1/navg) sum over the last navg of nsteps steps of the bodies' x-force (forceX), from
+// the level-0 conserved field u0 + eps du0 (5 x N, every node; NULL u0: the case's initial condition) and
+// the x-inlet profile factor inflow + eps dinflow (NJ x NK; NULL inflow: 1), with the dt sequence dts
+// (nsteps values) frozen. NULL du0 / dinflow: no derivative along that parameter. Returns 0, or 1 with
+// the message in err.
+int nsfo_dual_objective(const char* cfgText, const double* u0, const double* du0, const double* inflow,
+                        const double* dinflow, const double* dts, uint64_t nsteps, uint64_t navg, double* J,
+                        double* dJ, char* err, int errlen) {
+  using nsfo::Dual;
+  try {
+    libconfig::Config cfg;
+    cfg.readString(cfgText);
+    nsfo::Params P;
+    nsfo::Case C;
+    readParams(cfg, P, C);
+    Solver<Dual> s(P, C);
+    s.initialize();
+    const size_t N = s.N;
+    if (u0) {
+      std::vector<Dual> U[5];
+      for (int f = 0; f < 5; ++f) {
+        U[f].resize(N);
+        for (size_t q = 0; q < N; ++q) U[f][q] = Dual(u0[f * N + q], du0 ? du0[f * N + q] : 0.0);
+      }
+      s.setInitialConserved(U);
+    }
+    if (inflow) {
+      s.inflowProfile.resize(s.NJ * s.NK);
+      for (size_t q = 0; q < s.NJ * s.NK; ++q) s.inflowProfile[q] = Dual(inflow[q], dinflow ? dinflow[q] : 0.0);
+    }
+    s.frozenDt.assign(dts, dts + nsteps);
+    s.dt = Dual(s.frozenDt[0]);
+    double t = 0;
+    unsigned long level = 0;
+    Dual acc(0.0);
+    for (uint64_t n = 0; n < nsteps; ++n) {
+      s.marchTimeStep(t, level);
+      if (n + 1 > nsteps - navg) acc += s.forceX() * (1.0 / double(navg));
+    }
+    *J = acc.v;
+    *dJ = acc.d;
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", e.what());
+    return 1;
+  }
 }
 }

@@ -54,12 +54,30 @@ def lib():
         L.nsfo_history.restype = u64
         L.nsfo_history.argtypes = [vp, ctypes.POINTER(dbl)]
         L.nsfo_destroy.argtypes = [vp]
+        L.nsfo_dual_objective.argtypes = [ctypes.c_char_p] + [ctypes.POINTER(dbl)] * 5 + [u64, u64] + \
+            [ctypes.POINTER(dbl)] * 2 + [ctypes.c_char_p, ctypes.c_int]
         _lib = L
     return _lib
 
 
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def dual_objective(cfg_text, dts, navg, u0=None, du0=None, inflow=None, dinflow=None):
+    """(J, dJ): the adjoint's objective (the bodies' x-force averaged over the last navg steps of a run of
+    len(dts) steps with that frozen dt sequence) and its exact directional derivative along (du0, dinflow)
+    by dual-number differentiation of the oracle (nsfo_dual_objective)."""
+    keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+            for a in (u0, du0, inflow, dinflow)]
+    dts = np.ascontiguousarray(dts, dtype=np.float64)
+    J, dJ = ctypes.c_double(), ctypes.c_double()
+    err = ctypes.create_string_buffer(512)
+    st = lib().nsfo_dual_objective(cfg_text.encode(), *[None if a is None else _dp(a) for a in keep], _dp(dts),
+                                   len(dts), navg, ctypes.byref(J), ctypes.byref(dJ), err, 512)
+    if st:
+        raise RuntimeError(err.value.decode())
+    return J.value, dJ.value
 
 
 class Oracle:

@@ -83,3 +83,24 @@ def test_generated_gather_is_up_to_date():
     text = gen.emit_cuda(gen.adjoint_terms(gen.rhs_polys()))
     with open(os.path.join(ROOT, "3d-ns-fsi_b200", "csrc", "nsf_rhs_adjoint.cuh")) as f:
         assert f.read() == text
+
+
+def test_dual_number_oracle_matches_its_finite_differences():
+    """The oracle's dual-number run (nsfo_dual_objective) gives the directional derivative of the adjoint's
+    objective: on the small sphere case (12 steps, J over the last 4) it matches the oracle's own central
+    difference at h = 1e-5 to 1e-7, along a joint perturbation of the level-0 field and the inflow profile."""
+    cfg = open(os.path.join(ROOT, "tests/golden/cases/sphere_small.cfg")).read()
+    o = po.Oracle(cfg)
+    u0 = o.fields()[:5].copy()
+    o.march(12)
+    dts = o.history()[:, 1].copy()
+    o.close()
+    rng = np.random.default_rng(3)
+    du = rng.standard_normal(u0.shape) * np.maximum(np.abs(u0).max(axis=1), 1e-3)[:, None]
+    di = rng.standard_normal((16, 16))
+    J, dJ = po.dual_objective(cfg, dts, 4, u0=u0, du0=du, inflow=np.ones((16, 16)), dinflow=di)
+    assert J == po.dual_objective(cfg, dts, 4)[0]  # the case's own initial condition, factor 1
+    h = 1e-5
+    Jp = po.dual_objective(cfg, dts, 4, u0=u0 + h * du, inflow=1 + h * di)[0]
+    Jm = po.dual_objective(cfg, dts, 4, u0=u0 - h * du, inflow=1 - h * di)[0]
+    assert abs((Jp - Jm) / (2 * h) - dJ) <= 1e-7 * abs(dJ), (dJ, (Jp - Jm) / (2 * h))

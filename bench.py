@@ -194,7 +194,8 @@ def adjoint_leg(device, nsfsi, reps=3):
             fd = (s.adj_forward(u0 + h * du, 1 + h * di) - s.adj_forward(u0 - h * du, 1 - h * di)) / (2 * h)
             errs.append(abs(fd - ad) / abs(ad))
     f, b = float(np.median(fwd)), float(np.median(bwd))
-    return {"workload": "adj64: 64^3 channel, sphere D=0.2, M 0.3, Re 1667, 200 RK4 steps, J over the last 50",
+    return {"workload": "adj64: 64^3 channel, sphere D=0.2 at (0.4,0.5,0.5), M 0.3, Re_D 100 (Re 1666.7 per unit "
+                        "length on the speed of sound), 200 RK4 steps, J over the last 50",
             "snapshots": 20, "J": J, "forward_ms": f * 1e3, "backward_ms": b * 1e3, "backward_over_forward": b / f,
             "fd_step": 1e-6, "fd_rel_err_max": max(errs), "fd_directions": len(errs),
             "adjoint_step_phase_ms": {k: round(v, 4) for k, v in phases.items()}}

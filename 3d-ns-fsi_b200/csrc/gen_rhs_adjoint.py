@@ -239,8 +239,8 @@ def emit_cuda(terms):
     w("")
     w("namespace nsf {")
     w("")
-    w("template <class Lam, class Val, class Inner>")
-    w("__device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X, long long sI, long long sJ,")
+    w("template <class Idx, class Lam, class Val, class Inner>")
+    w("__device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx sI, Idx sJ,")
     w("                                                   const Lam& lam, const Val& val, const Inner& inner,")
     w("                                                   double bar[%d]) {" % len(VARS))
     w("  for (int q = 0; q < %d; ++q) bar[q] = 0.0;" % len(VARS))
@@ -274,7 +274,7 @@ def emit_cuda(terms):
             # the kernel runs out of registers)
             w("  asm volatile(\"\" ::: \"memory\");")
             w("  if (inner(%d, %d, %d)) {" % o)
-            w("    const long long b = X - (%d * sI + %d * sJ + %d);" % o)
+            w("    const Idx b = X - (%d * sI + %d * sJ + %d);" % o)
             for e in sorted({t[0] for t in by_o[o] if t[2] in outs}):
                 w("    const double l%d = lam(%d, b);" % (e, e))
             for q, a in sorted(vals, key=lambda x: (x[1], VIDX[x[0]])):

@@ -369,7 +369,7 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     // edge conditions: z, y, then x (reads the stage output before the edge conditions)
     for (int f = 0; f < 5; ++f) A.val[f] = snap + (6 + f) * N;
     for (int axis = 2; axis >= 0; --axis)
-      launch_adj_edge(s->dGrid, A, s->plan, axis, dR, q, a->fbar, a->lamInflow, a->inletX, st);
+      launch_adj_edge(s->hGrid, A, s->plan, axis, dR, q, a->fbar, a->lamInflow, a->inletX, st);
     mark(PH_EDGE);
     launch_adj_solid(s->dGrid, A, G.nSolid, R.copyMask[q], nSM, st);
     mark(PH_SOLID);

@@ -165,22 +165,19 @@ __global__ void k_adj_filter_clear(AdjPtrs A, int nFilter) {
 // One axis, both faces, same launch geometry as k_edge_bc. Phase 1 (periodic, outlet, inlet part 1):
 // consume the adjoint of every edge node; periodic and outlet add to their (one-to-one) source nodes,
 // the inlet keeps the adjoint of its filtered extrapolated density per node for phase 2.
-__global__ void k_adj_edge(const Grid* __restrict__ gp, AdjPtrs A, int axis, const StepCtl* __restrict__ roles, int s,
-                           double* __restrict__ fbar, double* __restrict__ lamInflow) {
-  const Grid& G = *gp;
+// The grid descriptor is a kernel parameter: the face boxes and sizes come from the constant bank, so the
+// first memory access of a thread is its own adjoint load.
+__global__ void k_adj_edge(const __grid_constant__ Grid G, const EdgeBlock* __restrict__ blocks, AdjPtrs A, int axis,
+                           const StepCtl* __restrict__ roles, int s, double* __restrict__ fbar,
+                           double* __restrict__ lamInflow) {
   const double stageT = roles->stageT[s];
   const Consts& C = G.C;
-  int e = -1, seen = 0;
-  for (int q = 0; q < G.nEdge; ++q)
-    if (G.eAxis[q] == axis) {
-      if (seen == (int)blockIdx.z) e = q;
-      ++seen;
-    }
-  if (e < 0) return;
+  const EdgeBlock eb = blocks[blockIdx.x];
+  const int e = eb.e;
   const int* b = G.eBox[e];
   const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
-  const int a = b[2 * ax1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int bb = b[2 * ax2] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = eb.a0 + threadIdx.y;
+  const int bb = eb.b0 + threadIdx.x;
   if (a > b[2 * ax1 + 1] || bb > b[2 * ax2 + 1]) return;
   int ijk[3];
   ijk[axis] = b[2 * axis];
@@ -240,13 +237,14 @@ __global__ void k_adj_edge(const Grid* __restrict__ gp, AdjPtrs A, int axis, con
 
 // Inlet phase 2 (x faces only): every node of the two planes behind the inlet gathers from the inlet
 // nodes whose filtered extrapolation used it.
-__global__ void k_adj_inlet_gather(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ fbar) {
-  const Grid& G = *gp;
-  const int e = blockIdx.z;
-  if (e >= G.nEdge || G.eAxis[e] != 0 || G.eBc[e] != NSF_BC_INLET) return;
+__global__ void k_adj_inlet_gather(const __grid_constant__ Grid G, const EdgeBlock* __restrict__ blocks, AdjPtrs A,
+                                   const double* __restrict__ fbar) {
+  const EdgeBlock eb = blocks[blockIdx.x];  // the x faces' blocks; only inlet faces gather
+  const int e = eb.e;
+  if (G.eBc[e] != NSF_BC_INLET) return;
   const int* b = G.eBox[e];
-  const int a = b[2] + blockIdx.y * blockDim.y + threadIdx.y;   // j
-  const int bb = b[4] + blockIdx.x * blockDim.x + threadIdx.x;  // k
+  const int a = eb.a0 + threadIdx.y;   // j
+  const int bb = eb.b0 + threadIdx.x;  // k
   if (a > b[3] || bb > b[5]) return;
   const int side = G.eSide[e];
   const long long base = side ? (long long)G.NJ * G.NKp : 0;
@@ -363,18 +361,21 @@ __global__ void k_copy_set(CopySet S) {
 // kept in registers across nodes).
 constexpr int kAdjRhsRows = 8;    // rows of 32 nodes per block
 constexpr int kAdjRhsBlocks = 2;  // resident blocks per SM the register budget is set for
-__global__ void __launch_bounds__(32 * kAdjRhsRows, kAdjRhsBlocks) k_adj_rhs(const Grid* __restrict__ gp, const __grid_constant__ Consts C,
-                                                    AdjPtrs A, const double* __restrict__ lam,
-                                                    const double* __restrict__ V) {
+// Idx: the index type of the node and field offsets (int where 11 N < 2^31, which saves the 64-bit
+// address arithmetic of about 330 loads per node).
+template <class Idx>
+__global__ void __launch_bounds__(32 * kAdjRhsRows, kAdjRhsBlocks)
+    k_adj_rhs(const Grid* __restrict__ gp, const __grid_constant__ Consts C, AdjPtrs A, const double* __restrict__ lam,
+              const double* __restrict__ V) {
   const Grid& G = *gp;
-  const long long N = G.N, sI = G.sI, sJ = G.sJ;
+  const Idx N = Idx(G.N), sI = Idx(G.sI), sJ = Idx(G.sJ);
   const int NI = G.NI, NJ = G.NJ, NK = G.NK;
   const int r = blockIdx.x * blockDim.y + threadIdx.y, k = blockIdx.y * 32 + threadIdx.x;
   if (r < NI * NJ && k < NK) {
     const int i = r / NJ, j = r - i * NJ;
-    const long long m = i * sI + j * sJ + k;
-    auto lamAt = [&](int e, long long b) { return lam[e * N + b]; };
-    auto valAt = [&](int q, long long b) { return V[q * N + b]; };
+    const Idx m = i * sI + j * sJ + k;
+    auto lamAt = [&](int e, Idx b) { return lam[e * N + b]; };
+    auto valAt = [&](int q, Idx b) { return V[q * N + b]; };
     // the per-RHS-node conditions also bound the compiler's scheduling regions (without them it
     // interleaves all 19 blocks and runs out of registers)
     auto inner = [&](int di, int dj, int dk) {
@@ -510,15 +511,14 @@ void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes,
   if (nFilter > 0) k_adj_filter_clear<<<blocks_for(2 * nFilter, nSM), 256, 0, st>>>(A, nFilter);
 }
 
-void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
+void launch_adj_edge(const Grid& hg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
                      double* fbar, double* lamInflow, bool inletGather, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  dim3 grid(L.edgeGrid[axis][0], L.edgeGrid[axis][1], 2);
-  k_adj_edge<<<grid, dim3(32, kEdgeRows), 0, st>>>(dg, A, axis, roles, s, fbar, lamInflow);
-  if (axis == 0 && inletGather) {
-    dim3 g2(L.edgeGrid[0][0], L.edgeGrid[0][1], 6);
-    k_adj_inlet_gather<<<g2, dim3(32, kEdgeRows), 0, st>>>(dg, A, fbar);
-  }
+  if (L.nEdgeBlocksAll[axis] == 0) return;
+  k_adj_edge<<<L.nEdgeBlocksAll[axis], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocksAll[axis], A, axis, roles, s,
+                                                                     fbar, lamInflow);
+  if (axis == 0 && inletGather)
+    k_adj_inlet_gather<<<L.nEdgeBlocksAll[0], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocksAll[0], A, fbar);
 }
 
 void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, int nSM, void* stream) {
@@ -534,7 +534,10 @@ void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s,
 void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V,
                     void* stream) {
   const dim3 grid((hg.NI * hg.NJ + kAdjRhsRows - 1) / kAdjRhsRows, (hg.NK + 31) / 32);
-  k_adj_rhs<<<grid, dim3(32, kAdjRhsRows), 0, static_cast<cudaStream_t>(stream)>>>(dg, hg.C, A, lam, V);
+  if (11 * hg.N < (1LL << 31))
+    k_adj_rhs<int><<<grid, dim3(32, kAdjRhsRows), 0, static_cast<cudaStream_t>(stream)>>>(dg, hg.C, A, lam, V);
+  else
+    k_adj_rhs<long long><<<grid, dim3(32, kAdjRhsRows), 0, static_cast<cudaStream_t>(stream)>>>(dg, hg.C, A, lam, V);
 }
 
 void launch_copies(const double* const* src, double* const* dst, const long long* words, int count, int nSM,

@@ -31,7 +31,7 @@ void launch_adj_ghost(const Grid* dg, const AdjPtrs& A, int nGhost, int nFilter,
 void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes, int count, int nFilter, int nSM,
                        void* stream);
 // roles: device copy of the step's control block (stage times, dt).
-void launch_adj_edge(const Grid* dg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
+void launch_adj_edge(const Grid& hg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
                      double* fbar, double* lamInflow, bool inletGather, void* stream);
 void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, int nSM, void* stream);
 // The stage kernel's adjoint: prepare = RK4 combine adjoint into lam and the RHS input quantities into V

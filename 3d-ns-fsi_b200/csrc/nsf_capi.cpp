@@ -230,6 +230,7 @@ nsf_status build_device(nsf_solver* s) {
     fpre[2 * q] = cons[fnode[q]];
     fpre[2 * q + 1] = cons[4 * N + fnode[q]];
   }
+  s->typeFlags = type;
   std::vector<uint8_t> typeDev(Nd, SOLID_INACTIVE);  // pitch padding never takes part
   for (size_t n = 0; n < N; ++n) typeDev[dev(n)] = type[n];
   for (auto& f : fnode) f = dev(size_t(f));
@@ -395,6 +396,11 @@ nsf_status build_device(nsf_solver* s) {
     int bx[6] = {int(b.i0), int(b.i1), int(b.j0), int(b.j1), int(b.k0), int(b.k1)};
     std::memcpy(G.eBox[e], bx, sizeof bx);
   }
+  {
+    int zPer = 0;
+    for (const auto& e : S.edges) zPer += e.axis == 2 && e.bc == NSF_BC_PERIODIC;
+    G.zFused = zPer == 2 && S.NK >= 4;
+  }
 
   // launch plan: stage work items (tile x i-chunk), grids of the small kernels
   LaunchPlan& L = s->plan;
@@ -444,18 +450,15 @@ nsf_status build_device(nsf_solver* s) {
   }
   if ((st = upload(s, &L.items, items)) != NSF_OK) return st;
   for (int a = 0; a < 3; ++a) {
-    int n1 = 1, n2 = 1;
-    for (auto& e : S.edges)
-      if (e.axis == a) {
-        const Box& b = e.owned;
-        size_t lo[3] = {b.i0, b.j0, b.k0}, hi[3] = {b.i1, b.j1, b.k1};
-        int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
-        n1 = std::max(n1, int(hi[ax1] - lo[ax1] + 1));
-        n2 = std::max(n2, int(hi[ax2] - lo[ax2] + 1));
-      }
-    L.edgeGrid[a][0] = (n2 + 31) / 32;
-    L.edgeGrid[a][1] = (n1 + kEdgeRows - 1) / kEdgeRows;
-    L.edgeGrid[a][2] = 2;
+    std::vector<EdgeBlock> eb, all;
+    edge_blocks(G, type.data(), 0, a, false, eb);
+    edge_blocks(G, type.data(), 0, a, true, all);
+    L.nEdgeBlocks[a] = int(eb.size());
+    L.edgeBlocks[a] = nullptr;
+    if (!eb.empty() && (st = upload(s, &L.edgeBlocks[a], eb)) != NSF_OK) return st;
+    L.nEdgeBlocksAll[a] = int(all.size());
+    L.edgeBlocksAll[a] = nullptr;
+    if (!all.empty() && (st = upload(s, &L.edgeBlocksAll[a], all)) != NSF_OK) return st;
   }
   L.hasFilter = G.nFilter > 0;
   L.filterBlocks = std::max(1, std::min(s->nSM, (G.nFilter + 255) / 256));

@@ -15,6 +15,7 @@
 #define NSF_DEVICE_CUH
 
 #include <cstdint>
+#include <vector>
 
 namespace nsf {
 
@@ -102,6 +103,10 @@ struct Grid {
   int nEdge;
   int eAxis[6], eSide[6], eBc[6];
   int eBox[6][6];           // owned box i0,i1,j0,j1,k0,k1
+  // Both z faces periodic: the stage kernel also writes the periodic copy of each interior node it
+  // computes at k = 1 and k = NK-2 into k = NK-1 and k = 0 (same values, same sectors), and the z edge
+  // kernel handles only the rows the stage kernel does not (see edge_blocks).
+  int zFused;
   // gradient support (NULL / 0 for a plain run): an x-inlet velocity profile factor per (j, k) node of the
   // inlet plane, and a prescribed dt per step (the adjoint differentiates with the dt sequence frozen)
   const double* inflow;     // [NJ * NKp], index j * NKp + k
@@ -126,8 +131,21 @@ struct StageItem {
 
 // Launch geometry of one step, fixed at initialisation.
 // Edge-condition kernels: blocks of 32 x kEdgeRows threads over a face (small blocks spread a face's
-// few thousand nodes over many SMs).
+// few thousand nodes over many SMs), listed one by one so that a launch holds only blocks with nodes
+// (an ensemble's faces differ in size from member to member).
 constexpr int kEdgeRows = 2;
+struct EdgeBlock {
+  int g;       // member (0 for a single grid)
+  int e;       // edge (face) of that member
+  int a0, b0;  // first in-plane coordinates of the block: (a, bb) = the two axes other than the face's
+  unsigned long long mask;  // thread ty * 32 + tx works iff its bit is set
+};
+// The blocks of one axis' faces of a grid, in launch order, appended to out (member g). type: the host
+// node types with their flag bits (k fastest), or NULL. With G.zFused and a type array, the z faces'
+// blocks cover only the rows the stage kernel does not copy (rows on an x or y face plane, and rows
+// whose source node is not an unfiltered interior fluid node); all: every node regardless (the adjoint
+// transposes the whole copy).
+void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, bool all, std::vector<EdgeBlock>& out);
 
 struct LaunchPlan {
   int nSM;
@@ -136,7 +154,10 @@ struct LaunchPlan {
   int nItems;
   StageItem* items;  // device; the items of CTA b are items[ctaStart[b] .. ctaStart[b + 1])
   int* ctaStart;     // device, stageBlocks + 1 entries
-  int edgeGrid[3][3];  // per axis: grid x, y, z of blocks of 32 x kEdgeRows threads
+  EdgeBlock* edgeBlocks[3];  // device, per axis
+  int nEdgeBlocks[3];
+  EdgeBlock* edgeBlocksAll[3];  // every node of the faces (the adjoint's; single grid only)
+  int nEdgeBlocksAll[3];
   int filterBlocks, ghostBlocks, solidBlocks, gfBlocks;
   int nSlots;
   bool hasBodies;

@@ -232,10 +232,17 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
   CKE(cudaMemcpy(L.ctaStart, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
   // small kernels: block counts = maxima over the members
   L.gfBlocks = std::max(8, 4 * e->nSM / M);  // grid-stride over each member's nodes
+  for (int a = 0; a < 3; ++a) {  // edge blocks: every member's own, member-major
+    std::vector<EdgeBlock> eb;
+    for (int g = 0; g < M; ++g) edge_blocks(e->members[g]->hGrid, e->members[g]->typeFlags.data(), g, a, false, eb);
+    L.nEdgeBlocks[a] = int(eb.size());
+    L.edgeBlocks[a] = nullptr;
+    if (eb.empty()) continue;
+    if ((st = ens_alloc(e, &L.edgeBlocks[a], eb.size())) != NSF_OK) return st;
+    CKE(cudaMemcpy(L.edgeBlocks[a], eb.data(), eb.size() * sizeof(EdgeBlock), cudaMemcpyHostToDevice));
+  }
   for (nsf_solver* s : e->members) {
     const LaunchPlan& P = s->plan;
-    for (int a = 0; a < 3; ++a)
-      for (int d = 0; d < 2; ++d) L.edgeGrid[a][d] = std::max(L.edgeGrid[a][d], P.edgeGrid[a][d]);
     L.filterBlocks = std::max(L.filterBlocks, P.filterBlocks);
     L.ghostBlocks = std::max(L.ghostBlocks, P.ghostBlocks);
     L.solidBlocks = std::max(L.solidBlocks, P.solidBlocks);

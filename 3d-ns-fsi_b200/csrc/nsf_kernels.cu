@@ -154,38 +154,23 @@ __global__ void k_solid_copy(const Grid* __restrict__ grids, int s) {
 // nodes). Launched for x, then y, then z: the reference's application order outlet/inlet (x), y-max,
 // y-min, z-max, z-min (Mesh.cpp:155-167 after the reversal at Mesh.cpp:70). Threads cover the owned box.
 // blockIdx.z = 2 * member + (which of the axis's edges).
-__global__ void k_edge_bc(const Grid* __restrict__ grids, int s, int axis) {
+__global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __restrict__ blocks, int s, int axis) {
   __shared__ double red[4 * 32];
-  const Grid& G = grids[blockIdx.z >> 1];
-  const int edgeSlot = blockIdx.z & 1;
+  const EdgeBlock eb = blocks[blockIdx.x];  // every listed block holds nodes of its face
+  const Grid& G = grids[eb.g];
   StepCtl* c = G.ctl;
   if (!c->active) return;
   const Consts& C = G.C;
-  int e = -1, seen = 0;
-  for (int q = 0; q < G.nEdge; ++q)
-    if (G.eAxis[q] == axis) {
-      if (seen == edgeSlot) e = q;
-      ++seen;
-    }
+  const int e = eb.e;
   DtAcc dta;
   int bad = 0;
-  // blocks outside this member's edge box (ensembles launch the largest member's grid) leave at once;
-  // the test is uniform over the block, so no thread of it reaches the block reductions below
-  if (e < 0) return;
-  {
-    const int* b = G.eBox[e];
-    const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
-    if (b[2 * ax1] + int(blockIdx.y * blockDim.y) > b[2 * ax1 + 1] ||
-        b[2 * ax2] + int(blockIdx.x * blockDim.x) > b[2 * ax2 + 1])
-      return;
-  }
   {
     const int* b = G.eBox[e];
     // in-plane coordinates: (a, bb) = the two axes other than `axis`, in (i, j, k) order
     const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
-    const int a = b[2 * ax1] + blockIdx.y * blockDim.y + threadIdx.y;
-    const int bb = b[2 * ax2] + blockIdx.x * blockDim.x + threadIdx.x;
-    if (a <= b[2 * ax1 + 1] && bb <= b[2 * ax2 + 1]) {
+    const int a = eb.a0 + threadIdx.y;
+    const int bb = eb.b0 + threadIdx.x;
+    if (a <= b[2 * ax1 + 1] && bb <= b[2 * ax2 + 1] && ((eb.mask >> (threadIdx.y * 32 + threadIdx.x)) & 1)) {
       int ijk[3];
       ijk[axis] = b[2 * axis];
       ijk[ax1] = a;
@@ -583,10 +568,39 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 
 // ----------------------------------------------------------------------------------------------
 // Host-side launch helpers (called from nsf_capi.cpp).
+
+void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, bool all, std::vector<EdgeBlock>& out) {
+  const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
+  const bool fused = axis == 2 && G.zFused && type && !all;
+  for (int e = 0; e < G.nEdge; ++e) {
+    if (G.eAxis[e] != axis) continue;
+    const int* b = G.eBox[e];
+    const int ks = G.eSide[e] == 0 ? G.NK - 2 : 1;  // the periodic source plane
+    for (int a0 = b[2 * ax1]; a0 <= b[2 * ax1 + 1]; a0 += kEdgeRows)
+      for (int b0 = b[2 * ax2]; b0 <= b[2 * ax2 + 1]; b0 += 32) {
+        unsigned long long mask = ~0ull;
+        if (fused) {  // (a, bb) = (i, j)
+          mask = 0;
+          for (int ty = 0; ty < kEdgeRows; ++ty)
+            for (int tx = 0; tx < 32; ++tx) {
+              const int i = a0 + ty, j = b0 + tx;
+              if (i > b[1] || j > b[3]) continue;
+              const uint8_t ts = type[(size_t(i) * G.NJ + j) * G.NK + ks];
+              const bool copiedByStage = i >= 1 && i <= G.NI - 2 && j >= 1 && j <= G.NJ - 2 &&
+                                         (ts & TYPE_MASK) == FLUID_INTERIOR && !(ts & FILTER_BIT);
+              if (!copiedByStage) mask |= 1ull << (ty * 32 + tx);
+            }
+          if (!mask) continue;
+        }
+        out.push_back(EdgeBlock{g, e, a0, b0, mask});
+      }
+  }
+}
+
 // One RK4 step for `members` grids (dg: device array of them). hg: the grid on the host for a single-grid
 // solver (its stage kernel takes the grid by value), or NULL for an ensemble (the ensemble stage kernel
-// reads every member from dg). The small kernels carry the member in a grid dimension; their block
-// counts in L are the maxima over the members.
+// reads every member from dg). The small kernels carry the member in a grid dimension, their block
+// counts in L being the maxima over the members; the edge kernels run the listed blocks of every member.
 static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev,
                         StepHook* hook = nullptr) {
   int launches = 0;
@@ -610,11 +624,11 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
       ++launches;
     }
     if (hook) hook->before_edges(s);
-    for (int a = 0; a < 3; ++a) {
-      dim3 grid(L.edgeGrid[a][0], L.edgeGrid[a][1], 2 * M);
-      k_edge_bc<<<grid, dim3(32, kEdgeRows), 0, st>>>(dg, s, a);
-      ++launches;
-    }
+    for (int a = 0; a < 3; ++a)
+      if (L.nEdgeBlocks[a] > 0) {
+        k_edge_bc<<<L.nEdgeBlocks[a], dim3(32, kEdgeRows), 0, st>>>(dg, L.edgeBlocks[a], s, a);
+        ++launches;
+      }
     if (L.hasFilter) {
       k_body_filter<<<dim3(L.filterBlocks, M), 256, 0, st>>>(dg, s);
       ++launches;

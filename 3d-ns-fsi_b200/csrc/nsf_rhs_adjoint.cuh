@@ -10,14 +10,14 @@
 
 namespace nsf {
 
-template <class Lam, class Val, class Inner>
-__device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X, long long sI, long long sJ,
+template <class Idx, class Lam, class Val, class Inner>
+__device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx sI, Idx sJ,
                                                    const Lam& lam, const Val& val, const Inner& inner,
                                                    double bar[11]) {
   for (int q = 0; q < 11; ++q) bar[q] = 0.0;
   asm volatile("" ::: "memory");
   if (inner(0, 0, 0)) {
-    const long long b = X - (0 * sI + 0 * sJ + 0);
+    const Idx b = X - (0 * sI + 0 * sJ + 0);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
     const double l3 = lam(3, b);
@@ -73,7 +73,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(-1, 0, 0)) {
-    const long long b = X - (-1 * sI + 0 * sJ + 0);
+    const Idx b = X - (-1 * sI + 0 * sJ + 0);
     const double l0 = lam(0, b);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
@@ -118,7 +118,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(0, -1, 0)) {
-    const long long b = X - (0 * sI + -1 * sJ + 0);
+    const Idx b = X - (0 * sI + -1 * sJ + 0);
     const double l0 = lam(0, b);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
@@ -163,7 +163,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(0, 0, -1)) {
-    const long long b = X - (0 * sI + 0 * sJ + -1);
+    const Idx b = X - (0 * sI + 0 * sJ + -1);
     const double l0 = lam(0, b);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
@@ -208,7 +208,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(0, 0, 1)) {
-    const long long b = X - (0 * sI + 0 * sJ + 1);
+    const Idx b = X - (0 * sI + 0 * sJ + 1);
     const double l0 = lam(0, b);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
@@ -253,7 +253,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(0, 1, 0)) {
-    const long long b = X - (0 * sI + 1 * sJ + 0);
+    const Idx b = X - (0 * sI + 1 * sJ + 0);
     const double l0 = lam(0, b);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
@@ -298,7 +298,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(1, 0, 0)) {
-    const long long b = X - (1 * sI + 0 * sJ + 0);
+    const Idx b = X - (1 * sI + 0 * sJ + 0);
     const double l0 = lam(0, b);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
@@ -343,7 +343,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(-1, -1, 0)) {
-    const long long b = X - (-1 * sI + -1 * sJ + 0);
+    const Idx b = X - (-1 * sI + -1 * sJ + 0);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
     const double l4 = lam(4, b);
@@ -358,7 +358,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(-1, 0, -1)) {
-    const long long b = X - (-1 * sI + 0 * sJ + -1);
+    const Idx b = X - (-1 * sI + 0 * sJ + -1);
     const double l1 = lam(1, b);
     const double l3 = lam(3, b);
     const double l4 = lam(4, b);
@@ -373,7 +373,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(-1, 0, 1)) {
-    const long long b = X - (-1 * sI + 0 * sJ + 1);
+    const Idx b = X - (-1 * sI + 0 * sJ + 1);
     const double l1 = lam(1, b);
     const double l3 = lam(3, b);
     const double l4 = lam(4, b);
@@ -388,7 +388,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(-1, 1, 0)) {
-    const long long b = X - (-1 * sI + 1 * sJ + 0);
+    const Idx b = X - (-1 * sI + 1 * sJ + 0);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
     const double l4 = lam(4, b);
@@ -403,7 +403,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(0, -1, -1)) {
-    const long long b = X - (0 * sI + -1 * sJ + -1);
+    const Idx b = X - (0 * sI + -1 * sJ + -1);
     const double l2 = lam(2, b);
     const double l3 = lam(3, b);
     const double l4 = lam(4, b);
@@ -418,7 +418,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(0, -1, 1)) {
-    const long long b = X - (0 * sI + -1 * sJ + 1);
+    const Idx b = X - (0 * sI + -1 * sJ + 1);
     const double l2 = lam(2, b);
     const double l3 = lam(3, b);
     const double l4 = lam(4, b);
@@ -433,7 +433,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(0, 1, -1)) {
-    const long long b = X - (0 * sI + 1 * sJ + -1);
+    const Idx b = X - (0 * sI + 1 * sJ + -1);
     const double l2 = lam(2, b);
     const double l3 = lam(3, b);
     const double l4 = lam(4, b);
@@ -448,7 +448,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(0, 1, 1)) {
-    const long long b = X - (0 * sI + 1 * sJ + 1);
+    const Idx b = X - (0 * sI + 1 * sJ + 1);
     const double l2 = lam(2, b);
     const double l3 = lam(3, b);
     const double l4 = lam(4, b);
@@ -463,7 +463,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(1, -1, 0)) {
-    const long long b = X - (1 * sI + -1 * sJ + 0);
+    const Idx b = X - (1 * sI + -1 * sJ + 0);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
     const double l4 = lam(4, b);
@@ -478,7 +478,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(1, 0, -1)) {
-    const long long b = X - (1 * sI + 0 * sJ + -1);
+    const Idx b = X - (1 * sI + 0 * sJ + -1);
     const double l1 = lam(1, b);
     const double l3 = lam(3, b);
     const double l4 = lam(4, b);
@@ -493,7 +493,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(1, 0, 1)) {
-    const long long b = X - (1 * sI + 0 * sJ + 1);
+    const Idx b = X - (1 * sI + 0 * sJ + 1);
     const double l1 = lam(1, b);
     const double l3 = lam(3, b);
     const double l4 = lam(4, b);
@@ -508,7 +508,7 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, long long X,
   }
   asm volatile("" ::: "memory");
   if (inner(1, 1, 0)) {
-    const long long b = X - (1 * sI + 1 * sJ + 0);
+    const Idx b = X - (1 * sI + 1 * sJ + 0);
     const double l1 = lam(1, b);
     const double l2 = lam(2, b);
     const double l4 = lam(4, b);

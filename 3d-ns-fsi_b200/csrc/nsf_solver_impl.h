@@ -16,6 +16,7 @@ struct nsf_solver {
   int device = 0;
   cudaStream_t stream = nullptr;
   nsf::HostSetup setup;
+  std::vector<uint8_t> typeFlags;  // host node types with the edge-plane and filter bits (k fastest)
   bool initialized = false;
   bool hostOnly = false;  // device < 0: host setup only (classification queries), no GPU work
   std::vector<void*> allocs;

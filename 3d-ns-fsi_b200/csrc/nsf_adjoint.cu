@@ -292,6 +292,8 @@ __global__ void k_adj_solid(const Grid* __restrict__ gp, AdjPtrs A, int mask) {
 // (inc = dt/2, dt), lam = k is the adjoint of the stage's RHS; U0 receives o, o is consumed.
 // Values: momenta and rho_E from I, density from R, filter nodes' density and rho_E from fpre (for the
 // primitives), then the primitives and transport properties, as the stage kernel stages them.
+// With periodic z faces (Grid::zFused) the stage kernel also wrote the z copies of the nodes at k = 1 and
+// k = NK-2 it computed: their adjoints are gathered here, before the combine's.
 __global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, const StepCtl* __restrict__ roles,
                               double* __restrict__ lam, double* __restrict__ V) {
   const Grid& G = *gp;
@@ -303,12 +305,16 @@ __global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, con
     const bool interior = (ty & TYPE_MASK) == FLUID_INTERIOR;
     const double m1 = A.val[1][n], m2 = A.val[2][n], m3 = A.val[3][n], e4 = A.val[4][n];
     double rho = A.valR[n], rE = e4;
-    double o[5], acc[5], u0[5];
+    double o[5], acc[5], u0[5], oz[5] = {0, 0, 0, 0, 0};
+    // the z copy the stage kernel wrote with this node
+    const bool zCopy = (ty & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT)) != 0;
+    const long long nz = (ty & ZCOPY_UP_BIT) ? n + (G.NK - 2) : n - (G.NK - 2);
     if (interior)
       for (int f = 0; f < 5; ++f) {
         o[f] = A.lamO[f][n];
         acc[f] = A.lamAcc[f][n];
         u0[f] = A.lamU0[f][n];
+        if (zCopy) oz[f] = A.lamO[f][nz];
       }
     if (ty & FILTER_BIT) {
       const int f = G.fidx[n];
@@ -322,6 +328,11 @@ __global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, con
       for (int f = 0; f < 5; ++f) lam[f * G.N + n] = 0.0;
       continue;
     }
+    if (zCopy)
+      for (int f = 0; f < 5; ++f) {
+        o[f] += oz[f];
+        A.lamO[f][nz] = 0.0;
+      }
     for (int f = 0; f < 5; ++f) {
       double k;
       if (s == 0) {
@@ -514,11 +525,11 @@ void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes,
 void launch_adj_edge(const Grid& hg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
                      double* fbar, double* lamInflow, bool inletGather, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (L.nEdgeBlocksAll[axis] == 0) return;
-  k_adj_edge<<<L.nEdgeBlocksAll[axis], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocksAll[axis], A, axis, roles, s,
-                                                                     fbar, lamInflow);
+  if (L.nEdgeBlocks[axis] == 0) return;
+  k_adj_edge<<<L.nEdgeBlocks[axis], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocks[axis], A, axis, roles, s, fbar,
+                                                                  lamInflow);
   if (axis == 0 && inletGather)
-    k_adj_inlet_gather<<<L.nEdgeBlocksAll[0], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocksAll[0], A, fbar);
+    k_adj_inlet_gather<<<L.nEdgeBlocks[0], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocks[0], A, fbar);
 }
 
 void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, int nSM, void* stream) {

@@ -230,6 +230,18 @@ nsf_status build_device(nsf_solver* s) {
     fpre[2 * q] = cons[fnode[q]];
     fpre[2 * q + 1] = cons[4 * N + fnode[q]];
   }
+  {  // periodic z faces: the nodes whose periodic copies the stage kernel writes
+    int zPer = 0;
+    for (const auto& e : S.edges) zPer += e.axis == 2 && e.bc == NSF_BC_PERIODIC;
+    G.zFused = zPer == 2 && S.NK >= 4;
+    if (G.zFused)
+      for (size_t i = 1; i + 1 < S.NI; ++i)
+        for (size_t j = 1; j + 1 < S.NJ; ++j)
+          for (size_t ks : {size_t(1), S.NK - 2}) {
+            uint8_t& t = type[(i * S.NJ + j) * S.NK + ks];
+            if ((t & TYPE_MASK) == FLUID_INTERIOR && !(t & FILTER_BIT)) t |= ks == 1 ? ZCOPY_UP_BIT : ZCOPY_DOWN_BIT;
+          }
+  }
   s->typeFlags = type;
   std::vector<uint8_t> typeDev(Nd, SOLID_INACTIVE);  // pitch padding never takes part
   for (size_t n = 0; n < N; ++n) typeDev[dev(n)] = type[n];
@@ -396,11 +408,6 @@ nsf_status build_device(nsf_solver* s) {
     int bx[6] = {int(b.i0), int(b.i1), int(b.j0), int(b.j1), int(b.k0), int(b.k1)};
     std::memcpy(G.eBox[e], bx, sizeof bx);
   }
-  {
-    int zPer = 0;
-    for (const auto& e : S.edges) zPer += e.axis == 2 && e.bc == NSF_BC_PERIODIC;
-    G.zFused = zPer == 2 && S.NK >= 4;
-  }
 
   // launch plan: stage work items (tile x i-chunk), grids of the small kernels
   LaunchPlan& L = s->plan;
@@ -450,15 +457,11 @@ nsf_status build_device(nsf_solver* s) {
   }
   if ((st = upload(s, &L.items, items)) != NSF_OK) return st;
   for (int a = 0; a < 3; ++a) {
-    std::vector<EdgeBlock> eb, all;
-    edge_blocks(G, type.data(), 0, a, false, eb);
-    edge_blocks(G, type.data(), 0, a, true, all);
+    std::vector<EdgeBlock> eb;
+    edge_blocks(G, type.data(), 0, a, eb);
     L.nEdgeBlocks[a] = int(eb.size());
     L.edgeBlocks[a] = nullptr;
     if (!eb.empty() && (st = upload(s, &L.edgeBlocks[a], eb)) != NSF_OK) return st;
-    L.nEdgeBlocksAll[a] = int(all.size());
-    L.edgeBlocksAll[a] = nullptr;
-    if (!all.empty() && (st = upload(s, &L.edgeBlocksAll[a], all)) != NSF_OK) return st;
   }
   L.hasFilter = G.nFilter > 0;
   L.filterBlocks = std::max(1, std::min(s->nSM, (G.nFilter + 255) / 256));

@@ -82,7 +82,7 @@ struct Grid {
   double* acc[5];
   int NKp;                // k pitch of the device layout (multiple of 4: rows start on 32-byte boundaries)
   const void* tmaps;      // device array of TMA descriptors (see nsf_stage_tma.cu)
-  const uint8_t* type;    // NodeTypeEnum | FILTER_BIT | EDGE_PLANE_BIT
+  const uint8_t* type;    // NodeTypeEnum | FILTER_BIT | EDGE_PLANE_BIT | ZCOPY_UP_BIT | ZCOPY_DOWN_BIT
   const int* fidx;        // node -> filter slot (only read where FILTER_BIT is set)
   double* fpre;           // [F][2] pre-filter rho, rho_E of the last near-body filter
   double* fnew;           // [F][2] filtered values (written back after the ghost update)
@@ -143,9 +143,8 @@ struct EdgeBlock {
 // The blocks of one axis' faces of a grid, in launch order, appended to out (member g). type: the host
 // node types with their flag bits (k fastest), or NULL. With G.zFused and a type array, the z faces'
 // blocks cover only the rows the stage kernel does not copy (rows on an x or y face plane, and rows
-// whose source node is not an unfiltered interior fluid node); all: every node regardless (the adjoint
-// transposes the whole copy).
-void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, bool all, std::vector<EdgeBlock>& out);
+// whose source node is not an unfiltered interior fluid node).
+void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vector<EdgeBlock>& out);
 
 struct LaunchPlan {
   int nSM;
@@ -156,8 +155,6 @@ struct LaunchPlan {
   int* ctaStart;     // device, stageBlocks + 1 entries
   EdgeBlock* edgeBlocks[3];  // device, per axis
   int nEdgeBlocks[3];
-  EdgeBlock* edgeBlocksAll[3];  // every node of the faces (the adjoint's; single grid only)
-  int nEdgeBlocksAll[3];
   int filterBlocks, ghostBlocks, solidBlocks, gfBlocks;
   int nSlots;
   bool hasBodies;

@@ -234,7 +234,7 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
   L.gfBlocks = std::max(8, 4 * e->nSM / M);  // grid-stride over each member's nodes
   for (int a = 0; a < 3; ++a) {  // edge blocks: every member's own, member-major
     std::vector<EdgeBlock> eb;
-    for (int g = 0; g < M; ++g) edge_blocks(e->members[g]->hGrid, e->members[g]->typeFlags.data(), g, a, false, eb);
+    for (int g = 0; g < M; ++g) edge_blocks(e->members[g]->hGrid, e->members[g]->typeFlags.data(), g, a, eb);
     L.nEdgeBlocks[a] = int(eb.size());
     L.edgeBlocks[a] = nullptr;
     if (eb.empty()) continue;

@@ -19,6 +19,10 @@ enum : uint8_t { FLUID_INTERIOR = 0, FLUID_EDGE = 1, FLUID_GHOST = 2, SOLID_INAC
 constexpr uint8_t TYPE_MASK = 0x7;
 constexpr uint8_t FILTER_BIT = 0x80;
 constexpr uint8_t EDGE_PLANE_BIT = 0x40;  // node lies in a mesh-edge boundary's owned box
+// Periodic z faces (Grid::zFused): an unfiltered interior fluid node of an interior row at k = 1 (UP) or
+// k = NK-2 (DOWN), whose value the stage kernel also writes to its periodic copy at k = NK-1 or k = 0.
+constexpr uint8_t ZCOPY_UP_BIT = 0x20;
+constexpr uint8_t ZCOPY_DOWN_BIT = 0x10;
 
 struct Box {  // IndexBoundingBox, src/SmallVectors.h:72-104 (inclusive bounds)
   size_t i0, i1, j0, j1, k0, k1;

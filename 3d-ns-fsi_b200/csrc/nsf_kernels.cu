@@ -569,9 +569,9 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 // ----------------------------------------------------------------------------------------------
 // Host-side launch helpers (called from nsf_capi.cpp).
 
-void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, bool all, std::vector<EdgeBlock>& out) {
+void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vector<EdgeBlock>& out) {
   const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
-  const bool fused = axis == 2 && G.zFused && type && !all;
+  const bool fused = axis == 2 && G.zFused && type;
   for (int e = 0; e < G.nEdge; ++e) {
     if (G.eAxis[e] != axis) continue;
     const int* b = G.eBox[e];
@@ -585,9 +585,7 @@ void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, bool all, 
             for (int tx = 0; tx < 32; ++tx) {
               const int i = a0 + ty, j = b0 + tx;
               if (i > b[1] || j > b[3]) continue;
-              const uint8_t ts = type[(size_t(i) * G.NJ + j) * G.NK + ks];
-              const bool copiedByStage = i >= 1 && i <= G.NI - 2 && j >= 1 && j <= G.NJ - 2 &&
-                                         (ts & TYPE_MASK) == FLUID_INTERIOR && !(ts & FILTER_BIT);
+              const bool copiedByStage = type[(size_t(i) * G.NJ + j) * G.NK + ks] & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT);
               if (!copiedByStage) mask |= 1ull << (ty * 32 + tx);
             }
           if (!mask) continue;

@@ -507,11 +507,11 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
             out2[nR] = res[2];
             out3[nR] = res[3];
             out4[nR] = res[4];
-            if (G.zFused && (k == 1 || k == G.NK - 2) && !(tc & FILTER_BIT)) {
+            if (tc & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT)) {
               // periodic z faces: this node's copy (PeriodicBoundary, Boundary.cpp:344-367) lands in the
               // 32-byte sector just written; k = 1 feeds k = NK-1, k = NK-2 feeds k = 0. (Rows whose
               // source is a filter node stay with the edge kernel, which adds the copy's dt terms.)
-              const long long m = k == 1 ? nR + (G.NK - 2) : nR - (G.NK - 2);
+              const long long m = (tc & ZCOPY_UP_BIT) ? nR + (G.NK - 2) : nR - (G.NK - 2);
               out0[m] = res[0];
               out1[m] = res[1];
               out2[m] = res[2];

@@ -230,19 +230,20 @@ def emit_cuda(terms):
     w("// Generated by gen_rhs_adjoint.py from the RHS term table: do not edit. The transposed stencil of the")
     w("// right-hand side (rhs_eval, nsf_physics.cuh) in gather form: rhs_adjoint_gather(...) returns, for node")
     w("// X = (i, j, k), the adjoint of each input quantity (RU, RV, RW, RE, u, v, w, p, T, mu, ka) summed over")
-    w("// every interior node whose RHS reads it. lam(e, b): RHS adjoint of equation e at linear node b (zero where")
-    w("// no RHS is taken); val(q, b): input quantity q at node b; inner(di, dj, dk): the node (i-di, j-dj, k-dk)")
-    w("// is one whose RHS was taken (its whole stencil then lies inside the grid). The terms of one RHS node")
-    w("// are grouped by equation.")
+    w("// every interior node whose RHS reads it. lam(e, di, dj, dk): RHS adjoint of equation e at node")
+    w("// (i+di, j+dj, k+dk) (zero where no RHS is taken); val(q, di, dj, dk): input quantity q there (offsets")
+    w("// within one node of X: the 7-point stencil for u, v, w, T, mu, ka, X itself for the others);")
+    w("// inner(di, dj, dk): the node (i-di, j-dj, k-dk) is one whose RHS was taken (its whole stencil then")
+    w("// lies inside the grid). All offsets are literals, so a caller's index arithmetic folds. The terms of")
+    w("// one RHS node are grouped by equation.")
     w("#ifndef NSF_RHS_ADJOINT_CUH")
     w("#define NSF_RHS_ADJOINT_CUH")
     w("")
     w("namespace nsf {")
     w("")
-    w("template <class Idx, class Lam, class Val, class Inner>")
-    w("__device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx sI, Idx sJ,")
-    w("                                                   const Lam& lam, const Val& val, const Inner& inner,")
-    w("                                                   double bar[%d]) {" % len(VARS))
+    w("template <class Lam, class Val, class Inner>")
+    w("__device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, const Lam& lam, const Val& val,")
+    w("                                                   const Inner& inner, double bar[%d]) {" % len(VARS))
     w("  for (int q = 0; q < %d; ++q) bar[q] = 0.0;" % len(VARS))
     rel = sorted({(q, tuple(o2[a] - t[1][a] for a in range(3))) for t in terms for (q, o2) in t[4]},
                  key=lambda x: (x[1], VIDX[x[0]]))
@@ -274,12 +275,10 @@ def emit_cuda(terms):
             # the kernel runs out of registers)
             w("  asm volatile(\"\" ::: \"memory\");")
             w("  if (inner(%d, %d, %d)) {" % o)
-            w("    const Idx b = X - (%d * sI + %d * sJ + %d);" % o)
             for e in sorted({t[0] for t in by_o[o] if t[2] in outs}):
-                w("    const double l%d = lam(%d, b);" % (e, e))
+                w("    const double l%d = lam(%d, %d, %d, %d);" % (e, e, -o[0], -o[1], -o[2]))
             for q, a in sorted(vals, key=lambda x: (x[1], VIDX[x[0]])):
-                w("    const double %s = val(%d, X + (%d * sI + %d * sJ + %d));  // %s %s"
-                  % (names[(q, a)], VIDX[q], *a, q, a))
+                w("    const double %s = val(%d, %d, %d, %d);  // %s %s" % (names[(q, a)], VIDX[q], *a, q, a))
             for q in VARS:
                 if q not in outs:
                     continue

@@ -46,6 +46,7 @@ struct AdjCtx {
   long long* fsNodes = nullptr;
   int nfs = 0;
   bool inletX = false;
+  bool xInOut = false;  // an x face is an inlet or an outlet (its adjoint reads the planes next to it)
   double* lam = nullptr;  // 20 x Nd: adjoint of bufs[b][f] at (5 b + f) Nd, accumulator at (15 + f) Nd
   double* lamFpre = nullptr;
   double* lamFnew = nullptr;
@@ -117,13 +118,17 @@ nsf_status setup(nsf_solver* s) {
     if (!ok) return fail(s, NSF_ERR_ARG, "the adjoint supports periodic faces and x-inlet/x-outlet faces only");
   }
   if (S.NI < 6 || S.NJ < 4 || S.NK < 4) return fail(s, NSF_ERR_ARG, "grid too small for the adjoint");
+  if (adj_kernels_init() != 0) return fail(s, NSF_ERR_CUDA, "adjoint kernel attributes could not be set");
   auto* a = new AdjCtx;
   s->adj = a;
   a->nsteps = int(c.stop_time_level);
   const Grid& G = s->hGrid;
   const size_t N = nd(s), F = nf(s), NG = size_t(G.nGhost), plane = size_t(G.NJ) * G.NKp;
   nsf_status st;
-  for (const auto& e : S.edges) a->inletX |= e.axis == 0 && e.bc == NSF_BC_INLET;
+  for (const auto& e : S.edges) {
+    a->inletX |= e.axis == 0 && e.bc == NSF_BC_INLET;
+    a->xInOut |= e.axis == 0 && (e.bc == NSF_BC_INLET || e.bc == NSF_BC_OUTLET);
+  }
   if ((st = aalloc(s, a, &a->dDt, size_t(a->nsteps) + 1)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->dInflow, plane)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->dU0, 5 * N)) != NSF_OK) return st;
@@ -259,6 +264,23 @@ nsf_status advance(nsf_solver* s, int n) {
 // Keeps the step's control block and, per stage, the values the nonlinear adjoints need. The step's roles
 // (which physical buffer plays which part) are known on the host from the forward run's record, so nothing
 // waits here and the whole adjoint step can be captured as a graph.
+// Which stage values the adjoint reads from the snapshot and which it reads live from the buffers after
+// the recomputed step. Outside global-filter steps, the stage-1 input is U0 and the stage-4 input is the
+// stage-3 output: no later kernel of the step writes either buffer, so both are read in place; the density
+// for the primitives is the input's own density buffer except on filter steps.
+struct SnapPlan {
+  bool inputLive, rSeparate;
+};
+SnapPlan snap_plan(const StepCtl& R, int q) {
+  const bool live = !R.filterNow && (q == 0 || q == 3);
+  return SnapPlan{live, !live && R.R[q] != R.I[q][0]};
+}
+
+// Keeps the step's control block and, per stage, the values the nonlinear adjoints need that the step
+// overwrites: the stage inputs (snap_plan), the near-body filter's pre-values and, for x inlet / outlet
+// faces, the four x-planes next to them (i = 1, 2, NI-3, NI-2) of the stage output before the edge
+// conditions. The step's roles (which physical buffer plays which part) are known on the host from the
+// forward run's record, so nothing waits here and the whole adjoint step can be captured as a graph.
 struct SnapHook : StepHook {
   nsf_solver* s;
   AdjCtx* a;
@@ -270,6 +292,7 @@ struct SnapHook : StepHook {
   int n = 0;
   SnapHook(nsf_solver* s_, AdjCtx* a_, const StepCtl& r) : s(s_), a(a_), R(r) {}
   void add(double* d, const double* sr, size_t w) {
+    if (n == kMaxCopies) flush();
     src[n] = sr;
     dst[n] = d;
     words[n++] = (long long)w;
@@ -284,15 +307,19 @@ struct SnapHook : StepHook {
   void before_stage(int q) override {
     const size_t N = nd(s);
     double* base = a->stageSnap + q * per_stage(s);
-    for (int f = 0; f < 5; ++f) add(base + f * N, R.I[q][f], N);
-    add(base + 5 * N, R.R[q], N);
+    const SnapPlan P = snap_plan(R, q);
+    if (!P.inputLive)
+      for (int f = 0; f < 5; ++f) add(base + f * N, R.I[q][f], N);
+    if (P.rSeparate) add(base + 5 * N, R.R[q], N);
     if (nf(s)) add(base + 11 * N, s->hGrid.fpre, 2 * nf(s));
     flush();
   }
   void before_edges(int q) override {
-    const size_t N = nd(s);
+    if (!a->xInOut) return;
+    const size_t N = nd(s), plane = size_t(s->hGrid.sI), NI = size_t(s->hGrid.NI);
     double* base = a->stageSnap + q * per_stage(s);
-    for (int f = 0; f < 5; ++f) add(base + (6 + f) * N, R.O[q][f], N);
+    for (size_t i : {size_t(1), size_t(2), NI - 3, NI - 2})
+      for (int f = 0; f < 4; ++f) add(base + (6 + f) * N + i * plane, R.O[q][f] + i * plane, plane);
     flush();
   }
 };
@@ -374,12 +401,13 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     launch_adj_solid(s->dGrid, A, G.nSolid, R.copyMask[q], nSM, st);
     mark(PH_SOLID);
     // stage kernel: RK4 combine, transposed RHS, primitives of the stage input
-    for (int f = 0; f < 5; ++f) A.val[f] = snap + f * N;
-    A.valR = snap + 5 * N;
+    const SnapPlan P = snap_plan(R, q);
+    for (int f = 0; f < 5; ++f) A.val[f] = P.inputLive ? R.I[q][f] : snap + f * N;
+    A.valR = P.inputLive ? R.R[q] : P.rSeparate ? snap + 5 * N : snap;
     A.valFpre = snap + 11 * N;
     launch_adj_prepare(s->dGrid, G, A, q, dR, a->tmpLam, a->tmpV, nSM, st);
     mark(PH_PREPARE);
-    launch_adj_rhs(s->dGrid, G, A, a->tmpLam, a->tmpV, st);
+    launch_adj_rhs(s->dGrid, G, A, a->tmpLam, a->tmpV, nSM, st);
     mark(PH_RHS);
   }
   if (R.filterNow) {

@@ -14,6 +14,8 @@
 // against finite differences and the dual-number oracle do.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "nsf_adjoint.h"
 #include "nsf_device.cuh"
 #include "nsf_internal.h"
@@ -368,66 +370,114 @@ __global__ void k_copy_set(CopySet S) {
 }
 
 // Transposed RHS (generated gather) and the chain rule through the primitive / transport values.
-// One node per thread: threads run along k (32 per row), 8 rows of (i, j) per block (no loop, so nothing is
-// kept in registers across nodes).
-constexpr int kAdjRhsRows = 8;    // rows of 32 nodes per block
-constexpr int kAdjRhsBlocks = 2;  // resident blocks per SM the register budget is set for
-// Idx: the index type of the node and field offsets (int where 11 N < 2^31, which saves the 64-bit
-// address arithmetic of about 330 loads per node).
-template <class Idx>
-__global__ void __launch_bounds__(32 * kAdjRhsRows, kAdjRhsBlocks)
+// A block takes an 8 (j) x 32 (k) tile of nodes through a chunk of i-planes. The generated gather reads
+// the RHS adjoints at the 19 RHS nodes around a node and u, v, w, T, mu, kappa at its 7-point stencil:
+// those 11 fields are staged per plane with a one-node halo in a 3-plane ring in shared memory (so every
+// read is a shared-memory load at a fixed offset), the other inputs (momenta, rho_E, p) are read at the
+// node itself from global memory. Planes and halo nodes outside the grid are staged as zeros.
+constexpr int RT_J = 8, RT_K = 32, RT_HK = RT_K + 2, RT_PLANE = (RT_J + 2) * RT_HK;
+constexpr int RT_FIELDS = 11;                     // RHS adjoints 0..4, then u, v, w, T, mu, kappa
+constexpr int RT_SLOT = RT_FIELDS * RT_PLANE;     // doubles per staged plane
+constexpr int RT_SMEM = 3 * RT_SLOT * 8;          // bytes: 89,760
+constexpr int kAdjRhsBlocks = 2;                  // resident blocks per SM (shared memory and registers)
+__host__ __device__ constexpr int rt_field(int q) {  // input quantity q -> staged field, or -1
+  return q == 4 ? 5 : q == 5 ? 6 : q == 6 ? 7 : q == 8 ? 8 : q == 9 ? 9 : q == 10 ? 10 : -1;
+}
+
+__global__ void __launch_bounds__(32 * RT_J, kAdjRhsBlocks)
     k_adj_rhs(const Grid* __restrict__ gp, const __grid_constant__ Consts C, AdjPtrs A, const double* __restrict__ lam,
-              const double* __restrict__ V) {
+              const double* __restrict__ V, int chunk) {
+  extern __shared__ double sm[];
   const Grid& G = *gp;
-  const Idx N = Idx(G.N), sI = Idx(G.sI), sJ = Idx(G.sJ);
+  const long long N = G.N, sI = G.sI, sJ = G.sJ;
   const int NI = G.NI, NJ = G.NJ, NK = G.NK;
-  const int r = blockIdx.x * blockDim.y + threadIdx.y, k = blockIdx.y * 32 + threadIdx.x;
-  if (r < NI * NJ && k < NK) {
-    const int i = r / NJ, j = r - i * NJ;
-    const Idx m = i * sI + j * sJ + k;
-    auto lamAt = [&](int e, Idx b) { return lam[e * N + b]; };
-    auto valAt = [&](int q, Idx b) { return V[q * N + b]; };
-    // the per-RHS-node conditions also bound the compiler's scheduling regions (without them it
-    // interleaves all 19 blocks and runs out of registers)
-    auto inner = [&](int di, int dj, int dk) {
-      const int a = i - di, b = j - dj, c = k - dk;
-      return a >= 1 && a <= NI - 2 && b >= 1 && b <= NJ - 2 && c >= 1 && c <= NK - 2;
-    };
-    double bar[11];
-    rhs_adjoint_gather(C, m, sI, sJ, lamAt, valAt, inner, bar);
-    // chain rule: u = m r1, p = gm1 (rE - (rho+1) K), T = (gamma p - rho) r1, mu = x sqrt(x) sc1/(re (T+sc1)),
-    // kappa = mu pf, with r1 = 1/(rho+1), K = |u|^2/2, x = 1 + T
-    // the density of the primitives: the stage's density input, or the pre-filter copy at filter nodes
-    const bool filt = (G.type[m] & FILTER_BIT) != 0;
-    const int fi = filt ? G.fidx[m] : 0;
-    const double rho = filt ? A.valFpre[2 * fi] : A.valR[m];
-    const double r1 = 1.0 / (rho + 1.0);
-    const double u = V[4 * N + m], v = V[5 * N + m], w = V[6 * N + m], T = V[8 * N + m];
-    const double K = 0.5 * (u * u + v * v + w * w);
-    double ub = bar[4], vb = bar[5], wb = bar[6], pb = bar[7], Tb = bar[8], mub = bar[9];
-    mub += C.pf * bar[10];
-    const double x = 1.0 + T, sx = sqrt(x), den = T + C.sc1;
-    Tb += mub * C.sc1 / C.re * (1.5 * sx * den - x * sx) / (den * den);
-    pb += C.gamma * r1 * Tb;
-    double rhob = -r1 * Tb - T * r1 * Tb;
-    double rEb = C.gm1 * pb;
-    rhob += -C.gm1 * K * pb;
-    const double Kb = -C.gm1 * (rho + 1.0) * pb;
-    ub += Kb * u;
-    vb += Kb * v;
-    wb += Kb * w;
-    rhob += -(u * ub + v * vb + w * wb) * r1;
-    A.lamI[1][m] += bar[0] + r1 * ub;
-    A.lamI[2][m] += bar[1] + r1 * vb;
-    A.lamI[3][m] += bar[2] + r1 * wb;
-    A.lamI[4][m] += bar[3];
-    if (filt) {
-      A.lamFpre[2 * fi] += rhob;
-      A.lamFpre[2 * fi + 1] += rEb;
-    } else {
-      A.lamR[m] += rhob;
-      A.lamI[4][m] += rEb;
+  const int tilesK = (NK + RT_K - 1) / RT_K;
+  const int j0 = (blockIdx.x / tilesK) * RT_J, k0 = (blockIdx.x % tilesK) * RT_K;
+  const int i0 = blockIdx.y * chunk, i1 = min(NI - 1, i0 + chunk - 1);
+  if (i0 > i1) return;  // uniform over the block
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int j = j0 + ty, k = k0 + tx;
+  auto stage = [&](int p, int slot) {
+    double* s = sm + slot * RT_SLOT;
+    for (int idx = tid; idx < RT_PLANE; idx += 32 * RT_J) {
+      const int hj = idx / RT_HK, jj = j0 - 1 + hj, kk = k0 - 1 + (idx - hj * RT_HK);
+      const bool in = p >= 0 && p < NI && jj >= 0 && jj < NJ && kk >= 0 && kk < NK;
+      const long long n = in ? p * sI + jj * sJ + kk : 0;
+      double v[RT_FIELDS];
+#pragma unroll
+      for (int e = 0; e < 5; ++e) v[e] = in ? lam[e * N + n] : 0.0;
+      v[5] = in ? V[4 * N + n] : 0.0;
+      v[6] = in ? V[5 * N + n] : 0.0;
+      v[7] = in ? V[6 * N + n] : 0.0;
+      v[8] = in ? V[8 * N + n] : 0.0;
+      v[9] = in ? V[9 * N + n] : 0.0;
+      v[10] = in ? V[10 * N + n] : 0.0;
+#pragma unroll
+      for (int f = 0; f < RT_FIELDS; ++f) s[f * RT_PLANE + idx] = v[f];
     }
+  };
+  stage(i0 - 1, 0);
+  stage(i0, 1);
+  int cur = 1;  // ring slot of plane i
+  for (int i = i0; i <= i1; ++i) {
+    const int nxt = cur == 2 ? 0 : cur + 1, prv = cur == 0 ? 2 : cur - 1;
+    stage(i + 1, nxt);
+    __syncthreads();
+    if (j < NJ && k < NK) {
+      const int sb[3] = {prv * RT_SLOT, cur * RT_SLOT, nxt * RT_SLOT};  // planes i-1, i, i+1
+      const int c = (ty + 1) * RT_HK + tx + 1;
+      const long long m = i * sI + j * sJ + k;
+      auto lamAt = [&](int e, int di, int dj, int dk) { return sm[sb[di + 1] + e * RT_PLANE + c + dj * RT_HK + dk]; };
+      auto valAt = [&](int q, int di, int dj, int dk) {
+        const int f = rt_field(q);
+        return f >= 0 ? sm[sb[di + 1] + f * RT_PLANE + c + dj * RT_HK + dk] : V[q * N + m];  // others at X only
+      };
+      // the per-RHS-node conditions also bound the compiler's scheduling regions (without them it
+      // interleaves all 19 blocks and runs out of registers)
+      auto inner = [&](int di, int dj, int dk) {
+        const int a = i - di, b = j - dj, d = k - dk;
+        return a >= 1 && a <= NI - 2 && b >= 1 && b <= NJ - 2 && d >= 1 && d <= NK - 2;
+      };
+      double bar[11];
+      rhs_adjoint_gather(C, lamAt, valAt, inner, bar);
+      // chain rule: u = m r1, p = gm1 (rE - (rho+1) K), T = (gamma p - rho) r1, mu = x sqrt(x) sc1/(re (T+sc1)),
+      // kappa = mu pf, with r1 = 1/(rho+1), K = |u|^2/2, x = 1 + T
+      // the density of the primitives: the stage's density input, or the pre-filter copy at filter nodes
+      const bool filt = (G.type[m] & FILTER_BIT) != 0;
+      const int fi = filt ? G.fidx[m] : 0;
+      const double rho = filt ? A.valFpre[2 * fi] : A.valR[m];
+      const double r1 = 1.0 / (rho + 1.0);
+      const int cc = sb[1] + c;  // this node in the staged plane
+      const double u = sm[cc + 5 * RT_PLANE], v = sm[cc + 6 * RT_PLANE], w = sm[cc + 7 * RT_PLANE],
+                   T = sm[cc + 8 * RT_PLANE];
+      const double K = 0.5 * (u * u + v * v + w * w);
+      double ub = bar[4], vb = bar[5], wb = bar[6], pb = bar[7], Tb = bar[8], mub = bar[9];
+      mub += C.pf * bar[10];
+      const double x = 1.0 + T, sx = sqrt(x), den = T + C.sc1;
+      Tb += mub * C.sc1 / C.re * (1.5 * sx * den - x * sx) / (den * den);
+      pb += C.gamma * r1 * Tb;
+      double rhob = -r1 * Tb - T * r1 * Tb;
+      double rEb = C.gm1 * pb;
+      rhob += -C.gm1 * K * pb;
+      const double Kb = -C.gm1 * (rho + 1.0) * pb;
+      ub += Kb * u;
+      vb += Kb * v;
+      wb += Kb * w;
+      rhob += -(u * ub + v * vb + w * wb) * r1;
+      A.lamI[1][m] += bar[0] + r1 * ub;
+      A.lamI[2][m] += bar[1] + r1 * vb;
+      A.lamI[3][m] += bar[2] + r1 * wb;
+      A.lamI[4][m] += bar[3];
+      if (filt) {
+        A.lamFpre[2 * fi] += rhob;
+        A.lamFpre[2 * fi + 1] += rEb;
+      } else {
+        A.lamR[m] += rhob;
+        A.lamI[4][m] += rEb;
+      }
+    }
+    __syncthreads();  // the next iteration restages the oldest slot
+    cur = nxt;
   }
 }
 
@@ -542,13 +592,21 @@ void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s,
   k_adj_prepare<<<blocks_for(hg.N, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, s, roles, lam, V);
 }
 
-void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V,
+int adj_kernels_init() {
+  return int(cudaFuncSetAttribute(k_adj_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, RT_SMEM));
+}
+
+void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V, int nSM,
                     void* stream) {
-  const dim3 grid((hg.NI * hg.NJ + kAdjRhsRows - 1) / kAdjRhsRows, (hg.NK + 31) / 32);
-  if (11 * hg.N < (1LL << 31))
-    k_adj_rhs<int><<<grid, dim3(32, kAdjRhsRows), 0, static_cast<cudaStream_t>(stream)>>>(dg, hg.C, A, lam, V);
-  else
-    k_adj_rhs<long long><<<grid, dim3(32, kAdjRhsRows), 0, static_cast<cudaStream_t>(stream)>>>(dg, hg.C, A, lam, V);
+  // i-chunks: enough blocks for kAdjRhsBlocks per SM, each chunk at least 4 planes (a chunk of L planes
+  // stages L + 2)
+  const int tiles = ((hg.NJ + RT_J - 1) / RT_J) * ((hg.NK + RT_K - 1) / RT_K);
+  int chunks = (kAdjRhsBlocks * nSM + tiles - 1) / tiles;
+  chunks = std::max(1, std::min(chunks, hg.NI / 4));
+  const int chunk = (hg.NI + chunks - 1) / chunks;
+  chunks = (hg.NI + chunk - 1) / chunk;
+  k_adj_rhs<<<dim3(tiles, chunks), dim3(32, RT_J), RT_SMEM, static_cast<cudaStream_t>(stream)>>>(dg, hg.C, A, lam, V,
+                                                                                                   chunk);
 }
 
 void launch_copies(const double* const* src, double* const* dst, const long long* words, int count, int nSM,

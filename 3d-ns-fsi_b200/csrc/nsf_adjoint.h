@@ -38,12 +38,14 @@ void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, in
 // (11 x N); rhs = transposed RHS gather and the chain rule into the stage input's adjoints.
 void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, double* lam,
                         double* V, int nSM, void* stream);
-void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V,
+void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V, int nSM,
                     void* stream);
+// Kernel attributes (shared-memory size of the transposed RHS); call once before the first launch.
+int adj_kernels_init();
 void launch_adj_density_filter(const Grid* dg, long long N, const double* lamDstConst, double* lamDst, double* lamSrc,
                                int nSM, void* stream);
 // count (<= kMaxCopies) device-to-device copies of words[c] doubles in one launch.
-constexpr int kMaxCopies = 8;
+constexpr int kMaxCopies = 16;
 void launch_copies(const double* const* src, double* const* dst, const long long* words, int count, int nSM,
                    void* stream);
 

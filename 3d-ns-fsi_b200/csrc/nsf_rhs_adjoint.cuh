@@ -1,69 +1,69 @@
 // Generated by gen_rhs_adjoint.py from the RHS term table: do not edit. The transposed stencil of the
 // right-hand side (rhs_eval, nsf_physics.cuh) in gather form: rhs_adjoint_gather(...) returns, for node
 // X = (i, j, k), the adjoint of each input quantity (RU, RV, RW, RE, u, v, w, p, T, mu, ka) summed over
-// every interior node whose RHS reads it. lam(e, b): RHS adjoint of equation e at linear node b (zero where
-// no RHS is taken); val(q, b): input quantity q at node b; inner(di, dj, dk): the node (i-di, j-dj, k-dk)
-// is one whose RHS was taken (its whole stencil then lies inside the grid). The terms of one RHS node
-// are grouped by equation.
+// every interior node whose RHS reads it. lam(e, di, dj, dk): RHS adjoint of equation e at node
+// (i+di, j+dj, k+dk) (zero where no RHS is taken); val(q, di, dj, dk): input quantity q there (offsets
+// within one node of X: the 7-point stencil for u, v, w, T, mu, ka, X itself for the others);
+// inner(di, dj, dk): the node (i-di, j-dj, k-dk) is one whose RHS was taken (its whole stencil then
+// lies inside the grid). All offsets are literals, so a caller's index arithmetic folds. The terms of
+// one RHS node are grouped by equation.
 #ifndef NSF_RHS_ADJOINT_CUH
 #define NSF_RHS_ADJOINT_CUH
 
 namespace nsf {
 
-template <class Idx, class Lam, class Val, class Inner>
-__device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx sI, Idx sJ,
-                                                   const Lam& lam, const Val& val, const Inner& inner,
-                                                   double bar[11]) {
+template <class Lam, class Val, class Inner>
+__device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, const Lam& lam, const Val& val,
+                                                   const Inner& inner, double bar[11]) {
   for (int q = 0; q < 11; ++q) bar[q] = 0.0;
   asm volatile("" ::: "memory");
   if (inner(0, 0, 0)) {
-    const Idx b = X - (0 * sI + 0 * sJ + 0);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w1 = val(5, X + (-1 * sI + 0 * sJ + 0));  // v (-1, 0, 0)
-    const double w2 = val(6, X + (-1 * sI + 0 * sJ + 0));  // w (-1, 0, 0)
-    const double w3 = val(8, X + (-1 * sI + 0 * sJ + 0));  // T (-1, 0, 0)
-    const double w4 = val(9, X + (-1 * sI + 0 * sJ + 0));  // mu (-1, 0, 0)
-    const double w5 = val(10, X + (-1 * sI + 0 * sJ + 0));  // ka (-1, 0, 0)
-    const double w6 = val(4, X + (0 * sI + -1 * sJ + 0));  // u (0, -1, 0)
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w8 = val(6, X + (0 * sI + -1 * sJ + 0));  // w (0, -1, 0)
-    const double w9 = val(8, X + (0 * sI + -1 * sJ + 0));  // T (0, -1, 0)
-    const double w10 = val(9, X + (0 * sI + -1 * sJ + 0));  // mu (0, -1, 0)
-    const double w11 = val(10, X + (0 * sI + -1 * sJ + 0));  // ka (0, -1, 0)
-    const double w12 = val(4, X + (0 * sI + 0 * sJ + -1));  // u (0, 0, -1)
-    const double w13 = val(5, X + (0 * sI + 0 * sJ + -1));  // v (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w15 = val(8, X + (0 * sI + 0 * sJ + -1));  // T (0, 0, -1)
-    const double w16 = val(9, X + (0 * sI + 0 * sJ + -1));  // mu (0, 0, -1)
-    const double w17 = val(10, X + (0 * sI + 0 * sJ + -1));  // ka (0, 0, -1)
-    const double w22 = val(4, X + (0 * sI + 0 * sJ + 0));  // u (0, 0, 0)
-    const double w23 = val(5, X + (0 * sI + 0 * sJ + 0));  // v (0, 0, 0)
-    const double w24 = val(6, X + (0 * sI + 0 * sJ + 0));  // w (0, 0, 0)
-    const double w26 = val(8, X + (0 * sI + 0 * sJ + 0));  // T (0, 0, 0)
-    const double w27 = val(9, X + (0 * sI + 0 * sJ + 0));  // mu (0, 0, 0)
-    const double w28 = val(10, X + (0 * sI + 0 * sJ + 0));  // ka (0, 0, 0)
-    const double w29 = val(4, X + (0 * sI + 0 * sJ + 1));  // u (0, 0, 1)
-    const double w30 = val(5, X + (0 * sI + 0 * sJ + 1));  // v (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w32 = val(8, X + (0 * sI + 0 * sJ + 1));  // T (0, 0, 1)
-    const double w33 = val(9, X + (0 * sI + 0 * sJ + 1));  // mu (0, 0, 1)
-    const double w34 = val(10, X + (0 * sI + 0 * sJ + 1));  // ka (0, 0, 1)
-    const double w35 = val(4, X + (0 * sI + 1 * sJ + 0));  // u (0, 1, 0)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w37 = val(6, X + (0 * sI + 1 * sJ + 0));  // w (0, 1, 0)
-    const double w38 = val(8, X + (0 * sI + 1 * sJ + 0));  // T (0, 1, 0)
-    const double w39 = val(9, X + (0 * sI + 1 * sJ + 0));  // mu (0, 1, 0)
-    const double w40 = val(10, X + (0 * sI + 1 * sJ + 0));  // ka (0, 1, 0)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w42 = val(5, X + (1 * sI + 0 * sJ + 0));  // v (1, 0, 0)
-    const double w43 = val(6, X + (1 * sI + 0 * sJ + 0));  // w (1, 0, 0)
-    const double w44 = val(8, X + (1 * sI + 0 * sJ + 0));  // T (1, 0, 0)
-    const double w45 = val(9, X + (1 * sI + 0 * sJ + 0));  // mu (1, 0, 0)
-    const double w46 = val(10, X + (1 * sI + 0 * sJ + 0));  // ka (1, 0, 0)
+    const double l1 = lam(1, 0, 0, 0);
+    const double l2 = lam(2, 0, 0, 0);
+    const double l3 = lam(3, 0, 0, 0);
+    const double l4 = lam(4, 0, 0, 0);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w1 = val(5, -1, 0, 0);  // v (-1, 0, 0)
+    const double w2 = val(6, -1, 0, 0);  // w (-1, 0, 0)
+    const double w3 = val(8, -1, 0, 0);  // T (-1, 0, 0)
+    const double w4 = val(9, -1, 0, 0);  // mu (-1, 0, 0)
+    const double w5 = val(10, -1, 0, 0);  // ka (-1, 0, 0)
+    const double w6 = val(4, 0, -1, 0);  // u (0, -1, 0)
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w8 = val(6, 0, -1, 0);  // w (0, -1, 0)
+    const double w9 = val(8, 0, -1, 0);  // T (0, -1, 0)
+    const double w10 = val(9, 0, -1, 0);  // mu (0, -1, 0)
+    const double w11 = val(10, 0, -1, 0);  // ka (0, -1, 0)
+    const double w12 = val(4, 0, 0, -1);  // u (0, 0, -1)
+    const double w13 = val(5, 0, 0, -1);  // v (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w15 = val(8, 0, 0, -1);  // T (0, 0, -1)
+    const double w16 = val(9, 0, 0, -1);  // mu (0, 0, -1)
+    const double w17 = val(10, 0, 0, -1);  // ka (0, 0, -1)
+    const double w22 = val(4, 0, 0, 0);  // u (0, 0, 0)
+    const double w23 = val(5, 0, 0, 0);  // v (0, 0, 0)
+    const double w24 = val(6, 0, 0, 0);  // w (0, 0, 0)
+    const double w26 = val(8, 0, 0, 0);  // T (0, 0, 0)
+    const double w27 = val(9, 0, 0, 0);  // mu (0, 0, 0)
+    const double w28 = val(10, 0, 0, 0);  // ka (0, 0, 0)
+    const double w29 = val(4, 0, 0, 1);  // u (0, 0, 1)
+    const double w30 = val(5, 0, 0, 1);  // v (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w32 = val(8, 0, 0, 1);  // T (0, 0, 1)
+    const double w33 = val(9, 0, 0, 1);  // mu (0, 0, 1)
+    const double w34 = val(10, 0, 0, 1);  // ka (0, 0, 1)
+    const double w35 = val(4, 0, 1, 0);  // u (0, 1, 0)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w37 = val(6, 0, 1, 0);  // w (0, 1, 0)
+    const double w38 = val(8, 0, 1, 0);  // T (0, 1, 0)
+    const double w39 = val(9, 0, 1, 0);  // mu (0, 1, 0)
+    const double w40 = val(10, 0, 1, 0);  // ka (0, 1, 0)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w42 = val(5, 1, 0, 0);  // v (1, 0, 0)
+    const double w43 = val(6, 1, 0, 0);  // w (1, 0, 0)
+    const double w44 = val(8, 1, 0, 0);  // T (1, 0, 0)
+    const double w45 = val(9, 1, 0, 0);  // mu (1, 0, 0)
+    const double w46 = val(10, 1, 0, 0);  // ka (1, 0, 0)
     bar[4] += l1 * (-C.xm_xx * w45 + (-2.0 * C.xm_xx + -2.0 * C.xm_yy + -2.0 * C.xm_zz) * w27 + -C.xm_xx * w4 + -C.xm_yy * w39 + -C.xm_yy * w10 + -C.xm_zz * w33 + -C.xm_zz * w16) + l4 * (-C.e_xx23 * w45 * w41 + C.e_xx23 * w27 * w41 + (-2.0 * C.e_xx23 + -2.0 * C.e_yy12 + -2.0 * C.e_zz12) * w27 * w22 + (-2.0 * C.e_xx23 + -2.0 * C.e_yy12 + -2.0 * C.e_zz12) * w27 * w22 + -C.e_xx23 * w4 * w0 + C.e_xx23 * w27 * w0 + -C.e_yy12 * w39 * w35 + C.e_yy12 * w27 * w35 + -C.e_yy12 * w10 * w6 + C.e_yy12 * w27 * w6 + -C.e_zz12 * w33 * w29 + C.e_zz12 * w27 * w29 + -C.e_zz12 * w16 * w12 + C.e_zz12 * w27 * w12);  // u
     bar[5] += l2 * (-C.ym_xx * w45 + (-2.0 * C.ym_xx + -2.0 * C.ym_yy + -2.0 * C.ym_zz) * w27 + -C.ym_xx * w4 + -C.ym_yy * w39 + -C.ym_yy * w10 + -C.ym_zz * w33 + -C.ym_zz * w16) + l4 * (-C.e_xx12 * w45 * w42 + C.e_xx12 * w27 * w42 + (-2.0 * C.e_xx12 + -2.0 * C.e_yy23 + -2.0 * C.e_zz12) * w27 * w23 + (-2.0 * C.e_xx12 + -2.0 * C.e_yy23 + -2.0 * C.e_zz12) * w27 * w23 + -C.e_xx12 * w4 * w1 + C.e_xx12 * w27 * w1 + -C.e_yy23 * w39 * w36 + C.e_yy23 * w27 * w36 + -C.e_yy23 * w10 * w7 + C.e_yy23 * w27 * w7 + -C.e_zz12 * w33 * w30 + C.e_zz12 * w27 * w30 + -C.e_zz12 * w16 * w13 + C.e_zz12 * w27 * w13);  // v
     bar[6] += l3 * (-C.zm_xx * w45 + (-2.0 * C.zm_xx + -2.0 * C.zm_yy + -2.0 * C.zm_zz) * w27 + -C.zm_xx * w4 + -C.zm_yy * w39 + -C.zm_yy * w10 + -C.zm_zz * w33 + -C.zm_zz * w16) + l4 * (-C.e_xx12 * w45 * w43 + C.e_xx12 * w27 * w43 + (-2.0 * C.e_xx12 + -2.0 * C.e_yy12 + -2.0 * C.e_zz23) * w27 * w24 + (-2.0 * C.e_xx12 + -2.0 * C.e_yy12 + -2.0 * C.e_zz23) * w27 * w24 + -C.e_xx12 * w4 * w2 + C.e_xx12 * w27 * w2 + -C.e_yy12 * w39 * w37 + C.e_yy12 * w27 * w37 + -C.e_yy12 * w10 * w8 + C.e_yy12 * w27 * w8 + -C.e_zz23 * w33 * w31 + C.e_zz23 * w27 * w31 + -C.e_zz23 * w16 * w14 + C.e_zz23 * w27 * w14);  // w
@@ -73,37 +73,36 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx s
   }
   asm volatile("" ::: "memory");
   if (inner(-1, 0, 0)) {
-    const Idx b = X - (-1 * sI + 0 * sJ + 0);
-    const double l0 = lam(0, b);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w6 = val(4, X + (0 * sI + -1 * sJ + 0));  // u (0, -1, 0)
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w12 = val(4, X + (0 * sI + 0 * sJ + -1));  // u (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w18 = val(0, X + (0 * sI + 0 * sJ + 0));  // RU (0, 0, 0)
-    const double w19 = val(1, X + (0 * sI + 0 * sJ + 0));  // RV (0, 0, 0)
-    const double w20 = val(2, X + (0 * sI + 0 * sJ + 0));  // RW (0, 0, 0)
-    const double w21 = val(3, X + (0 * sI + 0 * sJ + 0));  // RE (0, 0, 0)
-    const double w22 = val(4, X + (0 * sI + 0 * sJ + 0));  // u (0, 0, 0)
-    const double w23 = val(5, X + (0 * sI + 0 * sJ + 0));  // v (0, 0, 0)
-    const double w24 = val(6, X + (0 * sI + 0 * sJ + 0));  // w (0, 0, 0)
-    const double w25 = val(7, X + (0 * sI + 0 * sJ + 0));  // p (0, 0, 0)
-    const double w26 = val(8, X + (0 * sI + 0 * sJ + 0));  // T (0, 0, 0)
-    const double w27 = val(9, X + (0 * sI + 0 * sJ + 0));  // mu (0, 0, 0)
-    const double w28 = val(10, X + (0 * sI + 0 * sJ + 0));  // ka (0, 0, 0)
-    const double w29 = val(4, X + (0 * sI + 0 * sJ + 1));  // u (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w35 = val(4, X + (0 * sI + 1 * sJ + 0));  // u (0, 1, 0)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w42 = val(5, X + (1 * sI + 0 * sJ + 0));  // v (1, 0, 0)
-    const double w43 = val(6, X + (1 * sI + 0 * sJ + 0));  // w (1, 0, 0)
-    const double w44 = val(8, X + (1 * sI + 0 * sJ + 0));  // T (1, 0, 0)
-    const double w45 = val(9, X + (1 * sI + 0 * sJ + 0));  // mu (1, 0, 0)
-    const double w46 = val(10, X + (1 * sI + 0 * sJ + 0));  // ka (1, 0, 0)
+    const double l0 = lam(0, 1, 0, 0);
+    const double l1 = lam(1, 1, 0, 0);
+    const double l2 = lam(2, 1, 0, 0);
+    const double l3 = lam(3, 1, 0, 0);
+    const double l4 = lam(4, 1, 0, 0);
+    const double w6 = val(4, 0, -1, 0);  // u (0, -1, 0)
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w12 = val(4, 0, 0, -1);  // u (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w18 = val(0, 0, 0, 0);  // RU (0, 0, 0)
+    const double w19 = val(1, 0, 0, 0);  // RV (0, 0, 0)
+    const double w20 = val(2, 0, 0, 0);  // RW (0, 0, 0)
+    const double w21 = val(3, 0, 0, 0);  // RE (0, 0, 0)
+    const double w22 = val(4, 0, 0, 0);  // u (0, 0, 0)
+    const double w23 = val(5, 0, 0, 0);  // v (0, 0, 0)
+    const double w24 = val(6, 0, 0, 0);  // w (0, 0, 0)
+    const double w25 = val(7, 0, 0, 0);  // p (0, 0, 0)
+    const double w26 = val(8, 0, 0, 0);  // T (0, 0, 0)
+    const double w27 = val(9, 0, 0, 0);  // mu (0, 0, 0)
+    const double w28 = val(10, 0, 0, 0);  // ka (0, 0, 0)
+    const double w29 = val(4, 0, 0, 1);  // u (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w35 = val(4, 0, 1, 0);  // u (0, 1, 0)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w42 = val(5, 1, 0, 0);  // v (1, 0, 0)
+    const double w43 = val(6, 1, 0, 0);  // w (1, 0, 0)
+    const double w44 = val(8, 1, 0, 0);  // T (1, 0, 0)
+    const double w45 = val(9, 1, 0, 0);  // mu (1, 0, 0)
+    const double w46 = val(10, 1, 0, 0);  // ka (1, 0, 0)
     bar[0] += l0 * -C.ax + l1 * -C.ax * w22;  // RU
     bar[1] += l2 * -C.ax * w22;  // RV
     bar[2] += l3 * -C.ax * w22;  // RW
@@ -118,37 +117,36 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx s
   }
   asm volatile("" ::: "memory");
   if (inner(0, -1, 0)) {
-    const Idx b = X - (0 * sI + -1 * sJ + 0);
-    const double l0 = lam(0, b);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w1 = val(5, X + (-1 * sI + 0 * sJ + 0));  // v (-1, 0, 0)
-    const double w13 = val(5, X + (0 * sI + 0 * sJ + -1));  // v (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w18 = val(0, X + (0 * sI + 0 * sJ + 0));  // RU (0, 0, 0)
-    const double w19 = val(1, X + (0 * sI + 0 * sJ + 0));  // RV (0, 0, 0)
-    const double w20 = val(2, X + (0 * sI + 0 * sJ + 0));  // RW (0, 0, 0)
-    const double w21 = val(3, X + (0 * sI + 0 * sJ + 0));  // RE (0, 0, 0)
-    const double w22 = val(4, X + (0 * sI + 0 * sJ + 0));  // u (0, 0, 0)
-    const double w23 = val(5, X + (0 * sI + 0 * sJ + 0));  // v (0, 0, 0)
-    const double w24 = val(6, X + (0 * sI + 0 * sJ + 0));  // w (0, 0, 0)
-    const double w25 = val(7, X + (0 * sI + 0 * sJ + 0));  // p (0, 0, 0)
-    const double w26 = val(8, X + (0 * sI + 0 * sJ + 0));  // T (0, 0, 0)
-    const double w27 = val(9, X + (0 * sI + 0 * sJ + 0));  // mu (0, 0, 0)
-    const double w28 = val(10, X + (0 * sI + 0 * sJ + 0));  // ka (0, 0, 0)
-    const double w30 = val(5, X + (0 * sI + 0 * sJ + 1));  // v (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w35 = val(4, X + (0 * sI + 1 * sJ + 0));  // u (0, 1, 0)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w37 = val(6, X + (0 * sI + 1 * sJ + 0));  // w (0, 1, 0)
-    const double w38 = val(8, X + (0 * sI + 1 * sJ + 0));  // T (0, 1, 0)
-    const double w39 = val(9, X + (0 * sI + 1 * sJ + 0));  // mu (0, 1, 0)
-    const double w40 = val(10, X + (0 * sI + 1 * sJ + 0));  // ka (0, 1, 0)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w42 = val(5, X + (1 * sI + 0 * sJ + 0));  // v (1, 0, 0)
+    const double l0 = lam(0, 0, 1, 0);
+    const double l1 = lam(1, 0, 1, 0);
+    const double l2 = lam(2, 0, 1, 0);
+    const double l3 = lam(3, 0, 1, 0);
+    const double l4 = lam(4, 0, 1, 0);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w1 = val(5, -1, 0, 0);  // v (-1, 0, 0)
+    const double w13 = val(5, 0, 0, -1);  // v (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w18 = val(0, 0, 0, 0);  // RU (0, 0, 0)
+    const double w19 = val(1, 0, 0, 0);  // RV (0, 0, 0)
+    const double w20 = val(2, 0, 0, 0);  // RW (0, 0, 0)
+    const double w21 = val(3, 0, 0, 0);  // RE (0, 0, 0)
+    const double w22 = val(4, 0, 0, 0);  // u (0, 0, 0)
+    const double w23 = val(5, 0, 0, 0);  // v (0, 0, 0)
+    const double w24 = val(6, 0, 0, 0);  // w (0, 0, 0)
+    const double w25 = val(7, 0, 0, 0);  // p (0, 0, 0)
+    const double w26 = val(8, 0, 0, 0);  // T (0, 0, 0)
+    const double w27 = val(9, 0, 0, 0);  // mu (0, 0, 0)
+    const double w28 = val(10, 0, 0, 0);  // ka (0, 0, 0)
+    const double w30 = val(5, 0, 0, 1);  // v (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w35 = val(4, 0, 1, 0);  // u (0, 1, 0)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w37 = val(6, 0, 1, 0);  // w (0, 1, 0)
+    const double w38 = val(8, 0, 1, 0);  // T (0, 1, 0)
+    const double w39 = val(9, 0, 1, 0);  // mu (0, 1, 0)
+    const double w40 = val(10, 0, 1, 0);  // ka (0, 1, 0)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w42 = val(5, 1, 0, 0);  // v (1, 0, 0)
     bar[0] += l1 * -C.ay * w23;  // RU
     bar[1] += l0 * -C.ay + l2 * -C.ay * w23;  // RV
     bar[2] += l3 * -C.ay * w23;  // RW
@@ -163,37 +161,36 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx s
   }
   asm volatile("" ::: "memory");
   if (inner(0, 0, -1)) {
-    const Idx b = X - (0 * sI + 0 * sJ + -1);
-    const double l0 = lam(0, b);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w2 = val(6, X + (-1 * sI + 0 * sJ + 0));  // w (-1, 0, 0)
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w8 = val(6, X + (0 * sI + -1 * sJ + 0));  // w (0, -1, 0)
-    const double w18 = val(0, X + (0 * sI + 0 * sJ + 0));  // RU (0, 0, 0)
-    const double w19 = val(1, X + (0 * sI + 0 * sJ + 0));  // RV (0, 0, 0)
-    const double w20 = val(2, X + (0 * sI + 0 * sJ + 0));  // RW (0, 0, 0)
-    const double w21 = val(3, X + (0 * sI + 0 * sJ + 0));  // RE (0, 0, 0)
-    const double w22 = val(4, X + (0 * sI + 0 * sJ + 0));  // u (0, 0, 0)
-    const double w23 = val(5, X + (0 * sI + 0 * sJ + 0));  // v (0, 0, 0)
-    const double w24 = val(6, X + (0 * sI + 0 * sJ + 0));  // w (0, 0, 0)
-    const double w25 = val(7, X + (0 * sI + 0 * sJ + 0));  // p (0, 0, 0)
-    const double w26 = val(8, X + (0 * sI + 0 * sJ + 0));  // T (0, 0, 0)
-    const double w27 = val(9, X + (0 * sI + 0 * sJ + 0));  // mu (0, 0, 0)
-    const double w28 = val(10, X + (0 * sI + 0 * sJ + 0));  // ka (0, 0, 0)
-    const double w29 = val(4, X + (0 * sI + 0 * sJ + 1));  // u (0, 0, 1)
-    const double w30 = val(5, X + (0 * sI + 0 * sJ + 1));  // v (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w32 = val(8, X + (0 * sI + 0 * sJ + 1));  // T (0, 0, 1)
-    const double w33 = val(9, X + (0 * sI + 0 * sJ + 1));  // mu (0, 0, 1)
-    const double w34 = val(10, X + (0 * sI + 0 * sJ + 1));  // ka (0, 0, 1)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w37 = val(6, X + (0 * sI + 1 * sJ + 0));  // w (0, 1, 0)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w43 = val(6, X + (1 * sI + 0 * sJ + 0));  // w (1, 0, 0)
+    const double l0 = lam(0, 0, 0, 1);
+    const double l1 = lam(1, 0, 0, 1);
+    const double l2 = lam(2, 0, 0, 1);
+    const double l3 = lam(3, 0, 0, 1);
+    const double l4 = lam(4, 0, 0, 1);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w2 = val(6, -1, 0, 0);  // w (-1, 0, 0)
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w8 = val(6, 0, -1, 0);  // w (0, -1, 0)
+    const double w18 = val(0, 0, 0, 0);  // RU (0, 0, 0)
+    const double w19 = val(1, 0, 0, 0);  // RV (0, 0, 0)
+    const double w20 = val(2, 0, 0, 0);  // RW (0, 0, 0)
+    const double w21 = val(3, 0, 0, 0);  // RE (0, 0, 0)
+    const double w22 = val(4, 0, 0, 0);  // u (0, 0, 0)
+    const double w23 = val(5, 0, 0, 0);  // v (0, 0, 0)
+    const double w24 = val(6, 0, 0, 0);  // w (0, 0, 0)
+    const double w25 = val(7, 0, 0, 0);  // p (0, 0, 0)
+    const double w26 = val(8, 0, 0, 0);  // T (0, 0, 0)
+    const double w27 = val(9, 0, 0, 0);  // mu (0, 0, 0)
+    const double w28 = val(10, 0, 0, 0);  // ka (0, 0, 0)
+    const double w29 = val(4, 0, 0, 1);  // u (0, 0, 1)
+    const double w30 = val(5, 0, 0, 1);  // v (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w32 = val(8, 0, 0, 1);  // T (0, 0, 1)
+    const double w33 = val(9, 0, 0, 1);  // mu (0, 0, 1)
+    const double w34 = val(10, 0, 0, 1);  // ka (0, 0, 1)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w37 = val(6, 0, 1, 0);  // w (0, 1, 0)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w43 = val(6, 1, 0, 0);  // w (1, 0, 0)
     bar[0] += l1 * -C.az * w24;  // RU
     bar[1] += l2 * -C.az * w24;  // RV
     bar[2] += l0 * -C.az + l3 * -C.az * w24;  // RW
@@ -208,37 +205,36 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx s
   }
   asm volatile("" ::: "memory");
   if (inner(0, 0, 1)) {
-    const Idx b = X - (0 * sI + 0 * sJ + 1);
-    const double l0 = lam(0, b);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w2 = val(6, X + (-1 * sI + 0 * sJ + 0));  // w (-1, 0, 0)
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w8 = val(6, X + (0 * sI + -1 * sJ + 0));  // w (0, -1, 0)
-    const double w12 = val(4, X + (0 * sI + 0 * sJ + -1));  // u (0, 0, -1)
-    const double w13 = val(5, X + (0 * sI + 0 * sJ + -1));  // v (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w15 = val(8, X + (0 * sI + 0 * sJ + -1));  // T (0, 0, -1)
-    const double w16 = val(9, X + (0 * sI + 0 * sJ + -1));  // mu (0, 0, -1)
-    const double w17 = val(10, X + (0 * sI + 0 * sJ + -1));  // ka (0, 0, -1)
-    const double w18 = val(0, X + (0 * sI + 0 * sJ + 0));  // RU (0, 0, 0)
-    const double w19 = val(1, X + (0 * sI + 0 * sJ + 0));  // RV (0, 0, 0)
-    const double w20 = val(2, X + (0 * sI + 0 * sJ + 0));  // RW (0, 0, 0)
-    const double w21 = val(3, X + (0 * sI + 0 * sJ + 0));  // RE (0, 0, 0)
-    const double w22 = val(4, X + (0 * sI + 0 * sJ + 0));  // u (0, 0, 0)
-    const double w23 = val(5, X + (0 * sI + 0 * sJ + 0));  // v (0, 0, 0)
-    const double w24 = val(6, X + (0 * sI + 0 * sJ + 0));  // w (0, 0, 0)
-    const double w25 = val(7, X + (0 * sI + 0 * sJ + 0));  // p (0, 0, 0)
-    const double w26 = val(8, X + (0 * sI + 0 * sJ + 0));  // T (0, 0, 0)
-    const double w27 = val(9, X + (0 * sI + 0 * sJ + 0));  // mu (0, 0, 0)
-    const double w28 = val(10, X + (0 * sI + 0 * sJ + 0));  // ka (0, 0, 0)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w37 = val(6, X + (0 * sI + 1 * sJ + 0));  // w (0, 1, 0)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w43 = val(6, X + (1 * sI + 0 * sJ + 0));  // w (1, 0, 0)
+    const double l0 = lam(0, 0, 0, -1);
+    const double l1 = lam(1, 0, 0, -1);
+    const double l2 = lam(2, 0, 0, -1);
+    const double l3 = lam(3, 0, 0, -1);
+    const double l4 = lam(4, 0, 0, -1);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w2 = val(6, -1, 0, 0);  // w (-1, 0, 0)
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w8 = val(6, 0, -1, 0);  // w (0, -1, 0)
+    const double w12 = val(4, 0, 0, -1);  // u (0, 0, -1)
+    const double w13 = val(5, 0, 0, -1);  // v (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w15 = val(8, 0, 0, -1);  // T (0, 0, -1)
+    const double w16 = val(9, 0, 0, -1);  // mu (0, 0, -1)
+    const double w17 = val(10, 0, 0, -1);  // ka (0, 0, -1)
+    const double w18 = val(0, 0, 0, 0);  // RU (0, 0, 0)
+    const double w19 = val(1, 0, 0, 0);  // RV (0, 0, 0)
+    const double w20 = val(2, 0, 0, 0);  // RW (0, 0, 0)
+    const double w21 = val(3, 0, 0, 0);  // RE (0, 0, 0)
+    const double w22 = val(4, 0, 0, 0);  // u (0, 0, 0)
+    const double w23 = val(5, 0, 0, 0);  // v (0, 0, 0)
+    const double w24 = val(6, 0, 0, 0);  // w (0, 0, 0)
+    const double w25 = val(7, 0, 0, 0);  // p (0, 0, 0)
+    const double w26 = val(8, 0, 0, 0);  // T (0, 0, 0)
+    const double w27 = val(9, 0, 0, 0);  // mu (0, 0, 0)
+    const double w28 = val(10, 0, 0, 0);  // ka (0, 0, 0)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w37 = val(6, 0, 1, 0);  // w (0, 1, 0)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w43 = val(6, 1, 0, 0);  // w (1, 0, 0)
     bar[0] += l1 * C.az * w24;  // RU
     bar[1] += l2 * C.az * w24;  // RV
     bar[2] += l0 * C.az + l3 * C.az * w24;  // RW
@@ -253,37 +249,36 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx s
   }
   asm volatile("" ::: "memory");
   if (inner(0, 1, 0)) {
-    const Idx b = X - (0 * sI + 1 * sJ + 0);
-    const double l0 = lam(0, b);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w1 = val(5, X + (-1 * sI + 0 * sJ + 0));  // v (-1, 0, 0)
-    const double w6 = val(4, X + (0 * sI + -1 * sJ + 0));  // u (0, -1, 0)
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w8 = val(6, X + (0 * sI + -1 * sJ + 0));  // w (0, -1, 0)
-    const double w9 = val(8, X + (0 * sI + -1 * sJ + 0));  // T (0, -1, 0)
-    const double w10 = val(9, X + (0 * sI + -1 * sJ + 0));  // mu (0, -1, 0)
-    const double w11 = val(10, X + (0 * sI + -1 * sJ + 0));  // ka (0, -1, 0)
-    const double w13 = val(5, X + (0 * sI + 0 * sJ + -1));  // v (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w18 = val(0, X + (0 * sI + 0 * sJ + 0));  // RU (0, 0, 0)
-    const double w19 = val(1, X + (0 * sI + 0 * sJ + 0));  // RV (0, 0, 0)
-    const double w20 = val(2, X + (0 * sI + 0 * sJ + 0));  // RW (0, 0, 0)
-    const double w21 = val(3, X + (0 * sI + 0 * sJ + 0));  // RE (0, 0, 0)
-    const double w22 = val(4, X + (0 * sI + 0 * sJ + 0));  // u (0, 0, 0)
-    const double w23 = val(5, X + (0 * sI + 0 * sJ + 0));  // v (0, 0, 0)
-    const double w24 = val(6, X + (0 * sI + 0 * sJ + 0));  // w (0, 0, 0)
-    const double w25 = val(7, X + (0 * sI + 0 * sJ + 0));  // p (0, 0, 0)
-    const double w26 = val(8, X + (0 * sI + 0 * sJ + 0));  // T (0, 0, 0)
-    const double w27 = val(9, X + (0 * sI + 0 * sJ + 0));  // mu (0, 0, 0)
-    const double w28 = val(10, X + (0 * sI + 0 * sJ + 0));  // ka (0, 0, 0)
-    const double w30 = val(5, X + (0 * sI + 0 * sJ + 1));  // v (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w42 = val(5, X + (1 * sI + 0 * sJ + 0));  // v (1, 0, 0)
+    const double l0 = lam(0, 0, -1, 0);
+    const double l1 = lam(1, 0, -1, 0);
+    const double l2 = lam(2, 0, -1, 0);
+    const double l3 = lam(3, 0, -1, 0);
+    const double l4 = lam(4, 0, -1, 0);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w1 = val(5, -1, 0, 0);  // v (-1, 0, 0)
+    const double w6 = val(4, 0, -1, 0);  // u (0, -1, 0)
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w8 = val(6, 0, -1, 0);  // w (0, -1, 0)
+    const double w9 = val(8, 0, -1, 0);  // T (0, -1, 0)
+    const double w10 = val(9, 0, -1, 0);  // mu (0, -1, 0)
+    const double w11 = val(10, 0, -1, 0);  // ka (0, -1, 0)
+    const double w13 = val(5, 0, 0, -1);  // v (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w18 = val(0, 0, 0, 0);  // RU (0, 0, 0)
+    const double w19 = val(1, 0, 0, 0);  // RV (0, 0, 0)
+    const double w20 = val(2, 0, 0, 0);  // RW (0, 0, 0)
+    const double w21 = val(3, 0, 0, 0);  // RE (0, 0, 0)
+    const double w22 = val(4, 0, 0, 0);  // u (0, 0, 0)
+    const double w23 = val(5, 0, 0, 0);  // v (0, 0, 0)
+    const double w24 = val(6, 0, 0, 0);  // w (0, 0, 0)
+    const double w25 = val(7, 0, 0, 0);  // p (0, 0, 0)
+    const double w26 = val(8, 0, 0, 0);  // T (0, 0, 0)
+    const double w27 = val(9, 0, 0, 0);  // mu (0, 0, 0)
+    const double w28 = val(10, 0, 0, 0);  // ka (0, 0, 0)
+    const double w30 = val(5, 0, 0, 1);  // v (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w42 = val(5, 1, 0, 0);  // v (1, 0, 0)
     bar[0] += l1 * C.ay * w23;  // RU
     bar[1] += l0 * C.ay + l2 * C.ay * w23;  // RV
     bar[2] += l3 * C.ay * w23;  // RW
@@ -298,37 +293,36 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx s
   }
   asm volatile("" ::: "memory");
   if (inner(1, 0, 0)) {
-    const Idx b = X - (1 * sI + 0 * sJ + 0);
-    const double l0 = lam(0, b);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w1 = val(5, X + (-1 * sI + 0 * sJ + 0));  // v (-1, 0, 0)
-    const double w2 = val(6, X + (-1 * sI + 0 * sJ + 0));  // w (-1, 0, 0)
-    const double w3 = val(8, X + (-1 * sI + 0 * sJ + 0));  // T (-1, 0, 0)
-    const double w4 = val(9, X + (-1 * sI + 0 * sJ + 0));  // mu (-1, 0, 0)
-    const double w5 = val(10, X + (-1 * sI + 0 * sJ + 0));  // ka (-1, 0, 0)
-    const double w6 = val(4, X + (0 * sI + -1 * sJ + 0));  // u (0, -1, 0)
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w12 = val(4, X + (0 * sI + 0 * sJ + -1));  // u (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w18 = val(0, X + (0 * sI + 0 * sJ + 0));  // RU (0, 0, 0)
-    const double w19 = val(1, X + (0 * sI + 0 * sJ + 0));  // RV (0, 0, 0)
-    const double w20 = val(2, X + (0 * sI + 0 * sJ + 0));  // RW (0, 0, 0)
-    const double w21 = val(3, X + (0 * sI + 0 * sJ + 0));  // RE (0, 0, 0)
-    const double w22 = val(4, X + (0 * sI + 0 * sJ + 0));  // u (0, 0, 0)
-    const double w23 = val(5, X + (0 * sI + 0 * sJ + 0));  // v (0, 0, 0)
-    const double w24 = val(6, X + (0 * sI + 0 * sJ + 0));  // w (0, 0, 0)
-    const double w25 = val(7, X + (0 * sI + 0 * sJ + 0));  // p (0, 0, 0)
-    const double w26 = val(8, X + (0 * sI + 0 * sJ + 0));  // T (0, 0, 0)
-    const double w27 = val(9, X + (0 * sI + 0 * sJ + 0));  // mu (0, 0, 0)
-    const double w28 = val(10, X + (0 * sI + 0 * sJ + 0));  // ka (0, 0, 0)
-    const double w29 = val(4, X + (0 * sI + 0 * sJ + 1));  // u (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w35 = val(4, X + (0 * sI + 1 * sJ + 0));  // u (0, 1, 0)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
+    const double l0 = lam(0, -1, 0, 0);
+    const double l1 = lam(1, -1, 0, 0);
+    const double l2 = lam(2, -1, 0, 0);
+    const double l3 = lam(3, -1, 0, 0);
+    const double l4 = lam(4, -1, 0, 0);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w1 = val(5, -1, 0, 0);  // v (-1, 0, 0)
+    const double w2 = val(6, -1, 0, 0);  // w (-1, 0, 0)
+    const double w3 = val(8, -1, 0, 0);  // T (-1, 0, 0)
+    const double w4 = val(9, -1, 0, 0);  // mu (-1, 0, 0)
+    const double w5 = val(10, -1, 0, 0);  // ka (-1, 0, 0)
+    const double w6 = val(4, 0, -1, 0);  // u (0, -1, 0)
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w12 = val(4, 0, 0, -1);  // u (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w18 = val(0, 0, 0, 0);  // RU (0, 0, 0)
+    const double w19 = val(1, 0, 0, 0);  // RV (0, 0, 0)
+    const double w20 = val(2, 0, 0, 0);  // RW (0, 0, 0)
+    const double w21 = val(3, 0, 0, 0);  // RE (0, 0, 0)
+    const double w22 = val(4, 0, 0, 0);  // u (0, 0, 0)
+    const double w23 = val(5, 0, 0, 0);  // v (0, 0, 0)
+    const double w24 = val(6, 0, 0, 0);  // w (0, 0, 0)
+    const double w25 = val(7, 0, 0, 0);  // p (0, 0, 0)
+    const double w26 = val(8, 0, 0, 0);  // T (0, 0, 0)
+    const double w27 = val(9, 0, 0, 0);  // mu (0, 0, 0)
+    const double w28 = val(10, 0, 0, 0);  // ka (0, 0, 0)
+    const double w29 = val(4, 0, 0, 1);  // u (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w35 = val(4, 0, 1, 0);  // u (0, 1, 0)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
     bar[0] += l0 * C.ax + l1 * C.ax * w22;  // RU
     bar[1] += l2 * C.ax * w22;  // RV
     bar[2] += l3 * C.ax * w22;  // RW
@@ -343,181 +337,169 @@ __device__ __forceinline__ void rhs_adjoint_gather(const Consts& C, Idx X, Idx s
   }
   asm volatile("" ::: "memory");
   if (inner(-1, -1, 0)) {
-    const Idx b = X - (-1 * sI + -1 * sJ + 0);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l4 = lam(4, b);
-    const double w35 = val(4, X + (0 * sI + 1 * sJ + 0));  // u (0, 1, 0)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w39 = val(9, X + (0 * sI + 1 * sJ + 0));  // mu (0, 1, 0)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w42 = val(5, X + (1 * sI + 0 * sJ + 0));  // v (1, 0, 0)
-    const double w45 = val(9, X + (1 * sI + 0 * sJ + 0));  // mu (1, 0, 0)
+    const double l1 = lam(1, 1, 1, 0);
+    const double l2 = lam(2, 1, 1, 0);
+    const double l4 = lam(4, 1, 1, 0);
+    const double w35 = val(4, 0, 1, 0);  // u (0, 1, 0)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w39 = val(9, 0, 1, 0);  // mu (0, 1, 0)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w42 = val(5, 1, 0, 0);  // v (1, 0, 0)
+    const double w45 = val(9, 1, 0, 0);  // mu (1, 0, 0)
     bar[4] += l2 * (C.ym_yx * w39 + C.ym_xy * w45) + l4 * (C.e_yx4 * w39 * w36 + C.e_yx6 * w45 * w42);  // u
     bar[5] += l1 * (C.xm_xy * w45 + C.xm_yx * w39) + l4 * (C.e_yx6 * w39 * w35 + C.e_yx4 * w45 * w41);  // v
   }
   asm volatile("" ::: "memory");
   if (inner(-1, 0, -1)) {
-    const Idx b = X - (-1 * sI + 0 * sJ + -1);
-    const double l1 = lam(1, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w29 = val(4, X + (0 * sI + 0 * sJ + 1));  // u (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w33 = val(9, X + (0 * sI + 0 * sJ + 1));  // mu (0, 0, 1)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w43 = val(6, X + (1 * sI + 0 * sJ + 0));  // w (1, 0, 0)
-    const double w45 = val(9, X + (1 * sI + 0 * sJ + 0));  // mu (1, 0, 0)
+    const double l1 = lam(1, 1, 0, 1);
+    const double l3 = lam(3, 1, 0, 1);
+    const double l4 = lam(4, 1, 0, 1);
+    const double w29 = val(4, 0, 0, 1);  // u (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w33 = val(9, 0, 0, 1);  // mu (0, 0, 1)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w43 = val(6, 1, 0, 0);  // w (1, 0, 0)
+    const double w45 = val(9, 1, 0, 0);  // mu (1, 0, 0)
     bar[4] += l3 * (C.zm_zx * w33 + C.zm_xz * w45) + l4 * (C.e_zx4 * w33 * w31 + C.e_zx6 * w45 * w43);  // u
     bar[6] += l1 * (C.xm_xz * w45 + C.xm_zx * w33) + l4 * (C.e_zx6 * w33 * w29 + C.e_zx4 * w45 * w41);  // w
   }
   asm volatile("" ::: "memory");
   if (inner(-1, 0, 1)) {
-    const Idx b = X - (-1 * sI + 0 * sJ + 1);
-    const double l1 = lam(1, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w12 = val(4, X + (0 * sI + 0 * sJ + -1));  // u (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w16 = val(9, X + (0 * sI + 0 * sJ + -1));  // mu (0, 0, -1)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w43 = val(6, X + (1 * sI + 0 * sJ + 0));  // w (1, 0, 0)
-    const double w45 = val(9, X + (1 * sI + 0 * sJ + 0));  // mu (1, 0, 0)
+    const double l1 = lam(1, 1, 0, -1);
+    const double l3 = lam(3, 1, 0, -1);
+    const double l4 = lam(4, 1, 0, -1);
+    const double w12 = val(4, 0, 0, -1);  // u (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w16 = val(9, 0, 0, -1);  // mu (0, 0, -1)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w43 = val(6, 1, 0, 0);  // w (1, 0, 0)
+    const double w45 = val(9, 1, 0, 0);  // mu (1, 0, 0)
     bar[4] += l3 * (-C.zm_zx * w16 + -C.zm_xz * w45) + l4 * (-C.e_zx4 * w16 * w14 + -C.e_zx6 * w45 * w43);  // u
     bar[6] += l1 * (-C.xm_xz * w45 + -C.xm_zx * w16) + l4 * (-C.e_zx6 * w16 * w12 + -C.e_zx4 * w45 * w41);  // w
   }
   asm volatile("" ::: "memory");
   if (inner(-1, 1, 0)) {
-    const Idx b = X - (-1 * sI + 1 * sJ + 0);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l4 = lam(4, b);
-    const double w6 = val(4, X + (0 * sI + -1 * sJ + 0));  // u (0, -1, 0)
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w10 = val(9, X + (0 * sI + -1 * sJ + 0));  // mu (0, -1, 0)
-    const double w41 = val(4, X + (1 * sI + 0 * sJ + 0));  // u (1, 0, 0)
-    const double w42 = val(5, X + (1 * sI + 0 * sJ + 0));  // v (1, 0, 0)
-    const double w45 = val(9, X + (1 * sI + 0 * sJ + 0));  // mu (1, 0, 0)
+    const double l1 = lam(1, 1, -1, 0);
+    const double l2 = lam(2, 1, -1, 0);
+    const double l4 = lam(4, 1, -1, 0);
+    const double w6 = val(4, 0, -1, 0);  // u (0, -1, 0)
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w10 = val(9, 0, -1, 0);  // mu (0, -1, 0)
+    const double w41 = val(4, 1, 0, 0);  // u (1, 0, 0)
+    const double w42 = val(5, 1, 0, 0);  // v (1, 0, 0)
+    const double w45 = val(9, 1, 0, 0);  // mu (1, 0, 0)
     bar[4] += l2 * (-C.ym_yx * w10 + -C.ym_xy * w45) + l4 * (-C.e_yx4 * w10 * w7 + -C.e_yx6 * w45 * w42);  // u
     bar[5] += l1 * (-C.xm_xy * w45 + -C.xm_yx * w10) + l4 * (-C.e_yx6 * w10 * w6 + -C.e_yx4 * w45 * w41);  // v
   }
   asm volatile("" ::: "memory");
   if (inner(0, -1, -1)) {
-    const Idx b = X - (0 * sI + -1 * sJ + -1);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w30 = val(5, X + (0 * sI + 0 * sJ + 1));  // v (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w33 = val(9, X + (0 * sI + 0 * sJ + 1));  // mu (0, 0, 1)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w37 = val(6, X + (0 * sI + 1 * sJ + 0));  // w (0, 1, 0)
-    const double w39 = val(9, X + (0 * sI + 1 * sJ + 0));  // mu (0, 1, 0)
+    const double l2 = lam(2, 0, 1, 1);
+    const double l3 = lam(3, 0, 1, 1);
+    const double l4 = lam(4, 0, 1, 1);
+    const double w30 = val(5, 0, 0, 1);  // v (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w33 = val(9, 0, 0, 1);  // mu (0, 0, 1)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w37 = val(6, 0, 1, 0);  // w (0, 1, 0)
+    const double w39 = val(9, 0, 1, 0);  // mu (0, 1, 0)
     bar[5] += l3 * (C.zm_zy * w33 + C.zm_yz * w39) + l4 * (C.e_zy4 * w33 * w31 + C.e_zy6 * w39 * w37);  // v
     bar[6] += l2 * (C.ym_yz * w39 + C.ym_zy * w33) + l4 * (C.e_zy6 * w33 * w30 + C.e_zy4 * w39 * w36);  // w
   }
   asm volatile("" ::: "memory");
   if (inner(0, -1, 1)) {
-    const Idx b = X - (0 * sI + -1 * sJ + 1);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w13 = val(5, X + (0 * sI + 0 * sJ + -1));  // v (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w16 = val(9, X + (0 * sI + 0 * sJ + -1));  // mu (0, 0, -1)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w37 = val(6, X + (0 * sI + 1 * sJ + 0));  // w (0, 1, 0)
-    const double w39 = val(9, X + (0 * sI + 1 * sJ + 0));  // mu (0, 1, 0)
+    const double l2 = lam(2, 0, 1, -1);
+    const double l3 = lam(3, 0, 1, -1);
+    const double l4 = lam(4, 0, 1, -1);
+    const double w13 = val(5, 0, 0, -1);  // v (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w16 = val(9, 0, 0, -1);  // mu (0, 0, -1)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w37 = val(6, 0, 1, 0);  // w (0, 1, 0)
+    const double w39 = val(9, 0, 1, 0);  // mu (0, 1, 0)
     bar[5] += l3 * (-C.zm_zy * w16 + -C.zm_yz * w39) + l4 * (-C.e_zy4 * w16 * w14 + -C.e_zy6 * w39 * w37);  // v
     bar[6] += l2 * (-C.ym_yz * w39 + -C.ym_zy * w16) + l4 * (-C.e_zy6 * w16 * w13 + -C.e_zy4 * w39 * w36);  // w
   }
   asm volatile("" ::: "memory");
   if (inner(0, 1, -1)) {
-    const Idx b = X - (0 * sI + 1 * sJ + -1);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w8 = val(6, X + (0 * sI + -1 * sJ + 0));  // w (0, -1, 0)
-    const double w10 = val(9, X + (0 * sI + -1 * sJ + 0));  // mu (0, -1, 0)
-    const double w30 = val(5, X + (0 * sI + 0 * sJ + 1));  // v (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w33 = val(9, X + (0 * sI + 0 * sJ + 1));  // mu (0, 0, 1)
+    const double l2 = lam(2, 0, -1, 1);
+    const double l3 = lam(3, 0, -1, 1);
+    const double l4 = lam(4, 0, -1, 1);
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w8 = val(6, 0, -1, 0);  // w (0, -1, 0)
+    const double w10 = val(9, 0, -1, 0);  // mu (0, -1, 0)
+    const double w30 = val(5, 0, 0, 1);  // v (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w33 = val(9, 0, 0, 1);  // mu (0, 0, 1)
     bar[5] += l3 * (-C.zm_zy * w33 + -C.zm_yz * w10) + l4 * (-C.e_zy4 * w33 * w31 + -C.e_zy6 * w10 * w8);  // v
     bar[6] += l2 * (-C.ym_yz * w10 + -C.ym_zy * w33) + l4 * (-C.e_zy6 * w33 * w30 + -C.e_zy4 * w10 * w7);  // w
   }
   asm volatile("" ::: "memory");
   if (inner(0, 1, 1)) {
-    const Idx b = X - (0 * sI + 1 * sJ + 1);
-    const double l2 = lam(2, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w8 = val(6, X + (0 * sI + -1 * sJ + 0));  // w (0, -1, 0)
-    const double w10 = val(9, X + (0 * sI + -1 * sJ + 0));  // mu (0, -1, 0)
-    const double w13 = val(5, X + (0 * sI + 0 * sJ + -1));  // v (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w16 = val(9, X + (0 * sI + 0 * sJ + -1));  // mu (0, 0, -1)
+    const double l2 = lam(2, 0, -1, -1);
+    const double l3 = lam(3, 0, -1, -1);
+    const double l4 = lam(4, 0, -1, -1);
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w8 = val(6, 0, -1, 0);  // w (0, -1, 0)
+    const double w10 = val(9, 0, -1, 0);  // mu (0, -1, 0)
+    const double w13 = val(5, 0, 0, -1);  // v (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w16 = val(9, 0, 0, -1);  // mu (0, 0, -1)
     bar[5] += l3 * (C.zm_zy * w16 + C.zm_yz * w10) + l4 * (C.e_zy4 * w16 * w14 + C.e_zy6 * w10 * w8);  // v
     bar[6] += l2 * (C.ym_yz * w10 + C.ym_zy * w16) + l4 * (C.e_zy6 * w16 * w13 + C.e_zy4 * w10 * w7);  // w
   }
   asm volatile("" ::: "memory");
   if (inner(1, -1, 0)) {
-    const Idx b = X - (1 * sI + -1 * sJ + 0);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w1 = val(5, X + (-1 * sI + 0 * sJ + 0));  // v (-1, 0, 0)
-    const double w4 = val(9, X + (-1 * sI + 0 * sJ + 0));  // mu (-1, 0, 0)
-    const double w35 = val(4, X + (0 * sI + 1 * sJ + 0));  // u (0, 1, 0)
-    const double w36 = val(5, X + (0 * sI + 1 * sJ + 0));  // v (0, 1, 0)
-    const double w39 = val(9, X + (0 * sI + 1 * sJ + 0));  // mu (0, 1, 0)
+    const double l1 = lam(1, -1, 1, 0);
+    const double l2 = lam(2, -1, 1, 0);
+    const double l4 = lam(4, -1, 1, 0);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w1 = val(5, -1, 0, 0);  // v (-1, 0, 0)
+    const double w4 = val(9, -1, 0, 0);  // mu (-1, 0, 0)
+    const double w35 = val(4, 0, 1, 0);  // u (0, 1, 0)
+    const double w36 = val(5, 0, 1, 0);  // v (0, 1, 0)
+    const double w39 = val(9, 0, 1, 0);  // mu (0, 1, 0)
     bar[4] += l2 * (-C.ym_yx * w39 + -C.ym_xy * w4) + l4 * (-C.e_yx4 * w39 * w36 + -C.e_yx6 * w4 * w1);  // u
     bar[5] += l1 * (-C.xm_xy * w4 + -C.xm_yx * w39) + l4 * (-C.e_yx6 * w39 * w35 + -C.e_yx4 * w4 * w0);  // v
   }
   asm volatile("" ::: "memory");
   if (inner(1, 0, -1)) {
-    const Idx b = X - (1 * sI + 0 * sJ + -1);
-    const double l1 = lam(1, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w2 = val(6, X + (-1 * sI + 0 * sJ + 0));  // w (-1, 0, 0)
-    const double w4 = val(9, X + (-1 * sI + 0 * sJ + 0));  // mu (-1, 0, 0)
-    const double w29 = val(4, X + (0 * sI + 0 * sJ + 1));  // u (0, 0, 1)
-    const double w31 = val(6, X + (0 * sI + 0 * sJ + 1));  // w (0, 0, 1)
-    const double w33 = val(9, X + (0 * sI + 0 * sJ + 1));  // mu (0, 0, 1)
+    const double l1 = lam(1, -1, 0, 1);
+    const double l3 = lam(3, -1, 0, 1);
+    const double l4 = lam(4, -1, 0, 1);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w2 = val(6, -1, 0, 0);  // w (-1, 0, 0)
+    const double w4 = val(9, -1, 0, 0);  // mu (-1, 0, 0)
+    const double w29 = val(4, 0, 0, 1);  // u (0, 0, 1)
+    const double w31 = val(6, 0, 0, 1);  // w (0, 0, 1)
+    const double w33 = val(9, 0, 0, 1);  // mu (0, 0, 1)
     bar[4] += l3 * (-C.zm_zx * w33 + -C.zm_xz * w4) + l4 * (-C.e_zx4 * w33 * w31 + -C.e_zx6 * w4 * w2);  // u
     bar[6] += l1 * (-C.xm_xz * w4 + -C.xm_zx * w33) + l4 * (-C.e_zx6 * w33 * w29 + -C.e_zx4 * w4 * w0);  // w
   }
   asm volatile("" ::: "memory");
   if (inner(1, 0, 1)) {
-    const Idx b = X - (1 * sI + 0 * sJ + 1);
-    const double l1 = lam(1, b);
-    const double l3 = lam(3, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w2 = val(6, X + (-1 * sI + 0 * sJ + 0));  // w (-1, 0, 0)
-    const double w4 = val(9, X + (-1 * sI + 0 * sJ + 0));  // mu (-1, 0, 0)
-    const double w12 = val(4, X + (0 * sI + 0 * sJ + -1));  // u (0, 0, -1)
-    const double w14 = val(6, X + (0 * sI + 0 * sJ + -1));  // w (0, 0, -1)
-    const double w16 = val(9, X + (0 * sI + 0 * sJ + -1));  // mu (0, 0, -1)
+    const double l1 = lam(1, -1, 0, -1);
+    const double l3 = lam(3, -1, 0, -1);
+    const double l4 = lam(4, -1, 0, -1);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w2 = val(6, -1, 0, 0);  // w (-1, 0, 0)
+    const double w4 = val(9, -1, 0, 0);  // mu (-1, 0, 0)
+    const double w12 = val(4, 0, 0, -1);  // u (0, 0, -1)
+    const double w14 = val(6, 0, 0, -1);  // w (0, 0, -1)
+    const double w16 = val(9, 0, 0, -1);  // mu (0, 0, -1)
     bar[4] += l3 * (C.zm_zx * w16 + C.zm_xz * w4) + l4 * (C.e_zx4 * w16 * w14 + C.e_zx6 * w4 * w2);  // u
     bar[6] += l1 * (C.xm_xz * w4 + C.xm_zx * w16) + l4 * (C.e_zx6 * w16 * w12 + C.e_zx4 * w4 * w0);  // w
   }
   asm volatile("" ::: "memory");
   if (inner(1, 1, 0)) {
-    const Idx b = X - (1 * sI + 1 * sJ + 0);
-    const double l1 = lam(1, b);
-    const double l2 = lam(2, b);
-    const double l4 = lam(4, b);
-    const double w0 = val(4, X + (-1 * sI + 0 * sJ + 0));  // u (-1, 0, 0)
-    const double w1 = val(5, X + (-1 * sI + 0 * sJ + 0));  // v (-1, 0, 0)
-    const double w4 = val(9, X + (-1 * sI + 0 * sJ + 0));  // mu (-1, 0, 0)
-    const double w6 = val(4, X + (0 * sI + -1 * sJ + 0));  // u (0, -1, 0)
-    const double w7 = val(5, X + (0 * sI + -1 * sJ + 0));  // v (0, -1, 0)
-    const double w10 = val(9, X + (0 * sI + -1 * sJ + 0));  // mu (0, -1, 0)
+    const double l1 = lam(1, -1, -1, 0);
+    const double l2 = lam(2, -1, -1, 0);
+    const double l4 = lam(4, -1, -1, 0);
+    const double w0 = val(4, -1, 0, 0);  // u (-1, 0, 0)
+    const double w1 = val(5, -1, 0, 0);  // v (-1, 0, 0)
+    const double w4 = val(9, -1, 0, 0);  // mu (-1, 0, 0)
+    const double w6 = val(4, 0, -1, 0);  // u (0, -1, 0)
+    const double w7 = val(5, 0, -1, 0);  // v (0, -1, 0)
+    const double w10 = val(9, 0, -1, 0);  // mu (0, -1, 0)
     bar[4] += l2 * (C.ym_yx * w10 + C.ym_xy * w4) + l4 * (C.e_yx4 * w10 * w7 + C.e_yx6 * w4 * w1);  // u
     bar[5] += l1 * (C.xm_xy * w4 + C.xm_yx * w10) + l4 * (C.e_yx6 * w10 * w6 + C.e_yx4 * w4 * w0);  // v
   }

@@ -156,12 +156,6 @@ __global__ void k_adj_filter(const Grid* __restrict__ gp, AdjPtrs A, const long 
   }
 }
 
-__global__ void k_adj_filter_clear(AdjPtrs A, int nFilter) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * nFilter; q += gridDim.x * blockDim.x) {
-    A.lamFnew[q] = 0.0;
-    A.lamFpre[q] = 0.0;
-  }
-}
 
 // -------------------------------------------------------------------------------- edge boundaries
 // One axis, both faces, same launch geometry as k_edge_bc. Phase 1 (periodic, outlet, inlet part 1):
@@ -322,6 +316,12 @@ __global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, con
       const int f = G.fidx[n];
       rho = A.valFpre[2 * f];
       rE = A.valFpre[2 * f + 1];
+      // the near-body filter's adjoints were consumed by k_adj_filter: clear them for the transposed RHS
+      // (fpre) and the previous stage's ghosts (fnew)
+      A.lamFpre[2 * f] = 0.0;
+      A.lamFpre[2 * f + 1] = 0.0;
+      A.lamFnew[2 * f] = 0.0;
+      A.lamFnew[2 * f + 1] = 0.0;
     }
     const Prim pr = prims_of(G.C, rho, m1, m2, m3, rE);
     const double q[11] = {m1, m2, m3, e4, pr.u, pr.v, pr.w, pr.p, pr.T, pr.mu, pr.ka};
@@ -568,8 +568,8 @@ void launch_adj_ghost(const Grid* dg, const AdjPtrs& A, int nGhost, int nFilter,
 void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes, int count, int nFilter, int nSM,
                        void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  (void)nFilter;  // the filter adjoints are cleared by the combine kernel of the same stage
   if (count > 0) k_adj_filter<<<blocks_for(count, nSM), 256, 0, st>>>(dg, A, nodes, count);
-  if (nFilter > 0) k_adj_filter_clear<<<blocks_for(2 * nFilter, nSM), 256, 0, st>>>(A, nFilter);
 }
 
 void launch_adj_edge(const Grid& hg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,

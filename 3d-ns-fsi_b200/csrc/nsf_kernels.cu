@@ -152,8 +152,8 @@ __global__ void k_solid_copy(const Grid* __restrict__ grids, int s) {
 // ----------------------------------------------------------------------------------------------
 // Mesh-edge boundary conditions of one axis (both faces; the faces of one axis never read each other's
 // nodes). Launched for x, then y, then z: the reference's application order outlet/inlet (x), y-max,
-// y-min, z-max, z-min (Mesh.cpp:155-167 after the reversal at Mesh.cpp:70). Threads cover the owned box.
-// blockIdx.z = 2 * member + (which of the axis's edges).
+// y-min, z-max, z-min (Mesh.cpp:155-167 after the reversal at Mesh.cpp:70). Each block comes from the
+// launch plan's list (member, face, first in-plane coordinates, mask of the nodes it works on).
 __global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __restrict__ blocks, int s, int axis) {
   __shared__ double red[4 * 32];
   const EdgeBlock eb = blocks[blockIdx.x];  // every listed block holds nodes of its face

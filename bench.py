@@ -163,14 +163,17 @@ def ensemble_leg(steps, device, nsfsi, sequential=True):
             "stage_work_items": items, "nonfinite_members": nonfinite}
 
 
-def adjoint_leg(device, nsfsi, reps=3):
+def adjoint_leg(device, nsfsi, reps=3, steps=200):
     """Discrete adjoint on a 64^3 channel with a sphere (200 RK4 steps, J = the sphere's x-force averaged
     over the last 50 steps, 20 checkpoint slots): wall time of the synchronous forward and backward calls
     (host overhead included), their ratio, the finite-difference agreement along two seeded directions
     (h = 1e-6) and the device time of one adjoint step by phase."""
-    with nsfsi.Solver(nsfsi.config_load(nsfsi.case_path("adj64")), device=device) as s:
+    cfg = nsfsi.config_load(nsfsi.case_path("adj64"))
+    cfg.stop_time_level = steps
+    navg = max(1, min(50, steps // 4))
+    with nsfsi.Solver(cfg, device=device) as s:
         u0 = s.download(range(5))
-        s.adj_configure(50, 20)
+        s.adj_configure(navg, 20)
         s.adj_forward()
         s.adj_backward()  # captures the adjoint step graphs
         fwd, bwd = [], []
@@ -182,7 +185,7 @@ def adjoint_leg(device, nsfsi, reps=3):
             t2 = time.perf_counter()
             fwd.append(t1 - t0)
             bwd.append(t2 - t1)
-        phases = s.adj_profile_step(100)
+        phases = s.adj_profile_step(steps // 2)
         rng = np.random.default_rng(2024)
         scale = np.maximum(np.abs(u0).max(axis=1), 1e-3)[:, None]
         errs = []
@@ -195,7 +198,7 @@ def adjoint_leg(device, nsfsi, reps=3):
             errs.append(abs(fd - ad) / abs(ad))
     f, b = float(np.median(fwd)), float(np.median(bwd))
     return {"workload": "adj64: 64^3 channel, sphere D=0.2 at (0.4,0.5,0.5), M 0.3, Re_D 100 (Re 1666.7 per unit "
-                        "length on the speed of sound), 200 RK4 steps, J over the last 50",
+                        "length on the speed of sound), %d RK4 steps, J over the last %d" % (steps, navg),
             "snapshots": 20, "J": J, "forward_ms": f * 1e3, "backward_ms": b * 1e3, "backward_over_forward": b / f,
             "fd_step": 1e-6, "fd_rel_err_max": max(errs), "fd_directions": len(errs),
             "adjoint_step_phase_ms": {k: round(v, 4) for k, v in phases.items()}}
@@ -243,6 +246,7 @@ def main():
     ap.add_argument("--no-seq", action="store_true", help="ensemble leg without the sequential comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint leg")
     ap.add_argument("--adjoint-only", action="store_true", help="run only the discrete-adjoint leg (profiling)")
+    ap.add_argument("--adjoint-steps", type=int, default=200, help="RK4 steps of the adjoint leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -270,7 +274,7 @@ def main():
         print(json.dumps(ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq)), flush=True)
         return
     if args.adjoint_only:
-        print(json.dumps(adjoint_leg(local, nsfsi)), flush=True)
+        print(json.dumps(adjoint_leg(local, nsfsi, steps=args.adjoint_steps)), flush=True)
         return
     wl = WORKLOADS[args.workload]
     case = nsfsi.case_path(wl["case"])
@@ -352,7 +356,7 @@ def main():
         if args.ensemble_steps > 0 and args.workload == "tgv256":
             line["ensemble"] = ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq)
         if not args.no_adjoint and args.workload == "tgv256":
-            line["adjoint"] = adjoint_leg(local, nsfsi)
+            line["adjoint"] = adjoint_leg(local, nsfsi, steps=args.adjoint_steps)
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(case, nodes)

@@ -47,6 +47,10 @@ struct AdjCtx {
   int nfs = 0;
   bool inletX = false;
   bool xInOut = false;  // an x face is an inlet or an outlet (its adjoint reads the planes next to it)
+  // The x-planes the inlet / outlet adjoint reads (i = 1, 2, NI-3, NI-2, inside the faces' j, k range)
+  // hold only unfiltered interior fluid nodes: no kernel after the stage kernel writes them, so the next
+  // stage's input (or the step's result) has the values the edge conditions read, and no copy is taken.
+  bool edgePlanesClean = false;
   double* lam = nullptr;  // 20 x Nd: adjoint of bufs[b][f] at (5 b + f) Nd, accumulator at (15 + f) Nd
   double* lamFpre = nullptr;
   double* lamFnew = nullptr;
@@ -129,6 +133,13 @@ nsf_status setup(nsf_solver* s) {
     a->inletX |= e.axis == 0 && e.bc == NSF_BC_INLET;
     a->xInOut |= e.axis == 0 && (e.bc == NSF_BC_INLET || e.bc == NSF_BC_OUTLET);
   }
+  a->edgePlanesClean = true;
+  for (size_t i : {size_t(1), size_t(2), S.NI - 3, S.NI - 2})
+    for (size_t j = 1; j + 1 < S.NJ; ++j)
+      for (size_t k = 1; k + 1 < S.NK; ++k) {
+        const uint8_t t = s->typeFlags[(i * S.NJ + j) * S.NK + k];
+        if ((t & TYPE_MASK) != FLUID_INTERIOR || (t & FILTER_BIT)) a->edgePlanesClean = false;
+      }
   if ((st = aalloc(s, a, &a->dDt, size_t(a->nsteps) + 1)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->dInflow, plane)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->dU0, 5 * N)) != NSF_OK) return st;
@@ -278,8 +289,8 @@ SnapPlan snap_plan(const StepCtl& R, int q) {
 
 // Keeps the step's control block and, per stage, the values the nonlinear adjoints need that the step
 // overwrites: the stage inputs (snap_plan), the near-body filter's pre-values and, for x inlet / outlet
-// faces, the four x-planes next to them (i = 1, 2, NI-3, NI-2) of the stage output before the edge
-// conditions. The step's roles (which physical buffer plays which part) are known on the host from the
+// faces whose neighbouring planes are not clean (AdjCtx::edgePlanesClean), the four x-planes next to them
+// (i = 1, 2, NI-3, NI-2) of the stage output before the edge conditions. The step's roles (which physical buffer plays which part) are known on the host from the
 // forward run's record, so nothing waits here and the whole adjoint step can be captured as a graph.
 struct SnapHook : StepHook {
   nsf_solver* s;
@@ -315,7 +326,7 @@ struct SnapHook : StepHook {
     flush();
   }
   void before_edges(int q) override {
-    if (!a->xInOut) return;
+    if (!a->xInOut || a->edgePlanesClean) return;
     const size_t N = nd(s), plane = size_t(s->hGrid.sI), NI = size_t(s->hGrid.NI);
     double* base = a->stageSnap + q * per_stage(s);
     for (size_t i : {size_t(1), size_t(2), NI - 3, NI - 2})
@@ -393,8 +404,18 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     mark(PH_GHOST);
     launch_adj_filter(s->dGrid, A, a->fsNodes, a->nfs, G.nFilter, nSM, st);
     mark(PH_FILTER);
-    // edge conditions: z, y, then x (reads the stage output before the edge conditions)
-    for (int f = 0; f < 5; ++f) A.val[f] = snap + (6 + f) * N;
+    // edge conditions: z, y, then x (reads the stage output before the edge conditions: its copy, or,
+    // where the planes it reads are clean, the next stage's input / the step's result)
+    for (int f = 0; f < 5; ++f) {
+      if (!a->edgePlanesClean) {
+        A.val[f] = snap + (6 + f) * N;
+      } else if (q == 3) {
+        A.val[f] = R.O[3][f];
+      } else {
+        const SnapPlan Pn = snap_plan(R, q + 1);
+        A.val[f] = Pn.inputLive ? R.I[q + 1][f] : a->stageSnap + (q + 1) * per_stage(s) + f * N;
+      }
+    }
     for (int axis = 2; axis >= 0; --axis)
       launch_adj_edge(s->hGrid, A, s->plan, axis, dR, q, a->fbar, a->lamInflow, a->inletX, st);
     mark(PH_EDGE);

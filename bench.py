@@ -3,7 +3,9 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload tgv256|sphere48]
 
 A step is one RK4 step (Solver::marchTimeStep) over the whole grid. Each rank runs an independent replica
-(the single-grid path does not shard), so value = ranks x nodes x K / max-over-ranks device time.
+(the single-grid path does not shard), so value = ranks x nodes x K / max-over-ranks device time. The
+ensemble leg shards its members over the ranks (longest first, by node count) with no collective on the
+data path; its time is the slowest rank's.
 Timing: CUDA events on the solver's own stream around K graph-launched steps after W warm-up steps; the
 resident fields (2.7 GB) are far larger than L2, so no flush is needed between steps.
 """
@@ -121,11 +123,42 @@ def cpu_baseline(case_path, nodes):
 TUNE_CACHE = os.path.join(ROOT, "3d-ns-fsi_b200", "tuning", "stage_tiles.jsonl")
 
 
-def ensemble_leg(steps, device, nsfsi, sequential=True):
+def reduce_over_ranks(x, dist, op="max"):
+    """x reduced (max or sum) over all ranks of the process group (x itself without one)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def max_over_ranks(x, dist):
+    return reduce_over_ranks(x, dist, "max")
+
+
+def shard_members(nodes, world):
+    """The members each of `world` ranks advances: longest-processing-time-first over the members' node
+    counts (ties by index), each rank's list in member order."""
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for m in sorted(range(len(nodes)), key=lambda m: (-nodes[m], m)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        parts[r].append(m)
+        load[r] += nodes[m]
+    return [sorted(p) for p in parts]
+
+
+def ensemble_leg(steps, device, nsfsi, sequential=True, rank=0, world=1, dist=None):
     """Batched ensemble (64 seeded single-sphere flows on 5 grid shapes) against the same 64 runs made one
-    after another on the plain path. Both timed on the device (CUDA events), setup excluded."""
-    cfgs = nsfsi.ensemble_configs(n=64, steps=steps)
-    nodes = [int(c.NI * c.NJ * c.NK) for c in cfgs]
+    after another on the plain path. Both timed on the device (CUDA events), setup excluded. With several
+    ranks every rank advances its shard of the members (one graph per step for its shard) and the slowest
+    rank's time counts; every rank must call this (it holds collectives)."""
+    allCfgs = nsfsi.ensemble_configs(n=64, steps=steps)
+    allNodes = [int(c.NI * c.NJ * c.NK) for c in allCfgs]
+    mine = shard_members(allNodes, world)[rank]
+    cfgs = [allCfgs[m] for m in mine]
+    nodes = [allNodes[m] for m in mine]
     os.makedirs(os.path.dirname(TUNE_CACHE), exist_ok=True)
 
     def sync(x):
@@ -153,9 +186,14 @@ def ensemble_leg(steps, device, nsfsi, sequential=True):
             sync(s)
             seq_ms += s.march_timed(steps)
             nonfinite += sync(s)
-    work = sum(nodes) * steps
+    # the slowest rank's times; non-finite members summed over the ranks
+    ens_ms = max_over_ranks(ens_ms, dist)
+    seq_ms = max_over_ranks(seq_ms, dist)
+    nonfinite = int(reduce_over_ranks(nonfinite, dist, "sum"))
+    work = sum(allNodes) * steps
     return {"workload": "64 single-sphere flows, shapes 32^3/48^3/64^3/96x64x64/128x64x64, M U[0.2,0.4], "
-                        "Re_D U[50,300], D U[0.15,0.25]", "members": len(cfgs), "nodes": sum(nodes),
+                        "Re_D U[50,300], D U[0.15,0.25]", "members": len(allCfgs), "nodes": sum(allNodes),
+            "ranks": world, "members_per_rank": len(cfgs),
             "steps": steps, "value": work / (ens_ms / 1e3), "unit": "node-RK4-steps/s",
             "sequential_value": work / (seq_ms / 1e3) if sequential else None,
             "speedup_vs_sequential": seq_ms / ens_ms if sequential else None,
@@ -271,7 +309,13 @@ def main():
 
     import nsfsi
     if args.ensemble_only:
-        print(json.dumps(ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq)), flush=True)
+        leg = ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq, rank=rank, world=world,
+                           dist=dist)
+        if rank == 0:
+            print(json.dumps(leg), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
         return
     if args.adjoint_only:
         print(json.dumps(adjoint_leg(local, nsfsi, steps=args.adjoint_steps)), flush=True)
@@ -336,6 +380,10 @@ def main():
                "d2h_bytes_per_step": (5 * 8 * nodes + 24 * args.steps) / args.steps,
                "timing": "host wall clock around upload + K x (march 1, read t/dt/timeLevel) + download"}
 
+    ens = None
+    if args.ensemble_steps > 0 and args.workload == "tgv256":  # every rank takes its shard
+        ens = ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq, rank=rank, world=world,
+                           dist=dist)
     if rank == 0:
         line = {
             "metric": "node-RK4-steps/s (FP64)", "value": value, "unit": "node-RK4-steps/s", "n_gpus": world,
@@ -353,8 +401,8 @@ def main():
                          "algorithmic_bytes_per_node_step": BYTES_PER_NODE_STEP, "peak_kind": peak_kind,
                          "frac_of_8000": achieved / 8000.0},
         }
-        if args.ensemble_steps > 0 and args.workload == "tgv256":
-            line["ensemble"] = ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq)
+        if ens is not None:
+            line["ensemble"] = ens
         if not args.no_adjoint and args.workload == "tgv256":
             line["adjoint"] = adjoint_leg(local, nsfsi, steps=args.adjoint_steps)
         if world == 1 and not args.no_cpu_baseline:

@@ -1,5 +1,5 @@
 """GPU parity: the sm_100a path (through the C ABI) against the reference's own fields (golden fixtures)
-and against the CPU oracle run in-process. Tolerance (north star): every field within 1e-10 of the
+and against the CPU oracle run in-process. Tolerance: every field within 1e-10 of the
 reference, measured as max|gpu - ref| / max|ref| per field; dt and t within 1e-12 relative."""
 import os
 

@@ -323,7 +323,7 @@ __global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, con
       A.lamFnew[2 * f] = 0.0;
       A.lamFnew[2 * f + 1] = 0.0;
     }
-    const Prim pr = prims_of(G.C, rho, m1, m2, m3, rE);
+    const Prim pr = prims_of_nr(G.C, rho, m1, m2, m3, rE);  // as the stage kernel's staging warps
     const double q[11] = {m1, m2, m3, e4, pr.u, pr.v, pr.w, pr.p, pr.T, pr.mu, pr.ka};
     for (int v = 0; v < 11; ++v) V[v * G.N + n] = q[v];
     if (!interior) {
@@ -446,15 +446,15 @@ __global__ void __launch_bounds__(32 * RT_J, kAdjRhsBlocks)
       const bool filt = (G.type[m] & FILTER_BIT) != 0;
       const int fi = filt ? G.fidx[m] : 0;
       const double rho = filt ? A.valFpre[2 * fi] : A.valR[m];
-      const double r1 = 1.0 / (rho + 1.0);
+      const double r1 = recip_nr(rho + 1.0);
       const int cc = sb[1] + c;  // this node in the staged plane
       const double u = sm[cc + 5 * RT_PLANE], v = sm[cc + 6 * RT_PLANE], w = sm[cc + 7 * RT_PLANE],
                    T = sm[cc + 8 * RT_PLANE];
       const double K = 0.5 * (u * u + v * v + w * w);
       double ub = bar[4], vb = bar[5], wb = bar[6], pb = bar[7], Tb = bar[8], mub = bar[9];
       mub += C.pf * bar[10];
-      const double x = 1.0 + T, sx = sqrt(x), den = T + C.sc1;
-      Tb += mub * C.sc1 / C.re * (1.5 * sx * den - x * sx) / (den * den);
+      const double x = 1.0 + T, sx = sqrt_nr(x), den = T + C.sc1;
+      Tb += mub * C.sc1 * (1.5 * sx * den - x * sx) * recip_nr(C.re * den * den);
       pb += C.gamma * r1 * Tb;
       double rhob = -r1 * Tb - T * r1 * Tb;
       double rEb = C.gm1 * pb;

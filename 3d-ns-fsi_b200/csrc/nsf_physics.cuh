@@ -36,6 +36,46 @@ __device__ __forceinline__ Prim prims_of(const CT& C, double rho, double ru, dou
   return q;
 }
 
+// Reciprocal and square root by Newton-Raphson refinement of the hardware approximations
+// (rcp.approx.ftz.f64, rsqrt.approx.ftz.f64): y <- y (2 - a y) and r <- r (3 - a r^2) / 2, each iteration
+// doubling the correct bits, two of them from the approximation's ~20 bits, then one Heron correction of
+// s = a r for the square root. Arguments are positive normal numbers here (1 + rho, 1 + T, and the
+// viscosity denominator); results are within a couple of ulps of the correctly rounded ones.
+__device__ __forceinline__ double recip_nr(double a) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  double e = fma(-a, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-a, y, 1.0);
+  return fma(y, e, y);
+}
+__device__ __forceinline__ double sqrt_nr(double a) {
+  double r;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(a));
+  const double h = 0.5 * a;
+  r = r * fma(-h * r, r, 1.5);
+  r = r * fma(-h * r, r, 1.5);
+  const double s = a * r;
+  return fma(fma(-s, s, a), 0.5 * r, s);
+}
+
+// prims_of with the Newton-Raphson reciprocal and square root (the stage kernel's staging warps, where
+// the IEEE division and square root sequences are the longest dependency chains of a plane).
+template <class CT>
+__device__ __forceinline__ Prim prims_of_nr(const CT& C, double rho, double ru, double rv, double rw, double rE) {
+  Prim q;
+  const double r1 = recip_nr(rho + 1.0);
+  q.u = ru * r1;
+  q.v = rv * r1;
+  q.w = rw * r1;
+  q.p = C.gm1 * (rE - (rho + 1.0) * 0.5 * (q.u * q.u + q.v * q.v + q.w * q.w));
+  q.T = (C.gamma * q.p - rho) * r1;
+  const double x = 1.0 + q.T;
+  q.mu = x * sqrt_nr(x) * C.sc1 * recip_nr(C.re * (q.T + C.sc1));
+  q.ka = q.mu * C.pf;
+  return q;
+}
+
 __device__ __forceinline__ double mu_of_T(const Consts& C, double T) {
   const double x = 1.0 + T;
   return x * sqrt(x) * C.sc1 / (C.re * (T + C.sc1));

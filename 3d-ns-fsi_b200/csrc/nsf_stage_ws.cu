@@ -133,19 +133,20 @@ __device__ __forceinline__ void reg_alloc() {
 }
 
 // dt-limit terms of a node of the new state (getInviscidTimeStepLimit / getViscousTimeStepLimit,
-// Solver.cpp:91-126) with one reciprocal of 1 + rho for all the divisions by it. The terms only enter
-// maxima, so their last-bit rounding moves dt by at most an ulp or two.
+// Solver.cpp:91-126) with one reciprocal of 1 + rho for all the divisions by it, reciprocals and square
+// roots by Newton-Raphson (recip_nr, sqrt_nr). The terms only enter maxima, so their last-bit rounding
+// moves dt by at most an ulp or two.
 __device__ __forceinline__ void dt_terms(const Consts& C, const double (&u)[5], DtAcc& a) {
-  const double r1 = 1.0 / (u[0] + 1.0);
+  const double r1 = recip_nr(u[0] + 1.0);
   const double vx = u[1] * r1, vy = u[2] * r1, vz = u[3] * r1;
   const double p = C.gm1 * (u[4] - (u[0] + 1.0) * 0.5 * (vx * vx + vy * vy + vz * vz));
   const double T = (C.gamma * p - u[0]) * r1;
   const double x = 1.0 + T;
-  const double c = sqrt((1.0 + C.gamma * p) * r1);
+  const double c = sqrt_nr((1.0 + C.gamma * p) * r1);
   a.sx = fmax(a.sx, c + fabs(vx));
   a.sy = fmax(a.sy, c + fabs(vy));
   a.sz = fmax(a.sz, c + fabs(vz));
-  a.nu = fmax(a.nu, x * sqrt(x) * C.sc1 * r1 / (C.re * (T + C.sc1)) * C.vmod);
+  a.nu = fmax(a.nu, x * sqrt_nr(x) * C.sc1 * r1 * recip_nr(C.re * (T + C.sc1)) * C.vmod);
 }
 
 }  // namespace
@@ -353,8 +354,8 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
                 rE[h] = fpre[2 * f + 1];
               }
             }
-            const Prim a0 = prims_of(C, rho[0], cs[1 * FS + idx], cs[2 * FS + idx], cs[3 * FS + idx], rE[0]);
-            const Prim a1 = prims_of(C, rho[1], cs[1 * FS + idyc], cs[2 * FS + idyc], cs[3 * FS + idyc], rE[1]);
+            const Prim a0 = prims_of_nr(C, rho[0], cs[1 * FS + idx], cs[2 * FS + idx], cs[3 * FS + idx], rE[0]);
+            const Prim a1 = prims_of_nr(C, rho[1], cs[1 * FS + idyc], cs[2 * FS + idyc], cs[3 * FS + idyc], rE[1]);
             pv[0 * FS + idx] = a0.u;
             pv[1 * FS + idx] = a0.v;
             pv[2 * FS + idx] = a0.w;

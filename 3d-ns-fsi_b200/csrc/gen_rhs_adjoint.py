@@ -235,7 +235,7 @@ def emit_cuda(terms):
     w("// within one node of X: the 7-point stencil for u, v, w, T, mu, ka, X itself for the others);")
     w("// inner(di, dj, dk): the node (i-di, j-dj, k-dk) is one whose RHS was taken (its whole stencil then")
     w("// lies inside the grid). All offsets are literals, so a caller's index arithmetic folds. The terms of")
-    w("// one RHS node are grouped by equation.")
+    w("// one RHS node are grouped by equation and, within an equation, by coefficient.")
     w("#ifndef NSF_RHS_ADJOINT_CUH")
     w("#define NSF_RHS_ADJOINT_CUH")
     w("")
@@ -282,14 +282,36 @@ def emit_cuda(terms):
             for q in VARS:
                 if q not in outs:
                     continue
-                parts_by_e = {}
+                # per equation, the terms grouped by coefficient (one multiplication by it per group), and
+                # within a group a value shared by every product factored out
+                by_e = {}
                 for e, _, qq, coef, others in by_o[o]:
                     if qq != q:
                         continue
-                    prod = " * ".join(names[(q2, tuple(o2[a] - o[a] for a in range(3)))] for q2, o2 in others)
-                    parts_by_e.setdefault(e, []).append(_coef_expr(coef) + ((" * " + prod) if prod else ""))
-                parts = ["l%d * (%s)" % (e, " + ".join(g)) if len(g) > 1 else "l%d * %s" % (e, g[0])
-                         for e, g in sorted(parts_by_e.items())]
+                    factors = [names[(q2, tuple(o2[a] - o[a] for a in range(3)))] for q2, o2 in others]
+                    by_e.setdefault(e, {}).setdefault(tuple(sorted(coef.items())), []).append(factors)
+                parts = []
+                for e, by_c in sorted(by_e.items()):
+                    sums = []
+                    for ckey, prods in sorted(by_c.items()):
+                        cexpr = _coef_expr(dict(ckey))
+                        common = set(prods[0])
+                        for f in prods[1:]:
+                            common &= set(f)
+                        shared = sorted(common)[0] if common and len(prods) > 1 else None
+                        if shared:
+                            rest = []
+                            for f in prods:
+                                g = list(f)
+                                g.remove(shared)
+                                rest.append(" * ".join(g) if g else "1.0")
+                            inner = " + ".join(rest)
+                            sums.append("%s * %s * (%s)" % (cexpr, shared, inner))
+                        else:
+                            inner = " + ".join(" * ".join(f) if f else "1.0" for f in prods)
+                            sums.append("%s * (%s)" % (cexpr, inner) if len(prods) > 1 or prods[0] else cexpr)
+                    sums = [s.replace(" * (1.0)", "") for s in sums]
+                    parts.append("l%d * (%s)" % (e, " + ".join(sums)) if len(sums) > 1 else "l%d * %s" % (e, sums[0]))
                 w("    bar[%d] += %s;  // %s" % (VIDX[q], " + ".join(parts), q))
             w("  }")
     w("}")

@@ -419,14 +419,12 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     for (int axis = 2; axis >= 0; --axis)
       launch_adj_edge(s->hGrid, A, s->plan, axis, dR, q, a->fbar, a->lamInflow, a->inletX, st);
     mark(PH_EDGE);
-    launch_adj_solid(s->dGrid, A, G.nSolid, R.copyMask[q], nSM, st);
-    mark(PH_SOLID);
     // stage kernel: RK4 combine, transposed RHS, primitives of the stage input
     const SnapPlan P = snap_plan(R, q);
     for (int f = 0; f < 5; ++f) A.val[f] = P.inputLive ? R.I[q][f] : snap + f * N;
     A.valR = P.inputLive ? R.R[q] : P.rSeparate ? snap + 5 * N : snap;
     A.valFpre = snap + 11 * N;
-    launch_adj_prepare(s->dGrid, G, A, q, dR, a->tmpLam, a->tmpV, nSM, st);
+    launch_adj_prepare(s->dGrid, G, A, q, dR, R.copyMask[q], a->tmpLam, a->tmpV, nSM, st);
     mark(PH_PREPARE);
     launch_adj_rhs(s->dGrid, G, A, a->tmpLam, a->tmpV, nSM, st);
     mark(PH_RHS);

@@ -262,23 +262,6 @@ __global__ void k_adj_inlet_gather(const __grid_constant__ Grid G, const EdgeBlo
   A.lamO[0][side == 0 ? n + 2 * st : n - 2 * st] -= g;
 }
 
-// ------------------------------------------------------------------------------------ solid copy
-__global__ void k_adj_solid(const Grid* __restrict__ gp, AdjPtrs A, int mask) {
-  const Grid& G = *gp;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < G.nSolid; q += gridDim.x * blockDim.x) {
-    const long long n = G.snode[q];
-    if (mask & 1) {
-      A.lamR[n] += A.lamO[0][n];
-      A.lamO[0][n] = 0.0;
-    }
-    for (int f = 1; f < 5; ++f)
-      if (mask & (1 << f)) {
-        A.lamI[f][n] += A.lamO[f][n];
-        A.lamO[f][n] = 0.0;
-      }
-  }
-}
-
 // ------------------------------------------------------------------------------------------ stage
 // RK4 combine at the interior nodes: s = 0: O = U0 + inc k, acc = k; s = 1, 2: O = U0 + inc k,
 // acc += 2 k; s = 3: O = U0 + dt/6 (acc + k). Writes the RHS adjoint lam (zero elsewhere beforehand).
@@ -290,8 +273,10 @@ __global__ void k_adj_solid(const Grid* __restrict__ gp, AdjPtrs A, int mask) {
 // primitives), then the primitives and transport properties, as the stage kernel stages them.
 // With periodic z faces (Grid::zFused) the stage kernel also wrote the z copies of the nodes at k = 1 and
 // k = NK-2 it computed: their adjoints are gathered here, before the combine's.
+// Solid nodes (ghost and inactive): the adjoint of k_solid_copy, which copied the stage input into the
+// output of the fields in solidMask (bit 0: the density from R) before the edge conditions.
 __global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, const StepCtl* __restrict__ roles,
-                              double* __restrict__ lam, double* __restrict__ V) {
+                              int solidMask, double* __restrict__ lam, double* __restrict__ V) {
   const Grid& G = *gp;
   const double dtUsed = roles->dtUsed;
   const double inc = s == 2 ? dtUsed : dtUsed / 2, dtF = dtUsed / 6;
@@ -328,6 +313,18 @@ __global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, con
     for (int v = 0; v < 11; ++v) V[v * G.N + n] = q[v];
     if (!interior) {
       for (int f = 0; f < 5; ++f) lam[f * G.N + n] = 0.0;
+      const uint8_t t = ty & TYPE_MASK;
+      if (solidMask && (t == SOLID_GHOST || t == SOLID_INACTIVE)) {
+        if (solidMask & 1) {
+          A.lamR[n] += A.lamO[0][n];
+          A.lamO[0][n] = 0.0;
+        }
+        for (int f = 1; f < 5; ++f)
+          if (solidMask & (1 << f)) {
+            A.lamI[f][n] += A.lamO[f][n];
+            A.lamO[f][n] = 0.0;
+          }
+      }
       continue;
     }
     if (zCopy)
@@ -582,14 +579,11 @@ void launch_adj_edge(const Grid& hg, const AdjPtrs& A, const LaunchPlan& L, int 
     k_adj_inlet_gather<<<L.nEdgeBlocks[0], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocks[0], A, fbar);
 }
 
-void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, int nSM, void* stream) {
-  if (nSolid > 0 && mask)
-    k_adj_solid<<<blocks_for(nSolid, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, mask);
-}
 
-void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, double* lam,
-                        double* V, int nSM, void* stream) {
-  k_adj_prepare<<<blocks_for(hg.N, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, s, roles, lam, V);
+void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, int solidMask,
+                        double* lam, double* V, int nSM, void* stream) {
+  k_adj_prepare<<<blocks_for(hg.N, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, s, roles,
+                                                                                      hg.nSolid ? solidMask : 0, lam, V);
 }
 
 int adj_kernels_init() {

@@ -33,11 +33,11 @@ void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes,
 // roles: device copy of the step's control block (stage times, dt).
 void launch_adj_edge(const Grid& hg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
                      double* fbar, double* lamInflow, bool inletGather, void* stream);
-void launch_adj_solid(const Grid* dg, const AdjPtrs& A, int nSolid, int mask, int nSM, void* stream);
-// The stage kernel's adjoint: prepare = RK4 combine adjoint into lam and the RHS input quantities into V
-// (11 x N); rhs = transposed RHS gather and the chain rule into the stage input's adjoints.
-void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, double* lam,
-                        double* V, int nSM, void* stream);
+// The stage kernel's adjoint: prepare = RK4 combine adjoint into lam, the RHS input quantities into V
+// (11 x N) and, at solid nodes, the adjoint of the solid-node copy (solidMask: the stage's copy mask);
+// rhs = transposed RHS gather and the chain rule into the stage input's adjoints.
+void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, int solidMask,
+                        double* lam, double* V, int nSM, void* stream);
 void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V, int nSM,
                     void* stream);
 // Kernel attributes (shared-memory size of the transposed RHS); call once before the first launch.

@@ -227,7 +227,8 @@ nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* 
 nsf_status nsf_adj_get_dt(nsf_solver* s, double* dts, uint64_t* count);
 /* Device time (ms, CUDA events) of the phases of one adjoint step, launched eagerly after a forward run:
  * ms[0] recomputation of the step with its stage snapshots, [1] objective, [2] ghost nodes, [3] near-body
- * filter, [4] edge conditions, [5] solid-node copies, [6] RK4 combine and RHS input quantities,
+ * filter, [4] edge conditions, [5] unused (the solid-node copies' adjoint runs within [6]), [6] RK4
+ * combine, RHS input quantities and solid-node copies,
  * [7] transposed RHS, [8] density filter (summed over the four stages). Gradients are unaffected. */
 nsf_status nsf_adj_profile_step(nsf_solver* s, uint64_t step, double* ms);
 

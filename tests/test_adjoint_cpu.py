@@ -104,3 +104,57 @@ def test_dual_number_oracle_matches_its_finite_differences():
     Jp = po.dual_objective(cfg, dts, 4, u0=u0 + h * du, inflow=1 + h * di)[0]
     Jm = po.dual_objective(cfg, dts, 4, u0=u0 - h * du, inflow=1 - h * di)[0]
     assert abs((Jp - Jm) / (2 * h) - dJ) <= 1e-7 * abs(dJ), (dJ, (Jp - Jm) / (2 * h))
+
+
+def _gather_in_python(text):
+    """The generated CUDA gather as a Python function gather(C, lam, val, inner) -> bar[11] (a line-by-line
+    translation of its few statement forms)."""
+    import re
+    body = ["def gather(C, lam, val, inner):", "    bar = [0.0] * 11"]
+    indent = 1
+    for raw in text.split("\n"):
+        line = raw.split("//")[0].strip()
+        if not line or line.startswith(("#", "namespace", "template", "__device__", "const Lam", "const Inner",
+                                        "}  //", "for (int q")) or "asm volatile" in line:
+            continue
+        if line.startswith("if (inner("):
+            body.append("    " * indent + "if " + line[4:-3] + ":")
+            indent += 1
+            body.append("    " * indent + "pass")
+        elif line == "}":
+            indent = max(1, indent - 1)
+        elif line.startswith("const double"):
+            body.append("    " * indent + line[len("const double "):].rstrip(";"))
+        elif line.startswith("bar["):
+            body.append("    " * indent + line.rstrip(";"))
+    body.append("    return bar")
+    src = "\n".join(body)
+    src = re.sub(r"C\.(\w+)", r"C['\1']", src)
+    ns = {}
+    exec(src, ns)
+    return ns["gather"]
+
+
+def test_generated_gather_matches_the_numpy_adjoint():
+    """The emitted CUDA expressions (grouped and factored) give the numpy transposed stencil's values at an
+    inner node and at nodes next to the faces."""
+    rng = np.random.default_rng(11)
+    shape = (7, 7, 7)
+    fields = {q: rng.uniform(0.5, 1.5, shape) for q in gen.VARS}
+    C = consts(0.11, 0.13, 0.17, 1.4)
+    inner = np.zeros(shape, bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    lam = [rng.standard_normal(shape) * inner for _ in range(5)]
+    ref = gen.adjoint(gen.adjoint_terms(gen.rhs_polys()), fields, lam, C)
+    with open(os.path.join(ROOT, "3d-ns-fsi_b200", "csrc", "nsf_rhs_adjoint.cuh")) as f:
+        gather = _gather_in_python(f.read())
+    for X in [(3, 3, 3), (1, 3, 2), (0, 0, 0), (6, 5, 1), (2, 6, 6)]:
+        def ok(di, dj, dk):
+            return all(0 <= X[a] + d < shape[a] for a, d in enumerate((di, dj, dk)))
+        lamf = lambda e, di, dj, dk: lam[e][X[0] + di, X[1] + dj, X[2] + dk] if ok(di, dj, dk) else 0.0  # noqa: E731
+        valf = lambda q, di, dj, dk: fields[gen.VARS[q]][X[0] + di, X[1] + dj, X[2] + dk] if ok(di, dj, dk) else 0.0  # noqa: E731
+        innerf = lambda di, dj, dk: bool(ok(-di, -dj, -dk) and inner[X[0] - di, X[1] - dj, X[2] - dk])  # noqa: E731
+        bar = gather(C, lamf, valf, innerf)
+        for q, name in enumerate(gen.VARS):
+            r = ref[name][X]
+            assert abs(bar[q] - r) <= 1e-12 * max(1.0, abs(r)), (X, name, bar[q], r)

@@ -69,6 +69,9 @@ struct AdjCtx {
   StepCtl* dCur = nullptr;                 // the control block of the step being reversed (after its prologue)
   // one CUDA graph per distinct pattern of buffer roles (the roles rotate with a short period)
   std::map<std::vector<uintptr_t>, cudaGraphExec_t> graphs;
+  // Stage 4 of a recomputed step whose result enters no objective term: only the x-planes the inlet /
+  // outlet adjoint reads (i = 1, 2, NI-3, NI-2) are computed, and nothing after that stage kernel runs.
+  LaunchPlan lastStagePlan{};
   std::vector<void*> allocs;
 };
 
@@ -155,6 +158,38 @@ nsf_status setup(nsf_solver* s) {
   if ((st = aalloc(s, a, &a->stageSnap, 4 * per_stage(s))) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->dHist, size_t(a->nsteps))) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->dCur, 1)) != NSF_OK) return st;
+  {  // the partial stage-4 plan: the main plan's tiles over planes [1, 2] and [NI-3, NI-2], round robin
+    LaunchPlan& P = a->lastStagePlan;
+    P = s->plan;
+    P.items = nullptr;
+    P.ctaStart = nullptr;
+    P.nItems = 0;
+    P.stageBlocks = 0;
+    std::vector<StageItem> items;
+    if (a->xInOut) {
+      const int TJ = stage_tile_j(s->plan.tile), TK = stage_tile_k(s->plan.tile);
+      const int nj = int((S.NJ - 2 + TJ - 1) / TJ), nk = int((S.NK - 2 + TK - 1) / TK);
+      std::vector<std::pair<int, int>> ranges = {{1, 2}, {int(S.NI) - 3, int(S.NI) - 2}};
+      if (ranges[1].first <= ranges[0].second + 1) ranges = {{1, int(S.NI) - 2}};
+      for (auto& r : ranges)
+        for (int tj = 0; tj < nj; ++tj)
+          for (int tk = 0; tk < nk; ++tk) items.push_back(StageItem{1 + tj * TJ, 1 + tk * TK, r.first, r.second, 0});
+    }
+    if (!items.empty()) {
+      P.nItems = int(items.size());
+      P.stageBlocks = std::min(P.nItems, s->nSM);
+      std::vector<StageItem> ordered;
+      std::vector<int> start(1, 0);
+      for (int b = 0; b < P.stageBlocks; ++b) {
+        for (int q = b; q < P.nItems; q += P.stageBlocks) ordered.push_back(items[q]);
+        start.push_back(int(ordered.size()));
+      }
+      if ((st = aalloc(s, a, &P.items, ordered.size())) != NSF_OK) return st;
+      if ((st = aalloc(s, a, &P.ctaStart, start.size())) != NSF_OK) return st;
+      CKA(cudaMemcpy(P.items, ordered.data(), ordered.size() * sizeof(StageItem), cudaMemcpyHostToDevice));
+      CKA(cudaMemcpy(P.ctaStart, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+  }
   s->hGrid.ctlHist = a->dHist;
   s->hGrid.nCtlHist = a->nsteps;
   // objective: body normals at the ghosts' body-intercept points (gnode order), area weight
@@ -370,7 +405,9 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
   const StepCtl* dR = a->dCur;
   SnapHook hook(s, a, R);
   mark(-1);
-  enqueue_step_hooked(s->dGrid, s->hGrid, s->plan, s->stream, &hook);
+  // the whole step when its result enters J (the objective's adjoint reads it at the ghost nodes), else
+  // stage 4 only where the inlet / outlet adjoint reads it
+  enqueue_step_hooked(s->dGrid, s->hGrid, s->plan, s->stream, &hook, objective ? nullptr : &a->lastStagePlan);
   mark(PH_RECOMPUTE);
   if (hook.err != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint recomputation: ") + cudaGetErrorString(hook.err));
   CKA(cudaGetLastError());

@@ -191,7 +191,10 @@ struct StepHook {
   virtual void before_stage(int) {}
   virtual void before_edges(int) {}
 };
-int enqueue_step_hooked(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, StepHook* hook);
+// lastStage: NULL for a whole step, or a plan whose items stage 4 is limited to (the step then stops after
+// that stage kernel: the adjoint's recomputation when only some planes of the step's result are read).
+int enqueue_step_hooked(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, StepHook* hook,
+                        const LaunchPlan* lastStage = nullptr);
 // One RK4 step of every member of an ensemble (dGrids: device array of `members` grids; L: the ensemble's
 // combined plan). events: NULL, or 8 events recorded around the four stage kernels.
 int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* stream, void* events);

@@ -599,8 +599,10 @@ void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vecto
 // solver (its stage kernel takes the grid by value), or NULL for an ensemble (the ensemble stage kernel
 // reads every member from dg). The small kernels carry the member in a grid dimension, their block
 // counts in L being the maxima over the members; the edge kernels run the listed blocks of every member.
+// lastStage: NULL, or the plan of a partial stage 4 (single grid): stage 4 then runs the stage kernel over
+// that plan's items only and the step ends there (no stage-4 boundary conditions, no finalize).
 static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev,
-                        StepHook* hook = nullptr) {
+                        StepHook* hook = nullptr, const LaunchPlan* lastStage = nullptr) {
   int launches = 0;
   const unsigned M = unsigned(members);
   k_prologue<<<M, 32, 0, st>>>(dg);
@@ -611,6 +613,14 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
   for (int s = 0; s < 4; ++s) {
     if (ev) cudaEventRecord(ev[2 * s], st);
     if (hook) hook->before_stage(s);
+    if (s == 3 && lastStage && hg) {
+      if (lastStage->nItems > 0) {
+        launch_stage(*hg, *lastStage, s, st);
+        ++launches;
+      }
+      if (hook) hook->before_edges(s);
+      return launches;
+    }
     if (hg)
       launch_stage(*hg, L, s, st);
     else
@@ -645,8 +655,9 @@ int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream) {
   return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), nullptr);
 }
 
-int enqueue_step_hooked(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, StepHook* hook) {
-  return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), nullptr, hook);
+int enqueue_step_hooked(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, StepHook* hook,
+                        const LaunchPlan* lastStage) {
+  return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), nullptr, hook, lastStage);
 }
 
 int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* stream, void* events) {

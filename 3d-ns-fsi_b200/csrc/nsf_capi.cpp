@@ -799,4 +799,10 @@ void nsf_destroy(nsf_solver* s) {
   delete s;
 }
 
+nsf_status nsf_math_selftest(int32_t device, uint64_t n, const double* x, double* out) {
+  if (n && (!x || !out)) return NSF_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return NSF_ERR_CUDA;
+  return math_selftest((long long)n, x, out) == 0 ? NSF_OK : NSF_ERR_CUDA;
+}
+
 }  // extern "C"

@@ -195,6 +195,8 @@ struct StepHook {
 // that stage kernel: the adjoint's recomputation when only some planes of the step's result are read).
 int enqueue_step_hooked(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, StepHook* hook,
                         const LaunchPlan* lastStage = nullptr);
+// recip_nr, 1/x, sqrt_nr, sqrt of n host values on the current device (4 x n results); a cudaError_t.
+int math_selftest(long long n, const double* hostIn, double* hostOut);
 // One RK4 step of every member of an ensemble (dGrids: device array of `members` grids; L: the ensemble's
 // combined plan). events: NULL, or 8 events recorded around the four stage kernels.
 int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* stream, void* events);

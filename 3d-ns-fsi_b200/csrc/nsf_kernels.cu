@@ -681,4 +681,30 @@ void launch_download_prims(const Grid* dg, long long N, double* out, const long 
   if (nInactive > 0) k_download_inactive<<<(nInactive + 255) / 256, 256, 0, st>>>(dg, inodes, ip7, nInactive, out);
 }
 
+// The Newton-Raphson reciprocal and square root next to the IEEE ones, for a check of their error.
+__global__ void k_math_selftest(long long n, const double* __restrict__ x, double* __restrict__ out) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const double a = x[q];
+    out[4 * q + 0] = recip_nr(a);
+    out[4 * q + 1] = 1.0 / a;
+    out[4 * q + 2] = sqrt_nr(a);
+    out[4 * q + 3] = sqrt(a);
+  }
+}
+
+int math_selftest(long long n, const double* hostIn, double* hostOut) {
+  double *dx = nullptr, *dout = nullptr;
+  cudaError_t e = cudaMalloc(&dx, (n > 0 ? n : 1) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dout, 4 * (n > 0 ? n : 1) * sizeof(double));
+  if (e == cudaSuccess && n > 0) e = cudaMemcpy(dx, hostIn, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && n > 0) {
+    k_math_selftest<<<int((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024), 256>>>(n, dx, dout);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && n > 0) e = cudaMemcpy(hostOut, dout, 4 * n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(dx);
+  cudaFree(dout);
+  return int(e);
+}
+
 }  // namespace nsf

@@ -107,6 +107,7 @@ def lib():
         "nsf_adj_backward": (i32, [vp, ctypes.c_double, dp, dp]),
         "nsf_adj_get_dt": (i32, [vp, dp, ctypes.POINTER(u64)]),
         "nsf_adj_profile_step": (i32, [vp, u64, dp]),
+        "nsf_math_selftest": (i32, [i32, u64, dp, dp]),
         "nsf_last_error": (ctypes.c_char_p, [vp]),
         "nsf_destroy": (None, [vp]),
     }
@@ -148,6 +149,16 @@ def config_load(path):
 
 def case_path(name):
     return os.path.join(CASES, name + ".cfg")
+
+
+def math_selftest(x, device=0):
+    """(4, n): the device's Newton-Raphson reciprocal, IEEE 1/x, Newton-Raphson square root, IEEE sqrt."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros(4 * x.size)
+    st = lib().nsf_math_selftest(device, x.size, _dp(x), _dp(out))
+    if st:
+        raise NsfError(st, "nsf_math_selftest failed")
+    return out.reshape(-1, 4).T
 
 
 class Solver:

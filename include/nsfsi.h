@@ -232,6 +232,11 @@ nsf_status nsf_adj_get_dt(nsf_solver* s, double* dts, uint64_t* count);
  * [7] transposed RHS, [8] density filter (summed over the four stages). Gradients are unaffected. */
 nsf_status nsf_adj_profile_step(nsf_solver* s, uint64_t step, double* ms);
 
+/* Self-check of the device reciprocal and square root the stage kernel uses for the primitive values
+ * (Newton-Raphson refinement of the hardware approximations): for n positive inputs x, out[4 i .. 4 i + 3]
+ * = the refined reciprocal, the IEEE 1/x, the refined square root, the IEEE sqrt(x). */
+nsf_status nsf_math_selftest(int32_t device, uint64_t n, const double* x, double* out);
+
 /* Text of the last error on this handle (static storage owned by the handle). */
 const char* nsf_last_error(nsf_solver* s);
 

@@ -322,13 +322,14 @@ __device__ __forceinline__ void x_face(const Consts& C, const XOwn& a, const XOw
 
 // y- and z-direction part of the right-hand side at P (the reference's terms not covered by G and F).
 // cP/pP: staged centre plane; pE/pW: staged neighbour planes (only their N/S/U/D velocity values are
-// read, for the mixed x-derivatives at the in-plane neighbours); own: P's own values.
+// read, for the mixed x-derivatives at the in-plane neighbours); own: P's own values. The staged planes
+// hold u, v, w, p, T, mu (fields 0..5); kappa = pf mu is formed here, as prims_of forms it.
 template <int HK, int FS>
 __device__ __forceinline__ void yz_part(const Consts& C, const double* __restrict__ cP, const double* __restrict__ pW,
                                         const double* __restrict__ pP, const double* __restrict__ pE, int c,
                                         const XOwn& own, double out[5]) {
   enum { RU = 1, RV = 2, RW = 3, RE = 4 };
-  enum { U = 0, V = 1, W = 2, P = 3, TT = 4, MU = 5, KA = 6 };
+  enum { U = 0, V = 1, W = 2, P = 3, TT = 4, MU = 5 };
 #define F_(b, v, o) (b)[(v)*FS + c + (o)]
   constexpr int oN = HK, oS = -HK, oU = 1, oD = -1;
   const double muP = own.mu, uP = own.u, vP = own.v, wP = own.w, TP = own.T, kP = own.ka;
@@ -394,8 +395,8 @@ __device__ __forceinline__ void yz_part(const Consts& C, const double* __restric
                        C.e_zy6 * (muU * wU * (vNU - vSU) - muD * wD * (vND - vSD)) +
                        C.e_zx4 * (muU * uU * (wEU - wWU) - muD * uD * (wED - wWD)) +
                        C.e_zy4 * (muU * vU * (wNU - wSU) - muD * vD * (wND - wSD));
-    const double hf = C.e_yy12 * ((F_(pP, KA, oN) + kP) * (F_(pP, TT, oN) - TP) - (F_(pP, KA, oS) + kP) * (TP - F_(pP, TT, oS))) +
-                      C.e_zz12 * ((F_(pP, KA, oU) + kP) * (F_(pP, TT, oU) - TP) - (F_(pP, KA, oD) + kP) * (TP - F_(pP, TT, oD)));
+    const double hf = C.e_yy12 * (((muN * C.pf) + kP) * (F_(pP, TT, oN) - TP) - ((muS * C.pf) + kP) * (TP - F_(pP, TT, oS))) +
+                      C.e_zz12 * (((muU * C.pf) + kP) * (F_(pP, TT, oU) - TP) - ((muD * C.pf) + kP) * (TP - F_(pP, TT, oD)));
     out[4] = inv + vfY + vfZ + hf;
   }
 #undef F_

@@ -8,7 +8,7 @@
 //     plus a one-node halo (box 34 x 10) into the conserved ring, and for every computed plane the U0
 //     and RK4-accumulator tile (box 34 x 8) into the epilogue ring. It never blocks on one slot, so no
 //     ordering between the rings can deadlock.
-//   warpgroup 0, warps 1-3 -- staging: the primitive and transport values (u, v, w, p, T, mu, kappa) of
+//   warpgroup 0, warps 1-3 -- staging: the primitive and transport values (u, v, w, p, T, mu) of
 //     the 340 staged nodes of each plane, once per plane, into the primitive ring. Filtered nodes take
 //     their values from before the near-body filter, as the reference does (its primitives are not
 //     recomputed after the filter).
@@ -38,7 +38,8 @@
 namespace nsf {
 namespace ws {
 constexpr int NSTAGE = 96;                        // staging threads (warps 1-3)
-constexpr int NC = 5, NP = 4, NE = 3;             // conserved / primitive / epilogue ring depths
+constexpr int NC = 5, NP = 5, NE = 3;             // conserved / primitive / epilogue ring depths
+constexpr int NPRIM = 6;                          // staged primitive fields: u, v, w, p, T, mu (kappa = pf mu)
 constexpr int MAP_CONS = 0, MAP_EPI = 15, MAP_ACC = 30, MAP_TYPE = 35, NMAPS = 36;
 constexpr long long WAIT_LIMIT = 1ll << 22;  // polls before a wait is declared failed
 // Register split (setmaxnreg): the launch gives every thread 168 registers (384 x 168 = 64,512); the
@@ -61,7 +62,7 @@ struct Tile {
   static constexpr uint32_t EPI_BOX_BYTES = HK * TJ * 8;
   static constexpr size_t TYPE_OFF = size_t(5) * FS * 8;  // node types follow the five fields in a slot
   static constexpr size_t CONS_SLOT = TYPE_OFF + size_t(round_up(TYW * HJ, 128));
-  static constexpr size_t PRIM_SLOT = size_t(7) * FS * 8;
+  static constexpr size_t PRIM_SLOT = size_t(NPRIM) * FS * 8;
   static constexpr size_t EPI_SLOT = size_t(10) * EFS * 8;
   static constexpr size_t OFF_CONS = 0;
   static constexpr size_t OFF_PRIM = OFF_CONS + NC * CONS_SLOT;
@@ -362,7 +363,6 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
             pv[3 * FS + idx] = a0.p;
             pv[4 * FS + idx] = a0.T;
             pv[5 * FS + idx] = a0.mu;
-            pv[6 * FS + idx] = a0.ka;
             if (idy < HP) {
               pv[0 * FS + idy] = a1.u;
               pv[1 * FS + idy] = a1.v;
@@ -370,7 +370,6 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
               pv[3 * FS + idy] = a1.p;
               pv[4 * FS + idy] = a1.T;
               pv[5 * FS + idy] = a1.mu;
-              pv[6 * FS + idy] = a1.ka;
             }
           }
           __syncwarp();
@@ -439,7 +438,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           const double* cs = reinterpret_cast<const double*>(consBase + cX * CONS_SLOT);
           const double* ps = reinterpret_cast<const double*>(primBase + pX * PRIM_SLOT);
           ownCur = XOwn{ps[5 * FS + cidx], ps[0 * FS + cidx], ps[1 * FS + cidx],
-                        ps[2 * FS + cidx], ps[4 * FS + cidx], ps[6 * FS + cidx]};
+                        ps[2 * FS + cidx], ps[4 * FS + cidx], ps[5 * FS + cidx] * C.pf};
           gcur = x_node(C, cs[1 * FS + cidx], cs[2 * FS + cidx], cs[3 * FS + cidx], cs[4 * FS + cidx], ownCur.u,
                         ownCur.v, ownCur.w, ps[3 * FS + cidx], ownCur.mu,
                         ps[1 * FS + cidx + oN] - ps[1 * FS + cidx - oN], ps[0 * FS + cidx + oN] - ps[0 * FS + cidx - oN],

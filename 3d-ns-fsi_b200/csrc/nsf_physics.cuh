@@ -285,13 +285,16 @@ __device__ __forceinline__ void rhs_eval(const Consts& C, const double* __restri
 // with G the convective/inviscid flux and the mixed-derivative products of a node, and F the normal
 // viscous and heat-flux products of an x-face, e.g. for x-momentum
 //   G = ax (rho_u u + p) + xm_yx mu (v_N - v_S) + xm_zx mu (w_U - w_D),   F = xm_xx (mu_a + mu_b)(u_b - u_a).
-// F(W,P) is bit-for-bit the reference's (mu_W + mu_P)(u_P - u_W) (addition commutes); G differences
-// regroup the reference's sums and differ from it by rounding only.
+// F(W,P) is the reference's (mu_W + mu_P)(u_P - u_W) (addition commutes); G differences regroup the
+// reference's sums and differ from it by rounding only. Here and in yz_part the energy equation's mixed
+// terms reuse the momentum equations' products (mu_N u_N (v_EN - v_WN) is formed as u_N [mu_N (v_EN - v_WN)])
+// and the heat flux (kappa_a + kappa_b)(T_b - T_a) is formed as pf (mu_a + mu_b)(T_b - T_a), kappa = pf mu:
+// the same sums, rounded differently.
 struct XNode {  // G of one node for the five equations
   double g[5];
 };
 struct XOwn {  // a node's values that the next x-face needs
-  double mu, u, v, w, T, ka;
+  double mu, u, v, w, T;
 };
 
 // G at one node. own: rho_u, rho_v, rho_w, rho_E, u, v, w, p, mu; d*: in-plane differences at the node
@@ -300,12 +303,13 @@ __device__ __forceinline__ XNode x_node(const Consts& C, double ru, double rv, d
                                         double v, double w, double p, double mu, double dyv, double dyu, double dzw,
                                         double dzu) {
   XNode n;
+  const double myv = mu * dyv, mzw = mu * dzw, myu = mu * dyu, mzu = mu * dzu;
   n.g[0] = C.ax * ru;
-  n.g[1] = C.ax * (ru * u + p) + C.xm_yx * (mu * dyv) + C.xm_zx * (mu * dzw);
-  n.g[2] = C.ax * (rv * u) + C.ym_yx * (mu * dyu);
-  n.g[3] = C.ax * (rw * u) + C.zm_zx * (mu * dzu);
-  n.g[4] = C.ax * ((C.h0 + rE + p) * u) + C.e_yx6 * (mu * u * dyv) + C.e_zx6 * (mu * u * dzw) +
-           C.e_yx4 * (mu * v * dyu) + C.e_zx4 * (mu * w * dzu);
+  n.g[1] = C.ax * (ru * u + p) + C.xm_yx * myv + C.xm_zx * mzw;
+  n.g[2] = C.ax * (rv * u) + C.ym_yx * myu;
+  n.g[3] = C.ax * (rw * u) + C.zm_zx * mzu;
+  n.g[4] = C.ax * ((C.h0 + rE + p) * u) + C.e_yx6 * (u * myv) + C.e_zx6 * (u * mzw) + C.e_yx4 * (v * myu) +
+           C.e_zx4 * (w * mzu);
   return n;
 }
 
@@ -317,7 +321,7 @@ __device__ __forceinline__ void x_face(const Consts& C, const XOwn& a, const XOw
   f[2] = C.ym_xx * (ms * (b.v - a.v));
   f[3] = C.zm_xx * (ms * (b.w - a.w));
   f[4] = C.e_xx23 * ((a.mu * a.u + b.mu * b.u) * (b.u - a.u)) + C.e_xx12 * ((a.mu * a.v + b.mu * b.v) * (b.v - a.v)) +
-         C.e_xx12 * ((a.mu * a.w + b.mu * b.w) * (b.w - a.w)) + C.e_xx12 * ((a.ka + b.ka) * (b.T - a.T));
+         C.e_xx12 * ((a.mu * a.w + b.mu * b.w) * (b.w - a.w)) + C.e_xx12 * (C.pf * (ms * (b.T - a.T)));
 }
 
 // y- and z-direction part of the right-hand side at P (the reference's terms not covered by G and F).
@@ -332,49 +336,56 @@ __device__ __forceinline__ void yz_part(const Consts& C, const double* __restric
   enum { U = 0, V = 1, W = 2, P = 3, TT = 4, MU = 5 };
 #define F_(b, v, o) (b)[(v)*FS + c + (o)]
   constexpr int oN = HK, oS = -HK, oU = 1, oD = -1;
-  const double muP = own.mu, uP = own.u, vP = own.v, wP = own.w, TP = own.T, kP = own.ka;
+  const double muP = own.mu, uP = own.u, vP = own.v, wP = own.w, TP = own.T;
   const double muN = F_(pP, MU, oN), muS = F_(pP, MU, oS), muU = F_(pP, MU, oU), muD = F_(pP, MU, oD);
   const double uN = F_(pP, U, oN), uS = F_(pP, U, oS), uU = F_(pP, U, oU), uD = F_(pP, U, oD);
   const double vN = F_(pP, V, oN), vS = F_(pP, V, oS), vU = F_(pP, V, oU), vD = F_(pP, V, oD);
   const double wN = F_(pP, W, oN), wS = F_(pP, W, oS), wU = F_(pP, W, oU), wD = F_(pP, W, oD);
   const double pN = F_(pP, P, oN), pS = F_(pP, P, oS), pU = F_(pP, P, oU), pD = F_(pP, P, oD);
-  const double vEN = F_(pE, V, oN), vES = F_(pE, V, oS), vWN = F_(pW, V, oN), vWS = F_(pW, V, oS);
-  const double uEN = F_(pE, U, oN), uES = F_(pE, U, oS), uWN = F_(pW, U, oN), uWS = F_(pW, U, oS);
-  const double wEU = F_(pE, W, oU), wED = F_(pE, W, oD), wWU = F_(pW, W, oU), wWD = F_(pW, W, oD);
-  const double uEU = F_(pE, U, oU), uED = F_(pE, U, oD), uWU = F_(pW, U, oU), uWD = F_(pW, U, oD);
+  // face viscosity sums (mu_N + mu_P) ... of the normal viscous and heat-flux terms
+  const double msN = muN + muP, msS = muS + muP, msU = muU + muP, msD = muD + muP;
+  // mixed-derivative products mu_X (difference across X), shared by momentum and energy
+  const double mNdxv = muN * (F_(pE, V, oN) - F_(pW, V, oN)), mSdxv = muS * (F_(pE, V, oS) - F_(pW, V, oS));
+  const double mNdxu = muN * (F_(pE, U, oN) - F_(pW, U, oN)), mSdxu = muS * (F_(pE, U, oS) - F_(pW, U, oS));
+  const double mUdxw = muU * (F_(pE, W, oU) - F_(pW, W, oU)), mDdxw = muD * (F_(pE, W, oD) - F_(pW, W, oD));
+  const double mUdxu = muU * (F_(pE, U, oU) - F_(pW, U, oU)), mDdxu = muD * (F_(pE, U, oD) - F_(pW, U, oD));
   const double wNU = F_(pP, W, oN + oU), wND = F_(pP, W, oN + oD), wSU = F_(pP, W, oS + oU), wSD = F_(pP, W, oS + oD);
   const double vNU = F_(pP, V, oN + oU), vND = F_(pP, V, oN + oD), vSU = F_(pP, V, oS + oU), vSD = F_(pP, V, oS + oD);
+  const double mNdzw = muN * (wNU - wND), mSdzw = muS * (wSU - wSD);  // w_U - w_D at N, S
+  const double mUdyw = muU * (wNU - wSU), mDdyw = muD * (wND - wSD);  // w_N - w_S at U, D
+  const double mNdzv = muN * (vNU - vND), mSdzv = muS * (vSU - vSD);  // v_U - v_D at N, S
+  const double mUdyv = muU * (vNU - vSU), mDdyv = muD * (vND - vSD);  // v_N - v_S at U, D
   out[0] = C.ay * (F_(cP, RV, oN) - F_(cP, RV, oS)) + C.az * (F_(cP, RW, oU) - F_(cP, RW, oD));
   {
     const double ruN = F_(cP, RU, oN), ruS = F_(cP, RU, oS), ruU = F_(cP, RU, oU), ruD = F_(cP, RU, oD);
     const double cY = C.ay * (ruN * vN - ruS * vS);
     const double cZ = C.az * (ruU * wU - ruD * wD);
-    const double vYY = C.xm_yy * ((muN + muP) * (uN - uP) - (muS + muP) * (uP - uS));
-    const double vZZ = C.xm_zz * ((muU + muP) * (uU - uP) - (muD + muP) * (uP - uD));
-    const double vXY = C.xm_xy * (muN * (vEN - vWN) - muS * (vES - vWS));
-    const double vXZ = C.xm_xz * (muU * (wEU - wWU) - muD * (wED - wWD));
+    const double vYY = C.xm_yy * (msN * (uN - uP) - msS * (uP - uS));
+    const double vZZ = C.xm_zz * (msU * (uU - uP) - msD * (uP - uD));
+    const double vXY = C.xm_xy * (mNdxv - mSdxv);
+    const double vXZ = C.xm_xz * (mUdxw - mDdxw);
     out[1] = cY + cZ + vYY + vZZ + vXY + vXZ;
   }
   {
     const double rvN = F_(cP, RV, oN), rvS = F_(cP, RV, oS), rvU = F_(cP, RV, oU), rvD = F_(cP, RV, oD);
     const double cY = C.ay * (rvN * vN + pN - rvS * vS - pS);
     const double cZ = C.az * (rvU * wU - rvD * wD);
-    const double vYY = C.ym_yy * ((muN + muP) * (vN - vP) - (muS + muP) * (vP - vS));
-    const double vZZ = C.ym_zz * ((muU + muP) * (vU - vP) - (muD + muP) * (vP - vD));
-    const double vXY = C.ym_xy * (muN * (uEN - uWN) - muS * (uES - uWS));
-    const double vYZ = C.ym_yz * (muU * (wNU - wSU) - muD * (wND - wSD));
-    const double vZY = C.ym_zy * (muN * (wNU - wND) - muS * (wSU - wSD));
+    const double vYY = C.ym_yy * (msN * (vN - vP) - msS * (vP - vS));
+    const double vZZ = C.ym_zz * (msU * (vU - vP) - msD * (vP - vD));
+    const double vXY = C.ym_xy * (mNdxu - mSdxu);
+    const double vYZ = C.ym_yz * (mUdyw - mDdyw);
+    const double vZY = C.ym_zy * (mNdzw - mSdzw);
     out[2] = cY + cZ + vYY + vZZ + vXY + vYZ + vZY;
   }
   {
     const double rwN = F_(cP, RW, oN), rwS = F_(cP, RW, oS), rwU = F_(cP, RW, oU), rwD = F_(cP, RW, oD);
     const double cY = C.ay * (rwN * vN - rwS * vS);
     const double cZ = C.az * (rwU * wU + pU - rwD * wD - pD);
-    const double vYY = C.zm_yy * ((muN + muP) * (wN - wP) - (muS + muP) * (wP - wS));
-    const double vZZ = C.zm_zz * ((muU + muP) * (wU - wP) - (muD + muP) * (wP - wD));
-    const double vXZ = C.zm_xz * (muU * (uEU - uWU) - muD * (uED - uWD));
-    const double vZY = C.zm_zy * (muN * (vNU - vND) - muS * (vSU - vSD));
-    const double vYZ = C.zm_yz * (muU * (vNU - vSU) - muD * (vND - vSD));
+    const double vYY = C.zm_yy * (msN * (wN - wP) - msS * (wP - wS));
+    const double vZZ = C.zm_zz * (msU * (wU - wP) - msD * (wP - wD));
+    const double vXZ = C.zm_xz * (mUdxu - mDdxu);
+    const double vZY = C.zm_zy * (mNdzv - mSdzv);
+    const double vYZ = C.zm_yz * (mUdyv - mDdyv);
     out[3] = cY + cZ + vYY + vZZ + vXZ + vZY + vYZ;
   }
   {
@@ -384,19 +395,15 @@ __device__ __forceinline__ void yz_part(const Consts& C, const double* __restric
     const double vfY = C.e_yy12 * ((muN * uN + muP * uP) * (uN - uP) - (muS * uS + muP * uP) * (uP - uS)) +
                        C.e_yy23 * ((muN * vN + muP * vP) * (vN - vP) - (muS * vS + muP * vP) * (vP - vS)) +
                        C.e_yy12 * ((muN * wN + muP * wP) * (wN - wP) - (muS * wS + muP * wP) * (wP - wS)) +
-                       C.e_yx6 * (muN * vN * (uEN - uWN) - muS * vS * (uES - uWS)) +
-                       C.e_zy6 * (muN * vN * (wNU - wND) - muS * vS * (wSU - wSD)) +
-                       C.e_yx4 * (muN * uN * (vEN - vWN) - muS * uS * (vES - vWS)) +
-                       C.e_zy4 * (muN * wN * (vNU - vND) - muS * wS * (vSU - vSD));
+                       C.e_yx6 * (vN * mNdxu - vS * mSdxu) + C.e_zy6 * (vN * mNdzw - vS * mSdzw) +
+                       C.e_yx4 * (uN * mNdxv - uS * mSdxv) + C.e_zy4 * (wN * mNdzv - wS * mSdzv);
     const double vfZ = C.e_zz12 * ((muU * uU + muP * uP) * (uU - uP) - (muD * uD + muP * uP) * (uP - uD)) +
                        C.e_zz12 * ((muU * vU + muP * vP) * (vU - vP) - (muD * vD + muP * vP) * (vP - vD)) +
                        C.e_zz23 * ((muU * wU + muP * wP) * (wU - wP) - (muD * wD + muP * wP) * (wP - wD)) +
-                       C.e_zx6 * (muU * wU * (uEU - uWU) - muD * wD * (uED - uWD)) +
-                       C.e_zy6 * (muU * wU * (vNU - vSU) - muD * wD * (vND - vSD)) +
-                       C.e_zx4 * (muU * uU * (wEU - wWU) - muD * uD * (wED - wWD)) +
-                       C.e_zy4 * (muU * vU * (wNU - wSU) - muD * vD * (wND - wSD));
-    const double hf = C.e_yy12 * (((muN * C.pf) + kP) * (F_(pP, TT, oN) - TP) - ((muS * C.pf) + kP) * (TP - F_(pP, TT, oS))) +
-                      C.e_zz12 * (((muU * C.pf) + kP) * (F_(pP, TT, oU) - TP) - ((muD * C.pf) + kP) * (TP - F_(pP, TT, oD)));
+                       C.e_zx6 * (wU * mUdxu - wD * mDdxu) + C.e_zy6 * (wU * mUdyv - wD * mDdyv) +
+                       C.e_zx4 * (uU * mUdxw - uD * mDdxw) + C.e_zy4 * (vU * mUdyw - vD * mDdyw);
+    const double hf = C.e_yy12 * (C.pf * (msN * (F_(pP, TT, oN) - TP) - msS * (TP - F_(pP, TT, oS)))) +
+                      C.e_zz12 * (C.pf * (msU * (F_(pP, TT, oU) - TP) - msD * (TP - F_(pP, TT, oD))));
     out[4] = inv + vfY + vfZ + hf;
   }
 #undef F_

@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           const double* cs = reinterpret_cast<const double*>(consBase + cX * CONS_SLOT);
           const double* ps = reinterpret_cast<const double*>(primBase + pX * PRIM_SLOT);
           ownCur = XOwn{ps[5 * FS + cidx], ps[0 * FS + cidx], ps[1 * FS + cidx],
-                        ps[2 * FS + cidx], ps[4 * FS + cidx], ps[5 * FS + cidx] * C.pf};
+                        ps[2 * FS + cidx], ps[4 * FS + cidx]};
           gcur = x_node(C, cs[1 * FS + cidx], cs[2 * FS + cidx], cs[3 * FS + cidx], cs[4 * FS + cidx], ownCur.u,
                         ownCur.v, ownCur.w, ps[3 * FS + cidx], ownCur.mu,
                         ps[1 * FS + cidx + oN] - ps[1 * FS + cidx - oN], ps[0 * FS + cidx + oN] - ps[0 * FS + cidx - oN],

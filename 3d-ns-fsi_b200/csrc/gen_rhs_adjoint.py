@@ -1,7 +1,7 @@
 """Generator of the transposed right-hand-side stencil (discrete adjoint of the RHS, gather form).
 
-The right-hand side of the five flux loops (Solver.cpp:181-418; the device version is rhs_eval in
-nsf_physics.cuh) is written below once, as a polynomial in nodal quantities at stencil offsets
+The right-hand side of the five flux loops (Solver.cpp:181-418; the stage kernel evaluates it as x_node,
+x_face and yz_part in nsf_physics.cuh) is written below once, as a polynomial in nodal quantities at stencil offsets
 (RU, RV, RW, RE: conserved momenta and energy; u, v, w, p, T, mu, ka: primitive and transport values)
 with the reference's stencil coefficients. From it this script emits
 
@@ -79,7 +79,7 @@ class Poly:
 
 
 def rhs_polys():
-    """The five RHS equations (continuity, x/y/z momentum, energy), term by term as rhs_eval writes them."""
+    """The five RHS equations (continuity, x/y/z momentum, energy), term by term in the reference's order."""
     V, K = Poly.var, Poly.const
     ax, ay, az = K("ax"), K("ay"), K("az")
 
@@ -228,7 +228,7 @@ def emit_cuda(terms):
     lines = []
     w = lines.append
     w("// Generated by gen_rhs_adjoint.py from the RHS term table: do not edit. The transposed stencil of the")
-    w("// right-hand side (rhs_eval, nsf_physics.cuh) in gather form: rhs_adjoint_gather(...) returns, for node")
+    w("// right-hand side (Solver.cpp:181-418) in gather form: rhs_adjoint_gather(...) returns, for node")
     w("// X = (i, j, k), the adjoint of each input quantity (RU, RV, RW, RE, u, v, w, p, T, mu, ka) summed over")
     w("// every interior node whose RHS reads it. lam(e, di, dj, dk): RHS adjoint of equation e at node")
     w("// (i+di, j+dj, k+dk) (zero where no RHS is taken); val(q, di, dj, dk): input quantity q there (offsets")

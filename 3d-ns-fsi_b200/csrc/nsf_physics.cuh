@@ -159,127 +159,10 @@ __device__ inline void flush_norms(double* slot, const double s[5], double* scra
 }
 
 
-// Right-hand side of the five flux loops at one node (continuity Solver.cpp:181-196, x/y/z momentum
-// :199-339, energy :342-418), terms evaluated in the reference's order. Inputs are three staged planes
-// (W = i-1, P = i, E = i+1), each holding the conserved values (fields 0..4: rho, rho_u, rho_v, rho_w,
-// rho_E) and the primitive / transport values (fields 0..6: u, v, w, p, T, mu, kappa) of a (j, k) tile
-// with a one-node halo, rows of HK values, field stride FS. c = index of the node in its plane.
-template <int HK, int FS>
-__device__ __forceinline__ void rhs_eval(const Consts& C, const double* __restrict__ cW, const double* __restrict__ cP,
-                                         const double* __restrict__ cE, const double* __restrict__ pW,
-                                         const double* __restrict__ pP, const double* __restrict__ pE, int c,
-                                         double out[5]) {
-  enum { RU = 1, RV = 2, RW = 3, RE = 4 };
-  enum { U = 0, V = 1, W = 2, P = 3, TT = 4, MU = 5, KA = 6 };
-#define F_(b, v, o) (b)[(v)*FS + c + (o)]
-  constexpr int oN = HK, oS = -HK, oU = 1, oD = -1;
-  {
-    const double fx = C.ax * (F_(cE, RU, 0) - F_(cW, RU, 0));
-    const double fy = C.ay * (F_(cP, RV, oN) - F_(cP, RV, oS));
-    const double fz = C.az * (F_(cP, RW, oU) - F_(cP, RW, oD));
-    out[0] = fx + fy + fz;
-  }
-  const double muP = F_(pP, MU, 0), muE = F_(pE, MU, 0), muW = F_(pW, MU, 0), muN = F_(pP, MU, oN),
-               muS = F_(pP, MU, oS), muU = F_(pP, MU, oU), muD = F_(pP, MU, oD);
-  const double uP = F_(pP, U, 0), uE = F_(pE, U, 0), uW = F_(pW, U, 0), uN = F_(pP, U, oN), uS = F_(pP, U, oS),
-               uU = F_(pP, U, oU), uD = F_(pP, U, oD);
-  const double vP = F_(pP, V, 0), vE = F_(pE, V, 0), vW = F_(pW, V, 0), vN = F_(pP, V, oN), vS = F_(pP, V, oS),
-               vU = F_(pP, V, oU), vD = F_(pP, V, oD);
-  const double wP = F_(pP, W, 0), wE = F_(pE, W, 0), wW = F_(pW, W, 0), wN = F_(pP, W, oN), wS = F_(pP, W, oS),
-               wU = F_(pP, W, oU), wD = F_(pP, W, oD);
-  const double pE_ = F_(pE, P, 0), pW_ = F_(pW, P, 0), pN = F_(pP, P, oN), pS = F_(pP, P, oS), pU = F_(pP, P, oU),
-               pD = F_(pP, P, oD);
-  const double vEN = F_(pE, V, oN), vES = F_(pE, V, oS), vWN = F_(pW, V, oN), vWS = F_(pW, V, oS);
-  const double uEN = F_(pE, U, oN), uES = F_(pE, U, oS), uWN = F_(pW, U, oN), uWS = F_(pW, U, oS);
-  const double wEU = F_(pE, W, oU), wED = F_(pE, W, oD), wWU = F_(pW, W, oU), wWD = F_(pW, W, oD);
-  const double uEU = F_(pE, U, oU), uED = F_(pE, U, oD), uWU = F_(pW, U, oU), uWD = F_(pW, U, oD);
-  const double wNU = F_(pP, W, oN + oU), wND = F_(pP, W, oN + oD), wSU = F_(pP, W, oS + oU), wSD = F_(pP, W, oS + oD);
-  const double vNU = F_(pP, V, oN + oU), vND = F_(pP, V, oN + oD), vSU = F_(pP, V, oS + oU), vSD = F_(pP, V, oS + oD);
-  {
-    const double ruE = F_(cE, RU, 0), ruW = F_(cW, RU, 0), ruN = F_(cP, RU, oN), ruS = F_(cP, RU, oS),
-                 ruU = F_(cP, RU, oU), ruD = F_(cP, RU, oD);
-    const double cX = C.ax * (ruE * uE + pE_ - ruW * uW - pW_);
-    const double cY = C.ay * (ruN * vN - ruS * vS);
-    const double cZ = C.az * (ruU * wU - ruD * wD);
-    const double vXX = C.xm_xx * ((muE + muP) * (uE - uP) - (muW + muP) * (uP - uW));
-    const double vYY = C.xm_yy * ((muN + muP) * (uN - uP) - (muS + muP) * (uP - uS));
-    const double vZZ = C.xm_zz * ((muU + muP) * (uU - uP) - (muD + muP) * (uP - uD));
-    const double vXY = C.xm_xy * (muN * (vEN - vWN) - muS * (vES - vWS));
-    const double vYX = C.xm_yx * (muE * (vEN - vES) - muW * (vWN - vWS));
-    const double vXZ = C.xm_xz * (muU * (wEU - wWU) - muD * (wED - wWD));
-    const double vZX = C.xm_zx * (muE * (wEU - wED) - muW * (wWU - wWD));
-    out[1] = cX + cY + cZ + vXX + vYY + vZZ + vXY + vYX + vXZ + vZX;
-  }
-  {
-    const double rvE = F_(cE, RV, 0), rvW = F_(cW, RV, 0), rvN = F_(cP, RV, oN), rvS = F_(cP, RV, oS),
-                 rvU = F_(cP, RV, oU), rvD = F_(cP, RV, oD);
-    const double cX = C.ax * (rvE * uE - rvW * uW);
-    const double cY = C.ay * (rvN * vN + pN - rvS * vS - pS);
-    const double cZ = C.az * (rvU * wU - rvD * wD);
-    const double vXX = C.ym_xx * ((muE + muP) * (vE - vP) - (muW + muP) * (vP - vW));
-    const double vYY = C.ym_yy * ((muN + muP) * (vN - vP) - (muS + muP) * (vP - vS));
-    const double vZZ = C.ym_zz * ((muU + muP) * (vU - vP) - (muD + muP) * (vP - vD));
-    const double vYX = C.ym_yx * (muE * (uEN - uES) - muW * (uWN - uWS));
-    const double vXY = C.ym_xy * (muN * (uEN - uWN) - muS * (uES - uWS));
-    const double vYZ = C.ym_yz * (muU * (wNU - wSU) - muD * (wND - wSD));
-    const double vZY = C.ym_zy * (muN * (wNU - wND) - muS * (wSU - wSD));
-    out[2] = cX + cY + cZ + vXX + vYY + vZZ + vYX + vXY + vYZ + vZY;
-  }
-  {
-    const double rwE = F_(cE, RW, 0), rwW = F_(cW, RW, 0), rwN = F_(cP, RW, oN), rwS = F_(cP, RW, oS),
-                 rwU = F_(cP, RW, oU), rwD = F_(cP, RW, oD);
-    const double cX = C.ax * (rwE * uE - rwW * uW);
-    const double cY = C.ay * (rwN * vN - rwS * vS);
-    const double cZ = C.az * (rwU * wU + pU - rwD * wD - pD);
-    const double vXX = C.zm_xx * ((muE + muP) * (wE - wP) - (muW + muP) * (wP - wW));
-    const double vYY = C.zm_yy * ((muN + muP) * (wN - wP) - (muS + muP) * (wP - wS));
-    const double vZZ = C.zm_zz * ((muU + muP) * (wU - wP) - (muD + muP) * (wP - wD));
-    const double vZX = C.zm_zx * (muE * (uEU - uED) - muW * (uWU - uWD));
-    const double vXZ = C.zm_xz * (muU * (uEU - uWU) - muD * (uED - uWD));
-    const double vZY = C.zm_zy * (muN * (vNU - vND) - muS * (vSU - vSD));
-    const double vYZ = C.zm_yz * (muU * (vNU - vSU) - muD * (vND - vSD));
-    out[3] = cX + cY + cZ + vXX + vYY + vZZ + vZX + vXZ + vZY + vYZ;
-  }
-  {
-    const double H0 = C.h0;
-    const double EE = F_(cE, RE, 0), EW = F_(cW, RE, 0), EN = F_(cP, RE, oN), ES = F_(cP, RE, oS),
-                 EU = F_(cP, RE, oU), ED = F_(cP, RE, oD);
-    const double inv = C.ax * ((H0 + EE + pE_) * uE - (H0 + EW + pW_) * uW) +
-                       C.ay * ((H0 + EN + pN) * vN - (H0 + ES + pS) * vS) +
-                       C.az * ((H0 + EU + pU) * wU - (H0 + ED + pD) * wD);
-    const double vfX = C.e_xx23 * ((muE * uE + muP * uP) * (uE - uP) - (muW * uW + muP * uP) * (uP - uW)) +
-                       C.e_xx12 * ((muE * vE + muP * vP) * (vE - vP) - (muW * vW + muP * vP) * (vP - vW)) +
-                       C.e_xx12 * ((muE * wE + muP * wP) * (wE - wP) - (muW * wW + muP * wP) * (wP - wW)) +
-                       C.e_yx6 * (muE * uE * (vEN - vES) - muW * uW * (vWN - vWS)) +
-                       C.e_zx6 * (muE * uE * (wEU - wED) - muW * uW * (wWU - wWD)) +
-                       C.e_yx4 * (muE * vE * (uEN - uES) - muW * vW * (uWN - uWS)) +
-                       C.e_zx4 * (muE * wE * (uEU - uED) - muW * wW * (uWU - uWD));
-    const double vfY = C.e_yy12 * ((muN * uN + muP * uP) * (uN - uP) - (muS * uS + muP * uP) * (uP - uS)) +
-                       C.e_yy23 * ((muN * vN + muP * vP) * (vN - vP) - (muS * vS + muP * vP) * (vP - vS)) +
-                       C.e_yy12 * ((muN * wN + muP * wP) * (wN - wP) - (muS * wS + muP * wP) * (wP - wS)) +
-                       C.e_yx6 * (muN * vN * (uEN - uWN) - muS * vS * (uES - uWS)) +
-                       C.e_zy6 * (muN * vN * (wNU - wND) - muS * vS * (wSU - wSD)) +
-                       C.e_yx4 * (muN * uN * (vEN - vWN) - muS * uS * (vES - vWS)) +
-                       C.e_zy4 * (muN * wN * (vNU - vND) - muS * wS * (vSU - vSD));
-    const double vfZ = C.e_zz12 * ((muU * uU + muP * uP) * (uU - uP) - (muD * uD + muP * uP) * (uP - uD)) +
-                       C.e_zz12 * ((muU * vU + muP * vP) * (vU - vP) - (muD * vD + muP * vP) * (vP - vD)) +
-                       C.e_zz23 * ((muU * wU + muP * wP) * (wU - wP) - (muD * wD + muP * wP) * (wP - wD)) +
-                       C.e_zx6 * (muU * wU * (uEU - uWU) - muD * wD * (uED - uWD)) +
-                       C.e_zy6 * (muU * wU * (vNU - vSU) - muD * wD * (vND - vSD)) +
-                       C.e_zx4 * (muU * uU * (wEU - wWU) - muD * uD * (wED - wWD)) +
-                       C.e_zy4 * (muU * vU * (wNU - wSU) - muD * vD * (wND - wSD));
-    const double kP = F_(pP, KA, 0), TP = F_(pP, TT, 0);
-    const double hf = C.e_xx12 * ((F_(pE, KA, 0) + kP) * (F_(pE, TT, 0) - TP) - (F_(pW, KA, 0) + kP) * (TP - F_(pW, TT, 0))) +
-                      C.e_yy12 * ((F_(pP, KA, oN) + kP) * (F_(pP, TT, oN) - TP) - (F_(pP, KA, oS) + kP) * (TP - F_(pP, TT, oS))) +
-                      C.e_zz12 * ((F_(pP, KA, oU) + kP) * (F_(pP, TT, oU) - TP) - (F_(pP, KA, oD) + kP) * (TP - F_(pP, TT, oD)));
-    out[4] = inv + vfX + vfY + vfZ + hf;
-  }
-#undef F_
-}
-
 // ---------------------------------------------------------------------------------------------------
-// The same right-hand side split by direction, for kernels that stream along i and keep the thread's
-// own (j, k) column in registers. For the x direction the reference's terms are differences of
+// Right-hand side of the five flux loops (continuity Solver.cpp:181-196, x/y/z momentum :199-339, energy
+// :342-418) split by direction, for kernels that stream along i and keep the thread's own (j, k) column in
+// registers. For the x direction the reference's terms are differences of
 // per-node quantities and of per-face quantities along the column:
 //   x-part(P) = [G(E) - G(W)] + [F(P,E) - F(W,P)]
 // with G the convective/inviscid flux and the mixed-derivative products of a node, and F the normal

@@ -1,5 +1,5 @@
 // Generated by gen_rhs_adjoint.py from the RHS term table: do not edit. The transposed stencil of the
-// right-hand side (rhs_eval, nsf_physics.cuh) in gather form: rhs_adjoint_gather(...) returns, for node
+// right-hand side (Solver.cpp:181-418) in gather form: rhs_adjoint_gather(...) returns, for node
 // X = (i, j, k), the adjoint of each input quantity (RU, RV, RW, RE, u, v, w, p, T, mu, ka) summed over
 // every interior node whose RHS reads it. lam(e, di, dj, dk): RHS adjoint of equation e at node
 // (i+di, j+dj, k+dk) (zero where no RHS is taken); val(q, di, dj, dk): input quantity q there (offsets

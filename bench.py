@@ -102,6 +102,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def host_model():
+    """The host CPU's model name (first /proc/cpuinfo entry), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(case_path, nodes):
     """Serial CPU reference timed on this host: the reference build (oracle/_ref) if present, else the
     oracle port. Sample: one RK4 step of the same workload at full size."""
@@ -111,13 +123,13 @@ def cpu_baseline(case_path, nodes):
         return {"value": r["node_steps_per_s"], "unit": "node-RK4-steps/s", "cores": 1, "kind": "reference",
                 "sample": "1 RK4 step of the full workload grid (%d nodes), serial reference build, %.1f s" %
                           (nodes, r["seconds"]),
-                "host_cores_present": os.cpu_count()}
+                "host_cores_present": os.cpu_count(), "host_model": host_model()}
     o = po.Oracle(open(case_path).read())
     sec = o.march(1)
     o.close()
     return {"value": nodes / sec, "unit": "node-RK4-steps/s", "cores": 1, "kind": "port",
             "sample": "1 RK4 step of the full workload grid (%d nodes), serial oracle port, %.1f s" % (nodes, sec),
-            "host_cores_present": os.cpu_count()}
+            "host_cores_present": os.cpu_count(), "host_model": host_model()}
 
 
 TUNE_CACHE = os.path.join(ROOT, "3d-ns-fsi_b200", "tuning", "stage_tiles.jsonl")
@@ -265,7 +277,8 @@ def run_reference_arm(args, rank, world):
             "config": {"workload": args.workload, "desc": wl["desc"], "grid": [int(c.NI), int(c.NJ), int(c.NK)]},
             "cpu_baseline": {"value": value, "unit": "node-RK4-steps/s", "cores": 1, "kind": kind,
                              "sample": "%d of the requested %d RK4 steps of the full %s grid, serial, 1 core of %d" %
-                                       (k, args.steps, args.workload, os.cpu_count())},
+                                       (k, args.steps, args.workload, os.cpu_count()),
+                             "host_model": host_model()},
             "e2e": {"value": value, "unit": "node-RK4-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -351,6 +364,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * nodes * args.steps / (ms / 1e3)
+    interior = int((cfg.NI - 2) * (cfg.NJ - 2) * (cfg.NK - 2))  # nodes whose RHS is computed
     launches = s.launches_per_step()
 
     # dominant kernel: live CUDA-event timing of the four stage kernels in as many eagerly launched steps,
@@ -403,6 +417,7 @@ def main():
         line = {
             "metric": "node-RK4-steps/s (FP64)", "value": value, "unit": "node-RK4-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "interior_value": world * interior * args.steps / (ms / 1e3),
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "desc": wl["desc"], "grid": [int(cfg.NI), int(cfg.NJ), int(cfg.NK)],
                        "parallelism": "replicas" if world > 1 else "single",
@@ -416,6 +431,9 @@ def main():
                          "kernel": "k_stage", "stage_ms": [round(x, 4) for x in stage_ms],
                          "algorithmic_bytes_per_node_step": BYTES_PER_NODE_STEP, "peak_kind": peak_kind,
                          "frac_of_8000": achieved / 8000.0, "profile_step_ms": round(step_ms, 4),
+                         # whole step (edge and control launches included): node-steps/s per GPU against
+                         # the node-steps/s the peak bandwidth allows at 680 B per node-step
+                         "step_frac": value / world / (peak * 1e9 / BYTES_PER_NODE_STEP),
                          "profile_clocks": clkp.summary()},
         }
         if ens is not None:

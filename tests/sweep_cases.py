@@ -1,0 +1,94 @@
+"""Seeded random cases for the sweep tests (tests/test_oracle_sweep_cpu.py, tests/test_parity_sweep_gpu.py).
+
+random_case(seed) draws a grid, one boundary type per axis (inlet/outlet, periodic, symmetry or outlet
+pairs in x; periodic, symmetry or outlet in y; periodic or symmetry in z), 0-2 spheres or a z-cylinder kept
+clear of the faces, Mach and Reynolds numbers, a filter interval and an initial condition (every sixth
+case a fully periodic Taylor-Green box), and returns the case file's text.
+"""
+import numpy as np
+
+N_CASES = 32  # cases each sweep runs
+STEPS = 8
+
+COMMON = """stopCriterion = "timesteps"
+t_end = 200.
+convStabilityLimit = 0.5
+viscStabilityLimit = -0.68
+filterIntervalChangeTimes = []
+statusReportInterval = 2.
+saveDensity = true
+saveMomentum = false
+saveEnergy = false
+saveVelocity = true
+savePressure = true
+saveTemperature = true
+saveViscosity = false
+saveThermalCond = false
+saveIC = false
+saveFinal = false
+saveIntervals = false
+savePeriod = 5.
+saveIntervalsStartTime = 0.
+saveIntervalsEndTime = 0.
+saveConvergenceHistory = "all"
+Gamma = 1.4
+Pr = 0.71
+R = 287.
+sutherlands_C1 = 1.458E-6
+sutherlands_C2 = 110.4
+T_0 = 300.
+"""
+
+
+def spacing(bc, n, L):
+    """Grid spacing of one axis from its min-face boundary type (Mesh.cpp:44-49)."""
+    return L / (n - 2) if bc == "periodic" else L / (n - 3) if bc == "symmetry" else L / (n - 1)
+
+
+def random_case(seed):
+    """The text of one seeded case file."""
+    rng = np.random.default_rng(seed)
+    bx = [("inlet", "outlet"), ("periodic", "periodic"), ("symmetry", "symmetry"), ("outlet", "outlet")][rng.integers(4)]
+    by = [("periodic", "periodic"), ("symmetry", "symmetry"), ("outlet", "outlet")][rng.integers(3)]
+    bz = [("periodic", "periodic"), ("symmetry", "symmetry")][rng.integers(2)]
+    tgv = seed % 6 == 5  # every sixth case: a fully periodic box with the Taylor-Green initial condition
+    if tgv:
+        bx = by = bz = ("periodic", "periodic")
+    L = [float(rng.uniform(1.2, 2.0)), float(rng.uniform(0.8, 1.2)), float(rng.uniform(0.8, 1.2))]
+    bodies = int(rng.integers(4))  # 0: none, 1-2: spheres, 3: a z-cylinder
+    if bodies:
+        n = [int(rng.integers(22, 30)), int(rng.integers(16, 22)), int(rng.integers(14, 20))]
+    else:
+        n = [int(rng.integers(10, 22)), int(rng.integers(8, 16)), int(rng.integers(5, 14))]
+    d = [spacing(b[0], nn, LL) for b, nn, LL in zip((bx, by, bz), n, L)]
+    shapes = ""
+    if bodies in (1, 2):
+        spheres = []
+        for _ in range(200):
+            if len(spheres) == bodies:
+                break
+            r = float(rng.uniform(2.5, 3.5)) * max(d)
+            if min(L[a] - 2 * (r + 4 * d[a]) for a in (1, 2)) <= 0:
+                continue
+            c = [float(rng.uniform(0.3, 0.7)) * L[0]] + [float(rng.uniform(r + 4 * d[a], L[a] - r - 4 * d[a]))
+                                                          for a in (1, 2)]
+            if all(np.linalg.norm(np.subtract(c, s[:3])) > r + s[3] + 4 * max(d) for s in spheres):
+                spheres.append(c + [r])
+        shapes = "  spheres = ( %s );\n" % ", ".join("(%.6f, %.6f, %.6f, %.6f)" % tuple(s) for s in spheres)
+    elif bodies == 3:
+        r = min(float(rng.uniform(2.5, 3.5)) * max(d[0], d[1]), 0.5 * L[1] - 4.5 * d[1])
+        c = [float(rng.uniform(0.35, 0.6)) * L[0], float(rng.uniform(r + 4 * d[1], L[1] - r - 4 * d[1])), 0.5 * L[2]]
+        shapes = '  cylinders = ( ("z", %.6f, %.6f, %.6f, %.6f) );\n' % (c[0], c[1], c[2], r)
+    M0 = float(rng.uniform(0.1, 0.4))
+    ic = "tgv" if tgv else "freestream_noise"
+    text = "NI = %d\nNJ = %d\nNK = %d\nstopTimeLevel = %d\nfilterIntervals = [%d]\n" % (
+        n[0], n[1], n[2], STEPS, int(rng.integers(3, 7)))
+    text += COMMON
+    text += "Re = %.6f\nM_0 = %.6f\nL_x = %.6f\nL_y = %.6f\nL_z = %.6f\n" % (
+        float(rng.uniform(200, 2000)), M0, L[0], L[1], L[2])
+    text += "case = {\n  kind = \"custom\";\n"
+    for ax, b in zip("xyz", (bx, by, bz)):
+        text += '  bc_%s_min = "%s";\n  bc_%s_max = "%s";\n' % (ax, b[0], ax, b[1])
+    text += shapes
+    text += '  ic = "%s";\n  noise_amp = 1e-3;\n  seed = %dL;\n};\n' % (ic, 1000 + seed)
+    return text

@@ -2,9 +2,12 @@
 parameters beyond the fixed parity cases, each run for a few RK4 steps through the C ABI and by the CPU
 oracle (which the CPU sweep pins bit for bit to the reference). Node classification must agree exactly and
 every field within 1e-10 of its family's magnitude (test_parity_gpu.field_errors); a flow that goes
-non-finite in the oracle must be reported non-finite by the device path. A case with an image point whose
-surrounding box reaches past the last node (the reference clamps the box index to n and reads out of range
-there) must be refused at setup with NSF_ERR_GEOMETRY, and only such a case."""
+non-finite in the oracle must be reported non-finite by the device path. Two kinds of case must be refused
+at setup with NSF_ERR_GEOMETRY, and only those: an image point whose surrounding box reaches past the last
+node (the reference clamps the box index to n and reads out of range there), and bodies close enough that
+one body's ghost/filter layer, filter stencil or image-point cell reaches another body's nodes (the
+reference then filters the bodies one after another, each reading the other's new values; the device path
+filters them all at once)."""
 import math
 import re
 
@@ -30,6 +33,51 @@ def image_point_past_last_node(o, shape):
     return False
 
 
+def surrounding_box(geo, shape, ip):
+    """Lower and upper node index per axis of an image point's cell (ceil(x / d) + offset, kept in 1..n)."""
+    lo = []
+    for a in range(3):
+        nx = min(max(int(math.ceil(ip[a] / geo[a]) + geo[3 + a]), 1), shape[a])
+        lo.append(nx - 1)
+    return lo
+
+
+def bodies_interact(o, shape):
+    """Whether one body's filter nodes, their 6-neighbours or the cells of its image points hold nodes of
+    another body's ghost or filter layer (or another body's ghost node)."""
+    bodies = o.bodies()
+    if len(bodies) < 2:
+        return False
+    sI, sJ = shape[1] * shape[2], shape[2]
+    owner = {}
+    ghost_sets = []
+    for q, (ghosts, filt, _) in enumerate(bodies):
+        gs = {int(g[0]) * sI + int(g[1]) * sJ + int(g[2]) for g in ghosts}
+        ghost_sets.append(gs)
+        for n in gs:
+            owner[n] = q
+    for q, (_, filt, _) in enumerate(bodies):
+        for f in filt:
+            if owner.get(int(f), q) != q:
+                return True
+            owner[int(f)] = q
+    geo = o.geometry()
+    for q, (ghosts, filt, _) in enumerate(bodies):
+        for f in filt:
+            for off in (sI, -sI, sJ, -sJ, 1, -1):
+                if owner.get(int(f) + off, q) != q:
+                    return True
+        for g in ghosts:
+            lo = surrounding_box(geo, shape, g[6:9])
+            for di in (0, 1):
+                for dj in (0, 1):
+                    for dk in (0, 1):
+                        n = (lo[0] + di) * sI + (lo[1] + dj) * sJ + lo[2] + dk
+                        if owner.get(n, q) != q or any(n in gs for r, gs in enumerate(ghost_sets) if r != q):
+                            return True
+    return False
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("seed", range(N_CASES))
 def test_gpu_matches_oracle_random_case(seed):
@@ -37,7 +85,7 @@ def test_gpu_matches_oracle_random_case(seed):
     shape = [int(re.search(r"^N%s = (\d+)$" % c, text, re.M).group(1)) for c in "IJK"]
     o = po.Oracle(text)
     try:
-        refused = image_point_past_last_node(o, shape)
+        refused = image_point_past_last_node(o, shape) or bodies_interact(o, shape)
         types = o.node_types()
         o.march(STEPS)
         ref = o.fields()

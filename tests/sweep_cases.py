@@ -92,3 +92,54 @@ def random_case(seed):
     text += shapes
     text += '  ic = "%s";\n  noise_amp = 1e-3;\n  seed = %dL;\n};\n' % (ic, 1000 + seed)
     return text
+
+
+def wide_case(seed, dt0=None):
+    """A second family (oracle against the reference only): cylinders along any periodic axis, a stagnation
+    start behind an inlet, up to three filter intervals with change times, and every other case stopped by
+    end_time, whose last step the reference shortens to land on t_end. Change times and t_end are set in
+    units of the case's first dt: call once with dt0=None (placeholders) to read dt0, then with it."""
+    rng = np.random.default_rng(10_000 + seed)
+    bx = [("inlet", "outlet"), ("periodic", "periodic"), ("symmetry", "symmetry"), ("inlet", "outlet")][rng.integers(4)]
+    by = [("periodic", "periodic"), ("symmetry", "symmetry"), ("outlet", "outlet")][rng.integers(3)]
+    bz = [("periodic", "periodic"), ("symmetry", "symmetry")][rng.integers(2)]
+    L = [float(rng.uniform(1.2, 2.0)), float(rng.uniform(0.8, 1.2)), float(rng.uniform(0.8, 1.2))]
+    n = [int(rng.integers(22, 30)), int(rng.integers(16, 22)), int(rng.integers(14, 20))]
+    d = [spacing(b[0], nn, LL) for b, nn, LL in zip((bx, by, bz), n, L)]
+    shapes = ""
+    periodic = [a for a, b in enumerate((bx, by, bz)) if b[0] == "periodic"]
+    if periodic and rng.integers(2):
+        ax = int(periodic[rng.integers(len(periodic))])
+        o1, o2 = [a for a in range(3) if a != ax]
+        r = float(rng.uniform(2.5, 3.5)) * max(d[o1], d[o2])
+        r = min(r, 0.5 * L[o1] - 4.5 * d[o1], 0.5 * L[o2] - 4.5 * d[o2])
+        c = [0.5 * L[0], 0.5 * L[1], 0.5 * L[2]]
+        for a in (o1, o2):
+            lo, hi = (0.35 * L[0], 0.6 * L[0]) if a == 0 else (r + 4 * d[a], L[a] - r - 4 * d[a])
+            c[a] = float(rng.uniform(lo, hi))
+        shapes = '  cylinders = ( ("%s", %.6f, %.6f, %.6f, %.6f) );\n' % ("xyz"[ax], c[0], c[1], c[2], r)
+    elif rng.integers(2):
+        r = min(float(rng.uniform(2.5, 3.5)) * max(d), min(0.5 * L[a] - 4.5 * d[a] for a in (1, 2)))
+        c = [float(rng.uniform(0.35, 0.6)) * L[0]] + [float(rng.uniform(r + 4 * d[a], L[a] - r - 4 * d[a])) for a in (1, 2)]
+        shapes = "  spheres = ( (%.6f, %.6f, %.6f, %.6f) );\n" % (c[0], c[1], c[2], r)
+    ic = "stagnation" if bx[0] == "inlet" and rng.integers(2) else "freestream_noise"
+    nf = int(rng.integers(1, 4))
+    intervals = [int(rng.integers(2, 6)) for _ in range(nf)]
+    end_time = seed % 2 == 1
+    unit = dt0 if dt0 else 1.0
+    changes = ", ".join(repr((2.5 + 2 * q) * unit) for q in range(nf - 1))  # floats in the config grammar
+    text = "NI = %d\nNJ = %d\nNK = %d\nstopTimeLevel = %d\nfilterIntervals = [%s]\n" % (
+        n[0], n[1], n[2], STEPS, ", ".join(map(str, intervals)))
+    common = COMMON.replace("filterIntervalChangeTimes = []", "filterIntervalChangeTimes = [%s]" % changes)
+    if end_time:
+        common = common.replace('stopCriterion = "timesteps"', 'stopCriterion = "end_time"')
+        common = common.replace("t_end = 200.", "t_end = " + repr(5.5 * unit if dt0 else 200.0))
+    text += common
+    text += "Re = %.6f\nM_0 = %.6f\nL_x = %.6f\nL_y = %.6f\nL_z = %.6f\n" % (
+        float(rng.uniform(200, 2000)), float(rng.uniform(0.1, 0.4)), L[0], L[1], L[2])
+    text += "case = {\n  kind = \"custom\";\n"
+    for ax, b in zip("xyz", (bx, by, bz)):
+        text += '  bc_%s_min = "%s";\n  bc_%s_max = "%s";\n' % (ax, b[0], ax, b[1])
+    text += shapes
+    text += '  ic = "%s";\n  noise_amp = 1e-3;\n  seed = %dL;\n};\n' % (ic, 2000 + seed)
+    return text

@@ -1,5 +1,5 @@
-"""Pins the CPU oracle to the reference solver on seeded random cases (tests/sweep_cases.py), beyond the
-fixed golden cases: the unmodified reference (oracle/_ref/ref_runner, built from the reference sources by
+"""Pins the CPU oracle to the reference solver on seeded random cases (tests/sweep_cases.py: the random_case
+and wide_case families), beyond the fixed golden cases: the unmodified reference (oracle/_ref/ref_runner, built from the reference sources by
 oracle/Makefile.ref) and the oracle run a few RK4 steps of each case, and node classification, ghost and
 filter lists, the dt and norm histories and all twelve fields must agree bit for bit. Skipped where the
 reference build is absent.
@@ -11,22 +11,21 @@ import numpy as np
 import pytest
 
 from oracle import pyoracle as po
-from sweep_cases import N_CASES, STEPS, random_case
+from sweep_cases import N_CASES, STEPS, random_case, wide_case
 
 
-@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
-@pytest.mark.parametrize("seed", range(N_CASES))
-def test_oracle_matches_reference_random_case(seed):
-    text = random_case(seed)
+def compare(text, level=STEPS):
+    """Run the reference build and the oracle on one case file; level: the step to compare at ("final": where
+    the run stops, for an end_time case)."""
     with tempfile.TemporaryDirectory(prefix="nsf_sweep_") as tmp:
         cfg = os.path.join(tmp, "case.cfg")
         with open(cfg, "w") as f:
             f.write(text)
         out = os.path.join(tmp, "ref")
         os.makedirs(out)
-        po.run_reference(cfg, [STEPS], outdir=out)
+        po.run_reference(cfg, [STEPS], outdir=out, final=level == "final")
         ref = po.read_ref_setup(out)
-        fin = po.read_ref_fields(out, STEPS)
+        fin = po.read_ref_fields(out, level)
         hist = po.read_ref_history(out)
     o = po.Oracle(text)
     try:
@@ -37,7 +36,7 @@ def test_oracle_matches_reference_random_case(seed):
         assert len(bodies) == len(ref["bodies"])
         for (gh, fl, _), (rg, rf) in zip(bodies, ref["bodies"]):
             assert np.array_equal(gh, rg) and np.array_equal(fl, rf)
-        o.march(STEPS)
+        o.march(fin["level"])
         assert o.t == fin["t"]
         f = o.fields()
         # a drawn flow can go non-finite in the reference's own algorithm (it prints and marches on, as the
@@ -49,3 +48,19 @@ def test_oracle_matches_reference_random_case(seed):
         assert np.array_equal(h[:, 2:], hist[: len(h), 3:], equal_nan=True)
     finally:
         o.close()
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+@pytest.mark.parametrize("seed", range(N_CASES))
+def test_oracle_matches_reference_random_case(seed):
+    compare(random_case(seed))
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+@pytest.mark.parametrize("seed", range(N_CASES))
+def test_oracle_matches_reference_wide_case(seed):
+    """Cylinders along any periodic axis, stagnation starts, filter-interval changes, end_time stops."""
+    o = po.Oracle(wide_case(seed))
+    dt0 = o.dt
+    o.close()
+    compare(wide_case(seed, dt0), level="final")

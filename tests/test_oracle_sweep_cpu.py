@@ -1,8 +1,8 @@
 """Pins the CPU oracle to the reference solver on seeded random cases (tests/sweep_cases.py: the random_case
-and wide_case families), beyond the fixed golden cases: the unmodified reference (oracle/_ref/ref_runner, built from the reference sources by
-oracle/Makefile.ref) and the oracle run a few RK4 steps of each case, and node classification, ghost and
-filter lists, the dt and norm histories and all twelve fields must agree bit for bit. Skipped where the
-reference build is absent.
+and wide_case families), beyond the fixed golden cases: the unmodified reference (oracle/_ref/ref_runner,
+built from the reference sources by oracle/Makefile.ref) and the oracle run a few RK4 steps of each case,
+and node classification, ghost and filter lists, the dt and norm histories and all twelve fields must agree
+bit for bit. Skipped where the reference build is absent.
 """
 import os
 import tempfile

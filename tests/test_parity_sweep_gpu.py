@@ -1,5 +1,5 @@
-"""GPU parity on seeded random cases (tests/sweep_cases.py): boundary combinations, bodies and flow
-parameters beyond the fixed parity cases, each run for a few RK4 steps through the C ABI and by the CPU
+"""GPU parity on seeded random cases (tests/sweep_cases.py, both families): boundary combinations, bodies,
+stop criteria, filter schedules and flow parameters beyond the fixed parity cases, each run for a few RK4 steps through the C ABI and by the CPU
 oracle (which the CPU sweep pins bit for bit to the reference). Node classification must agree exactly and
 every field within 1e-10 of its family's magnitude (test_parity_gpu.field_errors); a flow that goes
 non-finite in the oracle must be reported non-finite by the device path. Two kinds of case must be refused
@@ -16,7 +16,7 @@ import pytest
 
 import nsfsi
 from oracle import pyoracle as po
-from sweep_cases import N_CASES, STEPS, random_case
+from sweep_cases import N_CASES, STEPS, random_case, wide_case
 from test_parity_gpu import FIELD_TOL, field_errors
 
 
@@ -78,16 +78,20 @@ def bodies_interact(o, shape):
     return False
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("seed", range(N_CASES))
-def test_gpu_matches_oracle_random_case(seed):
-    text = random_case(seed)
+def check_case(text):
+    """One case through the oracle and the device path. The oracle marches STEPS steps, or for an end_time
+    case until t reaches t_end (Simulation::run's stopping check; the last dt is shortened to land on it)."""
     shape = [int(re.search(r"^N%s = (\d+)$" % c, text, re.M).group(1)) for c in "IJK"]
+    end_time = 'stopCriterion = "end_time"' in text
+    t_end = float(re.search(r"^t_end = (\S+)$", text, re.M).group(1))
     o = po.Oracle(text)
     try:
         refused = image_point_past_last_node(o, shape) or bodies_interact(o, shape)
         types = o.node_types()
-        o.march(STEPS)
+        level = 0
+        while level < STEPS and not (end_time and o.t >= t_end):
+            o.march(1)
+            level += 1
         ref = o.fields()
         t_ref = o.t
     finally:
@@ -99,7 +103,7 @@ def test_gpu_matches_oracle_random_case(seed):
         return
     with nsfsi.Solver(text) as s:
         assert np.array_equal(s.node_types(), types)
-        s.march(STEPS)
+        s.march(level)
         try:
             s.sync()
             finite = True
@@ -111,6 +115,22 @@ def test_gpu_matches_oracle_random_case(seed):
             return
         assert finite
         t, lv, _ = s.time()
-        assert lv == STEPS and abs(t - t_ref) <= 1e-12 * abs(t_ref)
+        assert lv == level and abs(t - t_ref) <= 1e-12 * abs(t_ref)
         e = field_errors(s.download(), ref)
         assert (e <= FIELD_TOL).all(), dict(zip(nsfsi.FIELDS, e))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(N_CASES))
+def test_gpu_matches_oracle_random_case(seed):
+    check_case(random_case(seed))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(N_CASES))
+def test_gpu_matches_oracle_wide_case(seed):
+    """Cylinders along any periodic axis, stagnation starts, filter-interval changes, end_time stops."""
+    o = po.Oracle(wide_case(seed))
+    dt0 = o.dt
+    o.close()
+    check_case(wide_case(seed, dt0))

@@ -141,16 +141,30 @@ void nsfo_set_frozen_dt(void* hp, const double* dts, uint64_t n) {
   h->s->dt = h->s->frozenDt[std::min<size_t>(h->s->stepCounter, n - 1)];
 }
 
-// Runs nsteps calls of marchTimeStep; returns wall seconds spent in the loop.
+// Runs nsteps calls of marchTimeStep; returns wall seconds spent in the loop, or -1 if a step threw (the
+// reference's own exceptions, e.g. a solid node around an image point, Boundary.cpp:723-724; the message is
+// kept for nsfo_last_error).
 double nsfo_march(void* hp, uint64_t nsteps) {
   auto* h = static_cast<Handle*>(hp);
   auto t0 = std::chrono::steady_clock::now();
-  for (uint64_t s = 0; s < nsteps; ++s) {
-    h->dtHist.push_back(h->s->dt);
-    h->s->marchTimeStep(h->t, h->level);
-    h->tHist.push_back(h->t);
+  try {
+    for (uint64_t s = 0; s < nsteps; ++s) {
+      h->dtHist.push_back(h->s->dt);
+      h->s->marchTimeStep(h->t, h->level);
+      h->tHist.push_back(h->t);
+    }
+  } catch (const std::exception& e) {
+    h->err = e.what();
+    return -1.0;
   }
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// The message of the last failed call (empty if none); returns its length.
+int nsfo_last_error(void* hp, char* buf, int len) {
+  const std::string& e = static_cast<Handle*>(hp)->err;
+  if (buf && len > 0) std::snprintf(buf, len, "%s", e.c_str());
+  return int(e.size());
 }
 
 uint64_t nsfo_num_nodes(void* hp) { return static_cast<Handle*>(hp)->s->N; }

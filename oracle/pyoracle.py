@@ -36,6 +36,8 @@ def lib():
         L.nsfo_set_exact_image_solve.argtypes = [vp, ctypes.c_int]
         L.nsfo_march.restype = dbl
         L.nsfo_march.argtypes = [vp, u64]
+        L.nsfo_last_error.restype = ctypes.c_int
+        L.nsfo_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         for name, rt in [("nsfo_num_nodes", u64), ("nsfo_time", dbl), ("nsfo_time_level", u64), ("nsfo_dt", dbl),
                          ("nsfo_non_finite", ctypes.c_int), ("nsfo_num_bodies", u64)]:
             getattr(L, name).restype = rt
@@ -112,7 +114,13 @@ class Oracle:
         lib().nsfo_set_frozen_dt(self.h, _dp(a), len(a))
 
     def march(self, nsteps):
-        return lib().nsfo_march(self.h, nsteps)
+        """Wall seconds of nsteps steps; RuntimeError if the reference algorithm throws on the way."""
+        sec = lib().nsfo_march(self.h, nsteps)
+        if sec < 0:
+            buf = ctypes.create_string_buffer(512)
+            lib().nsfo_last_error(self.h, buf, 512)
+            raise RuntimeError("oracle march error: " + buf.value.decode())
+        return sec
 
     @property
     def t(self):

@@ -143,3 +143,26 @@ def wide_case(seed, dt0=None):
     text += shapes
     text += '  ic = "%s";\n  noise_amp = 1e-3;\n  seed = %dL;\n};\n' % (ic, 2000 + seed)
     return text
+
+
+def shipped_case(seed, dt0=None):
+    """The reference's own default case (kind "shipped": Solver::initialize unchanged — inlet/outlet x,
+    symmetry y, periodic z, its cylinder, stagnation start, end_time stop) with seeded grid, box, flow
+    and filter settings. t_end and the filter change times are in units of the first dt (see wide_case)."""
+    rng = np.random.default_rng(20_000 + seed)
+    unit = dt0 if dt0 else 1.0
+    nf = int(rng.integers(1, 4))
+    text = "NI = %d\nNJ = %d\nNK = %d\n" % (int(rng.integers(30, 60)), int(rng.integers(16, 32)),
+                                            int(rng.integers(3, 7)))
+    text += 'stopCriterion = "end_time"\nstopTimeLevel = 20\nt_end = %s\n' % repr(7.5 * unit if dt0 else 200.0)
+    text += "convStabilityLimit = %s\nviscStabilityLimit = -0.68\n" % repr(float(rng.uniform(0.5, 0.9)))
+    text += "filterIntervals = [%s]\nfilterIntervalChangeTimes = [%s]\n" % (
+        ", ".join(str(int(rng.integers(2, 6))) for _ in range(nf)),
+        ", ".join(repr((2.5 + 2 * q) * unit) for q in range(nf - 1)))
+    text += COMMON[COMMON.index("statusReportInterval"):].replace("Pr = 0.71", "Pr = %s" % repr(
+        float(rng.uniform(0.65, 0.75))))
+    text += "Re = %s\nM_0 = %s\nL_x = %s\nL_y = %s\nL_z = %s\n" % (
+        repr(float(rng.uniform(100, 1000))), repr(float(rng.uniform(0.1, 0.4))), repr(float(rng.uniform(1.5, 3.0))),
+        repr(float(rng.uniform(0.8, 1.5))), repr(float(rng.uniform(0.03, 0.1))))
+    text += 'case = {\n  kind = "shipped";\n};\n'
+    return text

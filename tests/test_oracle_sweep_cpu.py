@@ -1,17 +1,19 @@
-"""Pins the CPU oracle to the reference solver on seeded random cases (tests/sweep_cases.py: the random_case
-and wide_case families), beyond the fixed golden cases: the unmodified reference (oracle/_ref/ref_runner,
-built from the reference sources by oracle/Makefile.ref) and the oracle run a few RK4 steps of each case,
-and node classification, ghost and filter lists, the dt and norm histories and all twelve fields must agree
-bit for bit. Skipped where the reference build is absent.
+"""Pins the CPU oracle to the reference solver on seeded random cases (tests/sweep_cases.py: the random_case,
+wide_case and shipped_case families), beyond the fixed golden cases: the unmodified reference
+(oracle/_ref/ref_runner, built from the reference sources by oracle/Makefile.ref) and the oracle run a few
+RK4 steps of each case, and node classification, ghost and filter lists, the dt and norm histories and all
+twelve fields must agree bit for bit; where the reference stops on one of its own exceptions the oracle
+must stop too. Skipped where the reference build is absent.
 """
 import os
+import subprocess
 import tempfile
 
 import numpy as np
 import pytest
 
 from oracle import pyoracle as po
-from sweep_cases import N_CASES, STEPS, random_case, wide_case
+from sweep_cases import N_CASES, STEPS, random_case, shipped_case, wide_case
 
 
 def compare(text, level=STEPS):
@@ -23,7 +25,18 @@ def compare(text, level=STEPS):
             f.write(text)
         out = os.path.join(tmp, "ref")
         os.makedirs(out)
-        po.run_reference(cfg, [STEPS], outdir=out, final=level == "final")
+        try:
+            po.run_reference(cfg, [STEPS], outdir=out, final=level == "final")
+        except subprocess.CalledProcessError:
+            # the reference stopped on one of its own exceptions (for instance a solid node around an image
+            # point, Boundary.cpp:723-724): the oracle must stop there too
+            o = po.Oracle(text)
+            try:
+                with pytest.raises(RuntimeError):
+                    o.march(STEPS)
+            finally:
+                o.close()
+            return
         ref = po.read_ref_setup(out)
         fin = po.read_ref_fields(out, level)
         hist = po.read_ref_history(out)
@@ -64,3 +77,14 @@ def test_oracle_matches_reference_wide_case(seed):
     dt0 = o.dt
     o.close()
     compare(wide_case(seed, dt0), level="final")
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+@pytest.mark.parametrize("seed", list(range(N_CASES)) + [59])
+def test_oracle_matches_reference_shipped_case(seed):
+    """The reference's default case (Solver::initialize unchanged) with seeded settings; seed 59 is one where
+    the reference throws (a solid node around an image point)."""
+    o = po.Oracle(shipped_case(seed))
+    dt0 = o.dt
+    o.close()
+    compare(shipped_case(seed, dt0), level="final")

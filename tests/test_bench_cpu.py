@@ -1,0 +1,106 @@
+"""bench.py keeps its output contract, checked on the CPU: the main arm run in-process against a stand-in
+solver module (fixed device times, no device), the CPU-baseline helper on a small case, and the reference
+arm on the 48^3 sphere workload for one step."""
+import json
+import os
+import subprocess
+import sys
+import types
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+from oracle import pyoracle as po  # noqa: E402
+
+STAGE_MS = [0.7, 0.72, 0.72, 0.8]
+STEP_MS = 3.1
+
+
+def fake_nsfsi():
+    """A module with the solver API bench.py's main arm calls, reporting fixed times."""
+    m = types.ModuleType("nsfsi")
+
+    class NsfError(RuntimeError):
+        code = 0
+
+    class Cfg:
+        NI = NJ = NK = 256
+
+    class Solver:
+        def __init__(self, cfg, device=0):
+            pass
+
+        def march(self, n):
+            pass
+
+        def sync(self):
+            pass
+
+        def march_timed(self, n):
+            return STEP_MS * n
+
+        def launches_per_step(self):
+            return 19
+
+        def profile_steps(self, n):
+            return np.array(STAGE_MS), STEP_MS + 0.05
+
+        def close(self):
+            pass
+
+    m.NsfError, m.Solver = NsfError, Solver
+    m.case_path = lambda name: name
+    m.config_load = lambda path: Cfg()
+    return m
+
+
+def test_main_arm_line_keeps_the_contract(monkeypatch, capsys):
+    monkeypatch.setitem(sys.modules, "nsfsi", fake_nsfsi())
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "10", "--warmup", "3", "--no-e2e", "--ensemble-steps",
+                                      "0", "--no-adjoint", "--no-cpu-baseline"])
+    bench.main()
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    nodes = 256 ** 3
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "e2e", "gpu_launches", "clocks", "roofline"):
+        assert key in line, key
+    assert line["n_gpus"] == 1 and line["steps"] == 10 and line["warmup"] == 3
+    assert line["higher_is_better"] is True and line["scaling"] == "weak" and line["dtype"] == "f64"
+    assert line["config"]["workload"] == "tgv256"
+    assert line["value"] == pytest.approx(nodes * 10 / (STEP_MS * 10 / 1e3))
+    assert line["ms_per_step"] == pytest.approx(STEP_MS)
+    assert line["interior_value"] == pytest.approx(254 ** 3 * 10 / (STEP_MS * 10 / 1e3))
+    assert line["gpu_launches"] == 190
+    assert set(line["clocks"]) >= {"sm_mhz", "sm_max_mhz", "reasons"}
+    r = line["roofline"]
+    for key in ("bound", "achieved", "peak", "unit", "frac", "traffic"):
+        assert key in r, key
+    assert r["bound"] == "hbm" and r["unit"] == "GB/s"
+    assert r["achieved"] == pytest.approx(680 * nodes / (sum(STAGE_MS) / 1e3) / 1e9)
+    assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+    assert r["step_frac"] == pytest.approx(line["value"] / (r["peak"] * 1e9 / 680))
+    assert line["e2e"] is None  # --no-e2e
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+def test_cpu_baseline_describes_its_sample():
+    case = os.path.join(ROOT, "tests", "golden", "cases", "tgv_small.cfg")
+    b = bench.cpu_baseline(case, 14 * 12 * 13)
+    assert b["kind"] == "reference" and b["cores"] == 1 and b["unit"] == "node-RK4-steps/s"
+    assert b["value"] > 0 and "RK4 step" in b["sample"]
+    assert b["host_cores_present"] >= 1 and "host_model" in b
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+def test_reference_arm_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "sphere48", "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=300,
+                         check=True).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "node-RK4-steps/s"
+    assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["cores"] == 1
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}

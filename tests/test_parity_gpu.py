@@ -1,6 +1,8 @@
 """GPU parity: the sm_100a path (through the C ABI) against the reference's own fields (golden fixtures)
-and against the CPU oracle run in-process. Tolerance: every field within 1e-10 of the
-reference, measured as max|gpu - ref| / max|ref| per field; dt and t within 1e-12 relative."""
+and against the CPU oracle run in-process. Tolerance: every field within 1e-10 of the reference, measured
+as max|gpu - ref| / max|ref| per field; dt and t within 1e-12 relative. On the small cases also pointwise:
+|gpu - ref| / |ref| <= 1e-6 at every node where |ref| > 1e-8 (largest measured on a B200: 2.7e-8, at nodes
+whose value is barely above 1e-8, where rounding-level absolute differences are relatively large)."""
 import os
 
 import numpy as np
@@ -16,6 +18,8 @@ FIELD_TOL = 1e-10
 TIME_TOL = 1e-12  # t after the dumped step, relative
 DT_TOL = 1e-10    # every dt of the history, relative
 NORM_TOL = 1e-8   # change norms, relative to the largest recorded norm
+POINT_TOL = 1e-6  # pointwise relative difference where |ref| > POINT_FLOOR
+POINT_FLOOR = 1e-8
 SMALL = {
     "sphere_small": "tests/golden/cases/sphere_small.cfg",
     "tgv_small": "tests/golden/cases/tgv_small.cfg",
@@ -58,9 +62,15 @@ def test_small_cases_match_reference(name):
             t, lv, dt = s.time()
             ref_t = float(g["t_%d" % d])
             assert abs(t - ref_t) <= TIME_TOL * abs(ref_t)
-            e = field_errors(s.download(), g["fields_%d" % d])
+            a, ref = s.download(), g["fields_%d" % d]
+            e = field_errors(a, ref)
             assert (e[:5] <= FIELD_TOL).all(), dict(zip(nsfsi.FIELDS, e))
             assert (e <= FIELD_TOL).all(), dict(zip(nsfsi.FIELDS, e))
+            for f in range(ref.shape[0]):
+                m = np.abs(ref[f]) > POINT_FLOOR
+                if m.any():
+                    worst = float((np.abs(a[f][m] - ref[f][m]) / np.abs(ref[f][m])).max())
+                    assert worst <= POINT_TOL, (nsfsi.FIELDS[f], worst)
         h = s.history()
         gh = g["history"][: len(h)]
         dt_err = float(np.abs(h[:, 1] / gh[:, 1] - 1).max())

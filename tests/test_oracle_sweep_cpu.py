@@ -32,7 +32,7 @@ def compare(text, level=STEPS):
         out = os.path.join(tmp, "ref")
         os.makedirs(out)
         try:
-            po.run_reference(cfg, [STEPS], outdir=out, final=level == "final")
+            po.run_reference(cfg, [STEPS if level == "final" else level], outdir=out, final=level == "final")
         except subprocess.CalledProcessError:
             # the reference stopped on one of its own exceptions (for instance a solid node around an image
             # point, Boundary.cpp:723-724): the oracle must stop there too
@@ -93,3 +93,32 @@ def test_oracle_matches_reference_shipped_case(seed):
     dt0 = o.dt
     o.close()
     compare(shipped_case(seed, dt0), level="final")
+
+
+def ensemble_member_text(c, steps):
+    """The case file of one member of the batched-ensemble workload (nsfsi.ensemble_configs, built there from
+    the 48^3 sphere case) with `steps` RK4 steps."""
+    import re
+    import nsfsi
+    text = open(nsfsi.case_path("sphere48")).read()
+    sp = c.spheres[0]
+    for key, val in (("NI", str(c.NI)), ("NJ", str(c.NJ)), ("NK", str(c.NK)), ("stopTimeLevel", str(steps)),
+                     ("L_x", repr(c.lx)), ("L_y", repr(c.ly)), ("L_z", repr(c.lz)), ("M_0", repr(c.m0)),
+                     ("Re", repr(c.re))):
+        text, n = re.subn(r"^%s = .*$" % key, "%s = %s" % (key, val), text, flags=re.M)
+        assert n == 1, key
+    text, n = re.subn(r"spheres = .*;", "spheres = ( (%r, %r, %r, %r) );" % (sp.cx, sp.cy, sp.cz, sp.r), text)
+    assert n == 1
+    text, n = re.subn(r"seed = .*;", "seed = %dL;" % c.seed, text)
+    assert n == 1
+    return text
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+@pytest.mark.parametrize("member", range(0, 64, 8))
+def test_oracle_matches_reference_ensemble_member(member):
+    """Members of the batched-ensemble workload (the bench's 64 flows), three RK4 steps each."""
+    import nsfsi
+    c = nsfsi.ensemble_configs(n=64, steps=3)[member]
+    compare(ensemble_member_text(c, 3), level=3)
+

@@ -122,3 +122,12 @@ def test_oracle_matches_reference_ensemble_member(member):
     c = nsfsi.ensemble_configs(n=64, steps=3)[member]
     compare(ensemble_member_text(c, 3), level=3)
 
+
+@pytest.mark.slow
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+def test_oracle_matches_reference_tgv256_one_step():
+    """The benchmark workload at full size (Taylor-Green 256^3, 16.8 M nodes): one RK4 step."""
+    import nsfsi
+    text = open(nsfsi.case_path("tgv256")).read()
+    compare(text, level=1)
+

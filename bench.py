@@ -283,7 +283,7 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def main():
+def arg_parser():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -298,7 +298,11 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint leg")
     ap.add_argument("--adjoint-only", action="store_true", help="run only the discrete-adjoint leg (profiling)")
     ap.add_argument("--adjoint-steps", type=int, default=200, help="RK4 steps of the adjoint leg")
-    args = ap.parse_args()
+    return ap
+
+
+def main():
+    args = arg_parser().parse_args()
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", "0"))

@@ -104,3 +104,17 @@ def test_reference_arm_line():
     assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["cores"] == 1
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_profile_commands_parse():
+    """Every bench.py command a profile summary names still parses with bench.py's options."""
+    import glob
+    import re
+    import shlex
+    cmds = set()
+    for path in glob.glob(os.path.join(ROOT, "profiles", "*.md")):
+        text = open(path).read().replace("\\\n", " ")
+        cmds.update(m.strip() for m in re.findall(r"python bench\.py([^`\n]*)", text))
+    assert cmds
+    for c in cmds:
+        bench.arg_parser().parse_args(shlex.split(c))

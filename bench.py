@@ -1,6 +1,7 @@
 """Benchmark of the B200 time-marching path: FP64 node-RK4-steps/s on the 256^3 Taylor-Green workload.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload tgv256|sphere48]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload tgv256|sphere48|spheres16|tgv128]
 
 A step is one RK4 step (Solver::marchTimeStep) over the whole grid. Each rank runs an independent replica
 (the single-grid path does not shard), so value = ranks x nodes x K / max-over-ranks device time. The

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -594,6 +595,18 @@ nsf_status nsf_sync(nsf_solver* s) {
     s->err = "Non-finite value found in the conserved variables";
     return NSF_ERR_NONFINITE;
   }
+  return NSF_OK;
+}
+
+nsf_status nsf_debug_wait_limit(nsf_solver* s, uint64_t polls, int32_t withhold_epilogue) {
+  if (!s || !s->initialized || s->hostOnly) return s ? NSF_ERR_STATE : NSF_ERR_ARG;
+  CK(cudaSetDevice(s->device));
+  CK(cudaStreamSynchronize(s->stream));
+  const long long lim = static_cast<long long>(polls);
+  const int wh = withhold_epilogue ? 1 : 0;
+  char* base = reinterpret_cast<char*>(s->dCtl);
+  CK(cudaMemcpy(base + offsetof(StepCtl, waitLimit), &lim, sizeof lim, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(base + offsetof(StepCtl, withhold), &wh, sizeof wh, cudaMemcpyHostToDevice));
   return NSF_OK;
 }
 

@@ -51,7 +51,10 @@ struct StepCtl {
   unsigned long long level;  // timeLevel
   int perm[5][3];         // per field: physical buffer of [cons, old, scratch]
   int nonFinite;          // sticky NaN/Inf flag (Mesh::checkFinity)
-  int rhoIcBuffer;        // unused placeholder for layout stability
+  // Test support for the bounded waits of the stage kernel (left at 0 in normal runs): withhold = 1 makes
+  // its producer issue no epilogue-ring load, so the column warps' waits run out; waitLimit = polls
+  // before a wait gives up (0: the kernel's default).
+  int withhold;
   // per-step decisions (prologue)
   int active;             // 0: step is a no-op (end_time reached)
   int filterNow;          // global density filter on this step
@@ -66,6 +69,7 @@ struct StepCtl {
   int rPhys[4];           // physical buffer of the density used for primitives
   int u0Phys[5];          // physical buffer of each U0 field
   int timeout;            // sticky: a bounded device wait gave up (the step's results are invalid)
+  long long waitLimit;    // see withhold
   double stageT[4];       // boundary-condition time of each stage
   double dtUsed;
   // stage-4 reductions

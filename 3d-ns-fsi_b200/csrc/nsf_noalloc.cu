@@ -90,7 +90,8 @@ __global__ void k_metrics_partial(MetricParams p, const double* __restrict__ old
   }
 }
 
-// Fixed-order final pass (deterministic): out[0..4] = change norms, out[5] = next dt.
+// Fixed-order final pass (deterministic): out[0..4] = change norms, out[5] = next dt (min of the convective
+// and viscous limits; the end_time clip needs t, which the caller holds, so the caller applies it).
 __global__ void k_metrics_final(const double* __restrict__ partial, long long nPartials, double dxdydz, double dx,
                                 double dy, double dz, double convLim, double viscLim, double* __restrict__ out) {
   __shared__ double red[kQ][256];

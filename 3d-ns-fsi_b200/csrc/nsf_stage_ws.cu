@@ -41,7 +41,7 @@ constexpr int NSTAGE = 96;                        // staging threads (warps 1-3)
 constexpr int NC = 5, NP = 5, NE = 3;             // conserved / primitive / epilogue ring depths
 constexpr int NPRIM = 6;                          // staged primitive fields: u, v, w, p, T, mu (kappa = pf mu)
 constexpr int MAP_CONS = 0, MAP_EPI = 15, MAP_ACC = 30, MAP_TYPE = 35, NMAPS = 36;
-constexpr long long WAIT_LIMIT = 1ll << 22;  // polls before a wait is declared failed
+constexpr long long WAIT_LIMIT = 1ll << 22;  // default polls before a wait is declared failed (StepCtl::waitLimit)
 // Register split (setmaxnreg): the launch gives every thread 168 registers (384 x 168 = 64,512); the
 // split must not exceed that total: 128 x 88 + 256 x 208 = 64,512.
 constexpr int REG_LAUNCH = 168, REG_LOW = 88, REG_HIGH = 208;
@@ -109,10 +109,11 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for the completion of the phase with the given parity; gives up early when another
-// thread has raised the CTA's abort flag.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, const volatile int* abortFlag) {
-  for (long long it = 0; it < ws::WAIT_LIMIT; ++it) {
+// Bounded wait for the completion of the phase with the given parity: at most `limit` polls, and it gives
+// up early when another thread has raised the CTA's abort flag.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, const volatile int* abortFlag,
+                                          long long limit) {
+  for (long long it = 0; it < limit; ++it) {
     if (mbar_try(b, parity)) return true;
     if (*abortFlag) return false;
   }
@@ -178,6 +179,8 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
   uint64_t* epiFull = primEmpty + NP;
   uint64_t* epiEmpty = epiFull + NE;
   volatile int* abortFlag = reinterpret_cast<volatile int*>(sm + OFF_FLAG);
+  int* withholdSm = reinterpret_cast<int*>(sm + OFF_FLAG + 4);
+  long long* limitSm = reinterpret_cast<long long*>(sm + OFF_FLAG + 8);
   double* red = reinterpret_cast<double*>(sm + OFF_RED);
   StepCtl& ctl0 = *reinterpret_cast<StepCtl*>(sm + OFF_CTL);  // single grid: a copy of its StepCtl
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -193,6 +196,12 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
   if (tid == 0) {
     if (!ENS) ctl0 = *G0.ctl;
     *abortFlag = 0;
+    {  // wait limit and test switch: the grid's control block (an ensemble: its first member's)
+      const StepCtl* c = ENS ? grids[0].ctl : G0.ctl;
+      const long long l = c->waitLimit;
+      *limitSm = l > 0 ? l : WAIT_LIMIT;
+      *withholdSm = c->withhold;
+    }
     for (int q = 0; q < NC; ++q) {
       mbar_init(&consFull[q], 1);
       mbar_init(&consEmpty[q], NCOL / 32);
@@ -209,6 +218,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
   }
   __syncthreads();
   if (!ENS && !ctl0.active) return;
+  const long long lim = *limitSm;
   DtAcc dta;
   double nsum[5] = {0, 0, 0, 0, 0};
   int bad = 0;
@@ -231,6 +241,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
         };
         int cIt = next_item(itBegin), cP = cIt < itEnd ? items[cIt].i0 - 1 : 0;  // next staged plane
         int eIt = cIt, eP = eIt < itEnd ? items[eIt].i0 : 0;                     // next computed plane
+        if (*withholdSm) eIt = itEnd;  // test switch: no epilogue load is ever issued
         uint32_t cq = 0, eq = 0;
         long long idle = 0;
         // descriptors of the item each cursor is in (reloaded only when the cursor moves to a new item)
@@ -295,7 +306,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           }
           if (progressed) {
             idle = 0;
-          } else if (++idle > WAIT_LIMIT) {
+          } else if (++idle > lim) {
             fail(grid_of(items[cIt < itEnd ? cIt : eIt]));
             break;
           }
@@ -306,12 +317,12 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
         for (uint32_t sl = 0; sl < NC; ++sl)
           if (cq > sl) {
             const uint32_t last = cq - 1 - ((cq - 1 - sl) % NC);
-            if (!mbar_wait(&consFull[sl], (last / NC) & 1, &never)) atomicExch(&Gf.ctl->timeout, 1);
+            if (!mbar_wait(&consFull[sl], (last / NC) & 1, &never, lim)) atomicExch(&Gf.ctl->timeout, 1);
           }
         for (uint32_t se = 0; se < NE; ++se)
           if (eq > se) {
             const uint32_t last = eq - 1 - ((eq - 1 - se) % NE);
-            if (!mbar_wait(&epiFull[se], (last / NE) & 1, &never)) atomicExch(&Gf.ctl->timeout, 1);
+            if (!mbar_wait(&epiFull[se], (last / NE) & 1, &never, lim)) atomicExch(&Gf.ctl->timeout, 1);
           }
       }
     } else {
@@ -328,8 +339,8 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
         const long long sIs = G.sI, sJs = G.sJ;
         for (int p = w.i0 - 1; p <= w.i1 + 1; ++p, ++q) {
           const uint32_t sl = q % NC, ps = q % NP;
-          if (q >= NP) ok = mbar_wait(&primEmpty[ps], ((q / NP) - 1) & 1, abortFlag);
-          ok = ok && mbar_wait(&consFull[sl], (q / NC) & 1, abortFlag);
+          if (q >= NP) ok = mbar_wait(&primEmpty[ps], ((q / NP) - 1) & 1, abortFlag, lim);
+          ok = ok && mbar_wait(&consFull[sl], (q / NC) & 1, abortFlag, lim);
           if (!ok) {
             fail(G);
             break;
@@ -425,7 +436,8 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
       for (int a = 0; a <= L + 1; ++a) {
         const uint32_t qx = q + a;
         const int pX = qx % NP, cX = qx % NC;
-        ok = mbar_wait(&primFull[pX], (qx / NP) & 1, abortFlag) && mbar_wait(&consFull[cX], (qx / NC) & 1, abortFlag);
+        ok = mbar_wait(&primFull[pX], (qx / NP) & 1, abortFlag, lim) &&
+             mbar_wait(&consFull[cX], (qx / NC) & 1, abortFlag, lim);
         if (!ok) {
           fail(G);
           break;
@@ -452,7 +464,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
         if (a >= 2) {
           const int pR = (qx - 1) % NP, pW = (qx - 2) % NP, cR = (qx - 1) % NC;
           const uint32_t se = e % NE;
-          ok = mbar_wait(&epiFull[se], (e / NE) & 1, abortFlag);
+          ok = mbar_wait(&epiFull[se], (e / NE) & 1, abortFlag, lim);
           if (!ok) {
             fail(G);
             break;

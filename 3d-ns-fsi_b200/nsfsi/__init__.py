@@ -108,6 +108,7 @@ def lib():
         "nsf_adj_get_dt": (i32, [vp, dp, ctypes.POINTER(u64)]),
         "nsf_adj_profile_step": (i32, [vp, u64, dp]),
         "nsf_math_selftest": (i32, [i32, u64, dp, dp]),
+        "nsf_debug_wait_limit": (i32, [vp, u64, i32]),
         "nsf_last_error": (ctypes.c_char_p, [vp]),
         "nsf_destroy": (None, [vp]),
     }
@@ -219,6 +220,11 @@ class Solver:
         out = np.empty((len(fields), self.N))
         self._check(lib().nsf_download(self.h, mask, _dp(out)))
         return out
+
+    def debug_wait_limit(self, polls=0, withhold_epilogue=False):
+        """Test support: the stage kernel's wait limit in polls (0: default) and the switch that withholds
+        its epilogue loads (nsf_debug_wait_limit)."""
+        self._check(lib().nsf_debug_wait_limit(self.h, polls, 1 if withhold_epilogue else 0))
 
     def upload_conserved(self, u5):
         a = np.ascontiguousarray(u5, dtype=np.float64)

@@ -168,7 +168,9 @@ nsf_status nsf_launches_per_step(nsf_solver* s, uint64_t* launches);
  * (then every node off the mesh faces is interior); d_out: 6 doubles written on `stream` (a
  * cudaStream_t, NULL = default stream): the five change norms sqrt(dx*dy*dz*sum (old-new)^2) over
  * interior nodes, then the next dt from the primitive values of d_new at every node (what nsf_march
- * records when the case has no immersed body). Scratch is a fixed 8 MiB device array inside the library,
+ * records when the case has no immersed body and stops on a step count). out[5] is the dt before the
+ * end_time clip of Solver::updateTimeStepSize (Solver.cpp:85-87): a caller whose run stops at t_end
+ * applies it itself, dt = t_end - t wherever t + out[5] > t_end. Scratch is a fixed 8 MiB device array inside the library,
  * so at most 29,826,048 nodes (larger grids: NSF_ERR_ARG). The first call on a device resolves that
  * array's device address (cudaGetSymbolAddress); make it before any stream capture. Calls that overlap
  * on the GPU share the array and race: serialise them. */
@@ -236,6 +238,13 @@ nsf_status nsf_adj_profile_step(nsf_solver* s, uint64_t step, double* ms);
  * (Newton-Raphson refinement of the hardware approximations): for n positive inputs x, out[4 i .. 4 i + 3]
  * = the refined reciprocal, the IEEE 1/x, the refined square root, the IEEE sqrt(x). */
 nsf_status nsf_math_selftest(int32_t device, uint64_t n, const double* x, double* out);
+
+/* Test support for the bounded waits (no counterpart in the reference): every wait of the stage
+ * kernel gives up after `polls` polls (0 restores the default of 2^22), and withhold_epilogue = 1 makes
+ * the kernel's producer issue none of its epilogue loads, so the waits for them run out. A step that
+ * ran with the switch on is invalid: nsf_sync then returns NSF_ERR_TIMEOUT and the handle should be
+ * destroyed. Synchronises. */
+nsf_status nsf_debug_wait_limit(nsf_solver* s, uint64_t polls, int32_t withhold_epilogue);
 
 /* Text of the last error on this handle (static storage owned by the handle). */
 const char* nsf_last_error(nsf_solver* s);

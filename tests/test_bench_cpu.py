@@ -104,6 +104,40 @@ def test_reference_arm_line():
     assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["cores"] == 1
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+    assert line["steps"] == 1 and line["warmup"] == 3
+    assert line["config"] == bench.arm_config("sphere48", [48, 48, 48], 1)
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+def test_reference_arm_loads_nothing_of_the_product():
+    """The reference arm, run in a fresh process with the product's Python package made unimportable, maps
+    no product library into the process."""
+    script = (
+        "import json, sys\n"
+        "sys.modules['nsfsi'] = None\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'sphere48', '--steps', '2', '--warmup', '3']\n"
+        "import bench\n"
+        "bench.main()\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'libnsfsi_mapped': 'libnsfsi' in maps, 'liboracle_mapped': 'liboracle' in maps}))\n")
+    out = subprocess.run([sys.executable, "-c", script], cwd=ROOT, capture_output=True, text=True, timeout=300,
+                         check=True).stdout.strip().splitlines()
+    line, maps = json.loads(out[-2]), json.loads(out[-1])
+    assert line["impl"] == "reference" and line["steps"] == 2 and line["warmup"] == 3
+    assert maps == {"libnsfsi_mapped": False, "liboracle_mapped": False}
+
+
+def test_reference_arm_budget_bounds_the_timed_steps():
+    """A requested run longer than the arm's time budget is cut to the steps that fit, and says so."""
+    nodes = 256 ** 3
+    est = nodes / bench.REF_RATE_ESTIMATE
+    assert (5 + 20) * est <= bench.REF_ARM_BUDGET_S  # the round-end command (20 steps, 5 warm-up) runs whole
+    assert (5 + 200) * est > bench.REF_ARM_BUDGET_S
+
+
+def test_case_grid_reads_the_case_text():
+    assert bench.case_grid(bench.case_file("tgv256")) == [256, 256, 256]
+    assert bench.case_grid(bench.case_file("spheres16")) == [256, 128, 128]
 
 
 def test_profile_commands_parse():

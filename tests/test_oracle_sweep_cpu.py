@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from oracle import pyoracle as po
-from sweep_cases import N_CASES, STEPS, random_case, shipped_case, wide_case
+from sweep_cases import N_CASES, STEPS, ensemble_member_text, random_case, shipped_case, wide_case
 
 
 def compare(text, level=STEPS):
@@ -93,25 +93,6 @@ def test_oracle_matches_reference_shipped_case(seed):
     dt0 = o.dt
     o.close()
     compare(shipped_case(seed, dt0), level="final")
-
-
-def ensemble_member_text(c, steps):
-    """The case file of one member of the batched-ensemble workload (nsfsi.ensemble_configs, built there from
-    the 48^3 sphere case) with `steps` RK4 steps."""
-    import re
-    import nsfsi
-    text = open(nsfsi.case_path("sphere48")).read()
-    sp = c.spheres[0]
-    for key, val in (("NI", str(c.NI)), ("NJ", str(c.NJ)), ("NK", str(c.NK)), ("stopTimeLevel", str(steps)),
-                     ("L_x", repr(c.lx)), ("L_y", repr(c.ly)), ("L_z", repr(c.lz)), ("M_0", repr(c.m0)),
-                     ("Re", repr(c.re))):
-        text, n = re.subn(r"^%s = .*$" % key, "%s = %s" % (key, val), text, flags=re.M)
-        assert n == 1, key
-    text, n = re.subn(r"spheres = .*;", "spheres = ( (%r, %r, %r, %r) );" % (sp.cx, sp.cy, sp.cz, sp.r), text)
-    assert n == 1
-    text, n = re.subn(r"seed = .*;", "seed = %dL;" % c.seed, text)
-    assert n == 1
-    return text
 
 
 @pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")

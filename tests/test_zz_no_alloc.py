@@ -45,6 +45,39 @@ def test_noalloc_metrics_match_the_solver_on_two_consecutive_steps():
 
 
 @pytest.mark.gpu
+def test_noalloc_dt_with_the_callers_end_time_clip():
+    """An end_time run: the entry point returns the unclipped dt, and the clip the header asks callers to
+    apply (dt = t_end - t where t + dt > t_end, Solver.cpp:85-87) gives what the solver records."""
+    import torch
+
+    base = nsfsi.config_load("tests/golden/cases/tgv_small.cfg")
+    with nsfsi.Solver(base) as s:
+        s.march(1)
+        t1, _, dt1 = s.time()
+    cfg = nsfsi.config_load("tests/golden/cases/tgv_small.cfg")
+    cfg.stop_criterion = 1  # end_time
+    cfg.t_end = t1 + 0.5 * dt1  # the second step is shortened
+    L = nsfsi.lib()
+    with nsfsi.Solver(cfg) as s:
+        u_old = s.download(range(5))
+        s.march(1)
+        s.sync()
+        u_new = s.download(range(5))
+        t, level, dt_next = s.time()
+        assert level == 1 and t == t1 and dt_next == cfg.t_end - t
+        d_old, d_new = torch.tensor(u_old, device="cuda"), torch.tensor(u_new, device="cuda")
+        d_out = torch.full((6,), -1.0, dtype=torch.float64, device="cuda")
+        assert L.nsf_step_metrics_noalloc(ctypes.byref(cfg), ctypes.c_void_p(d_old.data_ptr()),
+                                          ctypes.c_void_p(d_new.data_ptr()), None, ctypes.c_void_p(d_out.data_ptr()),
+                                          None) == 0
+        torch.cuda.synchronize()
+        dt = float(d_out[5].item())
+        assert abs(dt / dt1 - 1) <= DT_TOL  # unclipped: the full limit of the new state
+        clipped = cfg.t_end - t if t + dt > cfg.t_end else dt
+        assert clipped == dt_next
+
+
+@pytest.mark.gpu
 def test_noalloc_rejects_grids_beyond_its_scratch():
     import torch
 

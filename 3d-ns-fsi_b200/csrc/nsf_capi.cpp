@@ -759,33 +759,52 @@ nsf_status nsf_march_timed(nsf_solver* s, uint64_t nsteps, double* elapsed_ms) {
   return NSF_OK;
 }
 
+// Steps per replay of the profiling graph: the graph holds this many RK4 steps back to back, as
+// consecutive replays of the step graph run them, with event nodes around the stage kernels.
+constexpr int kProfileSteps = 10;
+
+static nsf_status build_profile_graph(nsf_solver* s) {
+  s->profEv.assign(2 + 8 * kProfileSteps, nullptr);
+  for (auto& e : s->profEv) CK(cudaEventCreate(&e));
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaEventRecordWithFlags(s->profEv[0], s->stream, cudaEventRecordExternal);
+  for (int q = 0; q < kProfileSteps && e == cudaSuccess; ++q) {
+    enqueue_step_profiled(s->dGrid, s->hGrid, s->plan, s->stream, s->profEv.data() + 2 + 8 * q, true);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->profEv[1], s->stream, cudaEventRecordExternal);
+  const cudaError_t e2 = cudaStreamEndCapture(s->stream, &s->profGraph);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->profExec, s->profGraph, 0);
+  if (e != cudaSuccess) return cuda_fail(s, e, "capture of the profiling graph");
+  return NSF_OK;
+}
+
 nsf_status nsf_profile_steps(nsf_solver* s, uint64_t nsteps, double* stage_ms, double* step_ms) {
   if (!s || !stage_ms || !step_ms) return NSF_ERR_ARG;
   if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
   CK(cudaSetDevice(s->device));
-  std::vector<cudaEvent_t> ev(2 * 4 * nsteps + 2);
-  for (auto& e : ev) CK(cudaEventCreate(&e));
-  CK(cudaEventRecord(ev[0], s->stream));
-  for (uint64_t q = 0; q < nsteps; ++q) {
-    cudaEvent_t* se = ev.data() + 2 + 8 * q;
-    enqueue_step_profiled(s->dGrid, s->hGrid, s->plan, s->stream, se);
+  if (!s->profExec) {
+    const nsf_status st = build_profile_graph(s);
+    if (st != NSF_OK) return st;
   }
-  CK(cudaGetLastError());
-  CK(cudaEventRecord(ev[1], s->stream));
-  CK(cudaEventSynchronize(ev[1]));
-  float ms = 0;
-  CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-  *step_ms = ms / double(nsteps ? nsteps : 1);
-  for (int st = 0; st < 4; ++st) {
-    double tot = 0;
-    for (uint64_t q = 0; q < nsteps; ++q) {
-      float m = 0;
-      CK(cudaEventElapsedTime(&m, ev[2 + 8 * q + 2 * st], ev[2 + 8 * q + 2 * st + 1]));
-      tot += m;
-    }
-    stage_ms[st] = tot / double(nsteps ? nsteps : 1);
+  const uint64_t reps = (nsteps + kProfileSteps - 1) / kProfileSteps;
+  double tot[4] = {0, 0, 0, 0}, whole = 0;
+  for (uint64_t r = 0; r < reps; ++r) {
+    CK(cudaGraphLaunch(s->profExec, s->stream));
+    CK(cudaEventSynchronize(s->profEv[1]));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, s->profEv[0], s->profEv[1]));
+    whole += ms;
+    for (int q = 0; q < kProfileSteps; ++q)
+      for (int st = 0; st < 4; ++st) {
+        CK(cudaEventElapsedTime(&ms, s->profEv[2 + 8 * q + 2 * st], s->profEv[2 + 8 * q + 2 * st + 1]));
+        tot[st] += ms;
+      }
   }
-  for (auto& e : ev) cudaEventDestroy(e);
+  const double n = double(reps ? reps * kProfileSteps : 1);
+  *step_ms = whole / n;
+  for (int st = 0; st < 4; ++st) stage_ms[st] = tot[st] / n;
   return NSF_OK;
 }
 
@@ -806,6 +825,10 @@ void nsf_destroy(nsf_solver* s) {
   }
   if (s->graphExec) cudaGraphExecDestroy(s->graphExec);
   if (s->graph) cudaGraphDestroy(s->graph);
+  if (s->profExec) cudaGraphExecDestroy(s->profExec);
+  if (s->profGraph) cudaGraphDestroy(s->profGraph);
+  for (cudaEvent_t e : s->profEv)
+    if (e) cudaEventDestroy(e);
   nsf_adjoint_free(s);
   for (void* p : s->allocs) cudaFree(p);
   if (s->stream) cudaStreamDestroy(s->stream);

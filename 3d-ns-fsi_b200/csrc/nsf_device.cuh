@@ -184,9 +184,11 @@ void launch_stage_ensemble(const Grid* dGrids, const LaunchPlan& L, int s, void*
 // dg: the grid in device memory (read by the small kernels); hg: the same grid on the host (passed by
 // value to the stage kernel, whose coefficients then come from the constant bank).
 int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream);
-// Same sequence, launched eagerly, with events recorded around each of the four stage kernels
-// (events[2*s], events[2*s+1]); used for per-kernel timing.
-int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events);
+// Same sequence with events recorded around each of the four stage kernels (events[2*s], events[2*s+1]);
+// used for per-kernel timing. inGraph: the stream is being captured, and the events become event-record
+// nodes of the graph (so the kernels are timed inside graph replays, as the solver runs them).
+int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events,
+                          bool inGraph = false);
 // Callbacks of a step launched kernel by kernel (enqueue_step_hooked): after the prologue, before each
 // stage kernel, and before each stage's edge boundary conditions (after the solid-node copy).
 struct StepHook {

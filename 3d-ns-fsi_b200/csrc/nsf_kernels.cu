@@ -601,8 +601,16 @@ void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vecto
 // counts in L being the maxima over the members; the edge kernels run the listed blocks of every member.
 // lastStage: NULL, or the plan of a partial stage 4 (single grid): stage 4 then runs the stage kernel over
 // that plan's items only and the step ends there (no stage-4 boundary conditions, no finalize).
+// ev: NULL, or 8 events recorded around the four stage kernels; evExternal: record them as event nodes of
+// a graph being captured (cudaEventRecordExternal) rather than as plain stream events.
 static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan& L, cudaStream_t st, cudaEvent_t* ev,
-                        StepHook* hook = nullptr, const LaunchPlan* lastStage = nullptr) {
+                        StepHook* hook = nullptr, const LaunchPlan* lastStage = nullptr, bool evExternal = false) {
+  auto record = [&](cudaEvent_t e) {
+    if (evExternal)
+      cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+    else
+      cudaEventRecord(e, st);
+  };
   int launches = 0;
   const unsigned M = unsigned(members);
   k_prologue<<<M, 32, 0, st>>>(dg);
@@ -611,7 +619,7 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
   k_density_filter<<<dim3(L.gfBlocks, M), 256, 0, st>>>(dg);
   ++launches;
   for (int s = 0; s < 4; ++s) {
-    if (ev) cudaEventRecord(ev[2 * s], st);
+    if (ev) record(ev[2 * s]);
     if (hook) hook->before_stage(s);
     if (s == 3 && lastStage && hg) {
       if (lastStage->nItems > 0) {
@@ -625,7 +633,7 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
       launch_stage(*hg, L, s, st);
     else
       launch_stage_ensemble(dg, L, s, st);
-    if (ev) cudaEventRecord(ev[2 * s + 1], st);
+    if (ev) record(ev[2 * s + 1]);
     ++launches;
     if (L.hasSolid) {
       k_solid_copy<<<dim3(L.solidBlocks, M), 256, 0, st>>>(dg, s);
@@ -664,8 +672,9 @@ int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* 
   return enqueue_impl(dGrids, nullptr, members, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events));
 }
 
-int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events) {
-  return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events));
+int enqueue_step_profiled(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream, void* events, bool inGraph) {
+  return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), static_cast<cudaEvent_t*>(events), nullptr,
+                      nullptr, inGraph);
 }
 
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,

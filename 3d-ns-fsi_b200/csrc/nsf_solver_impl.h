@@ -27,6 +27,11 @@ struct nsf_solver {
   cudaGraphExec_t graphExec = nullptr;
   cudaGraph_t graph = nullptr;
   int launchesPerStep = 0;
+  // instrumentation (nsf_profile_steps): a graph of kProfileSteps steps with event nodes around the stage
+  // kernels, built on first use
+  cudaGraphExec_t profExec = nullptr;
+  cudaGraph_t profGraph = nullptr;
+  std::vector<cudaEvent_t> profEv;
   int nSM = 0;
   // solid inactive nodes with stored primitive values (downloads)
   long long* dDlNode = nullptr;

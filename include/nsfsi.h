@@ -153,8 +153,9 @@ nsf_status nsf_get_history(nsf_solver* s, uint64_t first, uint64_t count, double
 
 /* Instrumentation. nsf_march_timed: nsf_march with CUDA events recorded on the handle's stream around
  * the queued steps; waits and returns the elapsed device time. nsf_profile_steps: runs nsteps steps
- * launched one kernel at a time (not as a graph) with events around each of the four stage kernels;
- * returns their mean durations (stage_ms[4]) and the mean step time. Both advance the solution. */
+ * (rounded up to a multiple of 10) as replays of a graph of 10 consecutive steps that also holds event
+ * nodes around each of the four stage kernels; returns their mean durations (stage_ms[4]) and the mean
+ * step time, both measured inside those replays. Both advance the solution. */
 nsf_status nsf_march_timed(nsf_solver* s, uint64_t nsteps, double* elapsed_ms);
 nsf_status nsf_profile_steps(nsf_solver* s, uint64_t nsteps, double* stage_ms, double* step_ms);
 /* Kernel launches issued per RK4 step (for instrumentation). */

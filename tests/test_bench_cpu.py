@@ -79,7 +79,11 @@ def test_main_arm_line_keeps_the_contract(monkeypatch, capsys):
     for key in ("bound", "achieved", "peak", "unit", "frac", "traffic"):
         assert key in r, key
     assert r["bound"] == "hbm" and r["unit"] == "GB/s"
-    assert r["achieved"] == pytest.approx(680 * nodes / (sum(STAGE_MS) / 1e3) / 1e9)
+    share = sum(STAGE_MS) / (STEP_MS + 0.05)
+    assert r["stage_share"] == pytest.approx(share, abs=1e-4)
+    assert r["achieved"] == pytest.approx(680 * nodes / (share * STEP_MS / 1e3) / 1e9)
+    assert r["stage_ms_per_step"] <= line["ms_per_step"]
+    assert line["repeats"] == 10 and len(line["ms_per_step_repeats"]) == 10
     assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
     assert r["step_frac"] == pytest.approx(line["value"] / (r["peak"] * 1e9 / 680))
     assert line["e2e"] is None  # --no-e2e

@@ -109,11 +109,14 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for the completion of the phase with the given parity: at most `limit` polls, and it gives
-// up early when another thread has raised the CTA's abort flag.
+// Bounded wait for the completion of the phase with the given parity: at most *limit polls (the limit is
+// read from shared memory only once the first poll has failed, so it holds no register on the fast path),
+// and it gives up early when another thread has raised the CTA's abort flag.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, const volatile int* abortFlag,
-                                          long long limit) {
-  for (long long it = 0; it < limit; ++it) {
+                                          const long long* limit) {
+  if (mbar_try(b, parity)) return true;
+  const long long lim = *limit;
+  for (long long it = 1; it < lim; ++it) {
     if (mbar_try(b, parity)) return true;
     if (*abortFlag) return false;
   }
@@ -218,7 +221,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
   }
   __syncthreads();
   if (!ENS && !ctl0.active) return;
-  const long long lim = *limitSm;
+  const long long* const lim = limitSm;
   DtAcc dta;
   double nsum[5] = {0, 0, 0, 0, 0};
   int bad = 0;
@@ -306,7 +309,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           }
           if (progressed) {
             idle = 0;
-          } else if (++idle > lim) {
+          } else if (++idle > *lim) {
             fail(grid_of(items[cIt < itEnd ? cIt : eIt]));
             break;
           }

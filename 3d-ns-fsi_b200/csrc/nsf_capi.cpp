@@ -472,6 +472,20 @@ nsf_status build_device(nsf_solver* s) {
   L.hasGhostWork = ghostWork > 0;
   L.ghostBlocks = std::max(1, std::min(4 * s->nSM, (ghostWork + 255) / 256));
   L.gfBlocks = 4 * s->nSM;
+  {  // fused boundary kernel: enough blocks for the busiest phase, within what can be resident at once
+    const int cap = bc_capacity(s->nSM);
+    const long long work = bc_member_work(G, L.nEdgeBlocks);
+    L.bcBlocks = cap > 0 ? int(std::max<long long>(1, std::min<long long>(cap, (work + 255) / 256))) : 0;
+    if (L.bcBlocks > 0) {
+      L.filterBlocks = std::max(L.filterBlocks, L.bcBlocks);  // one norm slot per block of the fused kernel
+      for (int a = 0; a < 3; ++a) {
+        const std::vector<int> start = {0, L.nEdgeBlocks[a]};
+        if ((st = upload(s, &L.edgeStart[a], start)) != NSF_OK) return st;
+      }
+      const std::vector<unsigned> zero(2, 0u);
+      if ((st = upload(s, &L.bcSync, zero)) != NSF_OK) return st;
+    }
+  }
   L.nSlots = L.stageBlocks + (L.hasFilter ? L.filterBlocks : 0);
   double* dNorm;
   if ((st = dalloc(s, &dNorm, 5 * size_t(L.nSlots))) != NSF_OK) return st;

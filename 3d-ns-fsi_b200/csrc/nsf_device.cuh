@@ -150,6 +150,15 @@ struct EdgeBlock {
 // whose source node is not an unfiltered interior fluid node).
 void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vector<EdgeBlock>& out);
 
+// Arguments of one launch of the fused boundary kernel (k_bc, see nsf_kernels.cu).
+struct BcParams {
+  const EdgeBlock* edge[3];  // per axis: the edge blocks of every member, member-major
+  const int* edgeStart[3];   // per axis: members + 1 offsets into edge[axis]
+  unsigned* sync;            // grid barrier state: arrival count, generation
+  int hasEdge[3];
+  int hasSolid, hasFilter, hasGhost;
+};
+
 struct LaunchPlan {
   int nSM;
   int tile;  // StageTile
@@ -160,6 +169,12 @@ struct LaunchPlan {
   EdgeBlock* edgeBlocks[3];  // device, per axis
   int nEdgeBlocks[3];
   int filterBlocks, ghostBlocks, solidBlocks, gfBlocks;
+  // Fused boundary kernel: per stage one cooperative launch of bcBlocks x members blocks that runs the
+  // solid-node copy, the x, y and z edge conditions, the near-body filter and the ghost pass in that order
+  // with grid barriers between them (and, on stage 4, the end-of-step finalize). 0: separate launches.
+  int bcBlocks;
+  int* edgeStart[3];  // device, members + 1 offsets into edgeBlocks[axis]
+  unsigned* bcSync;   // device, 2 words, zero at creation
   int nSlots;
   bool hasBodies;
   bool hasFilter, hasGhostWork, hasSolid;
@@ -206,6 +221,12 @@ int math_selftest(long long n, const double* hostIn, double* hostOut);
 // One RK4 step of every member of an ensemble (dGrids: device array of `members` grids; L: the ensemble's
 // combined plan). events: NULL, or 8 events recorded around the four stage kernels.
 int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* stream, void* events);
+// Blocks of 256 threads of the fused boundary kernel that can be resident on the device at once (its
+// cooperative launches must not exceed this), or 0 if unknown.
+int bc_capacity(int nSM);
+// Threads one member needs in the busiest phase of the fused boundary kernel (ghost pass with stage 4's
+// inactive nodes; edge blocks count 64 threads each).
+long long bc_member_work(const Grid& G, const int nEdgeBlocks[3]);
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,
                           double dx, double dy, double dz, double* w, void* stream);
 void launch_download_prims(const Grid* dg, long long N, double* out, const long long* inodes, const double* ip7,

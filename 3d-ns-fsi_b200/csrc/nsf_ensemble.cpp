@@ -232,9 +232,14 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
   CKE(cudaMemcpy(L.ctaStart, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
   // small kernels: block counts = maxima over the members
   L.gfBlocks = std::max(8, 4 * e->nSM / M);  // grid-stride over each member's nodes
+  std::vector<int> edgeStart[3];
   for (int a = 0; a < 3; ++a) {  // edge blocks: every member's own, member-major
     std::vector<EdgeBlock> eb;
-    for (int g = 0; g < M; ++g) edge_blocks(e->members[g]->hGrid, e->members[g]->typeFlags.data(), g, a, eb);
+    edgeStart[a].push_back(0);
+    for (int g = 0; g < M; ++g) {
+      edge_blocks(e->members[g]->hGrid, e->members[g]->typeFlags.data(), g, a, eb);
+      edgeStart[a].push_back(int(eb.size()));
+    }
     L.nEdgeBlocks[a] = int(eb.size());
     L.edgeBlocks[a] = nullptr;
     if (eb.empty()) continue;
@@ -250,8 +255,27 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
     L.hasGhostWork |= P.hasGhostWork;
     L.hasSolid |= P.hasSolid;
   }
+  {  // fused boundary kernel: bcBlocks blocks per member, all members' blocks resident at once
+    const int cap = bc_capacity(e->nSM) / M;
+    long long work = 1;
+    for (int g = 0; g < M; ++g) {
+      int nEb[3];
+      for (int a = 0; a < 3; ++a) nEb[a] = edgeStart[a][g + 1] - edgeStart[a][g];
+      work = std::max(work, bc_member_work(e->members[g]->hGrid, nEb));
+    }
+    L.bcBlocks = cap > 0 ? int(std::min<long long>(cap, (work + 255) / 256)) : 0;
+    if (L.bcBlocks > 0) {
+      L.filterBlocks = std::max(L.filterBlocks, L.bcBlocks);
+      for (int a = 0; a < 3; ++a) {
+        if ((st = ens_alloc(e, &L.edgeStart[a], edgeStart[a].size())) != NSF_OK) return st;
+        CKE(cudaMemcpy(L.edgeStart[a], edgeStart[a].data(), edgeStart[a].size() * sizeof(int), cudaMemcpyHostToDevice));
+      }
+      if ((st = ens_alloc(e, &L.bcSync, 2)) != NSF_OK) return st;
+      CKE(cudaMemset(L.bcSync, 0, 2 * sizeof(unsigned)));
+    }
+  }
   // member grids: the stage kernel adds its norm partials into slot 0 of each member, the near-body
-  // filter's blocks use slots 1 .. filterBlocks
+  // filter's blocks (or the fused boundary kernel's) use slots 1 .. filterBlocks
   e->hGrids.resize(M);
   for (int g = 0; g < M; ++g) {
     Grid G = e->members[g]->hGrid;

@@ -13,6 +13,7 @@
 //
 // Stage 4 also carries the dt maxima, the change norms and the NaN check as block reductions, so no
 // kernel re-reads the fields for them.
+#include <algorithm>
 #include <cfloat>
 #include <cstdio>
 #include <cuda_runtime.h>
@@ -135,18 +136,23 @@ __global__ void k_density_filter(const Grid* __restrict__ grids) {
 
 // ----------------------------------------------------------------------------------------------
 // Solid-node values the reference's stage buffer still holds from earlier writes (see nsf_device.cuh).
+// One solid node q of a grid; the device functions here are shared by the separate kernels and the fused
+// boundary kernel (k_bc), which reads fields written earlier in the same launch: those reads bypass L1.
+__device__ __forceinline__ void solid_copy_item(const Grid& G, const StepCtl* c, int s, int mask, int q) {
+  const long long n = G.snode[q];
+  if (mask & 1) c->O[s][0][n] = __ldcg(c->R[s] + n);
+  for (int f = 1; f < 5; ++f)
+    if (mask & (1 << f)) c->O[s][f][n] = __ldcg(c->I[s][f] + n);
+}
+
 __global__ void k_solid_copy(const Grid* __restrict__ grids, int s) {
   const Grid* g = grids + blockIdx.y;
   const StepCtl* c = g->ctl;
   if (!c->active) return;
   const int mask = c->copyMask[s];
   if (!mask) return;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < g->nSolid; q += gridDim.x * blockDim.x) {
-    const long long n = g->snode[q];
-    if (mask & 1) c->O[s][0][n] = c->R[s][n];
-    for (int f = 1; f < 5; ++f)
-      if (mask & (1 << f)) c->O[s][f][n] = c->I[s][f][n];
-  }
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < g->nSolid; q += gridDim.x * blockDim.x)
+    solid_copy_item(*g, c, s, mask, q);
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -154,23 +160,19 @@ __global__ void k_solid_copy(const Grid* __restrict__ grids, int s) {
 // nodes). Launched for x, then y, then z: the reference's application order outlet/inlet (x), y-max,
 // y-min, z-max, z-min (Mesh.cpp:155-167 after the reversal at Mesh.cpp:70). Each block comes from the
 // launch plan's list (member, face, first in-plane coordinates, mask of the nodes it works on).
-__global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __restrict__ blocks, int s, int axis) {
-  __shared__ double red[4 * 32];
-  const EdgeBlock eb = blocks[blockIdx.x];  // every listed block holds nodes of its face
-  const Grid& G = grids[eb.g];
-  StepCtl* c = G.ctl;
-  if (!c->active) return;
+// edge_node: one node (thread tx, ty of an edge block) of a mesh-edge boundary condition; adds the stage-4
+// dt terms and the NaN check of edge and ghost-typed nodes.
+__device__ __forceinline__ void edge_node(const Grid& G, StepCtl* c, const EdgeBlock& eb, int tx, int ty, int s,
+                                          int axis, DtAcc& dta, int& bad) {
   const Consts& C = G.C;
   const int e = eb.e;
-  DtAcc dta;
-  int bad = 0;
   {
     const int* b = G.eBox[e];
     // in-plane coordinates: (a, bb) = the two axes other than `axis`, in (i, j, k) order
     const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
-    const int a = eb.a0 + threadIdx.y;
-    const int bb = eb.b0 + threadIdx.x;
-    if (a <= b[2 * ax1 + 1] && bb <= b[2 * ax2 + 1] && ((eb.mask >> (threadIdx.y * 32 + threadIdx.x)) & 1)) {
+    const int a = eb.a0 + ty;
+    const int bb = eb.b0 + tx;
+    if (a <= b[2 * ax1 + 1] && bb <= b[2 * ax2 + 1] && ((eb.mask >> (ty * 32 + tx)) & 1)) {
       int ijk[3];
       ijk[axis] = b[2 * axis];
       ijk[ax1] = a;
@@ -179,6 +181,7 @@ __global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __res
       const long long n = ijk[0] * G.sI + ijk[1] * G.sJ + ijk[2];
       const int side = G.eSide[e], bc = G.eBc[e];
       double** O = c->O[s];
+      auto ld = [&](int f, long long m) { return __ldcg(O[f] + m); };
       const long long a1 = side == 0 ? n + st : n - st, a2 = side == 0 ? n + 2 * st : n - 2 * st;  // Boundary.cpp:74-108
       double cv[5];
       double u = 0, v = 0, w = 0, p = 0, T = 0;
@@ -186,7 +189,7 @@ __global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __res
       if (bc == NSF_BC_INLET) {  // Boundary.cpp:250-296 with filterInletDensity :142-245
         // extrapolated density of this node and of its in-plane neighbours inside the owned box
         const long long s1 = ax1 == 0 ? G.sI : G.sJ, s2 = ax2 == 1 ? G.sJ : 1;
-        auto ext = [&](long long m) { return 2 * O[0][side == 0 ? m + st : m - st] - O[0][side == 0 ? m + 2 * st : m - 2 * st]; };
+        auto ext = [&](long long m) { return 2 * ld(0, side == 0 ? m + st : m - st) - ld(0, side == 0 ? m + 2 * st : m - 2 * st); };
         double f = 0;
         unsigned nn = 0;
         if (a < b[2 * ax1 + 1]) { f += ext(n + s1); ++nn; }
@@ -207,10 +210,10 @@ __global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __res
         cons_of(C, u, v, w, p, T, cv);
         primKnown = true;
       } else if (bc == NSF_BC_OUTLET) {  // Boundary.cpp:304-336
-        const double rho = 2 * O[0][a1] - O[0][a2];
-        const double ru = 2 * O[1][a1] - O[1][a2];
-        const double rv = 2 * O[2][a1] - O[2][a2];
-        const double rw = 2 * O[3][a1] - O[3][a2];
+        const double rho = 2 * ld(0, a1) - ld(0, a2);
+        const double ru = 2 * ld(1, a1) - ld(1, a2);
+        const double rv = 2 * ld(2, a1) - ld(2, a2);
+        const double rw = 2 * ld(3, a1) - ld(3, a2);
         p = 0;
         u = ru / (1 + rho);
         v = rv / (1 + rho);
@@ -227,9 +230,9 @@ __global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __res
         const int nAx = axis == 0 ? G.NI : axis == 1 ? G.NJ : G.NK;
         src[axis] = side == 0 ? nAx - 2 : 1;
         const long long m = src[0] * G.sI + src[1] * G.sJ + src[2];
-        for (int f = 0; f < 5; ++f) cv[f] = O[f][m];
+        for (int f = 0; f < 5; ++f) cv[f] = ld(f, m);
       } else {  // symmetry, Boundary.cpp:377-417: mirror the primitives of the second interior node
-        const Prim q = prims_of(C, O[0][a2], O[1][a2], O[2][a2], O[3][a2], O[4][a2]);
+        const Prim q = prims_of(C, ld(0, a2), ld(1, a2), ld(2, a2), ld(3, a2), ld(4, a2));
         u = q.u;
         v = q.v;
         w = q.w;
@@ -262,6 +265,17 @@ __global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __res
       }
     }
   }
+}
+
+__global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __restrict__ blocks, int s, int axis) {
+  __shared__ double red[4 * 32];
+  const EdgeBlock eb = blocks[blockIdx.x];  // every listed block holds nodes of its face
+  const Grid& G = grids[eb.g];
+  StepCtl* c = G.ctl;
+  if (!c->active) return;
+  DtAcc dta;
+  int bad = 0;
+  edge_node(G, c, eb, threadIdx.x, threadIdx.y, s, axis, dta, bad);
   if (s == 3) {
     flush_dt(c, dta, red);
     if (bad) atomicOr(&c->nonFinite, 1);
@@ -271,40 +285,46 @@ __global__ void k_edge_bc(const Grid* __restrict__ grids, const EdgeBlock* __res
 // ----------------------------------------------------------------------------------------------
 // Near-body filter (ImmersedBoundary::filterClosestFluidNodes, Boundary.cpp:618-652). Jacobi: every
 // filtered value is computed from unfiltered neighbours; results go to fnew and are written back by
-// k_ghost. The values before the filter go to fpre: the reference does not recompute the primitive
+// the ghost pass. The values before the filter go to fpre: the reference does not recompute the primitive
 // variables of these nodes after filtering, so the next stage builds their primitives from fpre.
+// filter_item: filter node f of a grid (stage-4 dt terms, change norms of rho and rho_E, NaN check).
+__device__ __forceinline__ void filter_item(const Grid& G, const StepCtl* c, int s, int f, DtAcc& dta, double nsum[5],
+                                            int& bad) {
+  double* const* O = c->O[s];
+  const long long n = G.fnode[f];
+  const double* r = O[0];
+  const double* e = O[4];
+  const double rf = (6 * __ldcg(r + n) + __ldcg(r + n + G.sI) + __ldcg(r + n - G.sI) + __ldcg(r + n + G.sJ) +
+                     __ldcg(r + n - G.sJ) + __ldcg(r + n + 1) + __ldcg(r + n - 1)) / 12;
+  const double ef = (6 * __ldcg(e + n) + __ldcg(e + n + G.sI) + __ldcg(e + n - G.sI) + __ldcg(e + n + G.sJ) +
+                     __ldcg(e + n - G.sJ) + __ldcg(e + n + 1) + __ldcg(e + n - 1)) / 12;
+  const double r0 = __ldcg(r + n), e0 = __ldcg(e + n);
+  G.fpre[2 * f] = r0;
+  G.fpre[2 * f + 1] = e0;
+  G.fnew[2 * f] = rf;
+  G.fnew[2 * f + 1] = ef;
+  if (s == 3) {
+    const Prim q = prims_of(G.C, r0, __ldcg(O[1] + n), __ldcg(O[2] + n), __ldcg(O[3] + n), e0);
+    dta.add(G.C, rf, q.u, q.v, q.w, q.p, q.mu);
+    const double d0 = c->U0[0][n] - rf, d4 = c->U0[4][n] - ef;
+    nsum[0] += d0 * d0;
+    nsum[4] += d4 * d4;
+    bad |= !isfinite(rf) || !isfinite(ef);
+  }
+}
+
 __global__ void k_body_filter(const Grid* __restrict__ grids, int s) {
   __shared__ double red[5 * 32];
   const Grid& G = grids[blockIdx.y];
   StepCtl* c = G.ctl;
   if (!c->active) return;
-  const Consts& C = G.C;
-  double* const* O = c->O[s];
   DtAcc dta;
   double nsum[5] = {0, 0, 0, 0, 0};
   int bad = 0;
   // a block past this member's filter nodes never writes its norm slot, which stays zero
   if (int(blockIdx.x * blockDim.x) >= G.nFilter) return;
-  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < G.nFilter; f += gridDim.x * blockDim.x) {
-    const long long n = G.fnode[f];
-    const double* r = O[0];
-    const double* e = O[4];
-    const double rf = (6 * r[n] + r[n + G.sI] + r[n - G.sI] + r[n + G.sJ] + r[n - G.sJ] + r[n + 1] + r[n - 1]) / 12;
-    const double ef = (6 * e[n] + e[n + G.sI] + e[n - G.sI] + e[n + G.sJ] + e[n - G.sJ] + e[n + 1] + e[n - 1]) / 12;
-    const double r0 = r[n], e0 = e[n];
-    G.fpre[2 * f] = r0;
-    G.fpre[2 * f + 1] = e0;
-    G.fnew[2 * f] = rf;
-    G.fnew[2 * f + 1] = ef;
-    if (s == 3) {
-      const Prim q = prims_of(C, r0, O[1][n], O[2][n], O[3][n], e0);
-      dta.add(C, rf, q.u, q.v, q.w, q.p, q.mu);
-      const double d0 = c->U0[0][n] - rf, d4 = c->U0[4][n] - ef;
-      nsum[0] += d0 * d0;
-      nsum[4] += d4 * d4;
-      bad |= !isfinite(rf) || !isfinite(ef);
-    }
-  }
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < G.nFilter; f += gridDim.x * blockDim.x)
+    filter_item(G, c, s, f, dta, nsum, bad);
   if (s == 3) {
     flush_dt(c, dta, red);
     flush_norms(G.normPart + 5 * (G.normSlotFilter + blockIdx.x), nsum, red);
@@ -314,66 +334,85 @@ __global__ void k_body_filter(const Grid* __restrict__ grids, int s) {
 
 // Ghost nodes (Boundary.cpp:432-456): image-point value = cached weights x the 8 surrounding values
 // (Neumann weights for rho and rho_E, Dirichlet weights for the momenta, zero weight on ghost corners);
-// ghost value = image value with momentum negated (getGhostNodeBCVariables, :777-785). The same
-// launch writes the filtered values back (ghosts read them through fnew) and, on stage 4, adds the dt
-// terms of the solid inactive nodes, whose primitive values the reference never updates.
+// ghost value = image value with momentum negated (getGhostNodeBCVariables, :777-785). The ghost lists
+// are stored sorted by image-point cell, so the lanes of a warp gather overlapping corner sets; every
+// corner's five values are loaded before any is used (40 independent loads in flight per ghost) and summed
+// in corner order, skipping corners whose two weights are both zero, as the reference's sums do.
+// ghost_pass_item: item q of the ghost pass: q < nGhost a ghost, then the filter write-backs (ghosts read
+// the filtered values through fnew), then on stage 4 the solid inactive nodes' dt terms (the reference
+// never updates their primitive values).
+__device__ __forceinline__ void ghost_pass_item(const Grid& G, const StepCtl* c, int s, int q, DtAcc& dta, int& bad) {
+  double* const* O = c->O[s];
+  const Consts& C = G.C;
+  if (q < G.nGhost) {
+    const long long* cell = G.gcell + 8 * (long long)q;
+    const double* w = G.gw + 16 * (long long)q;
+    double v[8][5], wn[8], wd[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const long long cn = cell[m];
+      wn[m] = w[m];
+      wd[m] = w[8 + m];
+#pragma unroll
+      for (int f = 0; f < 5; ++f) v[m][f] = __ldcg(O[f] + cn);
+      if (G.type[cn] & FILTER_BIT) {
+        const int fi = G.fidx[cn];
+        v[m][0] = __ldcg(G.fnew + 2 * fi);
+        v[m][4] = __ldcg(G.fnew + 2 * fi + 1);
+      }
+    }
+    double ip[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      if (wn[m] == 0.0 && wd[m] == 0.0) continue;
+      ip[0] += wn[m] * v[m][0];
+      ip[4] += wn[m] * v[m][4];
+      ip[1] += wd[m] * v[m][1];
+      ip[2] += wd[m] * v[m][2];
+      ip[3] += wd[m] * v[m][3];
+    }
+    const double gc[5] = {ip[0], -ip[1], -ip[2], -ip[3], ip[4]};
+    const long long n = G.gnode[q];
+    for (int f = 0; f < 5; ++f) O[f][n] = gc[f];
+    if (s == 3) {
+      const Prim p = prims_of(C, gc[0], gc[1], gc[2], gc[3], gc[4]);
+      dta.add(C, gc[0], p.u, p.v, p.w, p.p, p.mu);
+      for (int f = 0; f < 5; ++f) bad |= !isfinite(gc[f]);
+    }
+  } else if (q < G.nGhost + G.nFilter) {
+    const int f = q - G.nGhost;
+    const long long n = G.fnode[f];
+    O[0][n] = __ldcg(G.fnew + 2 * f);
+    O[4][n] = __ldcg(G.fnew + 2 * f + 1);
+  } else {
+    const int z = q - G.nGhost - G.nFilter;
+    const long long n = G.inode[z];
+    const double* pr = G.iprim + 5 * (long long)z;
+    const double r0 = __ldcg(O[0] + n);
+    if (isnan(pr[0])) {  // periodic copy of a node whose primitives follow its conserved values
+      const Prim p = prims_of(C, r0, __ldcg(O[1] + n), __ldcg(O[2] + n), __ldcg(O[3] + n), __ldcg(O[4] + n));
+      dta.add(C, r0, p.u, p.v, p.w, p.p, p.mu);
+    } else {
+      dta.add(C, r0, pr[0], pr[1], pr[2], pr[3], pr[4]);
+    }
+  }
+}
+
+__device__ __forceinline__ int ghost_pass_count(const Grid& G, int s) {
+  return G.nGhost + G.nFilter + (s == 3 ? G.nInactive : 0);
+}
+
 __global__ void k_ghost(const Grid* __restrict__ grids, int s) {
   __shared__ double red[4 * 32];
   const Grid& G = grids[blockIdx.y];
   StepCtl* c = G.ctl;
   if (!c->active) return;
-  const Consts& C = G.C;
-  double* const* O = c->O[s];
   DtAcc dta;
   int bad = 0;
-  const int total = G.nGhost + G.nFilter + (s == 3 ? G.nInactive : 0);
+  const int total = ghost_pass_count(G, s);
   if (int(blockIdx.x * blockDim.x) >= total) return;  // the whole block is past this member's work
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
-    if (q < G.nGhost) {
-      const long long* cell = G.gcell + 8 * (long long)q;
-      const double* w = G.gw + 16 * (long long)q;
-      double ip[5] = {0, 0, 0, 0, 0};
-      for (int m = 0; m < 8; ++m) {
-        const double wn = w[m], wd = w[8 + m];
-        if (wn == 0.0 && wd == 0.0) continue;
-        const long long cn = cell[m];
-        double rho = O[0][cn], rE = O[4][cn];
-        if (G.type[cn] & FILTER_BIT) {
-          const int f = G.fidx[cn];
-          rho = G.fnew[2 * f];
-          rE = G.fnew[2 * f + 1];
-        }
-        ip[0] += wn * rho;
-        ip[4] += wn * rE;
-        ip[1] += wd * O[1][cn];
-        ip[2] += wd * O[2][cn];
-        ip[3] += wd * O[3][cn];
-      }
-      const double gc[5] = {ip[0], -ip[1], -ip[2], -ip[3], ip[4]};
-      const long long n = G.gnode[q];
-      for (int f = 0; f < 5; ++f) O[f][n] = gc[f];
-      if (s == 3) {
-        const Prim p = prims_of(C, gc[0], gc[1], gc[2], gc[3], gc[4]);
-        dta.add(C, gc[0], p.u, p.v, p.w, p.p, p.mu);
-        for (int f = 0; f < 5; ++f) bad |= !isfinite(gc[f]);
-      }
-    } else if (q < G.nGhost + G.nFilter) {
-      const int f = q - G.nGhost;
-      const long long n = G.fnode[f];
-      O[0][n] = G.fnew[2 * f];
-      O[4][n] = G.fnew[2 * f + 1];
-    } else {
-      const int z = q - G.nGhost - G.nFilter;
-      const long long n = G.inode[z];
-      const double* pr = G.iprim + 5 * (long long)z;
-      if (isnan(pr[0])) {  // periodic copy of a node whose primitives follow its conserved values
-        const Prim p = prims_of(C, O[0][n], O[1][n], O[2][n], O[3][n], O[4][n]);
-        dta.add(C, O[0][n], p.u, p.v, p.w, p.p, p.mu);
-      } else {
-        dta.add(C, O[0][n], pr[0], pr[1], pr[2], pr[3], pr[4]);
-      }
-    }
-  }
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x)
+    ghost_pass_item(G, c, s, q, dta, bad);
   if (s == 3) {
     flush_dt(c, dta, red);
     if (bad) atomicOr(&c->nonFinite, 1);
@@ -382,22 +421,20 @@ __global__ void k_ghost(const Grid* __restrict__ grids, int s) {
 
 // ----------------------------------------------------------------------------------------------
 // End of step: change norms (Mesh::getNormOfChange, Mesh.cpp:171-178), next dt
-// (Solver::updateTimeStepSize, Solver.cpp:80-126), t += dt, ++timeLevel, history row.
-__global__ void k_finalize(Grid* grids) {
-  __shared__ double red[5 * 32];
-  Grid* g = grids + blockIdx.x;
+// (Solver::updateTimeStepSize, Solver.cpp:80-126), t += dt, ++timeLevel, history row. Called by every
+// thread of one block (block reductions); red: 5 x 32 doubles of shared memory.
+__device__ void finalize_grid(Grid* g, double* red) {
+  __shared__ double tot[5];
   const int nSlots = g->nNormSlots;
   StepCtl* c = g->ctl;
-  if (!c->active) return;
   const Consts& C = g->C;
   double s[5] = {0, 0, 0, 0, 0};
   for (int q = threadIdx.x; q < nSlots; q += blockDim.x)
-    for (int f = 0; f < 5; ++f) s[f] += g->normPart[5 * q + f];
-  __shared__ double tot[5];
+    for (int f = 0; f < 5; ++f) s[f] += __ldcg(g->normPart + 5 * q + f);
   flush_norms(tot, s, red);
   if (threadIdx.x != 0) return;
   double mx[4];
-  for (int q = 0; q < 4; ++q) mx[q] = __longlong_as_double(static_cast<long long>(c->mx[q]));
+  for (int q = 0; q < 4; ++q) mx[q] = __longlong_as_double(static_cast<long long>(atomicAdd(&c->mx[q], 0ull)));
   const double conv = C.convLim / (mx[0] / C.dx + mx[1] / C.dy + mx[2] / C.dz);
   const double dx2 = C.dx * C.dx, dy2 = C.dy * C.dy, dz2 = C.dz * C.dz;
   const double visc = C.viscLim / (mx[3] * (1 / dx2 + 1 / dy2 + 1 / dz2));
@@ -415,6 +452,13 @@ __global__ void k_finalize(Grid* grids) {
   c->t = tNew;
   c->dt = dt;
   c->level += 1;
+}
+
+__global__ void k_finalize(Grid* grids) {
+  __shared__ double red[5 * 32];
+  Grid* g = grids + blockIdx.x;
+  if (!g->ctl->active) return;
+  finalize_grid(g, red);
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -567,6 +611,136 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 }
 
 // ----------------------------------------------------------------------------------------------
+// Fused boundary kernel: everything a stage does after its stage kernel, in one cooperative launch of
+// bcBlocks x members blocks (blockIdx.y = member), phases in the order the separate kernels run --
+// solid-node copy, x edges, y edges, z edges (the reference's application order, Mesh.cpp:155-167),
+// near-body filter, ghost pass -- with a grid barrier between consecutive phases, since a phase reads what
+// the previous one wrote anywhere in the grid (reads of fields go through L2: __ldcg in the item
+// functions). Stage 4 then flushes the dt maxima, change norms and NaN flag and, after one more barrier,
+// block 0 of each member runs the end-of-step finalize. Every block of the launch passes every barrier
+// (an inactive member's blocks do no work), so the launch must be cooperative (all blocks resident).
+
+// Bounded grid barrier over nb blocks (self-resetting: the last arriver clears the count and advances the
+// generation). A wait longer than kBarrierPolls polls sets StepCtl::timeout and goes on: the run is then
+// reported invalid, and nothing hangs.
+constexpr long long kBarrierPolls = 1ll << 24;
+__device__ void grid_barrier(unsigned* S, unsigned nb, StepCtl* c) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = S + 1;
+    const unsigned g0 = *gen;
+    __threadfence();
+    if (atomicAdd(S, 1u) == nb - 1) {
+      atomicExch(S, 0u);
+      __threadfence();
+      atomicAdd(S + 1, 1u);
+    } else {
+      long long it = 0;
+      while (*gen == g0) {
+        if (++it > kBarrierPolls) {
+          atomicExch(&c->timeout, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__ BcParams P, int s, int fin) {
+  __shared__ double red[5 * 32];
+  Grid& G = grids[blockIdx.y];
+  StepCtl* c = G.ctl;
+  const bool active = c->active != 0;
+  const unsigned nb = gridDim.x * gridDim.y;
+  const int tid = threadIdx.x, gtid = blockIdx.x * blockDim.x + tid, nthr = gridDim.x * blockDim.x;
+  DtAcc dta;
+  double nsum[5] = {0, 0, 0, 0, 0};
+  int bad = 0;
+  bool first = true;
+  auto phase = [&]() {
+    if (!first) grid_barrier(P.sync, nb, c);
+    first = false;
+  };
+  if (P.hasSolid) {
+    phase();
+    const int mask = c->copyMask[s];
+    if (active && mask)
+      for (int q = gtid; q < G.nSolid; q += nthr) solid_copy_item(G, c, s, mask, q);
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (!P.hasEdge[a]) continue;
+    phase();
+    if (active) {  // four edge blocks (32 x 2 threads each) per pass of this block
+      const int e1 = P.edgeStart[a][blockIdx.y + 1], warp = tid >> 5;
+      for (int b = P.edgeStart[a][blockIdx.y] + blockIdx.x * 4 + (warp >> 1); b < e1; b += gridDim.x * 4)
+        edge_node(G, c, P.edge[a][b], tid & 31, warp & 1, s, a, dta, bad);
+    }
+  }
+  if (P.hasFilter) {
+    phase();
+    if (active)
+      for (int f = gtid; f < G.nFilter; f += nthr) filter_item(G, c, s, f, dta, nsum, bad);
+  }
+  if (P.hasGhost) {
+    phase();
+    if (active) {
+      const int total = ghost_pass_count(G, s);
+      for (int q = gtid; q < total; q += nthr) ghost_pass_item(G, c, s, q, dta, bad);
+    }
+  }
+  if (s == 3) {
+    flush_dt(c, dta, red);
+    // one norm slot per block (members have 1 + bcBlocks slots or more when a filter exists)
+    if (P.hasFilter) flush_norms(G.normPart + 5 * (G.normSlotFilter + blockIdx.x), nsum, red);
+    if (bad) atomicOr(&c->nonFinite, 1);
+  }
+  if (fin) {
+    grid_barrier(P.sync, nb, c);
+    if (blockIdx.x == 0 && active) finalize_grid(&G, red);
+  }
+}
+
+static void launch_bc(Grid* dg, int members, const LaunchPlan& L, int s, bool fin, cudaStream_t st) {
+  BcParams P{};
+  for (int a = 0; a < 3; ++a) {
+    P.edge[a] = L.edgeBlocks[a];
+    P.edgeStart[a] = L.edgeStart[a];
+    P.hasEdge[a] = L.nEdgeBlocks[a] > 0;
+  }
+  P.sync = L.bcSync;
+  P.hasSolid = L.hasSolid;
+  P.hasFilter = L.hasFilter;
+  P.hasGhost = L.hasGhostWork;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(unsigned(L.bcBlocks), unsigned(members));
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_bc, dg, P, s, fin ? 1 : 0);
+}
+
+int bc_capacity(int nSM) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bc, 256, 0) != cudaSuccess) return 0;
+  return nb * nSM;
+}
+
+long long bc_member_work(const Grid& G, const int nEdgeBlocks[3]) {
+  long long w = std::max<long long>(G.nSolid, G.nFilter);
+  w = std::max<long long>(w, (long long)G.nGhost + G.nFilter + G.nInactive);
+  for (int a = 0; a < 3; ++a) w = std::max<long long>(w, 64ll * nEdgeBlocks[a]);
+  return w;
+}
+
+// ----------------------------------------------------------------------------------------------
 // Host-side launch helpers (called from nsf_capi.cpp).
 
 void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vector<EdgeBlock>& out) {
@@ -613,6 +787,9 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
   };
   int launches = 0;
   const unsigned M = unsigned(members);
+  // the fused boundary kernel on the plain path (the hooked path keeps the separate launches: its hooks
+  // run between them)
+  const bool fused = L.bcBlocks > 0 && !hook && !lastStage;
   k_prologue<<<M, 32, 0, st>>>(dg);
   ++launches;
   if (hook) hook->after_prologue();
@@ -635,6 +812,15 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
       launch_stage_ensemble(dg, L, s, st);
     if (ev) record(ev[2 * s + 1]);
     ++launches;
+    if (fused) {
+      const bool work = L.hasSolid || L.nEdgeBlocks[0] || L.nEdgeBlocks[1] || L.nEdgeBlocks[2] || L.hasFilter ||
+                        L.hasGhostWork;
+      if (work || s == 3) {
+        launch_bc(dg, members, L, s, s == 3, st);
+        ++launches;
+      }
+      continue;
+    }
     if (L.hasSolid) {
       k_solid_copy<<<dim3(L.solidBlocks, M), 256, 0, st>>>(dg, s);
       ++launches;
@@ -654,8 +840,10 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
       ++launches;
     }
   }
-  k_finalize<<<M, 256, 0, st>>>(dg);
-  ++launches;
+  if (!fused) {
+    k_finalize<<<M, 256, 0, st>>>(dg);
+    ++launches;
+  }
   return launches;
 }
 

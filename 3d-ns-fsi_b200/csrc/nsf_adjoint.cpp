@@ -192,15 +192,18 @@ nsf_status setup(nsf_solver* s) {
   }
   s->hGrid.ctlHist = a->dHist;
   s->hGrid.nCtlHist = a->nsteps;
-  // objective: body normals at the ghosts' body-intercept points (gnode order), area weight
-  std::vector<double> nx;
+  // objective: body normals at the ghosts' body-intercept points (in the device's ghost order, gnode), area
+  // weight
+  std::vector<double> nxBody;
   for (const auto& b : S.bodies)
     for (const auto& g : b.ghosts) {
       double d[3] = {g.bi[0] - b.c[0], g.bi[1] - b.c[1], g.bi[2] - b.c[2]};
       if (!b.sphere) d[b.axis] = 0;
       const double len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-      nx.push_back(len > 0 ? d[0] / len : 0.0);
+      nxBody.push_back(len > 0 ? d[0] / len : 0.0);
     }
+  std::vector<double> nx(nxBody.size());
+  for (size_t q = 0; q < nx.size(); ++q) nx[q] = nxBody[size_t(s->ghostOrder[q])];
   a->dA = std::pow(S.d[0] * S.d[1] * S.d[2], 2.0 / 3.0);
   if ((st = aalloc(s, a, &a->dNx, nx.size())) != NSF_OK) return st;
   if (!nx.empty()) CKA(cudaMemcpy(a->dNx, nx.data(), nx.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -360,6 +363,7 @@ struct SnapHook : StepHook {
     if (nf(s)) add(base + 11 * N, s->hGrid.fpre, 2 * nf(s));
     flush();
   }
+  bool wants_before_edges() const override { return a->xInOut && !a->edgePlanesClean; }
   void before_edges(int q) override {
     if (!a->xInOut || a->edgePlanesClean) return;
     const size_t N = nd(s), plane = size_t(s->hGrid.sI), NI = size_t(s->hGrid.NI);

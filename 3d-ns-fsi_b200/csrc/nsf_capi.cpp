@@ -267,8 +267,9 @@ nsf_status build_device(nsf_solver* s) {
     G.tmaps = dMaps;
   }
   G.nFilter = int(fnode.size());
+  std::vector<int> fidx;
   if (!fnode.empty()) {
-    std::vector<int> fidx(Nd, -1);
+    fidx.assign(Nd, -1);
     for (size_t q = 0; q < fnode.size(); ++q) fidx[fnode[q]] = int(q);
     int* dF;
     if ((st = upload(s, &dF, fidx)) != NSF_OK) return st;
@@ -318,6 +319,26 @@ nsf_status build_device(nsf_solver* s) {
         }
       }
     }
+  {  // device order of the ghosts: by image-point cell (first corner), so the lanes of a warp gather
+     // overlapping corner sets; s->ghostOrder[q] = the ghost's position in the bodies' own order
+    const size_t ng = gnode.size();
+    std::vector<int> ord(ng);
+    for (size_t q = 0; q < ng; ++q) ord[q] = int(q);
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return gcell[8 * size_t(a)] < gcell[8 * size_t(b)]; });
+    auto permute = [&](auto& v, size_t per) {
+      auto w = v;
+      for (size_t q = 0; q < ng; ++q)
+        for (size_t r = 0; r < per; ++r) w[q * per + r] = v[size_t(ord[q]) * per + r];
+      v.swap(w);
+    };
+    permute(gnode, 1);
+    permute(gcell, 8);
+    permute(pts, 24);
+    permute(nrm, 24);
+    permute(ipl, 6);
+    permute(gfl, 8);
+    s->ghostOrder = ord;
+  }
   G.nGhost = int(gnode.size());
   long long *dGnode, *dGcell;
   double *dPts, *dNrm, *dIpl, *dW;
@@ -457,12 +478,24 @@ nsf_status build_device(nsf_solver* s) {
     if ((st = upload(s, &L.ctaStart, start)) != NSF_OK) return st;
   }
   if ((st = upload(s, &L.items, items)) != NSF_OK) return st;
+  std::vector<EdgeBlock> ebAxis[3];
   for (int a = 0; a < 3; ++a) {
-    std::vector<EdgeBlock> eb;
+    std::vector<EdgeBlock>& eb = ebAxis[a];
     edge_blocks(G, type.data(), 0, a, eb);
     L.nEdgeBlocks[a] = int(eb.size());
     L.edgeBlocks[a] = nullptr;
     if (!eb.empty() && (st = upload(s, &L.edgeBlocks[a], eb)) != NSF_OK) return st;
+  }
+  {  // dependency levels of the stage's boundary work, for the fused boundary kernel
+    BcMemberInput in;
+    in.snode = snode;
+    in.fnode = fnode;
+    in.gnode = gnode;
+    in.gcell = gcell;
+    in.inode = inode;
+    in.typeDev = typeDev;
+    in.fidx = fidx;
+    bc_plan_member(G, ebAxis, in, s->bcLevels);
   }
   L.hasFilter = G.nFilter > 0;
   L.filterBlocks = std::max(1, std::min(s->nSM, (G.nFilter + 255) / 256));
@@ -472,16 +505,18 @@ nsf_status build_device(nsf_solver* s) {
   L.hasGhostWork = ghostWork > 0;
   L.ghostBlocks = std::max(1, std::min(4 * s->nSM, (ghostWork + 255) / 256));
   L.gfBlocks = 4 * s->nSM;
-  {  // fused boundary kernel: enough blocks for the busiest phase, within what can be resident at once
+  {  // fused boundary kernel: enough blocks for the busiest level, within what can be resident at once
+    BcFlat fl;
+    bc_flatten({&s->bcLevels}, fl);
     const int cap = bc_capacity(s->nSM);
-    const long long work = bc_member_work(G, L.nEdgeBlocks);
-    L.bcBlocks = cap > 0 ? int(std::max<long long>(1, std::min<long long>(cap, (work + 255) / 256))) : 0;
+    L.bcBlocks = cap > 0 ? int(std::max<long long>(1, std::min<long long>(cap, (fl.maxWork + 255) / 256))) : 0;
+    L.bcLevels = fl.levels;
     if (L.bcBlocks > 0) {
       L.filterBlocks = std::max(L.filterBlocks, L.bcBlocks);  // one norm slot per block of the fused kernel
-      for (int a = 0; a < 3; ++a) {
-        const std::vector<int> start = {0, L.nEdgeBlocks[a]};
-        if ((st = upload(s, &L.edgeStart[a], start)) != NSF_OK) return st;
-      }
+      if ((st = upload(s, &L.bcEdges, fl.edges)) != NSF_OK) return st;
+      if ((st = upload(s, &L.bcEdgeStart, fl.edgeStart)) != NSF_OK) return st;
+      if ((st = upload(s, &L.bcItems, fl.items)) != NSF_OK) return st;
+      if ((st = upload(s, &L.bcItemStart, fl.itemStart)) != NSF_OK) return st;
       const std::vector<unsigned> zero(2, 0u);
       if ((st = upload(s, &L.bcSync, zero)) != NSF_OK) return st;
     }

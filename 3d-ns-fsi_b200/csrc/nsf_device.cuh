@@ -150,13 +150,37 @@ struct EdgeBlock {
 // whose source node is not an unfiltered interior fluid node).
 void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vector<EdgeBlock>& out);
 
-// Arguments of one launch of the fused boundary kernel (k_bc, see nsf_kernels.cu).
+// Arguments of one launch of the fused boundary kernel (k_bc, see nsf_kernels.cu): the stage's boundary
+// work in dependency levels (nsf_bc_plan.cpp). Level L (0-based here) of member g: edge blocks
+// edges[edgeStart[L * (M + 1) + g] ..), near-body filter items (class 0) and ghost-pass items (class 1, the
+// encoding of ghost_pass_item) items[itemStart[(L * 2 + c) * (M + 1) + g] ..). Solid-node copies: level 0.
 struct BcParams {
-  const EdgeBlock* edge[3];  // per axis: the edge blocks of every member, member-major
-  const int* edgeStart[3];   // per axis: members + 1 offsets into edge[axis]
-  unsigned* sync;            // grid barrier state: arrival count, generation
-  int hasEdge[3];
-  int hasSolid, hasFilter, hasGhost;
+  const EdgeBlock* edges;
+  const int* edgeStart;
+  const int* items;
+  const int* itemStart;
+  unsigned* sync;  // grid barrier state: arrival count, generation
+  int levels, members;
+};
+
+// Boundary work of one grid split into levels (bc_plan_member), and several grids' levels flattened into
+// the arrays BcParams points to (bc_flatten).
+struct BcMemberLevels {
+  int levels = 0;
+  long long solid = 0;
+  std::vector<std::vector<EdgeBlock>> edges;  // [level]
+  std::vector<std::vector<int>> filter, ghost;
+};
+struct BcMemberInput {  // device node indices (the padded device layout)
+  std::vector<long long> snode, fnode, gnode, gcell, inode;
+  std::vector<uint8_t> typeDev;  // node types with FILTER_BIT, per device node
+  std::vector<int> fidx;         // filter slot per device node, or -1
+};
+struct BcFlat {
+  int levels = 0;
+  long long maxWork = 1;  // threads one member needs in its busiest level
+  std::vector<EdgeBlock> edges;
+  std::vector<int> edgeStart, items, itemStart;
 };
 
 struct LaunchPlan {
@@ -170,11 +194,15 @@ struct LaunchPlan {
   int nEdgeBlocks[3];
   int filterBlocks, ghostBlocks, solidBlocks, gfBlocks;
   // Fused boundary kernel: per stage one cooperative launch of bcBlocks x members blocks that runs the
-  // solid-node copy, the x, y and z edge conditions, the near-body filter and the ghost pass in that order
-  // with grid barriers between them (and, on stage 4, the end-of-step finalize). 0: separate launches.
+  // stage's boundary work level by level with grid barriers between levels (and, on stage 4, the
+  // end-of-step finalize). 0: separate launches.
   int bcBlocks;
-  int* edgeStart[3];  // device, members + 1 offsets into edgeBlocks[axis]
-  unsigned* bcSync;   // device, 2 words, zero at creation
+  int bcLevels;
+  EdgeBlock* bcEdges;  // device arrays of BcParams
+  int* bcEdgeStart;
+  int* bcItems;
+  int* bcItemStart;
+  unsigned* bcSync;    // device, 2 words, zero at creation
   int nSlots;
   bool hasBodies;
   bool hasFilter, hasGhostWork, hasSolid;
@@ -211,6 +239,9 @@ struct StepHook {
   virtual void after_prologue() {}
   virtual void before_stage(int) {}
   virtual void before_edges(int) {}
+  // false: before_edges does nothing for this step, so the stage's boundary work may run as the fused
+  // boundary kernel (whose phases the hook cannot come between)
+  virtual bool wants_before_edges() const { return true; }
 };
 // lastStage: NULL for a whole step, or a plan whose items stage 4 is limited to (the step then stops after
 // that stage kernel: the adjoint's recomputation when only some planes of the step's result are read).
@@ -224,9 +255,13 @@ int enqueue_ensemble_step(Grid* dGrids, int members, const LaunchPlan& L, void* 
 // Blocks of 256 threads of the fused boundary kernel that can be resident on the device at once (its
 // cooperative launches must not exceed this), or 0 if unknown.
 int bc_capacity(int nSM);
-// Threads one member needs in the busiest phase of the fused boundary kernel (ghost pass with stage 4's
-// inactive nodes; edge blocks count 64 threads each).
-long long bc_member_work(const Grid& G, const int nEdgeBlocks[3]);
+// Dependency levels of one grid's boundary work (nsf_bc_plan.cpp); edgeBlocks: the grid's edge blocks per
+// axis (edge_blocks). Returns the number of levels.
+int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], const BcMemberInput& in,
+                   BcMemberLevels& out);
+void bc_flatten(const std::vector<const BcMemberLevels*>& members, BcFlat& out);
+// The node a periodic face node finally copies (opposite interior plane, then further periodic faces).
+void periodic_source_host(const Grid& G, int axis, int side, int ijk[3]);
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,
                           double dx, double dy, double dz, double* w, void* stream);
 void launch_download_prims(const Grid* dg, long long N, double* out, const long long* inodes, const double* ip7,

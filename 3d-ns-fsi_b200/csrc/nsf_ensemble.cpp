@@ -232,14 +232,9 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
   CKE(cudaMemcpy(L.ctaStart, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
   // small kernels: block counts = maxima over the members
   L.gfBlocks = std::max(8, 4 * e->nSM / M);  // grid-stride over each member's nodes
-  std::vector<int> edgeStart[3];
   for (int a = 0; a < 3; ++a) {  // edge blocks: every member's own, member-major
     std::vector<EdgeBlock> eb;
-    edgeStart[a].push_back(0);
-    for (int g = 0; g < M; ++g) {
-      edge_blocks(e->members[g]->hGrid, e->members[g]->typeFlags.data(), g, a, eb);
-      edgeStart[a].push_back(int(eb.size()));
-    }
+    for (int g = 0; g < M; ++g) edge_blocks(e->members[g]->hGrid, e->members[g]->typeFlags.data(), g, a, eb);
     L.nEdgeBlocks[a] = int(eb.size());
     L.edgeBlocks[a] = nullptr;
     if (eb.empty()) continue;
@@ -256,20 +251,28 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
     L.hasSolid |= P.hasSolid;
   }
   {  // fused boundary kernel: bcBlocks blocks per member, all members' blocks resident at once
+    std::vector<const BcMemberLevels*> lv;
+    for (nsf_solver* s : e->members) lv.push_back(&s->bcLevels);
+    BcFlat fl;
+    bc_flatten(lv, fl);
     const int cap = bc_capacity(e->nSM) / M;
-    long long work = 1;
-    for (int g = 0; g < M; ++g) {
-      int nEb[3];
-      for (int a = 0; a < 3; ++a) nEb[a] = edgeStart[a][g + 1] - edgeStart[a][g];
-      work = std::max(work, bc_member_work(e->members[g]->hGrid, nEb));
-    }
-    L.bcBlocks = cap > 0 ? int(std::min<long long>(cap, (work + 255) / 256)) : 0;
+    L.bcBlocks = cap > 0 ? int(std::min<long long>(cap, (fl.maxWork + 255) / 256)) : 0;
+    L.bcLevels = fl.levels;
     if (L.bcBlocks > 0) {
       L.filterBlocks = std::max(L.filterBlocks, L.bcBlocks);
-      for (int a = 0; a < 3; ++a) {
-        if ((st = ens_alloc(e, &L.edgeStart[a], edgeStart[a].size())) != NSF_OK) return st;
-        CKE(cudaMemcpy(L.edgeStart[a], edgeStart[a].data(), edgeStart[a].size() * sizeof(int), cudaMemcpyHostToDevice));
-      }
+      auto up = [&](auto** p, const auto& v) -> nsf_status {
+        nsf_status r = ens_alloc(e, p, v.size());
+        if (r != NSF_OK) return r;
+        if (!v.empty() && cudaMemcpy(*p, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice) != cudaSuccess) {
+          e->err = "could not upload the fused boundary kernel's plan";
+          return NSF_ERR_CUDA;
+        }
+        return NSF_OK;
+      };
+      if ((st = up(&L.bcEdges, fl.edges)) != NSF_OK) return st;
+      if ((st = up(&L.bcEdgeStart, fl.edgeStart)) != NSF_OK) return st;
+      if ((st = up(&L.bcItems, fl.items)) != NSF_OK) return st;
+      if ((st = up(&L.bcItemStart, fl.itemStart)) != NSF_OK) return st;
       if ((st = ens_alloc(e, &L.bcSync, 2)) != NSF_OK) return st;
       CKE(cudaMemset(L.bcSync, 0, 2 * sizeof(unsigned)));
     }

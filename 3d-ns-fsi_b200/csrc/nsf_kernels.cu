@@ -160,9 +160,30 @@ __global__ void k_solid_copy(const Grid* __restrict__ grids, int s) {
 // nodes). Launched for x, then y, then z: the reference's application order outlet/inlet (x), y-max,
 // y-min, z-max, z-min (Mesh.cpp:155-167 after the reversal at Mesh.cpp:70). Each block comes from the
 // launch plan's list (member, face, first in-plane coordinates, mask of the nodes it works on).
+// periodic_source: the node a periodic face node finally copies -- the opposite interior-plane node, and if
+// that node lies on another periodic face (which copied it earlier in the reference's order), that face's
+// source, and so on (at most two more hops). The copies are exact, so reading the final source gives the
+// value the reference copies; it lets chains of copies run together (nsf_bc_plan.cpp).
 // edge_node: one node (thread tx, ty of an edge block) of a mesh-edge boundary condition; adds the stage-4
 // dt terms and the NaN check of edge and ghost-typed nodes.
-__device__ __forceinline__ void edge_node(const Grid& G, StepCtl* c, const EdgeBlock& eb, int tx, int ty, int s,
+__device__ __forceinline__ void periodic_source(const Grid& G, int axis, int side, int ijk[3]) {
+  const int nAx[3] = {G.NI, G.NJ, G.NK};
+  ijk[axis] = side == 0 ? nAx[axis] - 2 : 1;
+  for (int hop = 0; hop < 2; ++hop) {
+    int found = -1;
+    for (int e = 0; e < G.nEdge && found < 0; ++e) {
+      const int* b = G.eBox[e];
+      if (G.eBc[e] == NSF_BC_PERIODIC && ijk[0] >= b[0] && ijk[0] <= b[1] && ijk[1] >= b[2] && ijk[1] <= b[3] &&
+          ijk[2] >= b[4] && ijk[2] <= b[5])
+        found = e;
+    }
+    if (found < 0) return;
+    const int a = G.eAxis[found];
+    ijk[a] = G.eSide[found] == 0 ? nAx[a] - 2 : 1;
+  }
+}
+
+__device__ __forceinline__ void edge_node(const Grid& G, const StepCtl* c, const EdgeBlock& eb, int tx, int ty, int s,
                                           int axis, DtAcc& dta, int& bad) {
   const Consts& C = G.C;
   const int e = eb.e;
@@ -180,7 +201,7 @@ __device__ __forceinline__ void edge_node(const Grid& G, StepCtl* c, const EdgeB
       const long long st = axis == 0 ? G.sI : axis == 1 ? G.sJ : 1;
       const long long n = ijk[0] * G.sI + ijk[1] * G.sJ + ijk[2];
       const int side = G.eSide[e], bc = G.eBc[e];
-      double** O = c->O[s];
+      double* const* O = c->O[s];
       auto ld = [&](int f, long long m) { return __ldcg(O[f] + m); };
       const long long a1 = side == 0 ? n + st : n - st, a2 = side == 0 ? n + 2 * st : n - 2 * st;  // Boundary.cpp:74-108
       double cv[5];
@@ -227,8 +248,7 @@ __device__ __forceinline__ void edge_node(const Grid& G, StepCtl* c, const EdgeB
         primKnown = true;
       } else if (bc == NSF_BC_PERIODIC) {  // Boundary.cpp:344-367, opposite index :111-133
         int src[3] = {ijk[0], ijk[1], ijk[2]};
-        const int nAx = axis == 0 ? G.NI : axis == 1 ? G.NJ : G.NK;
-        src[axis] = side == 0 ? nAx - 2 : 1;
+        periodic_source(G, axis, side, src);
         const long long m = src[0] * G.sI + src[1] * G.sJ + src[2];
         for (int f = 0; f < 5; ++f) cv[f] = ld(f, m);
       } else {  // symmetry, Boundary.cpp:377-417: mirror the primitives of the second interior node
@@ -612,13 +632,14 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 
 // ----------------------------------------------------------------------------------------------
 // Fused boundary kernel: everything a stage does after its stage kernel, in one cooperative launch of
-// bcBlocks x members blocks (blockIdx.y = member), phases in the order the separate kernels run --
-// solid-node copy, x edges, y edges, z edges (the reference's application order, Mesh.cpp:155-167),
-// near-body filter, ghost pass -- with a grid barrier between consecutive phases, since a phase reads what
-// the previous one wrote anywhere in the grid (reads of fields go through L2: __ldcg in the item
-// functions). Stage 4 then flushes the dt maxima, change norms and NaN flag and, after one more barrier,
-// block 0 of each member runs the end-of-step finalize. Every block of the launch passes every barrier
-// (an inactive member's blocks do no work), so the launch must be cooperative (all blocks resident).
+// bcBlocks x members blocks (blockIdx.y = member), in the dependency levels of nsf_bc_plan.cpp: level 0
+// holds the solid-node copies and every edge, filter and ghost-pass item whose inputs are final after the
+// stage kernel; each later level reads what earlier levels wrote anywhere in the grid, so a grid barrier
+// separates levels and those reads go through L2 (__ldcg in the item functions). The member's Grid and
+// control block are copied to shared memory first (every item reads them). Stage 4 then flushes the dt
+// maxima, change norms and NaN flag and, after one more barrier, block 0 of each member runs the end-of-step
+// finalize. Every block passes every barrier (an inactive member's blocks do no work), so the launch is
+// cooperative (all blocks resident).
 
 // Bounded grid barrier over nb blocks (self-resetting: the last arriver clears the count and advances the
 // generation). A wait longer than kBarrierPolls polls sets StepCtl::timeout and goes on: the run is then
@@ -651,69 +672,73 @@ __device__ void grid_barrier(unsigned* S, unsigned nb, StepCtl* c) {
 
 __global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__ BcParams P, int s, int fin) {
   __shared__ double red[5 * 32];
-  Grid& G = grids[blockIdx.y];
-  StepCtl* c = G.ctl;
-  const bool active = c->active != 0;
+  __shared__ __align__(16) unsigned char gsm[sizeof(Grid)];
+  __shared__ __align__(16) unsigned char csm[sizeof(StepCtl)];
+  const int g = blockIdx.y, M = P.members, tid = threadIdx.x;
+  Grid* gp = grids + g;
+  StepCtl* c = gp->ctl;  // global: atomics, flags and finalize write here
+  {
+    static_assert(sizeof(Grid) % 8 == 0 && sizeof(StepCtl) % 8 == 0, "copied as 8-byte words");
+    const unsigned long long* a = reinterpret_cast<const unsigned long long*>(gp);
+    const unsigned long long* b = reinterpret_cast<const unsigned long long*>(c);
+    for (int q = tid; q < int(sizeof(Grid) / 8); q += blockDim.x) reinterpret_cast<unsigned long long*>(gsm)[q] = a[q];
+    for (int q = tid; q < int(sizeof(StepCtl) / 8); q += blockDim.x)
+      reinterpret_cast<unsigned long long*>(csm)[q] = b[q];
+  }
+  __syncthreads();
+  const Grid& G = *reinterpret_cast<const Grid*>(gsm);
+  const StepCtl& cs = *reinterpret_cast<const StepCtl*>(csm);  // read-only copy for the item functions
+  const bool active = cs.active != 0;
   const unsigned nb = gridDim.x * gridDim.y;
-  const int tid = threadIdx.x, gtid = blockIdx.x * blockDim.x + tid, nthr = gridDim.x * blockDim.x;
+  const int gtid = blockIdx.x * blockDim.x + tid, nthr = gridDim.x * blockDim.x, warp = tid >> 5;
   DtAcc dta;
   double nsum[5] = {0, 0, 0, 0, 0};
   int bad = 0;
-  bool first = true;
-  auto phase = [&]() {
-    if (!first) grid_barrier(P.sync, nb, c);
-    first = false;
-  };
-  if (P.hasSolid) {
-    phase();
-    const int mask = c->copyMask[s];
-    if (active && mask)
-      for (int q = gtid; q < G.nSolid; q += nthr) solid_copy_item(G, c, s, mask, q);
-  }
-  for (int a = 0; a < 3; ++a) {
-    if (!P.hasEdge[a]) continue;
-    phase();
-    if (active) {  // four edge blocks (32 x 2 threads each) per pass of this block
-      const int e1 = P.edgeStart[a][blockIdx.y + 1], warp = tid >> 5;
-      for (int b = P.edgeStart[a][blockIdx.y] + blockIdx.x * 4 + (warp >> 1); b < e1; b += gridDim.x * 4)
-        edge_node(G, c, P.edge[a][b], tid & 31, warp & 1, s, a, dta, bad);
+  const int ghostCount = ghost_pass_count(G, s);
+  for (int L = 0; L < P.levels; ++L) {
+    if (L > 0) grid_barrier(P.sync, nb, c);
+    if (!active) continue;
+    if (L == 0 && cs.copyMask[s])
+      for (int q = gtid; q < G.nSolid; q += nthr) solid_copy_item(G, &cs, s, cs.copyMask[s], q);
+    {  // edge blocks (32 x 2 threads each), four per pass of this block
+      const int* es = P.edgeStart + L * (M + 1) + g;
+      const int e1 = es[1];
+      for (int b = es[0] + blockIdx.x * 4 + (warp >> 1); b < e1; b += gridDim.x * 4) {
+        const EdgeBlock eb = P.edges[b];
+        edge_node(G, &cs, eb, tid & 31, warp & 1, s, G.eAxis[eb.e], dta, bad);
+      }
     }
-  }
-  if (P.hasFilter) {
-    phase();
-    if (active)
-      for (int f = gtid; f < G.nFilter; f += nthr) filter_item(G, c, s, f, dta, nsum, bad);
-  }
-  if (P.hasGhost) {
-    phase();
-    if (active) {
-      const int total = ghost_pass_count(G, s);
-      for (int q = gtid; q < total; q += nthr) ghost_pass_item(G, c, s, q, dta, bad);
+    {
+      const int* is = P.itemStart + (L * 2) * (M + 1) + g;
+      for (int q = is[0] + gtid; q < is[1]; q += nthr) filter_item(G, &cs, s, P.items[q], dta, nsum, bad);
+      is += M + 1;
+      for (int q = is[0] + gtid; q < is[1]; q += nthr) {
+        const int item = P.items[q];
+        if (item < ghostCount) ghost_pass_item(G, &cs, s, item, dta, bad);
+      }
     }
   }
   if (s == 3) {
     flush_dt(c, dta, red);
-    // one norm slot per block (members have 1 + bcBlocks slots or more when a filter exists)
-    if (P.hasFilter) flush_norms(G.normPart + 5 * (G.normSlotFilter + blockIdx.x), nsum, red);
+    // one norm slot per block (a member has 1 + bcBlocks slots or more when a filter exists)
+    if (G.nFilter > 0) flush_norms(gp->normPart + 5 * (G.normSlotFilter + blockIdx.x), nsum, red);
     if (bad) atomicOr(&c->nonFinite, 1);
   }
   if (fin) {
     grid_barrier(P.sync, nb, c);
-    if (blockIdx.x == 0 && active) finalize_grid(&G, red);
+    if (blockIdx.x == 0 && active) finalize_grid(gp, red);
   }
 }
 
 static void launch_bc(Grid* dg, int members, const LaunchPlan& L, int s, bool fin, cudaStream_t st) {
   BcParams P{};
-  for (int a = 0; a < 3; ++a) {
-    P.edge[a] = L.edgeBlocks[a];
-    P.edgeStart[a] = L.edgeStart[a];
-    P.hasEdge[a] = L.nEdgeBlocks[a] > 0;
-  }
+  P.edges = L.bcEdges;
+  P.edgeStart = L.bcEdgeStart;
+  P.items = L.bcItems;
+  P.itemStart = L.bcItemStart;
   P.sync = L.bcSync;
-  P.hasSolid = L.hasSolid;
-  P.hasFilter = L.hasFilter;
-  P.hasGhost = L.hasGhostWork;
+  P.levels = L.bcLevels;
+  P.members = members;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(unsigned(L.bcBlocks), unsigned(members));
   cfg.blockDim = dim3(256);
@@ -731,13 +756,6 @@ int bc_capacity(int nSM) {
   int nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bc, 256, 0) != cudaSuccess) return 0;
   return nb * nSM;
-}
-
-long long bc_member_work(const Grid& G, const int nEdgeBlocks[3]) {
-  long long w = std::max<long long>(G.nSolid, G.nFilter);
-  w = std::max<long long>(w, (long long)G.nGhost + G.nFilter + G.nInactive);
-  for (int a = 0; a < 3; ++a) w = std::max<long long>(w, 64ll * nEdgeBlocks[a]);
-  return w;
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -787,9 +805,9 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
   };
   int launches = 0;
   const unsigned M = unsigned(members);
-  // the fused boundary kernel on the plain path (the hooked path keeps the separate launches: its hooks
-  // run between them)
-  const bool fused = L.bcBlocks > 0 && !hook && !lastStage;
+  // the fused boundary kernel, unless a hook must run between the solid-node copy and the edge conditions
+  // (a partial last stage ends before its boundary work, fused or not)
+  const bool fused = L.bcBlocks > 0 && (!hook || !hook->wants_before_edges());
   k_prologue<<<M, 32, 0, st>>>(dg);
   ++launches;
   if (hook) hook->after_prologue();
@@ -813,9 +831,7 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
     if (ev) record(ev[2 * s + 1]);
     ++launches;
     if (fused) {
-      const bool work = L.hasSolid || L.nEdgeBlocks[0] || L.nEdgeBlocks[1] || L.nEdgeBlocks[2] || L.hasFilter ||
-                        L.hasGhostWork;
-      if (work || s == 3) {
+      if (L.bcLevels > 0 || s == 3) {
         launch_bc(dg, members, L, s, s == 3, st);
         ++launches;
       }

@@ -43,6 +43,8 @@ struct nsf_solver {
   std::vector<CUtensorMap> hostMaps;
   void* encodeFn = nullptr;
   int tileRequest = -1;  // StageTile to use, or -1 for the default
+  std::vector<int> ghostOrder;   // device ghost slot -> position in the bodies' ghost lists
+  nsf::BcMemberLevels bcLevels;  // dependency levels of the boundary work (fused boundary kernel)
   nsf::StepCtl ctlInit{};  // the control block at level 0 (the discrete adjoint restarts from it)
   struct AdjCtx* adj = nullptr;  // discrete-adjoint state (nsf_adjoint.cpp), created on first use
 };

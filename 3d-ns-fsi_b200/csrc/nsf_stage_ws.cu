@@ -434,9 +434,23 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
       XNode gm1{}, gm2{};
       double fprev[5] = {0, 0, 0, 0, 0};
       XOwn ownPrev{};
-      // Iteration a forms the x quantities of plane i0-1+a and, from a = 2 on, computes the RHS of
-      // plane i0-2+a.
-      for (int a = 0; a <= L + 1; ++a) {
+      constexpr int oN = HK, oU = 1;
+      // x-direction quantities of the column's node in staged plane slot (cX, pX): G of the node, and F of
+      // the face towards the previous plane (a >= 1)
+      auto x_part = [&](int cX, int pX, bool face, XOwn& ownCur, XNode& gcur, double (&fcur)[5]) {
+        const double* cs = reinterpret_cast<const double*>(consBase + cX * CONS_SLOT);
+        const double* ps = reinterpret_cast<const double*>(primBase + pX * PRIM_SLOT);
+        ownCur = XOwn{ps[5 * FS + cidx], ps[0 * FS + cidx], ps[1 * FS + cidx], ps[2 * FS + cidx], ps[4 * FS + cidx]};
+        gcur = x_node(C, cs[1 * FS + cidx], cs[2 * FS + cidx], cs[3 * FS + cidx], cs[4 * FS + cidx], ownCur.u,
+                      ownCur.v, ownCur.w, ps[3 * FS + cidx], ownCur.mu,
+                      ps[1 * FS + cidx + oN] - ps[1 * FS + cidx - oN], ps[0 * FS + cidx + oN] - ps[0 * FS + cidx - oN],
+                      ps[2 * FS + cidx + oU] - ps[2 * FS + cidx - oU], ps[0 * FS + cidx + oU] - ps[0 * FS + cidx - oU]);
+#pragma unroll
+        for (int f = 0; f < 5; ++f) fcur[f] = 0.0;
+        if (face) x_face(C, ownPrev, ownCur, fcur);
+      };
+      // Planes i0-1 and i0: their x quantities only.
+      for (int a = 0; a < 2; ++a) {
         const uint32_t qx = q + a;
         const int pX = qx % NP, cX = qx % NC;
         ok = mbar_wait(&primFull[pX], (qx / NP) & 1, abortFlag, lim) &&
@@ -445,111 +459,122 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           fail(G);
           break;
         }
-        constexpr int oN = HK, oU = 1;
         XNode gcur;
         XOwn ownCur;
-        double fcur[5] = {0, 0, 0, 0, 0};
-        {
-          const double* cs = reinterpret_cast<const double*>(consBase + cX * CONS_SLOT);
-          const double* ps = reinterpret_cast<const double*>(primBase + pX * PRIM_SLOT);
-          ownCur = XOwn{ps[5 * FS + cidx], ps[0 * FS + cidx], ps[1 * FS + cidx],
-                        ps[2 * FS + cidx], ps[4 * FS + cidx]};
-          gcur = x_node(C, cs[1 * FS + cidx], cs[2 * FS + cidx], cs[3 * FS + cidx], cs[4 * FS + cidx], ownCur.u,
-                        ownCur.v, ownCur.w, ps[3 * FS + cidx], ownCur.mu,
-                        ps[1 * FS + cidx + oN] - ps[1 * FS + cidx - oN], ps[0 * FS + cidx + oN] - ps[0 * FS + cidx - oN],
-                        ps[2 * FS + cidx + oU] - ps[2 * FS + cidx - oU], ps[0 * FS + cidx + oU] - ps[0 * FS + cidx - oU]);
-          if (a >= 1) x_face(C, ownPrev, ownCur, fcur);
-        }
+        double fcur[5];
+        x_part(cX, pX, a >= 1, ownCur, gcur, fcur);
         if (a == 0) {  // plane i0-1: its conserved values have no other reader
           __syncwarp();
           if (lane == 0) mbar_arrive(&consEmpty[cX]);
         }
-        if (a >= 2) {
-          const int pR = (qx - 1) % NP, pW = (qx - 2) % NP, cR = (qx - 1) % NC;
-          const uint32_t se = e % NE;
-          ok = mbar_wait(&epiFull[se], (e / NE) & 1, abortFlag, lim);
-          if (!ok) {
+        gm2 = gm1;
+        gm1 = gcur;
+#pragma unroll
+        for (int f = 0; f < 5; ++f) fprev[f] = fcur[f];
+        ownPrev = ownCur;
+      }
+      // Iteration a forms the x quantities of plane X = i0-1+a and the RHS of plane P = i0-2+a. Every wait
+      // comes first, so the x quantities of X and the y/z terms of P (independent until their final sum)
+      // are one block of straight-line arithmetic the compiler can interleave.
+      for (int a = 2; a <= L + 1 && ok; ++a) {
+        const uint32_t qx = q + a;
+        const int pX = qx % NP, cX = qx % NC;
+        const uint32_t se = e % NE;
+        ok = mbar_wait(&primFull[pX], (qx / NP) & 1, abortFlag, lim) &&
+             mbar_wait(&consFull[cX], (qx / NC) & 1, abortFlag, lim);
+        // (the ensemble variant, short of registers, waits for the epilogue tile after the x quantities)
+        if constexpr (!ENS) ok = ok && mbar_wait(&epiFull[se], (e / NE) & 1, abortFlag, lim);
+        if (!ok) {
+          fail(G);
+          break;
+        }
+        const int pR = (qx - 1) % NP, pW = (qx - 2) % NP, cR = (qx - 1) % NC;
+        XNode gcur;
+        XOwn ownCur;
+        double fcur[5];
+        x_part(cX, pX, true, ownCur, gcur, fcur);
+        if constexpr (ENS) {
+          if (!mbar_wait(&epiFull[se], (e / NE) & 1, abortFlag, lim)) {
+            ok = false;
             fail(G);
             break;
           }
-          const double* cP = reinterpret_cast<const double*>(consBase + cR * CONS_SLOT);
-          const uint8_t tc = (reinterpret_cast<const uint8_t*>(cP) + TYPE_OFF)[tcix];
-          const bool valid = inTile && (tc & TYPE_MASK) == FLUID_INTERIOR;
-          double kk5[5];
-          yz_part<HK, FS>(C, cP, reinterpret_cast<const double*>(primBase + pW * PRIM_SLOT),
-                          reinterpret_cast<const double*>(primBase + pR * PRIM_SLOT),
-                          reinterpret_cast<const double*>(primBase + pX * PRIM_SLOT), cidx, ownPrev, kk5);
+        }
+        const double* cP = reinterpret_cast<const double*>(consBase + cR * CONS_SLOT);
+        const uint8_t tc = (reinterpret_cast<const uint8_t*>(cP) + TYPE_OFF)[tcix];
+        const bool valid = inTile && (tc & TYPE_MASK) == FLUID_INTERIOR;
+        double kk5[5];
+        yz_part<HK, FS>(C, cP, reinterpret_cast<const double*>(primBase + pW * PRIM_SLOT),
+                        reinterpret_cast<const double*>(primBase + pR * PRIM_SLOT),
+                        reinterpret_cast<const double*>(primBase + pX * PRIM_SLOT), cidx, ownPrev, kk5);
 #pragma unroll
-          for (int f = 0; f < 5; ++f) kk5[f] += (gcur.g[f] - gm2.g[f]) + (fcur[f] - fprev[f]);
-          const double* ep = reinterpret_cast<const double*>(sm + OFF_EPI + se * EPI_SLOT);
-          double u0[5], res[5];
+        for (int f = 0; f < 5; ++f) kk5[f] += (gcur.g[f] - gm2.g[f]) + (fcur[f] - fprev[f]);
+        const double* ep = reinterpret_cast<const double*>(sm + OFF_EPI + se * EPI_SLOT);
+        double u0[5], res[5];
 #pragma unroll
-          for (int f = 0; f < 5; ++f) u0[f] = ep[f * EFS + eidx];
-          if (s == 0) {
+        for (int f = 0; f < 5; ++f) u0[f] = ep[f * EFS + eidx];
+        if (s == 0) {
 #pragma unroll
-            for (int f = 0; f < 5; ++f) res[f] = u0[f] + inc * kk5[f];
-            if (valid) {
+          for (int f = 0; f < 5; ++f) res[f] = u0[f] + inc * kk5[f];
+          if (valid) {
 #pragma unroll
-              for (int f = 0; f < 5; ++f) accb[f * NdF + nR] = kk5[f];
-            }
-          } else if (s < 3) {
-            double an[5];
+            for (int f = 0; f < 5; ++f) accb[f * NdF + nR] = kk5[f];
+          }
+        } else if (s < 3) {
+          double an[5];
 #pragma unroll
-            for (int f = 0; f < 5; ++f) {
-              an[f] = ep[(5 + f) * EFS + eidx] + 2 * kk5[f];
-              res[f] = u0[f] + inc * kk5[f];
-            }
-            if (valid) {
-#pragma unroll
-              for (int f = 0; f < 5; ++f) accb[f * NdF + nR] = an[f];
-            }
-          } else {
-#pragma unroll
-            for (int f = 0; f < 5; ++f) res[f] = u0[f] + dtFactor * (ep[(5 + f) * EFS + eidx] + kk5[f]);
-            const bool filtered = (tc & FILTER_BIT) != 0;  // rho, rho_E change again in the near-body filter
-#pragma unroll
-            for (int f = 0; f < 5; ++f) {
-              const double d = u0[f] - res[f];
-              nsum[f] += (valid && !(filtered && (f == 0 || f == 4))) ? d * d : 0.0;
-            }
-            bad |= valid && !(isfinite(res[0]) && isfinite(res[1]) && isfinite(res[2]) && isfinite(res[3]) &&
-                              isfinite(res[4]));
-            if (valid && !filtered) dt_terms(C, res, dta);
+          for (int f = 0; f < 5; ++f) {
+            an[f] = ep[(5 + f) * EFS + eidx] + 2 * kk5[f];
+            res[f] = u0[f] + inc * kk5[f];
           }
           if (valid) {
-            out0[nR] = res[0];
-            out1[nR] = res[1];
-            out2[nR] = res[2];
-            out3[nR] = res[3];
-            out4[nR] = res[4];
-            if (tc & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT)) {
-              // periodic z faces: this node's copy (PeriodicBoundary, Boundary.cpp:344-367) lands in the
-              // 32-byte sector just written; k = 1 feeds k = NK-1, k = NK-2 feeds k = 0. (Rows whose
-              // source is a filter node stay with the edge kernel, which adds the copy's dt terms.)
-              const long long m = (tc & ZCOPY_UP_BIT) ? nR + (G.NK - 2) : nR - (G.NK - 2);
-              out0[m] = res[0];
-              out1[m] = res[1];
-              out2[m] = res[2];
-              out3[m] = res[3];
-              out4[m] = res[4];
-            }
+#pragma unroll
+            for (int f = 0; f < 5; ++f) accb[f * NdF + nR] = an[f];
           }
-          __syncwarp();
-          if (lane == 0) {
-            mbar_arrive(&epiEmpty[se]);
-            mbar_arrive(&consEmpty[cR]);   // plane i0-3+a: its last reader was this RHS
-            mbar_arrive(&primEmpty[pW]);   // plane i0-4+a: read for the last time as the west plane
+        } else {
+#pragma unroll
+          for (int f = 0; f < 5; ++f) res[f] = u0[f] + dtFactor * (ep[(5 + f) * EFS + eidx] + kk5[f]);
+          const bool filtered = (tc & FILTER_BIT) != 0;  // rho, rho_E change again in the near-body filter
+#pragma unroll
+          for (int f = 0; f < 5; ++f) {
+            const double d = u0[f] - res[f];
+            nsum[f] += (valid && !(filtered && (f == 0 || f == 4))) ? d * d : 0.0;
           }
-          ++e;
-          nR += sI;
-          if (a == L + 1) {  // the item's last two planes' primitives, its last plane's conserved values
-            if (lane == 0) {
-              mbar_arrive(&consEmpty[cX]);
-              mbar_arrive(&primEmpty[pR]);
-              mbar_arrive(&primEmpty[pX]);
-            }
+          bad |= valid && !(isfinite(res[0]) && isfinite(res[1]) && isfinite(res[2]) && isfinite(res[3]) &&
+                            isfinite(res[4]));
+          if (valid && !filtered) dt_terms(C, res, dta);
+        }
+        if (valid) {
+          out0[nR] = res[0];
+          out1[nR] = res[1];
+          out2[nR] = res[2];
+          out3[nR] = res[3];
+          out4[nR] = res[4];
+          if (tc & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT)) {
+            // periodic z faces: this node's copy (PeriodicBoundary, Boundary.cpp:344-367) lands in the
+            // 32-byte sector just written; k = 1 feeds k = NK-1, k = NK-2 feeds k = 0. (Rows whose
+            // source is a filter node stay with the edge kernel, which adds the copy's dt terms.)
+            const long long m = (tc & ZCOPY_UP_BIT) ? nR + (G.NK - 2) : nR - (G.NK - 2);
+            out0[m] = res[0];
+            out1[m] = res[1];
+            out2[m] = res[2];
+            out3[m] = res[3];
+            out4[m] = res[4];
           }
         }
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&epiEmpty[se]);
+          mbar_arrive(&consEmpty[cR]);   // plane i0-3+a: its last reader was this RHS
+          mbar_arrive(&primEmpty[pW]);   // plane i0-4+a: read for the last time as the west plane
+          if (a == L + 1) {  // the item's last two planes' primitives, its last plane's conserved values
+            mbar_arrive(&consEmpty[cX]);
+            mbar_arrive(&primEmpty[pR]);
+            mbar_arrive(&primEmpty[pX]);
+          }
+        }
+        ++e;
+        nR += sI;
         gm2 = gm1;
         gm1 = gcur;
 #pragma unroll

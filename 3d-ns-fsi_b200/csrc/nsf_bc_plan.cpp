@@ -54,6 +54,12 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
   for (long long n : in.snode) wl[size_t(n)] = 1;  // solid-node copies: level 1
   int levels = in.snode.empty() ? 0 : 1;
   auto dev = [&](const int ijk[3]) { return (long long)ijk[0] * G.sI + (long long)ijk[1] * G.sJ + ijk[2]; };
+  // level a read of node r waits for: reads of solid nodes off the mesh faces go to the solid copy's source
+  // (ld_after_copy), so they wait for nothing
+  auto rdl = [&](long long r) {
+    const uint8_t t = in.typeDev[size_t(r)], k = t & TYPE_MASK;
+    return ((k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT)) ? 0 : int(wl[size_t(r)]);
+  };
   auto grow = [&](std::vector<std::vector<EdgeBlock>>& v, int L) {
     if (int(v.size()) < L) v.resize(size_t(L));
   };
@@ -103,7 +109,7 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
             reads.push_back(n + 2 * sgn * st);
           }
           int L = std::max(1 + int(wl[size_t(n)]), 1 + int(rl[size_t(n)]));  // after earlier writes and reads of n
-          for (long long r : reads) L = std::max(L, 1 + int(wl[size_t(r)]));
+          for (long long r : reads) L = std::max(L, 1 + rdl(r));
           for (long long r : reads) rl[size_t(r)] = int8_t(std::max(int(rl[size_t(r)]), L));
           written.push_back({n, int8_t(L)});
           if (int(maskOf.size()) < L) maskOf.resize(size_t(L), 0ull);
@@ -127,7 +133,7 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
     const long long n = in.fnode[size_t(f)];
     const long long nb[7] = {n, n + G.sI, n - G.sI, n + G.sJ, n - G.sJ, n + 1, n - 1};
     int L = 1;
-    for (long long r : nb) L = std::max(L, 1 + int(wl[size_t(r)]));
+    for (long long r : nb) L = std::max(L, 1 + rdl(r));
     for (long long r : nb) rl[size_t(r)] = int8_t(std::max(int(rl[size_t(r)]), L));
     lf[size_t(f)] = L;
   }
@@ -146,7 +152,7 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
       const long long c = in.gcell[8 * size_t(q) + m];
       const uint8_t t = in.typeDev[size_t(c)];
       if ((t & TYPE_MASK) == SOLID_GHOST) continue;
-      L = std::max(L, 1 + int(wl[size_t(c)]));
+      L = std::max(L, 1 + rdl(c));
       if (t & FILTER_BIT) L = std::max(L, 1 + lf[size_t(in.fidx[size_t(c)])]);
     }
     item(out.ghost, L, q);
@@ -157,7 +163,7 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
     item(out.ghost, std::max({1 + lf[size_t(f)], 1 + int(rl[n]), 1 + int(wl[n])}), nG + f);
   }
   // stage-4 dt terms of the solid inactive nodes (their stored values, or their copied conserved values)
-  for (int z = 0; z < nZ; ++z) item(out.ghost, 1 + int(wl[size_t(in.inode[size_t(z)])]), nG + nF + z);
+  for (int z = 0; z < nZ; ++z) item(out.ghost, 1 + rdl(in.inode[size_t(z)]), nG + nF + z);
   out.levels = levels;
   out.solid = (long long)in.snode.size();
   return levels;

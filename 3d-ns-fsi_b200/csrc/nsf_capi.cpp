@@ -517,7 +517,7 @@ nsf_status build_device(nsf_solver* s) {
       if ((st = upload(s, &L.bcEdgeStart, fl.edgeStart)) != NSF_OK) return st;
       if ((st = upload(s, &L.bcItems, fl.items)) != NSF_OK) return st;
       if ((st = upload(s, &L.bcItemStart, fl.itemStart)) != NSF_OK) return st;
-      const std::vector<unsigned> zero(2, 0u);
+      const std::vector<unsigned long long> zero(2, 0ull);
       if ((st = upload(s, &L.bcSync, zero)) != NSF_OK) return st;
     }
   }

@@ -159,7 +159,7 @@ struct BcParams {
   const int* edgeStart;
   const int* items;
   const int* itemStart;
-  unsigned* sync;  // grid barrier state: arrival count, generation
+  unsigned long long* sync;  // arrival counters: [0] the level barrier, [1 + g] member g's blocks done (stage 4)
   int levels, members;
 };
 
@@ -202,7 +202,7 @@ struct LaunchPlan {
   int* bcEdgeStart;
   int* bcItems;
   int* bcItemStart;
-  unsigned* bcSync;    // device, 2 words, zero at creation
+  unsigned long long* bcSync;  // device, 1 + members counters, zero at creation
   int nSlots;
   bool hasBodies;
   bool hasFilter, hasGhostWork, hasSolid;

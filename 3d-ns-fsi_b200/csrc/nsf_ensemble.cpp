@@ -273,8 +273,8 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
       if ((st = up(&L.bcEdgeStart, fl.edgeStart)) != NSF_OK) return st;
       if ((st = up(&L.bcItems, fl.items)) != NSF_OK) return st;
       if ((st = up(&L.bcItemStart, fl.itemStart)) != NSF_OK) return st;
-      if ((st = ens_alloc(e, &L.bcSync, 2)) != NSF_OK) return st;
-      CKE(cudaMemset(L.bcSync, 0, 2 * sizeof(unsigned)));
+      if ((st = ens_alloc(e, &L.bcSync, size_t(M) + 1)) != NSF_OK) return st;
+      CKE(cudaMemset(L.bcSync, 0, (size_t(M) + 1) * sizeof(unsigned long long)));
     }
   }
   // member grids: the stage kernel adds its norm partials into slot 0 of each member, the near-body

@@ -145,6 +145,18 @@ __device__ __forceinline__ void solid_copy_item(const Grid& G, const StepCtl* c,
     if (mask & (1 << f)) c->O[s][f][n] = __ldcg(c->I[s][f] + n);
 }
 
+// Field f at node m as the stage's boundary work reads it after the solid-node copy: a solid node off the
+// mesh faces (which nothing but the copy writes in a stage) is read from the copy's source, so a reader
+// does not have to wait for the copy; other nodes from the stage output. Values are the same either way.
+__device__ __forceinline__ double ld_after_copy(const Grid& G, const StepCtl* c, int s, int f, long long m) {
+  const double o = __ldcg(c->O[s][f] + m);
+  if (!(c->copyMask[s] & (1 << f))) return o;
+  const double src = __ldcg((f == 0 ? c->R[s] : c->I[s][f]) + m);
+  const uint8_t t = G.type[m];
+  const uint8_t k = t & TYPE_MASK;
+  return ((k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT)) ? src : o;
+}
+
 __global__ void k_solid_copy(const Grid* __restrict__ grids, int s) {
   const Grid* g = grids + blockIdx.y;
   const StepCtl* c = g->ctl;
@@ -202,7 +214,7 @@ __device__ __forceinline__ void edge_node(const Grid& G, const StepCtl* c, const
       const long long n = ijk[0] * G.sI + ijk[1] * G.sJ + ijk[2];
       const int side = G.eSide[e], bc = G.eBc[e];
       double* const* O = c->O[s];
-      auto ld = [&](int f, long long m) { return __ldcg(O[f] + m); };
+      auto ld = [&](int f, long long m) { return ld_after_copy(G, c, s, f, m); };
       const long long a1 = side == 0 ? n + st : n - st, a2 = side == 0 ? n + 2 * st : n - 2 * st;  // Boundary.cpp:74-108
       double cv[5];
       double u = 0, v = 0, w = 0, p = 0, T = 0;
@@ -312,13 +324,11 @@ __device__ __forceinline__ void filter_item(const Grid& G, const StepCtl* c, int
                                             int& bad) {
   double* const* O = c->O[s];
   const long long n = G.fnode[f];
-  const double* r = O[0];
-  const double* e = O[4];
-  const double rf = (6 * __ldcg(r + n) + __ldcg(r + n + G.sI) + __ldcg(r + n - G.sI) + __ldcg(r + n + G.sJ) +
-                     __ldcg(r + n - G.sJ) + __ldcg(r + n + 1) + __ldcg(r + n - 1)) / 12;
-  const double ef = (6 * __ldcg(e + n) + __ldcg(e + n + G.sI) + __ldcg(e + n - G.sI) + __ldcg(e + n + G.sJ) +
-                     __ldcg(e + n - G.sJ) + __ldcg(e + n + 1) + __ldcg(e + n - 1)) / 12;
-  const double r0 = __ldcg(r + n), e0 = __ldcg(e + n);
+  auto r = [&](long long m) { return ld_after_copy(G, c, s, 0, m); };
+  auto e = [&](long long m) { return ld_after_copy(G, c, s, 4, m); };
+  const double r0 = r(n), e0 = e(n);
+  const double rf = (6 * r0 + r(n + G.sI) + r(n - G.sI) + r(n + G.sJ) + r(n - G.sJ) + r(n + 1) + r(n - 1)) / 12;
+  const double ef = (6 * e0 + e(n + G.sI) + e(n - G.sI) + e(n + G.sJ) + e(n - G.sJ) + e(n + 1) + e(n - 1)) / 12;
   G.fpre[2 * f] = r0;
   G.fpre[2 * f + 1] = e0;
   G.fnew[2 * f] = rf;
@@ -408,9 +418,10 @@ __device__ __forceinline__ void ghost_pass_item(const Grid& G, const StepCtl* c,
     const int z = q - G.nGhost - G.nFilter;
     const long long n = G.inode[z];
     const double* pr = G.iprim + 5 * (long long)z;
-    const double r0 = __ldcg(O[0] + n);
+    const double r0 = ld_after_copy(G, c, s, 0, n);
     if (isnan(pr[0])) {  // periodic copy of a node whose primitives follow its conserved values
-      const Prim p = prims_of(C, r0, __ldcg(O[1] + n), __ldcg(O[2] + n), __ldcg(O[3] + n), __ldcg(O[4] + n));
+      const Prim p = prims_of(C, r0, ld_after_copy(G, c, s, 1, n), ld_after_copy(G, c, s, 2, n),
+                              ld_after_copy(G, c, s, 3, n), ld_after_copy(G, c, s, 4, n));
       dta.add(C, r0, p.u, p.v, p.w, p.p, p.mu);
     } else {
       dta.add(C, r0, pr[0], pr[1], pr[2], pr[3], pr[4]);
@@ -641,31 +652,34 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 // finalize. Every block passes every barrier (an inactive member's blocks do no work), so the launch is
 // cooperative (all blocks resident).
 
-// Bounded grid barrier over nb blocks (self-resetting: the last arriver clears the count and advances the
-// generation). A wait longer than kBarrierPolls polls sets StepCtl::timeout and goes on: the run is then
-// reported invalid, and nothing hangs.
+// Bounded grid barrier over nb blocks on a 64-bit arrival counter that only grows: every barrier instance
+// takes exactly nb arrivals, so an arrival that reads `old` belongs to instance old / nb and waits until
+// the counter reaches (old / nb + 1) * nb (release on arrival, acquire on the poll). A wait longer than
+// kBarrierPolls polls sets StepCtl::timeout and goes on: the run is then reported invalid, nothing hangs.
 constexpr long long kBarrierPolls = 1ll << 24;
-__device__ void grid_barrier(unsigned* S, unsigned nb, StepCtl* c) {
+__device__ __forceinline__ unsigned long long atom_add_release(unsigned long long* a, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.add.release.gpu.u64 %0, [%1], %2;" : "=l"(old) : "l"(a), "l"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* a) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(a) : "memory");
+  return v;
+}
+__device__ void grid_barrier(unsigned long long* S, unsigned nb, StepCtl* c) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = S + 1;
-    const unsigned g0 = *gen;
-    __threadfence();
-    if (atomicAdd(S, 1u) == nb - 1) {
-      atomicExch(S, 0u);
-      __threadfence();
-      atomicAdd(S + 1, 1u);
-    } else {
-      long long it = 0;
-      while (*gen == g0) {
-        if (++it > kBarrierPolls) {
-          atomicExch(&c->timeout, 1);
-          break;
-        }
-        __nanosleep(64);
+    const unsigned long long old = atom_add_release(S, 1ull);
+    const unsigned long long target = (old / nb + 1) * nb;
+    long long it = 0;
+    while (ld_acquire(S) < target) {
+      if (++it > kBarrierPolls) {
+        atomicExch(&c->timeout, 1);
+        break;
       }
+      __nanosleep(32);
     }
-    __threadfence();
   }
   __syncthreads();
 }
@@ -724,9 +738,16 @@ __global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__
     if (G.nFilter > 0) flush_norms(gp->normPart + 5 * (G.normSlotFilter + blockIdx.x), nsum, red);
     if (bad) atomicOr(&c->nonFinite, 1);
   }
-  if (fin) {
-    grid_barrier(P.sync, nb, c);
-    if (blockIdx.x == 0 && active) finalize_grid(gp, red);
+  if (fin) {  // the member's last block to get here runs its end-of-step finalize (no waiting)
+    __shared__ int last;
+    __syncthreads();
+    if (tid == 0) {
+      const unsigned long long old = atom_add_release(P.sync + 1 + g, 1ull);
+      last = (old + 1) % gridDim.x == 0;
+      if (last) (void)ld_acquire(P.sync + 1 + g);
+    }
+    __syncthreads();
+    if (last && active) finalize_grid(gp, red);
   }
 }
 

@@ -198,17 +198,40 @@ void bc_flatten(const std::vector<const BcMemberLevels*>& members, BcFlat& out) 
       start[M] = int(out.items.size());
     }
   }
-  // threads one member needs in a level (edge blocks count 64 threads each)
+  // threads one member needs for a level: all its items at once (edge blocks count 64 threads each; the
+  // solid-node copies run in the first level)
   long long work = 1;
+  out.work.assign(size_t(M), 1);
   for (int L = 0; L < levels; ++L)
     for (int g = 0; g < M; ++g) {
       const size_t eb = size_t(L) * (M + 1) + g, ib = size_t(L) * 2 * (M + 1) + g;
-      work = std::max<long long>(work, 64ll * (out.edgeStart[eb + 1] - out.edgeStart[eb]));
-      work = std::max<long long>(work, out.itemStart[ib + 1] - out.itemStart[ib]);
-      work = std::max<long long>(work, out.itemStart[ib + M + 2] - out.itemStart[ib + M + 1]);
+      long long w = 64ll * (out.edgeStart[eb + 1] - out.edgeStart[eb]);
+      w += out.itemStart[ib + 1] - out.itemStart[ib];
+      w += out.itemStart[ib + M + 2] - out.itemStart[ib + M + 1];
+      if (L == 0) w += members[g]->solid;
+      work = std::max(work, w);
+      out.work[size_t(g)] = std::max(out.work[size_t(g)], w);
     }
-  for (const BcMemberLevels* m : members) work = std::max<long long>(work, m->solid);
   out.maxWork = work;
+}
+
+std::vector<int> bc_block_ranges(const BcFlat& fl, int capacity) {
+  const int M = int(fl.work.size());
+  if (M == 0 || capacity < M) return {};
+  std::vector<int> n(size_t(M));
+  long long total = 0;
+  for (long long w : fl.work) total += w;
+  int used = 0;
+  for (int g = 0; g < M; ++g) {
+    const long long need = (fl.work[size_t(g)] + 255) / 256;
+    const long long share = (long long)((double)fl.work[size_t(g)] / double(total) * (capacity - M)) + 1;
+    n[size_t(g)] = int(std::max<long long>(1, std::min(need, share)));
+    used += n[size_t(g)];
+  }
+  std::vector<int> start(size_t(M) + 1, 0);
+  for (int g = 0; g < M; ++g) start[size_t(g) + 1] = start[size_t(g)] + n[size_t(g)];
+  (void)used;
+  return start;
 }
 
 }  // namespace nsf

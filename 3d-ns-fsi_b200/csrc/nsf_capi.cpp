@@ -508,10 +508,11 @@ nsf_status build_device(nsf_solver* s) {
   {  // fused boundary kernel: enough blocks for the busiest level, within what can be resident at once
     BcFlat fl;
     bc_flatten({&s->bcLevels}, fl);
-    const int cap = bc_capacity(s->nSM);
-    L.bcBlocks = cap > 0 ? int(std::max<long long>(1, std::min<long long>(cap, (fl.maxWork + 255) / 256))) : 0;
+    const std::vector<int> ranges = bc_block_ranges(fl, bc_capacity(s->nSM));
+    L.bcBlocks = ranges.empty() ? 0 : ranges.back();
     L.bcLevels = fl.levels;
     if (L.bcBlocks > 0) {
+      if ((st = upload(s, &L.bcBlockStart, ranges)) != NSF_OK) return st;
       L.filterBlocks = std::max(L.filterBlocks, L.bcBlocks);  // one norm slot per block of the fused kernel
       if ((st = upload(s, &L.bcEdges, fl.edges)) != NSF_OK) return st;
       if ((st = upload(s, &L.bcEdgeStart, fl.edgeStart)) != NSF_OK) return st;

@@ -160,6 +160,7 @@ struct BcParams {
   const int* items;
   const int* itemStart;
   unsigned long long* sync;  // arrival counters: [0] the level barrier, [1 + g] member g's blocks done (stage 4)
+  const int* blockStart;     // members + 1: the blocks of member g are blockStart[g] .. blockStart[g + 1] - 1
   int levels, members;
 };
 
@@ -178,7 +179,8 @@ struct BcMemberInput {  // device node indices (the padded device layout)
 };
 struct BcFlat {
   int levels = 0;
-  long long maxWork = 1;  // threads one member needs in its busiest level
+  long long maxWork = 1;         // threads one member needs in its busiest level (the largest over members)
+  std::vector<long long> work;   // the same per member
   std::vector<EdgeBlock> edges;
   std::vector<int> edgeStart, items, itemStart;
 };
@@ -193,10 +195,11 @@ struct LaunchPlan {
   EdgeBlock* edgeBlocks[3];  // device, per axis
   int nEdgeBlocks[3];
   int filterBlocks, ghostBlocks, solidBlocks, gfBlocks;
-  // Fused boundary kernel: per stage one cooperative launch of bcBlocks x members blocks that runs the
-  // stage's boundary work level by level with grid barriers between levels (and, on stage 4, the
-  // end-of-step finalize). 0: separate launches.
+  // Fused boundary kernel: per stage one cooperative launch of bcBlocks blocks (bcBlockStart: each member's
+  // range) that runs the stage's boundary work level by level with grid barriers between levels (and, on
+  // stage 4, the end-of-step finalize). 0: separate launches.
   int bcBlocks;
+  int* bcBlockStart;
   int bcLevels;
   EdgeBlock* bcEdges;  // device arrays of BcParams
   int* bcEdgeStart;
@@ -260,6 +263,10 @@ int bc_capacity(int nSM);
 int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], const BcMemberInput& in,
                    BcMemberLevels& out);
 void bc_flatten(const std::vector<const BcMemberLevels*>& members, BcFlat& out);
+// Blocks of 256 threads per member for a fused-kernel launch of at most `capacity` blocks, in proportion to
+// the members' work (at least one each, never more than a member can use); returns the members + 1 range
+// starts, empty if the members do not fit.
+std::vector<int> bc_block_ranges(const BcFlat& fl, int capacity);
 // The node a periodic face node finally copies (opposite interior plane, then further periodic faces).
 void periodic_source_host(const Grid& G, int axis, int side, int ijk[3]);
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,

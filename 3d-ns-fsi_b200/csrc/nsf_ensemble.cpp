@@ -255,11 +255,13 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
     for (nsf_solver* s : e->members) lv.push_back(&s->bcLevels);
     BcFlat fl;
     bc_flatten(lv, fl);
-    const int cap = bc_capacity(e->nSM) / M;
-    L.bcBlocks = cap > 0 ? int(std::min<long long>(cap, (fl.maxWork + 255) / 256)) : 0;
+    const std::vector<int> ranges = bc_block_ranges(fl, bc_capacity(e->nSM));
+    L.bcBlocks = ranges.empty() ? 0 : ranges.back();
     L.bcLevels = fl.levels;
     if (L.bcBlocks > 0) {
-      L.filterBlocks = std::max(L.filterBlocks, L.bcBlocks);
+      int widest = 1;  // the most blocks one member has: its norm slots
+      for (int g = 0; g < M; ++g) widest = std::max(widest, ranges[size_t(g) + 1] - ranges[size_t(g)]);
+      L.filterBlocks = std::max(L.filterBlocks, widest);
       auto up = [&](auto** p, const auto& v) -> nsf_status {
         nsf_status r = ens_alloc(e, p, v.size());
         if (r != NSF_OK) return r;
@@ -269,6 +271,7 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
         }
         return NSF_OK;
       };
+      if ((st = up(&L.bcBlockStart, ranges)) != NSF_OK) return st;
       if ((st = up(&L.bcEdges, fl.edges)) != NSF_OK) return st;
       if ((st = up(&L.bcEdgeStart, fl.edgeStart)) != NSF_OK) return st;
       if ((st = up(&L.bcItems, fl.items)) != NSF_OK) return st;

@@ -643,7 +643,8 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 
 // ----------------------------------------------------------------------------------------------
 // Fused boundary kernel: everything a stage does after its stage kernel, in one cooperative launch of
-// bcBlocks x members blocks (blockIdx.y = member), in the dependency levels of nsf_bc_plan.cpp: level 0
+// bcBlocks blocks (a consecutive range of them per member, sized by its work), in the dependency levels of
+// nsf_bc_plan.cpp: level 0
 // holds the solid-node copies and every edge, filter and ghost-pass item whose inputs are final after the
 // stage kernel; each later level reads what earlier levels wrote anywhere in the grid, so a grid barrier
 // separates levels and those reads go through L2 (__ldcg in the item functions). The member's Grid and
@@ -688,7 +689,19 @@ __global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__
   __shared__ double red[5 * 32];
   __shared__ __align__(16) unsigned char gsm[sizeof(Grid)];
   __shared__ __align__(16) unsigned char csm[sizeof(StepCtl)];
-  const int g = blockIdx.y, M = P.members, tid = threadIdx.x;
+  __shared__ int gShared;
+  const int M = P.members, tid = threadIdx.x;
+  if (tid == 0) {  // this block's member: blocks blockStart[g] .. blockStart[g + 1] - 1 work for member g
+    int lo = 0, hi = M;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) / 2;
+      if (P.blockStart[mid] <= int(blockIdx.x)) lo = mid; else hi = mid;
+    }
+    gShared = lo;
+  }
+  __syncthreads();
+  const int g = gShared;
+  const int bx = int(blockIdx.x) - P.blockStart[g], nbx = P.blockStart[g + 1] - P.blockStart[g];
   Grid* gp = grids + g;
   StepCtl* c = gp->ctl;  // global: atomics, flags and finalize write here
   {
@@ -703,31 +716,36 @@ __global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__
   const Grid& G = *reinterpret_cast<const Grid*>(gsm);
   const StepCtl& cs = *reinterpret_cast<const StepCtl*>(csm);  // read-only copy for the item functions
   const bool active = cs.active != 0;
-  const unsigned nb = gridDim.x * gridDim.y;
-  const int gtid = blockIdx.x * blockDim.x + tid, nthr = gridDim.x * blockDim.x, warp = tid >> 5;
+  const unsigned nb = gridDim.x;
+  const int gtid = bx * blockDim.x + tid, nthr = nbx * blockDim.x;
   DtAcc dta;
   double nsum[5] = {0, 0, 0, 0, 0};
   int bad = 0;
   const int ghostCount = ghost_pass_count(G, s);
+  // A level's items of every kind form one index range -- solid copies (level 0), edge-block threads (64
+  // per block), filter items, ghost-pass items -- and each thread takes every nthr-th index, so items of
+  // different kinds run side by side rather than one list after another.
   for (int L = 0; L < P.levels; ++L) {
     if (L > 0) grid_barrier(P.sync, nb, c);
     if (!active) continue;
-    if (L == 0 && cs.copyMask[s])
-      for (int q = gtid; q < G.nSolid; q += nthr) solid_copy_item(G, &cs, s, cs.copyMask[s], q);
-    {  // edge blocks (32 x 2 threads each), four per pass of this block
-      const int* es = P.edgeStart + L * (M + 1) + g;
-      const int e1 = es[1];
-      for (int b = es[0] + blockIdx.x * 4 + (warp >> 1); b < e1; b += gridDim.x * 4) {
-        const EdgeBlock eb = P.edges[b];
-        edge_node(G, &cs, eb, tid & 31, warp & 1, s, G.eAxis[eb.e], dta, bad);
-      }
-    }
-    {
-      const int* is = P.itemStart + (L * 2) * (M + 1) + g;
-      for (int q = is[0] + gtid; q < is[1]; q += nthr) filter_item(G, &cs, s, P.items[q], dta, nsum, bad);
-      is += M + 1;
-      for (int q = is[0] + gtid; q < is[1]; q += nthr) {
-        const int item = P.items[q];
+    const int mask = cs.copyMask[s];
+    const int nS = (L == 0 && mask) ? G.nSolid : 0;
+    const int* es = P.edgeStart + L * (M + 1) + g;
+    const int* fs = P.itemStart + (L * 2) * (M + 1) + g;
+    const int* hs = fs + (M + 1);
+    const int e0 = es[0], nE = 64 * (es[1] - e0), f0 = fs[0], nF = fs[1] - f0, h0 = hs[0], nH = hs[1] - h0;
+    const int total = nS + nE + nF + nH;
+    for (int v = gtid; v < total; v += nthr) {
+      if (v < nS) {
+        solid_copy_item(G, &cs, s, mask, v);
+      } else if (v < nS + nE) {
+        const int t = v - nS, lane = t & 63;
+        const EdgeBlock eb = P.edges[e0 + (t >> 6)];
+        edge_node(G, &cs, eb, lane & 31, lane >> 5, s, G.eAxis[eb.e], dta, bad);
+      } else if (v < nS + nE + nF) {
+        filter_item(G, &cs, s, P.items[f0 + v - nS - nE], dta, nsum, bad);
+      } else {
+        const int item = P.items[h0 + v - nS - nE - nF];
         if (item < ghostCount) ghost_pass_item(G, &cs, s, item, dta, bad);
       }
     }
@@ -735,7 +753,7 @@ __global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__
   if (s == 3) {
     flush_dt(c, dta, red);
     // one norm slot per block (a member has 1 + bcBlocks slots or more when a filter exists)
-    if (G.nFilter > 0) flush_norms(gp->normPart + 5 * (G.normSlotFilter + blockIdx.x), nsum, red);
+    if (G.nFilter > 0) flush_norms(gp->normPart + 5 * (G.normSlotFilter + bx), nsum, red);
     if (bad) atomicOr(&c->nonFinite, 1);
   }
   if (fin) {  // the member's last block to get here runs its end-of-step finalize (no waiting)
@@ -743,7 +761,7 @@ __global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__
     __syncthreads();
     if (tid == 0) {
       const unsigned long long old = atom_add_release(P.sync + 1 + g, 1ull);
-      last = (old + 1) % gridDim.x == 0;
+      last = (old + 1) % (unsigned long long)nbx == 0;
       if (last) (void)ld_acquire(P.sync + 1 + g);
     }
     __syncthreads();
@@ -758,10 +776,11 @@ static void launch_bc(Grid* dg, int members, const LaunchPlan& L, int s, bool fi
   P.items = L.bcItems;
   P.itemStart = L.bcItemStart;
   P.sync = L.bcSync;
+  P.blockStart = L.bcBlockStart;
   P.levels = L.bcLevels;
   P.members = members;
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(unsigned(L.bcBlocks), unsigned(members));
+  cfg.gridDim = dim3(unsigned(L.bcBlocks));
   cfg.blockDim = dim3(256);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = st;

@@ -218,7 +218,7 @@ void bc_flatten(const std::vector<const BcMemberLevels*>& members, BcFlat& out) 
 std::vector<int> bc_block_ranges(const BcFlat& fl, int capacity) {
   const int M = int(fl.work.size());
   if (M == 0 || capacity < M) return {};
-  std::vector<int> n(size_t(M));
+  std::vector<int> n(static_cast<size_t>(M));
   long long total = 0;
   for (long long w : fl.work) total += w;
   int used = 0;

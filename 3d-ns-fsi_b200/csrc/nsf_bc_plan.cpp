@@ -55,11 +55,12 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
   int levels = in.snode.empty() ? 0 : 1;
   auto dev = [&](const int ijk[3]) { return (long long)ijk[0] * G.sI + (long long)ijk[1] * G.sJ + ijk[2]; };
   // level a read of node r waits for: reads of solid nodes off the mesh faces go to the solid copy's source
-  // (ld_after_copy), so they wait for nothing
-  auto rdl = [&](long long r) {
+  // (ld_res; EdgeBlock::solidSrc, Grid::fsolid), so they wait for nothing
+  auto solidOff = [&](long long r) {
     const uint8_t t = in.typeDev[size_t(r)], k = t & TYPE_MASK;
-    return ((k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT)) ? 0 : int(wl[size_t(r)]);
+    return (k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT);
   };
+  auto rdl = [&](long long r) { return solidOff(r) ? 0 : int(wl[size_t(r)]); };
   auto grow = [&](std::vector<std::vector<EdgeBlock>>& v, int L) {
     if (int(v.size()) < L) v.resize(size_t(L));
   };
@@ -76,6 +77,7 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
       const int side = G.eSide[eb.e], bc = G.eBc[eb.e];
       const long long st = axis == 0 ? G.sI : axis == 1 ? G.sJ : 1;
       std::vector<unsigned long long> maskOf;  // per level
+      unsigned long long solidSrc = 0;
       for (int ty = 0; ty < kEdgeRows; ++ty)
         for (int tx = 0; tx < 32; ++tx) {
           const int a = eb.a0 + ty, bb = eb.b0 + tx;
@@ -108,6 +110,8 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
           } else {
             reads.push_back(n + 2 * sgn * st);
           }
+          for (long long r : reads)
+            if (solidOff(r)) solidSrc |= 1ull << (ty * 32 + tx);
           int L = std::max(1 + int(wl[size_t(n)]), 1 + int(rl[size_t(n)]));  // after earlier writes and reads of n
           for (long long r : reads) L = std::max(L, 1 + rdl(r));
           for (long long r : reads) rl[size_t(r)] = int8_t(std::max(int(rl[size_t(r)]), L));
@@ -120,6 +124,7 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
           grow(out.edges, int(L) + 1);
           EdgeBlock e2 = eb;
           e2.mask = maskOf[L];
+          e2.solidSrc = solidSrc & maskOf[L];
           out.edges[L].push_back(e2);
           levels = std::max(levels, int(L) + 1);
         }

@@ -275,6 +275,20 @@ nsf_status build_device(nsf_solver* s) {
     if ((st = upload(s, &dF, fidx)) != NSF_OK) return st;
     G.fidx = dF;
   }
+  {  // stencil nodes of each filter node that are solid nodes off the mesh faces (read from the copy's source)
+    std::vector<uint8_t> fsolid(fnode.size(), 0);
+    for (size_t q = 0; q < fnode.size(); ++q) {
+      const long long n = fnode[q];
+      const long long nb[7] = {n, n + G.sI, n - G.sI, n + G.sJ, n - G.sJ, n + 1, n - 1};
+      for (int b = 0; b < 7; ++b) {
+        const uint8_t t = typeDev[size_t(nb[b])], k = t & TYPE_MASK;
+        if ((k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT)) fsolid[q] |= uint8_t(1u << b);
+      }
+    }
+    uint8_t* dFs;
+    if ((st = upload(s, &dFs, fsolid)) != NSF_OK) return st;
+    G.fsolid = dFs;
+  }
   long long* dFnode;
   double *dFpre, *dFnew;
   if ((st = upload(s, &dFnode, fnode)) != NSF_OK) return st;

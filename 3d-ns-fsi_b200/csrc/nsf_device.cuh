@@ -90,6 +90,7 @@ struct Grid {
   const int* fidx;        // node -> filter slot (only read where FILTER_BIT is set)
   double* fpre;           // [F][2] pre-filter rho, rho_E of the last near-body filter
   double* fnew;           // [F][2] filtered values (written back after the ghost update)
+  const uint8_t* fsolid;  // [F] bit q: stencil node q (centre, +i, -i, +j, -j, +k, -k) is a solid node off the faces
   const long long* fnode; // [F] node of each filter slot
   int nFilter;
   // ghost nodes
@@ -143,6 +144,9 @@ struct EdgeBlock {
   int e;       // edge (face) of that member
   int a0, b0;  // first in-plane coordinates of the block: (a, bb) = the two axes other than the face's
   unsigned long long mask;  // thread ty * 32 + tx works iff its bit is set
+  // thread ty * 32 + tx reads a solid node off the mesh faces, whose value it takes from the solid-node
+  // copy's source (set by the fused boundary kernel's plan; 0 for the separate kernels)
+  unsigned long long solidSrc;
 };
 // The blocks of one axis' faces of a grid, in launch order, appended to out (member g). type: the host
 // node types with their flag bits (k fastest), or NULL. With G.zFused and a type array, the z faces'

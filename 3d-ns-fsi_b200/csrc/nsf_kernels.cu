@@ -145,16 +145,12 @@ __device__ __forceinline__ void solid_copy_item(const Grid& G, const StepCtl* c,
     if (mask & (1 << f)) c->O[s][f][n] = __ldcg(c->I[s][f] + n);
 }
 
-// Field f at node m as the stage's boundary work reads it after the solid-node copy: a solid node off the
-// mesh faces (which nothing but the copy writes in a stage) is read from the copy's source, so a reader
-// does not have to wait for the copy; other nodes from the stage output. Values are the same either way.
-__device__ __forceinline__ double ld_after_copy(const Grid& G, const StepCtl* c, int s, int f, long long m) {
-  const double o = __ldcg(c->O[s][f] + m);
-  if (!(c->copyMask[s] & (1 << f))) return o;
-  const double src = __ldcg((f == 0 ? c->R[s] : c->I[s][f]) + m);
-  const uint8_t t = G.type[m];
-  const uint8_t k = t & TYPE_MASK;
-  return ((k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT)) ? src : o;
+// Field f at node m as the stage's boundary work reads it after the solid-node copy. For a solid node off
+// the mesh faces (solid = true; nothing but the copy writes it in a stage) the value comes from the copy's
+// source, so the reader does not wait for the copy; the values are the same either way.
+__device__ __forceinline__ double ld_res(const StepCtl* c, int s, int f, long long m, bool solid) {
+  if (solid && (c->copyMask[s] & (1 << f))) return __ldcg((f == 0 ? c->R[s] : c->I[s][f]) + m);
+  return __ldcg(c->O[s][f] + m);
 }
 
 __global__ void k_solid_copy(const Grid* __restrict__ grids, int s) {
@@ -214,7 +210,8 @@ __device__ __forceinline__ void edge_node(const Grid& G, const StepCtl* c, const
       const long long n = ijk[0] * G.sI + ijk[1] * G.sJ + ijk[2];
       const int side = G.eSide[e], bc = G.eBc[e];
       double* const* O = c->O[s];
-      auto ld = [&](int f, long long m) { return ld_after_copy(G, c, s, f, m); };
+      const bool solidSrc = (eb.solidSrc >> (ty * 32 + tx)) & 1;
+      auto ld = [&](int f, long long m) { return ld_res(c, s, f, m, solidSrc); };
       const long long a1 = side == 0 ? n + st : n - st, a2 = side == 0 ? n + 2 * st : n - 2 * st;  // Boundary.cpp:74-108
       double cv[5];
       double u = 0, v = 0, w = 0, p = 0, T = 0;
@@ -324,11 +321,14 @@ __device__ __forceinline__ void filter_item(const Grid& G, const StepCtl* c, int
                                             int& bad) {
   double* const* O = c->O[s];
   const long long n = G.fnode[f];
-  auto r = [&](long long m) { return ld_after_copy(G, c, s, 0, m); };
-  auto e = [&](long long m) { return ld_after_copy(G, c, s, 4, m); };
-  const double r0 = r(n), e0 = e(n);
-  const double rf = (6 * r0 + r(n + G.sI) + r(n - G.sI) + r(n + G.sJ) + r(n - G.sJ) + r(n + 1) + r(n - 1)) / 12;
-  const double ef = (6 * e0 + e(n + G.sI) + e(n - G.sI) + e(n + G.sJ) + e(n - G.sJ) + e(n + 1) + e(n - 1)) / 12;
+  const unsigned sb = G.fsolid ? G.fsolid[f] : 0u;
+  auto r = [&](long long m, int q) { return ld_res(c, s, 0, m, (sb >> q) & 1); };
+  auto e = [&](long long m, int q) { return ld_res(c, s, 4, m, (sb >> q) & 1); };
+  const double r0 = r(n, 0), e0 = e(n, 0);
+  const double rf =
+      (6 * r0 + r(n + G.sI, 1) + r(n - G.sI, 2) + r(n + G.sJ, 3) + r(n - G.sJ, 4) + r(n + 1, 5) + r(n - 1, 6)) / 12;
+  const double ef =
+      (6 * e0 + e(n + G.sI, 1) + e(n - G.sI, 2) + e(n + G.sJ, 3) + e(n - G.sJ, 4) + e(n + 1, 5) + e(n - 1, 6)) / 12;
   G.fpre[2 * f] = r0;
   G.fpre[2 * f + 1] = e0;
   G.fnew[2 * f] = rf;
@@ -418,10 +418,10 @@ __device__ __forceinline__ void ghost_pass_item(const Grid& G, const StepCtl* c,
     const int z = q - G.nGhost - G.nFilter;
     const long long n = G.inode[z];
     const double* pr = G.iprim + 5 * (long long)z;
-    const double r0 = ld_after_copy(G, c, s, 0, n);
+    const double r0 = ld_res(c, s, 0, n, true);  // inactive nodes lie off the mesh faces
     if (isnan(pr[0])) {  // periodic copy of a node whose primitives follow its conserved values
-      const Prim p = prims_of(C, r0, ld_after_copy(G, c, s, 1, n), ld_after_copy(G, c, s, 2, n),
-                              ld_after_copy(G, c, s, 3, n), ld_after_copy(G, c, s, 4, n));
+      const Prim p = prims_of(C, r0, ld_res(c, s, 1, n, true), ld_res(c, s, 2, n, true), ld_res(c, s, 3, n, true),
+                              ld_res(c, s, 4, n, true));
       dta.add(C, r0, p.u, p.v, p.w, p.p, p.mu);
     } else {
       dta.add(C, r0, pr[0], pr[1], pr[2], pr[3], pr[4]);
@@ -822,7 +822,7 @@ void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vecto
             }
           if (!mask) continue;
         }
-        out.push_back(EdgeBlock{g, e, a0, b0, mask});
+        out.push_back(EdgeBlock{g, e, a0, b0, mask, 0ull});
       }
   }
 }

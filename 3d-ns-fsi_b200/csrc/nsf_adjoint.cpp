@@ -125,6 +125,8 @@ nsf_status setup(nsf_solver* s) {
     if (!ok) return fail(s, NSF_ERR_ARG, "the adjoint supports periodic faces and x-inlet/x-outlet faces only");
   }
   if (S.NI < 6 || S.NJ < 4 || S.NK < 4) return fail(s, NSF_ERR_ARG, "grid too small for the adjoint");
+  if (S.bodiesInteract)
+    return fail(s, NSF_ERR_ARG, "the adjoint supports immersed bodies that do not reach each other's nodes only");
   if (adj_kernels_init() != 0) return fail(s, NSF_ERR_CUDA, "adjoint kernel attributes could not be set");
   auto* a = new AdjCtx;
   s->adj = a;

@@ -48,21 +48,36 @@ void periodic_source_host(const Grid& G, int axis, int side, int ijk[3]) {
 
 int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], const BcMemberInput& in,
                    BcMemberLevels& out) {
-  const long long Nd = G.N;
-  std::vector<int8_t> wl(size_t(Nd), 0);   // level of the item writing a node in this stage (0: none)
-  std::vector<int8_t> rl(size_t(Nd), 0);   // highest level of an item reading a node's value before a write
-  for (long long n : in.snode) wl[size_t(n)] = 1;  // solid-node copies: level 1
+  const size_t Nd = size_t(G.N);
+  // Per node: level of the last item writing all five fields (solid copy, edge condition, ghost) and of the
+  // last filter write-back (rho and rho_E only); highest level of an item reading rho / rho_E, and the
+  // momenta, from the stage buffer (a later writer must come after it).
+  std::vector<int8_t> wA(Nd, 0), wR(Nd, 0), rR(Nd, 0), rM(Nd, 0);
+  for (long long n : in.snode) wA[size_t(n)] = 1;  // solid-node copies: level 1
   int levels = in.snode.empty() ? 0 : 1;
   auto dev = [&](const int ijk[3]) { return (long long)ijk[0] * G.sI + (long long)ijk[1] * G.sJ + ijk[2]; };
-  // level a read of node r waits for: reads of solid nodes off the mesh faces go to the solid copy's source
-  // (ld_res; EdgeBlock::solidSrc, Grid::fsolid), so they wait for nothing
+  // reads of solid nodes off the mesh faces go to the solid copy's source (ld_res; EdgeBlock::solidSrc,
+  // Grid::fsolid), so they wait for nothing
   auto solidOff = [&](long long r) {
     const uint8_t t = in.typeDev[size_t(r)], k = t & TYPE_MASK;
     return (k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT);
   };
-  auto rdl = [&](long long r) { return solidOff(r) ? 0 : int(wl[size_t(r)]); };
+  auto depR = [&](long long r) { return solidOff(r) ? 0 : std::max(int(wA[size_t(r)]), int(wR[size_t(r)])); };
+  auto depM = [&](long long r) { return solidOff(r) ? 0 : int(wA[size_t(r)]); };
+  auto readR = [&](long long r, int L) { rR[size_t(r)] = int8_t(std::max(int(rR[size_t(r)]), L)); };
+  auto readM = [&](long long r, int L) { rM[size_t(r)] = int8_t(std::max(int(rM[size_t(r)]), L)); };
+  // a write of every field at n: after every earlier write and read of it
+  auto afterAll = [&](long long n) {
+    const size_t q = size_t(n);
+    return 1 + std::max({int(wA[q]), int(wR[q]), int(rR[q]), int(rM[q])});
+  };
   auto grow = [&](std::vector<std::vector<EdgeBlock>>& v, int L) {
     if (int(v.size()) < L) v.resize(size_t(L));
+  };
+  auto item = [&](std::vector<std::vector<int>>& v, int L, int q) {
+    if (int(v.size()) < L) v.resize(size_t(L));
+    v[size_t(L - 1)].push_back(q);
+    levels = std::max(levels, L);
   };
   out.edges.clear();
   out.filter.clear();
@@ -110,11 +125,15 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
           } else {
             reads.push_back(n + 2 * sgn * st);
           }
-          for (long long r : reads)
+          int L = afterAll(n);
+          for (long long r : reads) {
             if (solidOff(r)) solidSrc |= 1ull << (ty * 32 + tx);
-          int L = std::max(1 + int(wl[size_t(n)]), 1 + int(rl[size_t(n)]));  // after earlier writes and reads of n
-          for (long long r : reads) L = std::max(L, 1 + rdl(r));
-          for (long long r : reads) rl[size_t(r)] = int8_t(std::max(int(rl[size_t(r)]), L));
+            L = std::max({L, 1 + depR(r), 1 + depM(r)});
+          }
+          for (long long r : reads) {
+            readR(r, L);
+            readM(r, L);
+          }
           written.push_back({n, int8_t(L)});
           if (int(maskOf.size()) < L) maskOf.resize(size_t(L), 0ull);
           maskOf[size_t(L - 1)] |= 1ull << (ty * 32 + tx);
@@ -129,46 +148,66 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
           levels = std::max(levels, int(L) + 1);
         }
     }
-    for (auto& w : written) wl[size_t(w.first)] = w.second;  // the next axis reads this axis' results
+    for (auto& w : written) wA[size_t(w.first)] = w.second;  // the next axis reads this axis' results
   }
-  // near-body filter (reads the 7-point stencil of every filter node)
+  // immersed bodies, one after another in the reference's order (Mesh.cpp:164-165): each body's filter
+  // (Jacobi: every filtered value from the values before any of that body's write-backs), its write-backs,
+  // then its ghosts
   const int nF = int(in.fnode.size()), nG = int(in.gnode.size()), nZ = int(in.inode.size());
+  int nBodies = 0;
+  for (int b : in.fbody) nBodies = std::max(nBodies, b + 1);
+  for (int b : in.gbody) nBodies = std::max(nBodies, b + 1);
   std::vector<int> lf(size_t(nF), 1);
-  for (int f = 0; f < nF; ++f) {
-    const long long n = in.fnode[size_t(f)];
-    const long long nb[7] = {n, n + G.sI, n - G.sI, n + G.sJ, n - G.sJ, n + 1, n - 1};
-    int L = 1;
-    for (long long r : nb) L = std::max(L, 1 + rdl(r));
-    for (long long r : nb) rl[size_t(r)] = int8_t(std::max(int(rl[size_t(r)]), L));
-    lf[size_t(f)] = L;
-  }
-  auto item = [&](std::vector<std::vector<int>>& v, int L, int q) {
-    if (int(v.size()) < L) v.resize(size_t(L));
-    v[size_t(L - 1)].push_back(q);
-    levels = std::max(levels, L);
-  };
-  for (int f = 0; f < nF; ++f) item(out.filter, lf[size_t(f)], f);
-  // ghosts: their corners (ghost corners carry zero weights and are not read), the filtered values of filter
-  // corners, and after every reader of the ghost node's old value
-  for (int q = 0; q < nG; ++q) {
-    const size_t gn = size_t(in.gnode[size_t(q)]);
-    int L = std::max(1 + int(rl[gn]), 1 + int(wl[gn]));  // after the solid-node copy and every old-value read
-    for (int m = 0; m < 8; ++m) {
-      const long long c = in.gcell[8 * size_t(q) + m];
-      const uint8_t t = in.typeDev[size_t(c)];
-      if ((t & TYPE_MASK) == SOLID_GHOST) continue;
-      L = std::max(L, 1 + rdl(c));
-      if (t & FILTER_BIT) L = std::max(L, 1 + lf[size_t(in.fidx[size_t(c)])]);
+  for (int body = 0; body < nBodies; ++body) {
+    for (int f = 0; f < nF; ++f) {
+      if (in.fbody[size_t(f)] != body) continue;
+      const long long n = in.fnode[size_t(f)];
+      const long long nb[7] = {n, n + G.sI, n - G.sI, n + G.sJ, n - G.sJ, n + 1, n - 1};
+      int L = 1;
+      for (long long r : nb) L = std::max(L, 1 + depR(r));
+      // the node's earlier slot wrote fpre / fnew and (stage 4) this slot reads its fpre
+      if (in.fidx[size_t(n)] != f) L = std::max(L, 1 + lf[size_t(in.fidx[size_t(n)])]);
+      for (long long r : nb) readR(r, L);
+      readM(n, L);  // stage 4 reads the node's momenta
+      lf[size_t(f)] = L;
+      item(out.filter, L, f);
     }
-    item(out.ghost, L, q);
-  }
-  // filter write-back: after its own filter item and every reader of the node's old value
-  for (int f = 0; f < nF; ++f) {
-    const size_t n = size_t(in.fnode[size_t(f)]);
-    item(out.ghost, std::max({1 + lf[size_t(f)], 1 + int(rl[n]), 1 + int(wl[n])}), nG + f);
+    for (int f = 0; f < nF; ++f) {
+      if (in.fbody[size_t(f)] != body) continue;
+      const size_t n = size_t(in.fnode[size_t(f)]);
+      const int L = std::max({1 + lf[size_t(f)], 1 + int(wA[n]), 1 + int(wR[n]), 1 + int(rR[n])});
+      wR[n] = int8_t(L);
+      item(out.ghost, L, nG + f);
+    }
+    for (int q = 0; q < nG; ++q) {
+      if (in.gbody[size_t(q)] != body) continue;
+      const long long gn = in.gnode[size_t(q)];
+      int L = afterAll(gn);
+      std::vector<std::pair<long long, bool>> rd;  // corner, reads rho / rho_E from the stage buffer
+      for (int m = 0; m < 8; ++m) {
+        const long long c = in.gcell[8 * size_t(q) + m];
+        if ((in.typeDev[size_t(c)] & TYPE_MASK) == SOLID_GHOST) continue;  // zero weights: not read
+        const int src = in.gsrc[8 * size_t(q) + m];
+        L = std::max(L, 1 + depM(c));
+        if (src >= 0)
+          L = std::max(L, 1 + lf[size_t(src)]);
+        else
+          L = std::max(L, 1 + depR(c));
+        rd.push_back({c, src < 0});
+      }
+      for (auto& r : rd) {
+        readM(r.first, L);
+        if (r.second) readR(r.first, L);
+      }
+      wA[size_t(gn)] = int8_t(L);
+      item(out.ghost, L, q);
+    }
   }
   // stage-4 dt terms of the solid inactive nodes (their stored values, or their copied conserved values)
-  for (int z = 0; z < nZ; ++z) item(out.ghost, 1 + rdl(in.inode[size_t(z)]), nG + nF + z);
+  for (int z = 0; z < nZ; ++z) {
+    const long long n = in.inode[size_t(z)];
+    item(out.ghost, 1 + std::max(depR(n), depM(n)), nG + nF + z);
+  }
   out.levels = levels;
   out.solid = (long long)in.snode.size();
   return levels;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -222,9 +223,15 @@ nsf_status build_device(nsf_solver* s) {
     for (size_t i = e.owned.i0; i <= e.owned.i1; ++i)
       for (size_t j = e.owned.j0; j <= e.owned.j1; ++j)
         for (size_t k = e.owned.k0; k <= e.owned.k1; ++k) type[i * S.NJ * S.NK + j * S.NK + k] |= EDGE_PLANE_BIT;
-  std::vector<long long> fnode;
-  for (auto& b : S.bodies)
-    for (size_t f : b.filter) fnode.push_back((long long)f);
+  std::vector<long long> fnode;  // filter slots: one per (body, node), in body order
+  std::vector<int> fbody;
+  for (size_t q = 0; q < S.bodies.size(); ++q)
+    for (size_t f : S.bodies[q].filter) {
+      fnode.push_back((long long)f);
+      fbody.push_back(int(q));
+    }
+  std::map<long long, std::vector<int>> slotsOf;  // host node -> its filter slots (body order)
+  for (size_t q = 0; q < fnode.size(); ++q) slotsOf[fnode[q]].push_back(int(q));
   std::vector<double> fpre(2 * fnode.size());
   for (size_t q = 0; q < fnode.size(); ++q) {
     type[fnode[q]] |= FILTER_BIT;
@@ -269,11 +276,21 @@ nsf_status build_device(nsf_solver* s) {
   G.nFilter = int(fnode.size());
   std::vector<int> fidx;
   if (!fnode.empty()) {
-    fidx.assign(Nd, -1);
-    for (size_t q = 0; q < fnode.size(); ++q) fidx[fnode[q]] = int(q);
+    fidx.assign(Nd, -1);  // a node's first slot (the stage kernel takes its pre-filter values from it)
+    for (size_t q = 0; q < fnode.size(); ++q)
+      if (fidx[fnode[q]] < 0) fidx[fnode[q]] = int(q);
     int* dF;
     if ((st = upload(s, &dF, fidx)) != NSF_OK) return st;
     G.fidx = dF;
+  }
+  {  // per slot: the node's first slot, and whether this is its last
+    std::vector<int> fmeta(fnode.size());
+    for (const auto& kv : slotsOf)
+      for (size_t r = 0; r < kv.second.size(); ++r)
+        fmeta[size_t(kv.second[r])] = kv.second[0] | (r + 1 == kv.second.size() ? FMETA_LAST : 0);
+    int* dFm;
+    if ((st = upload(s, &dFm, fmeta)) != NSF_OK) return st;
+    G.fmeta = dFm;
   }
   {  // stencil nodes of each filter node that are solid nodes off the mesh faces (read from the copy's source)
     std::vector<uint8_t> fsolid(fnode.size(), 0);
@@ -301,9 +318,12 @@ nsf_status build_device(nsf_solver* s) {
   // ghost nodes: cells and the points / normals the weight solve needs
   std::vector<long long> gnode, gcell;
   std::vector<double> pts, nrm, ipl;
-  std::vector<uint8_t> gfl;
-  for (auto& b : S.bodies)
-    for (auto& g : b.ghosts) {
+  std::vector<uint8_t> gfl, glast;
+  std::vector<int> gbody, gsrc;
+  for (size_t bq = 0; bq < S.bodies.size(); ++bq)
+    for (auto& g : S.bodies[bq].ghosts) {
+      const auto& b = S.bodies[bq];
+      gbody.push_back(int(bq));
       gnode.push_back(dev(g.i * S.NJ * S.NK + g.j * S.NK + g.k));
       Box box;
       surrounding_box(S, g.ip, box);
@@ -316,6 +336,14 @@ nsf_status build_device(nsf_solver* s) {
       for (int m = 0; m < 8; ++m) {
         gcell.push_back(dev(size_t(cs[m])));
         const size_t cn = size_t(cs[m]);
+        {  // filtered values this ghost reads at a filter corner: the last slot of a body up to its own
+          int src = -1;
+          auto it = slotsOf.find((long long)cn);
+          if (it != slotsOf.end())
+            for (int sl : it->second)
+              if (fbody[size_t(sl)] <= int(bq)) src = sl;
+          gsrc.push_back(src);
+        }
         if (S.type[cn] == SOLID_GHOST) {
           const GhostRec& og = b.ghosts[b.ghostIndex.at(cn)];
           double d[3] = {og.ip[0] - og.bi[0], og.ip[1] - og.bi[1], og.ip[2] - og.bi[2]};
@@ -333,6 +361,15 @@ nsf_status build_device(nsf_solver* s) {
         }
       }
     }
+  {  // a ghost item is its node's last writer unless a later body's ghost list holds the node too
+    glast.assign(gnode.size(), 1);
+    std::map<long long, size_t> lastOf;
+    for (size_t q = 0; q < gnode.size(); ++q) {
+      auto it = lastOf.find(gnode[q]);
+      if (it != lastOf.end()) glast[it->second] = 0;
+      lastOf[gnode[q]] = q;
+    }
+  }
   {  // device order of the ghosts: by image-point cell (first corner), so the lanes of a warp gather
      // overlapping corner sets; s->ghostOrder[q] = the ghost's position in the bodies' own order
     const size_t ng = gnode.size();
@@ -351,6 +388,9 @@ nsf_status build_device(nsf_solver* s) {
     permute(nrm, 24);
     permute(ipl, 6);
     permute(gfl, 8);
+    permute(gbody, 1);
+    permute(glast, 1);
+    permute(gsrc, 8);
     s->ghostOrder = ord;
   }
   G.nGhost = int(gnode.size());
@@ -369,6 +409,14 @@ nsf_status build_device(nsf_solver* s) {
   G.gnode = dGnode;
   G.gcell = dGcell;
   G.gw = dW;
+  {
+    int* dGs;
+    uint8_t* dGl;
+    if ((st = upload(s, &dGs, gsrc)) != NSF_OK) return st;
+    if ((st = upload(s, &dGl, glast)) != NSF_OK) return st;
+    G.gsrc = dGs;
+    G.glast = dGl;
+  }
 
   // solid nodes: copy list (ghost + inactive); inactive primitive values as the reference holds them
   std::vector<long long> snode, inode, dlNode, dlNodeIc;
@@ -509,6 +557,9 @@ nsf_status build_device(nsf_solver* s) {
     in.inode = inode;
     in.typeDev = typeDev;
     in.fidx = fidx;
+    in.fbody = fbody;
+    in.gbody = gbody;
+    in.gsrc = gsrc;
     bc_plan_member(G, ebAxis, in, s->bcLevels);
   }
   L.hasFilter = G.nFilter > 0;
@@ -535,6 +586,10 @@ nsf_status build_device(nsf_solver* s) {
       const std::vector<unsigned long long> zero(2, 0ull);
       if ((st = upload(s, &L.bcSync, zero)) != NSF_OK) return st;
     }
+  }
+  if (S.bodiesInteract && L.bcBlocks == 0) {  // the separate boundary kernels treat all bodies at once
+    s->err = "interacting immersed bodies need the fused boundary kernel, which this device cannot host";
+    return NSF_ERR_GEOMETRY;
   }
   L.nSlots = L.stageBlocks + (L.hasFilter ? L.filterBlocks : 0);
   double* dNorm;
@@ -671,6 +726,13 @@ nsf_status nsf_debug_wait_limit(nsf_solver* s, uint64_t polls, int32_t withhold_
   char* base = reinterpret_cast<char*>(s->dCtl);
   CK(cudaMemcpy(base + offsetof(StepCtl, waitLimit), &lim, sizeof lim, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(base + offsetof(StepCtl, withhold), &wh, sizeof wh, cudaMemcpyHostToDevice));
+  return NSF_OK;
+}
+
+nsf_status nsf_get_body_interaction(nsf_solver* s, int32_t* interact) {
+  if (!s || !interact) return NSF_ERR_ARG;
+  if (!s->initialized) return NSF_ERR_STATE;
+  *interact = s->setup.bodiesInteract ? 1 : 0;
   return NSF_OK;
 }
 

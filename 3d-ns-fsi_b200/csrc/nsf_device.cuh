@@ -91,6 +91,10 @@ struct Grid {
   double* fpre;           // [F][2] pre-filter rho, rho_E of the last near-body filter
   double* fnew;           // [F][2] filtered values (written back after the ghost update)
   const uint8_t* fsolid;  // [F] bit q: stencil node q (centre, +i, -i, +j, -j, +k, -k) is a solid node off the faces
+  // [F] filter slots are per (body, node) in body order; fmeta = the node's first slot, | FMETA_LAST on its
+  // last slot (a node filtered by two bodies has two slots: the stage kernel's pre-filter values come from
+  // the first, the stage-4 dt and norm terms from the last)
+  const int* fmeta;
   const long long* fnode; // [F] node of each filter slot
   int nFilter;
   // ghost nodes
@@ -98,6 +102,10 @@ struct Grid {
   const long long* gnode;   // [G]
   const long long* gcell;   // [G][8]
   const double* gw;         // [G][16]: Neumann weights (rho, rho_E) then Dirichlet weights (momenta)
+  // [G][8]: per corner, the filter slot whose filtered rho, rho_E the ghost reads (the last slot of a body
+  // up to the ghost's own in body order), or -1: read the node's current value
+  const int* gsrc;
+  const uint8_t* glast;     // [G]: 1 if no later ghost item writes the same node (it adds the stage-4 dt terms)
   // solid-node copy list (ghost + inactive) and the inactive nodes' stored primitive values
   int nSolid;
   const long long* snode;   // [S]
@@ -178,6 +186,7 @@ struct BcMemberLevels {
 };
 struct BcMemberInput {  // device node indices (the padded device layout)
   std::vector<long long> snode, fnode, gnode, gcell, inode;
+  std::vector<int> fbody, gbody, gsrc;  // body of each filter slot and ghost; ghost corner sources (Grid::gsrc)
   std::vector<uint8_t> typeDev;  // node types with FILTER_BIT, per device node
   std::vector<int> fidx;         // filter slot per device node, or -1
 };

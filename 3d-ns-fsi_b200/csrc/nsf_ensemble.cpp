@@ -258,6 +258,13 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
     const std::vector<int> ranges = bc_block_ranges(fl, bc_capacity(e->nSM));
     L.bcBlocks = ranges.empty() ? 0 : ranges.back();
     L.bcLevels = fl.levels;
+    if (L.bcBlocks == 0)
+      for (nsf_solver* s : e->members)
+        if (s->setup.bodiesInteract) {
+          e->err = "ensemble members with interacting immersed bodies need the fused boundary kernel, and the "
+                   "members do not fit one launch of it";
+          return NSF_ERR_GEOMETRY;
+        }
     if (L.bcBlocks > 0) {
       int widest = 1;  // the most blocks one member has: its norm slots
       for (int g = 0; g < M; ++g) widest = std::max(widest, ranges[size_t(g) + 1] - ranges[size_t(g)]);

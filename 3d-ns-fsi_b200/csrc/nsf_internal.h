@@ -23,6 +23,7 @@ constexpr uint8_t EDGE_PLANE_BIT = 0x40;  // node lies in a mesh-edge boundary's
 // k = NK-2 (DOWN), whose value the stage kernel also writes to its periodic copy at k = NK-1 or k = 0.
 constexpr uint8_t ZCOPY_UP_BIT = 0x20;
 constexpr uint8_t ZCOPY_DOWN_BIT = 0x10;
+constexpr int FMETA_LAST = 1 << 30;  // Grid::fmeta: this slot is its node's last
 
 struct Box {  // IndexBoundingBox, src/SmallVectors.h:72-104 (inclusive bounds)
   size_t i0, i1, j0, j1, k0, k1;
@@ -56,6 +57,10 @@ struct HostSetup {
   std::vector<uint8_t> type;  // NodeTypeEnum per node
   std::vector<EdgeBC> edges;  // application order (reverse of the claim order)
   std::vector<BodyRec> bodies;
+  // Immersed bodies that act on each other's nodes within a stage (a node in two bodies' lists, a filter
+  // stencil or an image-point cell reaching another body's filter node): they must run in the reference's
+  // body order, which the fused boundary kernel's dependency levels provide.
+  bool bodiesInteract = false;
 };
 
 // Setup entry points (nsf_setup.cpp). Return NSF_OK or an error with a message in `err`.

@@ -333,8 +333,14 @@ __device__ __forceinline__ void filter_item(const Grid& G, const StepCtl* c, int
   G.fpre[2 * f + 1] = e0;
   G.fnew[2 * f] = rf;
   G.fnew[2 * f + 1] = ef;
-  if (s == 3) {
-    const Prim q = prims_of(G.C, r0, __ldcg(O[1] + n), __ldcg(O[2] + n), __ldcg(O[3] + n), e0);
+  // stage 4: the node's dt and change-norm terms, once, from its last slot (a node two bodies filter has
+  // two): the final filtered values, and primitives from the values before the node's first filter
+  const int meta = G.fmeta ? G.fmeta[f] : (f | FMETA_LAST);
+  if (s == 3 && (meta & FMETA_LAST)) {
+    const int first = meta & ~FMETA_LAST;
+    const double p0 = first == f ? r0 : __ldcg(G.fpre + 2 * first);
+    const double p4 = first == f ? e0 : __ldcg(G.fpre + 2 * first + 1);
+    const Prim q = prims_of(G.C, p0, __ldcg(O[1] + n), __ldcg(O[2] + n), __ldcg(O[3] + n), p4);
     dta.add(G.C, rf, q.u, q.v, q.w, q.p, q.mu);
     const double d0 = c->U0[0][n] - rf, d4 = c->U0[4][n] - ef;
     nsum[0] += d0 * d0;
@@ -385,8 +391,8 @@ __device__ __forceinline__ void ghost_pass_item(const Grid& G, const StepCtl* c,
       wd[m] = w[8 + m];
 #pragma unroll
       for (int f = 0; f < 5; ++f) v[m][f] = __ldcg(O[f] + cn);
-      if (G.type[cn] & FILTER_BIT) {
-        const int fi = G.fidx[cn];
+      const int fi = G.gsrc[8 * (long long)q + m];  // a filter corner: the filtered values it sees
+      if (fi >= 0) {
         v[m][0] = __ldcg(G.fnew + 2 * fi);
         v[m][4] = __ldcg(G.fnew + 2 * fi + 1);
       }
@@ -404,7 +410,7 @@ __device__ __forceinline__ void ghost_pass_item(const Grid& G, const StepCtl* c,
     const double gc[5] = {ip[0], -ip[1], -ip[2], -ip[3], ip[4]};
     const long long n = G.gnode[q];
     for (int f = 0; f < 5; ++f) O[f][n] = gc[f];
-    if (s == 3) {
+    if (s == 3 && G.glast[q]) {  // a node in two bodies' ghost lists: the dt terms of its final values
       const Prim p = prims_of(C, gc[0], gc[1], gc[2], gc[3], gc[4]);
       dta.add(C, gc[0], p.u, p.v, p.w, p.p, p.mu);
       for (int f = 0; f < 5; ++f) bad |= !isfinite(gc[f]);

@@ -300,16 +300,27 @@ nsf_status build_setup(const nsf_config& cfg, HostSetup& s, std::string& err) {
     if (st != NSF_OK) return st;
   }
 
-  // Checks for cases the reference cannot run: a solid node inside an image-point cell
-  // (Boundary.cpp:723-724 throws), and bodies close enough to read each other's ghost or filter nodes.
+  // Checks. The reference cannot run a solid inactive node inside an image-point cell (it throws,
+  // Boundary.cpp:723-724) nor another body's ghost node there (its ghost lookup, Boundary.cpp:681, throws
+  // std::out_of_range); both are refused. Bodies that otherwise reach each other's nodes -- a node filtered
+  // by two bodies, a ghost shared by two bodies, a filter stencil or an image-point cell touching another
+  // body's ghost or filter nodes -- run in the reference's body order (bodiesInteract). Refused as well: a
+  // filter node of one body that a later body made solid, whose stale primitive values (the reference never
+  // recomputes them at a filter node) the device does not keep for solid nodes.
   std::vector<int> owner(s.N, -1);
+  s.bodiesInteract = false;
   for (size_t q = 0; q < s.bodies.size(); ++q) {
-    for (auto& g : s.bodies[q].ghosts) owner[lin(s, g.i, g.j, g.k)] = int(q);
+    for (auto& g : s.bodies[q].ghosts) {
+      const size_t n = lin(s, g.i, g.j, g.k);
+      if (owner[n] >= 0 && owner[n] != int(q)) s.bodiesInteract = true;
+      owner[n] = int(q);
+    }
     for (size_t f : s.bodies[q].filter) {
-      if (owner[f] >= 0 && owner[f] != int(q)) {
-        err = "immersed bodies are too close: their ghost/filter layers overlap";
+      if (s.type[f] != FLUID_INTERIOR) {
+        err = "immersed bodies are too close: a filter node of one body lies inside another";
         return NSF_ERR_GEOMETRY;
       }
+      if (owner[f] >= 0 && owner[f] != int(q)) s.bodiesInteract = true;
       owner[f] = int(q);
     }
   }
@@ -318,10 +329,7 @@ nsf_status build_setup(const nsf_config& cfg, HostSetup& s, std::string& err) {
     for (size_t f : s.bodies[q].filter)
       for (long o : {sI, -sI, sJ, -sJ, 1L, -1L}) {
         long nb = long(f) + o;
-        if (owner[nb] >= 0 && owner[nb] != int(q)) {
-          err = "immersed bodies are too close: a filter stencil reaches another body";
-          return NSF_ERR_GEOMETRY;
-        }
+        if (owner[nb] >= 0 && owner[nb] != int(q)) s.bodiesInteract = true;
       }
     for (auto& g : s.bodies[q].ghosts) {
       Box box;
@@ -334,14 +342,11 @@ nsf_status build_setup(const nsf_config& cfg, HostSetup& s, std::string& err) {
           err = "Impossible situation. Found solid node around image point.";
           return NSF_ERR_GEOMETRY;
         }
-        if (owner[cn] >= 0 && owner[cn] != int(q)) {
-          err = "immersed bodies are too close: an image-point cell reaches another body";
-          return NSF_ERR_GEOMETRY;
-        }
         if (t == SOLID_GHOST && !s.bodies[q].ghostIndex.count(size_t(cn))) {
-          err = "immersed bodies are too close: an image-point cell holds another body's ghost";
+          err = "an image-point cell holds another body's ghost node (the reference's ghost lookup fails there)";
           return NSF_ERR_GEOMETRY;
         }
+        if (owner[cn] >= 0 && owner[cn] != int(q)) s.bodiesInteract = true;
       }
     }
   }

@@ -84,6 +84,7 @@ def lib():
         "nsf_get_node_types": (i32, [vp, ctypes.POINTER(ctypes.c_uint8)]),
         "nsf_get_geometry": (i32, [vp, dp]),
         "nsf_get_num_bodies": (i32, [vp, ctypes.POINTER(u32)]),
+        "nsf_get_body_interaction": (i32, [vp, ctypes.POINTER(i32)]),
         "nsf_get_body_counts": (i32, [vp, u32, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]),
         "nsf_get_ghosts": (i32, [vp, u32, dp]),
         "nsf_get_filter_nodes": (i32, [vp, u32, ctypes.POINTER(u64)]),
@@ -251,6 +252,12 @@ class Solver:
                 self._check(L.nsf_get_filter_nodes(self.h, b, f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
             res.append((g, f, cl.value))
         return res
+
+    def bodies_interact(self):
+        """True if immersed bodies reach each other's nodes (nsf_get_body_interaction)."""
+        v = ctypes.c_int32()
+        self._check(lib().nsf_get_body_interaction(self.h, ctypes.byref(v)))
+        return bool(v.value)
 
     def history(self, first=0, count=None):
         avail = ctypes.c_uint64()

@@ -141,6 +141,10 @@ nsf_status nsf_get_geometry(nsf_solver* s, double* out);
 nsf_status nsf_get_num_bodies(nsf_solver* s, uint32_t* nbodies);
 nsf_status nsf_get_body_counts(nsf_solver* s, uint32_t body, uint64_t* nghost, uint64_t* nfilter,
                                uint64_t* closure_added);
+/* *interact = 1 if immersed bodies reach each other's nodes (a node in two bodies' ghost or filter lists, a
+ * filter stencil or an image-point cell touching another body's ghost or filter nodes); such bodies act in
+ * the reference's body order, one after another in every stage (Mesh.cpp:164-165). */
+nsf_status nsf_get_body_interaction(nsf_solver* s, int32_t* interact);
 /* Per ghost, 9 doubles: i, j, k, body-intercept x,y,z, image point x,y,z (GhostNode, Node.h:15-22). */
 nsf_status nsf_get_ghosts(nsf_solver* s, uint32_t body, double* out);
 /* Filter-node indices of a body (ImmersedBoundary::filterNodes, Boundary.h:208). */

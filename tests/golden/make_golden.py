@@ -29,6 +29,7 @@ CASES = {
     "sphere_small": ("tests/golden/cases/sphere_small.cfg", [7, 30], None),
     "tgv_small": ("tests/golden/cases/tgv_small.cfg", [25], None),
     "two_spheres": ("tests/golden/cases/two_spheres.cfg", [20], None),
+    "close_spheres": ("tests/golden/cases/close_spheres.cfg", [6, 20], None),
     "cylinder_sym": ("tests/golden/cases/cylinder_sym.cfg", [4, 60], None),
     "shipped_small": ("tests/golden/cases/shipped_small.cfg", [40], None),
     "sphere48": ("3d-ns-fsi_b200/cases/sphere48.cfg", [100], 13),

@@ -18,6 +18,7 @@ CASES = {
     "sphere_small": "tests/golden/cases/sphere_small.cfg",
     "tgv_small": "tests/golden/cases/tgv_small.cfg",
     "two_spheres": "tests/golden/cases/two_spheres.cfg",
+    "close_spheres": "tests/golden/cases/close_spheres.cfg",
     "cylinder_sym": "tests/golden/cases/cylinder_sym.cfg",
     "shipped_small": "tests/golden/cases/shipped_small.cfg",
     "sphere48": "3d-ns-fsi_b200/cases/sphere48.cfg",

@@ -24,6 +24,7 @@ SMALL = {
     "sphere_small": "tests/golden/cases/sphere_small.cfg",
     "tgv_small": "tests/golden/cases/tgv_small.cfg",
     "two_spheres": "tests/golden/cases/two_spheres.cfg",
+    "close_spheres": "tests/golden/cases/close_spheres.cfg",
     "cylinder_sym": "tests/golden/cases/cylinder_sym.cfg",
     "shipped_small": "tests/golden/cases/shipped_small.cfg",
 }

@@ -77,3 +77,23 @@ def test_ensemble_workload_members_are_valid_cases():
 def test_ensemble_needs_a_device():
     with pytest.raises(nsfsi.NsfError):
         nsfsi.Ensemble(nsfsi.ensemble_configs(n=2))
+
+
+def test_interacting_bodies_run_and_are_flagged():
+    """Two spheres whose filter layers overlap (48 nodes filtered by both) run, flagged as interacting;
+    the well-separated pair does not interact."""
+    with Solver(os.path.join(ROOT, "tests", "golden", "cases", "close_spheres.cfg"), device=-1) as s:
+        assert s.bodies_interact()
+        (g1, f1, _), (g2, f2, _) = s.bodies()
+        assert len(set(f1.tolist()) & set(f2.tolist())) > 0
+    with Solver(os.path.join(ROOT, "tests", "golden", "cases", "two_spheres.cfg"), device=-1) as s:
+        assert not s.bodies_interact()
+
+
+def test_filter_node_inside_a_later_body_is_refused():
+    """A gap so small that a later sphere makes one of the first sphere's filter nodes solid."""
+    text = open(os.path.join(ROOT, "tests", "golden", "cases", "close_spheres.cfg")).read()
+    text = text.replace("(1.17, 0.55, 0.5, 0.2)", "(1.11, 0.55, 0.5, 0.2)")
+    with pytest.raises(nsfsi.NsfError) as e:
+        Solver(text, device=-1)
+    assert e.value.code == 4 and "inside another" in str(e.value)

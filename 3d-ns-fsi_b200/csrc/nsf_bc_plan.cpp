@@ -62,8 +62,12 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
     const uint8_t t = in.typeDev[size_t(r)], k = t & TYPE_MASK;
     return (k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT);
   };
-  auto depR = [&](long long r) { return solidOff(r) ? 0 : std::max(int(wA[size_t(r)]), int(wR[size_t(r)])); };
-  auto depM = [&](long long r) { return solidOff(r) ? 0 : int(wA[size_t(r)]); };
+  // (a ghost node stops being one once a body's ghost item has written it: readers of a later body read
+  // the ghost value, as the reference's next body does)
+  std::vector<uint8_t> ghostDone(Nd, 0);
+  auto resolved = [&](long long r) { return solidOff(r) && !ghostDone[size_t(r)]; };
+  auto depR = [&](long long r) { return resolved(r) ? 0 : std::max(int(wA[size_t(r)]), int(wR[size_t(r)])); };
+  auto depM = [&](long long r) { return resolved(r) ? 0 : int(wA[size_t(r)]); };
   auto readR = [&](long long r, int L) { rR[size_t(r)] = int8_t(std::max(int(rR[size_t(r)]), L)); };
   auto readM = [&](long long r, int L) { rM[size_t(r)] = int8_t(std::max(int(rM[size_t(r)]), L)); };
   // a write of every field at n: after every earlier write and read of it
@@ -202,6 +206,8 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
       wA[size_t(gn)] = int8_t(L);
       item(out.ghost, L, q);
     }
+    for (int q = 0; q < nG; ++q)
+      if (in.gbody[size_t(q)] == body) ghostDone[size_t(in.gnode[size_t(q)])] = 1;
   }
   // stage-4 dt terms of the solid inactive nodes (their stored values, or their copied conserved values)
   for (int z = 0; z < nZ; ++z) {

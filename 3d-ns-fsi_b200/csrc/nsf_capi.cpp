@@ -292,14 +292,21 @@ nsf_status build_device(nsf_solver* s) {
     if ((st = upload(s, &dFm, fmeta)) != NSF_OK) return st;
     G.fmeta = dFm;
   }
-  {  // stencil nodes of each filter node that are solid nodes off the mesh faces (read from the copy's source)
+  {  // stencil nodes of each filter node that are solid nodes off the mesh faces, read from the solid copy's
+     // source -- unless an earlier body's ghost item has written the node by then
+    std::map<long long, int> firstGhostBody;  // device node -> first body whose ghost list holds it
+    for (size_t q = S.bodies.size(); q-- > 0;)
+      for (auto& g : S.bodies[q].ghosts) firstGhostBody[dev(g.i * S.NJ * S.NK + g.j * S.NK + g.k)] = int(q);
     std::vector<uint8_t> fsolid(fnode.size(), 0);
     for (size_t q = 0; q < fnode.size(); ++q) {
       const long long n = fnode[q];
       const long long nb[7] = {n, n + G.sI, n - G.sI, n + G.sJ, n - G.sJ, n + 1, n - 1};
       for (int b = 0; b < 7; ++b) {
         const uint8_t t = typeDev[size_t(nb[b])], k = t & TYPE_MASK;
-        if ((k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT)) fsolid[q] |= uint8_t(1u << b);
+        auto it = firstGhostBody.find(nb[b]);
+        const bool written = it != firstGhostBody.end() && it->second < fbody[q];
+        if ((k == SOLID_GHOST || k == SOLID_INACTIVE) && !(t & EDGE_PLANE_BIT) && !written)
+          fsolid[q] |= uint8_t(1u << b);
       }
     }
     uint8_t* dFs;

@@ -169,7 +169,12 @@ nsf_status build_device(nsf_solver* s) {
 
   // initial condition
   std::vector<double> cons, prim;
-  initial_condition(cfg, S, cons, prim);
+  if (!s->slabCons.empty()) {  // an x-slab: its planes of the whole grid's initial condition
+    cons = s->slabCons;
+    prim = s->slabPrim;
+  } else {
+    initial_condition(cfg, S, cons, prim);
+  }
   double* fields = nullptr;
   nsf_status st = dalloc(s, &fields, 20 * Nd);
   if (st != NSF_OK) return st;
@@ -219,6 +224,8 @@ nsf_status build_device(nsf_solver* s) {
 
   // node types with the filter bit, filter slots
   std::vector<uint8_t> type = S.type;
+  if (!s->slabFlags.empty())
+    for (size_t n = 0; n < N; ++n) type[n] |= s->slabFlags[n];
   for (auto& e : S.edges)
     for (size_t i = e.owned.i0; i <= e.owned.i1; ++i)
       for (size_t j = e.owned.j0; j <= e.owned.j1; ++j)
@@ -636,6 +643,14 @@ nsf_status build_device(nsf_solver* s) {
 }
 
 }  // namespace
+
+// For the x-slab groups (nsf_slab.cpp): device set-up of a handle whose host setup is already in place,
+// and the initial dt of a whole grid.
+nsf_status nsf_build_device(nsf_solver* s) { return build_device(s); }
+double nsf_initial_dt(const nsf_config& c, const nsf::HostSetup& S, const std::vector<double>& cons,
+                      const std::vector<double>& prim) {
+  return initial_dt(c, S, cons, prim);
+}
 
 extern "C" {
 

@@ -243,6 +243,11 @@ void launch_stage_ensemble(const Grid* dGrids, const LaunchPlan& L, int s, void*
 // dg: the grid in device memory (read by the small kernels); hg: the same grid on the host (passed by
 // value to the stage kernel, whose coefficients then come from the constant bank).
 int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream);
+// Pieces of a step for callers that put work between them (x-slab groups, nsf_slab.cpp): the prologue and
+// the density filter of one grid; the fused boundary kernel of stage s (fin: with the end-of-step finalize).
+// Return the launches queued.
+int enqueue_step_begin(Grid* dg, const LaunchPlan& L, void* stream);
+int launch_bc_part(Grid* dg, const LaunchPlan& L, int s, bool fin, void* stream);
 // Same sequence with events recorded around each of the four stage kernels (events[2*s], events[2*s+1]);
 // used for per-kernel timing. inGraph: the stream is being captured, and the events become event-record
 // nodes of the graph (so the kernels are timed inside graph replays, as the solver runs them).

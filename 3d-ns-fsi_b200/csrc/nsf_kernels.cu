@@ -909,6 +909,19 @@ static int enqueue_impl(Grid* dg, const Grid* hg, int members, const LaunchPlan&
   return launches;
 }
 
+int enqueue_step_begin(Grid* dg, const LaunchPlan& L, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_prologue<<<1, 32, 0, st>>>(dg);
+  k_density_filter<<<dim3(L.gfBlocks, 1), 256, 0, st>>>(dg);
+  return 2;
+}
+
+int launch_bc_part(Grid* dg, const LaunchPlan& L, int s, bool fin, void* stream) {
+  if (L.bcBlocks <= 0 || (L.bcLevels == 0 && !fin)) return 0;
+  launch_bc(dg, 1, L, s, fin, static_cast<cudaStream_t>(stream));
+  return 1;
+}
+
 int enqueue_step(Grid* dg, const Grid& hg, const LaunchPlan& L, void* stream) {
   return enqueue_impl(dg, &hg, 1, L, static_cast<cudaStream_t>(stream), nullptr);
 }

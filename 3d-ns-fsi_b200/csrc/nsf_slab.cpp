@@ -1,0 +1,374 @@
+// x-slab decomposition of one grid (SURVEY (e): i is the slowest index, so an i-plane is contiguous).
+//
+// The interior planes 1 .. NI-2 are split into P contiguous ranges; slab p owns its range (slab 0 also owns
+// the x-min face plane, slab P-1 the x-max face plane) and holds one more plane on each side: a halo (a copy
+// of the neighbour's plane) or, at the ends, its own x face. Each slab is an ordinary solver handle on its
+// planes -- same kernels, same node classification restricted to the slab, its edge conditions clipped to
+// the planes it owns -- so the stage kernel computes exactly the slab's interior planes. Per RK4 step:
+//
+//   prologue + density filter of every slab;  exchange of the filtered density's halo planes
+//   4 x { stage kernel of every slab;
+//         periodic x faces: plane NI-2 -> slab 0's x-min face plane, plane 1 -> slab P-1's x-max face plane
+//           (the x faces' periodic copy, PeriodicBoundary, Boundary.cpp:344-367; the slabs' own edge
+//           conditions then treat the face planes' y/z rows, which read those copies, as the reference does);
+//         fused boundary kernel of every slab (no finalize);
+//         halo exchange: each slab's first and last owned planes -> its neighbours' halo planes }
+//   global reductions (dt maxima, change-norm sums) and the end of step of every slab.
+//
+// All slabs of a group live on one device and one stream, and a step is one CUDA graph; a transfer packs the
+// plane into the receiving slab's staging buffer and unpacks it there (the buffers each step's roles select
+// are read on the device). The node values and the dt sequence equal the single-grid solve's bit for bit
+// (the dt terms are maxima; the change norms are summed slab by slab, so they agree to rounding). Immersed
+// bodies are not supported across slabs (NSF_ERR_ARG).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "nsf_internal.h"
+#include "nsf_slab.h"
+#include "nsf_solver_impl.h"
+
+using namespace nsf;
+
+struct nsf_slab_group {
+  nsf_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  HostSetup whole;                 // the grid's own host setup (partition, downloads)
+  std::vector<nsf_solver*> slabs;
+  std::vector<int> a, b;           // slab p's interior planes a[p] .. b[p] (global)
+  std::vector<int> lo, hi;         // the global planes slab p owns: its interior planes, plus the x faces at the ends
+  std::vector<int> base;           // global plane of slab p's local plane 0 (= a[p] - 1)
+  bool xPeriodic = false;
+  Grid* dGrids = nullptr;          // copies of the slabs' grids, device
+  double* dRed = nullptr;          // [9] global dt maxima and norm sums
+  // transfers: one staging buffer per receiving side
+  std::vector<SlabTask> packStage, unpackStage, packWrap, unpackWrap, packFilter, unpackFilter;
+  SlabTask* dTasks = nullptr;      // all task lists, device, in the order above
+  size_t offs[7] = {0, 0, 0, 0, 0, 0, 0};
+  long long planeWords = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graphExec = nullptr;
+  int launchesPerStep = 0;
+  std::vector<void*> allocs;
+  std::string err;
+};
+
+namespace {
+
+nsf_status gfail(nsf_slab_group* g, nsf_status st, const std::string& m) {
+  g->err = m;
+  return st;
+}
+#define CKG(call)                                                                     \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) return gfail(g, NSF_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+nsf_status galloc(nsf_slab_group* g, T** p, size_t count) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess)
+    return gfail(g, NSF_ERR_CUDA, "cudaMalloc failed (slab group)");
+  g->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return NSF_OK;
+}
+
+// Host setup of slab p: the whole grid's planes base .. base + n - 1, edge conditions clipped to the planes
+// the slab owns (the x faces' periodic copies come from the exchange instead), halo planes typed as edge
+// nodes (no kernel computes or filters them; their values arrive from the neighbour).
+void slab_setup(const nsf_slab_group* g, int p, HostSetup& S, std::vector<uint8_t>& flags) {
+  const HostSetup& W = g->whole;
+  const int P = int(g->lo.size());
+  const int b0 = g->base[p], n = g->b[p] - g->a[p] + 3;
+  const size_t plane = W.NJ * W.NK;
+  S = HostSetup{};
+  S.NI = size_t(n);
+  S.NJ = W.NJ;
+  S.NK = W.NK;
+  S.N = S.NI * plane;
+  std::memcpy(S.d, W.d, sizeof S.d);
+  std::memcpy(S.off, W.off, sizeof S.off);
+  S.type.assign(W.type.begin() + size_t(b0) * plane, W.type.begin() + size_t(b0 + n) * plane);
+  flags.assign(S.N, 0);
+  const int ownLo = p == 0 ? 0 : 1, ownHi = p == P - 1 ? n - 1 : n - 2;  // local planes the slab owns
+  for (int li : {0, n - 1})
+    if (li < ownLo || li > ownHi) {  // halo plane
+      for (size_t q = 0; q < plane; ++q) {
+        S.type[size_t(li) * plane + q] = FLUID_EDGE;
+        flags[size_t(li) * plane + q] = EDGE_PLANE_BIT;
+      }
+    }
+  for (const EdgeBC& e : W.edges) {
+    // every node of the whole grid's edge planes keeps its edge-plane flag (the density filter copies them)
+    for (size_t i = e.owned.i0; i <= e.owned.i1; ++i) {
+      const int li = int(i) - b0;
+      if (li < 0 || li >= n) continue;
+      for (size_t j = e.owned.j0; j <= e.owned.j1; ++j)
+        for (size_t k = e.owned.k0; k <= e.owned.k1; ++k) flags[size_t(li) * plane + j * W.NK + k] |= EDGE_PLANE_BIT;
+    }
+    if (e.axis == 0 && e.bc == NSF_BC_PERIODIC) continue;  // from the exchange
+    const int i0 = std::max(int(e.owned.i0) - b0, ownLo), i1 = std::min(int(e.owned.i1) - b0, ownHi);
+    if (i0 > i1) continue;
+    EdgeBC c = e;
+    c.owned.i0 = size_t(i0);
+    c.owned.i1 = size_t(i1);
+    S.edges.push_back(c);
+  }
+}
+
+nsf_status build_group(nsf_slab_group* g, int P) {
+  const nsf_config& cfg = g->cfg;
+  std::string err;
+  nsf_status st = build_setup(cfg, g->whole, err);
+  if (st != NSF_OK) return gfail(g, st, err);
+  const HostSetup& W = g->whole;
+  if (!W.bodies.empty()) return gfail(g, NSF_ERR_ARG, "x-slab groups support grids without immersed bodies");
+  const int interior = int(W.NI) - 2;
+  if (P < 2 || interior < 2 * P) return gfail(g, NSF_ERR_ARG, "x-slabs: 2 <= slabs and at least 2 interior planes per slab");
+  for (const EdgeBC& e : W.edges)
+    if (e.axis == 0 && e.bc == NSF_BC_PERIODIC) g->xPeriodic = true;
+  for (int p = 0; p < P; ++p) {  // interior planes in P near-equal ranges
+    const int a = 1 + p * interior / P, b = (p + 1) * interior / P;
+    g->a.push_back(a);
+    g->b.push_back(b);
+    g->lo.push_back(p == 0 ? 0 : a);
+    g->hi.push_back(p == P - 1 ? int(W.NI) - 1 : b);
+    g->base.push_back(a - 1);
+  }
+  // the whole grid's initial condition, sliced per slab; its initial dt for every slab
+  std::vector<double> cons, prim;
+  initial_condition(cfg, W, cons, prim);
+  const double dt0 = nsf_initial_dt(cfg, W, cons, prim);
+  const size_t plane = W.NJ * W.NK;
+  CKG(cudaSetDevice(g->device));
+  for (int p = 0; p < P; ++p) {
+    nsf_solver* s = nullptr;
+    st = nsf_create(&cfg, g->device, &s);
+    if (st != NSF_OK) {
+      if (s) nsf_destroy(s);
+      return gfail(g, st, "slab solver");
+    }
+    g->slabs.push_back(s);
+    slab_setup(g, p, s->setup, s->slabFlags);
+    const size_t n = s->setup.NI, N = s->setup.N;
+    s->slabCons.resize(5 * N);
+    s->slabPrim.resize(7 * N);
+    for (int f = 0; f < 5; ++f)
+      std::memcpy(s->slabCons.data() + f * N, cons.data() + f * W.N + size_t(g->base[p]) * plane, N * sizeof(double));
+    for (int f = 0; f < 7; ++f)
+      std::memcpy(s->slabPrim.data() + f * N, prim.data() + f * W.N + size_t(g->base[p]) * plane, N * sizeof(double));
+    (void)n;
+    st = nsf_build_device(s);
+    if (st != NSF_OK) return gfail(g, st, "slab " + std::to_string(p) + ": " + s->err);
+    s->initialized = true;
+    s->ctlInit.dt = dt0;
+    CKG(cudaMemcpy(&s->dCtl->dt, &dt0, sizeof dt0, cudaMemcpyHostToDevice));
+    s->slabCons.clear();
+    s->slabPrim.clear();
+  }
+  // device copies of the slabs' grids (the reductions read them)
+  std::vector<Grid> hg;
+  for (nsf_solver* s : g->slabs) hg.push_back(s->hGrid);
+  if ((st = galloc(g, &g->dGrids, hg.size())) != NSF_OK) return st;
+  CKG(cudaMemcpy(g->dGrids, hg.data(), hg.size() * sizeof(Grid), cudaMemcpyHostToDevice));
+  if ((st = galloc(g, &g->dRed, 9)) != NSF_OK) return st;
+  // transfers
+  g->planeWords = g->slabs[0]->hGrid.sI;
+  auto add = [&](std::vector<SlabTask>& pk, std::vector<SlabTask>& up, int from, int fromPlane, int to, int toPlane,
+                 int which) -> nsf_status {
+    double* buf = nullptr;
+    nsf_status r = galloc(g, &buf, size_t(5) * size_t(g->planeWords));
+    if (r != NSF_OK) return r;
+    pk.push_back(SlabTask{g->slabs[size_t(from)]->dGrid, fromPlane, which, buf});
+    up.push_back(SlabTask{g->slabs[size_t(to)]->dGrid, toPlane, which, buf});
+    return NSF_OK;
+  };
+  for (int p = 0; p + 1 < P; ++p) {
+    const int nLast = int(g->slabs[size_t(p)]->setup.NI) - 2;  // slab p's last owned plane, local
+    for (int which : {SLAB_STAGE, SLAB_FILTER}) {
+      auto& pk = which == SLAB_STAGE ? g->packStage : g->packFilter;
+      auto& up = which == SLAB_STAGE ? g->unpackStage : g->unpackFilter;
+      if ((st = add(pk, up, p, nLast, p + 1, 0, which)) != NSF_OK) return st;
+      if ((st = add(pk, up, p + 1, 1, p, nLast + 1, which)) != NSF_OK) return st;
+    }
+  }
+  if (g->xPeriodic) {  // global plane NI-2 -> slab 0's plane 0; global plane 1 -> slab P-1's last plane
+    const int nl = int(g->slabs[size_t(P - 1)]->setup.NI);
+    if ((st = add(g->packWrap, g->unpackWrap, P - 1, nl - 2, 0, 0, SLAB_STAGE)) != NSF_OK) return st;
+    if ((st = add(g->packWrap, g->unpackWrap, 0, 1, P - 1, nl - 1, SLAB_STAGE)) != NSF_OK) return st;
+  }
+  std::vector<SlabTask> all;
+  const std::vector<SlabTask>* lists[6] = {&g->packStage, &g->unpackStage, &g->packWrap, &g->unpackWrap,
+                                           &g->packFilter, &g->unpackFilter};
+  for (int q = 0; q < 6; ++q) {
+    g->offs[q] = all.size();
+    all.insert(all.end(), lists[q]->begin(), lists[q]->end());
+  }
+  g->offs[6] = all.size();
+  if ((st = galloc(g, &g->dTasks, all.size())) != NSF_OK) return st;
+  CKG(cudaMemcpy(g->dTasks, all.data(), all.size() * sizeof(SlabTask), cudaMemcpyHostToDevice));
+  CKG(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  CKG(cudaDeviceSynchronize());
+  // one step as a CUDA graph
+  CKG(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+  int launches = 0;
+  auto copies = [&](int list, int s, int dir) {
+    const int n = int(g->offs[list + 1] - g->offs[list]);
+    if (n > 0) {
+      launch_slab_copy(g->dTasks + g->offs[list], n, g->planeWords, s, dir, g->stream);
+      ++launches;
+    }
+  };
+  for (nsf_solver* s : g->slabs) launches += enqueue_step_begin(s->dGrid, s->plan, g->stream);
+  copies(4, 0, 0);  // filtered density halos (filter steps)
+  copies(5, 0, 1);
+  for (int q = 0; q < 4; ++q) {
+    for (nsf_solver* s : g->slabs) {
+      launch_stage(s->hGrid, s->plan, q, g->stream);
+      ++launches;
+    }
+    copies(2, q, 0);  // periodic x faces
+    copies(3, q, 1);
+    for (nsf_solver* s : g->slabs) launches += launch_bc_part(s->dGrid, s->plan, q, false, g->stream);
+    copies(0, q, 0);  // halos
+    copies(1, q, 1);
+  }
+  launch_slab_reduce(g->dGrids, P, g->dRed, g->stream);
+  launch_slab_finalize(g->dGrids, P, g->dRed, g->stream);
+  launches += 2;
+  const cudaError_t e1 = cudaGetLastError();
+  const cudaError_t e2 = cudaStreamEndCapture(g->stream, &g->graph);
+  if (e1 != cudaSuccess || e2 != cudaSuccess)
+    return gfail(g, NSF_ERR_CUDA, std::string("slab step capture: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+  CKG(cudaGraphInstantiate(&g->graphExec, g->graph, 0));
+  g->launchesPerStep = launches;
+  return NSF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nsf_status nsf_slab_plan(const nsf_config* cfg, int32_t nslabs, int32_t* first, int32_t* last) {
+  if (!cfg || !first || !last || nslabs < 2) return NSF_ERR_ARG;
+  const int interior = int(cfg->NI) - 2;
+  if (interior < 2 * nslabs) return NSF_ERR_ARG;
+  for (int p = 0; p < nslabs; ++p) {
+    first[p] = 1 + p * interior / nslabs;
+    last[p] = (p + 1) * interior / nslabs;
+  }
+  return NSF_OK;
+}
+
+nsf_status nsf_slab_group_create(const nsf_config* cfg, int32_t nslabs, int32_t device, nsf_slab_group** out) {
+  if (!cfg || !out || device < 0) return NSF_ERR_ARG;
+  *out = nullptr;
+  auto* g = new nsf_slab_group;
+  g->cfg = *cfg;
+  g->device = device;
+  nsf_status st = build_group(g, nslabs);
+  *out = g;
+  return st;
+}
+
+nsf_status nsf_slab_group_march(nsf_slab_group* g, uint64_t nsteps) {
+  if (!g || !g->graphExec) return NSF_ERR_STATE;
+  CKG(cudaSetDevice(g->device));
+  for (uint64_t q = 0; q < nsteps; ++q) CKG(cudaGraphLaunch(g->graphExec, g->stream));
+  return NSF_OK;
+}
+
+nsf_status nsf_slab_group_march_timed(nsf_slab_group* g, uint64_t nsteps, double* elapsed_ms) {
+  if (!g || !g->graphExec || !elapsed_ms) return NSF_ERR_STATE;
+  CKG(cudaSetDevice(g->device));
+  cudaEvent_t a, b;
+  CKG(cudaEventCreate(&a));
+  CKG(cudaEventCreate(&b));
+  CKG(cudaEventRecord(a, g->stream));
+  for (uint64_t q = 0; q < nsteps; ++q) CKG(cudaGraphLaunch(g->graphExec, g->stream));
+  CKG(cudaEventRecord(b, g->stream));
+  CKG(cudaEventSynchronize(b));
+  float ms = 0;
+  CKG(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *elapsed_ms = ms;
+  return NSF_OK;
+}
+
+nsf_status nsf_slab_group_sync(nsf_slab_group* g) {
+  if (!g || !g->graphExec) return NSF_ERR_STATE;
+  CKG(cudaSetDevice(g->device));
+  CKG(cudaStreamSynchronize(g->stream));
+  nsf_status worst = NSF_OK;
+  for (nsf_solver* s : g->slabs) {
+    const nsf_status st = nsf_sync(s);
+    if (st == NSF_ERR_TIMEOUT) return gfail(g, st, s->err);
+    if (st != NSF_OK) {
+      worst = st;
+      g->err = s->err;
+    }
+  }
+  return worst;
+}
+
+nsf_status nsf_slab_group_solver(nsf_slab_group* g, int32_t slab, nsf_solver** s) {
+  if (!g || !s || slab < 0 || slab >= int32_t(g->slabs.size())) return NSF_ERR_ARG;
+  CKG(cudaSetDevice(g->device));
+  CKG(cudaStreamSynchronize(g->stream));
+  *s = g->slabs[size_t(slab)];
+  return NSF_OK;
+}
+
+nsf_status nsf_slab_group_info(nsf_slab_group* g, int32_t* nslabs, int32_t* first_planes, uint64_t* launches_per_step) {
+  if (!g) return NSF_ERR_ARG;
+  if (nslabs) *nslabs = int32_t(g->slabs.size());
+  if (first_planes)
+    for (size_t p = 0; p < g->slabs.size(); ++p) first_planes[p] = g->lo[p];
+  if (launches_per_step) *launches_per_step = uint64_t(g->launchesPerStep);
+  return NSF_OK;
+}
+
+nsf_status nsf_slab_group_download(nsf_slab_group* g, uint32_t mask, double* host) {
+  if (!g || !host || g->slabs.empty()) return NSF_ERR_ARG;
+  CKG(cudaSetDevice(g->device));
+  CKG(cudaStreamSynchronize(g->stream));
+  const HostSetup& W = g->whole;
+  const size_t plane = W.NJ * W.NK;
+  int nf = 0;
+  for (int f = 0; f < NSF_NUM_FIELDS; ++f) nf += (mask >> f) & 1;
+  for (size_t p = 0; p < g->slabs.size(); ++p) {
+    nsf_solver* s = g->slabs[p];
+    std::vector<double> loc(size_t(nf) * s->setup.N);
+    const nsf_status st = nsf_download(s, mask, loc.data());
+    if (st != NSF_OK) return gfail(g, st, s->err);
+    const int b0 = g->base[p];
+    for (int q = 0; q < nf; ++q)
+      for (int i = g->lo[p]; i <= g->hi[p]; ++i)
+        std::memcpy(host + size_t(q) * W.N + size_t(i) * plane, loc.data() + size_t(q) * s->setup.N + size_t(i - b0) * plane,
+                    plane * sizeof(double));
+  }
+  return NSF_OK;
+}
+
+const char* nsf_slab_group_last_error(nsf_slab_group* g) { return g ? g->err.c_str() : "null slab group"; }
+
+void nsf_slab_group_destroy(nsf_slab_group* g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->graphExec) cudaGraphExecDestroy(g->graphExec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  for (nsf_solver* s : g->slabs) nsf_destroy(s);
+  for (void* p : g->allocs) cudaFree(p);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+}  // extern "C"

@@ -43,6 +43,10 @@ struct nsf_solver {
   std::vector<CUtensorMap> hostMaps;
   void* encodeFn = nullptr;
   int tileRequest = -1;  // StageTile to use, or -1 for the default
+  // x-slab member of a slab group (nsf_slab.cpp): the initial condition sliced from the whole grid's, and
+  // node flags to add (EDGE_PLANE_BIT on halo planes and on the whole grid's edge planes); empty otherwise
+  std::vector<double> slabCons, slabPrim;
+  std::vector<uint8_t> slabFlags;
   std::vector<int> ghostOrder;   // device ghost slot -> position in the bodies' ghost lists
   nsf::BcMemberLevels bcLevels;  // dependency levels of the boundary work (fused boundary kernel)
   nsf::StepCtl ctlInit{};  // the control block at level 0 (the discrete adjoint restarts from it)
@@ -51,5 +55,10 @@ struct nsf_solver {
 
 // Frees the adjoint state of a handle (nsf_adjoint.cpp).
 void nsf_adjoint_free(nsf_solver* s);
+// Device set-up of a handle whose host setup (s->setup) is in place (nsf_capi.cpp), and the initial dt of a
+// grid from its initial fields (Solver::updateTimeStepSize at t = 0).
+nsf_status nsf_build_device(nsf_solver* s);
+double nsf_initial_dt(const nsf_config& c, const nsf::HostSetup& S, const std::vector<double>& cons,
+                      const std::vector<double>& prim);
 
 #endif

@@ -103,6 +103,16 @@ def lib():
         "nsf_ensemble_last_error": (ctypes.c_char_p, [vp]),
         "nsf_ensemble_destroy": (None, [vp]),
         "nsf_autotune": (i32, [cp, i32, ctypes.c_char_p, ctypes.POINTER(i32), dp]),
+        "nsf_slab_plan": (i32, [cp, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+        "nsf_slab_group_create": (i32, [cp, i32, i32, ctypes.POINTER(vp)]),
+        "nsf_slab_group_march": (i32, [vp, u64]),
+        "nsf_slab_group_march_timed": (i32, [vp, u64, dp]),
+        "nsf_slab_group_sync": (i32, [vp]),
+        "nsf_slab_group_download": (i32, [vp, u32, dp]),
+        "nsf_slab_group_solver": (i32, [vp, i32, ctypes.POINTER(vp)]),
+        "nsf_slab_group_info": (i32, [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(u64)]),
+        "nsf_slab_group_last_error": (ctypes.c_char_p, [vp]),
+        "nsf_slab_group_destroy": (None, [vp]),
         "nsf_adj_configure": (i32, [vp, u32, u32]),
         "nsf_adj_forward": (i32, [vp, dp, dp, dp]),
         "nsf_adj_backward": (i32, [vp, ctypes.c_double, dp, dp]),
@@ -406,6 +416,89 @@ class Ensemble:
         tile, lps, items = ctypes.c_int32(), ctypes.c_uint64(), ctypes.c_uint32()
         self._check(lib().nsf_ensemble_info(self.h, ctypes.byref(tile), ctypes.byref(lps), ctypes.byref(items)))
         return tile.value, lps.value, items.value
+
+
+def slab_plan(cfg, nslabs):
+    """[(first, last)] interior planes each of nslabs x-slabs computes (nsf_slab_plan)."""
+    if isinstance(cfg, str):
+        cfg = config_load(cfg) if os.path.exists(cfg) else config_parse(cfg)
+    a = (ctypes.c_int32 * nslabs)()
+    b = (ctypes.c_int32 * nslabs)()
+    st = lib().nsf_slab_plan(ctypes.byref(cfg), nslabs, a, b)
+    if st:
+        raise NsfError(st, "nsf_slab_plan")
+    return list(zip(list(a), list(b)))
+
+
+class SlabGroup:
+    """One grid split into x-slabs (nsf_slab_group_*), all on one device."""
+
+    def __init__(self, cfg, nslabs, device=0):
+        if isinstance(cfg, str):
+            cfg = config_load(cfg) if os.path.exists(cfg) else config_parse(cfg)
+        self.cfg = cfg
+        self.N = int(cfg.NI * cfg.NJ * cfg.NK)
+        self.h = ctypes.c_void_p()
+        st = lib().nsf_slab_group_create(ctypes.byref(cfg), nslabs, device, ctypes.byref(self.h))
+        if st:
+            msg = lib().nsf_slab_group_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise NsfError(st, msg)
+
+    def _check(self, st):
+        if st:
+            raise NsfError(st, lib().nsf_slab_group_last_error(self.h).decode())
+
+    def close(self):
+        if self.h:
+            lib().nsf_slab_group_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def march(self, nsteps):
+        self._check(lib().nsf_slab_group_march(self.h, nsteps))
+
+    def march_timed(self, nsteps):
+        ms = ctypes.c_double()
+        self._check(lib().nsf_slab_group_march_timed(self.h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        self._check(lib().nsf_slab_group_sync(self.h))
+
+    def download(self, fields=range(12)):
+        fields = sorted(fields)
+        mask = 0
+        for f in fields:
+            mask |= 1 << f
+        out = np.empty((len(fields), self.N))
+        self._check(lib().nsf_slab_group_download(self.h, mask, _dp(out)))
+        return out
+
+    def slab(self, p):
+        """Slab p's solver (read-only view: time, history)."""
+        h = ctypes.c_void_p()
+        self._check(lib().nsf_slab_group_solver(self.h, p, ctypes.byref(h)))
+        return Member(h, self.cfg)
+
+    def info(self):
+        n = ctypes.c_int32()
+        self._check(lib().nsf_slab_group_info(self.h, ctypes.byref(n), None, None))
+        first = (ctypes.c_int32 * n.value)()
+        lps = ctypes.c_uint64()
+        self._check(lib().nsf_slab_group_info(self.h, None, first, ctypes.byref(lps)))
+        return n.value, list(first), lps.value
 
 
 def autotune(cfg, device=0, cache=None):

@@ -215,6 +215,30 @@ nsf_status nsf_autotune(const nsf_config* cfg, int32_t device, const char* cache
                         double* ns_per_node);
 
 /* ---------------------------------------------------------------------------------------------------
+ * x-slab decomposition of one grid (no counterpart in the reference, whose grid is one array per field;
+ * its k-fastest, i-slowest layout, Array3D.h:41-42, makes every i-plane contiguous). The interior planes
+ * 1 .. NI-2 are split into nslabs near-equal contiguous ranges (nsf_slab_plan); each slab is a solver on its
+ * planes plus a halo plane on each side, and a step exchanges the halo planes after every stage, the x
+ * faces' periodic copies between the end slabs, and reduces the dt maxima and change norms over all slabs.
+ * The result equals the single-grid solve node for node. Grids without immersed bodies; at least two
+ * interior planes per slab. All slabs of a group run on one device (one CUDA graph per step). */
+typedef struct nsf_slab_group nsf_slab_group;
+/* first[p], last[p]: the interior planes slab p computes (host only). */
+nsf_status nsf_slab_plan(const nsf_config* cfg, int32_t nslabs, int32_t* first, int32_t* last);
+nsf_status nsf_slab_group_create(const nsf_config* cfg, int32_t nslabs, int32_t device, nsf_slab_group** out);
+nsf_status nsf_slab_group_march(nsf_slab_group* g, uint64_t nsteps);
+nsf_status nsf_slab_group_march_timed(nsf_slab_group* g, uint64_t nsteps, double* elapsed_ms);
+nsf_status nsf_slab_group_sync(nsf_slab_group* g);
+/* Fields of the whole grid assembled from the slabs (as nsf_download). */
+nsf_status nsf_slab_group_download(nsf_slab_group* g, uint32_t field_mask, double* host);
+/* Slab p's solver handle (t, dt, history, ...; valid until nsf_slab_group_destroy; do not march it). */
+nsf_status nsf_slab_group_solver(nsf_slab_group* g, int32_t slab, nsf_solver** s);
+/* Slab count, the first plane each slab owns, launches per step. */
+nsf_status nsf_slab_group_info(nsf_slab_group* g, int32_t* nslabs, int32_t* first_planes, uint64_t* launches_per_step);
+const char* nsf_slab_group_last_error(nsf_slab_group* g);
+void nsf_slab_group_destroy(nsf_slab_group* g);
+
+/* ---------------------------------------------------------------------------------------------------
  * Discrete adjoint (a forward / backward pair; no counterpart in the reference, whose marchTimeStep,
  * Solver.cpp:130-167, it differentiates). Objective of a run of stop_time_level steps from level 0:
  *   J = (1/n_avg) sum over the last n_avg steps of F_x(U_n),  F_x = -(dx dy dz)^(2/3) sum_g p(U_g) n_x(g)

@@ -122,6 +122,8 @@ int bc_plan_member(const Grid& G, const std::vector<EdgeBlock> edgeBlocks[3], co
           } else if (bc == NSF_BC_OUTLET) {
             reads.push_back(n + sgn * st);
             reads.push_back(n + 2 * sgn * st);
+          } else if (bc == BC_SLAB_COPY) {
+            reads.push_back(n);
           } else if (bc == NSF_BC_PERIODIC) {
             int src[3] = {ijk[0], ijk[1], ijk[2]};
             periodic_source_host(G, axis, side, src);

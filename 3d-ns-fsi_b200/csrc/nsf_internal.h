@@ -24,6 +24,9 @@ constexpr uint8_t EDGE_PLANE_BIT = 0x40;  // node lies in a mesh-edge boundary's
 constexpr uint8_t ZCOPY_UP_BIT = 0x20;
 constexpr uint8_t ZCOPY_DOWN_BIT = 0x10;
 constexpr int FMETA_LAST = 1 << 30;  // Grid::fmeta: this slot is its node's last
+// Edge condition of an x-slab's periodic x face (nsf_slab.cpp): the plane exchange has already copied the
+// face's values; the edge item only adds the nodes' stage-4 dt terms, as the whole grid's periodic face does.
+constexpr int BC_SLAB_COPY = 16;
 
 struct Box {  // IndexBoundingBox, src/SmallVectors.h:72-104 (inclusive bounds)
   size_t i0, i1, j0, j1, k0, k1;

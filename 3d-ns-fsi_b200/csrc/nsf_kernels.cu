@@ -255,6 +255,8 @@ __device__ __forceinline__ void edge_node(const Grid& G, const StepCtl* c, const
         cv[3] = rw;
         cv[4] = p / C.gm1 + (1 + rho) / 2 * (u * u + v * v + w * w);
         primKnown = true;
+      } else if (bc == BC_SLAB_COPY) {  // an x-slab's periodic x face: already copied by the plane exchange
+        for (int f = 0; f < 5; ++f) cv[f] = ld(f, n);
       } else if (bc == NSF_BC_PERIODIC) {  // Boundary.cpp:344-367, opposite index :111-133
         int src[3] = {ijk[0], ijk[1], ijk[2]};
         periodic_source(G, axis, side, src);

@@ -17,9 +17,10 @@
 //
 // All slabs of a group live on one device and one stream, and a step is one CUDA graph; a transfer packs the
 // plane into the receiving slab's staging buffer and unpacks it there (the buffers each step's roles select
-// are read on the device). The node values and the dt sequence equal the single-grid solve's bit for bit
-// (the dt terms are maxima; the change norms are summed slab by slab, so they agree to rounding). Immersed
-// bodies are not supported across slabs (NSF_ERR_ARG).
+// are read on the device). The node values and the dt sequence equal the single-grid solve's bit for bit:
+// every node's dt terms are formed by the same kernel as in the whole grid (the periodic x faces' by their
+// edge items, BC_SLAB_COPY), and maxima do not depend on the order; the change norms are summed slab by slab,
+// so they agree to rounding. Immersed bodies are not supported across slabs (NSF_ERR_ARG).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -112,10 +113,11 @@ void slab_setup(const nsf_slab_group* g, int p, HostSetup& S, std::vector<uint8_
       for (size_t j = e.owned.j0; j <= e.owned.j1; ++j)
         for (size_t k = e.owned.k0; k <= e.owned.k1; ++k) flags[size_t(li) * plane + j * W.NK + k] |= EDGE_PLANE_BIT;
     }
-    if (e.axis == 0 && e.bc == NSF_BC_PERIODIC) continue;  // from the exchange
     const int i0 = std::max(int(e.owned.i0) - b0, ownLo), i1 = std::min(int(e.owned.i1) - b0, ownHi);
     if (i0 > i1) continue;
     EdgeBC c = e;
+    // a periodic x face's values come from the exchange; its edge items only add the dt terms
+    if (e.axis == 0 && e.bc == NSF_BC_PERIODIC) c.bc = BC_SLAB_COPY;
     c.owned.i0 = size_t(i0);
     c.owned.i1 = size_t(i1);
     S.edges.push_back(c);

@@ -182,29 +182,43 @@ struct XOwn {  // a node's values that the next x-face needs
 
 // G at one node. own: rho_u, rho_v, rho_w, rho_E, u, v, w, p, mu; d*: in-plane differences at the node
 // (v_N - v_S, u_N - u_S, w_U - w_D, u_U - u_D).
+// x_node and x_face spell out every rounding (__dmul_rn, __dadd_rn, __fma_rn are never contracted or
+// reordered by the compiler): the stage kernel evaluates them in two places (the first planes of a work item
+// and its main loop), and a plane's G and F must come out bit for bit the same in either, whatever the
+// i-planes a work item covers (a grid run whole or in x-slabs gives identical values).
 __device__ __forceinline__ XNode x_node(const Consts& C, double ru, double rv, double rw, double rE, double u,
                                         double v, double w, double p, double mu, double dyv, double dyu, double dzw,
                                         double dzu) {
   XNode n;
-  const double myv = mu * dyv, mzw = mu * dzw, myu = mu * dyu, mzu = mu * dzu;
-  n.g[0] = C.ax * ru;
-  n.g[1] = C.ax * (ru * u + p) + C.xm_yx * myv + C.xm_zx * mzw;
-  n.g[2] = C.ax * (rv * u) + C.ym_yx * myu;
-  n.g[3] = C.ax * (rw * u) + C.zm_zx * mzu;
-  n.g[4] = C.ax * ((C.h0 + rE + p) * u) + C.e_yx6 * (u * myv) + C.e_zx6 * (u * mzw) + C.e_yx4 * (v * myu) +
-           C.e_zx4 * (w * mzu);
+  const double myv = __dmul_rn(mu, dyv), mzw = __dmul_rn(mu, dzw), myu = __dmul_rn(mu, dyu), mzu = __dmul_rn(mu, dzu);
+  n.g[0] = __dmul_rn(C.ax, ru);
+  n.g[1] = __fma_rn(C.xm_zx, mzw, __fma_rn(C.xm_yx, myv, __dmul_rn(C.ax, __fma_rn(ru, u, p))));
+  n.g[2] = __fma_rn(C.ym_yx, myu, __dmul_rn(C.ax, __dmul_rn(rv, u)));
+  n.g[3] = __fma_rn(C.zm_zx, mzu, __dmul_rn(C.ax, __dmul_rn(rw, u)));
+  const double h = __dmul_rn(__dadd_rn(__dadd_rn(C.h0, rE), p), u);
+  double e4 = __dmul_rn(C.ax, h);
+  e4 = __fma_rn(C.e_yx6, __dmul_rn(u, myv), e4);
+  e4 = __fma_rn(C.e_zx6, __dmul_rn(u, mzw), e4);
+  e4 = __fma_rn(C.e_yx4, __dmul_rn(v, myu), e4);
+  n.g[4] = __fma_rn(C.e_zx4, __dmul_rn(w, mzu), e4);
   return n;
 }
 
 // F of the x-face between a (lower i) and b.
 __device__ __forceinline__ void x_face(const Consts& C, const XOwn& a, const XOwn& b, double f[5]) {
-  const double ms = a.mu + b.mu;
+  const double ms = __dadd_rn(a.mu, b.mu);
+  const double du = __dsub_rn(b.u, a.u), dv = __dsub_rn(b.v, a.v), dw = __dsub_rn(b.w, a.w);
   f[0] = 0.0;
-  f[1] = C.xm_xx * (ms * (b.u - a.u));
-  f[2] = C.ym_xx * (ms * (b.v - a.v));
-  f[3] = C.zm_xx * (ms * (b.w - a.w));
-  f[4] = C.e_xx23 * ((a.mu * a.u + b.mu * b.u) * (b.u - a.u)) + C.e_xx12 * ((a.mu * a.v + b.mu * b.v) * (b.v - a.v)) +
-         C.e_xx12 * ((a.mu * a.w + b.mu * b.w) * (b.w - a.w)) + C.e_xx12 * (C.pf * (ms * (b.T - a.T)));
+  f[1] = __dmul_rn(C.xm_xx, __dmul_rn(ms, du));
+  f[2] = __dmul_rn(C.ym_xx, __dmul_rn(ms, dv));
+  f[3] = __dmul_rn(C.zm_xx, __dmul_rn(ms, dw));
+  const double su = __fma_rn(a.mu, a.u, __dmul_rn(b.mu, b.u));
+  const double sv = __fma_rn(a.mu, a.v, __dmul_rn(b.mu, b.v));
+  const double sw = __fma_rn(a.mu, a.w, __dmul_rn(b.mu, b.w));
+  double e4 = __dmul_rn(C.e_xx23, __dmul_rn(su, du));
+  e4 = __fma_rn(C.e_xx12, __dmul_rn(sv, dv), e4);
+  e4 = __fma_rn(C.e_xx12, __dmul_rn(sw, dw), e4);
+  f[4] = __fma_rn(C.e_xx12, __dmul_rn(C.pf, __dmul_rn(ms, __dsub_rn(b.T, a.T))), e4);
 }
 
 // y- and z-direction part of the right-hand side at P (the reference's terms not covered by G and F).

@@ -59,6 +59,7 @@ struct AdjCtx {
   double* tmpV = nullptr;
   double* ipbar = nullptr;
   double* fbar = nullptr;
+  unsigned long long* bcSync = nullptr;  // grid-barrier counter of k_adj_bc
   std::vector<double*> slot;
   std::vector<StepCtl*> slotCtl;
   double* stageSnap = nullptr;  // 4 x (11 Nd + 2F): I (5), R (1), O before the edge conditions (5), fpre
@@ -157,6 +158,8 @@ nsf_status setup(nsf_solver* s) {
   if ((st = aalloc(s, a, &a->tmpV, 11 * N)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->ipbar, 5 * NG)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->fbar, 2 * plane)) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->bcSync, 1)) != NSF_OK) return st;
+  CKA(cudaMemset(a->bcSync, 0, sizeof(unsigned long long)));
   if ((st = aalloc(s, a, &a->stageSnap, 4 * per_stage(s))) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->dHist, size_t(a->nsteps))) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->dCur, 1)) != NSF_OK) return st;
@@ -377,7 +380,9 @@ struct SnapHook : StepHook {
 };
 
 // Phases of an adjoint step, for nsf_adj_profile_step.
-enum AdjPhase { PH_RECOMPUTE, PH_OBJECTIVE, PH_GHOST, PH_FILTER, PH_EDGE, PH_SOLID, PH_PREPARE, PH_RHS, PH_DFILTER,
+// PH_BC: one launch per stage for ghosts, near-body filter, edge conditions and the RK4 combine (and, on
+// steps whose result enters J, the objective); slots 1 and 3-6 stay, empty, for the layout of the result.
+enum AdjPhase { PH_RECOMPUTE, PH_OBJECTIVE, PH_BC, PH_UNUSED3, PH_UNUSED4, PH_UNUSED5, PH_UNUSED6, PH_RHS, PH_DFILTER,
                 PH_COUNT };
 
 // Events recorded between the phases of an eagerly launched adjoint step.
@@ -421,18 +426,10 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
   const size_t N = nd(s);
   const int nSM = s->nSM;
   cudaStream_t st = s->stream;
-  if (objective) {
-    AdjPtrs A{};
-    for (int f = 0; f < 5; ++f) {
-      A.val[f] = R.O[3][f];
-      A.lamO[f] = lamOf(s, a, phys(s, R.O[3][f], f), f);
-    }
-    launch_adj_objective(s->dGrid, A, G.nGhost, a->dNx, a->dA, 1.0 / a->navg, nSM, st);
-    mark(PH_OBJECTIVE);
-  }
   for (int q = 3; q >= 0; --q) {
     const double* snap = a->stageSnap + q * per_stage(s);
-    AdjPtrs A{};
+    AdjBcParams P{};
+    AdjPtrs& A = P.A;
     for (int f = 0; f < 5; ++f) {
       A.lamO[f] = lamOf(s, a, phys(s, R.O[q][f], f), f);
       A.lamI[f] = lamOf(s, a, phys(s, R.I[q][f], f), f);
@@ -442,33 +439,52 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     A.lamR = lamOf(s, a, phys(s, R.R[q], 0), 0);
     A.lamFpre = a->lamFpre;
     A.lamFnew = a->lamFnew;
+    // the objective's adjoint (F_x of the step's result) joins the ghost phase of the last stage
+    P.objective = (objective && q == 3) ? 1 : 0;
+    for (int f = 0; f < 5; ++f) P.objVal[f] = R.O[3][f];
+    P.nx = a->dNx;
+    P.dA = a->dA;
+    P.weight = 1.0 / a->navg;
     // near-body filter and ghosts
-    launch_adj_ghost(s->dGrid, A, G.nGhost, G.nFilter, a->ipbar, a->cnode, a->coff, a->cent, a->ncell, nSM, st);
-    mark(PH_GHOST);
-    launch_adj_filter(s->dGrid, A, a->fsNodes, a->nfs, G.nFilter, nSM, st);
-    mark(PH_FILTER);
+    P.ipbar = a->ipbar;
+    P.cnode = a->cnode;
+    P.coff = a->coff;
+    P.cent = a->cent;
+    P.ncell = a->ncell;
+    P.fsNodes = a->fsNodes;
+    P.nfs = a->nfs;
     // edge conditions: z, y, then x (reads the stage output before the edge conditions: its copy, or,
     // where the planes it reads are clean, the next stage's input / the step's result)
     for (int f = 0; f < 5; ++f) {
       if (!a->edgePlanesClean) {
-        A.val[f] = snap + (6 + f) * N;
+        P.edgeVal[f] = snap + (6 + f) * N;
       } else if (q == 3) {
-        A.val[f] = R.O[3][f];
+        P.edgeVal[f] = R.O[3][f];
       } else {
         const SnapPlan Pn = snap_plan(R, q + 1);
-        A.val[f] = Pn.inputLive ? R.I[q + 1][f] : a->stageSnap + (q + 1) * per_stage(s) + f * N;
+        P.edgeVal[f] = Pn.inputLive ? R.I[q + 1][f] : a->stageSnap + (q + 1) * per_stage(s) + f * N;
       }
     }
-    for (int axis = 2; axis >= 0; --axis)
-      launch_adj_edge(s->hGrid, A, s->plan, axis, dR, q, a->fbar, a->lamInflow, a->inletX, st);
-    mark(PH_EDGE);
-    // stage kernel: RK4 combine, transposed RHS, primitives of the stage input
-    const SnapPlan P = snap_plan(R, q);
-    for (int f = 0; f < 5; ++f) A.val[f] = P.inputLive ? R.I[q][f] : snap + f * N;
-    A.valR = P.inputLive ? R.R[q] : P.rSeparate ? snap + 5 * N : snap;
+    for (int axis = 0; axis < 3; ++axis) {
+      P.edges[axis] = s->plan.edgeBlocks[axis];
+      P.nEdge[axis] = s->plan.nEdgeBlocks[axis];
+    }
+    P.inletGather = a->inletX ? 1 : 0;
+    P.fbar = a->fbar;
+    P.lamInflow = a->lamInflow;
+    P.roles = dR;
+    // stage kernel: RK4 combine and the RHS inputs (from the stage input's values), then the transposed RHS
+    const SnapPlan SP = snap_plan(R, q);
+    for (int f = 0; f < 5; ++f) A.val[f] = SP.inputLive ? R.I[q][f] : snap + f * N;
+    A.valR = SP.inputLive ? R.R[q] : SP.rSeparate ? snap + 5 * N : snap;
     A.valFpre = snap + 11 * N;
-    launch_adj_prepare(s->dGrid, G, A, q, dR, R.copyMask[q], a->tmpLam, a->tmpV, nSM, st);
-    mark(PH_PREPARE);
+    P.solidMask = G.nSolid ? R.copyMask[q] : 0;
+    P.lam = a->tmpLam;
+    P.V = a->tmpV;
+    P.sync = a->bcSync;
+    P.timeout = &s->dCtl->timeout;
+    launch_adj_bc(G, P, q, nSM, st);
+    mark(PH_BC);
     launch_adj_rhs(s->dGrid, G, A, a->tmpLam, a->tmpV, nSM, st);
     mark(PH_RHS);
   }

@@ -65,115 +65,103 @@ __global__ void k_objective(const Grid* __restrict__ gp, const double* __restric
   }
 }
 
-__global__ void k_adj_objective(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ nx, double dA,
-                                double weight) {
-  const Grid& G = *gp;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < G.nGhost; q += gridDim.x * blockDim.x) {
-    const long long n = G.gnode[q];
-    double u[5], g[5];
-    for (int f = 0; f < 5; ++f) u[f] = A.val[f][n];
-    pressure(G.C, u, g);
-    for (int f = 0; f < 5; ++f) A.lamO[f][n] += weight * (-dA * nx[q]) * g[f];
-  }
+// The adjoint of the objective's pressure at ghost q (added to the adjoint of the step's result there).
+__device__ __forceinline__ void adj_objective_term(const Grid& G, const double* const val[5], const double* nx,
+                                                   double dA, double weight, int q, double lam[5]) {
+  const long long n = G.gnode[q];
+  double u[5], g[5];
+  for (int f = 0; f < 5; ++f) u[f] = val[f][n];
+  pressure(G.C, u, g);
+  for (int f = 0; f < 5; ++f) lam[f] += weight * (-dA * nx[q]) * g[f];
 }
 
 // ------------------------------------------------------------------------------------------- ghosts
 // k_ghost writes the ghost values (weights x cell values, momenta negated) and writes the filtered
-// values back to the filter nodes. Phase 1: consume the adjoints of everything k_ghost wrote.
-__global__ void k_adj_ghost_consume(const Grid* __restrict__ gp, AdjPtrs A, double* __restrict__ ipbar) {
-  const Grid& G = *gp;
-  const int total = G.nGhost + G.nFilter;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
-    if (q < G.nGhost) {
-      const long long n = G.gnode[q];
-      const double sgn[5] = {1, -1, -1, -1, 1};
-      for (int f = 0; f < 5; ++f) {
-        ipbar[f * (long long)G.nGhost + q] = sgn[f] * A.lamO[f][n];
-        A.lamO[f][n] = 0.0;
-      }
-    } else {
-      const int f = q - G.nGhost;
-      const long long n = G.fnode[f];
-      A.lamFnew[2 * f] += A.lamO[0][n];
-      A.lamFnew[2 * f + 1] += A.lamO[4][n];
-      A.lamO[0][n] = 0.0;
-      A.lamO[4][n] = 0.0;
+// values back to the filter nodes. Phase 1: consume the adjoints of everything k_ghost wrote (with, on a
+// step whose result enters J, the objective's adjoint at the ghost nodes first).
+__device__ __forceinline__ void adj_ghost_consume_item(const Grid& G, const AdjPtrs& A, double* ipbar,
+                                                       const AdjBcParams& P, int q) {
+  if (q < G.nGhost) {
+    const long long n = G.gnode[q];
+    const double sgn[5] = {1, -1, -1, -1, 1};
+    double lam[5];
+    for (int f = 0; f < 5; ++f) lam[f] = A.lamO[f][n];
+    if (P.objective) adj_objective_term(G, P.objVal, P.nx, P.dA, P.weight, q, lam);
+    for (int f = 0; f < 5; ++f) {
+      ipbar[f * (long long)G.nGhost + q] = sgn[f] * lam[f];
+      A.lamO[f][n] = 0.0;
     }
+  } else {
+    const int f = q - G.nGhost;
+    const long long n = G.fnode[f];
+    A.lamFnew[2 * f] += A.lamO[0][n];
+    A.lamFnew[2 * f + 1] += A.lamO[4][n];
+    A.lamO[0][n] = 0.0;
+    A.lamO[4][n] = 0.0;
   }
 }
 
 // Phase 2: every image-point cell node gathers weight x image-point adjoint from the ghosts that read it
 // (reverse map in CSR form: entries 8 * ghost + corner).
-__global__ void k_adj_ghost_gather(const Grid* __restrict__ gp, AdjPtrs A, const double* __restrict__ ipbar,
-                                   const long long* __restrict__ cnode, const int* __restrict__ coff,
-                                   const int* __restrict__ cent, int ncell) {
-  const Grid& G = *gp;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-    const long long m = cnode[c];
-    double a[5] = {0, 0, 0, 0, 0};
-    for (int e = coff[c]; e < coff[c + 1]; ++e) {
-      const int q = cent[e] >> 3, slot = cent[e] & 7;
-      const double wn = G.gw[16 * (long long)q + slot], wd = G.gw[16 * (long long)q + 8 + slot];
-      a[0] += wn * ipbar[q];
-      a[4] += wn * ipbar[4 * (long long)G.nGhost + q];
-      for (int f = 1; f < 4; ++f) a[f] += wd * ipbar[f * (long long)G.nGhost + q];
-    }
-    if (G.type[m] & FILTER_BIT) {  // k_ghost read the filtered values of this node
-      const int f = G.fidx[m];
-      A.lamFnew[2 * f] += a[0];
-      A.lamFnew[2 * f + 1] += a[4];
-    } else {
-      A.lamO[0][m] += a[0];
-      A.lamO[4][m] += a[4];
-    }
-    for (int f = 1; f < 4; ++f) A.lamO[f][m] += a[f];
+__device__ __forceinline__ void adj_ghost_gather_item(const Grid& G, const AdjPtrs& A, const double* ipbar,
+                                                      const AdjBcParams& P, int c) {
+  const long long m = P.cnode[c];
+  double a[5] = {0, 0, 0, 0, 0};
+  for (int e = P.coff[c]; e < P.coff[c + 1]; ++e) {
+    const int q = P.cent[e] >> 3, slot = P.cent[e] & 7;
+    const double wn = G.gw[16 * (long long)q + slot], wd = G.gw[16 * (long long)q + 8 + slot];
+    a[0] += wn * ipbar[q];
+    a[4] += wn * ipbar[4 * (long long)G.nGhost + q];
+    for (int f = 1; f < 4; ++f) a[f] += wd * ipbar[f * (long long)G.nGhost + q];
   }
+  if (G.type[m] & FILTER_BIT) {  // k_ghost read the filtered values of this node
+    const int f = G.fidx[m];
+    A.lamFnew[2 * f] += a[0];
+    A.lamFnew[2 * f + 1] += a[4];
+  } else {
+    A.lamO[0][m] += a[0];
+    A.lamO[4][m] += a[4];
+  }
+  for (int f = 1; f < 4; ++f) A.lamO[f][m] += a[f];
 }
 
 // ------------------------------------------------------------------------------- near-body filter
 // k_body_filter: fpre = O at the filter node, fnew = (6 O[n] + sum of the 6 neighbours)/12 (rho, rho_E).
 // Every node of the filter stencils gathers from the filter nodes whose stencil holds it.
-__global__ void k_adj_filter(const Grid* __restrict__ gp, AdjPtrs A, const long long* __restrict__ nodes, int count) {
-  const Grid& G = *gp;
+__device__ __forceinline__ void adj_filter_item(const Grid& G, const AdjPtrs& A, const long long* nodes, int q) {
   const long long off[6] = {G.sI, -G.sI, G.sJ, -G.sJ, 1, -1};
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
-    const long long m = nodes[q];
-    double ar = 0, ae = 0;
-    if (G.type[m] & FILTER_BIT) {
-      const int f = G.fidx[m];
-      ar += 0.5 * A.lamFnew[2 * f] + A.lamFpre[2 * f];
-      ae += 0.5 * A.lamFnew[2 * f + 1] + A.lamFpre[2 * f + 1];
-    }
-    for (int d = 0; d < 6; ++d) {
-      const long long n = m + off[d];
-      if (n < 0 || n >= G.N || !(G.type[n] & FILTER_BIT)) continue;
-      const int f = G.fidx[n];
-      ar += A.lamFnew[2 * f] / 12;
-      ae += A.lamFnew[2 * f + 1] / 12;
-    }
-    A.lamO[0][m] += ar;
-    A.lamO[4][m] += ae;
+  const long long m = nodes[q];
+  double ar = 0, ae = 0;
+  if (G.type[m] & FILTER_BIT) {
+    const int f = G.fidx[m];
+    ar += 0.5 * A.lamFnew[2 * f] + A.lamFpre[2 * f];
+    ae += 0.5 * A.lamFnew[2 * f + 1] + A.lamFpre[2 * f + 1];
   }
+  for (int d = 0; d < 6; ++d) {
+    const long long n = m + off[d];
+    if (n < 0 || n >= G.N || !(G.type[n] & FILTER_BIT)) continue;
+    const int f = G.fidx[n];
+    ar += A.lamFnew[2 * f] / 12;
+    ae += A.lamFnew[2 * f + 1] / 12;
+  }
+  A.lamO[0][m] += ar;
+  A.lamO[4][m] += ae;
 }
 
-
 // -------------------------------------------------------------------------------- edge boundaries
-// One axis, both faces, same launch geometry as k_edge_bc. Phase 1 (periodic, outlet, inlet part 1):
-// consume the adjoint of every edge node; periodic and outlet add to their (one-to-one) source nodes,
-// the inlet keeps the adjoint of its filtered extrapolated density per node for phase 2.
-// The grid descriptor is a kernel parameter: the face boxes and sizes come from the constant bank, so the
-// first memory access of a thread is its own adjoint load.
-__global__ void k_adj_edge(const __grid_constant__ Grid G, const EdgeBlock* __restrict__ blocks, AdjPtrs A, int axis,
-                           const StepCtl* __restrict__ roles, int s, double* __restrict__ fbar,
-                           double* __restrict__ lamInflow) {
-  const double stageT = roles->stageT[s];
+// One node of an edge block (k_edge_bc's geometry: 32 x kEdgeRows nodes, (tx, ty) within it). Phase 1
+// (periodic, outlet, inlet part 1): consume the adjoint of the edge node; periodic and outlet add to their
+// (one-to-one) source nodes, the inlet keeps the adjoint of its filtered extrapolated density per node for
+// phase 2.
+__device__ __forceinline__ void adj_edge_item(const Grid& G, const EdgeBlock& eb, int tx, int ty, const AdjPtrs& A,
+                                              const double* const val[5], int axis, double stageT, double* fbar,
+                                              double* lamInflow) {
   const Consts& C = G.C;
-  const EdgeBlock eb = blocks[blockIdx.x];
   const int e = eb.e;
   const int* b = G.eBox[e];
   const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
-  const int a = eb.a0 + threadIdx.y;
-  const int bb = eb.b0 + threadIdx.x;
+  const int a = eb.a0 + ty;
+  const int bb = eb.b0 + tx;
   if (a > b[2 * ax1 + 1] || bb > b[2 * ax2 + 1]) return;
   int ijk[3];
   ijk[axis] = b[2 * axis];
@@ -195,9 +183,9 @@ __global__ void k_adj_edge(const __grid_constant__ Grid G, const EdgeBlock* __re
     for (int f = 0; f < 5; ++f) A.lamO[f][m] += lam[f];
   } else if (bc == NSF_BC_OUTLET) {
     const long long a1 = side == 0 ? n + st : n - st, a2 = side == 0 ? n + 2 * st : n - 2 * st;
-    const double rho = 2 * A.val[0][a1] - A.val[0][a2];
+    const double rho = 2 * val[0][a1] - val[0][a2];
     double u[3];
-    for (int f = 1; f < 4; ++f) u[f - 1] = (2 * A.val[f][a1] - A.val[f][a2]) / (1 + rho);
+    for (int f = 1; f < 4; ++f) u[f - 1] = (2 * val[f][a1] - val[f][a2]) / (1 + rho);
     // rho_E = (1 + rho)/2 |u|^2 with u = m/(1 + rho): d/drho = -|u|^2/2, d/dm = u
     const double rbar = lam[0] - 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) * lam[4];
     A.lamO[0][a1] += 2 * rbar;
@@ -211,7 +199,7 @@ __global__ void k_adj_edge(const __grid_constant__ Grid G, const EdgeBlock* __re
     // rho = f (filtered extrapolation); u_axis = ramp * M0 * profile; T = 0; p = rho / gamma
     const long long s1 = ax1 == 0 ? G.sI : G.sJ, s2 = ax2 == 1 ? G.sJ : 1;
     auto ext = [&](long long m) {
-      return 2 * A.val[0][side == 0 ? m + st : m - st] - A.val[0][side == 0 ? m + 2 * st : m - 2 * st];
+      return 2 * val[0][side == 0 ? m + st : m - st] - val[0][side == 0 ? m + 2 * st : m - 2 * st];
     };
     double f = 0;
     unsigned nn = 0;
@@ -233,14 +221,13 @@ __global__ void k_adj_edge(const __grid_constant__ Grid G, const EdgeBlock* __re
 
 // Inlet phase 2 (x faces only): every node of the two planes behind the inlet gathers from the inlet
 // nodes whose filtered extrapolation used it.
-__global__ void k_adj_inlet_gather(const __grid_constant__ Grid G, const EdgeBlock* __restrict__ blocks, AdjPtrs A,
-                                   const double* __restrict__ fbar) {
-  const EdgeBlock eb = blocks[blockIdx.x];  // the x faces' blocks; only inlet faces gather
-  const int e = eb.e;
+__device__ __forceinline__ void adj_inlet_gather_item(const Grid& G, const EdgeBlock& eb, int tx, int ty,
+                                                      const AdjPtrs& A, const double* fbar) {
+  const int e = eb.e;  // the x faces' blocks; only inlet faces gather
   if (G.eBc[e] != NSF_BC_INLET) return;
   const int* b = G.eBox[e];
-  const int a = eb.a0 + threadIdx.y;   // j
-  const int bb = eb.b0 + threadIdx.x;  // k
+  const int a = eb.a0 + ty;   // j
+  const int bb = eb.b0 + tx;  // k
   if (a > b[3] || bb > b[5]) return;
   const int side = G.eSide[e];
   const long long base = side ? (long long)G.NJ * G.NKp : 0;
@@ -263,8 +250,6 @@ __global__ void k_adj_inlet_gather(const __grid_constant__ Grid G, const EdgeBlo
 }
 
 // ------------------------------------------------------------------------------------------ stage
-// RK4 combine at the interior nodes: s = 0: O = U0 + inc k, acc = k; s = 1, 2: O = U0 + inc k,
-// acc += 2 k; s = 3: O = U0 + dt/6 (acc + k). Writes the RHS adjoint lam (zero elsewhere beforehand).
 // Before the stage kernel's adjoint: the RK4 combine's adjoint and the stage's RHS input quantities.
 // Combine (interior fluid nodes; lam is zero elsewhere): with o = the adjoint of the stage output,
 //   stage 1:    k = dt/2 o + acc, acc = 0      stages 2, 3: k = inc o + 2 acc      stage 4: k = dt/6 o, acc += k
@@ -275,79 +260,125 @@ __global__ void k_adj_inlet_gather(const __grid_constant__ Grid G, const EdgeBlo
 // k = NK-2 it computed: their adjoints are gathered here, before the combine's.
 // Solid nodes (ghost and inactive): the adjoint of k_solid_copy, which copied the stage input into the
 // output of the fields in solidMask (bit 0: the density from R) before the edge conditions.
-__global__ void k_adj_prepare(const Grid* __restrict__ gp, AdjPtrs A, int s, const StepCtl* __restrict__ roles,
-                              int solidMask, double* __restrict__ lam, double* __restrict__ V) {
-  const Grid& G = *gp;
-  const double dtUsed = roles->dtUsed;
+__device__ __forceinline__ void adj_prepare_item(const Grid& G, const AdjPtrs& A, int s, double dtUsed, int solidMask,
+                                                 double* __restrict__ lam, double* __restrict__ V, long long n) {
   const double inc = s == 2 ? dtUsed : dtUsed / 2, dtF = dtUsed / 6;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x) {
-    // every load first (about twenty independent loads in flight per thread), then the arithmetic
-    const uint8_t ty = G.type[n];
-    const bool interior = (ty & TYPE_MASK) == FLUID_INTERIOR;
-    const double m1 = A.val[1][n], m2 = A.val[2][n], m3 = A.val[3][n], e4 = A.val[4][n];
-    double rho = A.valR[n], rE = e4;
-    double o[5], acc[5], u0[5], oz[5] = {0, 0, 0, 0, 0};
-    // the z copy the stage kernel wrote with this node
-    const bool zCopy = (ty & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT)) != 0;
-    const long long nz = (ty & ZCOPY_UP_BIT) ? n + (G.NK - 2) : n - (G.NK - 2);
-    if (interior)
-      for (int f = 0; f < 5; ++f) {
-        o[f] = A.lamO[f][n];
-        acc[f] = A.lamAcc[f][n];
-        u0[f] = A.lamU0[f][n];
-        if (zCopy) oz[f] = A.lamO[f][nz];
-      }
-    if (ty & FILTER_BIT) {
-      const int f = G.fidx[n];
-      rho = A.valFpre[2 * f];
-      rE = A.valFpre[2 * f + 1];
-      // the near-body filter's adjoints were consumed by k_adj_filter: clear them for the transposed RHS
-      // (fpre) and the previous stage's ghosts (fnew)
-      A.lamFpre[2 * f] = 0.0;
-      A.lamFpre[2 * f + 1] = 0.0;
-      A.lamFnew[2 * f] = 0.0;
-      A.lamFnew[2 * f + 1] = 0.0;
-    }
-    const Prim pr = prims_of_nr(G.C, rho, m1, m2, m3, rE);  // as the stage kernel's staging warps
-    const double q[11] = {m1, m2, m3, e4, pr.u, pr.v, pr.w, pr.p, pr.T, pr.mu, pr.ka};
-    for (int v = 0; v < 11; ++v) V[v * G.N + n] = q[v];
-    if (!interior) {
-      for (int f = 0; f < 5; ++f) lam[f * G.N + n] = 0.0;
-      const uint8_t t = ty & TYPE_MASK;
-      if (solidMask && (t == SOLID_GHOST || t == SOLID_INACTIVE)) {
-        if (solidMask & 1) {
-          A.lamR[n] += A.lamO[0][n];
-          A.lamO[0][n] = 0.0;
-        }
-        for (int f = 1; f < 5; ++f)
-          if (solidMask & (1 << f)) {
-            A.lamI[f][n] += A.lamO[f][n];
-            A.lamO[f][n] = 0.0;
-          }
-      }
-      continue;
-    }
-    if (zCopy)
-      for (int f = 0; f < 5; ++f) {
-        o[f] += oz[f];
-        A.lamO[f][nz] = 0.0;
-      }
+  // every load first (about twenty independent loads in flight per thread), then the arithmetic
+  const uint8_t ty = G.type[n];
+  const bool interior = (ty & TYPE_MASK) == FLUID_INTERIOR;
+  const double m1 = A.val[1][n], m2 = A.val[2][n], m3 = A.val[3][n], e4 = A.val[4][n];
+  double rho = A.valR[n], rE = e4;
+  double o[5], acc[5], u0[5], oz[5] = {0, 0, 0, 0, 0};
+  // the z copy the stage kernel wrote with this node
+  const bool zCopy = (ty & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT)) != 0;
+  const long long nz = (ty & ZCOPY_UP_BIT) ? n + (G.NK - 2) : n - (G.NK - 2);
+  if (interior)
     for (int f = 0; f < 5; ++f) {
-      double k;
-      if (s == 0) {
-        k = inc * o[f] + acc[f];
-        A.lamAcc[f][n] = 0.0;
-      } else if (s < 3) {
-        k = inc * o[f] + 2 * acc[f];
-      } else {
-        k = dtF * o[f];
-        A.lamAcc[f][n] = acc[f] + dtF * o[f];
-      }
-      lam[f * G.N + n] = k;
-      A.lamU0[f][n] = u0[f] + o[f];
-      A.lamO[f][n] = 0.0;
+      o[f] = A.lamO[f][n];
+      acc[f] = A.lamAcc[f][n];
+      u0[f] = A.lamU0[f][n];
+      if (zCopy) oz[f] = A.lamO[f][nz];
     }
+  if (ty & FILTER_BIT) {
+    const int f = G.fidx[n];
+    rho = A.valFpre[2 * f];
+    rE = A.valFpre[2 * f + 1];
+    // the near-body filter's adjoints were consumed by the filter phase: clear them for the transposed
+    // RHS (fpre) and the previous stage's ghosts (fnew)
+    A.lamFpre[2 * f] = 0.0;
+    A.lamFpre[2 * f + 1] = 0.0;
+    A.lamFnew[2 * f] = 0.0;
+    A.lamFnew[2 * f + 1] = 0.0;
   }
+  const Prim pr = prims_of_nr(G.C, rho, m1, m2, m3, rE);  // as the stage kernel's staging warps
+  const double q[11] = {m1, m2, m3, e4, pr.u, pr.v, pr.w, pr.p, pr.T, pr.mu, pr.ka};
+  for (int v = 0; v < 11; ++v) V[v * G.N + n] = q[v];
+  if (!interior) {
+    for (int f = 0; f < 5; ++f) lam[f * G.N + n] = 0.0;
+    const uint8_t t = ty & TYPE_MASK;
+    if (solidMask && (t == SOLID_GHOST || t == SOLID_INACTIVE)) {
+      if (solidMask & 1) {
+        A.lamR[n] += A.lamO[0][n];
+        A.lamO[0][n] = 0.0;
+      }
+      for (int f = 1; f < 5; ++f)
+        if (solidMask & (1 << f)) {
+          A.lamI[f][n] += A.lamO[f][n];
+          A.lamO[f][n] = 0.0;
+        }
+    }
+    return;
+  }
+  if (zCopy)
+    for (int f = 0; f < 5; ++f) {
+      o[f] += oz[f];
+      A.lamO[f][nz] = 0.0;
+    }
+  for (int f = 0; f < 5; ++f) {
+    double k;
+    if (s == 0) {
+      k = inc * o[f] + acc[f];
+      A.lamAcc[f][n] = 0.0;
+    } else if (s < 3) {
+      k = inc * o[f] + 2 * acc[f];
+    } else {
+      k = dtF * o[f];
+      A.lamAcc[f][n] = acc[f] + dtF * o[f];
+    }
+    lam[f * G.N + n] = k;
+    A.lamU0[f][n] = u0[f] + o[f];
+    A.lamO[f][n] = 0.0;
+  }
+}
+
+// ----------------------------------------------------------------------- two launches per stage
+// Everything of a stage's adjoint before the transposed RHS, in the forward kernels' reverse order. The
+// boundary work runs as phases of one cooperative launch: ghost consume (and the objective) | ghost gather
+// | near-body filter | edges z | y | x | inlet gather. Each phase reads what the one before it wrote
+// anywhere in the grid, so a grid barrier (bounded: a wait that gives up marks the run invalid through
+// StepCtl::timeout) separates non-empty phases. Every phase is a thread-stride loop over its items; an
+// edge block counts 64 items (32 x kEdgeRows nodes). The RK4 combine and RHS inputs, one item per node,
+// follow as a kernel of their own (measured faster than a last phase of the cooperative launch, whose
+// grid is sized for the few boundary items).
+constexpr int kAdjBcThreads = 256, kAdjBcBlocksPerSM = 4;  // registers capped for 4 resident blocks per SM
+__global__ void __launch_bounds__(kAdjBcThreads, kAdjBcBlocksPerSM)
+    k_adj_bc(const __grid_constant__ Grid G, const __grid_constant__ AdjBcParams P, int s) {
+  const AdjPtrs& A = P.A;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+  bool started = false;
+  auto barrier = [&](long long count) {
+    if (count == 0) return false;
+    if (started) grid_barrier(P.sync, gridDim.x, P.timeout);
+    started = true;
+    return true;
+  };
+  if (barrier(G.nGhost + G.nFilter))
+    for (int v = gtid; v < G.nGhost + G.nFilter; v += nthr) adj_ghost_consume_item(G, A, P.ipbar, P, v);
+  if (barrier(P.ncell))
+    for (int v = gtid; v < P.ncell; v += nthr) adj_ghost_gather_item(G, A, P.ipbar, P, v);
+  if (barrier(P.nfs))
+    for (int v = gtid; v < P.nfs; v += nthr) adj_filter_item(G, A, P.fsNodes, v);
+  const double stageT = P.roles->stageT[s];
+  for (int axis = 2; axis >= 0; --axis)  // z, y, then x
+    if (barrier(P.nEdge[axis]))
+      for (int v = gtid; v < 64 * P.nEdge[axis]; v += nthr) {
+        const int lane = v & 63;
+        adj_edge_item(G, P.edges[axis][v >> 6], lane & 31, lane >> 5, A, P.edgeVal, axis, stageT, P.fbar,
+                      P.lamInflow);
+      }
+  if (barrier(P.inletGather ? P.nEdge[0] : 0))
+    for (int v = gtid; v < 64 * P.nEdge[0]; v += nthr) {
+      const int lane = v & 63;
+      adj_inlet_gather_item(G, P.edges[0][v >> 6], lane & 31, lane >> 5, A, P.fbar);
+    }
+}
+
+// The RK4 combine's adjoint and the RHS inputs: one thread per node.
+__global__ void __launch_bounds__(256) k_adj_combine(const __grid_constant__ Grid G, const __grid_constant__ AdjBcParams P,
+                                                     int s) {
+  const double dtUsed = P.roles->dtUsed;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x)
+    adj_prepare_item(G, P.A, s, dtUsed, P.solidMask, P.lam, P.V, n);
 }
 
 // Several device-to-device copies in one launch (blockIdx.y: the copy).
@@ -549,41 +580,29 @@ void launch_fpre_init_adj(const Grid* dg, int nFilter, const double* lamFpre, do
     k_fpre_init_adj<<<blocks_for(nFilter, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, lamFpre, lamRho, lamRE);
 }
 
-void launch_adj_objective(const Grid* dg, const AdjPtrs& A, int nGhost, const double* nx, double dA, double weight,
-                          int nSM, void* stream) {
-  if (nGhost > 0)
-    k_adj_objective<<<blocks_for(nGhost, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, nx, dA, weight);
-}
-
-void launch_adj_ghost(const Grid* dg, const AdjPtrs& A, int nGhost, int nFilter, double* ipbar, const long long* cnode,
-                      const int* coff, const int* cent, int ncell, int nSM, void* stream) {
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (nGhost + nFilter > 0) k_adj_ghost_consume<<<blocks_for(nGhost + nFilter, nSM), 256, 0, st>>>(dg, A, ipbar);
-  if (ncell > 0) k_adj_ghost_gather<<<blocks_for(ncell, nSM), 256, 0, st>>>(dg, A, ipbar, cnode, coff, cent, ncell);
-}
-
-void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes, int count, int nFilter, int nSM,
-                       void* stream) {
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  (void)nFilter;  // the filter adjoints are cleared by the combine kernel of the same stage
-  if (count > 0) k_adj_filter<<<blocks_for(count, nSM), 256, 0, st>>>(dg, A, nodes, count);
-}
-
-void launch_adj_edge(const Grid& hg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
-                     double* fbar, double* lamInflow, bool inletGather, void* stream) {
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (L.nEdgeBlocks[axis] == 0) return;
-  k_adj_edge<<<L.nEdgeBlocks[axis], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocks[axis], A, axis, roles, s, fbar,
-                                                                  lamInflow);
-  if (axis == 0 && inletGather)
-    k_adj_inlet_gather<<<L.nEdgeBlocks[0], dim3(32, kEdgeRows), 0, st>>>(hg, L.edgeBlocks[0], A, fbar);
-}
-
-
-void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, int solidMask,
-                        double* lam, double* V, int nSM, void* stream) {
-  k_adj_prepare<<<blocks_for(hg.N, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(dg, A, s, roles,
-                                                                                      hg.nSolid ? solidMask : 0, lam, V);
+void launch_adj_bc(const Grid& hg, const AdjBcParams& P, int s, int nSM, void* stream) {
+  static int perSM = -1;
+  if (perSM < 0) {
+    int nb = 0;
+    perSM = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_adj_bc, kAdjBcThreads, 0) == cudaSuccess ? nb : 0;
+  }
+  // enough blocks for the largest phase, all resident (cooperative launch)
+  long long items = std::max<long long>(hg.nGhost + hg.nFilter, 64ll * std::max(P.nEdge[0], std::max(P.nEdge[1], P.nEdge[2])));
+  items = std::max<long long>(items, std::max(P.ncell, P.nfs));
+  const long long want = std::max<long long>(1, (items + kAdjBcThreads - 1) / kAdjBcThreads);
+  const long long cap = (long long)(perSM > 0 ? perSM : 1) * nSM;
+  const unsigned blocks = unsigned(want < cap ? want : cap);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kAdjBcThreads);
+  cfg.stream = static_cast<cudaStream_t>(stream);
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_adj_bc, hg, P, s);
+  k_adj_combine<<<blocks_for(hg.N, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(hg, P, s);
 }
 
 int adj_kernels_init() {

@@ -24,20 +24,44 @@ void launch_objective(const Grid* dg, const double* nx, double dA, double weight
 void launch_fpre_init(const Grid* dg, int nFilter, const double* rho, const double* rE, int nSM, void* stream);
 void launch_fpre_init_adj(const Grid* dg, int nFilter, const double* lamFpre, double* lamRho, double* lamRE, int nSM,
                           void* stream);
-void launch_adj_objective(const Grid* dg, const AdjPtrs& A, int nGhost, const double* nx, double dA, double weight,
-                          int nSM, void* stream);
-void launch_adj_ghost(const Grid* dg, const AdjPtrs& A, int nGhost, int nFilter, double* ipbar, const long long* cnode,
-                      const int* coff, const int* cent, int ncell, int nSM, void* stream);
-void launch_adj_filter(const Grid* dg, const AdjPtrs& A, const long long* nodes, int count, int nFilter, int nSM,
-                       void* stream);
-// roles: device copy of the step's control block (stage times, dt).
-void launch_adj_edge(const Grid& hg, const AdjPtrs& A, const LaunchPlan& L, int axis, const StepCtl* roles, int s,
-                     double* fbar, double* lamInflow, bool inletGather, void* stream);
-// The stage kernel's adjoint: prepare = RK4 combine adjoint into lam, the RHS input quantities into V
-// (11 x N) and, at solid nodes, the adjoint of the solid-node copy (solidMask: the stage's copy mask);
-// rhs = transposed RHS gather and the chain rule into the stage input's adjoints.
-void launch_adj_prepare(const Grid* dg, const Grid& hg, const AdjPtrs& A, int s, const StepCtl* roles, int solidMask,
-                        double* lam, double* V, int nSM, void* stream);
+// Everything of a stage's adjoint before the transposed RHS: ghost nodes (and, with `objective`, the
+// objective's adjoint at them), near-body filter and edge conditions in one cooperative launch (k_adj_bc),
+// then the RK4 combine and RHS input quantities (k_adj_combine).
+struct AdjBcParams {
+  AdjPtrs A;
+  // ghosts: image-point adjoints (5 x nGhost), reverse map of the image-point cells (CSR)
+  double* ipbar;
+  const long long* cnode;
+  const int* coff;
+  const int* cent;
+  int ncell;
+  // near-body filter: the nodes of the filter stencils
+  const long long* fsNodes;
+  int nfs;
+  // edge blocks per axis (k_edge_bc's), the values the edge conditions read (the stage output before
+  // them), the inlet's per-node adjoints, the inflow profile's adjoint
+  const EdgeBlock* edges[3];
+  const double* edgeVal[5];
+  int nEdge[3];
+  int inletGather;
+  double* fbar;
+  double* lamInflow;
+  const StepCtl* roles;  // device copy of the step's control block (stage times, dt)
+  // combine: the stage's copy mask, RHS adjoint lam (5 x N) and input quantities V (11 x N)
+  int solidMask;
+  double* lam;
+  double* V;
+  // objective (the last stage of a step whose result enters J): F_x's pressure at the ghost nodes
+  int objective;
+  const double* objVal[5];
+  const double* nx;
+  double dA, weight;
+  unsigned long long* sync;  // grid-barrier arrival counter (zero at creation, only grows)
+  int* timeout;              // StepCtl::timeout of the solver: set when a barrier gives up
+};
+void launch_adj_bc(const Grid& hg, const AdjBcParams& P, int s, int nSM, void* stream);
+// The transposed RHS (gather) and the chain rule through the primitives into the stage input's adjoints,
+// from launch_adj_bc's lam and V.
 void launch_adj_rhs(const Grid* dg, const Grid& hg, const AdjPtrs& A, const double* lam, const double* V, int nSM,
                     void* stream);
 // Kernel attributes (shared-memory size of the transposed RHS); call once before the first launch.

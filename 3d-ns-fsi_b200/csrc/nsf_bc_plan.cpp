@@ -226,6 +226,8 @@ void bc_flatten(const std::vector<const BcMemberLevels*>& members, BcFlat& out) 
   int levels = 0;
   for (const BcMemberLevels* m : members) levels = std::max(levels, m->levels);
   out.levels = levels;
+  out.memberLevels.clear();
+  for (const BcMemberLevels* m : members) out.memberLevels.push_back(m->levels);
   out.edges.clear();
   out.items.clear();
   out.edgeStart.assign(size_t(levels) * (M + 1), 0);

@@ -592,12 +592,13 @@ nsf_status build_device(nsf_solver* s) {
     L.bcLevels = fl.levels;
     if (L.bcBlocks > 0) {
       if ((st = upload(s, &L.bcBlockStart, ranges)) != NSF_OK) return st;
+      if ((st = upload(s, &L.bcMemberLevels, fl.memberLevels)) != NSF_OK) return st;
       L.filterBlocks = std::max(L.filterBlocks, L.bcBlocks);  // one norm slot per block of the fused kernel
       if ((st = upload(s, &L.bcEdges, fl.edges)) != NSF_OK) return st;
       if ((st = upload(s, &L.bcEdgeStart, fl.edgeStart)) != NSF_OK) return st;
       if ((st = upload(s, &L.bcItems, fl.items)) != NSF_OK) return st;
       if ((st = upload(s, &L.bcItemStart, fl.itemStart)) != NSF_OK) return st;
-      const std::vector<unsigned long long> zero(2, 0ull);
+      const std::vector<unsigned long long> zero(3, 0ull);
       if ((st = upload(s, &L.bcSync, zero)) != NSF_OK) return st;
     }
   }

@@ -171,8 +171,11 @@ struct BcParams {
   const int* edgeStart;
   const int* items;
   const int* itemStart;
-  unsigned long long* sync;  // arrival counters: [0] the level barrier, [1 + g] member g's blocks done (stage 4)
+  // arrival counters: [1 + g] member g's blocks done (stage 4), [1 + members + g] member g's level barrier
+  // (members share no boundary data, so each member's blocks wait for one another only)
+  unsigned long long* sync;
   const int* blockStart;     // members + 1: the blocks of member g are blockStart[g] .. blockStart[g + 1] - 1
+  const int* memberLevels;   // members: the levels member g has (at most `levels`)
   int levels, members;
 };
 
@@ -192,6 +195,7 @@ struct BcMemberInput {  // device node indices (the padded device layout)
 };
 struct BcFlat {
   int levels = 0;
+  std::vector<int> memberLevels;  // each member's own level count
   long long maxWork = 1;         // threads one member needs in its busiest level (the largest over members)
   std::vector<long long> work;   // the same per member
   std::vector<EdgeBlock> edges;
@@ -214,11 +218,12 @@ struct LaunchPlan {
   int bcBlocks;
   int* bcBlockStart;
   int bcLevels;
+  int* bcMemberLevels;
   EdgeBlock* bcEdges;  // device arrays of BcParams
   int* bcEdgeStart;
   int* bcItems;
   int* bcItemStart;
-  unsigned long long* bcSync;  // device, 1 + members counters, zero at creation
+  unsigned long long* bcSync;  // device, 1 + 2 members counters, zero at creation
   int nSlots;
   bool hasBodies;
   bool hasFilter, hasGhostWork, hasSolid;

@@ -39,6 +39,7 @@ struct nsf_ensemble {
   std::vector<void*> allocs;
   std::string err;
   int tile = STAGE_TILE_32x8;
+  int forceTile = -1;  // >= 0: this tile shape, no tuning (the tuner's own ensembles)
 };
 
 namespace {
@@ -166,25 +167,55 @@ nsf_status tune(const nsf_config& cfg, int device, const char* cache, Tuned& out
   return NSF_OK;
 }
 
+nsf_status create_ensemble(const nsf_config* cfgs, uint32_t n, int32_t device, const char* tune_cache, int forceTile,
+                           nsf_ensemble** out);
+
+// The ensemble's tile shape: the stage kernels of throwaway ensembles of the same members are timed with
+// each tile shape (the ensemble kernel's cost per node depends on the mix of members, not only on each
+// member's shape). Cached per device and composition under "<device>/ensemble/<count>x<NI>x<NJ>x<NK>+...".
+nsf_status tune_ensemble(const nsf_config* cfgs, uint32_t n, int device, const char* cache, Tuned& out,
+                         std::string& err) {
+  std::map<std::string, int> shapes;
+  double nodes = 0;
+  for (uint32_t m = 0; m < n; ++m) {
+    std::ostringstream k;
+    k << cfgs[m].NI << "x" << cfgs[m].NJ << "x" << cfgs[m].NK;
+    ++shapes[k.str()];
+    nodes += double(cfgs[m].NI) * double(cfgs[m].NJ) * double(cfgs[m].NK);
+  }
+  std::ostringstream k;
+  k << device_name(device) << "/ensemble/";
+  bool first = true;
+  for (const auto& kv : shapes) {
+    k << (first ? "" : "+") << kv.second << "x" << kv.first;
+    first = false;
+  }
+  const std::string key = k.str();
+  if (cache_lookup(cache, key, out)) return NSF_OK;
+  for (int tile = 0; tile < 2; ++tile) {
+    nsf_ensemble* t = nullptr;
+    nsf_status st = create_ensemble(cfgs, n, device, nullptr, tile, &t);
+    double stage[4] = {0, 0, 0, 0}, step = 0;
+    if (st == NSF_OK) st = nsf_ensemble_profile_steps(t, 2, stage, &step);
+    if (st == NSF_OK) st = nsf_ensemble_profile_steps(t, 4, stage, &step);
+    if (st != NSF_OK) {
+      err = std::string("ensemble autotune: ") + (t ? t->err : std::string("create failed"));
+      nsf_ensemble_destroy(t);
+      return st;
+    }
+    nsf_ensemble_destroy(t);
+    out.nsPerNode[tile] = 1e6 * (stage[0] + stage[1] + stage[2] + stage[3]) / 4 / nodes;
+  }
+  out.tile = out.nsPerNode[1] < out.nsPerNode[0] ? STAGE_TILE_16x16 : STAGE_TILE_32x8;
+  cache_store(cache, key, out);
+  return NSF_OK;
+}
+
 nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
   const int M = int(e->members.size());
-  // tile shape: the one with the smaller tuned total time over all members (32 x 8 without a cache)
-  if (cache) {
-    std::map<std::string, Tuned> byShape;
-    double total[2] = {0, 0};
-    for (nsf_solver* s : e->members) {
-      const std::string key = shape_key(e->device, s->cfg);
-      if (!byShape.count(key)) {
-        Tuned t;
-        nsf_status st = tune(s->cfg, e->device, cache, t, e->err);
-        if (st != NSF_OK) return st;
-        byShape[key] = t;
-      }
-      const double nodes = double(s->cfg.NI) * double(s->cfg.NJ) * double(s->cfg.NK);
-      for (int v = 0; v < 2; ++v) total[v] += byShape[key].nsPerNode[v] * nodes;
-    }
-    e->tile = total[1] < total[0] ? STAGE_TILE_16x16 : STAGE_TILE_32x8;
-  }
+  // tile shape: chosen by create_ensemble (forced or tuned), 32 x 8 without a cache
+  (void)cache;
+  if (e->forceTile >= 0) e->tile = e->forceTile;
   // members: ordinary solver handles on this device with the chosen tile shape
   for (nsf_solver* s : e->members) {
     s->tileRequest = e->tile;
@@ -279,12 +310,13 @@ nsf_status build_ensemble(nsf_ensemble* e, const char* cache) {
         return NSF_OK;
       };
       if ((st = up(&L.bcBlockStart, ranges)) != NSF_OK) return st;
+      if ((st = up(&L.bcMemberLevels, fl.memberLevels)) != NSF_OK) return st;
       if ((st = up(&L.bcEdges, fl.edges)) != NSF_OK) return st;
       if ((st = up(&L.bcEdgeStart, fl.edgeStart)) != NSF_OK) return st;
       if ((st = up(&L.bcItems, fl.items)) != NSF_OK) return st;
       if ((st = up(&L.bcItemStart, fl.itemStart)) != NSF_OK) return st;
-      if ((st = ens_alloc(e, &L.bcSync, size_t(M) + 1)) != NSF_OK) return st;
-      CKE(cudaMemset(L.bcSync, 0, (size_t(M) + 1) * sizeof(unsigned long long)));
+      if ((st = ens_alloc(e, &L.bcSync, 2 * size_t(M) + 1)) != NSF_OK) return st;
+      CKE(cudaMemset(L.bcSync, 0, (2 * size_t(M) + 1) * sizeof(unsigned long long)));
     }
   }
   // member grids: the stage kernel adds its norm partials into slot 0 of each member, the near-body
@@ -334,10 +366,25 @@ nsf_status nsf_autotune(const nsf_config* cfg, int32_t device, const char* cache
 
 nsf_status nsf_ensemble_create(const nsf_config* cfgs, uint32_t n, int32_t device, const char* tune_cache,
                                nsf_ensemble** out) {
+  return create_ensemble(cfgs, n, device, tune_cache, -1, out);
+}
+
+}  // extern "C"
+
+namespace {
+nsf_status create_ensemble(const nsf_config* cfgs, uint32_t n, int32_t device, const char* tune_cache, int forceTile,
+                           nsf_ensemble** out) {
   if (!cfgs || !out || n == 0 || device < 0) return NSF_ERR_ARG;
   auto* e = new nsf_ensemble;
   *out = e;
   e->device = device;
+  if (forceTile < 0 && tune_cache) {  // throwaway ensembles time both tile shapes (once per composition)
+    Tuned t;
+    const nsf_status st = tune_ensemble(cfgs, n, device, tune_cache, t, e->err);
+    if (st != NSF_OK) return st;
+    forceTile = t.tile;
+  }
+  e->forceTile = forceTile;
   cudaDeviceProp prop{};
   if (cudaSetDevice(device) != cudaSuccess || cudaGetDeviceProperties(&prop, device) != cudaSuccess ||
       prop.major != 10) {
@@ -360,6 +407,9 @@ nsf_status nsf_ensemble_create(const nsf_config* cfgs, uint32_t n, int32_t devic
   }
   return build_ensemble(e, tune_cache);
 }
+}  // namespace
+
+extern "C" {
 
 nsf_status nsf_ensemble_march(nsf_ensemble* e, uint64_t nsteps) {
   if (!e || !e->graphExec) return NSF_ERR_STATE;

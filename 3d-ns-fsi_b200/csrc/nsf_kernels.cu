@@ -654,46 +654,24 @@ __global__ void k_download_inactive(const Grid* __restrict__ gp, const long long
 // bcBlocks blocks (a consecutive range of them per member, sized by its work), in the dependency levels of
 // nsf_bc_plan.cpp: level 0
 // holds the solid-node copies and every edge, filter and ghost-pass item whose inputs are final after the
-// stage kernel; each later level reads what earlier levels wrote anywhere in the grid, so a grid barrier
-// separates levels and those reads go through L2 (__ldcg in the item functions). The member's Grid and
-// control block are copied to shared memory first (every item reads them). Stage 4 then flushes the dt
-// maxima, change norms and NaN flag and, after one more barrier, block 0 of each member runs the end-of-step
-// finalize. Every block passes every barrier (an inactive member's blocks do no work), so the launch is
-// cooperative (all blocks resident).
+// stage kernel; each later level reads what earlier levels wrote anywhere in the member's grid, so a barrier
+// over the member's blocks separates levels (members share nothing, an ensemble's members do not wait for
+// one another, and each member runs only its own levels) and those reads go through L2 (__ldcg in the item
+// functions). The member's Grid and control block are copied to shared memory first (every item reads
+// them). Stage 4 then flushes the dt maxima, change norms and NaN flag, and the member's last block to
+// finish runs the end-of-step finalize. Every block of a member passes every barrier of that member (an
+// inactive member's blocks do no work), so the launch is cooperative (all blocks resident).
 
-// Bounded grid barrier over nb blocks on a 64-bit arrival counter that only grows: every barrier instance
-// takes exactly nb arrivals, so an arrival that reads `old` belongs to instance old / nb and waits until
-// the counter reaches (old / nb + 1) * nb (release on arrival, acquire on the poll). A wait longer than
-// kBarrierPolls polls sets StepCtl::timeout and goes on: the run is then reported invalid, nothing hangs.
-constexpr long long kBarrierPolls = 1ll << 24;
-__device__ __forceinline__ unsigned long long atom_add_release(unsigned long long* a, unsigned long long v) {
-  unsigned long long old;
-  asm volatile("atom.add.release.gpu.u64 %0, [%1], %2;" : "=l"(old) : "l"(a), "l"(v) : "memory");
-  return old;
-}
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* a) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(a) : "memory");
-  return v;
-}
-__device__ void grid_barrier(unsigned long long* S, unsigned nb, StepCtl* c) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned long long old = atom_add_release(S, 1ull);
-    const unsigned long long target = (old / nb + 1) * nb;
-    long long it = 0;
-    while (ld_acquire(S) < target) {
-      if (++it > kBarrierPolls) {
-        atomicExch(&c->timeout, 1);
-        break;
-      }
-      __nanosleep(32);
-    }
-  }
-  __syncthreads();
-}
+// Resident blocks of the fused boundary kernel per SM (its registers are capped to fit): the kernel is
+// latency-bound, each member's items spread over its blocks' threads.
+constexpr int kBcBlocksPerSM = 4;
 
-__global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__ BcParams P, int s, int fin) {
+// LAST: stage 4 (s == 3), the one stage with dt terms, change norms and the NaN check; stages 1-3 run the
+// other instantiation, whose item functions see s <= 2 and drop that work and its registers.
+template <bool LAST>
+__global__ void __launch_bounds__(256, kBcBlocksPerSM) k_bc(Grid* grids, const __grid_constant__ BcParams P, int sArg,
+                                                            int fin) {
+  const int s = LAST ? 3 : min(sArg, 2);
   __shared__ double red[5 * 32];
   __shared__ __align__(16) unsigned char gsm[sizeof(Grid)];
   __shared__ __align__(16) unsigned char csm[sizeof(StepCtl)];
@@ -724,7 +702,6 @@ __global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__
   const Grid& G = *reinterpret_cast<const Grid*>(gsm);
   const StepCtl& cs = *reinterpret_cast<const StepCtl*>(csm);  // read-only copy for the item functions
   const bool active = cs.active != 0;
-  const unsigned nb = gridDim.x;
   const int gtid = bx * blockDim.x + tid, nthr = nbx * blockDim.x;
   DtAcc dta;
   double nsum[5] = {0, 0, 0, 0, 0};
@@ -733,8 +710,9 @@ __global__ void __launch_bounds__(256) k_bc(Grid* grids, const __grid_constant__
   // A level's items of every kind form one index range -- solid copies (level 0), edge-block threads (64
   // per block), filter items, ghost-pass items -- and each thread takes every nthr-th index, so items of
   // different kinds run side by side rather than one list after another.
-  for (int L = 0; L < P.levels; ++L) {
-    if (L > 0) grid_barrier(P.sync, nb, c);
+  const int levels = P.memberLevels[g];
+  for (int L = 0; L < levels; ++L) {
+    if (L > 0) grid_barrier(P.sync + 1 + M + g, unsigned(nbx), &c->timeout);
     if (!active) continue;
     const int mask = cs.copyMask[s];
     const int nS = (L == 0 && mask) ? G.nSolid : 0;
@@ -785,6 +763,7 @@ static void launch_bc(Grid* dg, int members, const LaunchPlan& L, int s, bool fi
   P.itemStart = L.bcItemStart;
   P.sync = L.bcSync;
   P.blockStart = L.bcBlockStart;
+  P.memberLevels = L.bcMemberLevels;
   P.levels = L.bcLevels;
   P.members = members;
   cudaLaunchConfig_t cfg{};
@@ -797,12 +776,18 @@ static void launch_bc(Grid* dg, int members, const LaunchPlan& L, int s, bool fi
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_bc, dg, P, s, fin ? 1 : 0);
+  if (s == 3)
+    cudaLaunchKernelEx(&cfg, k_bc<true>, dg, P, s, fin ? 1 : 0);
+  else
+    cudaLaunchKernelEx(&cfg, k_bc<false>, dg, P, s, fin ? 1 : 0);
 }
 
 int bc_capacity(int nSM) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bc, 256, 0) != cudaSuccess) return 0;
+  int nb2 = 0;  // both instantiations run the same plan: the smaller residency bounds it
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bc<true>, 256, 0) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_bc<false>, 256, 0) != cudaSuccess) return 0;
+  nb = nb2 < nb ? nb2 : nb;
   return nb * nSM;
 }
 

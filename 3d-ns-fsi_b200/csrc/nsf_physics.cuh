@@ -159,6 +159,40 @@ __device__ inline void flush_norms(double* slot, const double s[5], double* scra
 }
 
 
+// Bounded grid barrier over nb blocks on a 64-bit arrival counter that only grows: every barrier instance
+// takes exactly nb arrivals, so an arrival that reads `old` belongs to instance old / nb and waits until
+// the counter reaches (old / nb + 1) * nb (release on arrival, acquire on the poll). A wait longer than
+// kBarrierPolls polls sets *timeout (a StepCtl::timeout) and goes on: the run is then reported invalid,
+// nothing hangs.
+constexpr long long kBarrierPolls = 1ll << 24;
+__device__ __forceinline__ unsigned long long atom_add_release(unsigned long long* a, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.add.release.gpu.u64 %0, [%1], %2;" : "=l"(old) : "l"(a), "l"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* a) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(a) : "memory");
+  return v;
+}
+__device__ inline void grid_barrier(unsigned long long* S, unsigned nb, int* timeout) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned long long old = atom_add_release(S, 1ull);
+    const unsigned long long target = (old / nb + 1) * nb;
+    long long it = 0;
+    while (ld_acquire(S) < target) {
+      if (++it > kBarrierPolls) {
+        atomicExch(timeout, 1);
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();  // the block's later loads see what the other blocks wrote before they arrived
+  }
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------------------------------------------
 // Right-hand side of the five flux loops (continuity Solver.cpp:181-196, x/y/z momentum :199-339, energy
 // :342-418) split by direction, for kernels that stream along i and keep the thread's own (j, k) column in

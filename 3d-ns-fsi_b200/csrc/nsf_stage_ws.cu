@@ -29,6 +29,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cstdint>
 
 #include "nsf_device.cuh"
@@ -45,8 +47,21 @@ constexpr long long WAIT_LIMIT = 1ll << 22;  // default polls before a wait is d
 // Register split (setmaxnreg): the launch gives every thread 168 registers (384 x 168 = 64,512); the
 // split must not exceed that total: 128 x 88 + 256 x 208 = 64,512.
 constexpr int REG_LAUNCH = 168, REG_LOW = 88, REG_HIGH = 208;
+// The ensemble's stage-4 instantiation (per-item coefficients and the dt / norm accumulators) gives its
+// column threads 8 more: 128 x 72 + 256 x 216 = 64,512.
+constexpr int REG_LOW_ENS4 = 72, REG_HIGH_ENS4 = 216;
 
 constexpr int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// An ensemble column warp's per-item values, kept in shared memory and read where they are used (through
+// volatile loads): held in registers across the item's loop they would push the column threads past their
+// register budget.
+struct ItemSm {
+  double* out[5];  // stage output fields
+  double* acc;     // accumulator fields (contiguous, N doubles apart)
+  long long N, sI;
+  double inc, dtFactor;
+};
 
 // Tile geometry of one kernel variant: TK x TJ columns (one column thread each, 256 in total).
 template <int TK_, int TJ_>
@@ -71,8 +86,10 @@ struct Tile {
   static constexpr size_t OFF_FLAG = OFF_BAR + 2 * (NC + NP + NE) * 8;
   static constexpr size_t OFF_RED = (OFF_FLAG + 16 + 127) / 128 * 128;
   static constexpr size_t OFF_CTL = OFF_RED + 5 * 32 * 8;
-  // ensemble kernels: one copy of the current member's Consts per column warp
-  static constexpr size_t CSM_BYTES = (sizeof(Consts) + 15) / 16 * 16;
+  // ensemble kernels: per column warp, a copy of the current member's Consts and of the item's output
+  // pointers and step factors (ItemSm)
+  static constexpr size_t CONSTS_BYTES = (sizeof(Consts) + 15) / 16 * 16;
+  static constexpr size_t CSM_BYTES = CONSTS_BYTES + (sizeof(ItemSm) + 15) / 16 * 16;
   static constexpr size_t OFF_CSM = OFF_CTL + ((sizeof(StepCtl) + 127) / 128) * 128;
   static constexpr size_t SMEM = OFF_CSM + 8 * CSM_BYTES;
   static_assert(NCOL == 256, "two column warpgroups");
@@ -83,6 +100,7 @@ struct Tile {
   static_assert(SMEM <= 227 * 1024, "shared memory budget");
   static_assert(NSTAGE * 4 >= HP, "four staging passes cover a plane");
   static_assert(128 * REG_LOW + NCOL * REG_HIGH <= NTHREADS * REG_LAUNCH, "register split exceeds the launch total");
+  static_assert(128 * REG_LOW_ENS4 + NCOL * REG_HIGH_ENS4 <= NTHREADS * REG_LAUNCH, "register split exceeds the launch total");
 };
 }  // namespace ws
 
@@ -160,7 +178,11 @@ __device__ __forceinline__ void dt_terms(const Consts& C, const double (&u)[5], 
 // ENS = true: an ensemble; every work item names its member (StageItem::g) in the device array `grids`,
 // and each member's StepCtl is read from device memory.
 // Work items of CTA b: items[ctaStart[b] .. ctaStart[b + 1]).
-template <int TK_, int TJ_, bool ENS>
+// MODE: which stages an instantiation serves -- 0 any (s at run time), 1 stages 1-3, 2 stage 4 (s == 3, the
+// only stage with dt maxima, change norms and the NaN check; mode 1 carries none of their registers). The
+// single grid runs mode 0 for stages 1-3 and mode 2 for stage 4, an ensemble modes 1 and 2: the fastest
+// pairing measured (mode 1 frees registers an ensemble needs, but its schedule is slower for one grid).
+template <int TK_, int TJ_, bool ENS, int MODE>
 __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
     k_stage_ws(const __grid_constant__ Grid G0, const Grid* __restrict__ grids, const StageItem* __restrict__ items,
                const int* __restrict__ ctaStart, int s) {
@@ -233,7 +255,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
   auto skip = [&](const StageItem& w) { return ENS && !ctl_of(grid_of(w)).active; };
 
   if (warp < 4) {
-    reg_dealloc<REG_LOW>();
+    reg_dealloc<(ENS && MODE == 2) ? REG_LOW_ENS4 : REG_LOW>();
     if (warp == 0) {
       // ------------------------------------------------------------------ producer (one thread)
       if (lane == 0) {
@@ -392,7 +414,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
       }
     }
   } else {
-    reg_alloc<REG_HIGH>();
+    reg_alloc<(ENS && MODE == 2) ? REG_HIGH_ENS4 : REG_HIGH>();
     // -------------------------------------------------------------------- columns (warpgroups 1-2)
     const int ct = tid - 128, tx = ct % TK, ty = ct / TK;
     const int cidx = (ty + 1) * HK + (tx + 1);   // this column's node in a staged plane
@@ -408,29 +430,58 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
       const Grid& G = grid_of(w);
       const StepCtl& ctl = ctl_of(G);
       Consts* const myC = reinterpret_cast<Consts*>(sm + OFF_CSM + (warp - 4) * CSM_BYTES);
+      ItemSm* const myI = reinterpret_cast<ItemSm*>(sm + OFF_CSM + (warp - 4) * CSM_BYTES + TL::CONSTS_BYTES);
+      const double dtUsed = ctl.dtUsed;
       if constexpr (ENS) {  // this warp's copy of the member's coefficients (shared-memory operands)
         __syncwarp();
         const double* src = reinterpret_cast<const double*>(&G.C);
         double* dst = reinterpret_cast<double*>(myC);
         for (int q = lane; q < int(sizeof(Consts) / 8); q += 32) dst[q] = src[q];
+        if (lane == 0) {
+          for (int f = 0; f < 5; ++f) myI->out[f] = ctl.O[s][f];
+          myI->acc = G.acc[0];
+          myI->N = G.N;
+          myI->sI = G.sI;
+          myI->inc = (s == 2) ? dtUsed : dtUsed / 2;
+          myI->dtFactor = dtUsed / 6;
+        }
         __syncwarp();
       }
       const Consts& C = ENS ? *myC : G.C;
-      const long long sI = G.sI;
-      const double dtUsed = ctl.dtUsed;
-      const double inc = (s == 2) ? dtUsed : dtUsed / 2;
-      const double dtFactor = dtUsed / 6;
-      double* const out0 = ctl.O[s][0];
-      double* const out1 = ctl.O[s][1];
-      double* const out2 = ctl.O[s][2];
-      double* const out3 = ctl.O[s][3];
-      double* const out4 = ctl.O[s][4];
-      double* const accb = G.acc[0];  // accumulator fields are contiguous, G.N doubles apart
-      const long long NdF = G.N;
+      // single grid: registers; ensemble: shared-memory loads at each use
+      const long long sIR = G.sI, NdR = G.N;
+      const double incR = (s == 2) ? dtUsed : dtUsed / 2, dtFactorR = dtUsed / 6;
+      double* const outR[5] = {ctl.O[s][0], ctl.O[s][1], ctl.O[s][2], ctl.O[s][3], ctl.O[s][4]};
+      double* const accR = G.acc[0];
+      const volatile ItemSm* const vI = myI;
+      auto outp = [&](int f) -> double* {
+        if constexpr (ENS) return vI->out[f];
+        else return outR[f];
+      };
+      auto accp = [&]() -> double* {
+        if constexpr (ENS) return vI->acc;
+        else return accR;
+      };
+      auto nodes = [&]() -> long long {
+        if constexpr (ENS) return vI->N;
+        else return NdR;
+      };
+      auto planeStride = [&]() -> long long {
+        if constexpr (ENS) return vI->sI;
+        else return sIR;
+      };
+      auto incf = [&]() -> double {
+        if constexpr (ENS) return vI->inc;
+        else return incR;
+      };
+      auto dtFactorf = [&]() -> double {
+        if constexpr (ENS) return vI->dtFactor;
+        else return dtFactorR;
+      };
       const int j = w.j0 + ty, k = w.k0 + tx;
       const bool inTile = (j <= G.NJ - 2) && (k <= G.NK - 2);
       const int L = w.i1 - w.i0 + 1;
-      long long nR = (long long)w.i0 * sI + (long long)j * G.sJ + k;  // node of the next computed plane
+      long long nR = (long long)w.i0 * planeStride() + (long long)j * G.sJ + k;  // node of the next computed plane
       XNode gm1{}, gm2{};
       double fprev[5] = {0, 0, 0, 0, 0};
       XOwn ownPrev{};
@@ -513,14 +564,18 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
         double u0[5], res[5];
 #pragma unroll
         for (int f = 0; f < 5; ++f) u0[f] = ep[f * EFS + eidx];
-        if (s == 0) {
+        if (MODE != 2 && s == 0) {
+          const double inc = incf();
 #pragma unroll
           for (int f = 0; f < 5; ++f) res[f] = u0[f] + inc * kk5[f];
           if (valid) {
+            double* const accb = accp();
+            const long long NdF = nodes();
 #pragma unroll
             for (int f = 0; f < 5; ++f) accb[f * NdF + nR] = kk5[f];
           }
-        } else if (s < 3) {
+        } else if (MODE == 1 || (MODE == 0 && s < 3)) {
+          const double inc = incf();
           double an[5];
 #pragma unroll
           for (int f = 0; f < 5; ++f) {
@@ -528,10 +583,13 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
             res[f] = u0[f] + inc * kk5[f];
           }
           if (valid) {
+            double* const accb = accp();
+            const long long NdF = nodes();
 #pragma unroll
             for (int f = 0; f < 5; ++f) accb[f * NdF + nR] = an[f];
           }
         } else {
+          const double dtFactor = dtFactorf();
 #pragma unroll
           for (int f = 0; f < 5; ++f) res[f] = u0[f] + dtFactor * (ep[(5 + f) * EFS + eidx] + kk5[f]);
           const bool filtered = (tc & FILTER_BIT) != 0;  // rho, rho_E change again in the near-body filter
@@ -545,6 +603,11 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           if (valid && !filtered) dt_terms(C, res, dta);
         }
         if (valid) {
+          double* const out0 = outp(0);
+          double* const out1 = outp(1);
+          double* const out2 = outp(2);
+          double* const out3 = outp(3);
+          double* const out4 = outp(4);
           out0[nR] = res[0];
           out1[nR] = res[1];
           out2[nR] = res[2];
@@ -574,7 +637,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
           }
         }
         ++e;
-        nR += sI;
+        nR += planeStride();
         gm2 = gm1;
         gm1 = gcur;
 #pragma unroll
@@ -582,7 +645,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
         ownPrev = ownCur;
       }
       q += L + 2;
-      if (ENS && s == 3) {
+      if (ENS && MODE != 1 && s == 3) {
         // an ensemble CTA moves between members: hand this item's dt maxima, change norms and NaN flag
         // to its member now (warp reductions, then one atomic per warp and quantity)
         const double mx[4] = {warp_max(dta.sx), warp_max(dta.sy), warp_max(dta.sz), warp_max(dta.nu)};
@@ -603,7 +666,7 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
     }
   }
   __syncwarp();
-  if (!ENS && s == 3) {
+  if (!ENS && MODE != 1 && s == 3) {
     flush_dt(G0.ctl, dta, red);
     flush_norms(G0.normPart + 5 * blockIdx.x, nsum, red);
     if (bad) atomicOr(&G0.ctl->nonFinite, 1);
@@ -615,29 +678,41 @@ namespace {
 struct VariantInfo {
   int tk, tj, threads, typeBoxW;
   size_t smem;
-  const void* fn;     // single grid
-  const void* fnEns;  // ensemble
+  const void* fn[2];     // single grid: stages 1-3 (mode 0), stage 4 (mode 2)
+  const void* fnEns[2];  // ensemble: stages 1-3 (mode 1), stage 4 (mode 2)
 };
 template <int TK, int TJ>
 VariantInfo variant_info() {
   using TL = ws::Tile<TK, TJ>;
-  return VariantInfo{TK, TJ, TL::NTHREADS, TL::TYW, TL::SMEM, reinterpret_cast<const void*>(&k_stage_ws<TK, TJ, false>),
-                     reinterpret_cast<const void*>(&k_stage_ws<TK, TJ, true>)};
+  return VariantInfo{TK,
+                     TJ,
+                     TL::NTHREADS,
+                     TL::TYW,
+                     TL::SMEM,
+                     {reinterpret_cast<const void*>(&k_stage_ws<TK, TJ, false, 0>),
+                      reinterpret_cast<const void*>(&k_stage_ws<TK, TJ, false, 2>)},
+                     {reinterpret_cast<const void*>(&k_stage_ws<TK, TJ, true, 1>),
+                      reinterpret_cast<const void*>(&k_stage_ws<TK, TJ, true, 2>)}};
 }
 VariantInfo info(int v) { return v == STAGE_TILE_16x16 ? variant_info<16, 16>() : variant_info<32, 8>(); }
 
 template <int TK, int TJ, bool ENS>
 void launch_variant(const Grid& hg, const Grid* dGrids, const LaunchPlan& L, int s, cudaStream_t st) {
   using TL = ws::Tile<TK, TJ>;
-  k_stage_ws<TK, TJ, ENS><<<L.stageBlocks, TL::NTHREADS, TL::SMEM, st>>>(hg, dGrids, L.items, L.ctaStart, s);
+  constexpr int early = ENS ? 1 : 0;  // the instantiation of stages 1-3
+  if (s == 3)
+    k_stage_ws<TK, TJ, ENS, 2><<<L.stageBlocks, TL::NTHREADS, TL::SMEM, st>>>(hg, dGrids, L.items, L.ctaStart, s);
+  else
+    k_stage_ws<TK, TJ, ENS, early><<<L.stageBlocks, TL::NTHREADS, TL::SMEM, st>>>(hg, dGrids, L.items, L.ctaStart, s);
 }
 }  // namespace
 
 size_t stage_smem_bytes(int v) { return info(v).smem; }
 int stage_configure(int v) {
   const VariantInfo vi = info(v);
-  cudaError_t e = cudaFuncSetAttribute(vi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vi.smem));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(vi.fnEns, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vi.smem));
+  cudaError_t e = cudaSuccess;
+  for (const void* fn : {vi.fn[0], vi.fn[1], vi.fnEns[0], vi.fnEns[1]})
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(vi.smem));
   return int(e);
 }
 int stage_tile_j(int v) { return info(v).tj; }
@@ -647,21 +722,26 @@ int stage_threads(int v) { return info(v).threads; }
 int stage_occupancy(int v) {
   const VariantInfo vi = info(v);
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, vi.fn, vi.threads, vi.smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, vi.fn[1], vi.threads, vi.smem);
   return nb;
 }
 int stage_num_maps() { return ws::NMAPS; }
 // Registers per thread the kernels are launched with (the setmaxnreg split assumes ws::REG_LAUNCH); the
-// smaller of the single-grid and ensemble instantiations.
+// smallest over the instantiations.
 int stage_launch_registers(int v) {
-  cudaFuncAttributes a{}, b{};
-  if (cudaFuncGetAttributes(&a, info(v).fn) != cudaSuccess) return -1;
-  if (cudaFuncGetAttributes(&b, info(v).fnEns) != cudaSuccess) return -1;
-  return a.numRegs < b.numRegs ? a.numRegs : b.numRegs;
+  const VariantInfo vi = info(v);
+  int r = 1 << 30;
+  for (const void* fn : {vi.fn[0], vi.fn[1], vi.fnEns[0], vi.fnEns[1]}) {
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, fn) != cudaSuccess) return -1;
+    r = a.numRegs < r ? a.numRegs : r;
+  }
+  return r;
 }
 bool stage_register_split_ok(int v) {
   const int r = stage_launch_registers(v);
-  return r > 0 && 128 * ws::REG_LOW + 256 * ws::REG_HIGH <= info(v).threads * r;
+  const int need = std::max(128 * ws::REG_LOW + 256 * ws::REG_HIGH, 128 * ws::REG_LOW_ENS4 + 256 * ws::REG_HIGH_ENS4);
+  return r > 0 && need <= info(v).threads * r;
 }
 void launch_stage(const Grid& hg, const LaunchPlan& L, int s, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -318,13 +318,14 @@ class Solver:
         self._check(lib().nsf_adj_backward(self.h, dJ, _dp(gi), _dp(gu)))
         return gi, gu
 
-    ADJ_PHASES = ("recompute", "objective", "ghost", "filter", "edge", "solid", "prepare", "rhs", "density_filter")
+    # slots of nsf_adj_profile_step's result (None: unused)
+    ADJ_PHASES = ("recompute", None, "boundary_combine", None, None, None, None, "rhs", "density_filter")
 
     def adj_profile_step(self, step=0):
         """{phase: device ms} of one eagerly launched adjoint step (after adj_forward)."""
         ms = np.zeros(len(self.ADJ_PHASES))
         self._check(lib().nsf_adj_profile_step(self.h, step, _dp(ms)))
-        return dict(zip(self.ADJ_PHASES, ms.tolist()))
+        return {k: v for k, v in zip(self.ADJ_PHASES, ms.tolist()) if k}
 
     def adj_dt(self):
         n = ctypes.c_uint64()

@@ -188,7 +188,9 @@ nsf_status nsf_step_metrics_noalloc(const nsf_config* cfg, const double* d_old, 
  * persistent kernel over the union of the members' work items. No counterpart in the reference; every
  * member advances exactly as Solver::marchTimeStep (Solver.cpp:130-167) advances its own grid.
  * tune_cache: NULL (default 32 x 8 tiles), or a file of autotuner results (created/extended as needed)
- * from which the stage-kernel tile shape is chosen; shapes not yet in it are timed on the device first.
+ * from which the stage-kernel tile shape is chosen: per device and composition of grid shapes, the
+ * ensemble stage kernel's time per node with each tile shape (a composition not yet in it is timed first,
+ * on throwaway ensembles of the same members).
  * Results: nsf_ensemble_member returns member m's handle (valid until nsf_ensemble_destroy; do not
  * destroy or march it) after waiting for the queued ensemble steps, for nsf_get_time / nsf_download / ... */
 typedef struct nsf_ensemble nsf_ensemble;
@@ -257,10 +259,10 @@ nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* 
 /* The frozen dt sequence (count values: dt of step n). */
 nsf_status nsf_adj_get_dt(nsf_solver* s, double* dts, uint64_t* count);
 /* Device time (ms, CUDA events) of the phases of one adjoint step, launched eagerly after a forward run:
- * ms[0] recomputation of the step with its stage snapshots, [1] objective, [2] ghost nodes, [3] near-body
- * filter, [4] edge conditions, [5] unused (the solid-node copies' adjoint runs within [6]), [6] RK4
- * combine, RHS input quantities and solid-node copies,
- * [7] transposed RHS, [8] density filter (summed over the four stages). Gradients are unaffected. */
+ * ms[0] recomputation of the step with its stage snapshots, [2] ghost nodes (with the objective), near-body
+ * filter, edge conditions, solid-node copies, RK4 combine and RHS input quantities (one launch per stage),
+ * [7] transposed RHS, [8] density filter (summed over the four stages); [1] and [3]-[6] are 0. Gradients
+ * are unaffected. */
 nsf_status nsf_adj_profile_step(nsf_solver* s, uint64_t step, double* ms);
 
 /* Self-check of the device reciprocal and square root the stage kernel uses for the primitive values

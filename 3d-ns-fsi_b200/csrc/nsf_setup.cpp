@@ -1,9 +1,9 @@
 // Host-side mesh setup: boundary claims, node classification, immersed-body ghost / filter lists,
 // image points and the initial condition. Runs once per solver, before the first step.
 //
-// The north-star requires node classification, ghost lists and image-point cells to be bit-exact with
-// the reference, so every floating-point expression here is evaluated in the reference's order and the
-// file is compiled with -ffp-contract=off (no fused multiply-add contraction). Reference functions:
+// Node classification, ghost lists and image-point cells must be bit-exact with the reference, so every
+// floating-point expression here is evaluated in the reference's order and the file is compiled with
+// -ffp-contract=off (no fused multiply-add contraction). Reference functions:
 //   Mesh::setupBoundaries            src/Mesh.cpp:25-58     (spacing / offset rules, claim order)
 //   Mesh::categorizeNodes            src/Mesh.cpp:61-82
 //   MeshEdgeBoundary::identifyOwnedNodes  src/Boundary.cpp:18-71

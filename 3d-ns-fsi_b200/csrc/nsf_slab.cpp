@@ -1,4 +1,4 @@
-// x-slab decomposition of one grid (SURVEY (e): i is the slowest index, so an i-plane is contiguous).
+// x-slab decomposition of one grid (i is the slowest index, so an i-plane is contiguous).
 //
 // The interior planes 1 .. NI-2 are split into P contiguous ranges; slab p owns its range (slab 0 also owns
 // the x-min face plane, slab P-1 the x-max face plane) and holds one more plane on each side: a halo (a copy

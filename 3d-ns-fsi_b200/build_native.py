@@ -21,7 +21,8 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["nsf_kernels.cu", "nsf_stage_ws.cu", "nsf_noalloc.cu", "nsf_adjoint.cu", "nsf_slab.cu"]
-CXX_SOURCES = ["nsf_config.cpp", "nsf_setup.cpp", "nsf_capi.cpp", "nsf_ensemble.cpp", "nsf_adjoint.cpp", "nsf_bc_plan.cpp", "nsf_slab.cpp"]
+CXX_SOURCES = ["nsf_config.cpp", "nsf_setup.cpp", "nsf_capi.cpp", "nsf_ensemble.cpp", "nsf_adjoint.cpp", "nsf_bc_plan.cpp", "nsf_slab.cpp",
+               "nsf_nccl.cpp"]
 
 
 def _run(cmd):

@@ -15,9 +15,14 @@
 //         halo exchange: each slab's first and last owned planes -> its neighbours' halo planes }
 //   global reductions (dt maxima, change-norm sums) and the end of step of every slab.
 //
-// All slabs of a group live on one device and one stream, and a step is one CUDA graph; a transfer packs the
-// plane into the receiving slab's staging buffer and unpacks it there (the buffers each step's roles select
-// are read on the device). The node values and the dt sequence equal the single-grid solve's bit for bit:
+// A group lives in one process or spans several (one GPU each, nsf_slab_group_create_ranks): rank r holds
+// the consecutive slabs p with p * world / P == r. Each process's slabs share one device and one stream,
+// and a step is one CUDA graph; a transfer packs the plane into a staging buffer and unpacks it on the
+// receiving side (the buffers each step's roles select are read on the device) -- within a process the
+// two sides share the buffer, across processes NCCL send/recv moves it (captured in the graph, between
+// the pack and the unpack launches). The global reductions gather every slab's partials (NCCL all-gather
+// across processes) and combine them in slab order, so every process computes the same dt and norms.
+// The node values and the dt sequence equal the single-grid solve's bit for bit:
 // every node's dt terms are formed by the same kernel as in the whole grid (the periodic x faces' by their
 // edge items, BC_SLAB_COPY), and maxima do not depend on the order; the change norms are summed slab by slab,
 // so they agree to rounding. Immersed bodies are not supported across slabs (NSF_ERR_ARG).
@@ -29,6 +34,7 @@
 #include <vector>
 
 #include "nsf_internal.h"
+#include "nsf_nccl.h"
 #include "nsf_slab.h"
 #include "nsf_solver_impl.h"
 
@@ -39,17 +45,34 @@ struct nsf_slab_group {
   int device = 0;
   cudaStream_t stream = nullptr;
   HostSetup whole;                 // the grid's own host setup (partition, downloads)
-  std::vector<nsf_solver*> slabs;
-  std::vector<int> a, b;           // slab p's interior planes a[p] .. b[p] (global)
+  int P = 0;                       // slabs of the whole group
+  int rank = 0, world = 1;         // this process among the group's processes
+  int first = 0;                   // global index of this process's first slab (slabs[l] is slab first + l)
+  bool ncclAll = false;            // route transfers within this process through NCCL too (self send/recv)
+  std::vector<nsf_solver*> slabs;  // this process's slabs
+  std::vector<int> a, b;           // slab p's interior planes a[p] .. b[p] (global), every slab of the group
   std::vector<int> lo, hi;         // the global planes slab p owns: its interior planes, plus the x faces at the ends
   std::vector<int> base;           // global plane of slab p's local plane 0 (= a[p] - 1)
   bool xPeriodic = false;
-  Grid* dGrids = nullptr;          // copies of the slabs' grids, device
+  Grid* dGrids = nullptr;          // copies of this process's slabs' grids, device
+  double* dPart = nullptr;         // [9 x local slabs] this process's slab partials
+  double* dGather = nullptr;       // [9 x maxLocal x world] every process's partials (several processes)
+  int* dAt = nullptr;              // [P] where slab p's partials are (in dPart, or in dGather)
+  int maxLocal = 0;
   double* dRed = nullptr;          // [9] global dt maxima and norm sums
-  // transfers: one staging buffer per receiving side
+  // transfers: pack tasks (this process's sending side) and unpack tasks (its receiving side), per list
   std::vector<SlabTask> packStage, unpackStage, packWrap, unpackWrap, packFilter, unpackFilter;
   SlabTask* dTasks = nullptr;      // all task lists, device, in the order above
   size_t offs[7] = {0, 0, 0, 0, 0, 0, 0};
+  // NCCL moves of each list (0 halos, 1 periodic x faces, 2 filtered density), in the group's global order
+  struct Move {
+    bool send;   // send (else receive)
+    int peer;    // the other process
+    double* buf;
+    size_t words;
+  };
+  std::vector<Move> moves[3];
+  void* comm = nullptr;            // ncclComm_t (several processes, or ncclAll)
   long long planeWords = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graphExec = nullptr;
@@ -124,7 +147,52 @@ void slab_setup(const nsf_slab_group* g, int p, HostSetup& S, std::vector<uint8_
   }
 }
 
-nsf_status build_group(nsf_slab_group* g, int P) {
+// The process that holds slab p: consecutive slabs per process, p * world / P.
+int slab_owner(int p, int P, int world) { return int((long long)p * world / P); }
+
+// One plane transfer of a step: list 0 halos (stage output), 1 periodic x faces (stage output), 2 the
+// filtered density's halos; planes local to each slab (local plane l of slab p is global plane a[p] - 1 + l).
+struct SlabXfer {
+  int list, from, fromPlane, to, toPlane, which;
+};
+
+// Every transfer of a group, in the order every process walks them (NCCL pairs a process's sends to a peer
+// with the peer's receives in issue order).
+std::vector<SlabXfer> slab_transfers(const std::vector<int>& a, const std::vector<int>& b, bool xPeriodic) {
+  const int P = int(a.size());
+  std::vector<SlabXfer> out;
+  auto n = [&](int p) { return b[size_t(p)] - a[size_t(p)] + 3; };  // local planes of slab p
+  for (int which : {SLAB_STAGE, SLAB_FILTER})
+    for (int p = 0; p + 1 < P; ++p) {  // last owned plane -> next slab's plane 0; first owned -> previous's last
+      const int list = which == SLAB_STAGE ? 0 : 2;
+      out.push_back(SlabXfer{list, p, n(p) - 2, p + 1, 0, which});
+      out.push_back(SlabXfer{list, p + 1, 1, p, n(p) - 1, which});
+    }
+  if (xPeriodic) {  // global plane NI-2 -> slab 0's plane 0; global plane 1 -> slab P-1's last plane
+    out.push_back(SlabXfer{1, P - 1, n(P - 1) - 2, 0, 0, SLAB_STAGE});
+    out.push_back(SlabXfer{1, 0, 1, P - 1, n(P - 1) - 1, SLAB_STAGE});
+  }
+  return out;
+}
+
+// The partition of the interior planes 1 .. NI-2 into P near-equal ranges.
+void slab_partition(const HostSetup& W, int P, std::vector<int>& a, std::vector<int>& b) {
+  const int interior = int(W.NI) - 2;
+  a.clear();
+  b.clear();
+  for (int p = 0; p < P; ++p) {
+    a.push_back(1 + p * interior / P);
+    b.push_back((p + 1) * interior / P);
+  }
+}
+
+bool has_x_periodic(const HostSetup& W) {
+  for (const EdgeBC& e : W.edges)
+    if (e.axis == 0 && e.bc == NSF_BC_PERIODIC) return true;
+  return false;
+}
+
+nsf_status build_group(nsf_slab_group* g, int P, const void* ncclId) {
   const nsf_config& cfg = g->cfg;
   std::string err;
   nsf_status st = build_setup(cfg, g->whole, err);
@@ -133,15 +201,29 @@ nsf_status build_group(nsf_slab_group* g, int P) {
   if (!W.bodies.empty()) return gfail(g, NSF_ERR_ARG, "x-slab groups support grids without immersed bodies");
   const int interior = int(W.NI) - 2;
   if (P < 2 || interior < 2 * P) return gfail(g, NSF_ERR_ARG, "x-slabs: 2 <= slabs and at least 2 interior planes per slab");
-  for (const EdgeBC& e : W.edges)
-    if (e.axis == 0 && e.bc == NSF_BC_PERIODIC) g->xPeriodic = true;
-  for (int p = 0; p < P; ++p) {  // interior planes in P near-equal ranges
-    const int a = 1 + p * interior / P, b = (p + 1) * interior / P;
-    g->a.push_back(a);
-    g->b.push_back(b);
-    g->lo.push_back(p == 0 ? 0 : a);
-    g->hi.push_back(p == P - 1 ? int(W.NI) - 1 : b);
-    g->base.push_back(a - 1);
+  if (g->world < 1 || g->world > P || g->rank < 0 || g->rank >= g->world)
+    return gfail(g, NSF_ERR_ARG, "x-slabs: 0 <= rank < world <= slabs");
+  g->P = P;
+  g->xPeriodic = has_x_periodic(W);
+  slab_partition(W, P, g->a, g->b);
+  for (int p = 0; p < P; ++p) {
+    g->lo.push_back(p == 0 ? 0 : g->a[size_t(p)]);
+    g->hi.push_back(p == P - 1 ? int(W.NI) - 1 : g->b[size_t(p)]);
+    g->base.push_back(g->a[size_t(p)] - 1);
+  }
+  // this process's slabs, and the most any process holds
+  std::vector<int> count(size_t(g->world), 0);
+  for (int p = 0; p < P; ++p) ++count[size_t(slab_owner(p, P, g->world))];
+  g->maxLocal = *std::max_element(count.begin(), count.end());
+  g->first = 0;
+  while (slab_owner(g->first, P, g->world) != g->rank) ++g->first;
+  const int nLocal = count[size_t(g->rank)];
+  const bool useNccl = g->world > 1 || g->ncclAll;
+  const NcclApi* nccl = nullptr;
+  if (useNccl) {
+    std::string why;
+    if (!(nccl = nccl_api(&why))) return gfail(g, NSF_ERR_CUDA, why);
+    if (!ncclId) return gfail(g, NSF_ERR_ARG, "x-slabs over NCCL need the communicator id");
   }
   // the whole grid's initial condition, sliced per slab; its initial dt for every slab
   std::vector<double> cons, prim;
@@ -149,7 +231,7 @@ nsf_status build_group(nsf_slab_group* g, int P) {
   const double dt0 = nsf_initial_dt(cfg, W, cons, prim);
   const size_t plane = W.NJ * W.NK;
   CKG(cudaSetDevice(g->device));
-  for (int p = 0; p < P; ++p) {
+  for (int p = g->first; p < g->first + nLocal; ++p) {
     nsf_solver* s = nullptr;
     st = nsf_create(&cfg, g->device, &s);
     if (st != NSF_OK) {
@@ -180,30 +262,58 @@ nsf_status build_group(nsf_slab_group* g, int P) {
   if ((st = galloc(g, &g->dGrids, hg.size())) != NSF_OK) return st;
   CKG(cudaMemcpy(g->dGrids, hg.data(), hg.size() * sizeof(Grid), cudaMemcpyHostToDevice));
   if ((st = galloc(g, &g->dRed, 9)) != NSF_OK) return st;
-  // transfers
+  if ((st = galloc(g, &g->dPart, size_t(9) * size_t(g->maxLocal))) != NSF_OK) return st;
+  CKG(cudaMemset(g->dPart, 0, size_t(9) * size_t(g->maxLocal) * sizeof(double)));
+  {  // where each slab's partials are read: this process's own (one process), or the gathered copies
+    std::vector<int> at(static_cast<size_t>(P));
+    std::vector<int> firstOf(size_t(g->world), -1);
+    for (int p = 0; p < P; ++p) {
+      const int r = slab_owner(p, P, g->world);
+      if (firstOf[size_t(r)] < 0) firstOf[size_t(r)] = p;
+      at[size_t(p)] = useNccl ? r * g->maxLocal + (p - firstOf[size_t(r)]) : p;
+    }
+    if ((st = galloc(g, &g->dAt, at.size())) != NSF_OK) return st;
+    CKG(cudaMemcpy(g->dAt, at.data(), at.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (useNccl && (st = galloc(g, &g->dGather, size_t(9) * g->maxLocal * g->world)) != NSF_OK) return st;
+  }
+  // transfers, in the group's global order: within this process one staging buffer per transfer (pack and
+  // unpack share it); across processes (or all of them with ncclAll) a send buffer on the sending side and
+  // a receive buffer on the receiving side, moved by NCCL
   g->planeWords = g->slabs[0]->hGrid.sI;
-  auto add = [&](std::vector<SlabTask>& pk, std::vector<SlabTask>& up, int from, int fromPlane, int to, int toPlane,
-                 int which) -> nsf_status {
-    double* buf = nullptr;
-    nsf_status r = galloc(g, &buf, size_t(5) * size_t(g->planeWords));
-    if (r != NSF_OK) return r;
-    pk.push_back(SlabTask{g->slabs[size_t(from)]->dGrid, fromPlane, which, buf});
-    up.push_back(SlabTask{g->slabs[size_t(to)]->dGrid, toPlane, which, buf});
-    return NSF_OK;
-  };
-  for (int p = 0; p + 1 < P; ++p) {
-    const int nLast = int(g->slabs[size_t(p)]->setup.NI) - 2;  // slab p's last owned plane, local
-    for (int which : {SLAB_STAGE, SLAB_FILTER}) {
-      auto& pk = which == SLAB_STAGE ? g->packStage : g->packFilter;
-      auto& up = which == SLAB_STAGE ? g->unpackStage : g->unpackFilter;
-      if ((st = add(pk, up, p, nLast, p + 1, 0, which)) != NSF_OK) return st;
-      if ((st = add(pk, up, p + 1, 1, p, nLast + 1, which)) != NSF_OK) return st;
+  auto local = [&](int p) { return slab_owner(p, P, g->world) == g->rank; };
+  auto gridOf = [&](int p) { return g->slabs[size_t(p - g->first)]->dGrid; };
+  for (const SlabXfer& x : slab_transfers(g->a, g->b, g->xPeriodic)) {
+    auto& pk = x.list == 0 ? g->packStage : x.list == 1 ? g->packWrap : g->packFilter;
+    auto& up = x.list == 0 ? g->unpackStage : x.list == 1 ? g->unpackWrap : g->unpackFilter;
+    const size_t words = size_t(x.which == SLAB_STAGE ? 5 : 1) * size_t(g->planeWords);
+    const bool fromHere = local(x.from), toHere = local(x.to);
+    if (fromHere && toHere && !g->ncclAll) {
+      double* buf = nullptr;
+      if ((st = galloc(g, &buf, words)) != NSF_OK) return st;
+      pk.push_back(SlabTask{gridOf(x.from), x.fromPlane, x.which, buf});
+      up.push_back(SlabTask{gridOf(x.to), x.toPlane, x.which, buf});
+      continue;
+    }
+    if (fromHere) {
+      double* buf = nullptr;
+      if ((st = galloc(g, &buf, words)) != NSF_OK) return st;
+      pk.push_back(SlabTask{gridOf(x.from), x.fromPlane, x.which, buf});
+      g->moves[x.list].push_back(nsf_slab_group::Move{true, slab_owner(x.to, P, g->world), buf, words});
+    }
+    if (toHere) {
+      double* buf = nullptr;
+      if ((st = galloc(g, &buf, words)) != NSF_OK) return st;
+      up.push_back(SlabTask{gridOf(x.to), x.toPlane, x.which, buf});
+      g->moves[x.list].push_back(nsf_slab_group::Move{false, slab_owner(x.from, P, g->world), buf, words});
     }
   }
-  if (g->xPeriodic) {  // global plane NI-2 -> slab 0's plane 0; global plane 1 -> slab P-1's last plane
-    const int nl = int(g->slabs[size_t(P - 1)]->setup.NI);
-    if ((st = add(g->packWrap, g->unpackWrap, P - 1, nl - 2, 0, 0, SLAB_STAGE)) != NSF_OK) return st;
-    if ((st = add(g->packWrap, g->unpackWrap, 0, 1, P - 1, nl - 1, SLAB_STAGE)) != NSF_OK) return st;
+  if (useNccl) {  // the communicator (every process of the group joins here)
+    ncclUniqueId id;
+    std::memcpy(&id, ncclId, sizeof id);
+    ncclComm_t comm = nullptr;
+    const ncclResult_t r = nccl->commInitRank(&comm, g->world, id, g->rank);
+    if (r != ncclSuccess) return gfail(g, NSF_ERR_CUDA, std::string("ncclCommInitRank: ") + nccl->errorString(r));
+    g->comm = comm;
   }
   std::vector<SlabTask> all;
   const std::vector<SlabTask>* lists[6] = {&g->packStage, &g->unpackStage, &g->packWrap, &g->unpackWrap,
@@ -227,8 +337,22 @@ nsf_status build_group(nsf_slab_group* g, int P) {
       ++launches;
     }
   };
+  ncclResult_t nr = ncclSuccess;
+  auto move = [&](int list) {  // this process's NCCL sends and receives of one list, as one group
+    if (g->moves[list].empty() || nr != ncclSuccess) return;
+    const ncclComm_t comm = static_cast<ncclComm_t>(g->comm);
+    nr = nccl->groupStart();
+    for (const auto& m : g->moves[list]) {
+      if (nr != ncclSuccess) break;
+      nr = m.send ? nccl->send(m.buf, m.words, ncclDouble, m.peer, comm, g->stream)
+                  : nccl->recv(m.buf, m.words, ncclDouble, m.peer, comm, g->stream);
+    }
+    const ncclResult_t e = nccl->groupEnd();
+    if (nr == ncclSuccess) nr = e;
+  };
   for (nsf_solver* s : g->slabs) launches += enqueue_step_begin(s->dGrid, s->plan, g->stream);
   copies(4, 0, 0);  // filtered density halos (filter steps)
+  move(2);
   copies(5, 0, 1);
   for (int q = 0; q < 4; ++q) {
     for (nsf_solver* s : g->slabs) {
@@ -236,14 +360,26 @@ nsf_status build_group(nsf_slab_group* g, int P) {
       ++launches;
     }
     copies(2, q, 0);  // periodic x faces
+    move(1);
     copies(3, q, 1);
     for (nsf_solver* s : g->slabs) launches += launch_bc_part(s->dGrid, s->plan, q, false, g->stream);
     copies(0, q, 0);  // halos
+    move(0);
     copies(1, q, 1);
   }
-  launch_slab_reduce(g->dGrids, P, g->dRed, g->stream);
-  launch_slab_finalize(g->dGrids, P, g->dRed, g->stream);
-  launches += 2;
+  launch_slab_partials(g->dGrids, nLocal, g->dPart, g->stream);
+  if (useNccl && nr == ncclSuccess)
+    nr = nccl->allGather(g->dPart, g->dGather, size_t(9) * g->maxLocal, ncclDouble, static_cast<ncclComm_t>(g->comm),
+                         g->stream);
+  launch_slab_combine(useNccl ? g->dGather : g->dPart, g->dAt, P, g->dRed, g->stream);
+  launch_slab_finalize(g->dGrids, nLocal, g->dRed, g->stream);
+  launches += 3;
+  if (nr != ncclSuccess) {
+    cudaGraph_t dropped = nullptr;
+    cudaStreamEndCapture(g->stream, &dropped);
+    if (dropped) cudaGraphDestroy(dropped);
+    return gfail(g, NSF_ERR_CUDA, std::string("NCCL in the slab step: ") + nccl->errorString(nr));
+  }
   const cudaError_t e1 = cudaGetLastError();
   const cudaError_t e2 = cudaStreamEndCapture(g->stream, &g->graph);
   if (e1 != cudaSuccess || e2 != cudaSuccess)
@@ -274,9 +410,62 @@ nsf_status nsf_slab_group_create(const nsf_config* cfg, int32_t nslabs, int32_t 
   auto* g = new nsf_slab_group;
   g->cfg = *cfg;
   g->device = device;
-  nsf_status st = build_group(g, nslabs);
+  nsf_status st = build_group(g, nslabs, nullptr);
   *out = g;
   return st;
+}
+
+nsf_status nsf_slab_nccl_id(uint8_t* id) {
+  if (!id) return NSF_ERR_ARG;
+  const NcclApi* nccl = nccl_api(nullptr);
+  if (!nccl) return NSF_ERR_CUDA;
+  ncclUniqueId u;
+  if (nccl->getUniqueId(&u) != ncclSuccess) return NSF_ERR_CUDA;
+  static_assert(sizeof(u) == NSF_NCCL_ID_BYTES, "NCCL unique id size");
+  std::memcpy(id, &u, sizeof u);
+  return NSF_OK;
+}
+
+nsf_status nsf_slab_group_create_ranks(const nsf_config* cfg, int32_t nslabs, int32_t rank, int32_t world,
+                                       const uint8_t* nccl_id, int32_t flags, int32_t device, nsf_slab_group** out) {
+  if (!cfg || !out || !nccl_id || device < 0) return NSF_ERR_ARG;
+  *out = nullptr;
+  auto* g = new nsf_slab_group;
+  g->cfg = *cfg;
+  g->device = device;
+  g->rank = rank;
+  g->world = world;
+  g->ncclAll = (flags & NSF_SLAB_NCCL_ALL) != 0;
+  nsf_status st = build_group(g, nslabs, nccl_id);
+  *out = g;
+  return st;
+}
+
+nsf_status nsf_slab_schedule(const nsf_config* cfg, int32_t nslabs, int32_t world, int32_t* owner,
+                             int32_t* transfers, int32_t* count) {
+  if (!cfg || !count || nslabs < 2 || world < 1 || world > nslabs) return NSF_ERR_ARG;
+  HostSetup W;
+  std::string err;
+  const nsf_status st = build_setup(*cfg, W, err);
+  if (st != NSF_OK) return st;
+  if (int(W.NI) - 2 < 2 * nslabs) return NSF_ERR_ARG;
+  std::vector<int> a, b;
+  slab_partition(W, nslabs, a, b);
+  if (owner)
+    for (int p = 0; p < nslabs; ++p) owner[p] = slab_owner(p, nslabs, world);
+  const std::vector<SlabXfer> xs = slab_transfers(a, b, has_x_periodic(W));
+  const int cap = *count;
+  *count = int32_t(xs.size());
+  if (transfers && cap >= int(xs.size()))
+    for (size_t q = 0; q < xs.size(); ++q) {
+      int32_t* t = transfers + 5 * q;
+      t[0] = xs[q].list;
+      t[1] = xs[q].from;
+      t[2] = a[size_t(xs[q].from)] - 1 + xs[q].fromPlane;
+      t[3] = xs[q].to;
+      t[4] = a[size_t(xs[q].to)] - 1 + xs[q].toPlane;
+    }
+  return NSF_OK;
 }
 
 nsf_status nsf_slab_group_march(nsf_slab_group* g, uint64_t nsteps) {
@@ -332,7 +521,7 @@ nsf_status nsf_slab_group_info(nsf_slab_group* g, int32_t* nslabs, int32_t* firs
   if (!g) return NSF_ERR_ARG;
   if (nslabs) *nslabs = int32_t(g->slabs.size());
   if (first_planes)
-    for (size_t p = 0; p < g->slabs.size(); ++p) first_planes[p] = g->lo[p];
+    for (size_t l = 0; l < g->slabs.size(); ++l) first_planes[l] = g->lo[size_t(g->first) + l];
   if (launches_per_step) *launches_per_step = uint64_t(g->launchesPerStep);
   return NSF_OK;
 }
@@ -345,8 +534,9 @@ nsf_status nsf_slab_group_download(nsf_slab_group* g, uint32_t mask, double* hos
   const size_t plane = W.NJ * W.NK;
   int nf = 0;
   for (int f = 0; f < NSF_NUM_FIELDS; ++f) nf += (mask >> f) & 1;
-  for (size_t p = 0; p < g->slabs.size(); ++p) {
-    nsf_solver* s = g->slabs[p];
+  for (size_t l = 0; l < g->slabs.size(); ++l) {
+    const size_t p = size_t(g->first) + l;
+    nsf_solver* s = g->slabs[l];
     std::vector<double> loc(size_t(nf) * s->setup.N);
     const nsf_status st = nsf_download(s, mask, loc.data());
     if (st != NSF_OK) return gfail(g, st, s->err);
@@ -365,8 +555,12 @@ void nsf_slab_group_destroy(nsf_slab_group* g) {
   if (!g) return;
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
-  if (g->graphExec) cudaGraphExecDestroy(g->graphExec);
+  if (g->graphExec) cudaGraphExecDestroy(g->graphExec);  // the graph holds NCCL work: before the communicator
   if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->comm) {
+    const NcclApi* nccl = nccl_api(nullptr);
+    if (nccl) nccl->commDestroy(static_cast<ncclComm_t>(g->comm));
+  }
   for (nsf_solver* s : g->slabs) nsf_destroy(s);
   for (void* p : g->allocs) cudaFree(p);
   if (g->stream) cudaStreamDestroy(g->stream);

@@ -45,14 +45,11 @@ __global__ void k_slab_copy(const SlabTask* __restrict__ tasks, int s, int dir) 
   }
 }
 
-// The step's global quantities from every slab of this process: out[0..3] = the largest of each dt maximum
-// (c + |u|, c + |v|, c + |w|, the viscous term), out[4..8] = the change-norm sums (slabs in order, each slab's
-// partial slots in order). One block.
-__global__ void k_slab_reduce(const Grid* __restrict__ grids, int n, double* __restrict__ out) {
+// Each slab of this process: part[9 g .. 9 g + 8] = its four dt maxima (c + |u|, c + |v|, c + |w|, the
+// viscous term) and its five change-norm sums (its partial slots in order). One block.
+__global__ void k_slab_partials(const Grid* __restrict__ grids, int n, double* __restrict__ part) {
   __shared__ double red[5 * 32];
   __shared__ double tot[5];
-  double mx[4] = {0, 0, 0, 0};
-  double sum[5] = {0, 0, 0, 0, 0};
   for (int g = 0; g < n; ++g) {
     const Grid& G = grids[g];
     double s[5] = {0, 0, 0, 0, 0};
@@ -60,15 +57,28 @@ __global__ void k_slab_reduce(const Grid* __restrict__ grids, int n, double* __r
       for (int f = 0; f < 5; ++f) s[f] += G.normPart[5 * q + f];
     flush_norms(tot, s, red);
     if (threadIdx.x == 0) {
-      for (int f = 0; f < 5; ++f) sum[f] += tot[f];
-      for (int q = 0; q < 4; ++q) mx[q] = fmax(mx[q], __longlong_as_double(static_cast<long long>(G.ctl->mx[q])));
+      for (int q = 0; q < 4; ++q) part[9 * g + q] = __longlong_as_double(static_cast<long long>(G.ctl->mx[q]));
+      for (int f = 0; f < 5; ++f) part[9 * g + 4 + f] = tot[f];
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < 4; ++q) out[q] = mx[q];
-    for (int f = 0; f < 5; ++f) out[4 + f] = sum[f];
+}
+
+// The step's global quantities from every slab's partials (slab p's at part[9 at[p]]): out[0..3] the
+// largest dt maxima, out[4..8] the change-norm sums, slabs in order -- the same arithmetic whichever
+// process holds which slab. One thread.
+__global__ void k_slab_combine(const double* __restrict__ part, const int* __restrict__ at, int P,
+                               double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double mx[4] = {0, 0, 0, 0};
+  double sum[5] = {0, 0, 0, 0, 0};
+  for (int p = 0; p < P; ++p) {
+    const double* v = part + 9 * (long long)at[p];
+    for (int q = 0; q < 4; ++q) mx[q] = fmax(mx[q], v[q]);
+    for (int f = 0; f < 5; ++f) sum[f] += v[4 + f];
   }
+  for (int q = 0; q < 4; ++q) out[q] = mx[q];
+  for (int f = 0; f < 5; ++f) out[4 + f] = sum[f];
 }
 
 // End of step for every slab from the global quantities (finalize_grid's arithmetic): next dt, t, level,
@@ -108,8 +118,12 @@ void launch_slab_copy(const SlabTask* tasks, int ntasks, long long planeWords, i
       tasks, s, dir);
 }
 
-void launch_slab_reduce(const Grid* grids, int n, double* out, void* stream) {
-  k_slab_reduce<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(grids, n, out);
+void launch_slab_partials(const Grid* grids, int n, double* part, void* stream) {
+  k_slab_partials<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(grids, n, part);
+}
+
+void launch_slab_combine(const double* part, const int* at, int P, double* out, void* stream) {
+  k_slab_combine<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(part, at, P, out);
 }
 
 void launch_slab_finalize(Grid* grids, int n, const double* in, void* stream) {

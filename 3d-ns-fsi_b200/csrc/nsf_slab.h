@@ -22,8 +22,11 @@ struct SlabTask {
 // dir 0: pack the tasks' planes into their buffers; dir 1: unpack buffers into planes. planeWords: the
 // largest sI of the tasks' grids.
 void launch_slab_copy(const SlabTask* tasks, int ntasks, long long planeWords, int s, int dir, void* stream);
-// out[0..3]: the dt maxima over the grids, out[4..8]: the change-norm sums (fixed order).
-void launch_slab_reduce(const Grid* grids, int n, double* out, void* stream);
+// part[9 g ..]: grid g's four dt maxima and five change-norm sums.
+void launch_slab_partials(const Grid* grids, int n, double* part, void* stream);
+// out[0..3]: the dt maxima over all slabs, out[4..8]: the change-norm sums in slab order; slab p's partials
+// at part[9 at[p] ..].
+void launch_slab_combine(const double* part, const int* at, int P, double* out, void* stream);
 // The end of step of every grid from those global quantities.
 void launch_slab_finalize(Grid* grids, int n, const double* in, void* stream);
 

@@ -113,6 +113,10 @@ def lib():
         "nsf_slab_group_info": (i32, [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(u64)]),
         "nsf_slab_group_last_error": (ctypes.c_char_p, [vp]),
         "nsf_slab_group_destroy": (None, [vp]),
+        "nsf_slab_nccl_id": (i32, [ctypes.POINTER(ctypes.c_uint8)]),
+        "nsf_slab_group_create_ranks": (i32, [cp, i32, i32, i32, ctypes.POINTER(ctypes.c_uint8), i32, i32,
+                                              ctypes.POINTER(vp)]),
+        "nsf_slab_schedule": (i32, [cp, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
         "nsf_adj_configure": (i32, [vp, u32, u32]),
         "nsf_adj_forward": (i32, [vp, dp, dp, dp]),
         "nsf_adj_backward": (i32, [vp, ctypes.c_double, dp, dp]),
@@ -431,16 +435,54 @@ def slab_plan(cfg, nslabs):
     return list(zip(list(a), list(b)))
 
 
-class SlabGroup:
-    """One grid split into x-slabs (nsf_slab_group_*), all on one device."""
+NCCL_ID_BYTES = 128
+SLAB_NCCL_ALL = 1
 
-    def __init__(self, cfg, nslabs, device=0):
+
+def slab_nccl_id():
+    """The NCCL communicator id (bytes) for nsf_slab_group_create_ranks, made on one process of the group."""
+    buf = (ctypes.c_uint8 * NCCL_ID_BYTES)()
+    st = lib().nsf_slab_nccl_id(buf)
+    if st:
+        raise NsfError(st, "nsf_slab_nccl_id: NCCL (libnccl.so.2) unavailable")
+    return bytes(buf)
+
+
+def slab_schedule(cfg, nslabs, world):
+    """(owner per slab, [(list, from slab, from plane, to slab, to plane)]) of nslabs x-slabs over `world`
+    processes, transfers in the order every process issues them (nsf_slab_schedule; host only)."""
+    if isinstance(cfg, str):
+        cfg = config_load(cfg) if os.path.exists(cfg) else config_parse(cfg)
+    owner = (ctypes.c_int32 * nslabs)()
+    n = ctypes.c_int32(0)
+    st = lib().nsf_slab_schedule(ctypes.byref(cfg), nslabs, world, owner, None, ctypes.byref(n))
+    if st:
+        raise NsfError(st, "nsf_slab_schedule")
+    t = (ctypes.c_int32 * (5 * n.value))()
+    st = lib().nsf_slab_schedule(ctypes.byref(cfg), nslabs, world, owner, t, ctypes.byref(n))
+    if st:
+        raise NsfError(st, "nsf_slab_schedule")
+    return list(owner), [tuple(t[5 * q:5 * q + 5]) for q in range(n.value)]
+
+
+class SlabGroup:
+    """One grid split into x-slabs (nsf_slab_group_*): all slabs on one device, or (rank, world, nccl_id
+    given) this process's share of a group spread over `world` processes that exchange planes by NCCL.
+    With torch.distributed, e.g.: ids = [nsfsi.slab_nccl_id() if rank == 0 else None];
+    dist.broadcast_object_list(ids, src=0); SlabGroup(cfg, n, device, rank, world, ids[0])."""
+
+    def __init__(self, cfg, nslabs, device=0, rank=None, world=None, nccl_id=None, flags=0):
         if isinstance(cfg, str):
             cfg = config_load(cfg) if os.path.exists(cfg) else config_parse(cfg)
         self.cfg = cfg
         self.N = int(cfg.NI * cfg.NJ * cfg.NK)
         self.h = ctypes.c_void_p()
-        st = lib().nsf_slab_group_create(ctypes.byref(cfg), nslabs, device, ctypes.byref(self.h))
+        if nccl_id is None:
+            st = lib().nsf_slab_group_create(ctypes.byref(cfg), nslabs, device, ctypes.byref(self.h))
+        else:
+            idb = (ctypes.c_uint8 * NCCL_ID_BYTES).from_buffer_copy(bytes(nccl_id))
+            st = lib().nsf_slab_group_create_ranks(ctypes.byref(cfg), nslabs, int(rank or 0), int(world or 1), idb,
+                                                   int(flags), device, ctypes.byref(self.h))
         if st:
             msg = lib().nsf_slab_group_last_error(self.h).decode() if self.h else ""
             self.close()
@@ -483,7 +525,7 @@ class SlabGroup:
         mask = 0
         for f in fields:
             mask |= 1 << f
-        out = np.empty((len(fields), self.N))
+        out = np.zeros((len(fields), self.N))  # a process of a multi-process group fills its own planes
         self._check(lib().nsf_slab_group_download(self.h, mask, _dp(out)))
         return out
 

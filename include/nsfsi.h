@@ -223,7 +223,8 @@ nsf_status nsf_autotune(const nsf_config* cfg, int32_t device, const char* cache
  * planes plus a halo plane on each side, and a step exchanges the halo planes after every stage, the x
  * faces' periodic copies between the end slabs, and reduces the dt maxima and change norms over all slabs.
  * The result equals the single-grid solve node for node. Grids without immersed bodies; at least two
- * interior planes per slab. All slabs of a group run on one device (one CUDA graph per step). */
+ * interior planes per slab. nsf_slab_group_create: all slabs in this process on one device (one CUDA graph
+ * per step). nsf_slab_group_create_ranks: the slabs spread over `world` processes (one GPU each). */
 typedef struct nsf_slab_group nsf_slab_group;
 /* first[p], last[p]: the interior planes slab p computes (host only). */
 nsf_status nsf_slab_plan(const nsf_config* cfg, int32_t nslabs, int32_t* first, int32_t* last);
@@ -239,6 +240,26 @@ nsf_status nsf_slab_group_solver(nsf_slab_group* g, int32_t slab, nsf_solver** s
 nsf_status nsf_slab_group_info(nsf_slab_group* g, int32_t* nslabs, int32_t* first_planes, uint64_t* launches_per_step);
 const char* nsf_slab_group_last_error(nsf_slab_group* g);
 void nsf_slab_group_destroy(nsf_slab_group* g);
+/* A group over several processes: process `rank` of `world` (world <= nslabs) holds the consecutive slabs p
+ * with p * world / nslabs == rank, on `device`; the planes that cross processes move by NCCL send/recv
+ * inside the step graph, and every slab's dt maxima and change-norm sums are all-gathered and combined in
+ * slab order (every process computes the same dt; the fields equal the single-grid solve's). Collective:
+ * every process of the group calls it with the same cfg, nslabs, world and nccl_id (NSF_NCCL_ID_BYTES bytes
+ * from nsf_slab_nccl_id on one of them, passed on by any host channel). flags: NSF_SLAB_NCCL_ALL also moves
+ * the planes between slabs of the same process through NCCL (send/recv to itself; with world = 1 a check of
+ * the NCCL path on one GPU). NCCL is loaded at run time (libnccl.so.2; NSF_ERR_CUDA without it). The other
+ * nsf_slab_group_* calls see this process's slabs (info, solver, download: its own planes only). */
+#define NSF_NCCL_ID_BYTES 128
+#define NSF_SLAB_NCCL_ALL 1
+nsf_status nsf_slab_nccl_id(uint8_t* id);
+nsf_status nsf_slab_group_create_ranks(const nsf_config* cfg, int32_t nslabs, int32_t rank, int32_t world,
+                                       const uint8_t* nccl_id, int32_t flags, int32_t device, nsf_slab_group** out);
+/* Host only: owner[p] = the process of slab p for `world` processes, and the group's plane transfers in the
+ * order every process issues them, 5 int32 each: list (0 halo of the stage output, 1 periodic x face,
+ * 2 halo of the filtered density), from slab, its global plane, to slab, its global plane. *count: in, the
+ * capacity of transfers (entries); out, the number of transfers. */
+nsf_status nsf_slab_schedule(const nsf_config* cfg, int32_t nslabs, int32_t world, int32_t* owner,
+                             int32_t* transfers, int32_t* count);
 
 /* ---------------------------------------------------------------------------------------------------
  * Discrete adjoint (a forward / backward pair; no counterpart in the reference, whose marchTimeStep,

@@ -75,3 +75,27 @@ def test_random_cases_slabs(seed):
 def test_taylor_green_256_four_slabs():
     """The benchmark workload split into four slabs, three RK4 steps, against the single-grid solve."""
     compare(open(nsfsi.case_path("tgv256")).read(), 4, 3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nslabs", [2, 3])
+def test_nccl_path_on_one_gpu(nslabs):
+    """A group created for several processes, here one (world = 1), with every plane moved by NCCL (send and
+    receive to itself) and the partials all-gathered: the same fields, t and dt as the single-grid solve."""
+    text = open(os.path.join(CASES, "tgv_small.cfg")).read()
+    steps = 12
+    with nsfsi.Solver(text) as s:
+        s.march(steps)
+        s.sync()
+        ref = s.download()
+        t, lv, dt = s.time()
+    nid = nsfsi.slab_nccl_id()
+    with nsfsi.SlabGroup(text, nslabs, 0, rank=0, world=1, nccl_id=nid, flags=nsfsi.SLAB_NCCL_ALL) as g:
+        n, first, lps = g.info()
+        assert n == nslabs
+        g.march(steps)
+        g.sync()
+        got = g.download()
+        assert np.array_equal(got, ref), [float(np.abs(a - b).max()) for a, b in zip(got, ref)]
+        for p in range(nslabs):
+            assert g.slab(p).time() == (t, lv, dt)

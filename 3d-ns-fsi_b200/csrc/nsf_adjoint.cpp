@@ -11,7 +11,10 @@
 // Backward: binomial checkpointing over the steps (Griewank's schedule: with c free snapshots the longest
 // reversible run in t sweeps is C(c+t, t)); a step whose adjoint is due is recomputed kernel by kernel
 // from its snapshot, keeping each stage's inputs, and the adjoint kernels (nsf_adjoint.cu) then run in
-// reverse kernel order on adjoint arrays that mirror the physical field buffers.
+// reverse kernel order on adjoint arrays that mirror the physical field buffers. The recomputation and
+// the schedule's restores and advances run on the solver's stream, the adjoint kernels on a second
+// stream, with two snapshot sets between them: the forward work of the next step overlaps the adjoint
+// kernels of the current one (at the grid sizes of the adjoint both use a fraction of the GPU).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,15 +63,26 @@ struct AdjCtx {
   double* ipbar = nullptr;
   double* fbar = nullptr;
   unsigned long long* bcSync = nullptr;  // grid-barrier counter of k_adj_bc
+  int* dTimeout = nullptr;               // set when a barrier of k_adj_bc gives up (checked after the backward run)
   std::vector<double*> slot;
   std::vector<StepCtl*> slotCtl;
-  double* stageSnap = nullptr;  // 4 x (11 Nd + 2F): I (5), R (1), O before the edge conditions (5), fpre
+  // Two snapshot sets: the recomputation of one step fills one set (on the solver's stream) while the
+  // adjoint kernels of the step before read the other (on adjStream). A set holds per stage
+  // (11 Nd + 2F): I (5), R (1), O before the edge conditions (5), fpre; then the step's result O (5 Nd);
+  // and the step's control block after its prologue.
+  double* snapStage[2] = {nullptr, nullptr};
+  double* snapResult[2] = {nullptr, nullptr};
+  StepCtl* snapCtl[2] = {nullptr, nullptr};
+  int nextSet = 0;
+  cudaStream_t adjStream = nullptr;
+  cudaEvent_t setReady[2] = {nullptr, nullptr};  // recorded on the solver's stream once a set is filled
+  cudaEvent_t setFree[2] = {nullptr, nullptr};   // recorded on adjStream once the adjoint kernels read it
   StepCtl* dHist = nullptr;      // [nsteps]: each step's control block after its prologue (written on the device)
   std::vector<StepCtl> hist;     // host copy of dHist from the last forward run
   std::vector<std::pair<int, int>> chain;  // (level, slot) checkpoints the forward run stores
   bool chainStored = false;                // the slots still hold the last forward run's checkpoints
-  StepCtl* dCur = nullptr;                 // the control block of the step being reversed (after its prologue)
-  // one CUDA graph per distinct pattern of buffer roles (the roles rotate with a short period)
+  // CUDA graphs per distinct pattern of buffer roles (the roles rotate with a short period) and snapshot
+  // set: the recomputation (solver's stream) and the adjoint kernels (adjStream)
   std::map<std::vector<uintptr_t>, cudaGraphExec_t> graphs;
   // Stage 4 of a recomputed step whose result enters no objective term: only the x-planes the inlet /
   // outlet adjoint reads (i = 1, 2, NI-3, NI-2) are computed, and nothing after that stage kernel runs.
@@ -160,9 +174,17 @@ nsf_status setup(nsf_solver* s) {
   if ((st = aalloc(s, a, &a->fbar, 2 * plane)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->bcSync, 1)) != NSF_OK) return st;
   CKA(cudaMemset(a->bcSync, 0, sizeof(unsigned long long)));
-  if ((st = aalloc(s, a, &a->stageSnap, 4 * per_stage(s))) != NSF_OK) return st;
+  if ((st = aalloc(s, a, &a->dTimeout, 1)) != NSF_OK) return st;
+  CKA(cudaMemset(a->dTimeout, 0, sizeof(int)));
+  for (int j = 0; j < 2; ++j) {
+    if ((st = aalloc(s, a, &a->snapStage[j], 4 * per_stage(s))) != NSF_OK) return st;
+    if ((st = aalloc(s, a, &a->snapResult[j], 5 * N)) != NSF_OK) return st;
+    if ((st = aalloc(s, a, &a->snapCtl[j], 1)) != NSF_OK) return st;
+    CKA(cudaEventCreateWithFlags(&a->setReady[j], cudaEventDisableTiming));
+    CKA(cudaEventCreateWithFlags(&a->setFree[j], cudaEventDisableTiming));
+  }
+  CKA(cudaStreamCreateWithFlags(&a->adjStream, cudaStreamNonBlocking));
   if ((st = aalloc(s, a, &a->dHist, size_t(a->nsteps))) != NSF_OK) return st;
-  if ((st = aalloc(s, a, &a->dCur, 1)) != NSF_OK) return st;
   {  // the partial stage-4 plan: the main plan's tiles over planes [1, 2] and [NI-3, NI-2], round robin
     LaunchPlan& P = a->lastStagePlan;
     P = s->plan;
@@ -315,36 +337,31 @@ nsf_status advance(nsf_solver* s, int n) {
   return NSF_OK;
 }
 
-// Keeps the step's control block and, per stage, the values the nonlinear adjoints need. The step's roles
-// (which physical buffer plays which part) are known on the host from the forward run's record, so nothing
-// waits here and the whole adjoint step can be captured as a graph.
-// Which stage values the adjoint reads from the snapshot and which it reads live from the buffers after
-// the recomputed step. Outside global-filter steps, the stage-1 input is U0 and the stage-4 input is the
-// stage-3 output: no later kernel of the step writes either buffer, so both are read in place; the density
-// for the primitives is the input's own density buffer except on filter steps.
-struct SnapPlan {
-  bool inputLive, rSeparate;
+// What the adjoint kernels of a step read, all from one snapshot set, so the next step's recomputation may
+// overwrite the working buffers meanwhile: per stage its input values I (and its density R when that is
+// another buffer), the near-body filter's pre-values and, for x inlet / outlet faces whose neighbouring
+// planes are not clean (AdjCtx::edgePlanesClean), the four x-planes next to them (i = 1, 2, NI-3, NI-2) of
+// the stage output before the edge conditions; the step's result; the step's control block. The step's
+// roles (which physical buffer plays which part) are known on the host from the forward run's record, so
+// nothing waits here and the recomputation can be captured as a graph.
+struct SnapSet {
+  double* stage;  // 4 x per_stage
+  double* result;  // 5 Nd
+  StepCtl* ctl;
 };
-SnapPlan snap_plan(const StepCtl& R, int q) {
-  const bool live = !R.filterNow && (q == 0 || q == 3);
-  return SnapPlan{live, !live && R.R[q] != R.I[q][0]};
-}
+SnapSet snap_set(const AdjCtx* a, int j) { return SnapSet{a->snapStage[j], a->snapResult[j], a->snapCtl[j]}; }
 
-// Keeps the step's control block and, per stage, the values the nonlinear adjoints need that the step
-// overwrites: the stage inputs (snap_plan), the near-body filter's pre-values and, for x inlet / outlet
-// faces whose neighbouring planes are not clean (AdjCtx::edgePlanesClean), the four x-planes next to them
-// (i = 1, 2, NI-3, NI-2) of the stage output before the edge conditions. The step's roles (which physical buffer plays which part) are known on the host from the
-// forward run's record, so nothing waits here and the whole adjoint step can be captured as a graph.
 struct SnapHook : StepHook {
   nsf_solver* s;
   AdjCtx* a;
   const StepCtl& R;
+  SnapSet set;
   cudaError_t err = cudaSuccess;
   const double* src[kMaxCopies];
   double* dst[kMaxCopies];
   long long words[kMaxCopies];
   int n = 0;
-  SnapHook(nsf_solver* s_, AdjCtx* a_, const StepCtl& r) : s(s_), a(a_), R(r) {}
+  SnapHook(nsf_solver* s_, AdjCtx* a_, const StepCtl& r, SnapSet st) : s(s_), a(a_), R(r), set(st) {}
   void add(double* d, const double* sr, size_t w) {
     if (n == kMaxCopies) flush();
     src[n] = sr;
@@ -356,15 +373,13 @@ struct SnapHook : StepHook {
     n = 0;
   }
   void after_prologue() override {
-    if (err == cudaSuccess) err = cudaMemcpyAsync(a->dCur, s->dCtl, sizeof(StepCtl), cudaMemcpyDeviceToDevice, s->stream);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(set.ctl, s->dCtl, sizeof(StepCtl), cudaMemcpyDeviceToDevice, s->stream);
   }
   void before_stage(int q) override {
     const size_t N = nd(s);
-    double* base = a->stageSnap + q * per_stage(s);
-    const SnapPlan P = snap_plan(R, q);
-    if (!P.inputLive)
-      for (int f = 0; f < 5; ++f) add(base + f * N, R.I[q][f], N);
-    if (P.rSeparate) add(base + 5 * N, R.R[q], N);
+    double* base = set.stage + q * per_stage(s);
+    for (int f = 0; f < 5; ++f) add(base + f * N, R.I[q][f], N);
+    if (R.R[q] != R.I[q][0]) add(base + 5 * N, R.R[q], N);
     if (nf(s)) add(base + 11 * N, s->hGrid.fpre, 2 * nf(s));
     flush();
   }
@@ -372,9 +387,15 @@ struct SnapHook : StepHook {
   void before_edges(int q) override {
     if (!a->xInOut || a->edgePlanesClean) return;
     const size_t N = nd(s), plane = size_t(s->hGrid.sI), NI = size_t(s->hGrid.NI);
-    double* base = a->stageSnap + q * per_stage(s);
+    double* base = set.stage + q * per_stage(s);
     for (size_t i : {size_t(1), size_t(2), NI - 3, NI - 2})
       for (int f = 0; f < 4; ++f) add(base + (6 + f) * N + i * plane, R.O[q][f] + i * plane, plane);
+    flush();
+  }
+  // after the step: its result (the objective's pressure, the inlet / outlet adjoint of stage 4)
+  void result() {
+    const size_t N = nd(s);
+    for (int f = 0; f < 5; ++f) add(set.result + f * N, R.O[3][f], N);
     flush();
   }
 };
@@ -406,28 +427,34 @@ struct PhaseTimer {
   }
 };
 
-// Enqueues the adjoint of a step with roles R: the working state holds U_k on entry (U_{k+1} on exit);
-// the adjoint arrays hold the adjoint of U_{k+1} on entry and of U_k on exit. objective: F_x(U_{k+1})
-// enters J. pt: NULL, or events between the phases (eager launches only).
-nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool objective, PhaseTimer* pt = nullptr) {
+// Enqueues the recomputation of a step with roles R on the solver's stream, filling snapshot set `set`:
+// the working state holds U_k on entry, U_{k+1} on exit. objective: F_x(U_{k+1}) enters J (the whole step
+// runs; else stage 4 only where the inlet / outlet adjoint reads it). pt: NULL, or phase events.
+nsf_status enqueue_recompute(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool objective, int set,
+                             PhaseTimer* pt = nullptr) {
+  SnapHook hook(s, a, R, snap_set(a, set));
+  if (pt) pt->mark(-1);
+  enqueue_step_hooked(s->dGrid, s->hGrid, s->plan, s->stream, &hook, objective ? nullptr : &a->lastStagePlan);
+  hook.result();
+  if (pt) pt->mark(PH_RECOMPUTE);
+  if (hook.err != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint recomputation: ") + cudaGetErrorString(hook.err));
+  CKA(cudaGetLastError());
+  return NSF_OK;
+}
+
+// Enqueues the adjoint kernels of that step on `stream`, reading only snapshot set `set` and fixed
+// buffers: the adjoint arrays hold the adjoint of U_{k+1} on entry and of U_k on exit.
+nsf_status enqueue_adjoint_kernels(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool objective, int set,
+                                   cudaStream_t st, PhaseTimer* pt = nullptr) {
   auto mark = [&](int ph) {
     if (pt) pt->mark(ph);
   };
-  const StepCtl* dR = a->dCur;
-  SnapHook hook(s, a, R);
-  mark(-1);
-  // the whole step when its result enters J (the objective's adjoint reads it at the ghost nodes), else
-  // stage 4 only where the inlet / outlet adjoint reads it
-  enqueue_step_hooked(s->dGrid, s->hGrid, s->plan, s->stream, &hook, objective ? nullptr : &a->lastStagePlan);
-  mark(PH_RECOMPUTE);
-  if (hook.err != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint recomputation: ") + cudaGetErrorString(hook.err));
-  CKA(cudaGetLastError());
+  const SnapSet S = snap_set(a, set);
   const Grid& G = s->hGrid;
   const size_t N = nd(s);
   const int nSM = s->nSM;
-  cudaStream_t st = s->stream;
   for (int q = 3; q >= 0; --q) {
-    const double* snap = a->stageSnap + q * per_stage(s);
+    const double* snap = S.stage + q * per_stage(s);
     AdjBcParams P{};
     AdjPtrs& A = P.A;
     for (int f = 0; f < 5; ++f) {
@@ -441,7 +468,7 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     A.lamFnew = a->lamFnew;
     // the objective's adjoint (F_x of the step's result) joins the ghost phase of the last stage
     P.objective = (objective && q == 3) ? 1 : 0;
-    for (int f = 0; f < 5; ++f) P.objVal[f] = R.O[3][f];
+    for (int f = 0; f < 5; ++f) P.objVal[f] = S.result + f * N;
     P.nx = a->dNx;
     P.dA = a->dA;
     P.weight = 1.0 / a->navg;
@@ -456,14 +483,12 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     // edge conditions: z, y, then x (reads the stage output before the edge conditions: its copy, or,
     // where the planes it reads are clean, the next stage's input / the step's result)
     for (int f = 0; f < 5; ++f) {
-      if (!a->edgePlanesClean) {
+      if (!a->edgePlanesClean)
         P.edgeVal[f] = snap + (6 + f) * N;
-      } else if (q == 3) {
-        P.edgeVal[f] = R.O[3][f];
-      } else {
-        const SnapPlan Pn = snap_plan(R, q + 1);
-        P.edgeVal[f] = Pn.inputLive ? R.I[q + 1][f] : a->stageSnap + (q + 1) * per_stage(s) + f * N;
-      }
+      else if (q == 3)
+        P.edgeVal[f] = S.result + f * N;
+      else
+        P.edgeVal[f] = S.stage + (q + 1) * per_stage(s) + f * N;
     }
     for (int axis = 0; axis < 3; ++axis) {
       P.edges[axis] = s->plan.edgeBlocks[axis];
@@ -472,17 +497,16 @@ nsf_status enqueue_adjoint_step(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool
     P.inletGather = a->inletX ? 1 : 0;
     P.fbar = a->fbar;
     P.lamInflow = a->lamInflow;
-    P.roles = dR;
+    P.roles = S.ctl;
     // stage kernel: RK4 combine and the RHS inputs (from the stage input's values), then the transposed RHS
-    const SnapPlan SP = snap_plan(R, q);
-    for (int f = 0; f < 5; ++f) A.val[f] = SP.inputLive ? R.I[q][f] : snap + f * N;
-    A.valR = SP.inputLive ? R.R[q] : SP.rSeparate ? snap + 5 * N : snap;
+    for (int f = 0; f < 5; ++f) A.val[f] = snap + f * N;
+    A.valR = R.R[q] != R.I[q][0] ? snap + 5 * N : snap;
     A.valFpre = snap + 11 * N;
     P.solidMask = G.nSolid ? R.copyMask[q] : 0;
     P.lam = a->tmpLam;
     P.V = a->tmpV;
     P.sync = a->bcSync;
-    P.timeout = &s->dCtl->timeout;
+    P.timeout = a->dTimeout;
     launch_adj_bc(G, P, q, nSM, st);
     mark(PH_BC);
     launch_adj_rhs(s->dGrid, G, A, a->tmpLam, a->tmpV, nSM, st);
@@ -518,20 +542,24 @@ std::vector<uintptr_t> role_key(const StepCtl& R, bool objective) {
   return key;
 }
 
-// The adjoint of step k, launched as the cached graph of its role pattern.
-nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
+// A cached graph of one part of an adjoint step (0: recomputation, 1: adjoint kernels) for a role pattern
+// and snapshot set, captured on `st` at first use.
+nsf_status step_graph(nsf_solver* s, AdjCtx* a, int k, int part, int set, cudaStream_t st, cudaGraphExec_t* out) {
   const StepCtl& R = a->hist[k];
   const bool objective = k + 1 > a->nsteps - a->navg;
-  const auto key = role_key(R, objective);
+  auto key = role_key(R, objective);
+  key.push_back(uintptr_t(part));
+  key.push_back(uintptr_t(set));
   auto it = a->graphs.find(key);
   if (it == a->graphs.end()) {
-    CKA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    const nsf_status st = enqueue_adjoint_step(s, a, R, objective);
+    CKA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const nsf_status r = part == 0 ? enqueue_recompute(s, a, R, objective, set)
+                                   : enqueue_adjoint_kernels(s, a, R, objective, set, st);
     cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
-    if (st != NSF_OK) {
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (r != NSF_OK) {
       if (g) cudaGraphDestroy(g);
-      return st;
+      return r;
     }
     if (e != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint step capture: ") + cudaGetErrorString(e));
     cudaGraphExec_t x = nullptr;
@@ -540,7 +568,28 @@ nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
     if (e2 != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("adjoint step graph: ") + cudaGetErrorString(e2));
     it = a->graphs.emplace(key, x).first;
   }
-  CKA(cudaGraphLaunch(it->second, s->stream));
+  *out = it->second;
+  return NSF_OK;
+}
+
+// The adjoint of step k, pipelined over two streams: the recomputation fills the next snapshot set on the
+// solver's stream (after the adjoint kernels that last read that set are done), and the adjoint kernels
+// read it on adjStream. The solver's stream then goes on with the schedule (restoring and advancing
+// towards the step before) while those kernels run: every adjoint kernel reads only its set and fixed
+// buffers, and only the adjoint kernels write the adjoint arrays, in step order on one stream.
+nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
+  const int j = a->nextSet;
+  a->nextSet ^= 1;
+  cudaGraphExec_t rec = nullptr, adj = nullptr;
+  nsf_status st = step_graph(s, a, k, 0, j, s->stream, &rec);
+  if (st == NSF_OK) st = step_graph(s, a, k, 1, j, a->adjStream, &adj);
+  if (st != NSF_OK) return st;
+  CKA(cudaStreamWaitEvent(s->stream, a->setFree[j], 0));
+  CKA(cudaGraphLaunch(rec, s->stream));
+  CKA(cudaEventRecord(a->setReady[j], s->stream));
+  CKA(cudaStreamWaitEvent(a->adjStream, a->setReady[j], 0));
+  CKA(cudaGraphLaunch(adj, a->adjStream));
+  CKA(cudaEventRecord(a->setFree[j], a->adjStream));
   return NSF_OK;
 }
 
@@ -601,8 +650,15 @@ nsf_status reverse(nsf_solver* s, AdjCtx* a, int a0, int b, int c, int depth, bo
 
 void nsf_adjoint_free(nsf_solver* s) {
   if (!s || !s->adj) return;
-  for (auto& kv : s->adj->graphs) cudaGraphExecDestroy(kv.second);
-  for (void* p : s->adj->allocs) cudaFree(p);
+  AdjCtx* a = s->adj;
+  if (a->adjStream) cudaStreamSynchronize(a->adjStream);
+  for (auto& kv : a->graphs) cudaGraphExecDestroy(kv.second);
+  for (int j = 0; j < 2; ++j) {
+    if (a->setReady[j]) cudaEventDestroy(a->setReady[j]);
+    if (a->setFree[j]) cudaEventDestroy(a->setFree[j]);
+  }
+  if (a->adjStream) cudaStreamDestroy(a->adjStream);
+  for (void* p : a->allocs) cudaFree(p);
   delete s->adj;
   s->adj = nullptr;
 }
@@ -703,15 +759,24 @@ nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* 
   }
   CKA(cudaMemsetAsync(a->lamInflow, 0, plane * sizeof(double), s->stream));
   CKA(cudaMemsetAsync(a->fbar, 0, 2 * plane * sizeof(double), s->stream));
+  CKA(cudaMemsetAsync(a->dTimeout, 0, sizeof(int), s->stream));
+  CKA(cudaStreamSynchronize(s->stream));  // the adjoint kernels on adjStream start from these
   st = reverse(s, a, 0, a->nsteps, a->nsnap, 0, a->chainStored);
   a->chainStored = false;  // the schedule has reused the slots
-  if (st != NSF_OK) return st;
+  if (st != NSF_OK) {
+    cudaStreamSynchronize(a->adjStream);
+    return st;
+  }
   // level-0 fpre was copied from U0
-  launch_fpre_init_adj(s->dGrid, G.nFilter, a->lamFpre, lamOf(s, a, 0, 0), lamOf(s, a, 0, 4), s->nSM, s->stream);
+  launch_fpre_init_adj(s->dGrid, G.nFilter, a->lamFpre, lamOf(s, a, 0, 0), lamOf(s, a, 0, 4), s->nSM, a->adjStream);
+  CKA(cudaStreamSynchronize(a->adjStream));
   CKA(cudaStreamSynchronize(s->stream));
   StepCtl ctl;
+  int adjTimeout = 0;
   CKA(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  CKA(cudaMemcpy(&adjTimeout, a->dTimeout, sizeof adjTimeout, cudaMemcpyDeviceToHost));
   if (ctl.timeout) return fail(s, NSF_ERR_TIMEOUT, "a bounded wait in the stage kernel gave up during the adjoint");
+  if (adjTimeout) return fail(s, NSF_ERR_TIMEOUT, "a grid barrier of the adjoint boundary kernel gave up");
   const size_t hp = S.NK * sizeof(double), dp = size_t(G.NKp) * sizeof(double);
   if (g_u0) {
     for (int f = 0; f < 5; ++f)
@@ -735,8 +800,11 @@ nsf_status nsf_adj_profile_step(nsf_solver* s, uint64_t step, double* ms) {
   nsf_status st = restore(s, a, 0);
   if (st == NSF_OK) st = advance(s, int(step));
   if (st != NSF_OK) return st;
-  PhaseTimer pt{s->stream, {}, {}};
-  st = enqueue_adjoint_step(s, a, a->hist[step], int(step) + 1 > a->nsteps - a->navg, &pt);
+  PhaseTimer pt{s->stream, {}, {}};  // both parts on the solver's stream, one after the other
+  const bool objective = int(step) + 1 > a->nsteps - a->navg;
+  CKA(cudaStreamSynchronize(a->adjStream));
+  st = enqueue_recompute(s, a, a->hist[step], objective, 0, &pt);
+  if (st == NSF_OK) st = enqueue_adjoint_kernels(s, a, a->hist[step], objective, 0, s->stream, &pt);
   CKA(cudaStreamSynchronize(s->stream));
   for (int q = 0; q < PH_COUNT; ++q) ms[q] = 0;
   pt.collect(ms);

@@ -47,6 +47,7 @@ struct AdjCtx {
   int* cent = nullptr;
   int ncell = 0;
   long long* fsNodes = nullptr;
+  int* fsSlots = nullptr;
   int nfs = 0;
   bool inletX = false;
   bool xInOut = false;  // an x face is an inlet or an outlet (its adjoint reads the planes next to it)
@@ -272,6 +273,21 @@ nsf_status setup(nsf_solver* s) {
   a->nfs = int(fsv.size());
   if ((st = aalloc(s, a, &a->fsNodes, fsv.size())) != NSF_OK) return st;
   if (!fsv.empty()) CKA(cudaMemcpy(a->fsNodes, fsv.data(), fsv.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  {  // per stencil node: its own filter slot and its six neighbours' (the order of the filter's gather)
+    std::map<long long, int> slotOf;
+    for (size_t q = 0; q < fnode.size(); ++q) slotOf.emplace(fnode[q], int(q));
+    const long long off[6] = {G.sI, -G.sI, G.sJ, -G.sJ, 1, -1};
+    std::vector<int> slots(7 * fsv.size(), -1);
+    for (size_t q = 0; q < fsv.size(); ++q)
+      for (int d = 0; d < 7; ++d) {
+        const long long n = d == 0 ? fsv[q] : fsv[q] + off[d - 1];
+        if (n < 0 || n >= G.N) continue;
+        const auto it = slotOf.find(n);
+        if (it != slotOf.end()) slots[7 * q + size_t(d)] = it->second;
+      }
+    if ((st = aalloc(s, a, &a->fsSlots, slots.size())) != NSF_OK) return st;
+    if (!slots.empty()) CKA(cudaMemcpy(a->fsSlots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
   // inflow profile factor 1; the initial condition of the case as the default level-0 state
   std::vector<double> ones(plane, 1.0);
   CKA(cudaMemcpy(a->dInflow, ones.data(), plane * sizeof(double), cudaMemcpyHostToDevice));
@@ -479,6 +495,7 @@ nsf_status enqueue_adjoint_kernels(nsf_solver* s, AdjCtx* a, const StepCtl& R, b
     P.cent = a->cent;
     P.ncell = a->ncell;
     P.fsNodes = a->fsNodes;
+    P.fsSlots = a->fsSlots;
     P.nfs = a->nfs;
     // edge conditions: z, y, then x (reads the stage output before the edge conditions: its copy, or,
     // where the planes it reads are clean, the next stage's input / the step's result)

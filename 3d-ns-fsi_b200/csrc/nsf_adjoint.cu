@@ -106,46 +106,56 @@ __device__ __forceinline__ void adj_ghost_consume_item(const Grid& G, const AdjP
 __device__ __forceinline__ void adj_ghost_gather_item(const Grid& G, const AdjPtrs& A, const double* ipbar,
                                                       const AdjBcParams& P, int c) {
   const long long m = P.cnode[c];
+  const int e0 = P.coff[c], e1 = P.coff[c + 1];
+  // the node's own values first (they depend on m only), so their loads overlap the entries' loads
+  const bool filt = (G.type[m] & FILTER_BIT) != 0;
+  const int fi = filt ? G.fidx[m] : 0;
+  double* const t0 = filt ? A.lamFnew + 2 * fi : A.lamO[0] + m;  // where the density's adjoint goes
+  double* const t4 = filt ? A.lamFnew + 2 * fi + 1 : A.lamO[4] + m;
+  double o[5];
+  o[0] = *t0;
+  o[4] = *t4;
+  for (int f = 1; f < 4; ++f) o[f] = A.lamO[f][m];
   double a[5] = {0, 0, 0, 0, 0};
-  for (int e = P.coff[c]; e < P.coff[c + 1]; ++e) {
+  for (int e = e0; e < e1; ++e) {
     const int q = P.cent[e] >> 3, slot = P.cent[e] & 7;
     const double wn = G.gw[16 * (long long)q + slot], wd = G.gw[16 * (long long)q + 8 + slot];
     a[0] += wn * ipbar[q];
     a[4] += wn * ipbar[4 * (long long)G.nGhost + q];
     for (int f = 1; f < 4; ++f) a[f] += wd * ipbar[f * (long long)G.nGhost + q];
   }
-  if (G.type[m] & FILTER_BIT) {  // k_ghost read the filtered values of this node
-    const int f = G.fidx[m];
-    A.lamFnew[2 * f] += a[0];
-    A.lamFnew[2 * f + 1] += a[4];
-  } else {
-    A.lamO[0][m] += a[0];
-    A.lamO[4][m] += a[4];
-  }
-  for (int f = 1; f < 4; ++f) A.lamO[f][m] += a[f];
+  *t0 = o[0] + a[0];  // filter node: k_ghost read its filtered values
+  *t4 = o[4] + a[4];
+  for (int f = 1; f < 4; ++f) A.lamO[f][m] = o[f] + a[f];
 }
 
 // ------------------------------------------------------------------------------- near-body filter
 // k_body_filter: fpre = O at the filter node, fnew = (6 O[n] + sum of the 6 neighbours)/12 (rho, rho_E).
-// Every node of the filter stencils gathers from the filter nodes whose stencil holds it.
-__device__ __forceinline__ void adj_filter_item(const Grid& G, const AdjPtrs& A, const long long* nodes, int q) {
-  const long long off[6] = {G.sI, -G.sI, G.sJ, -G.sJ, 1, -1};
+// Every node of the filter stencils gathers from the filter nodes whose stencil holds it. slots[7 q ..]:
+// the node's own filter slot, then those of its neighbours at +-i, +-j, +-k (-1: not a filter node),
+// listed at setup so that an item's loads take two round trips (indices, then values).
+__device__ __forceinline__ void adj_filter_item(const AdjPtrs& A, const long long* nodes, const int* slots, int q) {
   const long long m = nodes[q];
+  int sl[7];
+  for (int d = 0; d < 7; ++d) sl[d] = slots[7 * (long long)q + d];
+  double fn[7][2], fp[2] = {0, 0};
+  for (int d = 0; d < 7; ++d)
+    for (int c = 0; c < 2; ++c) fn[d][c] = sl[d] >= 0 ? A.lamFnew[2 * sl[d] + c] : 0.0;
+  if (sl[0] >= 0)
+    for (int c = 0; c < 2; ++c) fp[c] = A.lamFpre[2 * sl[0] + c];
+  const double o0 = A.lamO[0][m], o4 = A.lamO[4][m];
   double ar = 0, ae = 0;
-  if (G.type[m] & FILTER_BIT) {
-    const int f = G.fidx[m];
-    ar += 0.5 * A.lamFnew[2 * f] + A.lamFpre[2 * f];
-    ae += 0.5 * A.lamFnew[2 * f + 1] + A.lamFpre[2 * f + 1];
+  if (sl[0] >= 0) {
+    ar += 0.5 * fn[0][0] + fp[0];
+    ae += 0.5 * fn[0][1] + fp[1];
   }
-  for (int d = 0; d < 6; ++d) {
-    const long long n = m + off[d];
-    if (n < 0 || n >= G.N || !(G.type[n] & FILTER_BIT)) continue;
-    const int f = G.fidx[n];
-    ar += A.lamFnew[2 * f] / 12;
-    ae += A.lamFnew[2 * f + 1] / 12;
+  for (int d = 1; d < 7; ++d) {
+    if (sl[d] < 0) continue;
+    ar += fn[d][0] / 12;
+    ae += fn[d][1] / 12;
   }
-  A.lamO[0][m] += ar;
-  A.lamO[4][m] += ae;
+  A.lamO[0][m] = o0 + ar;
+  A.lamO[4][m] = o4 + ae;
 }
 
 // -------------------------------------------------------------------------------- edge boundaries
@@ -170,33 +180,53 @@ __device__ __forceinline__ void adj_edge_item(const Grid& G, const EdgeBlock& eb
   const long long st = axis == 0 ? G.sI : axis == 1 ? G.sJ : 1;
   const long long n = ijk[0] * G.sI + ijk[1] * G.sJ + ijk[2];
   const int side = G.eSide[e], bc = G.eBc[e];
+  // Every load of an item is issued before its first store (one memory round trip, not two): the nodes
+  // an item reads and writes are its own -- no other item of the phase touches them.
   double lam[5];
-  for (int f = 0; f < 5; ++f) {
-    lam[f] = A.lamO[f][n];
-    A.lamO[f][n] = 0.0;
-  }
   if (bc == NSF_BC_PERIODIC) {
     int src[3] = {ijk[0], ijk[1], ijk[2]};
     const int nAx = axis == 0 ? G.NI : axis == 1 ? G.NJ : G.NK;
     src[axis] = side == 0 ? nAx - 2 : 1;
     const long long m = src[0] * G.sI + src[1] * G.sJ + src[2];
-    for (int f = 0; f < 5; ++f) A.lamO[f][m] += lam[f];
-  } else if (bc == NSF_BC_OUTLET) {
+    double acc[5];
+    for (int f = 0; f < 5; ++f) {
+      lam[f] = A.lamO[f][n];
+      acc[f] = A.lamO[f][m];
+    }
+    for (int f = 0; f < 5; ++f) {
+      A.lamO[f][n] = 0.0;
+      A.lamO[f][m] = acc[f] + lam[f];
+    }
+    return;
+  }
+  if (bc == NSF_BC_OUTLET) {
     const long long a1 = side == 0 ? n + st : n - st, a2 = side == 0 ? n + 2 * st : n - 2 * st;
-    const double rho = 2 * val[0][a1] - val[0][a2];
+    double v1[4], v2[4], l1[4], l2[4];
+    for (int f = 0; f < 5; ++f) lam[f] = A.lamO[f][n];
+    for (int f = 0; f < 4; ++f) {
+      v1[f] = val[f][a1];
+      v2[f] = val[f][a2];
+      l1[f] = A.lamO[f][a1];
+      l2[f] = A.lamO[f][a2];
+    }
+    for (int f = 0; f < 5; ++f) A.lamO[f][n] = 0.0;
+    const double rho = 2 * v1[0] - v2[0];
     double u[3];
-    for (int f = 1; f < 4; ++f) u[f - 1] = (2 * val[f][a1] - val[f][a2]) / (1 + rho);
+    for (int f = 1; f < 4; ++f) u[f - 1] = (2 * v1[f] - v2[f]) / (1 + rho);
     // rho_E = (1 + rho)/2 |u|^2 with u = m/(1 + rho): d/drho = -|u|^2/2, d/dm = u
     const double rbar = lam[0] - 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) * lam[4];
-    A.lamO[0][a1] += 2 * rbar;
-    A.lamO[0][a2] -= rbar;
+    A.lamO[0][a1] = l1[0] + 2 * rbar;
+    A.lamO[0][a2] = l2[0] - rbar;
     for (int f = 1; f < 4; ++f) {
       const double mbar = lam[f] + u[f - 1] * lam[4];
-      A.lamO[f][a1] += 2 * mbar;
-      A.lamO[f][a2] -= mbar;
+      A.lamO[f][a1] = l1[f] + 2 * mbar;
+      A.lamO[f][a2] = l2[f] - mbar;
     }
-  } else if (bc == NSF_BC_INLET) {
+    return;
+  }
+  if (bc == NSF_BC_INLET) {
     // rho = f (filtered extrapolation); u_axis = ramp * M0 * profile; T = 0; p = rho / gamma
+    for (int f = 0; f < 5; ++f) lam[f] = A.lamO[f][n];
     const long long s1 = ax1 == 0 ? G.sI : G.sJ, s2 = ax2 == 1 ? G.sJ : 1;
     auto ext = [&](long long m) {
       return 2 * val[0][side == 0 ? m + st : m - st] - val[0][side == 0 ? m + 2 * st : m - 2 * st];
@@ -211,12 +241,16 @@ __device__ __forceinline__ void adj_edge_item(const Grid& G, const EdgeBlock& eb
     f /= 2 * nn;
     const double ramp = fmin(1., stageT / 10.) * C.m0 * (side == 1 ? -1.0 : 1.0);
     const double prof = (G.inflow && axis == 0) ? G.inflow[a * G.NKp + bb] : 1.0;
+    const double inflowBar = axis == 0 ? lamInflow[a * G.NKp + bb] : 0.0;
+    for (int f = 0; f < 5; ++f) A.lamO[f][n] = 0.0;
     const double vel = ramp * prof;
     const double fb = lam[0] + vel * lam[axis + 1] + (1 / (C.gamma * C.gm1) + 0.5 * vel * vel) * lam[4];
     const double velbar = (1 + f) * (lam[axis + 1] + vel * lam[4]);
-    if (axis == 0) lamInflow[a * G.NKp + bb] += velbar * ramp;
+    if (axis == 0) lamInflow[a * G.NKp + bb] = inflowBar + velbar * ramp;
     fbar[(long long)a * G.NKp + bb + (side ? (long long)G.NJ * G.NKp : 0)] = fb;
+    return;
   }
+  for (int f = 0; f < 5; ++f) A.lamO[f][n] = 0.0;  // any other condition: the value is consumed
 }
 
 // Inlet phase 2 (x faces only): every node of the two planes behind the inlet gathers from the inlet
@@ -340,8 +374,8 @@ __device__ __forceinline__ void adj_prepare_item(const Grid& G, const AdjPtrs& A
 // edge block counts 64 items (32 x kEdgeRows nodes). The RK4 combine and RHS inputs, one item per node,
 // follow as a kernel of their own (measured faster than a last phase of the cooperative launch, whose
 // grid is sized for the few boundary items).
-constexpr int kAdjBcThreads = 256, kAdjBcBlocksPerSM = 4;  // registers capped for 4 resident blocks per SM
-__global__ void __launch_bounds__(kAdjBcThreads, kAdjBcBlocksPerSM)
+constexpr int kAdjBcThreads = 256;  // the grid is sized by the largest phase: a few dozen blocks
+__global__ void __launch_bounds__(kAdjBcThreads)
     k_adj_bc(const __grid_constant__ Grid G, const __grid_constant__ AdjBcParams P, int s) {
   const AdjPtrs& A = P.A;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
@@ -357,7 +391,7 @@ __global__ void __launch_bounds__(kAdjBcThreads, kAdjBcBlocksPerSM)
   if (barrier(P.ncell))
     for (int v = gtid; v < P.ncell; v += nthr) adj_ghost_gather_item(G, A, P.ipbar, P, v);
   if (barrier(P.nfs))
-    for (int v = gtid; v < P.nfs; v += nthr) adj_filter_item(G, A, P.fsNodes, v);
+    for (int v = gtid; v < P.nfs; v += nthr) adj_filter_item(A, P.fsNodes, P.fsSlots, v);
   const double stageT = P.roles->stageT[s];
   for (int axis = 2; axis >= 0; --axis)  // z, y, then x
     if (barrier(P.nEdge[axis]))

@@ -35,8 +35,10 @@ struct AdjBcParams {
   const int* coff;
   const int* cent;
   int ncell;
-  // near-body filter: the nodes of the filter stencils
+  // near-body filter: the nodes of the filter stencils and, per node, its own and its six neighbours'
+  // filter slots (7 each, -1: none)
   const long long* fsNodes;
+  const int* fsSlots;
   int nfs;
   // edge blocks per axis (k_edge_bc's), the values the edge conditions read (the stage output before
   // them), the inlet's per-node adjoints, the inflow profile's adjoint

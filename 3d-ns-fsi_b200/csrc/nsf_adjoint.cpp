@@ -63,7 +63,11 @@ struct AdjCtx {
   double* tmpV = nullptr;
   double* ipbar = nullptr;
   double* fbar = nullptr;
-  unsigned long long* bcSync = nullptr;  // grid-barrier counter of k_adj_bc
+  unsigned long long* bcSync = nullptr;  // grid-barrier counters of k_adj_bc (one per chain)
+  // No node of the bodies' adjoint work (ghosts, filter nodes, image-point cells, filter stencils) lies in
+  // the planes the edge conditions' adjoint touches (the faces and the two planes inside each): the two
+  // chains of the boundary kernel run side by side.
+  bool bodiesClearOfFaces = false;
   int* dTimeout = nullptr;               // set when a barrier of k_adj_bc gives up (checked after the backward run)
   std::vector<double*> slot;
   std::vector<StepCtl*> slotCtl;
@@ -173,8 +177,8 @@ nsf_status setup(nsf_solver* s) {
   if ((st = aalloc(s, a, &a->tmpV, 11 * N)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->ipbar, 5 * NG)) != NSF_OK) return st;
   if ((st = aalloc(s, a, &a->fbar, 2 * plane)) != NSF_OK) return st;
-  if ((st = aalloc(s, a, &a->bcSync, 1)) != NSF_OK) return st;
-  CKA(cudaMemset(a->bcSync, 0, sizeof(unsigned long long)));
+  if ((st = aalloc(s, a, &a->bcSync, 2)) != NSF_OK) return st;
+  CKA(cudaMemset(a->bcSync, 0, 2 * sizeof(unsigned long long)));
   if ((st = aalloc(s, a, &a->dTimeout, 1)) != NSF_OK) return st;
   CKA(cudaMemset(a->dTimeout, 0, sizeof(int)));
   for (int j = 0; j < 2; ++j) {
@@ -287,6 +291,18 @@ nsf_status setup(nsf_solver* s) {
       }
     if ((st = aalloc(s, a, &a->fsSlots, slots.size())) != NSF_OK) return st;
     if (!slots.empty()) CKA(cudaMemcpy(a->fsSlots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  {  // the bodies' adjoint nodes against the face planes (device indices: k fastest, rows of NKp)
+    std::vector<long long> gnode(NG);
+    if (NG) CKA(cudaMemcpy(gnode.data(), G.gnode, NG * sizeof(long long), cudaMemcpyDeviceToHost));
+    auto clear = [&](long long n) {
+      const long long i = n / G.sI, j = (n % G.sI) / G.sJ, k = n % G.sJ;
+      return i >= 3 && i <= G.NI - 4 && j >= 2 && j <= G.NJ - 3 && k >= 2 && k <= G.NK - 3;
+    };
+    bool ok = true;
+    for (const auto* v : {&gnode, &fnode, &cn, &fsv})
+      for (long long n : *v) ok = ok && clear(n);
+    a->bodiesClearOfFaces = ok;
   }
   // inflow profile factor 1; the initial condition of the case as the default level-0 state
   std::vector<double> ones(plane, 1.0);
@@ -523,6 +539,7 @@ nsf_status enqueue_adjoint_kernels(nsf_solver* s, AdjCtx* a, const StepCtl& R, b
     P.lam = a->tmpLam;
     P.V = a->tmpV;
     P.sync = a->bcSync;
+    P.bodyBlocks = a->bodiesClearOfFaces ? 1 : 0;
     P.timeout = a->dTimeout;
     launch_adj_bc(G, P, q, nSM, st);
     mark(PH_BC);

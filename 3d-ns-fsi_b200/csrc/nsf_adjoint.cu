@@ -378,20 +378,32 @@ constexpr int kAdjBcThreads = 256;  // the grid is sized by the largest phase: a
 __global__ void __launch_bounds__(kAdjBcThreads)
     k_adj_bc(const __grid_constant__ Grid G, const __grid_constant__ AdjBcParams P, int s) {
   const AdjPtrs& A = P.A;
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+  // One chain of phases over all blocks, or (P.bodyBlocks > 0: the host found the bodies' nodes and the
+  // face planes disjoint) two independent chains -- the body phases on the first bodyBlocks blocks, the
+  // edge phases on the rest -- each with its own barrier counter.
+  const bool split = P.bodyBlocks > 0;
+  const bool bodyChain = !split || int(blockIdx.x) < P.bodyBlocks;
+  const bool edgeChain = !split || int(blockIdx.x) >= P.bodyBlocks;
+  const int b0 = (split && edgeChain) ? P.bodyBlocks : 0;
+  const int nb = split ? (bodyChain ? P.bodyBlocks : int(gridDim.x) - P.bodyBlocks) : int(gridDim.x);
+  const int gtid = (int(blockIdx.x) - b0) * blockDim.x + threadIdx.x, nthr = nb * blockDim.x;
+  unsigned long long* const sync = P.sync + ((split && edgeChain) ? 1 : 0);
   bool started = false;
   auto barrier = [&](long long count) {
     if (count == 0) return false;
-    if (started) grid_barrier(P.sync, gridDim.x, P.timeout);
+    if (started) grid_barrier(sync, unsigned(nb), P.timeout);
     started = true;
     return true;
   };
-  if (barrier(G.nGhost + G.nFilter))
-    for (int v = gtid; v < G.nGhost + G.nFilter; v += nthr) adj_ghost_consume_item(G, A, P.ipbar, P, v);
-  if (barrier(P.ncell))
-    for (int v = gtid; v < P.ncell; v += nthr) adj_ghost_gather_item(G, A, P.ipbar, P, v);
-  if (barrier(P.nfs))
-    for (int v = gtid; v < P.nfs; v += nthr) adj_filter_item(A, P.fsNodes, P.fsSlots, v);
+  if (bodyChain) {
+    if (barrier(G.nGhost + G.nFilter))
+      for (int v = gtid; v < G.nGhost + G.nFilter; v += nthr) adj_ghost_consume_item(G, A, P.ipbar, P, v);
+    if (barrier(P.ncell))
+      for (int v = gtid; v < P.ncell; v += nthr) adj_ghost_gather_item(G, A, P.ipbar, P, v);
+    if (barrier(P.nfs))
+      for (int v = gtid; v < P.nfs; v += nthr) adj_filter_item(A, P.fsNodes, P.fsSlots, v);
+  }
+  if (!edgeChain) return;
   const double stageT = P.roles->stageT[s];
   for (int axis = 2; axis >= 0; --axis)  // z, y, then x
     if (barrier(P.nEdge[axis]))
@@ -620,11 +632,22 @@ void launch_adj_bc(const Grid& hg, const AdjBcParams& P, int s, int nSM, void* s
     int nb = 0;
     perSM = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_adj_bc, kAdjBcThreads, 0) == cudaSuccess ? nb : 0;
   }
-  // enough blocks for the largest phase, all resident (cooperative launch)
-  long long items = std::max<long long>(hg.nGhost + hg.nFilter, 64ll * std::max(P.nEdge[0], std::max(P.nEdge[1], P.nEdge[2])));
-  items = std::max<long long>(items, std::max(P.ncell, P.nfs));
-  const long long want = std::max<long long>(1, (items + kAdjBcThreads - 1) / kAdjBcThreads);
+  // enough blocks for the largest phase (of each chain when split), all resident (cooperative launch)
+  auto blocks_of = [](long long items) { return std::max<long long>(1, (items + kAdjBcThreads - 1) / kAdjBcThreads); };
+  const long long bodyItems = std::max<long long>(hg.nGhost + hg.nFilter, std::max(P.ncell, P.nfs));
+  const long long edgeItems = 64ll * std::max(P.nEdge[0], std::max(P.nEdge[1], P.nEdge[2]));
   const long long cap = (long long)(perSM > 0 ? perSM : 1) * nSM;
+  AdjBcParams Q = P;
+  long long want = blocks_of(std::max(bodyItems, edgeItems));
+  if (P.bodyBlocks > 0) {  // two chains: blocks for each (the request is a flag; the size is set here)
+    const long long nbB = blocks_of(bodyItems), nbE = blocks_of(edgeItems);
+    if (nbB + nbE <= cap) {
+      Q.bodyBlocks = int(nbB);
+      want = nbB + nbE;
+    } else {
+      Q.bodyBlocks = 0;
+    }
+  }
   const unsigned blocks = unsigned(want < cap ? want : cap);
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(blocks);
@@ -635,7 +658,7 @@ void launch_adj_bc(const Grid& hg, const AdjBcParams& P, int s, int nSM, void* s
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_adj_bc, hg, P, s);
+  cudaLaunchKernelEx(&cfg, k_adj_bc, hg, Q, s);
   k_adj_combine<<<blocks_for(hg.N, nSM), 256, 0, static_cast<cudaStream_t>(stream)>>>(hg, P, s);
 }
 

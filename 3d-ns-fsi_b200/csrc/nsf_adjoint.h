@@ -58,7 +58,10 @@ struct AdjBcParams {
   const double* objVal[5];
   const double* nx;
   double dA, weight;
-  unsigned long long* sync;  // grid-barrier arrival counter (zero at creation, only grows)
+  unsigned long long* sync;  // [2] grid-barrier arrival counters (zero at creation, only grow)
+  // non-zero: the bodies' nodes and the face planes are disjoint, so the body phases and the edge phases
+  // run as two independent chains (the launcher sets the blocks of the body chain)
+  int bodyBlocks;
   int* timeout;              // StepCtl::timeout of the solver: set when a barrier gives up
 };
 void launch_adj_bc(const Grid& hg, const AdjBcParams& P, int s, int nSM, void* stream);

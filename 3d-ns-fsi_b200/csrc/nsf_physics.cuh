@@ -177,7 +177,7 @@ __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long lon
 }
 __device__ inline void grid_barrier(unsigned long long* S, unsigned nb, int* timeout) {
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {  // one arrival per block, any block shape
     const unsigned long long old = atom_add_release(S, 1ull);
     const unsigned long long target = (old / nb + 1) * nb;
     long long it = 0;

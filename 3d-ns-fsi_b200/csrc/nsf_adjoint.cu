@@ -291,7 +291,9 @@ __device__ __forceinline__ void adj_inlet_gather_item(const Grid& G, const EdgeB
 // Values: momenta and rho_E from I, density from R, filter nodes' density and rho_E from fpre (for the
 // primitives), then the primitives and transport properties, as the stage kernel stages them.
 // With periodic z faces (Grid::zFused) the stage kernel also wrote the z copies of the nodes at k = 1 and
-// k = NK-2 it computed: their adjoints are gathered here, before the combine's.
+// k = NK-2 it computed, with periodic y faces (Grid::yFused) the y copies of those at j = 1 and j = NJ-2:
+// their adjoints are gathered here, before the combine's (edge blocks left with only such nodes are not
+// listed, so the edge phase has not consumed them).
 // Solid nodes (ghost and inactive): the adjoint of k_solid_copy, which copied the stage input into the
 // output of the fields in solidMask (bit 0: the density from R) before the edge conditions.
 __device__ __forceinline__ void adj_prepare_item(const Grid& G, const AdjPtrs& A, int s, double dtUsed, int solidMask,
@@ -302,16 +304,19 @@ __device__ __forceinline__ void adj_prepare_item(const Grid& G, const AdjPtrs& A
   const bool interior = (ty & TYPE_MASK) == FLUID_INTERIOR;
   const double m1 = A.val[1][n], m2 = A.val[2][n], m3 = A.val[3][n], e4 = A.val[4][n];
   double rho = A.valR[n], rE = e4;
-  double o[5], acc[5], u0[5], oz[5] = {0, 0, 0, 0, 0};
-  // the z copy the stage kernel wrote with this node
+  double o[5], acc[5], u0[5], oz[5] = {0, 0, 0, 0, 0}, oy[5] = {0, 0, 0, 0, 0};
+  // the z and y copies the stage kernel wrote with this node
   const bool zCopy = (ty & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT)) != 0;
   const long long nz = (ty & ZCOPY_UP_BIT) ? n + (G.NK - 2) : n - (G.NK - 2);
+  const bool yCopy = (ty & YCOPY_BIT) != 0;
+  const long long ny = (n % G.sI) / G.sJ == 1 ? n + (G.NJ - 2) * G.sJ : n - (G.NJ - 2) * G.sJ;
   if (interior)
     for (int f = 0; f < 5; ++f) {
       o[f] = A.lamO[f][n];
       acc[f] = A.lamAcc[f][n];
       u0[f] = A.lamU0[f][n];
       if (zCopy) oz[f] = A.lamO[f][nz];
+      if (yCopy) oy[f] = A.lamO[f][ny];
     }
   if (ty & FILTER_BIT) {
     const int f = G.fidx[n];
@@ -347,6 +352,11 @@ __device__ __forceinline__ void adj_prepare_item(const Grid& G, const AdjPtrs& A
     for (int f = 0; f < 5; ++f) {
       o[f] += oz[f];
       A.lamO[f][nz] = 0.0;
+    }
+  if (yCopy)
+    for (int f = 0; f < 5; ++f) {
+      o[f] += oy[f];
+      A.lamO[f][ny] = 0.0;
     }
   for (int f = 0; f < 5; ++f) {
     double k;

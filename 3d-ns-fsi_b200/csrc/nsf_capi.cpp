@@ -245,6 +245,20 @@ nsf_status build_device(nsf_solver* s) {
     fpre[2 * q] = cons[fnode[q]];
     fpre[2 * q + 1] = cons[4 * N + fnode[q]];
   }
+  {  // periodic y faces: the nodes whose periodic copies the stage kernel writes. The edge conditions run
+     // x, y, z: every reader of a y-face node (later y rows, the z faces, the bodies) wants the value after
+     // the y copy, and the copy's source, an unfiltered interior node, is final after the stage kernel.
+    int yPer = 0;
+    for (const auto& e : S.edges) yPer += e.axis == 1 && e.bc == NSF_BC_PERIODIC;
+    G.yFused = yPer == 2 && S.NJ >= 4;
+    if (G.yFused)
+      for (size_t i = 1; i + 1 < S.NI; ++i)
+        for (size_t js : {size_t(1), S.NJ - 2})
+          for (size_t k = 1; k + 1 < S.NK; ++k) {
+            uint8_t& t = type[(i * S.NJ + js) * S.NK + k];
+            if ((t & TYPE_MASK) == FLUID_INTERIOR && !(t & FILTER_BIT)) t |= YCOPY_BIT;
+          }
+  }
   {  // periodic z faces: the nodes whose periodic copies the stage kernel writes
     int zPer = 0;
     for (const auto& e : S.edges) zPer += e.axis == 2 && e.bc == NSF_BC_PERIODIC;

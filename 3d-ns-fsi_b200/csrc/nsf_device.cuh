@@ -120,6 +120,7 @@ struct Grid {
   // computes at k = 1 and k = NK-2 into k = NK-1 and k = 0 (same values, same sectors), and the z edge
   // kernel handles only the rows the stage kernel does not (see edge_blocks).
   int zFused;
+  int yFused;  // periodic y faces: the stage kernel writes the copies of its YCOPY_BIT nodes
   // gradient support (NULL / 0 for a plain run): an x-inlet velocity profile factor per (j, k) node of the
   // inlet plane, and a prescribed dt per step (the adjoint differentiates with the dt sequence frozen)
   const double* inflow;     // [NJ * NKp], index j * NKp + k

@@ -23,6 +23,9 @@ constexpr uint8_t EDGE_PLANE_BIT = 0x40;  // node lies in a mesh-edge boundary's
 // k = NK-2 (DOWN), whose value the stage kernel also writes to its periodic copy at k = NK-1 or k = 0.
 constexpr uint8_t ZCOPY_UP_BIT = 0x20;
 constexpr uint8_t ZCOPY_DOWN_BIT = 0x10;
+// Periodic y faces (Grid::yFused): an unfiltered interior fluid node at j = 1 or j = NJ-2 (the row tells
+// which), whose value the stage kernel also writes to its periodic copy at j = NJ-1 or j = 0.
+constexpr uint8_t YCOPY_BIT = 0x08;
 constexpr int FMETA_LAST = 1 << 30;  // Grid::fmeta: this slot is its node's last
 // Edge condition of an x-slab's periodic x face (nsf_slab.cpp): the plane exchange has already copied the
 // face's values; the edge item only adds the nodes' stage-4 dt terms, as the whole grid's periodic face does.

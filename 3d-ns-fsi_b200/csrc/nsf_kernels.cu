@@ -796,21 +796,26 @@ int bc_capacity(int nSM) {
 
 void edge_blocks(const Grid& G, const uint8_t* type, int g, int axis, std::vector<EdgeBlock>& out) {
   const int ax1 = axis == 0 ? 1 : 0, ax2 = axis == 2 ? 1 : 2;
-  const bool fused = axis == 2 && G.zFused && type;
+  // periodic faces whose copies the stage kernel writes: those nodes leave the blocks (z: (a, bb) = (i, j),
+  // y: (a, bb) = (i, k))
+  const bool fused = type && ((axis == 2 && G.zFused) || (axis == 1 && G.yFused));
   for (int e = 0; e < G.nEdge; ++e) {
     if (G.eAxis[e] != axis) continue;
     const int* b = G.eBox[e];
     const int ks = G.eSide[e] == 0 ? G.NK - 2 : 1;  // the periodic source plane
+    const int js = G.eSide[e] == 0 ? G.NJ - 2 : 1;
     for (int a0 = b[2 * ax1]; a0 <= b[2 * ax1 + 1]; a0 += kEdgeRows)
       for (int b0 = b[2 * ax2]; b0 <= b[2 * ax2 + 1]; b0 += 32) {
         unsigned long long mask = ~0ull;
-        if (fused) {  // (a, bb) = (i, j)
+        if (fused && G.eBc[e] == NSF_BC_PERIODIC) {
           mask = 0;
           for (int ty = 0; ty < kEdgeRows; ++ty)
             for (int tx = 0; tx < 32; ++tx) {
-              const int i = a0 + ty, j = b0 + tx;
-              if (i > b[1] || j > b[3]) continue;
-              const bool copiedByStage = type[(size_t(i) * G.NJ + j) * G.NK + ks] & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT);
+              const int a = a0 + ty, bb = b0 + tx;
+              if (a > b[2 * ax1 + 1] || bb > b[2 * ax2 + 1]) continue;
+              const bool copiedByStage =
+                  axis == 2 ? (type[(size_t(a) * G.NJ + bb) * G.NK + ks] & (ZCOPY_UP_BIT | ZCOPY_DOWN_BIT)) != 0
+                            : (type[(size_t(a) * G.NJ + js) * G.NK + bb] & YCOPY_BIT) != 0;
               if (!copiedByStage) mask |= 1ull << (ty * 32 + tx);
             }
           if (!mask) continue;

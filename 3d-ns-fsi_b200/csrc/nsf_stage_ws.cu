@@ -624,6 +624,16 @@ __global__ void __launch_bounds__(ws::Tile<TK_, TJ_>::NTHREADS, 1)
             out3[m] = res[3];
             out4[m] = res[4];
           }
+          if (tc & YCOPY_BIT) {
+            // periodic y faces likewise: j = 1 feeds j = NJ-1, j = NJ-2 feeds j = 0 (a row of the tile's
+            // neighbour across the grid; the whole warp's row when the tile spans k)
+            const long long m = j == 1 ? nR + (long long)(G.NJ - 2) * G.sJ : nR - (long long)(G.NJ - 2) * G.sJ;
+            out0[m] = res[0];
+            out1[m] = res[1];
+            out2[m] = res[2];
+            out3[m] = res[3];
+            out4[m] = res[4];
+          }
         }
         __syncwarp();
         if (lane == 0) {

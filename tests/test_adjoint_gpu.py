@@ -197,3 +197,25 @@ def test_adjoint_all_periodic_box():
         for du, _ in seeded_directions(s, u0, 4, seed=9)[:3]:
             ad, fd, terms = fd_check(s, u0, gi, gu, du, None, h)
             assert abs(fd - ad) <= 1e-7 * max(abs(ad), terms) + floor, (ad, fd, terms)
+
+
+@pytest.mark.gpu
+def test_adjoint_body_near_the_inlet():
+    """The sphere of adj32 moved next to the inlet: its filter and ghost nodes reach the planes the inlet's
+    adjoint reads, so the adjoint boundary kernel runs its body and edge phases as one chain and the inlet
+    planes come from the stage snapshots. 10 steps, J over the last 4: the gradient matches the central
+    difference at h = 1e-5 to 1e-8."""
+    h = 1e-5
+    text = open(nsfsi.case_path("adj32")).read().replace("spheres = ( (0.4, 0.5, 0.5, 0.1) );",
+                                                          "spheres = ( (0.21, 0.5, 0.5, 0.1) );")
+    c = nsfsi.config_parse(text)
+    c.stop_time_level = 10
+    with nsfsi.Solver(c) as s:
+        u0 = s.download(range(5))
+        s.adj_configure(4, 3)
+        J = s.adj_forward()
+        gi, gu = s.adj_backward()
+        floor = 16 * np.finfo(float).eps * abs(J) / h
+        for du, di in seeded_directions(s, u0, 4, seed=11):
+            ad, fd, terms = fd_check(s, u0, gi, gu, du, di, h)
+            assert abs(fd - ad) <= 1e-8 * max(abs(ad), terms) + floor, (ad, fd, terms, floor)

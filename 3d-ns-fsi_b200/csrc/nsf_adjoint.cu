@@ -512,9 +512,16 @@ __global__ void __launch_bounds__(32 * RT_J, kAdjRhsBlocks)
       const int c = (ty + 1) * RT_HK + tx + 1;
       const long long m = i * sI + j * sJ + k;
       auto lamAt = [&](int e, int di, int dj, int dk) { return sm[sb[di + 1] + e * RT_PLANE + c + dj * RT_HK + dk]; };
+      // the inputs read at X only (momenta, rho_E, p) and the node's type: loaded before the gather, so
+      // their latency overlaps it
+      const double xv[5] = {V[m], V[N + m], V[2 * N + m], V[3 * N + m], V[7 * N + m]};
+      const uint8_t tym = G.type[m];
+      const bool filt = (tym & FILTER_BIT) != 0;
+      const int fi = filt ? G.fidx[m] : 0;
+      const double rho = filt ? A.valFpre[2 * fi] : A.valR[m];
       auto valAt = [&](int q, int di, int dj, int dk) {
         const int f = rt_field(q);
-        return f >= 0 ? sm[sb[di + 1] + f * RT_PLANE + c + dj * RT_HK + dk] : V[q * N + m];  // others at X only
+        return f >= 0 ? sm[sb[di + 1] + f * RT_PLANE + c + dj * RT_HK + dk] : xv[q == 7 ? 4 : q];
       };
       // the per-RHS-node conditions also bound the compiler's scheduling regions (without them it
       // interleaves all 19 blocks and runs out of registers)
@@ -527,9 +534,6 @@ __global__ void __launch_bounds__(32 * RT_J, kAdjRhsBlocks)
       // chain rule: u = m r1, p = gm1 (rE - (rho+1) K), T = (gamma p - rho) r1, mu = x sqrt(x) sc1/(re (T+sc1)),
       // kappa = mu pf, with r1 = 1/(rho+1), K = |u|^2/2, x = 1 + T
       // the density of the primitives: the stage's density input, or the pre-filter copy at filter nodes
-      const bool filt = (G.type[m] & FILTER_BIT) != 0;
-      const int fi = filt ? G.fidx[m] : 0;
-      const double rho = filt ? A.valFpre[2 * fi] : A.valR[m];
       const double r1 = recip_nr(rho + 1.0);
       const int cc = sb[1] + c;  // this node in the staged plane
       const double u = sm[cc + 5 * RT_PLANE], v = sm[cc + 6 * RT_PLANE], w = sm[cc + 7 * RT_PLANE],

@@ -519,6 +519,11 @@ __global__ void __launch_bounds__(32 * RT_J, kAdjRhsBlocks)
       const bool filt = (tym & FILTER_BIT) != 0;
       const int fi = filt ? G.fidx[m] : 0;
       const double rho = filt ? A.valFpre[2 * fi] : A.valR[m];
+      // the adjoints this node adds into (only this thread writes them in this kernel)
+      double* const dR = filt ? A.lamFpre + 2 * fi : A.lamR + m;      // density's
+      double* const dE = filt ? A.lamFpre + 2 * fi + 1 : nullptr;     // rho_E's, filter nodes
+      const double aI1 = A.lamI[1][m], aI2 = A.lamI[2][m], aI3 = A.lamI[3][m], aI4 = A.lamI[4][m];
+      const double aR = *dR, aE = filt ? *dE : 0.0;
       auto valAt = [&](int q, int di, int dj, int dk) {
         const int f = rt_field(q);
         return f >= 0 ? sm[sb[di + 1] + f * RT_PLANE + c + dj * RT_HK + dk] : xv[q == 7 ? 4 : q];
@@ -552,16 +557,15 @@ __global__ void __launch_bounds__(32 * RT_J, kAdjRhsBlocks)
       vb += Kb * v;
       wb += Kb * w;
       rhob += -(u * ub + v * vb + w * wb) * r1;
-      A.lamI[1][m] += bar[0] + r1 * ub;
-      A.lamI[2][m] += bar[1] + r1 * vb;
-      A.lamI[3][m] += bar[2] + r1 * wb;
-      A.lamI[4][m] += bar[3];
+      A.lamI[1][m] = aI1 + (bar[0] + r1 * ub);
+      A.lamI[2][m] = aI2 + (bar[1] + r1 * vb);
+      A.lamI[3][m] = aI3 + (bar[2] + r1 * wb);
+      *dR = aR + rhob;
       if (filt) {
-        A.lamFpre[2 * fi] += rhob;
-        A.lamFpre[2 * fi + 1] += rEb;
+        A.lamI[4][m] = aI4 + bar[3];
+        *dE = aE + rEb;
       } else {
-        A.lamR[m] += rhob;
-        A.lamI[4][m] += rEb;
+        A.lamI[4][m] = (aI4 + bar[3]) + rEb;
       }
     }
     __syncthreads();  // the next iteration restages the oldest slot

@@ -331,7 +331,7 @@ __device__ __forceinline__ void adj_prepare_item(const Grid& G, const AdjPtrs& A
   }
   const Prim pr = prims_of_nr(G.C, rho, m1, m2, m3, rE);  // as the stage kernel's staging warps
   const double q[11] = {m1, m2, m3, e4, pr.u, pr.v, pr.w, pr.p, pr.T, pr.mu, pr.ka};
-  for (int v = 0; v < 11; ++v) V[v * G.N + n] = q[v];
+  for (int v = 4; v < 11; ++v) V[v * G.N + n] = q[v];  // 0..3 are the stage input's own values (A.val)
   if (!interior) {
     for (int f = 0; f < 5; ++f) lam[f * G.N + n] = 0.0;
     const uint8_t t = ty & TYPE_MASK;
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(32 * RT_J, kAdjRhsBlocks)
       auto lamAt = [&](int e, int di, int dj, int dk) { return sm[sb[di + 1] + e * RT_PLANE + c + dj * RT_HK + dk]; };
       // the inputs read at X only (momenta, rho_E, p) and the node's type: loaded before the gather, so
       // their latency overlaps it
-      const double xv[5] = {V[m], V[N + m], V[2 * N + m], V[3 * N + m], V[7 * N + m]};
+      const double xv[5] = {A.val[1][m], A.val[2][m], A.val[3][m], A.val[4][m], V[7 * N + m]};
       const uint8_t tym = G.type[m];
       const bool filt = (tym & FILTER_BIT) != 0;
       const int fi = filt ? G.fidx[m] : 0;

@@ -49,7 +49,8 @@ struct AdjBcParams {
   double* fbar;
   double* lamInflow;
   const StepCtl* roles;  // device copy of the step's control block (stage times, dt)
-  // combine: the stage's copy mask, RHS adjoint lam (5 x N) and input quantities V (11 x N)
+  // combine: the stage's copy mask, RHS adjoint lam (5 x N) and input quantities V (11 x N; rows 4-10, the
+  // primitives and transport values -- rows 0-3 would repeat the stage input's own values)
   int solidMask;
   double* lam;
   double* V;

@@ -168,3 +168,14 @@ def test_two_gloo_ranks_follow_the_slab_schedule(nslabs):
             for (m1, s1), (m2, s2) in zip(terms, ref_terms):
                 assert m1 == m2 and abs(s1 - s2) <= 1e-12 * s2
     assert np.array_equal(got, ref)
+
+
+def test_multi_process_group_checks_its_arguments_before_any_device_work():
+    cfg = nsfsi.config_load(nsfsi.case_path("tgv256"))
+    for rank, world in ((0, 5), (2, 2), (-1, 2)):  # more processes than slabs, rank outside the group
+        with pytest.raises(nsfsi.NsfError) as e:
+            nsfsi.SlabGroup(cfg, 4, 0, rank=rank, world=world, nccl_id=bytes(nsfsi.NCCL_ID_BYTES))
+        assert e.value.code == 6  # NSF_ERR_ARG
+    with pytest.raises(nsfsi.NsfError) as e:  # immersed bodies stay refused across processes too
+        nsfsi.SlabGroup(nsfsi.case_path("sphere48"), 2, 0, rank=0, world=2, nccl_id=bytes(nsfsi.NCCL_ID_BYTES))
+    assert e.value.code == 6

@@ -75,7 +75,7 @@ def build(verbose=False, ptxas_info=False):
     if _stale(MAIN, deps):
         os.makedirs(os.path.dirname(MAIN), exist_ok=True)
         _run(["g++", "-std=c++17", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(PKG, "host"),
-              main_src, "-o", MAIN, "-L" + LIB_DIR, "-lnsfsi", "-Wl,-rpath,$ORIGIN/../lib"])
+              main_src, "-o", MAIN, "-L" + LIB_DIR, "-lnsfsi", "-Wl,-rpath,$ORIGIN/../lib", "-pthread"])
     return LIB
 
 

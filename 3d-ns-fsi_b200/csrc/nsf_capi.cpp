@@ -657,6 +657,20 @@ nsf_status build_device(nsf_solver* s) {
   return NSF_OK;
 }
 
+// Slots of the asked-for fields in a packed download (increasing field order), and how many there are.
+SnapSlots snap_slots(uint32_t mask, int* count) {
+  SnapSlots sl;
+  int q = 0;
+  for (int f = 0; f < NSF_SNAP_FIELDS; ++f) sl.slot[f] = (mask >> f) & 1u ? q++ : -1;
+  *count = q;
+  return sl;
+}
+
+SnapInactive snap_inactive(const nsf_solver* s) {
+  return SnapInactive{s->dDlNode, s->dDlPrim, s->nDl, s->dDlNodeIc, s->dDlPrimIc, s->nDlIc};
+}
+
+
 }  // namespace
 
 // For the x-slab groups (nsf_slab.cpp): device set-up of a handle whose host setup is already in place,
@@ -784,33 +798,117 @@ nsf_status nsf_get_time(nsf_solver* s, double* t, uint64_t* level, double* dt) {
   return NSF_OK;
 }
 
+
 nsf_status nsf_download(nsf_solver* s, uint32_t mask, double* host) {
   if (!s || !host) return NSF_ERR_ARG;
   if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
-  CK(cudaStreamSynchronize(s->stream));
-  StepCtl ctl;
-  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
-  const HostSetup& S = s->setup;
-  const size_t N = S.N, NKp = size_t(s->hGrid.NKp), Nd = size_t(s->hGrid.N);
-  const size_t hp = S.NK * sizeof(double), dp = NKp * sizeof(double), rows = S.NI * S.NJ;
-  size_t outF = 0;
-  for (int f = 0; f < 5; ++f)
-    if (mask & (1u << f))
-      CK(cudaMemcpy2D(host + (outF++) * N, hp, s->hGrid.bufs[ctl.perm[f][0]][f], dp, hp, rows, cudaMemcpyDeviceToHost));
-  if (mask & 0xFE0u) {
-    double* tmp = nullptr;
-    CK(cudaMalloc(&tmp, 7 * Nd * sizeof(double)));
-    if (ctl.level == 0)
-      launch_download_prims(s->dGrid, (long long)Nd, tmp, s->dDlNodeIc, s->dDlPrimIc, s->nDlIc, s->nSM, s->stream);
-    else
-      launch_download_prims(s->dGrid, (long long)Nd, tmp, s->dDlNode, s->dDlPrim, s->nDl, s->nSM, s->stream);
-    cudaError_t e = cudaStreamSynchronize(s->stream);
-    for (int f = 5; f < 12 && e == cudaSuccess; ++f)
-      if (mask & (1u << f))
-        e = cudaMemcpy2D(host + (outF++) * N, hp, tmp + (f - 5) * Nd, dp, hp, rows, cudaMemcpyDeviceToHost);
-    cudaFree(tmp);
-    if (e != cudaSuccess) return cuda_fail(s, e, "download primitive fields");
+  int nf = 0;
+  const SnapSlots sl = snap_slots(mask, &nf);
+  if (!nf) return NSF_OK;
+  CK(cudaSetDevice(s->device));
+  const size_t bytes = size_t(nf) * s->setup.N * sizeof(double);
+  double* tmp = nullptr;
+  CK(cudaMalloc(&tmp, bytes));
+  launch_snapshot(s->dGrid, sl, snap_inactive(s), tmp, s->nSM, s->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(s, e, "download");
+  return NSF_OK;
+}
+
+nsf_status nsf_download_async(nsf_solver* s, uint32_t mask, double* host, uint64_t* ticket) {
+  if (!s || !host || !ticket) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  if (s->grouped) {
+    s->err = "nsf_download_async: the handle is a member of an ensemble or slab group (use nsf_download)";
+    return NSF_ERR_STATE;
   }
+  int nf = 0;
+  const SnapSlots sl = snap_slots(mask, &nf);
+  if (!nf) {
+    s->err = "nsf_download_async: the field mask selects no field";
+    return NSF_ERR_ARG;
+  }
+  CK(cudaSetDevice(s->device));
+  cudaPointerAttributes pa{};
+  if (cudaPointerGetAttributes(&pa, host) != cudaSuccess || pa.type != cudaMemoryTypeHost) {
+    cudaGetLastError();
+    s->err = "nsf_download_async: the host buffer is not page-locked (nsf_host_alloc)";
+    return NSF_ERR_ARG;
+  }
+  if (!s->dlStream) {
+    CK(cudaStreamCreateWithFlags(&s->dlStream, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      CK(cudaEventCreateWithFlags(&s->dlTaken[b], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&s->dlDone[b], cudaEventDisableTiming));
+    }
+  }
+  const uint64_t t = s->dlIssued.load() + 1;
+  const int b = int(t & 1u);
+  const size_t count = size_t(nf) * s->setup.N;
+  if (s->dlCap[b] < count) {
+    CK(cudaEventSynchronize(s->dlDone[b]));  // the buffer's last copy to the host has finished
+    if (s->dlStage[b]) CK(cudaFree(s->dlStage[b]));
+    s->dlStage[b] = nullptr;
+    s->dlCap[b] = 0;
+    CK(cudaMalloc(&s->dlStage[b], count * sizeof(double)));
+    s->dlCap[b] = count;
+  }
+  // the snapshot overwrites the buffer only after its previous copy to the host has left it
+  CK(cudaStreamWaitEvent(s->stream, s->dlDone[b], 0));
+  launch_snapshot(s->dGrid, sl, snap_inactive(s), s->dlStage[b], s->nSM, s->stream);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(s->dlTaken[b], s->stream));
+  CK(cudaStreamWaitEvent(s->dlStream, s->dlTaken[b], 0));
+  CK(cudaMemcpyAsync(host, s->dlStage[b], count * sizeof(double), cudaMemcpyDeviceToHost, s->dlStream));
+  CK(cudaEventRecord(s->dlDone[b], s->dlStream));
+  s->dlIssued.store(t);
+  *ticket = t;
+  return NSF_OK;
+}
+
+// Ticket t's copy is done once buffer (t & 1)'s done event has completed: that event marks t's copy or, if
+// the buffer was reused since, a later copy that started after t's had finished.
+nsf_status nsf_download_wait(nsf_solver* s, uint64_t ticket) {
+  if (!s) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  if (ticket == 0 || ticket > s->dlIssued.load()) return NSF_ERR_ARG;
+  if (cudaSetDevice(s->device) != cudaSuccess || cudaEventSynchronize(s->dlDone[ticket & 1u]) != cudaSuccess)
+    return NSF_ERR_CUDA;
+  return NSF_OK;
+}
+
+nsf_status nsf_download_done(nsf_solver* s, uint64_t ticket, int32_t* done) {
+  if (!s || !done) return NSF_ERR_ARG;
+  if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
+  if (ticket == 0 || ticket > s->dlIssued.load()) return NSF_ERR_ARG;
+  if (cudaSetDevice(s->device) != cudaSuccess) return NSF_ERR_CUDA;
+  const cudaError_t e = cudaEventQuery(s->dlDone[ticket & 1u]);
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return NSF_OK;
+  }
+  if (e != cudaSuccess) return NSF_ERR_CUDA;
+  *done = 1;
+  return NSF_OK;
+}
+
+nsf_status nsf_host_alloc(size_t bytes, void** out) {
+  if (!out) return NSF_ERR_ARG;
+  *out = nullptr;
+  if (!bytes) return NSF_ERR_ARG;
+  if (cudaHostAlloc(out, bytes, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return NSF_ERR_CUDA;
+  }
+  return NSF_OK;
+}
+
+nsf_status nsf_host_free(void* p) {
+  if (p && cudaFreeHost(p) != cudaSuccess) return NSF_ERR_CUDA;
   return NSF_OK;
 }
 
@@ -993,6 +1091,15 @@ void nsf_destroy(nsf_solver* s) {
   for (cudaEvent_t e : s->profEv)
     if (e) cudaEventDestroy(e);
   nsf_adjoint_free(s);
+  if (s->dlStream) {
+    cudaStreamSynchronize(s->dlStream);
+    for (int b = 0; b < 2; ++b) {
+      if (s->dlStage[b]) cudaFree(s->dlStage[b]);
+      if (s->dlTaken[b]) cudaEventDestroy(s->dlTaken[b]);
+      if (s->dlDone[b]) cudaEventDestroy(s->dlDone[b]);
+    }
+    cudaStreamDestroy(s->dlStream);
+  }
   for (void* p : s->allocs) cudaFree(p);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;

@@ -295,8 +295,24 @@ std::vector<int> bc_block_ranges(const BcFlat& fl, int capacity);
 void periodic_source_host(const Grid& G, int axis, int side, int ijk[3]);
 void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, const uint8_t* flags, const double* ipl,
                           double dx, double dy, double dz, double* w, void* stream);
-void launch_download_prims(const Grid* dg, long long N, double* out, const long long* inodes, const double* ip7,
-                           int nInactive, int nSM, void* stream);
+// Downloads (nsf_download, nsf_download_async): per field (rho, rho_u, rho_v, rho_w, rho_E, u, v, w, p, T, mu,
+// kappa) its slot in the packed snapshot, or -1 when it is not asked for.
+constexpr int NSF_SNAP_FIELDS = 12;
+struct SnapSlots {
+  int slot[NSF_SNAP_FIELDS];
+};
+// Solid inactive nodes with stored primitive values (device node index, 7 values each): the list for time
+// level 0 and the one for later levels.
+struct SnapInactive {
+  const long long* nodes;
+  const double* p7;
+  int count;
+  const long long* nodesIc;
+  const double* p7Ic;
+  int countIc;
+};
+// Queues the snapshot of the slots' fields into `out` (packed, NI*NJ*NK doubles per slot) on `stream`.
+void launch_snapshot(const Grid* dg, const SnapSlots& sl, const SnapInactive& in, double* out, int nSM, void* stream);
 
 }  // namespace nsf
 #endif

@@ -399,6 +399,7 @@ nsf_status create_ensemble(const nsf_config* cfgs, uint32_t n, int32_t device, c
   for (uint32_t m = 0; m < n; ++m) {
     nsf_solver* s = nullptr;
     nsf_status st = nsf_create(&cfgs[m], device, &s);
+    if (s) s->grouped = true;
     e->members.push_back(s);
     if (st != NSF_OK) {
       e->err = "ensemble member " + std::to_string(m) + ": " + (s ? s->err : std::string("nsf_create failed"));

@@ -611,41 +611,59 @@ __global__ void k_ghost_weights(int nGhost, const double* __restrict__ pts, cons
   }
 }
 
-// Primitive / transport fields as the reference holds them, for downloads: recomputed from the
-// conserved values, except filtered nodes (values before the last near-body filter) and solid inactive
-// nodes (never updated by the reference; stored).
-__global__ void k_download_prims(const Grid* __restrict__ gp, double* __restrict__ out) {
+// Snapshot of the fields a download asks for, packed in the reference's layout (k fastest, no row padding):
+// field f goes to out + slot[f] * NI*NJ*NK, or nowhere for slot -1. Conserved fields are the current
+// buffers; primitive / transport fields are recomputed from them as the reference holds them, except at
+// filtered nodes (values before the last near-body filter) and solid inactive nodes (never updated by the
+// reference; k_snapshot_inactive writes their stored values). The buffers are found through the control
+// block, so the kernel can be queued behind any number of steps without the host reading it.
+__global__ void k_snapshot(const Grid* __restrict__ gp, SnapSlots sl, double* __restrict__ out) {
   const Grid& G = *gp;
   const StepCtl* c = G.ctl;
   const Consts& C = G.C;
   const double* U[5];
   for (int f = 0; f < 5; ++f) U[f] = G.bufs[c->perm[f][0]][f];
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < G.N; n += (long long)gridDim.x * blockDim.x) {
-    double rho = U[0][n], rE = U[4][n];
-    const uint8_t t = G.type[n];
-    if (t & FILTER_BIT) {
-      const int f = G.fidx[n];
-      rho = G.fpre[2 * f];
-      rE = G.fpre[2 * f + 1];
+  bool prim = false;
+#pragma unroll
+  for (int f = 5; f < NSF_SNAP_FIELDS; ++f) prim |= sl.slot[f] >= 0;
+  const long long NK = G.NK, M = (long long)G.NI * G.NJ * NK;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < M; q += (long long)gridDim.x * blockDim.x) {
+    const long long n = (q / NK) * G.NKp + q % NK;
+    double v[5];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+      v[f] = U[f][n];
+      if (sl.slot[f] >= 0) out[sl.slot[f] * M + q] = v[f];
     }
-    const Prim q = prims_of(C, rho, U[1][n], U[2][n], U[3][n], rE);
-    out[0 * G.N + n] = q.u;
-    out[1 * G.N + n] = q.v;
-    out[2 * G.N + n] = q.w;
-    out[3 * G.N + n] = q.p;
-    out[4 * G.N + n] = q.T;
-    out[5 * G.N + n] = q.mu;
-    out[6 * G.N + n] = q.ka;
+    if (!prim) continue;
+    if (G.type[n] & FILTER_BIT) {
+      const int f = G.fidx[n];
+      v[0] = G.fpre[2 * f];
+      v[4] = G.fpre[2 * f + 1];
+    }
+    const Prim p = prims_of(C, v[0], v[1], v[2], v[3], v[4]);
+    const double pv[7] = {p.u, p.v, p.w, p.p, p.T, p.mu, p.ka};
+#pragma unroll
+    for (int f = 0; f < 7; ++f)
+      if (sl.slot[5 + f] >= 0) out[sl.slot[5 + f] * M + q] = pv[f];
   }
 }
 
-// Solid inactive nodes: overwrite the recomputed download values with the stored ones.
-__global__ void k_download_inactive(const Grid* __restrict__ gp, const long long* __restrict__ nodes,
-                                    const double* __restrict__ p7, int count, double* __restrict__ out) {
+// Solid inactive nodes of a snapshot: their stored primitive values, from the list for the time level the
+// control block holds (level 0: each node's own initial values; later: the values after the first step).
+__global__ void k_snapshot_inactive(const Grid* __restrict__ gp, SnapSlots sl, SnapInactive in,
+                                    double* __restrict__ out) {
   const Grid& G = *gp;
+  const bool ic = G.ctl->level == 0;
+  const long long* nodes = ic ? in.nodesIc : in.nodes;
+  const double* p7 = ic ? in.p7Ic : in.p7;
+  const int count = ic ? in.countIc : in.count;
+  const long long NK = G.NK, M = (long long)G.NI * G.NJ * NK;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
-    const long long n = nodes[q];
-    for (int f = 0; f < 7; ++f) out[f * G.N + n] = p7[7 * (long long)q + f];
+    const long long n = nodes[q], cq = (n / G.NKp) * NK + n % G.NKp;
+#pragma unroll
+    for (int f = 0; f < 7; ++f)
+      if (sl.slot[5 + f] >= 0) out[sl.slot[5 + f] * M + cq] = p7[7 * (long long)q + f];
   }
 }
 
@@ -938,11 +956,13 @@ void launch_ghost_weights(int nGhost, const double* pts, const double* nrm, cons
   if (nGhost > 0) k_ghost_weights<<<(nGhost + 127) / 128, 128, 0, st>>>(nGhost, pts, nrm, flags, ipl, dx, dy, dz, w);
 }
 
-void launch_download_prims(const Grid* dg, long long N, double* out, const long long* inodes, const double* ip7,
-                           int nInactive, int nSM, void* stream) {
+void launch_snapshot(const Grid* dg, const SnapSlots& sl, const SnapInactive& in, double* out, int nSM, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_download_prims<<<nSM * 8, 256, 0, st>>>(dg, out);
-  if (nInactive > 0) k_download_inactive<<<(nInactive + 255) / 256, 256, 0, st>>>(dg, inodes, ip7, nInactive, out);
+  k_snapshot<<<nSM * 8, 256, 0, st>>>(dg, sl, out);
+  bool prim = false;
+  for (int f = 5; f < NSF_SNAP_FIELDS; ++f) prim |= sl.slot[f] >= 0;
+  const int most = in.count > in.countIc ? in.count : in.countIc;
+  if (prim && most > 0) k_snapshot_inactive<<<(most + 255) / 256, 256, 0, st>>>(dg, sl, in, out);
 }
 
 // The Newton-Raphson reciprocal and square root next to the IEEE ones, for a check of their error.

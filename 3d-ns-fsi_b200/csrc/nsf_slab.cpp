@@ -238,6 +238,7 @@ nsf_status build_group(nsf_slab_group* g, int P, const void* ncclId) {
       if (s) nsf_destroy(s);
       return gfail(g, st, "slab solver");
     }
+    s->grouped = true;
     g->slabs.push_back(s);
     slab_setup(g, p, s->setup, s->slabFlags);
     const size_t n = s->setup.NI, N = s->setup.N;

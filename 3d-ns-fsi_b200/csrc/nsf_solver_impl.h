@@ -5,6 +5,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -51,6 +52,17 @@ struct nsf_solver {
   nsf::BcMemberLevels bcLevels;  // dependency levels of the boundary work (fused boundary kernel)
   nsf::StepCtl ctlInit{};  // the control block at level 0 (the discrete adjoint restarts from it)
   struct AdjCtx* adj = nullptr;  // discrete-adjoint state (nsf_adjoint.cpp), created on first use
+  // member of an ensemble or x-slab group: its steps are queued on the group's stream, not on `stream`
+  bool grouped = false;
+  // asynchronous downloads (nsf_download_async): a copy stream and two device staging buffers used in turn,
+  // each with the events that mark its snapshot taken (on `stream`) and its copy to the host done (on
+  // dlStream); ticket t uses buffer t & 1
+  cudaStream_t dlStream = nullptr;
+  double* dlStage[2] = {nullptr, nullptr};
+  size_t dlCap[2] = {0, 0};  // doubles
+  cudaEvent_t dlTaken[2] = {nullptr, nullptr};
+  cudaEvent_t dlDone[2] = {nullptr, nullptr};
+  std::atomic<uint64_t> dlIssued{0};  // tickets handed out; read by nsf_download_wait from other threads
 };
 
 // Frees the adjoint state of a handle (nsf_adjoint.cpp).

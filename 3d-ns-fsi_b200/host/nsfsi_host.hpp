@@ -8,8 +8,9 @@
 //     simulation.run();
 //
 // compiles unchanged against this header (namespace nsfsi) and runs the time marching on a B200. The
-// flow fields stay resident on the device; Mesh holds host mirrors that are filled only when output
-// needs them (Mesh::syncFromDevice), which is where the reference's OutputManager reads them.
+// flow fields stay resident on the device. Snapshots download only the fields the settings save, into
+// page-locked buffers, while the march goes on; a worker thread writes each file once its fields have
+// landed (SnapshotWriter). Mesh keeps host mirrors for callers that read its arrays (Mesh::syncFromDevice).
 //
 // Header-only; link with 3d-ns-fsi_b200/lib/libnsfsi.so.
 #ifndef NSFSI_HOST_HPP
@@ -17,13 +18,20 @@
 
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
+#include <deque>
+#include <exception>
 #include <filesystem>
 #include <fstream>
+#include <functional>
 #include <iomanip>
 #include <iostream>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "nsfsi.h"
@@ -167,17 +175,37 @@ class Mesh {
 
   NodeTypeEnum nodeType(size_t i, size_t j, size_t k) const { return NodeTypeEnum(nodeTypes[i * NJ * NK + j * NK + k]); }
 
-  // Copy the current fields from the device (one synchronising download of all twelve fields).
-  void syncFromDevice() const {
-    std::vector<double> all(size_t(NSF_NUM_FIELDS) * nNodesTotal);
-    check(nsf_download(handle_, (1u << NSF_NUM_FIELDS) - 1, all.data()), handle_, "nsf_download");
+  // Copy the current fields (bit f of `fieldMask` = field f, NSF_RHO..NSF_KAPPA) from the device into
+  // the host mirrors, one synchronising download; the mirrors of fields not asked for are left as they are.
+  void syncFromDevice(uint32_t fieldMask = (1u << NSF_NUM_FIELDS) - 1) const {
+    fieldMask &= (1u << NSF_NUM_FIELDS) - 1;
+    size_t nf = 0;
+    for (int f = 0; f < NSF_NUM_FIELDS; ++f) nf += (fieldMask >> f) & 1u;
+    if (!nf) return;
+    std::vector<double> all(nf * nNodesTotal);
+    check(nsf_download(handle_, fieldMask, all.data()), handle_, "nsf_download");
     Array3D_d* dst[NSF_NUM_FIELDS] = {&conservedVariables.rho,  &conservedVariables.rho_u, &conservedVariables.rho_v,
                                       &conservedVariables.rho_w, &conservedVariables.rho_E, &primitiveVariables.u,
                                       &primitiveVariables.v,     &primitiveVariables.w,     &primitiveVariables.p,
                                       &primitiveVariables.T,     &transportProperties.mu,   &transportProperties.kappa};
+    size_t q = 0;
     for (int f = 0; f < NSF_NUM_FIELDS; ++f)
-      dst[f]->data.assign(all.begin() + f * nNodesTotal, all.begin() + (f + 1) * nNodesTotal);
+      if ((fieldMask >> f) & 1u) {
+        dst[f]->data.assign(all.begin() + q * nNodesTotal, all.begin() + (q + 1) * nNodesTotal);
+        ++q;
+      }
   }
+
+  // Host data of field f (NSF_RHO..NSF_KAPPA) in the mirrors, or nullptr if it was never downloaded.
+  const double* mirror(int f) const {
+    const Array3D_d* src[NSF_NUM_FIELDS] = {
+        &conservedVariables.rho, &conservedVariables.rho_u, &conservedVariables.rho_v, &conservedVariables.rho_w,
+        &conservedVariables.rho_E, &primitiveVariables.u, &primitiveVariables.v, &primitiveVariables.w,
+        &primitiveVariables.p, &primitiveVariables.T, &transportProperties.mu, &transportProperties.kappa};
+    return src[f]->data.size() == nNodesTotal ? src[f]->data.data() : nullptr;
+  }
+
+  nsf_solver* handle() const { return handle_; }
 
  private:
   friend class Solver;
@@ -265,6 +293,148 @@ class Solver {
   mutable ConservedVariablesVectorGroup history_;
 };
 
+// Snapshot writer behind OutputManager: each snapshot is downloaded with nsf_download_async into one of two
+// page-locked host buffers and written by a worker thread once it has landed, so the solver marches on while
+// the snapshot crosses to the host and is formatted. The main thread blocks only when both buffers are still
+// owned by snapshots that are in flight or being written.
+class SnapshotWriter {
+ public:
+  // Receives the downloaded fields: fields[f] holds field f (NSF_RHO..NSF_KAPPA) for every node, or is
+  // nullptr if f was not asked for.
+  using WriteFn = std::function<void(const double* const* fields)>;
+
+  SnapshotWriter() = default;
+  SnapshotWriter(const SnapshotWriter&) = delete;
+  SnapshotWriter& operator=(const SnapshotWriter&) = delete;
+  ~SnapshotWriter() {
+    try {
+      finish();
+    } catch (...) {
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    if (worker_.joinable()) worker_.join();
+    for (Buffer& b : bufs_)
+      if (b.host) nsf_host_free(b.host);
+  }
+
+  // Queue the fields in `fieldMask` of the solution `h` holds now (behind the steps already marched), to
+  // be passed to `write` once they are on the host. A mask of 0 calls `write` with no fields.
+  void submit(nsf_solver* h, uint32_t fieldMask, size_t nNodes, WriteFn write) {
+    fieldMask &= (1u << NSF_NUM_FIELDS) - 1;
+    Job job;
+    job.h = h;
+    job.write = std::move(write);
+    size_t nf = 0;
+    for (int f = 0; f < NSF_NUM_FIELDS; ++f) job.slot[f] = (fieldMask >> f) & 1u ? int(nf++) : -1;
+    job.nNodes = nNodes;
+    if (nf) {
+      std::unique_lock<std::mutex> lk(mu_);
+      const int b = next_;
+      next_ ^= 1;
+      cv_.wait(lk, [&] { return !bufs_[b].busy; });
+      rethrow_locked();
+      lk.unlock();
+      Buffer& buf = bufs_[b];
+      const size_t bytes = nf * nNodes * sizeof(double);
+      if (buf.bytes < bytes) {
+        if (buf.host) nsf_host_free(buf.host);
+        buf.host = nullptr;
+        buf.bytes = 0;
+        void* p = nullptr;
+        check(nsf_host_alloc(bytes, &p), nullptr, "nsf_host_alloc");
+        buf.host = static_cast<double*>(p);
+        buf.bytes = bytes;
+      }
+      check(nsf_download_async(h, fieldMask, buf.host, &job.ticket), h, "nsf_download_async");
+      job.buffer = b;
+      lk.lock();
+      buf.busy = true;
+    }
+    std::lock_guard<std::mutex> lk(mu_);
+    jobs_.push_back(std::move(job));
+    ++pending_;
+    if (!worker_.joinable()) worker_ = std::thread([this] { run(); });
+    cv_.notify_all();
+  }
+
+  // Wait until every queued snapshot is written; rethrows the first error of a download or a write.
+  void finish() {
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return pending_ == 0; });
+    rethrow_locked();
+  }
+
+ private:
+  struct Buffer {
+    double* host = nullptr;
+    size_t bytes = 0;
+    bool busy = false;
+  };
+  struct Job {
+    nsf_solver* h = nullptr;
+    uint64_t ticket = 0;  // 0: nothing downloaded
+    int buffer = -1;
+    int slot[NSF_NUM_FIELDS];
+    size_t nNodes = 0;
+    WriteFn write;
+  };
+
+  void rethrow_locked() {
+    if (error_) {
+      std::exception_ptr e = error_;
+      error_ = nullptr;
+      std::rethrow_exception(e);
+    }
+  }
+
+  void run() {
+    for (;;) {
+      Job job;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return stop_ || !jobs_.empty(); });
+        if (jobs_.empty()) return;
+        job = std::move(jobs_.front());
+        jobs_.pop_front();
+      }
+      std::exception_ptr err;
+      try {
+        const double* fields[NSF_NUM_FIELDS] = {};
+        if (job.ticket) {
+          const nsf_status st = nsf_download_wait(job.h, job.ticket);
+          if (st != NSF_OK) throw Error(st, std::string("nsf_download_wait: ") + status_name(st));
+          for (int f = 0; f < NSF_NUM_FIELDS; ++f)
+            if (job.slot[f] >= 0) fields[f] = bufs_[job.buffer].host + size_t(job.slot[f]) * job.nNodes;
+        }
+        job.write(fields);
+      } catch (...) {
+        err = std::current_exception();
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (err && !error_) error_ = err;
+        if (job.buffer >= 0) bufs_[job.buffer].busy = false;
+        --pending_;
+      }
+      cv_.notify_all();
+    }
+  }
+
+  Buffer bufs_[2];
+  int next_ = 0;
+  std::deque<Job> jobs_;
+  size_t pending_ = 0;
+  bool stop_ = false;
+  std::exception_ptr error_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::thread worker_;
+};
+
 // OutputManager (src/OutputManager.h:19-73): ASCII legacy VTK snapshots (i fastest), times.dat,
 // norm_*.dat and the status report, in the reference's formats. `dir` replaces the hard-coded ./output.
 class OutputManager {
@@ -312,13 +482,28 @@ class OutputManager {
   void processFinalOutput(const Mesh& mesh, double t, ulong timeLevel, double dt,
                           const ConservedVariablesVectorGroup& convergenceHistory) {  // :86-97
     if (params.saveFinal) storeCurrentSolution(mesh, t);
+    writer_.finish();
     writeStatusReport_toScreen(t, timeLevel, dt);
     writeOutputTimes();
     writeConvergenceHistoryFiles(convergenceHistory);
   }
 
-  // The VTK text of the current solution (storeCurrentSolution_vtk, :268-284), written to `os`.
+  // The VTK text of the current solution (storeCurrentSolution_vtk, :268-284) from the Mesh's host mirrors
+  // (Mesh::syncFromDevice), written to `os`.
   void writeVtk(const Mesh& mesh, double t, std::ostream& os) const {
+    const double* fields[NSF_NUM_FIELDS];
+    for (int f = 0; f < NSF_NUM_FIELDS; ++f) fields[f] = mesh.mirror(f);
+    writeVtkFields(mesh, t, fields, os);
+  }
+
+  // The same text from field arrays: fields[f] holds field f (NSF_RHO..NSF_KAPPA) for every node, k fastest;
+  // only the fields the settings save are read.
+  void writeVtkFields(const Mesh& mesh, double t, const double* const* fields, std::ostream& os) const {
+    const uint32_t need = savedFieldMask();
+    for (int f = 0; f < NSF_NUM_FIELDS; ++f)
+      if ((need >> f) & 1u && !fields[f])
+        throw std::logic_error("writeVtk: field " + std::to_string(f) + " is not on the host");
+    const size_t sj = mesh.NK, si = mesh.NJ * mesh.NK;
     os << "# vtk DataFile Version 5.1\n";
     os << "Output at time t = " + std::to_string(t) + "\n";
     os << "ASCII\n";
@@ -337,35 +522,52 @@ class OutputManager {
       for (size_t j = 0; j < mesh.NJ; ++j)
         for (size_t i = 0; i < mesh.NI; ++i) os << flag[int(mesh.nodeType(i, j, k))] << "\n";
     // Scalars (writeVtkScalarData, :196-211) and vectors (writeVtkVectorData, :246-263).
-    const Array3D_d* sc[6] = {&mesh.conservedVariables.rho,  &mesh.conservedVariables.rho_E,
-                              &mesh.primitiveVariables.p,     &mesh.primitiveVariables.T,
-                              &mesh.transportProperties.mu,   &mesh.transportProperties.kappa};
+    const int sc[6] = {NSF_RHO, NSF_RHO_E, NSF_P, NSF_T, NSF_MU, NSF_KAPPA};
     const bool scOn[6] = {params.saveDensity,     params.saveEnergy,    params.savePressure,
                           params.saveTemperature, params.saveViscosity, params.saveThermalCond};
     const char* scName[6] = {"Density",     "Total_Specific_Energy_per_Volume", "Pressure",
                              "Temperature", "Dynamic_Viscosity",                "Thermal_Conductivity"};
     for (int q = 0; q < 6; ++q) {
       if (!scOn[q]) continue;
+      const double* v = fields[sc[q]];
       os << "SCALARS " << scName[q] << " double 1\n";
       os << "LOOKUP_TABLE default\n";
       for (size_t k = 0; k < mesh.NK; ++k)
         for (size_t j = 0; j < mesh.NJ; ++j)
-          for (size_t i = 0; i < mesh.NI; ++i) os << sc[q]->at(i, j, k) << "\n";
+          for (size_t i = 0; i < mesh.NI; ++i) os << v[i * si + j * sj + k] << "\n";
     }
-    const Array3D_d* vec[2][3] = {
-        {&mesh.conservedVariables.rho_u, &mesh.conservedVariables.rho_v, &mesh.conservedVariables.rho_w},
-        {&mesh.primitiveVariables.u, &mesh.primitiveVariables.v, &mesh.primitiveVariables.w}};
+    const int vec[2] = {NSF_RHO_U, NSF_U};
     const bool vecOn[2] = {params.saveMomentum, params.saveVelocity};
     const char* vecName[2] = {"Momentum_Density", "Velocity"};
     for (int q = 0; q < 2; ++q) {
       if (!vecOn[q]) continue;
+      const double *x = fields[vec[q]], *y = fields[vec[q] + 1], *z = fields[vec[q] + 2];
       os << "VECTORS " << vecName[q] << " double\n";
       for (size_t k = 0; k < mesh.NK; ++k)
         for (size_t j = 0; j < mesh.NJ; ++j)
-          for (size_t i = 0; i < mesh.NI; ++i)
-            os << vec[q][0]->at(i, j, k) << " " << vec[q][1]->at(i, j, k) << " " << vec[q][2]->at(i, j, k) << "\n";
+          for (size_t i = 0; i < mesh.NI; ++i) {
+            const size_t n = i * si + j * sj + k;
+            os << x[n] << " " << y[n] << " " << z[n] << "\n";
+          }
     }
   }
+
+  // Fields a snapshot writes (bit f = NSF_RHO..NSF_KAPPA), from the save* settings.
+  uint32_t savedFieldMask() const {
+    uint32_t m = 0;
+    if (params.saveDensity) m |= 1u << NSF_RHO;
+    if (params.saveMomentum) m |= 7u << NSF_RHO_U;
+    if (params.saveEnergy) m |= 1u << NSF_RHO_E;
+    if (params.saveVelocity) m |= 7u << NSF_U;
+    if (params.savePressure) m |= 1u << NSF_P;
+    if (params.saveTemperature) m |= 1u << NSF_T;
+    if (params.saveViscosity) m |= 1u << NSF_MU;
+    if (params.saveThermalCond) m |= 1u << NSF_KAPPA;
+    return m;
+  }
+
+  // Wait until every snapshot queued so far is on disk (processFinalOutput does this).
+  void finishWrites() { writer_.finish(); }
 
   uint32_t savedSolutions = 0;
   std::vector<double> outputTimes;
@@ -375,17 +577,22 @@ class OutputManager {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - since).count();
   }
 
-  void storeCurrentSolution(const Mesh& mesh, double t) {  // :101-106
-    mesh.syncFromDevice();
+  // :101-106. The saved fields of the current solution are queued for download and the file is written by
+  // the snapshot writer once they have landed; `mesh` must outlive the write (finishWrites).
+  void storeCurrentSolution(const Mesh& mesh, double t) {
     const std::string filename = dir_ + "/out.vtk." + std::to_string(savedSolutions);
-    std::ofstream f(filename);
-    if (!f) {
+    auto f = std::make_shared<std::ofstream>(filename);
+    if (!*f) {
       std::cout << "Could not open file:  " + filename << std::endl << "Solution was not saved." << std::endl;
       return;
     }
-    writeVtk(mesh, t, f);
     ++savedSolutions;
     outputTimes.push_back(t);
+    const Mesh* m = &mesh;
+    writer_.submit(mesh.handle(), savedFieldMask(), mesh.nNodesTotal, [this, m, t, f](const double* const* fields) {
+      writeVtkFields(*m, t, fields, *f);
+      f->close();
+    });
   }
 
   void writeStatusReport_toScreen(double t, ulong timeLevel, double dt) {  // :289-311
@@ -438,6 +645,7 @@ class OutputManager {
   const ConfigSettings params;
   std::string dir_;
   std::chrono::steady_clock::time_point wallClock_ = std::chrono::steady_clock::now(), statusClock_ = wallClock_;
+  SnapshotWriter writer_;  // last: its pending writes finish before the members they read are destroyed
 };
 
 // Simulation (src/Simulation.h:18-35): initialise, march until the stopping criterion, write output.

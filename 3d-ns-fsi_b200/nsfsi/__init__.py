@@ -80,6 +80,11 @@ def lib():
         "nsf_sync": (i32, [vp]),
         "nsf_get_time": (i32, [vp, dp, ctypes.POINTER(u64), dp]),
         "nsf_download": (i32, [vp, u32, dp]),
+        "nsf_download_async": (i32, [vp, u32, dp, ctypes.POINTER(u64)]),
+        "nsf_download_wait": (i32, [vp, u64]),
+        "nsf_download_done": (i32, [vp, u64, ctypes.POINTER(i32)]),
+        "nsf_host_alloc": (i32, [ctypes.c_size_t, ctypes.POINTER(vp)]),
+        "nsf_host_free": (i32, [vp]),
         "nsf_upload_conserved": (i32, [vp, dp]),
         "nsf_get_node_types": (i32, [vp, ctypes.POINTER(ctypes.c_uint8)]),
         "nsf_get_geometry": (i32, [vp, dp]),
@@ -177,6 +182,47 @@ def math_selftest(x, device=0):
     return out.reshape(-1, 4).T
 
 
+class Snapshot:
+    """A download in flight (Solver.download_async): its page-locked host buffer and ticket. The buffer is
+    released after the copy has landed, so dropping a Snapshot early is safe."""
+
+    def __init__(self, solver, nfields):
+        self.solver, self.ticket, self.shape = solver, 0, (nfields, solver.N)
+        self.mem = ctypes.c_void_p()
+        st = lib().nsf_host_alloc(8 * nfields * solver.N, ctypes.byref(self.mem))
+        if st:
+            raise NsfError(st, "nsf_host_alloc of %d bytes failed" % (8 * nfields * solver.N))
+
+    def _ptr(self):
+        return ctypes.cast(self.mem, ctypes.POINTER(ctypes.c_double))
+
+    def done(self):
+        d = ctypes.c_int32()
+        self.solver._check(lib().nsf_download_done(self.solver.h, self.ticket, ctypes.byref(d)))
+        return bool(d.value)
+
+    def wait(self):
+        """Block until the snapshot has landed; returns a copy of it as a (fields, N) array."""
+        st = lib().nsf_download_wait(self.solver.h, self.ticket)
+        if st:
+            raise NsfError(st, "nsf_download_wait failed")
+        n = self.shape[0] * self.shape[1]
+        return np.ctypeslib.as_array(self._ptr(), shape=(n,)).reshape(self.shape).copy()
+
+    def release(self):
+        if self.mem:
+            if self.ticket and self.solver.h:
+                lib().nsf_download_wait(self.solver.h, self.ticket)
+            lib().nsf_host_free(self.mem)
+            self.mem = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
 class Solver:
     """One solver handle: Solver / Mesh / Simulation state resident on one GPU."""
 
@@ -235,6 +281,19 @@ class Solver:
         out = np.empty((len(fields), self.N))
         self._check(lib().nsf_download(self.h, mask, _dp(out)))
         return out
+
+    def download_async(self, fields=range(12)):
+        """Start a snapshot of `fields` that travels to the host while later steps march
+        (nsf_download_async); returns a Snapshot whose wait() gives the (len(fields), N) array."""
+        fields = sorted(fields)
+        mask = 0
+        for f in fields:
+            mask |= 1 << f
+        snap = Snapshot(self, len(fields))
+        t = ctypes.c_uint64()
+        self._check(lib().nsf_download_async(self.h, mask, snap._ptr(), ctypes.byref(t)))
+        snap.ticket = t.value
+        return snap
 
     def debug_wait_limit(self, polls=0, withhold_epilogue=False):
         """Test support: the stage kernel's wait limit in polls (0: default) and the switch that withholds

@@ -272,6 +272,84 @@ def adjoint_leg(device, nsfsi, reps=3, steps=200):
             "adjoint_step_phase_ms": {k: round(v, 4) for k, v in phases.items()}}
 
 
+SAVE_FIELDS = (("save_density", [0]), ("save_momentum", [1, 2, 3]), ("save_energy", [4]),
+               ("save_velocity", [5, 6, 7]), ("save_pressure", [8]), ("save_temperature", [9]),
+               ("save_viscosity", [10]), ("save_thermal_cond", [11]))
+
+
+def snapshot_leg(cfg, device, nsfsi, steps=60, every=20):
+    """Cost of snapshot output inside the march: the host loop of Simulation::run (march one step, read
+    t/dt/timeLevel) with a snapshot of the fields the case saves every `every` steps, as
+    OutputManager::storeCurrentSolution takes them. Modes: no snapshot; a synchronous download of all twelve
+    fields into pageable memory (what a host mirror of every field costs); a synchronous download of the saved
+    fields; nsf_download_async of the saved fields into two reused page-locked buffers (the snapshot writer's
+    scheme, without the file formatting, which runs on the writer's thread). Host wall clock per step, each
+    mode run twice and the second run kept (the first allocates staging buffers)."""
+    import ctypes
+    L = nsfsi.lib()
+    saved = [f for name, fs in SAVE_FIELDS if getattr(cfg, name) for f in fs]
+    mask = sum(1 << f for f in saved)
+    s = nsfsi.Solver(cfg, device=device)
+    N, nf = s.N, len(saved)
+    dp = ctypes.POINTER(ctypes.c_double)
+    bufs = []
+    for _ in range(2):
+        p = ctypes.c_void_p()
+        s._check(L.nsf_host_alloc(8 * nf * N, ctypes.byref(p)))
+        bufs.append(p)
+    host_all, host_saved = np.empty((12, N)), np.empty((nf, N))
+
+    def run(mode):
+        tickets = [0, 0]
+        s.march(3)
+        s.sync()
+        t0 = time.perf_counter()
+        for q in range(1, steps + 1):
+            s.march(1)
+            s.time()
+            if q % every:
+                continue
+            if mode == "sync_all":
+                s._check(L.nsf_download(s.h, 0xFFF, host_all.ctypes.data_as(dp)))
+            elif mode == "sync_saved":
+                s._check(L.nsf_download(s.h, mask, host_saved.ctypes.data_as(dp)))
+            elif mode == "async":
+                b = (q // every) & 1
+                if tickets[b]:
+                    s._check(L.nsf_download_wait(s.h, tickets[b]))
+                t = ctypes.c_uint64()
+                s._check(L.nsf_download_async(s.h, mask, ctypes.cast(bufs[b], dp), ctypes.byref(t)))
+                tickets[b] = t.value
+        for t in tickets:
+            if t:
+                s._check(L.nsf_download_wait(s.h, t))
+        return (time.perf_counter() - t0) * 1e3 / steps
+
+    try:
+        ms = {}
+        for mode in ("none", "sync_all", "sync_saved", "async"):
+            run(mode)
+            ms[mode] = run(mode)
+        # one snapshot's trip to the host with nothing else queued: the bound on how often snapshots hide
+        s.sync()
+        t = ctypes.c_uint64()
+        t0 = time.perf_counter()
+        s._check(L.nsf_download_async(s.h, mask, ctypes.cast(bufs[0], dp), ctypes.byref(t)))
+        s._check(L.nsf_download_wait(s.h, t.value))
+        trip_ms = (time.perf_counter() - t0) * 1e3
+    finally:
+        s.close()
+        for p in bufs:
+            L.nsf_host_free(p)
+    n_snap = steps // every
+    return {"steps": steps, "every": every, "fields_saved": nf, "bytes_per_snapshot": 8 * nf * N,
+            "async_trip_ms": round(trip_ms, 3), "async_trip_gbs": round(8 * nf * N / trip_ms / 1e6, 2),
+            "ms_per_step": {k: round(v, 4) for k, v in ms.items()},
+            "ms_per_snapshot_over_none": {k: round((ms[k] - ms["none"]) * steps / n_snap, 3)
+                                          for k in ("sync_all", "sync_saved", "async")},
+            "timing": "host wall clock; march 1 + t/dt/timeLevel read per step, snapshot every `every` steps"}
+
+
 def case_file(workload):
     return os.path.join(ROOT, "3d-ns-fsi_b200", "cases", WORKLOADS[workload]["case"] + ".cfg")
 
@@ -347,6 +425,7 @@ def arg_parser():
     ap.add_argument("--ensemble-only", action="store_true", help="run only the ensemble leg (profiling)")
     ap.add_argument("--no-seq", action="store_true", help="ensemble leg without the sequential comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint leg")
+    ap.add_argument("--no-snapshots", action="store_true", help="skip the snapshot-output leg")
     ap.add_argument("--adjoint-only", action="store_true", help="run only the discrete-adjoint leg (profiling)")
     ap.add_argument("--adjoint-steps", type=int, default=200, help="RK4 steps of the adjoint leg")
     return ap
@@ -472,6 +551,10 @@ def main():
                "d2h_bytes_per_step": (5 * 8 * nodes + 24 * args.steps) / args.steps,
                "timing": "host wall clock around upload + K x (march 1, read t/dt/timeLevel) + download"}
 
+    snaps = None
+    if not args.no_snapshots and args.workload == "tgv256" and rank == 0:
+        snaps = snapshot_leg(cfg, local, nsfsi)
+
     ens = None
     if args.ensemble_steps > 0 and args.workload == "tgv256":  # every rank takes its shard
         ens = ensemble_leg(args.ensemble_steps, local, nsfsi, sequential=not args.no_seq, rank=rank, world=world,
@@ -503,6 +586,8 @@ def main():
                          "step_frac": value / world / (peak * 1e9 / BYTES_PER_NODE_STEP),
                          "profile_clocks": clkp.summary()},
         }
+        if snaps is not None:
+            line["snapshots"] = snaps
         if ens is not None:
             line["ensemble"] = ens
         if not args.no_adjoint and args.workload == "tgv256":

@@ -11,7 +11,8 @@
  * freed in nsf_destroy) and one CUDA stream. Fields stay resident in HBM in the reference's SoA layout
  * (one array per variable, index i*NJ*NK + j*NK + k, k fastest). Host buffers passed to the download /
  * upload calls belong to the caller. No device pointer escapes through this interface.
- * Threading: calls on one handle must be serialised by the caller; different handles are independent.
+ * Threading: calls on one handle must be serialised by the caller (nsf_download_wait and
+ * nsf_download_done excepted); different handles are independent.
  */
 #ifndef NSFSI_H
 #define NSFSI_H
@@ -125,6 +126,28 @@ nsf_status nsf_get_time(nsf_solver* s, double* t, uint64_t* time_level, double* 
  * in increasing field order, N doubles each, reference layout. Replaces reading Mesh's public arrays
  * (Mesh.h:82-86), as OutputManager does (OutputManager.cpp:152-258). Synchronises. */
 nsf_status nsf_download(nsf_solver* s, uint32_t field_mask, double* host);
+
+/* Snapshot output that overlaps the march (the writes of OutputManager::storeCurrentSolution,
+ * OutputManager.cpp:101-106, called from processIntermediateOutput, :57-83). Queues, behind the steps
+ * already marched, a device copy of the fields in field_mask (packed as nsf_download packs them) into one
+ * of two staging buffers in HBM, then the copy of that buffer into `host` on a copy stream of its own, and
+ * returns without waiting: the steps marched after the call run while the snapshot travels to the host.
+ * `host` must be page-locked (nsf_host_alloc, or memory the caller pinned with CUDA) and hold
+ * popcount(field_mask) * N doubles; it must not be read or freed before nsf_download_wait returns for
+ * `*ticket`. The two staging buffers are used in turn: a third download waits on the device (not on the
+ * host) until the first one's copy has left its buffer. The first download of a larger field set than
+ * before allocates that buffer (and synchronises). Refused (NSF_ERR_STATE) for members of an ensemble or
+ * x-slab group, whose steps run on the group's stream: use nsf_download there. */
+nsf_status nsf_download_async(nsf_solver* s, uint32_t field_mask, double* host, uint64_t* ticket);
+/* Blocks until the download `ticket` has landed in its host buffer. May be called from another thread
+ * than the one marching the handle (e.g. a snapshot writer); it leaves nsf_last_error untouched. */
+nsf_status nsf_download_wait(nsf_solver* s, uint64_t ticket);
+/* *done = 1 if the download `ticket` has landed in its host buffer, else 0; never blocks. Thread rules as
+ * nsf_download_wait. */
+nsf_status nsf_download_done(nsf_solver* s, uint64_t ticket, int32_t* done);
+/* Page-locked host memory for nsf_download_async (the caller needs no CUDA headers), and its release. */
+nsf_status nsf_host_alloc(size_t bytes, void** out);
+nsf_status nsf_host_free(void* p);
 
 /* Overwrite the current conserved fields (5 x N doubles: rho, rho_u, rho_v, rho_w, rho_E) from host
  * memory at every node. The stored primitive state is not recomputed, exactly as writing

@@ -32,3 +32,27 @@ def test_no_device_is_a_loud_cuda_error_here():
         assert e.code == 2
     else:
         raise AssertionError("expected NSF_ERR_CUDA without a GPU")
+
+
+def test_async_download_argument_checks_without_device():
+    """nsf_download_async / _wait / _done refuse null arguments and host-only handles before any device work;
+    nsf_host_alloc fails loudly without a device and nsf_host_free accepts null."""
+    L = nsfsi.lib()
+    t, d = ctypes.c_uint64(), ctypes.c_int32()
+    buf = (ctypes.c_double * 8)()
+    assert L.nsf_download_async(None, 1, buf, ctypes.byref(t)) == 6
+    assert L.nsf_download_wait(None, 1) == 6
+    assert L.nsf_download_done(None, 1, ctypes.byref(d)) == 6
+    s = nsfsi.Solver(nsfsi.case_path("sphere48"), device=-1)
+    assert L.nsf_download_async(s.h, 1, buf, None) == 6
+    assert L.nsf_download_async(s.h, 1, buf, ctypes.byref(t)) == 7
+    assert L.nsf_download_wait(s.h, 1) == 7
+    assert L.nsf_download_done(s.h, 1, ctypes.byref(d)) == 7
+    s.close()
+    p = ctypes.c_void_p()
+    assert L.nsf_host_alloc(0, ctypes.byref(p)) == 6 and not p.value
+    assert L.nsf_host_alloc(64, None) == 6
+    import torch
+    if not torch.cuda.is_available():
+        assert L.nsf_host_alloc(64, ctypes.byref(p)) == 2 and not p.value
+    assert L.nsf_host_free(None) == 0

@@ -60,7 +60,7 @@ def fake_nsfsi():
 def test_main_arm_line_keeps_the_contract(monkeypatch, capsys):
     monkeypatch.setitem(sys.modules, "nsfsi", fake_nsfsi())
     monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "10", "--warmup", "3", "--no-e2e", "--ensemble-steps",
-                                      "0", "--no-adjoint", "--no-cpu-baseline"])
+                                      "0", "--no-adjoint", "--no-cpu-baseline", "--no-snapshots"])
     bench.main()
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     nodes = 256 ** 3

@@ -11,6 +11,7 @@ import subprocess
 import tempfile
 
 import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "3d-ns-fsi_b200")
@@ -21,11 +22,14 @@ def build_check(tmp):
     exe = os.path.join(tmp, "vtk_check")
     subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "host"),
                     os.path.join(ROOT, "tests", "host", "vtk_check.cpp"), "-o", exe, "-L", os.path.join(PKG, "lib"),
-                    "-lnsfsi", "-Wl,-rpath," + os.path.join(PKG, "lib")], check=True)
+                    "-lnsfsi", "-Wl,-rpath," + os.path.join(PKG, "lib"), "-pthread"], check=True)
     return exe
 
 
-def test_vtk_writer_matches_reference_bytes():
+@pytest.mark.parametrize("mode", ["mirrors", "packed", "writer"])
+def test_vtk_writer_matches_reference_bytes(mode):
+    """The VTK text from the Mesh mirrors, from packed saved fields only (the snapshot download's layout) and
+    from the snapshot writer's worker thread, each byte for byte against the reference's own file."""
     g = np.load(os.path.join(GOLD, "sphere_small.npz"))
     lvl = int(g["final_level"])
     fields = g["fields_%d" % lvl]
@@ -36,7 +40,11 @@ def test_vtk_writer_matches_reference_bytes():
         fb = os.path.join(tmp, "fields.bin")
         np.ascontiguousarray(fields, dtype=np.float64).tofile(fb)
         out = os.path.join(tmp, "out.vtk")
-        subprocess.run([exe, os.path.join(ROOT, "tests/golden/cases/sphere_small.cfg"), fb, repr(t), out], check=True)
+        r = subprocess.run([exe, os.path.join(ROOT, "tests/golden/cases/sphere_small.cfg"), fb, repr(t), out, mode],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+        if mode == "writer":
+            assert "refused: NSF_ERR_" in r.stdout
         mine = open(out, "rb").read()
     assert mine == ref
 

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <set>
@@ -92,6 +93,14 @@ struct AdjCtx {
   // Stage 4 of a recomputed step whose result enters no objective term: only the x-planes the inlet /
   // outlet adjoint reads (i = 1, 2, NI-3, NI-2) are computed, and nothing after that stage kernel runs.
   LaunchPlan lastStagePlan{};
+  // Tape: the snapshot set of every step, recorded by the forward run when nsteps sets fit the limit, so
+  // the backward run is the adjoint kernels alone (no checkpoint restores, re-advancing or recomputation).
+  // A set has the layout of a snapshot set; its control block is the step's entry of dHist.
+  uint64_t tapeLimit = UINT64_MAX;   // bytes; UINT64_MAX: half the free device memory at the forward run
+  double* tape = nullptr;
+  size_t tapeSetWords = 0;
+  bool tapeValid = false;            // the tape holds the last forward run's sets
+  cudaGraphExec_t tapeExec = nullptr;  // one step with its tape copies (sources and set resolved on the device)
   std::vector<void*> allocs;
 };
 
@@ -432,6 +441,101 @@ struct SnapHook : StepHook {
   }
 };
 
+size_t tape_set_words(const nsf_solver* s) { return 4 * per_stage(s) + 5 * nd(s); }
+
+SnapSet tape_set(const nsf_solver* s, const AdjCtx* a, int k) {
+  double* base = a->tape + size_t(k) * a->tapeSetWords;
+  return SnapSet{base, base + 4 * per_stage(s), a->dHist + k};
+}
+
+// The copies of SnapHook, into the tape set of the running step: the forward run records every step's set
+// with one captured step graph (the copy kernel reads the buffer roles and the time level from the control
+// block).
+struct TapeHook : StepHook {
+  nsf_solver* s;
+  AdjCtx* a;
+  TapeCopy T{};
+  TapeHook(nsf_solver* s_, AdjCtx* a_) : s(s_), a(a_) {
+    T.tape = a->tape;
+    T.setWords = (long long)a->tapeSetWords;
+    T.nSets = a->nsteps;
+  }
+  void add(int kind, int q, int f, const double* src, size_t srcOff, size_t dstOff, size_t words) {
+    if (T.n == kMaxCopies) flush();
+    const int c = T.n++;
+    T.kind[c] = kind;
+    T.q[c] = q;
+    T.f[c] = f;
+    T.src[c] = src;
+    T.srcOff[c] = (long long)srcOff;
+    T.dstOff[c] = (long long)dstOff;
+    T.words[c] = (long long)words;
+  }
+  void flush() {
+    launch_tape_copy(s->dCtl, T, s->nSM, s->stream);
+    T.n = 0;
+  }
+  void before_stage(int q) override {
+    const size_t N = nd(s), base = q * per_stage(s);
+    for (int f = 0; f < 5; ++f) add(TAPE_I, q, f, nullptr, 0, base + f * N, N);
+    add(TAPE_R_SEP, q, 0, nullptr, 0, base + 5 * N, N);
+    if (nf(s)) add(TAPE_FIXED, q, 0, s->hGrid.fpre, 0, base + 11 * N, 2 * nf(s));
+    flush();
+  }
+  bool wants_before_edges() const override { return a->xInOut && !a->edgePlanesClean; }
+  void before_edges(int q) override {
+    if (!wants_before_edges()) return;
+    const size_t N = nd(s), plane = size_t(s->hGrid.sI), NI = size_t(s->hGrid.NI), base = q * per_stage(s);
+    for (size_t i : {size_t(1), size_t(2), NI - 3, NI - 2})
+      for (int f = 0; f < 4; ++f) add(TAPE_O, q, f, nullptr, i * plane, base + (6 + f) * N + i * plane, plane);
+    flush();
+  }
+  // after the step (its finalize has advanced the level): the result
+  void result() {
+    const size_t N = nd(s);
+    T.levelOffset = -1;
+    for (int f = 0; f < 5; ++f) add(TAPE_O, 3, f, nullptr, 0, 4 * per_stage(s) + f * N, N);
+    flush();
+    T.levelOffset = 0;
+  }
+};
+
+// Whether the coming forward run records a tape (allocating it on first use), under the limit.
+nsf_status prepare_tape(nsf_solver* s, AdjCtx* a, bool* use) {
+  *use = false;
+  const size_t words = tape_set_words(s);
+  const double bytes = double(words) * 8.0 * a->nsteps;
+  if (a->tapeLimit == 0) return NSF_OK;
+  if (!a->tape) {
+    size_t fr = 0, tot = 0;
+    CKA(cudaMemGetInfo(&fr, &tot));
+    const double limit = a->tapeLimit == UINT64_MAX ? double(fr) / 2 : double(a->tapeLimit);
+    if (bytes > limit) return NSF_OK;
+    if (cudaMalloc(&a->tape, size_t(bytes)) != cudaSuccess) {
+      cudaGetLastError();  // not enough memory after all: checkpoints instead
+      a->tape = nullptr;
+      return NSF_OK;
+    }
+    a->tapeSetWords = words;
+  } else if (a->tapeLimit != UINT64_MAX && bytes > double(a->tapeLimit)) {
+    return NSF_OK;
+  }
+  if (!a->tapeExec) {
+    CKA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    TapeHook hook(s, a);
+    enqueue_step_hooked(s->dGrid, s->hGrid, s->plan, s->stream, &hook, nullptr);
+    hook.result();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (e != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("tape step capture: ") + cudaGetErrorString(e));
+    const cudaError_t e2 = cudaGraphInstantiate(&a->tapeExec, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("tape step graph: ") + cudaGetErrorString(e2));
+  }
+  *use = true;
+  return NSF_OK;
+}
+
 // Phases of an adjoint step, for nsf_adj_profile_step.
 // PH_BC: one launch per stage for ghosts, near-body filter, edge conditions and the RK4 combine (and, on
 // steps whose result enters J, the objective); slots 1 and 3-6 stay, empty, for the layout of the result.
@@ -474,14 +578,14 @@ nsf_status enqueue_recompute(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool ob
   return NSF_OK;
 }
 
-// Enqueues the adjoint kernels of that step on `stream`, reading only snapshot set `set` and fixed
-// buffers: the adjoint arrays hold the adjoint of U_{k+1} on entry and of U_k on exit.
-nsf_status enqueue_adjoint_kernels(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool objective, int set,
+// Enqueues the adjoint kernels of that step on `stream`, reading only snapshot set S (a pipelined set or the
+// step's tape set) and fixed buffers: the adjoint arrays hold the adjoint of U_{k+1} on entry and of U_k on
+// exit.
+nsf_status enqueue_adjoint_kernels(nsf_solver* s, AdjCtx* a, const StepCtl& R, bool objective, const SnapSet& S,
                                    cudaStream_t st, PhaseTimer* pt = nullptr) {
   auto mark = [&](int ph) {
     if (pt) pt->mark(ph);
   };
-  const SnapSet S = snap_set(a, set);
   const Grid& G = s->hGrid;
   const size_t N = nd(s);
   const int nSM = s->nSM;
@@ -588,7 +692,7 @@ nsf_status step_graph(nsf_solver* s, AdjCtx* a, int k, int part, int set, cudaSt
   if (it == a->graphs.end()) {
     CKA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     const nsf_status r = part == 0 ? enqueue_recompute(s, a, R, objective, set)
-                                   : enqueue_adjoint_kernels(s, a, R, objective, set, st);
+                                   : enqueue_adjoint_kernels(s, a, R, objective, snap_set(a, set), st);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &g);
     if (r != NSF_OK) {
@@ -687,6 +791,8 @@ void nsf_adjoint_free(nsf_solver* s) {
   AdjCtx* a = s->adj;
   if (a->adjStream) cudaStreamSynchronize(a->adjStream);
   for (auto& kv : a->graphs) cudaGraphExecDestroy(kv.second);
+  if (a->tapeExec) cudaGraphExecDestroy(a->tapeExec);
+  if (a->tape) cudaFree(a->tape);
   for (int j = 0; j < 2; ++j) {
     if (a->setReady[j]) cudaEventDestroy(a->setReady[j]);
     if (a->setFree[j]) cudaEventDestroy(a->setFree[j]);
@@ -713,6 +819,32 @@ nsf_status nsf_adj_configure(nsf_solver* s, uint32_t avg_last_steps, uint32_t sn
   a->navg = int(avg_last_steps);
   if (int(snapshots) != a->nsnap) a->chainStored = false;
   a->nsnap = int(snapshots);
+  return NSF_OK;
+}
+
+nsf_status nsf_adj_set_tape_limit(nsf_solver* s, uint64_t bytes) {
+  if (!s) return NSF_ERR_ARG;
+  nsf_status st = setup(s);
+  if (st != NSF_OK) return st;
+  AdjCtx* a = s->adj;
+  a->tapeLimit = bytes;
+  if (a->tape && bytes != UINT64_MAX && double(tape_set_words(s)) * 8.0 * a->nsteps > double(bytes)) {
+    CKA(cudaSetDevice(s->device));
+    CKA(cudaStreamSynchronize(a->adjStream));
+    CKA(cudaStreamSynchronize(s->stream));
+    if (a->tapeExec) cudaGraphExecDestroy(a->tapeExec);
+    a->tapeExec = nullptr;
+    cudaFree(a->tape);
+    a->tape = nullptr;
+    a->tapeValid = false;
+  }
+  return NSF_OK;
+}
+
+nsf_status nsf_adj_tape_bytes(nsf_solver* s, uint64_t* bytes) {
+  if (!s || !bytes) return NSF_ERR_ARG;
+  const AdjCtx* a = s->adj;
+  *bytes = a && a->tapeValid ? uint64_t(tape_set_words(s)) * 8u * uint64_t(a->nsteps) : 0u;
   return NSF_OK;
 }
 
@@ -746,10 +878,13 @@ nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow
   if ((st = reset(s, a)) != NSF_OK) return st;
   if ((st = save(s, a, 0)) != NSF_OK) return st;
   CKA(cudaMemsetAsync(a->dAcc, 0, sizeof(double), s->stream));
-  a->chain = first_descent(a->nsteps, a->nsnap);
+  bool tape = false;
+  a->tapeValid = false;
+  if ((st = prepare_tape(s, a, &tape)) != NSF_OK) return st;
+  a->chain = tape ? std::vector<std::pair<int, int>>{} : first_descent(a->nsteps, a->nsnap);
   size_t next = 0;
   for (int n = 0; n < a->nsteps; ++n) {
-    CKA(cudaGraphLaunch(s->graphExec, s->stream));
+    CKA(cudaGraphLaunch(tape ? a->tapeExec : s->graphExec, s->stream));
     if (n + 1 > a->nsteps - a->navg) launch_objective(s->dGrid, a->dNx, a->dA, 1.0 / a->navg, a->dAcc, s->stream);
     if (next < a->chain.size() && a->chain[next].first == n + 1)
       if ((st = save(s, a, a->chain[next++].second)) != NSF_OK) return st;
@@ -772,7 +907,8 @@ nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow
     if ((st = push_grid(s)) != NSF_OK) return st;
   }
   a->haveForward = true;
-  a->chainStored = true;
+  a->chainStored = !tape;
+  a->tapeValid = tape;
   return NSF_OK;
 }
 
@@ -795,8 +931,13 @@ nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* 
   CKA(cudaMemsetAsync(a->fbar, 0, 2 * plane * sizeof(double), s->stream));
   CKA(cudaMemsetAsync(a->dTimeout, 0, sizeof(int), s->stream));
   CKA(cudaStreamSynchronize(s->stream));  // the adjoint kernels on adjStream start from these
-  st = reverse(s, a, 0, a->nsteps, a->nsnap, 0, a->chainStored);
-  a->chainStored = false;  // the schedule has reused the slots
+  if (a->tapeValid) {  // every step's set is on the tape: the adjoint kernels alone, last step first
+    for (int k = a->nsteps - 1; k >= 0 && st == NSF_OK; --k)
+      st = enqueue_adjoint_kernels(s, a, a->hist[k], k + 1 > a->nsteps - a->navg, tape_set(s, a, k), a->adjStream);
+  } else {
+    st = reverse(s, a, 0, a->nsteps, a->nsnap, 0, a->chainStored);
+    a->chainStored = false;  // the schedule has reused the slots
+  }
   if (st != NSF_OK) {
     cudaStreamSynchronize(a->adjStream);
     return st;
@@ -838,7 +979,7 @@ nsf_status nsf_adj_profile_step(nsf_solver* s, uint64_t step, double* ms) {
   const bool objective = int(step) + 1 > a->nsteps - a->navg;
   CKA(cudaStreamSynchronize(a->adjStream));
   st = enqueue_recompute(s, a, a->hist[step], objective, 0, &pt);
-  if (st == NSF_OK) st = enqueue_adjoint_kernels(s, a, a->hist[step], objective, 0, s->stream, &pt);
+  if (st == NSF_OK) st = enqueue_adjoint_kernels(s, a, a->hist[step], objective, snap_set(a, 0), s->stream, &pt);
   CKA(cudaStreamSynchronize(s->stream));
   for (int q = 0; q < PH_COUNT; ++q) ms[q] = 0;
   pt.collect(ms);

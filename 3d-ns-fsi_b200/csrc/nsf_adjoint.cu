@@ -453,6 +453,30 @@ __global__ void k_copy_set(CopySet S) {
     dst[m] = src[m];
 }
 
+// Tape copies (blockIdx.y: the copy), sources and set from the control block of the running step.
+__global__ void k_tape_copy(const StepCtl* __restrict__ ctl, const __grid_constant__ TapeCopy T) {
+  const int c = blockIdx.y;
+  const StepCtl& C = *ctl;
+  const long long set = (long long)C.level + T.levelOffset;
+  if (set < 0 || set >= T.nSets) return;
+  const int q = T.q[c], f = T.f[c];
+  const double* src;
+  switch (T.kind[c]) {
+    case TAPE_I: src = C.I[q][f]; break;
+    case TAPE_R_SEP:
+      if (C.R[q] == C.I[q][0]) return;
+      src = C.R[q];
+      break;
+    case TAPE_O: src = C.O[q][f]; break;
+    default: src = T.src[c];
+  }
+  src += T.srcOff[c];
+  double* __restrict__ dst = T.tape + set * T.setWords + T.dstOff[c];
+  const long long n = T.words[c];
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x)
+    dst[m] = src[m];
+}
+
 // Transposed RHS (generated gather) and the chain rule through the primitive / transport values.
 // A block takes an 8 (j) x 32 (k) tile of nodes through a chunk of i-planes. The generated gather reads
 // the RHS adjoints at the 19 RHS nodes around a node and u, v, w, T, mu, kappa at its 7-point stencil:
@@ -710,6 +734,14 @@ void launch_copies(const double* const* src, double* const* dst, const long long
   }
   const long long b = (most + 255) / 256, cap = 2LL * nSM;
   k_copy_set<<<dim3(unsigned(b < cap ? b : cap), count), 256, 0, static_cast<cudaStream_t>(stream)>>>(S);
+}
+
+void launch_tape_copy(const StepCtl* ctl, const TapeCopy& T, int nSM, void* stream) {
+  if (T.n <= 0) return;
+  long long most = 1;
+  for (int c = 0; c < T.n; ++c) most = T.words[c] > most ? T.words[c] : most;
+  const long long b = (most + 255) / 256, cap = 2LL * nSM;
+  k_tape_copy<<<dim3(unsigned(b < cap ? b : cap), T.n), 256, 0, static_cast<cudaStream_t>(stream)>>>(ctl, T);
 }
 
 void launch_adj_density_filter(const Grid* dg, long long N, const double* lamDstConst, double* lamDst, double* lamSrc,

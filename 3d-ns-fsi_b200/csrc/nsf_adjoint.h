@@ -79,5 +79,27 @@ constexpr int kMaxCopies = 16;
 void launch_copies(const double* const* src, double* const* dst, const long long* words, int count, int nSM,
                    void* stream);
 
+// Copies into the adjoint's tape (the snapshot sets of every step of a forward run), with the sources and
+// the set resolved on the device from the live control block, so one captured step serves every step.
+enum TapeSource : int {
+  TAPE_I = 0,       // ctl->I[q][f]
+  TAPE_R_SEP = 1,   // ctl->R[q], copied only when it is another buffer than ctl->I[q][0]
+  TAPE_O = 2,       // ctl->O[q][f]
+  TAPE_FIXED = 3,   // src as given
+};
+struct TapeCopy {
+  int kind[kMaxCopies], q[kMaxCopies], f[kMaxCopies];
+  const double* src[kMaxCopies];
+  long long srcOff[kMaxCopies];  // added to the resolved source
+  long long dstOff[kMaxCopies];  // within the step's set
+  long long words[kMaxCopies];
+  int n;
+  double* tape;
+  long long setWords;
+  int levelOffset;  // set = ctl->level + levelOffset (-1 after the step, whose finalize advanced the level)
+  int nSets;        // a set outside [0, nSets) is not written
+};
+void launch_tape_copy(const StepCtl* ctl, const TapeCopy& T, int nSM, void* stream);
+
 }  // namespace nsf
 #endif

@@ -124,6 +124,8 @@ def lib():
         "nsf_slab_schedule": (i32, [cp, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
         "nsf_adj_configure": (i32, [vp, u32, u32]),
         "nsf_adj_forward": (i32, [vp, dp, dp, dp]),
+        "nsf_adj_set_tape_limit": (i32, [vp, u64]),
+        "nsf_adj_tape_bytes": (i32, [vp, ctypes.POINTER(u64)]),
         "nsf_adj_backward": (i32, [vp, ctypes.c_double, dp, dp]),
         "nsf_adj_get_dt": (i32, [vp, dp, ctypes.POINTER(u64)]),
         "nsf_adj_profile_step": (i32, [vp, u64, dp]),
@@ -362,6 +364,16 @@ class Solver:
     # ---------------------------------------------------------------- discrete adjoint
     def adj_configure(self, avg_last_steps=50, snapshots=20):
         self._check(lib().nsf_adj_configure(self.h, avg_last_steps, snapshots))
+
+    def adj_tape_limit(self, nbytes):
+        """Device memory the adjoint's tape may take (0: checkpointing only; None: the default, half the
+        free device memory)."""
+        self._check(lib().nsf_adj_set_tape_limit(self.h, (1 << 64) - 1 if nbytes is None else int(nbytes)))
+
+    def adj_tape_bytes(self):
+        n = ctypes.c_uint64()
+        self._check(lib().nsf_adj_tape_bytes(self.h, ctypes.byref(n)))
+        return n.value
 
     def adj_forward(self, u0=None, inflow=None):
         """J of a run from level 0 (u0: (5, N) conserved field or None for the case's IC; inflow: (NJ, NK)

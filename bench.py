@@ -218,15 +218,15 @@ def ensemble_leg(steps, device, nsfsi, sequential=True, rank=0, world=1, dist=No
 
 def adjoint_leg(device, nsfsi, reps=3, steps=200):
     """Discrete adjoint on a 64^3 channel with a sphere (200 RK4 steps, J = the sphere's x-force averaged
-    over the last 50 steps, 20 checkpoint slots): wall time of the synchronous forward and backward calls
-    (host overhead included), their ratio, the finite-difference agreement along two seeded directions
-    (h = 1e-6) and the device time of one adjoint step by phase."""
+    over the last 50 steps): wall time of the synchronous forward and backward calls (host overhead
+    included) with the default tape limit (the forward run records every step's snapshot set when they fit
+    in half the free device memory) and with checkpointing only (20 slots), against one plain forward
+    solve; the finite-difference agreement along two seeded directions (h = 1e-6) and the device time of
+    one adjoint step by phase."""
     cfg = nsfsi.config_load(nsfsi.case_path("adj64"))
     cfg.stop_time_level = steps
     navg = max(1, min(50, steps // 4))
-    with nsfsi.Solver(cfg, device=device) as s:
-        u0 = s.download(range(5))
-        s.adj_configure(navg, 20)
+    def timed(s):
         s.adj_forward()
         s.adj_backward()  # captures the adjoint step graphs
         fwd, bwd = [], []
@@ -238,6 +238,17 @@ def adjoint_leg(device, nsfsi, reps=3, steps=200):
             t2 = time.perf_counter()
             fwd.append(t1 - t0)
             bwd.append(t2 - t1)
+        return J, gi, gu, float(np.median(fwd)), float(np.median(bwd))
+
+    with nsfsi.Solver(cfg, device=device) as s:  # checkpointing only (20 slots), for comparison
+        s.adj_configure(navg, 20)
+        s.adj_tape_limit(0)
+        _, _, _, cf, cb = timed(s)
+    with nsfsi.Solver(cfg, device=device) as s:
+        u0 = s.download(range(5))
+        s.adj_configure(navg, 20)
+        J, gi, gu, f, b = timed(s)
+        tape_bytes = s.adj_tape_bytes()
         phases = s.adj_profile_step(steps // 2)
         rng = np.random.default_rng(2024)
         scale = np.maximum(np.abs(u0).max(axis=1), 1e-3)[:, None]
@@ -261,13 +272,15 @@ def adjoint_leg(device, nsfsi, reps=3, steps=200):
             p.sync()
             plain_wall.append(time.perf_counter() - t0)
             plain_dev.append(p.march_timed(steps) / 1e3)
-    f, b = float(np.median(fwd)), float(np.median(bwd))
     pf = float(np.median(plain_wall))
     return {"workload": "adj64: 64^3 channel, sphere D=0.2 at (0.4,0.5,0.5), M 0.3, Re_D 100 (Re 1666.7 per unit "
                         "length on the speed of sound), %d RK4 steps, J over the last %d" % (steps, navg),
-            "snapshots": 20, "J": J, "forward_ms": f * 1e3, "backward_ms": b * 1e3, "backward_over_forward": b / f,
+            "mode": "tape" if tape_bytes else "checkpoints", "tape_bytes": tape_bytes,
+            "J": J, "forward_ms": f * 1e3, "backward_ms": b * 1e3, "backward_over_forward": b / f,
             "plain_forward_ms": pf * 1e3, "plain_forward_device_ms": float(np.median(plain_dev)) * 1e3,
             "backward_over_plain_forward": b / pf, "gradient_over_plain_forward": (f + b) / pf,
+            "checkpointed": {"snapshots": 20, "forward_ms": cf * 1e3, "backward_ms": cb * 1e3,
+                             "gradient_over_plain_forward": (cf + cb) / pf},
             "fd_step": 1e-6, "fd_rel_err_max": max(errs), "fd_directions": len(errs),
             "adjoint_step_phase_ms": {k: round(v, 4) for k, v in phases.items()}}
 

@@ -295,9 +295,18 @@ nsf_status nsf_slab_schedule(const nsf_config* cfg, int32_t nslabs, int32_t worl
  * inlet's own nodes j, k in [1, N-2] matter). Cases: periodic faces and x inlet / outlet faces, spheres
  * and cylinders; stopCriterion "timesteps".
  * The first nsf_adj_forward freezes its dt sequence; later runs (and the backward pass) use it.
- * nsf_adj_backward: gradients of dJ * J; binomial checkpointing with `snapshots` stored states
- * (default 20) and recomputation. Both leave the handle's state at some level of the run. */
+ * nsf_adj_backward: gradients of dJ * J. When every step's snapshot set fits the tape limit
+ * (nsf_adj_set_tape_limit), the forward run records them all and the backward run is the adjoint kernels
+ * alone; otherwise binomial checkpointing with `snapshots` stored states (default 20) and recomputation.
+ * The gradients are the same bit for bit either way. Both leave the handle's state at some level of the
+ * run. */
 nsf_status nsf_adj_configure(nsf_solver* s, uint32_t avg_last_steps, uint32_t snapshots);
+/* Device memory the tape may take, in bytes: 0 never records one (checkpointing), UINT64_MAX (default)
+ * allows up to half the device memory free at the first forward run. A tape larger than a new limit is
+ * released. */
+nsf_status nsf_adj_set_tape_limit(nsf_solver* s, uint64_t bytes);
+/* Bytes of the tape the last forward run recorded (0: it checkpointed). */
+nsf_status nsf_adj_tape_bytes(nsf_solver* s, uint64_t* bytes);
 nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow, double* J);
 nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* g_u0);
 /* The frozen dt sequence (count values: dt of step n). */

@@ -88,7 +88,9 @@ def test_adjoint_short_run_tight():
     with solver("adj32", steps=12) as s:
         u0 = s.download(range(5))
         s.adj_configure(4, 3)
+        s.adj_tape_limit(0)  # checkpoints, so that the schedule recurses
         J = s.adj_forward()
+        assert s.adj_tape_bytes() == 0
         gi, gu = s.adj_backward()
         floor = 16 * np.finfo(float).eps * abs(J) / h
         dirs = seeded_directions(s, u0, 4, seed=7)
@@ -107,12 +109,16 @@ def test_adjoint_short_run_tight():
 def test_adjoint_schedule_does_not_change_the_gradient():
     """The recomputation is deterministic and the adjoint kernels run in the same order whatever the
     checkpointing schedule, so the gradient is bit-identical for 1, 4 and 40 snapshots (40 > steps: no
-    recomputation), and a second backward run after one forward run repeats it."""
+    recomputation) and for the tape (every step's snapshot set recorded by the forward run, no
+    recomputation at all), and a second backward run after one forward run repeats it."""
     ref = None
-    for snaps in (40, 4, 1):
+    for snaps in ("tape", 40, 4, 1):
         with solver("adj32", steps=30) as s:
-            s.adj_configure(10, snaps)
+            s.adj_configure(10, 20 if snaps == "tape" else snaps)
+            if snaps != "tape":
+                s.adj_tape_limit(0)
             s.adj_forward()
+            assert (s.adj_tape_bytes() > 0) == (snaps == "tape"), snaps
             gi, gu = s.adj_backward()
             gi2, gu2 = s.adj_backward()
             assert np.array_equal(gi, gi2) and np.array_equal(gu, gu2)
@@ -120,6 +126,29 @@ def test_adjoint_schedule_does_not_change_the_gradient():
                 ref = (gi, gu)
             else:
                 assert np.array_equal(gi, ref[0]) and np.array_equal(gu, ref[1]), snaps
+
+
+@pytest.mark.gpu
+def test_adjoint_tape_limit():
+    """The tape is recorded when every step's snapshot set fits the limit, and not when it does not; a
+    limit below a recorded tape releases it, and a forward run after that checkpoints."""
+    with solver("adj32", steps=12) as s:
+        s.adj_configure(4, 3)
+        s.adj_forward()
+        full = s.adj_tape_bytes()
+        assert full > 0
+        gi, gu = s.adj_backward()
+        s.adj_tape_limit(full - 1)
+        assert s.adj_tape_bytes() == 0
+        s.adj_forward()
+        assert s.adj_tape_bytes() == 0
+        gi2, gu2 = s.adj_backward()
+        assert np.array_equal(gi, gi2) and np.array_equal(gu, gu2)
+        s.adj_tape_limit(full)
+        s.adj_forward()
+        assert s.adj_tape_bytes() == full
+        gi3, gu3 = s.adj_backward()
+        assert np.array_equal(gi, gi3) and np.array_equal(gu, gu3)
 
 
 @pytest.mark.gpu

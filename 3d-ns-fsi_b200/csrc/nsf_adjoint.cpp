@@ -96,10 +96,18 @@ struct AdjCtx {
   // Tape: the snapshot set of every step, recorded by the forward run when nsteps sets fit the limit, so
   // the backward run is the adjoint kernels alone (no checkpoint restores, re-advancing or recomputation).
   // A set has the layout of a snapshot set; its control block is the step's entry of dHist.
+  // Segment tape, when the whole run's sets exceed the limit: the forward run stores a checkpoint every
+  // segLen steps in slots 0, 1, ... (segLen = ceil(nsteps / (nsnap + 1)), so the slots suffice), and the
+  // backward run restores each segment's checkpoint, records that segment's sets with the tape step graph
+  // and runs their adjoint kernels. The tape then holds two segments' sets (or one, when only one fits):
+  // the recording of a segment on the solver's stream overlaps the adjoint kernels of the one after it.
   uint64_t tapeLimit = UINT64_MAX;   // bytes; UINT64_MAX: half the free device memory at the forward run
   double* tape = nullptr;
   size_t tapeSetWords = 0;
+  int tapeSets = 0;                  // sets the tape holds (nsteps, or 1-2 segments of segLen)
+  int segLen = 0;
   bool tapeValid = false;            // the tape holds the last forward run's sets
+  bool segValid = false;             // the slots hold the last forward run's segment checkpoints
   cudaGraphExec_t tapeExec = nullptr;  // one step with its tape copies (sources and set resolved on the device)
   std::vector<void*> allocs;
 };
@@ -443,8 +451,9 @@ struct SnapHook : StepHook {
 
 size_t tape_set_words(const nsf_solver* s) { return 4 * per_stage(s) + 5 * nd(s); }
 
+// The tape set of step k (the tape holds every step's set, or a ring of segments' sets).
 SnapSet tape_set(const nsf_solver* s, const AdjCtx* a, int k) {
-  double* base = a->tape + size_t(k) * a->tapeSetWords;
+  double* base = a->tape + size_t(k % a->tapeSets) * a->tapeSetWords;
   return SnapSet{base, base + 4 * per_stage(s), a->dHist + k};
 }
 
@@ -458,7 +467,7 @@ struct TapeHook : StepHook {
   TapeHook(nsf_solver* s_, AdjCtx* a_) : s(s_), a(a_) {
     T.tape = a->tape;
     T.setWords = (long long)a->tapeSetWords;
-    T.nSets = a->nsteps;
+    T.nSets = a->tapeSets;
   }
   void add(int kind, int q, int f, const double* src, size_t srcOff, size_t dstOff, size_t words) {
     if (T.n == kMaxCopies) flush();
@@ -500,25 +509,56 @@ struct TapeHook : StepHook {
   }
 };
 
-// Whether the coming forward run records a tape (allocating it on first use), under the limit.
-nsf_status prepare_tape(nsf_solver* s, AdjCtx* a, bool* use) {
-  *use = false;
-  const size_t words = tape_set_words(s);
-  const double bytes = double(words) * 8.0 * a->nsteps;
+enum TapeMode { TAPE_NONE, TAPE_FULL, TAPE_SEGMENTS };
+
+void release_tape(AdjCtx* a) {
+  if (a->tapeExec) cudaGraphExecDestroy(a->tapeExec);
+  a->tapeExec = nullptr;
+  if (a->tape) cudaFree(a->tape);
+  a->tape = nullptr;
+  a->tapeSets = 0;
+  a->tapeValid = false;
+  a->segValid = false;
+}
+
+// The tape of the coming forward run under the limit (allocating it, and capturing the tape step graph, on
+// first use): every step's set when they all fit (TAPE_FULL: recorded by the forward run); else two
+// checkpoint segments' sets, or one, when the schedule has fewer slots than steps (TAPE_SEGMENTS: recorded
+// by the backward run, segment by segment); else none (binomial checkpointing).
+nsf_status prepare_tape(nsf_solver* s, AdjCtx* a, int* mode) {
+  *mode = TAPE_NONE;
   if (a->tapeLimit == 0) return NSF_OK;
-  if (!a->tape) {
+  const size_t words = tape_set_words(s);
+  const double setBytes = double(words) * 8.0;
+  double limit = double(a->tapeLimit);
+  if (a->tapeLimit == UINT64_MAX) {
     size_t fr = 0, tot = 0;
     CKA(cudaMemGetInfo(&fr, &tot));
-    const double limit = a->tapeLimit == UINT64_MAX ? double(fr) / 2 : double(a->tapeLimit);
-    if (bytes > limit) return NSF_OK;
-    if (cudaMalloc(&a->tape, size_t(bytes)) != cudaSuccess) {
+    limit = (double(fr) + setBytes * a->tapeSets) / 2;  // the free memory as it was before the tape
+  }
+  const int L = (a->nsteps + a->nsnap) / (a->nsnap + 1);
+  int sets = 0, m = TAPE_NONE;
+  if (setBytes * a->nsteps <= limit) {
+    sets = a->nsteps;
+    m = TAPE_FULL;
+  } else if (L < a->nsteps && setBytes * L <= limit) {
+    sets = setBytes * 2 * L <= limit ? 2 * L : L;
+    m = TAPE_SEGMENTS;
+  }
+  if (m == TAPE_NONE) return NSF_OK;
+  if (a->tape && a->tapeSets != sets) {
+    CKA(cudaStreamSynchronize(a->adjStream));
+    CKA(cudaStreamSynchronize(s->stream));
+    release_tape(a);
+  }
+  if (!a->tape) {
+    if (cudaMalloc(&a->tape, size_t(setBytes * sets)) != cudaSuccess) {
       cudaGetLastError();  // not enough memory after all: checkpoints instead
       a->tape = nullptr;
       return NSF_OK;
     }
     a->tapeSetWords = words;
-  } else if (a->tapeLimit != UINT64_MAX && bytes > double(a->tapeLimit)) {
-    return NSF_OK;
+    a->tapeSets = sets;
   }
   if (!a->tapeExec) {
     CKA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -532,7 +572,8 @@ nsf_status prepare_tape(nsf_solver* s, AdjCtx* a, bool* use) {
     cudaGraphDestroy(g);
     if (e2 != cudaSuccess) return fail(s, NSF_ERR_CUDA, std::string("tape step graph: ") + cudaGetErrorString(e2));
   }
-  *use = true;
+  a->segLen = m == TAPE_SEGMENTS ? L : 0;
+  *mode = m;
   return NSF_OK;
 }
 
@@ -731,6 +772,28 @@ nsf_status adjoint_step(nsf_solver* s, AdjCtx* a, int k) {
   return NSF_OK;
 }
 
+// The backward run over the segment tape: segments last first; each restores its checkpoint and records
+// its steps' sets with the tape step graph on the solver's stream (after the adjoint kernels that last read
+// that part of the tape), then its adjoint kernels run on adjStream, last step first, reading the sets.
+nsf_status reverse_segments(nsf_solver* s, AdjCtx* a) {
+  const int L = a->segLen, H = a->tapeSets / L, M = (a->nsteps + L - 1) / L;
+  nsf_status st;
+  for (int m = M - 1; m >= 0; --m) {
+    const int h = m % H, k0 = m * L, k1 = std::min(a->nsteps, k0 + L);
+    CKA(cudaStreamWaitEvent(s->stream, a->setFree[h], 0));
+    if ((st = restore(s, a, m)) != NSF_OK) return st;
+    for (int k = k0; k < k1; ++k) CKA(cudaGraphLaunch(a->tapeExec, s->stream));
+    CKA(cudaEventRecord(a->setReady[h], s->stream));
+    CKA(cudaStreamWaitEvent(a->adjStream, a->setReady[h], 0));
+    for (int k = k1 - 1; k >= k0; --k)
+      if ((st = enqueue_adjoint_kernels(s, a, a->hist[k], k + 1 > a->nsteps - a->navg, tape_set(s, a, k),
+                                        a->adjStream)) != NSF_OK)
+        return st;
+    CKA(cudaEventRecord(a->setFree[h], a->adjStream));
+  }
+  return NSF_OK;
+}
+
 double binom(int n, int k) {
   double r = 1;
   for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
@@ -791,8 +854,7 @@ void nsf_adjoint_free(nsf_solver* s) {
   AdjCtx* a = s->adj;
   if (a->adjStream) cudaStreamSynchronize(a->adjStream);
   for (auto& kv : a->graphs) cudaGraphExecDestroy(kv.second);
-  if (a->tapeExec) cudaGraphExecDestroy(a->tapeExec);
-  if (a->tape) cudaFree(a->tape);
+  release_tape(a);
   for (int j = 0; j < 2; ++j) {
     if (a->setReady[j]) cudaEventDestroy(a->setReady[j]);
     if (a->setFree[j]) cudaEventDestroy(a->setFree[j]);
@@ -817,7 +879,7 @@ nsf_status nsf_adj_configure(nsf_solver* s, uint32_t avg_last_steps, uint32_t sn
     a->graphs.clear();
   }
   a->navg = int(avg_last_steps);
-  if (int(snapshots) != a->nsnap) a->chainStored = false;
+  if (int(snapshots) != a->nsnap) a->chainStored = a->segValid = false;
   a->nsnap = int(snapshots);
   return NSF_OK;
 }
@@ -828,15 +890,11 @@ nsf_status nsf_adj_set_tape_limit(nsf_solver* s, uint64_t bytes) {
   if (st != NSF_OK) return st;
   AdjCtx* a = s->adj;
   a->tapeLimit = bytes;
-  if (a->tape && bytes != UINT64_MAX && double(tape_set_words(s)) * 8.0 * a->nsteps > double(bytes)) {
+  if (a->tape && bytes != UINT64_MAX && double(a->tapeSetWords) * 8.0 * a->tapeSets > double(bytes)) {
     CKA(cudaSetDevice(s->device));
     CKA(cudaStreamSynchronize(a->adjStream));
     CKA(cudaStreamSynchronize(s->stream));
-    if (a->tapeExec) cudaGraphExecDestroy(a->tapeExec);
-    a->tapeExec = nullptr;
-    cudaFree(a->tape);
-    a->tape = nullptr;
-    a->tapeValid = false;
+    release_tape(a);
   }
   return NSF_OK;
 }
@@ -845,6 +903,15 @@ nsf_status nsf_adj_tape_bytes(nsf_solver* s, uint64_t* bytes) {
   if (!s || !bytes) return NSF_ERR_ARG;
   const AdjCtx* a = s->adj;
   *bytes = a && a->tapeValid ? uint64_t(tape_set_words(s)) * 8u * uint64_t(a->nsteps) : 0u;
+  return NSF_OK;
+}
+
+nsf_status nsf_adj_segment_tape(nsf_solver* s, uint64_t* bytes, uint32_t* segment_steps) {
+  if (!s || !bytes || !segment_steps) return NSF_ERR_ARG;
+  const AdjCtx* a = s->adj;
+  const bool on = a && a->segValid && a->tape;
+  *bytes = on ? uint64_t(a->tapeSetWords) * 8u * uint64_t(a->tapeSets) : 0u;
+  *segment_steps = on ? uint32_t(a->segLen) : 0u;
   return NSF_OK;
 }
 
@@ -878,10 +945,15 @@ nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow
   if ((st = reset(s, a)) != NSF_OK) return st;
   if ((st = save(s, a, 0)) != NSF_OK) return st;
   CKA(cudaMemsetAsync(a->dAcc, 0, sizeof(double), s->stream));
-  bool tape = false;
-  a->tapeValid = false;
-  if ((st = prepare_tape(s, a, &tape)) != NSF_OK) return st;
-  a->chain = tape ? std::vector<std::pair<int, int>>{} : first_descent(a->nsteps, a->nsnap);
+  int mode = TAPE_NONE;
+  a->tapeValid = a->segValid = false;
+  if ((st = prepare_tape(s, a, &mode)) != NSF_OK) return st;
+  const bool tape = mode == TAPE_FULL;
+  a->chain.clear();
+  if (mode == TAPE_SEGMENTS)  // a checkpoint at the start of every segment (level 0 is in slot 0)
+    for (int m = 1; m * a->segLen < a->nsteps; ++m) a->chain.push_back({m * a->segLen, m});
+  else if (mode == TAPE_NONE)
+    a->chain = first_descent(a->nsteps, a->nsnap);
   size_t next = 0;
   for (int n = 0; n < a->nsteps; ++n) {
     CKA(cudaGraphLaunch(tape ? a->tapeExec : s->graphExec, s->stream));
@@ -907,8 +979,9 @@ nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow
     if ((st = push_grid(s)) != NSF_OK) return st;
   }
   a->haveForward = true;
-  a->chainStored = !tape;
+  a->chainStored = mode == TAPE_NONE;
   a->tapeValid = tape;
+  a->segValid = mode == TAPE_SEGMENTS;
   return NSF_OK;
 }
 
@@ -934,6 +1007,8 @@ nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* 
   if (a->tapeValid) {  // every step's set is on the tape: the adjoint kernels alone, last step first
     for (int k = a->nsteps - 1; k >= 0 && st == NSF_OK; --k)
       st = enqueue_adjoint_kernels(s, a, a->hist[k], k + 1 > a->nsteps - a->navg, tape_set(s, a, k), a->adjStream);
+  } else if (a->segValid && a->tape) {  // each segment recorded from its checkpoint, then its adjoint kernels
+    st = reverse_segments(s, a);
   } else {
     st = reverse(s, a, 0, a->nsteps, a->nsnap, 0, a->chainStored);
     a->chainStored = false;  // the schedule has reused the slots

@@ -457,8 +457,9 @@ __global__ void k_copy_set(CopySet S) {
 __global__ void k_tape_copy(const StepCtl* __restrict__ ctl, const __grid_constant__ TapeCopy T) {
   const int c = blockIdx.y;
   const StepCtl& C = *ctl;
-  const long long set = (long long)C.level + T.levelOffset;
-  if (set < 0 || set >= T.nSets) return;
+  long long set = (long long)C.level + T.levelOffset;
+  if (set < 0) return;
+  set %= T.nSets;
   const int q = T.q[c], f = T.f[c];
   const double* src;
   switch (T.kind[c]) {

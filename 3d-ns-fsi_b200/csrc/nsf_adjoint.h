@@ -96,8 +96,9 @@ struct TapeCopy {
   int n;
   double* tape;
   long long setWords;
-  int levelOffset;  // set = ctl->level + levelOffset (-1 after the step, whose finalize advanced the level)
-  int nSets;        // a set outside [0, nSets) is not written
+  int levelOffset;  // set = (ctl->level + levelOffset) mod nSets (levelOffset -1 after the step, whose
+                    // finalize advanced the level); nothing is written for a negative level + levelOffset
+  int nSets;        // sets the tape holds: every step's, or a ring of checkpoint segments' sets
 };
 void launch_tape_copy(const StepCtl* ctl, const TapeCopy& T, int nSM, void* stream);
 

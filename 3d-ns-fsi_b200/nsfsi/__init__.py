@@ -126,6 +126,7 @@ def lib():
         "nsf_adj_forward": (i32, [vp, dp, dp, dp]),
         "nsf_adj_set_tape_limit": (i32, [vp, u64]),
         "nsf_adj_tape_bytes": (i32, [vp, ctypes.POINTER(u64)]),
+        "nsf_adj_segment_tape": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(u32)]),
         "nsf_adj_backward": (i32, [vp, ctypes.c_double, dp, dp]),
         "nsf_adj_get_dt": (i32, [vp, dp, ctypes.POINTER(u64)]),
         "nsf_adj_profile_step": (i32, [vp, u64, dp]),
@@ -374,6 +375,13 @@ class Solver:
         n = ctypes.c_uint64()
         self._check(lib().nsf_adj_tape_bytes(self.h, ctypes.byref(n)))
         return n.value
+
+    def adj_segment_tape(self):
+        """(bytes, steps per segment) of the segment tape the last forward run left for the backward run
+        ((0, 0): none)."""
+        n, L = ctypes.c_uint64(), ctypes.c_uint32()
+        self._check(lib().nsf_adj_segment_tape(self.h, ctypes.byref(n), ctypes.byref(L)))
+        return n.value, L.value
 
     def adj_forward(self, u0=None, inflow=None):
         """J of a run from level 0 (u0: (5, N) conserved field or None for the case's IC; inflow: (NJ, NK)

@@ -221,8 +221,8 @@ def adjoint_leg(device, nsfsi, reps=3, steps=200):
     over the last 50 steps): wall time of the synchronous forward and backward calls (host overhead
     included) with the default tape limit (the forward run records every step's snapshot set when they fit
     in half the free device memory) and with checkpointing only (20 slots), against one plain forward
-    solve; the finite-difference agreement along two seeded directions (h = 1e-6) and the device time of
-    one adjoint step by phase."""
+    solve; with 20 slots and a segment tape of two segments' sets; the finite-difference agreement along
+    two seeded directions (h = 1e-6) and the device time of one adjoint step by phase."""
     cfg = nsfsi.config_load(nsfsi.case_path("adj64"))
     cfg.stop_time_level = steps
     navg = max(1, min(50, steps // 4))
@@ -240,7 +240,7 @@ def adjoint_leg(device, nsfsi, reps=3, steps=200):
             bwd.append(t2 - t1)
         return J, gi, gu, float(np.median(fwd)), float(np.median(bwd))
 
-    with nsfsi.Solver(cfg, device=device) as s:  # checkpointing only (20 slots), for comparison
+    with nsfsi.Solver(cfg, device=device) as s:  # binomial checkpointing only (20 slots), for comparison
         s.adj_configure(navg, 20)
         s.adj_tape_limit(0)
         _, _, _, cf, cb = timed(s)
@@ -260,6 +260,20 @@ def adjoint_leg(device, nsfsi, reps=3, steps=200):
             h = 1e-6
             fd = (s.adj_forward(u0 + h * du, 1 + h * di) - s.adj_forward(u0 - h * du, 1 - h * di)) / (2 * h)
             errs.append(abs(fd - ad) / abs(ad))
+    # 20 slots and a tape of two segments' sets (a state every ceil(steps / 21) steps; the backward run
+    # records each segment's sets from its state)
+    seg = {}
+    if tape_bytes:
+        set_bytes = tape_bytes // steps
+        seg_steps = -(-steps // 21)
+        with nsfsi.Solver(cfg, device=device) as s:
+            s.adj_configure(navg, 20)
+            s.adj_tape_limit(2 * seg_steps * set_bytes)
+            _, sgi, sgu, sf, sb = timed(s)
+            seg_bytes, seg_len = s.adj_segment_tape()
+            seg = {"snapshots": 20, "segment_steps": seg_len, "segment_tape_bytes": seg_bytes,
+                   "forward_ms": sf * 1e3, "backward_ms": sb * 1e3,
+                   "same_gradient_as_tape": bool(np.array_equal(sgi, gi) and np.array_equal(sgu, gu))}
     # one plain forward solve of the same case and length (the solver's step graph, no checkpoints), timed
     # after a warm-up run: wall time of the synchronous march + sync, and device time
     plain_wall, plain_dev = [], []
@@ -281,6 +295,8 @@ def adjoint_leg(device, nsfsi, reps=3, steps=200):
             "backward_over_plain_forward": b / pf, "gradient_over_plain_forward": (f + b) / pf,
             "checkpointed": {"snapshots": 20, "forward_ms": cf * 1e3, "backward_ms": cb * 1e3,
                              "gradient_over_plain_forward": (cf + cb) / pf},
+            "segment_tape": dict(seg, gradient_over_plain_forward=(seg["forward_ms"] + seg["backward_ms"]) / 1e3 / pf)
+            if seg else None,
             "fd_step": 1e-6, "fd_rel_err_max": max(errs), "fd_directions": len(errs),
             "adjoint_step_phase_ms": {k: round(v, 4) for k, v in phases.items()}}
 

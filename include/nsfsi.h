@@ -297,9 +297,12 @@ nsf_status nsf_slab_schedule(const nsf_config* cfg, int32_t nslabs, int32_t worl
  * The first nsf_adj_forward freezes its dt sequence; later runs (and the backward pass) use it.
  * nsf_adj_backward: gradients of dJ * J. When every step's snapshot set fits the tape limit
  * (nsf_adj_set_tape_limit), the forward run records them all and the backward run is the adjoint kernels
- * alone; otherwise binomial checkpointing with `snapshots` stored states (default 20) and recomputation.
- * The gradients are the same bit for bit either way. Both leave the handle's state at some level of the
- * run. */
+ * alone. Otherwise the forward run stores `snapshots` + 1 states (default 20 + the initial one): when two
+ * segments' sets fit the limit (or one), a state every ceil(steps / (snapshots + 1)) steps, and the
+ * backward run restores each segment's state, records that segment's sets and runs its adjoint kernels
+ * (the recording of one segment overlaps the adjoint kernels of the next); else binomial checkpointing
+ * with recomputation. The gradients are the same bit for bit either way. Both leave the handle's state at
+ * some level of the run. */
 nsf_status nsf_adj_configure(nsf_solver* s, uint32_t avg_last_steps, uint32_t snapshots);
 /* Device memory the tape may take, in bytes: 0 never records one (checkpointing), UINT64_MAX (default)
  * allows up to half the device memory free at the first forward run. A tape larger than a new limit is
@@ -307,6 +310,9 @@ nsf_status nsf_adj_configure(nsf_solver* s, uint32_t avg_last_steps, uint32_t sn
 nsf_status nsf_adj_set_tape_limit(nsf_solver* s, uint64_t bytes);
 /* Bytes of the tape the last forward run recorded (0: it checkpointed). */
 nsf_status nsf_adj_tape_bytes(nsf_solver* s, uint64_t* bytes);
+/* The segment tape the last forward run left for the backward run: its bytes and the steps per segment
+ * (both 0: none, the run was taped whole or checkpoints binomially). */
+nsf_status nsf_adj_segment_tape(nsf_solver* s, uint64_t* bytes, uint32_t* segment_steps);
 nsf_status nsf_adj_forward(nsf_solver* s, const double* u0, const double* inflow, double* J);
 nsf_status nsf_adj_backward(nsf_solver* s, double dJ, double* g_inflow, double* g_u0);
 /* The frozen dt sequence (count values: dt of step n). */

@@ -112,13 +112,19 @@ def test_adjoint_schedule_does_not_change_the_gradient():
     recomputation) and for the tape (every step's snapshot set recorded by the forward run, no
     recomputation at all), and a second backward run after one forward run repeats it."""
     ref = None
-    for snaps in ("tape", 40, 4, 1):
+    set_bytes = None
+    for snaps in ("tape", 40, 4, 1, "segments"):
         with solver("adj32", steps=30) as s:
-            s.adj_configure(10, 20 if snaps == "tape" else snaps)
-            if snaps != "tape":
+            s.adj_configure(10, {"tape": 20, "segments": 3}.get(snaps, snaps))
+            if snaps == "segments":  # 3 + 1 slots: segments of 8 steps (the last of 6), a ring of two
+                s.adj_tape_limit(16 * set_bytes)
+            elif snaps != "tape":
                 s.adj_tape_limit(0)
             s.adj_forward()
             assert (s.adj_tape_bytes() > 0) == (snaps == "tape"), snaps
+            if snaps == "tape":
+                set_bytes = s.adj_tape_bytes() // 30
+            assert s.adj_segment_tape() == ((16 * set_bytes, 8) if snaps == "segments" else (0, 0)), snaps
             gi, gu = s.adj_backward()
             gi2, gu2 = s.adj_backward()
             assert np.array_equal(gi, gi2) and np.array_equal(gu, gu2)
@@ -131,17 +137,34 @@ def test_adjoint_schedule_does_not_change_the_gradient():
 @pytest.mark.gpu
 def test_adjoint_tape_limit():
     """The tape is recorded when every step's snapshot set fits the limit, and not when it does not; a
-    limit below a recorded tape releases it, and a forward run after that checkpoints."""
+    limit below a recorded tape releases it. Below the whole run's tape, the forward run stores a state
+    every ceil(12 / (3 + 1)) = 3 steps and leaves a segment tape of two segments' sets (or one) for the
+    backward run; with no segment's sets under the limit it checkpoints binomially. Same gradient in every
+    mode."""
     with solver("adj32", steps=12) as s:
         s.adj_configure(4, 3)
         s.adj_forward()
         full = s.adj_tape_bytes()
-        assert full > 0
+        assert full > 0 and full % 12 == 0 and s.adj_segment_tape() == (0, 0)
         gi, gu = s.adj_backward()
         s.adj_tape_limit(full - 1)
         assert s.adj_tape_bytes() == 0
         s.adj_forward()
         assert s.adj_tape_bytes() == 0
+        assert s.adj_segment_tape() == (full // 2, 3)
+        gi2, gu2 = s.adj_backward()
+        assert np.array_equal(gi, gi2) and np.array_equal(gu, gu2)
+        gi2, gu2 = s.adj_backward()  # a second backward run from the same checkpoints
+        assert np.array_equal(gi, gi2) and np.array_equal(gu, gu2)
+        s.adj_tape_limit(full // 4)  # one segment's sets
+        s.adj_forward()
+        assert s.adj_segment_tape() == (full // 4, 3)
+        gi2, gu2 = s.adj_backward()
+        assert np.array_equal(gi, gi2) and np.array_equal(gu, gu2)
+        s.adj_tape_limit(full // 4 - 1)  # releases the segment tape: binomial checkpointing
+        assert s.adj_segment_tape() == (0, 0)
+        s.adj_forward()
+        assert s.adj_tape_bytes() == 0 and s.adj_segment_tape() == (0, 0)
         gi2, gu2 = s.adj_backward()
         assert np.array_equal(gi, gi2) and np.array_equal(gu, gu2)
         s.adj_tape_limit(full)

@@ -311,7 +311,7 @@ def snapshot_leg(cfg, device, nsfsi, steps=60, every=20):
     t/dt/timeLevel) with a snapshot of the fields the case saves every `every` steps, as
     OutputManager::storeCurrentSolution takes them. Modes: no snapshot; a synchronous download of all twelve
     fields into pageable memory (what a host mirror of every field costs); a synchronous download of the saved
-    fields; nsf_download_async of the saved fields into two reused page-locked buffers (the snapshot writer's
+    fields into a page-locked buffer; nsf_download_async of the saved fields into two reused page-locked buffers (the snapshot writer's
     scheme, without the file formatting, which runs on the writer's thread). Host wall clock per step, each
     mode run twice and the second run kept (the first allocates staging buffers)."""
     import ctypes
@@ -326,7 +326,7 @@ def snapshot_leg(cfg, device, nsfsi, steps=60, every=20):
         p = ctypes.c_void_p()
         s._check(L.nsf_host_alloc(8 * nf * N, ctypes.byref(p)))
         bufs.append(p)
-    host_all, host_saved = np.empty((12, N)), np.empty((nf, N))
+    host_all = np.empty((12, N))
 
     def run(mode):
         tickets = [0, 0]
@@ -341,7 +341,7 @@ def snapshot_leg(cfg, device, nsfsi, steps=60, every=20):
             if mode == "sync_all":
                 s._check(L.nsf_download(s.h, 0xFFF, host_all.ctypes.data_as(dp)))
             elif mode == "sync_saved":
-                s._check(L.nsf_download(s.h, mask, host_saved.ctypes.data_as(dp)))
+                s._check(L.nsf_download(s.h, mask, ctypes.cast(bufs[0], dp)))
             elif mode == "async":
                 b = (q // every) & 1
                 if tickets[b]:

@@ -752,11 +752,21 @@ nsf_status nsf_march(nsf_solver* s, uint64_t nsteps) {
   return NSF_OK;
 }
 
+// The control block after everything queued on the solver's stream: one copy into page-locked memory
+// queued behind that work, then one wait.
+static nsf_status read_ctl(nsf_solver* s, StepCtl* out) {
+  if (!s->hCtl) CK(cudaMallocHost(&s->hCtl, sizeof(StepCtl)));
+  CK(cudaMemcpyAsync(s->hCtl, s->dCtl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *out = *s->hCtl;
+  return NSF_OK;
+}
+
 nsf_status nsf_sync(nsf_solver* s) {
   if (!s || !s->initialized || s->hostOnly) return s ? NSF_ERR_STATE : NSF_ERR_ARG;
-  CK(cudaStreamSynchronize(s->stream));
   StepCtl ctl;
-  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  const nsf_status st = read_ctl(s, &ctl);
+  if (st != NSF_OK) return st;
   if (ctl.timeout) {
     s->err = "a bounded wait in the stage kernel gave up; results of the affected steps are invalid";
     return NSF_ERR_TIMEOUT;
@@ -789,9 +799,9 @@ nsf_status nsf_get_body_interaction(nsf_solver* s, int32_t* interact) {
 
 nsf_status nsf_get_time(nsf_solver* s, double* t, uint64_t* level, double* dt) {
   if (!s || !s->initialized || s->hostOnly) return s ? NSF_ERR_STATE : NSF_ERR_ARG;
-  CK(cudaStreamSynchronize(s->stream));
   StepCtl ctl;
-  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  const nsf_status st = read_ctl(s, &ctl);
+  if (st != NSF_OK) return st;
   if (t) *t = ctl.t;
   if (level) *level = ctl.level;
   if (dt) *dt = ctl.dt;
@@ -806,6 +816,19 @@ nsf_status nsf_download(nsf_solver* s, uint32_t mask, double* host) {
   const SnapSlots sl = snap_slots(mask, &nf);
   if (!nf) return NSF_OK;
   CK(cudaSetDevice(s->device));
+  if ((mask & ~0x1Fu) == 0) {  // conserved fields only: copied straight from their current buffers
+    StepCtl ctl;
+    const nsf_status st = read_ctl(s, &ctl);
+    if (st != NSF_OK) return st;
+    const HostSetup& S = s->setup;
+    const size_t hp = S.NK * sizeof(double), dp = size_t(s->hGrid.NKp) * sizeof(double);
+    for (int f = 0; f < 5; ++f)
+      if (sl.slot[f] >= 0)
+        CK(cudaMemcpy2DAsync(host + size_t(sl.slot[f]) * S.N, hp, s->hGrid.bufs[ctl.perm[f][0]][f], dp, hp,
+                             S.NI * S.NJ, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return NSF_OK;
+  }
   const size_t bytes = size_t(nf) * s->setup.N * sizeof(double);
   double* tmp = nullptr;
   CK(cudaMalloc(&tmp, bytes));
@@ -915,9 +938,9 @@ nsf_status nsf_host_free(void* p) {
 nsf_status nsf_upload_conserved(nsf_solver* s, const double* host) {
   if (!s || !host) return NSF_ERR_ARG;
   if (!s->initialized || s->hostOnly) return NSF_ERR_STATE;
-  CK(cudaStreamSynchronize(s->stream));
   StepCtl ctl;
-  CK(cudaMemcpy(&ctl, s->dCtl, sizeof ctl, cudaMemcpyDeviceToHost));
+  const nsf_status st = read_ctl(s, &ctl);
+  if (st != NSF_OK) return st;
   const HostSetup& S = s->setup;
   const size_t N = S.N, NKp = size_t(s->hGrid.NKp);
   for (int f = 0; f < 5; ++f)
@@ -1101,6 +1124,7 @@ void nsf_destroy(nsf_solver* s) {
     cudaStreamDestroy(s->dlStream);
   }
   for (void* p : s->allocs) cudaFree(p);
+  if (s->hCtl) cudaFreeHost(s->hCtl);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }

@@ -24,6 +24,7 @@ struct nsf_solver {
   nsf::Grid hGrid{};
   nsf::Grid* dGrid = nullptr;
   nsf::StepCtl* dCtl = nullptr;
+  nsf::StepCtl* hCtl = nullptr;  // page-locked host copy of the control block (nsf_get_time, nsf_sync)
   nsf::LaunchPlan plan{};
   cudaGraphExec_t graphExec = nullptr;
   cudaGraph_t graph = nullptr;

@@ -166,7 +166,7 @@ def shard_members(nodes, world):
 
 def ensemble_leg(steps, device, nsfsi, sequential=True, rank=0, world=1, dist=None):
     """Batched ensemble (64 seeded single-sphere flows on 5 grid shapes) against the same 64 runs made one
-    after another on the plain path. Both timed on the device (CUDA events), setup excluded. With several
+    after another on the plain path. Both timed on the device (CUDA events), setup excluded, alternating. With several
     ranks every rank advances its shard of the members (one graph per step for its shard) and the slowest
     rank's time counts; every rank must call this (it holds collectives)."""
     allCfgs = nsfsi.ensemble_configs(n=64, steps=steps)
@@ -187,20 +187,35 @@ def ensemble_leg(steps, device, nsfsi, sequential=True, rank=0, world=1, dist=No
                 raise
             return 1
 
+    # The ensemble run and the pass over the plain solves alternate, ENS_REPEATS times, so both see the same
+    # thermal and power-cap history; the medians are compared (every run advances the same flows by `steps`).
+    ens_runs, seq_runs = [], []
+    nonfinite = 0
     with nsfsi.Ensemble(cfgs, device=device, tune_cache=TUNE_CACHE) as ens:
         tile, lps, items = ens.info()
         ens.march(3)
         sync(ens)
-        ens_ms = ens.march_timed(steps)
-        sync(ens)
-    seq_ms = 0.0
-    nonfinite = 0
-    for c in (cfgs if sequential else []):
-        with nsfsi.Solver(c, device=device) as s:
-            s.march(3)
-            sync(s)
-            seq_ms += s.march_timed(steps)
-            nonfinite += sync(s)
+        solvers = [nsfsi.Solver(c, device=device) for c in cfgs] if sequential else []
+        try:
+            for s in solvers:
+                s.march(3)
+                sync(s)
+            for r in range(ENS_REPEATS):
+                ens_runs.append(ens.march_timed(steps))
+                sync(ens)
+                if sequential:
+                    t = 0.0
+                    for s in solvers:
+                        t += s.march_timed(steps)
+                        bad = sync(s)
+                        if r == 0:
+                            nonfinite += bad  # after the first `steps` steps, as the configurations state
+                    seq_runs.append(t)
+        finally:
+            for s in solvers:
+                s.close()
+    ens_ms = statistics.median(ens_runs)
+    seq_ms = statistics.median(seq_runs) if sequential else 0.0
     # the slowest rank's times; non-finite members summed over the ranks
     ens_ms = max_over_ranks(ens_ms, dist)
     seq_ms = max_over_ranks(seq_ms, dist)
@@ -213,7 +228,8 @@ def ensemble_leg(steps, device, nsfsi, sequential=True, rank=0, world=1, dist=No
             "sequential_value": work / (seq_ms / 1e3) if sequential else None,
             "speedup_vs_sequential": seq_ms / ens_ms if sequential else None,
             "ms": ens_ms, "sequential_ms": seq_ms if sequential else None, "tile": ["32x8", "16x16"][tile], "launches_per_step": lps,
-            "stage_work_items": items, "nonfinite_members": nonfinite}
+            "stage_work_items": items, "nonfinite_members": nonfinite, "repeats": len(ens_runs),
+            "ms_repeats": [round(x, 2) for x in ens_runs], "sequential_ms_repeats": [round(x, 2) for x in seq_runs]}
 
 
 def adjoint_leg(device, nsfsi, reps=3, steps=200):
@@ -398,6 +414,7 @@ def arm_config(workload, grid, world):
                   "resident fields larger than the 126 MB L2; no flush"}
 
 
+ENS_REPEATS = 3           # alternating ensemble runs and passes over the plain solves; medians compared
 E2E_REPEATS = 3           # end-to-end runs (upload, K steps, download); the median is reported
 REF_ARM_BUDGET_S = 330.0   # the reference arm's whole run (warm-up and timed steps) stays within minutes
 REF_RATE_ESTIMATE = 1.5e6  # node-RK4-steps/s of the serial reference build on one host core

@@ -156,3 +156,80 @@ def test_profile_commands_parse():
     assert cmds
     for c in cmds:
         bench.arg_parser().parse_args(shlex.split(c))
+
+
+def test_ensemble_leg_alternates_and_compares_medians():
+    """The ensemble leg alternates ensemble runs with passes over the plain solves (ENS_REPEATS of each, on a
+    stand-in module whose device times drift run by run) and compares the medians; the non-finite members are
+    counted once, after the first pass."""
+    calls = []
+
+    class Cfg:
+        def __init__(self, n):
+            self.NI = self.NJ = self.NK = n
+
+    class NsfError(RuntimeError):
+        def __init__(self, code):
+            self.code = code
+
+    ens_ms = iter([100.0, 90.0, 95.0])
+
+    class Ensemble:
+        def __init__(self, cfgs, device=0, tune_cache=None):
+            self.n = len(cfgs)
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *a):
+            return False
+
+        def info(self):
+            return 0, 10, 7
+
+        def march(self, n):
+            pass
+
+        def sync(self):
+            pass
+
+        def march_timed(self, n):
+            calls.append("ens")
+            return next(ens_ms)
+
+    seq_ms = {0: 2.0, 1: 3.0, 2: 2.5}
+
+    class Solver:
+        passes = 0
+
+        def __init__(self, cfg, device=0):
+            self.cfg = cfg
+            self.runs = 0
+
+        def march(self, n):
+            pass
+
+        def sync(self):
+            if self.cfg.NI == 8 and self.runs > 0:  # one member goes non-finite
+                raise NsfError(3)
+
+        def march_timed(self, n):
+            calls.append("seq")
+            t = seq_ms[self.runs] * self.cfg.NI
+            self.runs += 1
+            return t
+
+        def close(self):
+            pass
+
+    m = types.ModuleType("nsfsi")
+    m.NsfError, m.Solver, m.Ensemble = NsfError, Solver, Ensemble
+    m.ensemble_configs = lambda n, steps: [Cfg(8), Cfg(16)]
+    out = bench.ensemble_leg(20, 0, m)
+    assert calls == ["ens", "seq", "seq"] * 3
+    assert out["repeats"] == 3 and out["ms_repeats"] == [100.0, 90.0, 95.0]
+    assert out["sequential_ms_repeats"] == [2.0 * 24, 3.0 * 24, 2.5 * 24]
+    assert out["ms"] == 95.0 and out["sequential_ms"] == 2.5 * 24
+    assert out["speedup_vs_sequential"] == pytest.approx(2.5 * 24 / 95.0)
+    assert out["nonfinite_members"] == 1
+    assert out["value"] == pytest.approx((8 ** 3 + 16 ** 3) * 20 / 0.095)

@@ -413,14 +413,16 @@ nsf_status create_ensemble(const nsf_config* cfgs, uint32_t n, int32_t device, c
 extern "C" {
 
 nsf_status nsf_ensemble_march(nsf_ensemble* e, uint64_t nsteps) {
-  if (!e || !e->graphExec) return NSF_ERR_STATE;
+  if (!e) return NSF_ERR_ARG;
+  if (!e->graphExec) return NSF_ERR_STATE;
   CKE(cudaSetDevice(e->device));
   for (uint64_t q = 0; q < nsteps; ++q) CKE(cudaGraphLaunch(e->graphExec, e->stream));
   return NSF_OK;
 }
 
 nsf_status nsf_ensemble_march_timed(nsf_ensemble* e, uint64_t nsteps, double* ms) {
-  if (!e || !e->graphExec || !ms) return NSF_ERR_STATE;
+  if (!e || !ms) return NSF_ERR_ARG;
+  if (!e->graphExec) return NSF_ERR_STATE;
   CKE(cudaSetDevice(e->device));
   cudaEvent_t a, b;
   CKE(cudaEventCreate(&a));
@@ -438,7 +440,8 @@ nsf_status nsf_ensemble_march_timed(nsf_ensemble* e, uint64_t nsteps, double* ms
 }
 
 nsf_status nsf_ensemble_profile_steps(nsf_ensemble* e, uint64_t nsteps, double* stage_ms, double* step_ms) {
-  if (!e || !e->graphExec || !stage_ms || !step_ms) return NSF_ERR_STATE;
+  if (!e || !stage_ms || !step_ms) return NSF_ERR_ARG;
+  if (!e->graphExec) return NSF_ERR_STATE;
   CKE(cudaSetDevice(e->device));
   std::vector<cudaEvent_t> ev(2 + 8 * nsteps);
   for (auto& x : ev) CKE(cudaEventCreate(&x));
@@ -465,7 +468,8 @@ nsf_status nsf_ensemble_profile_steps(nsf_ensemble* e, uint64_t nsteps, double* 
 }
 
 nsf_status nsf_ensemble_sync(nsf_ensemble* e) {
-  if (!e || !e->graphExec) return NSF_ERR_STATE;
+  if (!e) return NSF_ERR_ARG;
+  if (!e->graphExec) return NSF_ERR_STATE;
   CKE(cudaStreamSynchronize(e->stream));
   for (size_t m = 0; m < e->members.size(); ++m) {
     nsf_status st = nsf_sync(e->members[m]);
@@ -485,7 +489,8 @@ nsf_status nsf_ensemble_member(nsf_ensemble* e, uint32_t m, nsf_solver** member)
 }
 
 nsf_status nsf_ensemble_info(nsf_ensemble* e, int32_t* tile, uint64_t* launches_per_step, uint32_t* work_items) {
-  if (!e || !e->graphExec) return NSF_ERR_STATE;
+  if (!e) return NSF_ERR_ARG;
+  if (!e->graphExec) return NSF_ERR_STATE;
   if (tile) *tile = e->tile;
   if (launches_per_step) *launches_per_step = uint64_t(e->launchesPerStep);
   if (work_items) *work_items = uint32_t(e->plan.nItems);

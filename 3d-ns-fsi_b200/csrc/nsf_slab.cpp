@@ -470,14 +470,16 @@ nsf_status nsf_slab_schedule(const nsf_config* cfg, int32_t nslabs, int32_t worl
 }
 
 nsf_status nsf_slab_group_march(nsf_slab_group* g, uint64_t nsteps) {
-  if (!g || !g->graphExec) return NSF_ERR_STATE;
+  if (!g) return NSF_ERR_ARG;
+  if (!g->graphExec) return NSF_ERR_STATE;
   CKG(cudaSetDevice(g->device));
   for (uint64_t q = 0; q < nsteps; ++q) CKG(cudaGraphLaunch(g->graphExec, g->stream));
   return NSF_OK;
 }
 
 nsf_status nsf_slab_group_march_timed(nsf_slab_group* g, uint64_t nsteps, double* elapsed_ms) {
-  if (!g || !g->graphExec || !elapsed_ms) return NSF_ERR_STATE;
+  if (!g || !elapsed_ms) return NSF_ERR_ARG;
+  if (!g->graphExec) return NSF_ERR_STATE;
   CKG(cudaSetDevice(g->device));
   cudaEvent_t a, b;
   CKG(cudaEventCreate(&a));
@@ -495,7 +497,8 @@ nsf_status nsf_slab_group_march_timed(nsf_slab_group* g, uint64_t nsteps, double
 }
 
 nsf_status nsf_slab_group_sync(nsf_slab_group* g) {
-  if (!g || !g->graphExec) return NSF_ERR_STATE;
+  if (!g) return NSF_ERR_ARG;
+  if (!g->graphExec) return NSF_ERR_STATE;
   CKG(cudaSetDevice(g->device));
   CKG(cudaStreamSynchronize(g->stream));
   nsf_status worst = NSF_OK;

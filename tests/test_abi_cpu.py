@@ -56,3 +56,30 @@ def test_async_download_argument_checks_without_device():
     if not torch.cuda.is_available():
         assert L.nsf_host_alloc(64, ctypes.byref(p)) == 2 and not p.value
     assert L.nsf_host_free(None) == 0
+
+
+def test_every_handle_entry_refuses_a_null_handle():
+    """Every entry point that takes a solver, ensemble or slab-group handle returns NSF_ERR_ARG for a null
+    handle (other arguments null or zero) before any device work; the error-text calls name the null handle
+    and the destroy calls accept it."""
+    import inspect
+    L = nsfsi.lib()
+    src = inspect.getsource(nsfsi.lib)
+    names = [ln.split('"')[1] for ln in src.splitlines() if ln.strip().startswith('"nsf_')]
+    checked = 0
+    for n in names:
+        f = getattr(L, n)
+        args = f.argtypes
+        if not args or args[0] is not ctypes.c_void_p or f.restype is not ctypes.c_int32 or n == "nsf_host_free":
+            continue
+        vals = [None] + [0 if a in (ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t)
+                         else 0.0 if a is ctypes.c_double else None for a in args[1:]]
+        assert f(*vals) == 6, n
+        checked += 1
+    assert checked >= 40
+    assert b"null" in L.nsf_last_error(None)
+    assert b"null" in L.nsf_ensemble_last_error(None)
+    assert b"null" in L.nsf_slab_group_last_error(None)
+    L.nsf_destroy(None)
+    L.nsf_ensemble_destroy(None)
+    L.nsf_slab_group_destroy(None)

@@ -158,6 +158,20 @@ def test_profile_commands_parse():
         bench.arg_parser().parse_args(shlex.split(c))
 
 
+def test_roofline_traffic_comes_from_the_committed_capture():
+    """roofline.traffic is the mean DRAM bytes per stage launch of the committed 256^3 capture: four launches,
+    each within 5 % of its stage's algorithmic bytes (120 / 200 / 200 / 160 B per node), the step within 2 %."""
+    t = bench.profile_traffic("tgv256")
+    assert t is not None and t["source"] == os.path.join("profiles", "k_stage_ws_tgv256_dram.md")
+    nodes = 256 ** 3
+    alg = [120 * nodes, 200 * nodes, 200 * nodes, 160 * nodes]
+    assert len(t["per_stage"]) == 4
+    for got, want in zip(t["per_stage"], alg):
+        assert abs(got / want - 1) < 0.05
+    assert abs(sum(t["per_stage"]) / (bench.BYTES_PER_NODE_STEP * nodes) - 1) < 0.02
+    assert t["per_launch"] == pytest.approx(sum(t["per_stage"]) / 4)
+
+
 def test_ensemble_leg_alternates_and_compares_medians():
     """The ensemble leg alternates ensemble runs with passes over the plain solves (ENS_REPEATS of each, on a
     stand-in module whose device times drift run by run) and compares the medians; the non-finite members are

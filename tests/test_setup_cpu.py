@@ -97,3 +97,46 @@ def test_filter_node_inside_a_later_body_is_refused():
     with pytest.raises(nsfsi.NsfError) as e:
         Solver(text, device=-1)
     assert e.value.code == 4 and "inside another" in str(e.value)
+
+
+def _grid_case(name, n):
+    text = open(nsfsi.case_path(name)).read()
+    for ax in "IJK":
+        text = text.replace("N%s = 48" % ax, "N%s = %d" % (ax, n)).replace("N%s = 128" % ax, "N%s = %d" % (ax, n))
+    return nsfsi.config_parse(text)
+
+
+@pytest.mark.parametrize("n", [0, 1, 2])
+def test_grids_below_the_minimum_node_count_are_refused(n):
+    """An axis with fewer nodes than its boundary type needs (3; 4 for symmetry faces, the reference
+    ConfigFile's minimum counts) is a config error at setup, on a host-only handle, with no device work."""
+    import ctypes
+    L = nsfsi.lib()
+    for name in ("tgv128", "sphere48"):
+        c = _grid_case(name, n)
+        h = ctypes.c_void_p()
+        assert L.nsf_create(ctypes.byref(c), -1, ctypes.byref(h)) == 0
+        try:
+            assert L.nsf_initialize(h) == 1
+            assert b"too few nodes" in L.nsf_last_error(h)
+        finally:
+            L.nsf_destroy(h)
+
+
+def test_smallest_periodic_grid_sets_up():
+    """Three nodes per periodic axis is the smallest grid the setup accepts: one interior fluid node, every
+    face node a periodic boundary node (the reference's fluid ghost type)."""
+    import ctypes
+    L = nsfsi.lib()
+    c = _grid_case("tgv128", 3)
+    h = ctypes.c_void_p()
+    assert L.nsf_create(ctypes.byref(c), -1, ctypes.byref(h)) == 0
+    try:
+        assert L.nsf_initialize(h) == 0
+        types = np.empty(27, dtype=np.uint8)
+        assert L.nsf_get_node_types(h, types.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))) == 0
+        want = np.full(27, 2, dtype=np.uint8)
+        want[13] = 0
+        np.testing.assert_array_equal(types, want)
+    finally:
+        L.nsf_destroy(h)

@@ -112,3 +112,25 @@ def test_oracle_matches_reference_tgv256_one_step():
     text = open(nsfsi.case_path("tgv256")).read()
     compare(text, level=1)
 
+
+
+def _smallest(name, n, periodic_y=True):
+    text = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "3d-ns-fsi_b200", "cases",
+                             name + ".cfg")).read()
+    for ax in "IJK":
+        text = text.replace("N%s = 48" % ax, "N%s = %d" % (ax, n)).replace("N%s = 128" % ax, "N%s = %d" % (ax, n))
+    text = text.replace("  spheres = ( (0.4, 0.5, 0.5, 0.1) );\n", "")
+    if not periodic_y:
+        text = text.replace('bc_y_min = "periodic"', 'bc_y_min = "symmetry"').replace('bc_y_max = "periodic"',
+                                                                                       'bc_y_max = "symmetry"')
+    return text
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build oracle/_ref/ref_runner absent")
+@pytest.mark.parametrize("name,n,periodic_y", [("tgv128", 3, True), ("tgv128", 4, True), ("sphere48", 3, True),
+                                               ("sphere48", 4, False), ("sphere48", 5, False)])
+def test_oracle_matches_reference_on_the_smallest_grids(name, n, periodic_y):
+    """The smallest grids each boundary type allows (3 nodes per periodic or inlet/outlet axis, 4 per
+    symmetry axis): a 3^3 and 4^3 periodic Taylor-Green box and body-free channels with periodic or
+    symmetry y faces match the reference bit for bit."""
+    compare(_smallest(name, n, periodic_y))
